@@ -1,0 +1,495 @@
+"""System, storage, boundary conditions and pair lists of the drop-in API.
+
+Mirrors the Python classes of ESPResSo++ that sit in front of the short-range MD step
+(src/System.py, src/storage/DomainDecomposition.py, src/bc/OrthorhombicBC.py,
+src/esutil/RNG.py, src/VerletList.py, src/FixedPairList.py) on one process.  All
+particle state lives on the GPU behind one C-ABI system handle that the storage
+creates; the classes here keep configuration and forward to the handle.
+"""
+import ctypes
+import math
+import os
+
+import numpy as np
+
+from . import _abi
+from ._abi import call, dptr, i32ptr, i64ptr
+from ._lib import load_library
+
+infinity = float("inf")
+
+_DEFAULT_PRECISION = os.environ.get("ESPP_B200_PRECISION", "fp64")
+
+
+def set_default_precision(precision):
+    """'fp64' (reference arithmetic, plain form) or 'mixed' (FP32 pair forces with int64
+    fixed-point sums, FP64 integrator); used by storages created afterwards."""
+    global _DEFAULT_PRECISION
+    _precision_code(precision)
+    _DEFAULT_PRECISION = precision
+
+
+def _precision_code(p):
+    if p in ("fp64", "double", _abi.PREC_FP64):
+        return _abi.PREC_FP64
+    if p in ("mixed", _abi.PREC_MIXED):
+        return _abi.PREC_MIXED
+    raise ValueError("precision must be 'fp64' or 'mixed', got %r" % (p,))
+
+
+class Real3D(tuple):
+    """3-vector of reals (src/Real3D.hpp)."""
+
+    def __new__(cls, *args):
+        if len(args) == 0:
+            v = (0.0, 0.0, 0.0)
+        elif len(args) == 1:
+            a = args[0]
+            v = (float(a),) * 3 if np.isscalar(a) else tuple(float(x) for x in a)
+        else:
+            v = tuple(float(x) for x in args)
+        if len(v) != 3:
+            raise TypeError("Real3D needs 3 components")
+        return tuple.__new__(cls, v)
+
+    x = property(lambda self: self[0])
+    y = property(lambda self: self[1])
+    z = property(lambda self: self[2])
+
+    def __add__(self, o):
+        return Real3D(self[0] + o[0], self[1] + o[1], self[2] + o[2])
+
+    def __sub__(self, o):
+        return Real3D(self[0] - o[0], self[1] - o[1], self[2] - o[2])
+
+    def __mul__(self, o):
+        if np.isscalar(o):
+            return Real3D(self[0] * o, self[1] * o, self[2] * o)
+        return self[0] * o[0] + self[1] * o[1] + self[2] * o[2]
+
+    __rmul__ = __mul__
+
+    def sqr(self):
+        return self[0] * self[0] + self[1] * self[1] + self[2] * self[2]
+
+    def abs(self):
+        return math.sqrt(self.sqr())
+
+
+class Int3D(tuple):
+    """3-vector of ints (src/Int3D.hpp)."""
+
+    def __new__(cls, *args):
+        if len(args) == 0:
+            v = (0, 0, 0)
+        elif len(args) == 1:
+            a = args[0]
+            v = (int(a),) * 3 if np.isscalar(a) else tuple(int(x) for x in a)
+        else:
+            v = tuple(int(x) for x in args)
+        if len(v) != 3:
+            raise TypeError("Int3D needs 3 components")
+        return tuple.__new__(cls, v)
+
+
+class Tensor(tuple):
+    """Symmetric tensor, components xx, yy, zz, xy, xz, yz (src/Tensor.hpp:125-133)."""
+
+    def __new__(cls, *args):
+        v = tuple(float(x) for x in (args[0] if len(args) == 1 else args))
+        if len(v) != 6:
+            raise TypeError("Tensor needs 6 components")
+        return tuple.__new__(cls, v)
+
+
+class RNG:
+    """esutil.RNG(seed): uniform [0,1) draws on the host (src/esutil/RNG.cpp:40-66).
+    The seed also keys the GPU Langevin noise of a system that uses this RNG."""
+
+    def __init__(self, seed=12345):
+        self.seed = int(seed)
+        self._g = np.random.Generator(np.random.PCG64(self.seed))
+
+    def __call__(self, n=None):
+        if n is None:
+            return float(self._g.random())
+        return int(self._g.integers(0, n))
+
+    def uniform(self):
+        return float(self._g.random())
+
+    def normal(self):
+        return float(self._g.normal())
+
+    def get_seed(self):
+        return self.seed
+
+
+class OrthorhombicBC:
+    """bc.OrthorhombicBC(rng, boxL) (src/bc/OrthorhombicBC.cpp:40-178)."""
+
+    def __init__(self, rng, boxL):
+        self.rng = rng
+        self.boxL = boxL
+
+    @property
+    def boxL(self):
+        return self._boxL
+
+    @boxL.setter
+    def boxL(self, v):
+        self._boxL = Real3D(v)
+
+    def getRandomPos(self):
+        return Real3D(self._boxL[0] * self.rng(), self._boxL[1] * self.rng(),
+                      self._boxL[2] * self.rng())
+
+    def getMinimumImageVector(self, pos1, pos2):
+        d = []
+        for k in range(3):
+            dk = pos1[k] - pos2[k]
+            dk -= round(dk / self._boxL[k]) * self._boxL[k]
+            d.append(dk)
+        return Real3D(d)
+
+    def getFoldedPosition(self, pos, imageBox=None):
+        p = list(pos)
+        img = list(imageBox) if imageBox is not None else [0, 0, 0]
+        for k in range(3):
+            t = int(math.floor(p[k] * (1.0 / self._boxL[k])))
+            img[k] += t
+            p[k] -= t * self._boxL[k]
+        return Real3D(p), Int3D(img)
+
+    def getUnfoldedPosition(self, pos, imageBox):
+        return Real3D([pos[k] + imageBox[k] * self._boxL[k] for k in range(3)])
+
+
+class System:
+    """espressopp.System (src/System.cpp:40-105): holds bc, rng, skin, storage and the
+    short-range interactions; maxCutoff is the largest interaction cutoff."""
+
+    def __init__(self):
+        self.rng = None
+        self.bc = None
+        self._skin = 0.0
+        self._storage = None
+        self.shortRangeInteractions = []
+        self.maxCutoff = 0.0
+
+    @property
+    def skin(self):
+        return self._skin
+
+    @skin.setter
+    def skin(self, v):
+        self._skin = float(v)
+        if self._storage is not None:
+            call(self._storage._lib, "espp_set_skin", self._storage._h, self._skin)
+
+    @property
+    def storage(self):
+        return self._storage
+
+    @storage.setter
+    def storage(self, st):
+        self._storage = st
+
+    def addInteraction(self, interaction, name=None):
+        self.shortRangeInteractions.append(interaction)
+        interaction._attach(self)
+        self.maxCutoff = max(self.maxCutoff, interaction.getMaxCutoff())
+        return True
+
+    def removeInteraction(self, i):
+        ia = self.shortRangeInteractions.pop(i)
+        ia._detach()
+
+    def getInteraction(self, i):
+        return self.shortRangeInteractions[i]
+
+    def getNumberOfInteractions(self):
+        return len(self.shortRangeInteractions)
+
+    def scaleVolume(self, *args):
+        raise NotImplementedError("volume scaling is outside the GPU short-range MD step")
+
+
+class Particle:
+    """Read view of one particle (Storage.getParticle); values are fetched on access."""
+
+    def __init__(self, storage, pid):
+        self._st = storage
+        self.id = int(pid)
+
+    def _get(self):
+        return self._st._fetch(np.array([self.id], np.int64))
+
+    @property
+    def pos(self):
+        return Real3D(self._get()[0][0])
+
+    @property
+    def v(self):
+        return Real3D(self._get()[1][0])
+
+    @property
+    def f(self):
+        return Real3D(self._get()[2][0])
+
+    @property
+    def imageBox(self):
+        return Int3D(self._get()[3][0])
+
+    @property
+    def type(self):
+        return int(self._st._types.get(self.id, 0))
+
+    @property
+    def mass(self):
+        return float(self._st._masses.get(self.id, 1.0))
+
+    def isGhost(self):
+        return False
+
+
+class DomainDecomposition:
+    """storage.DomainDecomposition(system, nodeGrid, cellGrid, halfCellInt) on one node
+    (src/storage/DomainDecomposition.py:84-130, DomainDecomposition.cpp:70-85).
+
+    Creates the GPU system handle.  ``precision`` ('fp64' or 'mixed') selects the pair
+    force arithmetic; it defaults to set_default_precision()."""
+
+    def __init__(self, system, nodeGrid="auto", cellGrid="auto", halfCellInt="auto",
+                 nocheck=False, precision=None):
+        if system.bc is None:
+            raise RuntimeError("system has no boundary conditions")
+        if nodeGrid != "auto" and tuple(Int3D(nodeGrid)) != (1, 1, 1):
+            raise ValueError("the GPU storage holds all particles on one device: nodeGrid "
+                             "must be (1,1,1)")
+        if halfCellInt == "auto":
+            halfCellInt = 1
+        if int(halfCellInt) != 1:
+            raise ValueError("halfCellInt > 1 is not supported by the GPU storage")
+        if cellGrid == "auto":
+            cellGrid = Int3D(2, 2, 2)
+        cellGrid = list(Int3D(cellGrid))
+        for k in range(3):
+            if cellGrid[k] == 1:
+                cellGrid[k] = 2
+        self.system = system
+        self._cellGrid = Int3D(cellGrid)
+        self._lib = load_library()
+        self._h = ctypes.c_void_p()
+        prec = _precision_code(precision if precision is not None else _DEFAULT_PRECISION)
+        self.precision = prec
+        box = np.ascontiguousarray(system.bc.boxL, np.float64)
+        cg = np.ascontiguousarray(self._cellGrid, np.int32)
+        seed = system.rng.get_seed() if system.rng is not None else 12345
+        call(self._lib, "espp_system_create", dptr(box), float(system.skin), i32ptr(cg), prec,
+             int(seed) & 0xFFFFFFFFFFFFFFFF, ctypes.byref(self._h))
+        self._types = {}
+        self._masses = {}
+        self.next_id = 0
+
+    def __del__(self):
+        try:
+            if self._h:
+                self._lib.espp_system_destroy(self._h)
+                self._h = ctypes.c_void_p()
+        except Exception:
+            pass
+
+    # -- particles --------------------------------------------------------------------
+    def addParticles(self, particleList, *properties):
+        """Storage.addParticles (src/storage/Storage.py:233-330).  Known properties: id,
+        type, mass, pos, v; other per-particle properties are accepted and ignored."""
+        if len(particleList) == 0:
+            return
+        props = list(properties) if properties else ["id", "pos"]
+        if "id" not in props or "pos" not in props:
+            raise ValueError("particle properties must include 'id' and 'pos'")
+        n = len(particleList)
+        ids = np.empty(n, np.int64)
+        pos = np.empty((n, 3))
+        vel = np.zeros((n, 3))
+        typ = np.zeros(n, np.int32)
+        mass = np.ones(n)
+        col = {p: k for k, p in enumerate(props)}
+        for r, part in enumerate(particleList):
+            ids[r] = int(part[col["id"]])
+            pos[r] = tuple(part[col["pos"]])
+            if "v" in col:
+                vel[r] = tuple(part[col["v"]])
+            if "type" in col:
+                typ[r] = int(part[col["type"]])
+            if "mass" in col:
+                mass[r] = float(part[col["mass"]])
+        call(self._lib, "espp_add_particles", self._h, n, i64ptr(ids), i32ptr(typ),
+             dptr(mass), dptr(pos.reshape(-1)), dptr(vel.reshape(-1)))
+        for k in range(n):
+            self._types[int(ids[k])] = int(typ[k])
+            self._masses[int(ids[k])] = float(mass[k])
+        self.next_id = max(self.next_id, int(ids.max()) + 1)
+
+    def addParticle(self, pid, pos):
+        self.addParticles([[pid, Real3D(pos)]], "id", "pos")
+
+    def decompose(self):
+        call(self._lib, "espp_decompose", self._h)
+
+    def getParticle(self, pid):
+        if int(pid) not in self._types:
+            return None
+        return Particle(self, pid)
+
+    def particleExists(self, pid):
+        return int(pid) in self._types
+
+    def getRealParticleIDs(self):
+        return sorted(self._types)
+
+    def getNRealParticles(self):
+        return len(self._types)
+
+    def modifyParticle(self, pid, prop, value):
+        ids = np.array([int(pid)], np.int64)
+        v = np.ascontiguousarray(tuple(value), np.float64)
+        if prop == "pos":
+            call(self._lib, "espp_set_particles", self._h, 1, i64ptr(ids), dptr(v), None)
+        elif prop == "v":
+            call(self._lib, "espp_set_particles", self._h, 1, i64ptr(ids), None, dptr(v))
+        else:
+            raise ValueError("only 'pos' and 'v' can be modified on the GPU storage")
+
+    def getCellGrid(self):
+        return self._cellGrid
+
+    def getNodeGrid(self):
+        return Int3D(1, 1, 1)
+
+    def _fetch(self, ids):
+        n = len(ids)
+        pos = np.zeros((n, 3))
+        vel = np.zeros((n, 3))
+        frc = np.zeros((n, 3))
+        img = np.zeros((n, 3), np.int32)
+        call(self._lib, "espp_get_particles", self._h, n, i64ptr(ids), dptr(pos), dptr(vel),
+             dptr(frc), i32ptr(img))
+        return pos, vel, frc, img
+
+    def getAll(self):
+        """(ids, pos, v, f, imageBox) arrays of all particles, sorted by id."""
+        ids = np.array(sorted(self._types), np.int64)
+        pos, vel, frc, img = self._fetch(ids)
+        return ids, pos, vel, frc, img
+
+    def setVelocities(self, ids, vel):
+        ids = np.ascontiguousarray(ids, np.int64)
+        v = np.ascontiguousarray(vel, np.float64).reshape(-1)
+        call(self._lib, "espp_set_particles", self._h, len(ids), i64ptr(ids), None, dptr(v))
+
+
+class VerletList:
+    """VerletList(system, cutoff, exclusionlist=[], useBuffers=True, useSOA=False)
+    (src/VerletList.py:66-126, src/VerletList.cpp:196-536).  ``useBuffers`` and
+    ``useSOA`` select CPU code paths in the reference and do not change the pair set;
+    they are accepted and ignored."""
+
+    def __init__(self, system, cutoff, exclusionlist=[], useBuffers=True, useSOA=False):
+        if system.storage is None:
+            raise RuntimeError("system has no storage")
+        self.system = system
+        self.cutoff = float(cutoff)
+        st = system.storage
+        ex = np.ascontiguousarray(list(exclusionlist), np.int64).reshape(-1)
+        call(st._lib, "espp_vl_create", st._h, self.cutoff, len(ex) // 2,
+             i64ptr(ex) if len(ex) else None)
+        self._connected = True
+
+    @property
+    def _st(self):
+        return self.system.storage
+
+    @property
+    def builds(self):
+        v = ctypes.c_int64()
+        call(self._st._lib, "espp_vl_builds", self._st._h, ctypes.byref(v))
+        return v.value
+
+    def totalSize(self):
+        v = ctypes.c_int64()
+        call(self._st._lib, "espp_vl_size", self._st._h, ctypes.byref(v))
+        return v.value
+
+    localSize = totalSize
+
+    def exclude(self, exclusionlist):
+        ex = np.ascontiguousarray(list(exclusionlist), np.int64).reshape(-1)
+        call(self._st._lib, "espp_vl_create", self._st._h, self.cutoff, len(ex) // 2,
+             i64ptr(ex) if len(ex) else None)
+
+    def rebuild(self):
+        call(self._st._lib, "espp_vl_rebuild", self._st._h)
+
+    def pairs(self):
+        """All pairs as an (n, 2) int64 array of (smaller id, larger id), sorted."""
+        n = self.totalSize()
+        out = np.zeros((max(n, 1), 2), np.int64)
+        got = ctypes.c_int64()
+        call(self._st._lib, "espp_vl_pairs", self._st._h, n, i64ptr(out), ctypes.byref(got))
+        return out[: got.value]
+
+    def getAllPairs(self):
+        """Like the reference's PMI proxy: one list of (id1, id2) tuples per worker."""
+        return [[(int(a), int(b)) for a, b in self.pairs()]]
+
+    def getVerletCutoff(self):
+        return self.cutoff + self.system.skin
+
+    def connect(self):
+        self._connected = True
+
+    def disconnect(self):
+        self._connected = False
+
+    def resetTimers(self):
+        pass
+
+    def getTimers(self):
+        return [(0.0,)]
+
+
+class FixedPairList:
+    """FixedPairList(storage) (src/FixedPairList.py:60-148, FixedPairList.cpp:88-315)."""
+
+    def __init__(self, storage):
+        self.storage = storage
+        self._bonds = []
+
+    def add(self, pid1, pid2):
+        self.addBonds([(pid1, pid2)])
+        return True
+
+    def addBonds(self, bondlist):
+        b = np.ascontiguousarray([(int(a), int(c)) for a, c in bondlist], np.int64).reshape(-1)
+        if len(b) == 0:
+            return
+        call(self.storage._lib, "espp_bonds_add", self.storage._h, len(b) // 2, i64ptr(b))
+        self._bonds.extend((min(int(a), int(c)), max(int(a), int(c))) for a, c in bondlist)
+
+    def getBonds(self):
+        return [list(self._bonds)]
+
+    def size(self):
+        return len(self._bonds)
+
+    totalSize = size
+
+    def getLongtimeMaxBondSqr(self):
+        v = ctypes.c_double()
+        call(self.storage._lib, "espp_bonds_max_sqr", self.storage._h, ctypes.byref(v))
+        return v.value
+
+    def getLongtimeMaxBond(self):
+        return math.sqrt(self.getLongtimeMaxBondSqr())

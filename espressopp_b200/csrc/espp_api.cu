@@ -1,0 +1,1092 @@
+// espp_api.cu - host runtime and C ABI (include/espp_b200.h) of the B200 MD step.
+//
+// One espp_system owns all particles of one box on the current CUDA device, in
+// cell-sorted SoA arrays (two copies, swapped at each re-sort), plus the Verlet list,
+// force buffers and the device scalars of the rebuild criterion.  The run loop follows
+// VelocityVerlet::run (src/integrator/VelocityVerlet.cpp:63-169): start-of-run force
+// with the Langevin heat-up factor, then per step integrate1 -> (re-sort + list build
+// when the accumulated max displacement exceeds skin/2) -> forces -> aftCalcF ->
+// integrate2.  integrate2 of step n and integrate1 of step n+1 run as one kernel.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <new>
+#include <string>
+#include <unordered_map>
+#include <utility>
+#include <vector>
+
+#include "../../include/espp_b200.h"
+#include "espp_internal.h"
+
+using namespace espp;
+
+namespace {
+
+thread_local std::string g_err;
+
+struct Fail {
+  int code;
+  std::string msg;
+};
+
+[[noreturn]] void raise(int code, const std::string& msg) { throw Fail{code, msg}; }
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess)
+    raise(ESPP_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class T>
+T* dalloc(size_t count) {
+  void* p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    raise(ESPP_ENOMEM, std::string("device allocation of ") +
+                           std::to_string(count * sizeof(T)) + " bytes failed");
+  }
+  return (T*)p;
+}
+
+template <class T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+}  // namespace
+
+struct espp_system {
+  // configuration
+  double L[3];
+  double skin;
+  int nc[3];
+  int precision;
+  uint64_t seed;
+  int device = 0;
+  cudaStream_t st = nullptr;
+
+  // particles on the device
+  int n = 0, cap = 0;
+  ParticleArrays A{}, B{};
+  int4* posq = nullptr;
+  int32_t* pcell = nullptr;
+  int32_t* cellStart = nullptr;
+  int32_t* nl = nullptr;
+  int32_t* nn = nullptr;
+  int32_t* nnZero = nullptr;  // all-zero counts (no pair interaction)
+  int K = 0;
+  long long* ffix = nullptr;
+  double* f64 = nullptr;
+  double* ftot = nullptr;
+  RebuildScratch scr{};
+  bool binned = false;
+
+  // id-indexed structures
+  int64_t idMin = 0;
+  int idSpan = 0;
+  int32_t* id2idx = nullptr;
+  int32_t* bondStart = nullptr;
+  int64_t* bondPartner = nullptr;
+  uint8_t* langExcl = nullptr;
+  int32_t* exclStart = nullptr;
+  int64_t* exclIds = nullptr;
+  bool idDirty = true;
+
+  // device scalars
+  unsigned* err = nullptr;
+  unsigned long long* maxSq = nullptr;
+  double* maxDist = nullptr;
+  int* flag = nullptr;
+  double* obs = nullptr;
+  double* partials = nullptr;
+  int partialsCap = 0;
+  int* hflag = nullptr;  // pinned
+
+  // Verlet list
+  bool has_vl = false;
+  double vl_cut = 0.0;
+  std::vector<std::pair<int64_t, int64_t>> vlExcl;
+  int64_t builds = 0;
+
+  // potentials
+  LJTable lj{};
+  LJPair* d_lj = nullptr;
+  LJPairF* d_ljf = nullptr;
+  bool lj_any = false;
+  FENEParams fene{};
+  std::vector<std::pair<int64_t, int64_t>> bonds;
+
+  // integrator
+  double dt = 0.005;
+  int64_t step = 0;
+  int64_t nResorts = 0;
+  bool resortFlag = true;
+  bool lang_on = false;
+  double gamma = 0.0, temperature = 0.0;
+  std::vector<int64_t> langExclIds;
+  int capMode = ESPP_CAP_OFF;
+  double cap3[3] = {0, 0, 0};
+  int tpp = 4;
+  double timers[10] = {0};
+
+  // host id list (all particle ids, for the id map) and the largest type present
+  std::vector<int64_t> allIds;
+  int maxType = 0;
+
+  DevView view() const {
+    DevView d{};
+    d.a = A;
+    d.n = n;
+    d.cap = cap;
+    for (int k = 0; k < 3; ++k) {
+      d.L[k] = L[k];
+      d.invL[k] = 1.0 / L[k];
+      d.halfL[k] = 0.5 * L[k];
+      d.cellSize[k] = (L[k] - 0.0) / double(nc[k]);
+      d.invCellSize[k] = 1.0 / d.cellSize[k];
+      d.nc[k] = nc[k];
+      d.fixScale[k] = kFix / L[k];
+      d.fixUnit[k] = (float)(L[k] / kFix);
+    }
+    d.ncells = nc[0] * nc[1] * nc[2];
+    d.posq = posq;
+    d.pcell = pcell;
+    d.cellStart = cellStart;
+    d.nl = nl;
+    d.nn = nn;
+    d.K = K;
+    d.ffix = ffix;
+    d.f64 = f64;
+    d.ftot = ftot;
+    d.idMin = idMin;
+    d.idSpan = idSpan;
+    d.id2idx = id2idx;
+    d.bondStart = bondStart;
+    d.bondPartner = bondPartner;
+    d.langExcl = langExcl;
+    d.exclStart = exclStart;
+    d.exclIds = exclIds;
+    d.lj = d_lj;
+    d.ljf = d_ljf;
+    d.ntypes = lj.ntypes;
+    d.ljSingle = lj.single;
+    int capped = 0;
+    for (int k = 0; k < kMaxTypes * kMaxTypes; ++k)
+      if (lj.p[k].set && lj.p[k].caprad > 0) capped = 1;
+    d.ljCapped = capped;
+    d.err = err;
+    d.maxSq = maxSq;
+    return d;
+  }
+};
+
+namespace {
+
+void free_particles(ParticleArrays& a) {
+  dfree(a.x);
+  dfree(a.v);
+  dfree(a.id);
+  dfree(a.type);
+  dfree(a.mass);
+  dfree(a.img);
+}
+
+void alloc_particles(ParticleArrays& a, int cap) {
+  a.x = dalloc<double>(3 * (size_t)cap);
+  a.v = dalloc<double>(3 * (size_t)cap);
+  a.id = dalloc<int64_t>(cap);
+  a.type = dalloc<int32_t>(cap);
+  a.mass = dalloc<double>(cap);
+  a.img = dalloc<int32_t>(3 * (size_t)cap);
+}
+
+void sync(espp_system* s) { cuda_check(cudaStreamSynchronize(s->st), "stream synchronize"); }
+
+// Host copy of every particle in storage order.
+struct HostParticles {
+  std::vector<int64_t> id;
+  std::vector<int32_t> type, img;
+  std::vector<double> mass, x, v, f;  // interleaved 3-vectors
+};
+
+template <class T>
+void copy_soa_down(espp_system* s, std::vector<T>& out, const T* dsrc, int comps) {
+  std::vector<T> tmp((size_t)comps * s->cap);
+  if (s->cap)
+    cuda_check(cudaMemcpy(tmp.data(), dsrc, sizeof(T) * tmp.size(), cudaMemcpyDeviceToHost),
+               "download");
+  out.resize((size_t)comps * s->n);
+  for (int i = 0; i < s->n; ++i)
+    for (int c = 0; c < comps; ++c) out[(size_t)comps * i + c] = tmp[(size_t)c * s->cap + i];
+}
+
+HostParticles download(espp_system* s, bool withForce) {
+  sync(s);
+  HostParticles h;
+  copy_soa_down(s, h.id, s->A.id, 1);
+  copy_soa_down(s, h.type, s->A.type, 1);
+  copy_soa_down(s, h.mass, s->A.mass, 1);
+  copy_soa_down(s, h.x, s->A.x, 3);
+  copy_soa_down(s, h.v, s->A.v, 3);
+  copy_soa_down(s, h.img, s->A.img, 3);
+  if (withForce) copy_soa_down(s, h.f, s->ftot, 3);
+  return h;
+}
+
+template <class T>
+void copy_soa_up(espp_system* s, T* ddst, const std::vector<T>& in, int comps) {
+  std::vector<T> tmp((size_t)comps * s->cap, T(0));
+  for (int i = 0; i < s->n; ++i)
+    for (int c = 0; c < comps; ++c) tmp[(size_t)c * s->cap + i] = in[(size_t)comps * i + c];
+  cuda_check(cudaMemcpy(ddst, tmp.data(), sizeof(T) * tmp.size(), cudaMemcpyHostToDevice),
+             "upload");
+}
+
+void free_buffers(espp_system* s) {
+  free_particles(s->A);
+  free_particles(s->B);
+  dfree(s->posq);
+  dfree(s->pcell);
+  dfree(s->nl);
+  dfree(s->nn);
+  dfree(s->nnZero);
+  dfree(s->ffix);
+  dfree(s->f64);
+  dfree(s->ftot);
+  dfree(s->scr.cellOf);
+  dfree(s->scr.slot);
+  dfree(s->scr.perm);
+}
+
+// Reallocates the per-particle buffers for cap >= n and uploads h.
+void upload(espp_system* s, const HostParticles& h) {
+  int n = (int)h.id.size();
+  if (n > s->cap) {
+    free_buffers(s);
+    int cap = std::max(n, 32);
+    cap = (cap + 31) / 32 * 32;
+    s->cap = cap;
+    alloc_particles(s->A, cap);
+    alloc_particles(s->B, cap);
+    s->posq = dalloc<int4>(cap);
+    s->pcell = dalloc<int32_t>(cap);
+    s->nn = dalloc<int32_t>(cap);
+    s->nnZero = dalloc<int32_t>(cap);
+    cuda_check(cudaMemset(s->nnZero, 0, sizeof(int32_t) * cap), "memset");
+    s->ffix = dalloc<long long>(3 * (size_t)cap);
+    s->f64 = dalloc<double>(3 * (size_t)cap);
+    s->ftot = dalloc<double>(3 * (size_t)cap);
+    s->scr.cellOf = dalloc<int32_t>(cap);
+    s->scr.slot = dalloc<int32_t>(cap);
+    s->scr.perm = dalloc<int32_t>(cap);
+    cuda_check(cudaMemset(s->nn, 0, sizeof(int32_t) * cap), "memset");
+    s->K = 0;
+    dfree(s->nl);
+  }
+  s->n = n;
+  copy_soa_up(s, s->A.id, h.id, 1);
+  copy_soa_up(s, s->A.type, h.type, 1);
+  copy_soa_up(s, s->A.mass, h.mass, 1);
+  copy_soa_up(s, s->A.x, h.x, 3);
+  copy_soa_up(s, s->A.v, h.v, 3);
+  copy_soa_up(s, s->A.img, h.img, 3);
+  std::vector<double> f = h.f;
+  if (f.size() != h.x.size()) f.assign(h.x.size(), 0.0);
+  copy_soa_up(s, s->ftot, f, 3);
+  cuda_check(cudaMemset(s->ffix, 0, sizeof(long long) * 3 * s->cap), "memset");
+  cuda_check(cudaMemset(s->f64, 0, sizeof(double) * 3 * s->cap), "memset");
+  s->binned = false;
+}
+
+// Dense id map, bond and exclusion CSRs indexed by id - idMin.
+void rebuild_id_tables(espp_system* s) {
+  dfree(s->id2idx);
+  dfree(s->bondStart);
+  dfree(s->bondPartner);
+  dfree(s->langExcl);
+  dfree(s->exclStart);
+  dfree(s->exclIds);
+  if (s->allIds.empty()) {
+    s->idMin = 0;
+    s->idSpan = 0;
+    s->idDirty = false;
+    return;
+  }
+  auto mm = std::minmax_element(s->allIds.begin(), s->allIds.end());
+  s->idMin = *mm.first;
+  int64_t span = *mm.second - *mm.first + 1;
+  if (span > 4 * (int64_t)s->allIds.size() + (1 << 20) || span > (1LL << 31) - 2)
+    raise(ESPP_ERANGE, "particle ids are too sparse for the dense id map (span " +
+                           std::to_string(span) + ")");
+  s->idSpan = (int)span;
+  s->id2idx = dalloc<int32_t>(span);
+  cuda_check(cudaMemset(s->id2idx, 0xff, sizeof(int32_t) * span), "memset");
+  auto csr = [&](const std::vector<std::pair<int64_t, int64_t>>& pairs, int32_t*& dstart,
+                 int64_t*& dids) {
+    std::vector<int32_t> start(span + 1, 0);
+    for (auto& p : pairs) {
+      start[p.first - s->idMin + 1]++;
+      start[p.second - s->idMin + 1]++;
+    }
+    for (int64_t k = 0; k < span; ++k) start[k + 1] += start[k];
+    std::vector<int64_t> ids(std::max<int64_t>(start[span], 1));
+    std::vector<int32_t> fill(start.begin(), start.end() - 1);
+    for (auto& p : pairs) {
+      ids[fill[p.first - s->idMin]++] = p.second;
+      ids[fill[p.second - s->idMin]++] = p.first;
+    }
+    dstart = dalloc<int32_t>(span + 1);
+    dids = dalloc<int64_t>(ids.size());
+    cuda_check(cudaMemcpy(dstart, start.data(), sizeof(int32_t) * (span + 1),
+                          cudaMemcpyHostToDevice), "upload");
+    cuda_check(cudaMemcpy(dids, ids.data(), sizeof(int64_t) * ids.size(),
+                          cudaMemcpyHostToDevice), "upload");
+  };
+  for (auto& b : s->bonds)
+    if (b.first < s->idMin || b.second < s->idMin || b.first - s->idMin >= span ||
+        b.second - s->idMin >= span)
+      raise(ESPP_EINVAL, "bond partner does not exist");
+  csr(s->bonds, s->bondStart, s->bondPartner);
+  std::vector<std::pair<int64_t, int64_t>> ex;
+  for (auto& e : s->vlExcl)
+    if (e.first >= s->idMin && e.second >= s->idMin && e.first - s->idMin < span &&
+        e.second - s->idMin < span)
+      ex.push_back(e);
+  if (!ex.empty()) csr(ex, s->exclStart, s->exclIds);
+  std::vector<uint8_t> le(span, 0);
+  for (int64_t id : s->langExclIds)
+    if (id >= s->idMin && id - s->idMin < span) le[id - s->idMin] = 1;
+  s->langExcl = dalloc<uint8_t>(span);
+  cuda_check(cudaMemcpy(s->langExcl, le.data(), span, cudaMemcpyHostToDevice), "upload");
+  s->idDirty = false;
+  s->binned = false;
+}
+
+unsigned read_err(espp_system* s) {
+  unsigned e = 0;
+  cuda_check(cudaMemcpyAsync(&e, s->err, sizeof(unsigned), cudaMemcpyDeviceToHost, s->st),
+             "error word");
+  sync(s);
+  return e;
+}
+
+void check_err(espp_system* s) {
+  unsigned e = read_err(s);
+  if (!e) return;
+  cuda_check(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->st), "memset");
+  if (e & kErrOutside)
+    raise(ESPP_ENAN, "a particle has moved to outer space (non-finite coordinate)");
+  if (e & kErrFixOverflow)
+    raise(ESPP_ERANGE, "force beyond the int64 2^-32 fixed-point range (|F| >= 1e9)");
+  if (e & kErrBondMissing) raise(ESPP_ESTATE, "bond partner not present");
+  if (e & kErrIdRange) raise(ESPP_ESTATE, "particle id outside the id map");
+  if (e & kErrNlOverflow) raise(ESPP_EOVERFLOW, "Verlet list capacity exceeded");
+}
+
+// Re-sort the particles by cell (fold = Storage::decompose semantics).
+void bin(espp_system* s, bool fold) {
+  if (s->idDirty) rebuild_id_tables(s);
+  DevView d = s->view();
+  if (s->n == 0) {
+    cuda_check(cudaMemsetAsync(s->cellStart, 0, sizeof(int32_t) * (d.ncells + 1), s->st),
+               "memset");
+    s->binned = true;
+    return;
+  }
+  launch_fold_bin(d, s->scr, fold, s->st);
+  launch_sort_cells(d, s->scr, s->st);
+  d = s->view();  // fold updated A in place
+  launch_gather(d, s->A, s->B, s->scr, s->st);
+  std::swap(s->A, s->B);
+  d = s->view();
+  launch_id_map(d, s->st);
+  cuda_check(cudaGetLastError(), "re-binning kernels");
+  s->binned = true;
+}
+
+int estimate_K(espp_system* s) {
+  double V = s->L[0] * s->L[1] * s->L[2];
+  double rho = s->n / V;
+  double rcut = s->vl_cut + s->skin;
+  double expected = rho * 4.0 / 3.0 * M_PI * rcut * rcut * rcut;
+  int K = (int)std::ceil(expected * 1.6) + 32;
+  return (K + 7) / 8 * 8;
+}
+
+void build_list(espp_system* s) {
+  if (!s->has_vl) return;
+  if (!s->binned) bin(s, false);
+  double cutVerlet = s->vl_cut + s->skin;
+  double cutsq = cutVerlet * cutVerlet;
+  if (s->K == 0 || !s->nl) {
+    s->K = estimate_K(s);
+    dfree(s->nl);
+    s->nl = dalloc<int32_t>((size_t)s->K * s->cap);
+  }
+  for (int attempt = 0; attempt < 6; ++attempt) {
+    DevView d = s->view();
+    launch_build_nl(d, cutsq, s->st);
+    cuda_check(cudaGetLastError(), "Verlet list kernel");
+    unsigned e = read_err(s);
+    if (!(e & kErrNlOverflow)) break;
+    cuda_check(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->st), "memset");
+    s->K *= 2;
+    dfree(s->nl);
+    s->nl = dalloc<int32_t>((size_t)s->K * s->cap);
+  }
+  check_err(s);
+  s->builds++;
+}
+
+void decompose(espp_system* s) {
+  bin(s, true);
+  check_err(s);
+  build_list(s);
+}
+
+void upload_lj(espp_system* s) {
+  // the table covers every particle type present, unset pairs interact with nothing
+  int nt = std::max(s->lj.ntypes, s->maxType + 1);
+  s->lj.ntypes = nt;
+  std::vector<LJPair> compact((size_t)nt * nt);
+  for (int a = 0; a < nt; ++a)
+    for (int b = 0; b < nt; ++b) compact[(size_t)a * nt + b] = s->lj.p[a * kMaxTypes + b];
+  LJTable t{};
+  t.ntypes = nt;
+  for (size_t k = 0; k < compact.size(); ++k) t.p[k] = compact[k];
+  std::vector<LJPairF> f(kMaxTypes * kMaxTypes);
+  make_float_table(t, f.data());
+  dfree(s->d_lj);
+  dfree(s->d_ljf);
+  s->d_lj = dalloc<LJPair>(std::max<size_t>(compact.size(), 1));
+  s->d_ljf = dalloc<LJPairF>(std::max<size_t>(compact.size(), 1));
+  cuda_check(cudaMemcpy(s->d_lj, t.p, sizeof(LJPair) * compact.size(), cudaMemcpyHostToDevice),
+             "upload");
+  cuda_check(cudaMemcpy(s->d_ljf, f.data(), sizeof(LJPairF) * compact.size(),
+                        cudaMemcpyHostToDevice), "upload");
+  s->lj.single = (nt == 1 && compact[0].set) ? 1 : 0;
+}
+
+void forces(espp_system* s) {
+  DevView d = s->view();
+  if (!s->has_vl || !s->lj_any) d.nn = s->nnZero;  // no pair term: bonds only
+  launch_forces(d, s->precision == ESPP_PREC_MIXED, s->fene, s->tpp, s->st);
+}
+
+
+IntegrateArgs integrate_args(espp_system* s) {
+  IntegrateArgs a{};
+  a.mixed = s->precision == ESPP_PREC_MIXED;
+  a.dt = s->dt;
+  a.langevin = s->lang_on ? 1 : 0;
+  a.pref1 = -s->gamma;
+  a.pref2 = std::sqrt(24.0 * s->temperature * s->gamma / s->dt);
+  a.capMode = s->capMode;
+  for (int k = 0; k < 3; ++k) a.cap[k] = s->cap3[k];
+  a.seed = s->seed;
+  return a;
+}
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+// VelocityVerlet::run (src/integrator/VelocityVerlet.cpp:63-169).
+void run(espp_system* s, int64_t nsteps) {
+  const double t0 = now_s();
+  double tResort = 0.0;
+  s->nResorts = 0;
+  const double skinHalf = 0.5 * s->skin;
+  if (s->idDirty) rebuild_id_tables(s);
+  if (s->resortFlag) {
+    double tr = now_s();
+    decompose(s);
+    cuda_check(cudaMemsetAsync(s->maxDist, 0, sizeof(double), s->st), "memset");
+    s->resortFlag = false;
+    tResort += now_s() - tr;
+  } else if (s->has_vl && !s->binned) {
+    build_list(s);
+  }
+  if (!s->binned) bin(s, false);
+  cuda_check(cudaMemsetAsync(s->maxSq, 0, sizeof(unsigned long long), s->st), "memset");
+  // start-of-run force (recalc1 = heatUp: pref2 * sqrt(3); recalc2 restores it)
+  IntegrateArgs a = integrate_args(s);
+  forces(s);
+  IntegrateArgs a0 = a;
+  a0.pref2 = a.pref2 * std::sqrt(3.0);
+  a0.phase = 1;
+  a0.step = s->step;
+  a0.do_i2 = 0;
+  a0.do_i1 = nsteps > 0 ? 1 : 0;
+  a0.storeFtot = nsteps > 0 ? 0 : 1;
+  launch_integrate(s->view(), a0, s->st);
+  cuda_check(cudaGetLastError(), "start-of-run kernels");
+  for (int64_t i = 0; i < nsteps; ++i) {
+    DevView d = s->view();
+    launch_decide(d, s->maxDist, s->flag, skinHalf, s->st);
+    cuda_check(cudaMemcpyAsync(s->hflag, s->flag, sizeof(int), cudaMemcpyDeviceToHost, s->st),
+               "flag");
+    sync(s);
+    if (*s->hflag) {
+      double tr = now_s();
+      decompose(s);
+      s->nResorts++;
+      tResort += now_s() - tr;
+    }
+    forces(s);
+    IntegrateArgs ai = a;
+    ai.phase = 0;
+    ai.step = s->step;
+    ai.do_i2 = 1;
+    ai.do_i1 = (i + 1 < nsteps) ? 1 : 0;
+    ai.storeFtot = (i + 1 < nsteps) ? 0 : 1;
+    launch_integrate(s->view(), ai, s->st);
+    cuda_check(cudaGetLastError(), "step kernels");
+    s->step++;
+  }
+  sync(s);
+  check_err(s);
+  const double t1 = now_s();
+  s->timers[0] = t1 - t0;
+  s->timers[8] = tResort;
+  s->timers[9] = s->timers[0] - tResort;
+}
+
+double* obs_partials(espp_system* s, int& nb) {
+  nb = observable_blocks(s->n);
+  if (nb * 7 > s->partialsCap) {
+    dfree(s->partials);
+    s->partialsCap = nb * 7;
+    s->partials = dalloc<double>(s->partialsCap);
+  }
+  return s->partials;
+}
+
+void prepare_observables(espp_system* s) {
+  if (s->idDirty) rebuild_id_tables(s);
+  if (s->resortFlag && !s->binned) bin(s, false);
+  if (s->has_vl && !s->binned) build_list(s);
+  if (!s->binned) bin(s, false);
+}
+
+void observable(espp_system* s, int which, int energy, double out[7]) {
+  prepare_observables(s);
+  for (int k = 0; k < 7; ++k) out[k] = 0.0;
+  if (s->n == 0) return;
+  int nb;
+  double* part = obs_partials(s, nb);
+  DevView d = s->view();
+  if (which == ESPP_IA_LJ) {
+    if (!s->has_vl || !s->lj_any) return;
+    launch_lj_observables(d, part, nb, s->obs, energy, s->st);
+  } else if (which == ESPP_IA_FENE) {
+    if (!s->fene.on) return;
+    launch_fene_observables(d, s->fene, part, nb, s->obs, energy, s->st);
+  } else {
+    raise(ESPP_EINVAL, "unknown interaction kind");
+  }
+  cuda_check(cudaGetLastError(), "observable kernels");
+  cuda_check(cudaMemcpyAsync(out, s->obs, sizeof(double) * 7, cudaMemcpyDeviceToHost, s->st),
+             "download");
+  sync(s);
+}
+
+espp_system* checked(espp_system* s) {
+  if (!s) raise(ESPP_EINVAL, "null system handle");
+  cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
+  return s;
+}
+
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    return ESPP_OK;
+  } catch (const Fail& e) {
+    g_err = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_err = "host allocation failed";
+    return ESPP_ENOMEM;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return ESPP_EINVAL;
+  }
+}
+
+void destroy(espp_system* s) {
+  if (!s) return;
+  cudaSetDevice(s->device);
+  if (s->st) cudaStreamSynchronize(s->st);
+  free_buffers(s);
+  dfree(s->cellStart);
+  dfree(s->scr.cellCount);
+  dfree(s->id2idx);
+  dfree(s->bondStart);
+  dfree(s->bondPartner);
+  dfree(s->langExcl);
+  dfree(s->exclStart);
+  dfree(s->exclIds);
+  dfree(s->err);
+  dfree(s->maxSq);
+  dfree(s->maxDist);
+  dfree(s->flag);
+  dfree(s->obs);
+  dfree(s->partials);
+  dfree(s->d_lj);
+  dfree(s->d_ljf);
+  if (s->hflag) cudaFreeHost(s->hflag);
+  if (s->st) cudaStreamDestroy(s->st);
+  delete s;
+}
+
+}  // namespace
+
+extern "C" {
+
+int espp_abi_version(void) { return 1; }
+
+size_t espp_last_error(char* buf, size_t cap) {
+  if (buf && cap) {
+    size_t n = std::min(cap - 1, g_err.size());
+    std::memcpy(buf, g_err.data(), n);
+    buf[n] = 0;
+  }
+  return g_err.size();
+}
+
+int espp_system_create(const double box[3], double skin, const int32_t cell_grid[3],
+                       int32_t precision, uint64_t seed, espp_system** out) {
+  return guard([&] {
+    if (!box || !cell_grid || !out) raise(ESPP_EINVAL, "null argument");
+    for (int i = 0; i < 3; ++i) {
+      if (!(box[i] > 0)) raise(ESPP_EINVAL, "box lengths must be positive");
+      if (cell_grid[i] <= 0) raise(ESPP_EINVAL, "cell grid dimensions have to be positive");
+      if (cell_grid[i] < 3)
+        raise(ESPP_ERANGE,
+              "the GPU storage needs at least 3 cells per dimension (box >= 3 (cutoff + skin))");
+    }
+    if (precision != ESPP_PREC_FP64 && precision != ESPP_PREC_MIXED)
+      raise(ESPP_EINVAL, "unknown precision mode");
+    int ndev = 0;
+    cuda_check(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+    if (ndev <= 0) raise(ESPP_ECUDA, "no CUDA device");
+    std::unique_ptr<espp_system> s(new espp_system());
+    cuda_check(cudaGetDevice(&s->device), "cudaGetDevice");
+    for (int i = 0; i < 3; ++i) {
+      s->L[i] = box[i];
+      s->nc[i] = cell_grid[i];
+    }
+    s->skin = skin;
+    s->precision = precision;
+    s->seed = seed;
+    cuda_check(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking), "stream");
+    const long long ncells = (long long)cell_grid[0] * cell_grid[1] * cell_grid[2];
+    if (ncells > (1LL << 30)) raise(ESPP_ERANGE, "cell grid too large");
+    s->cellStart = dalloc<int32_t>(ncells + 1);
+    s->scr.cellCount = dalloc<int32_t>(ncells);
+    cuda_check(cudaMemset(s->cellStart, 0, sizeof(int32_t) * (ncells + 1)), "memset");
+    s->err = dalloc<unsigned>(1);
+    s->maxSq = dalloc<unsigned long long>(1);
+    s->maxDist = dalloc<double>(1);
+    s->flag = dalloc<int>(1);
+    s->obs = dalloc<double>(8);
+    cuda_check(cudaMemset(s->err, 0, sizeof(unsigned)), "memset");
+    cuda_check(cudaMemset(s->maxSq, 0, sizeof(unsigned long long)), "memset");
+    cuda_check(cudaMemset(s->maxDist, 0, sizeof(double)), "memset");
+    cuda_check(cudaMallocHost(&s->hflag, sizeof(int)), "pinned flag");
+    s->lj.ntypes = 1;
+    upload_lj(s.get());
+    *out = s.release();
+  });
+}
+
+int espp_system_destroy(espp_system* s) {
+  return guard([&] { destroy(s); });
+}
+
+int espp_set_skin(espp_system* s, double skin) {
+  return guard([&] {
+    checked(s)->skin = skin;
+  });
+}
+
+int espp_add_particles(espp_system* s, int64_t n, const int64_t* id, const int32_t* type,
+                       const double* mass, const double* pos, const double* vel) {
+  return guard([&] {
+    checked(s);
+    if (n < 0 || (n > 0 && (!id || !pos))) raise(ESPP_EINVAL, "bad particle arrays");
+    if (n == 0) return;
+    if ((int64_t)s->n + n > (1LL << 30)) raise(ESPP_ERANGE, "too many particles");
+    HostParticles h = download(s, true);
+    std::unordered_map<int64_t, int> seen;
+    seen.reserve(h.id.size() + n);
+    for (size_t k = 0; k < h.id.size(); ++k) seen[h.id[k]] = 1;
+    const double L[3] = {s->L[0], s->L[1], s->L[2]};
+    for (int64_t i = 0; i < n; ++i) {
+      if (seen.count(id[i])) raise(ESPP_EINVAL, "duplicate particle id " + std::to_string(id[i]));
+      seen[id[i]] = 1;
+      int ty = type ? type[i] : 0;
+      if (ty < 0 || ty >= kMaxTypes) raise(ESPP_ERANGE, "particle type out of range [0, 8)");
+      h.id.push_back(id[i]);
+      h.type.push_back(ty);
+      s->maxType = std::max(s->maxType, ty);
+      h.mass.push_back(mass ? mass[i] : 1.0);
+      for (int k = 0; k < 3; ++k) {
+        // Storage::addParticle folds the position (OrthorhombicBC::foldCoordinate)
+        double x = pos[3 * i + k];
+        int tmp = static_cast<int>(std::floor(x * (1.0 / L[k])));
+        x -= tmp * L[k];
+        h.x.push_back(x);
+        h.img.push_back(tmp);
+        h.v.push_back(vel ? vel[3 * i + k] : 0.0);
+        h.f.push_back(0.0);
+      }
+      s->allIds.push_back(id[i]);
+    }
+    upload(s, h);
+    upload_lj(s);
+    s->idDirty = true;
+    s->resortFlag = true;
+    s->K = 0;
+    dfree(s->nl);
+  });
+}
+
+int espp_decompose(espp_system* s) {
+  return guard([&] {
+    checked(s);
+    decompose(s);
+    cuda_check(cudaMemsetAsync(s->maxDist, 0, sizeof(double), s->st), "memset");
+    sync(s);
+    s->resortFlag = false;
+  });
+}
+
+int espp_num_particles(espp_system* s, int64_t* n) {
+  return guard([&] { *n = checked(s)->n; });
+}
+
+int espp_get_particles(espp_system* s, int64_t n, const int64_t* ids, double* pos,
+                       double* vel, double* force, int32_t* image) {
+  return guard([&] {
+    checked(s);
+    HostParticles h = download(s, true);
+    std::unordered_map<int64_t, int> where;
+    where.reserve(h.id.size());
+    for (size_t k = 0; k < h.id.size(); ++k) where[h.id[k]] = (int)k;
+    for (int64_t i = 0; i < n; ++i) {
+      auto it = where.find(ids[i]);
+      if (it == where.end()) raise(ESPP_EINVAL, "unknown particle id " + std::to_string(ids[i]));
+      const int k = it->second;
+      for (int c = 0; c < 3; ++c) {
+        if (pos) pos[3 * i + c] = h.x[3 * k + c];
+        if (vel) vel[3 * i + c] = h.v[3 * k + c];
+        if (force) force[3 * i + c] = h.f[3 * k + c];
+        if (image) image[3 * i + c] = h.img[3 * k + c];
+      }
+    }
+  });
+}
+
+int espp_set_particles(espp_system* s, int64_t n, const int64_t* ids, const double* pos,
+                       const double* vel) {
+  return guard([&] {
+    checked(s);
+    HostParticles h = download(s, true);
+    std::unordered_map<int64_t, int> where;
+    for (size_t k = 0; k < h.id.size(); ++k) where[h.id[k]] = (int)k;
+    for (int64_t i = 0; i < n; ++i) {
+      auto it = where.find(ids[i]);
+      if (it == where.end()) raise(ESPP_EINVAL, "unknown particle id " + std::to_string(ids[i]));
+      for (int c = 0; c < 3; ++c) {
+        if (pos) h.x[3 * it->second + c] = pos[3 * i + c];
+        if (vel) h.v[3 * it->second + c] = vel[3 * i + c];
+      }
+    }
+    bool keepBinned = s->binned && !pos;
+    upload(s, h);
+    if (keepBinned) {
+      // same order as before: the cell structure and lists are still valid
+      s->binned = true;
+    }
+    if (pos) s->resortFlag = true;
+  });
+}
+
+int espp_vl_create(espp_system* s, double cutoff, int64_t nexcl, const int64_t* excl) {
+  return guard([&] {
+    checked(s);
+    if (!(cutoff > 0)) raise(ESPP_EINVAL, "Verlet list cutoff must be positive");
+    double cs = cutoff + s->skin;
+    for (int k = 0; k < 3; ++k)
+      if (s->L[k] / s->nc[k] < cs && s->L[k] < 3 * cs)
+        raise(ESPP_ERANGE, "box smaller than 3 (cutoff + skin) in a dimension");
+    s->has_vl = true;
+    s->vl_cut = cutoff;
+    for (int64_t i = 0; i < nexcl; ++i) s->vlExcl.push_back({excl[2 * i], excl[2 * i + 1]});
+    if (nexcl > 0) s->idDirty = true;
+    s->K = 0;
+    dfree(s->nl);
+    if (s->idDirty) rebuild_id_tables(s);
+    if (!s->binned) bin(s, false);
+    build_list(s);
+  });
+}
+
+int espp_vl_rebuild(espp_system* s) {
+  return guard([&] {
+    checked(s);
+    if (!s->has_vl) raise(ESPP_ESTATE, "no Verlet list");
+    if (s->idDirty) rebuild_id_tables(s);
+    build_list(s);
+  });
+}
+
+int espp_vl_size(espp_system* s, int64_t* npairs) {
+  return guard([&] {
+    checked(s);
+    *npairs = 0;
+    if (!s->has_vl || s->n == 0) return;
+    DevView d = s->view();
+    int32_t* counts = dalloc<int32_t>(s->n);
+    launch_pair_count(d, counts, s->st);
+    std::vector<int32_t> h(s->n);
+    cudaError_t e = cudaMemcpyAsync(h.data(), counts, sizeof(int32_t) * s->n,
+                                    cudaMemcpyDeviceToHost, s->st);
+    cudaStreamSynchronize(s->st);
+    dfree(counts);
+    cuda_check(e, "download");
+    int64_t t = 0;
+    for (int32_t c : h) t += c;
+    *npairs = t;
+  });
+}
+
+int espp_vl_pairs(espp_system* s, int64_t capn, int64_t* pairs, int64_t* npairs) {
+  return guard([&] {
+    checked(s);
+    *npairs = 0;
+    if (!s->has_vl || s->n == 0) return;
+    DevView d = s->view();
+    int32_t* counts = dalloc<int32_t>(s->n);
+    launch_pair_count(d, counts, s->st);
+    std::vector<int32_t> h(s->n);
+    cuda_check(cudaMemcpyAsync(h.data(), counts, sizeof(int32_t) * s->n,
+                               cudaMemcpyDeviceToHost, s->st), "download");
+    sync(s);
+    dfree(counts);
+    std::vector<int64_t> off(s->n);
+    int64_t t = 0;
+    for (int i = 0; i < s->n; ++i) {
+      off[i] = t;
+      t += h[i];
+    }
+    int64_t* doff = dalloc<int64_t>(s->n);
+    int64_t* dout = dalloc<int64_t>(2 * std::max<int64_t>(t, 1));
+    std::vector<int64_t> out(2 * std::max<int64_t>(t, 1));
+    cudaMemcpy(doff, off.data(), sizeof(int64_t) * s->n, cudaMemcpyHostToDevice);
+    launch_pair_write(d, doff, dout, s->st);
+    cudaError_t e = cudaMemcpyAsync(out.data(), dout, sizeof(int64_t) * 2 * t,
+                                    cudaMemcpyDeviceToHost, s->st);
+    cudaStreamSynchronize(s->st);
+    dfree(doff);
+    dfree(dout);
+    cuda_check(e, "download");
+    std::vector<std::pair<int64_t, int64_t>> v(t);
+    for (int64_t k = 0; k < t; ++k) v[k] = {out[2 * k], out[2 * k + 1]};
+    std::sort(v.begin(), v.end());
+    *npairs = t;
+    for (int64_t k = 0; k < std::min(capn, t); ++k) {
+      pairs[2 * k] = v[k].first;
+      pairs[2 * k + 1] = v[k].second;
+    }
+  });
+}
+
+int espp_vl_builds(espp_system* s, int64_t* builds) {
+  return guard([&] { *builds = checked(s)->builds; });
+}
+
+int espp_lj_set(espp_system* s, int32_t t1, int32_t t2, double eps, double sig, double rc,
+                double shift, double caprad) {
+  return guard([&] {
+    checked(s);
+    if (t1 < 0 || t2 < 0 || t1 >= kMaxTypes || t2 >= kMaxTypes)
+      raise(ESPP_ERANGE, "particle type out of range [0, 8)");
+    LJPair P{};
+    P.set = 1;
+    double sig2 = sig * sig;
+    double sig6 = sig2 * sig2 * sig2;
+    P.ff1 = 48.0 * eps * sig6 * sig6;
+    P.ff2 = 24.0 * eps * sig6;
+    P.ef1 = 4.0 * eps;
+    P.ef2 = sig * sig;
+    P.rcsq = rc * rc;
+    P.shift = shift;
+    P.caprad = caprad;
+    if (caprad > 0) {
+      double frac2 = (sig / caprad) * (sig / caprad);
+      double frac6 = frac2 * frac2 * frac2;
+      P.capff = 48.0 * eps * frac6 * (frac6 - 0.5) / caprad;
+    }
+    s->lj.p[t1 * kMaxTypes + t2] = P;
+    s->lj.p[t2 * kMaxTypes + t1] = P;
+    s->lj.ntypes = std::max(s->lj.ntypes, std::max(t1, t2) + 1);
+    s->lj_any = true;
+    upload_lj(s);
+  });
+}
+
+int espp_bonds_add(espp_system* s, int64_t n, const int64_t* pairs) {
+  return guard([&] {
+    checked(s);
+    std::unordered_map<int64_t, int> have;
+    for (int64_t id : s->allIds) have[id] = 1;
+    for (int64_t i = 0; i < n; ++i) {
+      int64_t a = pairs[2 * i], b = pairs[2 * i + 1];
+      if (a > b) std::swap(a, b);
+      if (!have.count(a) || !have.count(b)) raise(ESPP_EINVAL, "bond partner does not exist");
+      s->bonds.push_back({a, b});
+    }
+    s->idDirty = true;
+  });
+}
+
+int espp_bonds_size(espp_system* s, int64_t* n) {
+  return guard([&] { *n = (int64_t)checked(s)->bonds.size(); });
+}
+
+int espp_fene_set(espp_system* s, double K, double r0, double rmax, double rc, double shift) {
+  return guard([&] {
+    checked(s);
+    s->fene.on = 1;
+    s->fene.K = K;
+    s->fene.r0 = r0;
+    s->fene.rmax = rmax;
+    s->fene.rmaxsq = rmax * rmax;
+    s->fene.rcsq = rc * rc;
+    s->fene.shift = shift;
+  });
+}
+
+int espp_bonds_max_sqr(espp_system* s, double* m) {
+  return guard([&] {
+    checked(s);
+    prepare_observables(s);
+    *m = 0.0;
+    if (s->n == 0 || s->bonds.empty()) return;
+    int nb;
+    double* part = obs_partials(s, nb);
+    launch_bond_maxsq(s->view(), part, nb, s->obs, s->st);
+    cuda_check(cudaMemcpyAsync(m, s->obs, sizeof(double), cudaMemcpyDeviceToHost, s->st),
+               "download");
+    sync(s);
+  });
+}
+
+int espp_integrator_set(espp_system* s, double dt) {
+  return guard([&] {
+    checked(s);
+    if (dt == 0.0) raise(ESPP_EINVAL, "Timestep 'dt' must be non-zero!");
+    s->dt = dt;
+  });
+}
+
+int espp_step_get(espp_system* s, int64_t* step) {
+  return guard([&] { *step = checked(s)->step; });
+}
+
+int espp_step_set(espp_system* s, int64_t step) {
+  return guard([&] { checked(s)->step = step; });
+}
+
+int espp_langevin_set(espp_system* s, int32_t enabled, double gamma, double T, int64_t nexcl,
+                      const int64_t* excl) {
+  return guard([&] {
+    checked(s);
+    s->lang_on = enabled != 0;
+    s->gamma = gamma;
+    s->temperature = T;
+    s->langExclIds.assign(excl, excl + nexcl);
+    s->idDirty = true;
+  });
+}
+
+int espp_capforce_set(espp_system* s, int32_t mode, const double cap[3]) {
+  return guard([&] {
+    checked(s);
+    if (mode < 0 || mode > 2) raise(ESPP_EINVAL, "unknown force-capping mode");
+    s->capMode = mode;
+    for (int k = 0; k < 3; ++k) s->cap3[k] = cap ? cap[k] : 0.0;
+  });
+}
+
+int espp_run(espp_system* s, int64_t nsteps) {
+  return guard([&] {
+    checked(s);
+    if (nsteps < 0) raise(ESPP_EINVAL, "negative step count");
+    run(s, nsteps);
+  });
+}
+
+int espp_num_resorts(espp_system* s, int64_t* n) {
+  return guard([&] { *n = checked(s)->nResorts; });
+}
+
+int espp_timers(espp_system* s, double t[10]) {
+  return guard([&] {
+    checked(s);
+    for (int k = 0; k < 10; ++k) t[k] = s->timers[k];
+  });
+}
+
+int espp_energy(espp_system* s, int32_t which, double* e) {
+  return guard([&] {
+    double o[7];
+    observable(checked(s), which, 1, o);
+    *e = o[0];
+  });
+}
+
+int espp_virial(espp_system* s, int32_t which, double* w) {
+  return guard([&] {
+    double o[7];
+    observable(checked(s), which, 0, o);
+    *w = o[0];
+  });
+}
+
+int espp_virial_tensor(espp_system* s, int32_t which, double w[6]) {
+  return guard([&] {
+    double o[7];
+    observable(checked(s), which, 0, o);
+    for (int k = 0; k < 6; ++k) w[k] = o[k + 1];
+  });
+}
+
+int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n) {
+  return guard([&] {
+    checked(s);
+    *sum_mv2 = 0.0;
+    *n = s->n;
+    if (s->n == 0) return;
+    int nb;
+    double* part = obs_partials(s, nb);
+    launch_kinetic(s->view(), part, nb, s->obs, s->st);
+    cuda_check(cudaMemcpyAsync(sum_mv2, s->obs, sizeof(double), cudaMemcpyDeviceToHost, s->st),
+               "download");
+    sync(s);
+  });
+}
+
+}  // extern "C"

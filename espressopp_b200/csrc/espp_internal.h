@@ -1,0 +1,146 @@
+// espp_internal.h - device data layout and kernel launch interface shared by the host
+// runtime (espp_api.cu) and the kernels (espp_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace espp {
+
+constexpr int kMaxTypes = 8;
+constexpr double kFix = 4294967296.0;        // 2^32: fixed-point force scale
+constexpr double kInvFix = 1.0 / 4294967296.0;
+
+// device error word bits
+enum : unsigned {
+  kErrNlOverflow = 1u << 0,    // a particle has more Verlet neighbours than the capacity
+  kErrFixOverflow = 1u << 1,   // |F| beyond the int64 2^-32 fixed-point range
+  kErrOutside = 1u << 2,       // non-finite or out-of-grid coordinate at re-binning
+  kErrBondMissing = 1u << 3,   // bond partner id not present
+  kErrIdRange = 1u << 4,       // particle id outside the dense id map
+};
+
+// Lennard-Jones parameters of one type pair (LennardJones.hpp:79-87 preset()).
+struct LJPair {
+  double ff1, ff2;   // 48 eps sig^12, 24 eps sig^6
+  double ef1, ef2;   // 4 eps, sig^2 (energy uses 4 eps ((sig^2/r^2)^6 - (sig^2/r^2)^3))
+  double rcsq;       // cutoff^2 (pairs with r^2 > rcsq feel nothing)
+  double shift;      // energy shift
+  double caprad;     // > 0: LennardJonesCapped
+  double capff;      // capped branch: 48 eps frac6 (frac6 - 0.5) / caprad
+  int set;
+  int pad;
+};
+
+struct LJTable {
+  int ntypes;
+  int single;        // one type pair only: skip the type lookup
+  LJPair p[kMaxTypes * kMaxTypes];
+};
+
+// float copy of the table used by the mixed-precision force kernel
+struct LJPairF {
+  float ff1, ff2, rcsq, capsq, capff;
+  int set;
+};
+
+struct FENEParams {
+  int on;
+  double K, r0, rmax, rmaxsq, rcsq, shift;
+};
+
+// Per-particle arrays in cell-sorted order.  Two copies exist; the re-sort gathers
+// from one into the other and swaps.
+struct ParticleArrays {
+  double* x;     // 3*cap, SoA: x[0..cap) y[cap..2cap) z[2cap..3cap)
+  double* v;     // 3*cap
+  int64_t* id;   // cap
+  int32_t* type; // cap
+  double* mass;  // cap
+  int32_t* img;  // 3*cap
+};
+
+// Pointers and scalars every kernel needs; passed by value.
+struct DevView {
+  ParticleArrays a;       // current arrays
+  int n;                  // particles
+  int cap;                // allocated rows
+  double L[3], invL[3], halfL[3];
+  double cellSize[3], invCellSize[3];
+  int nc[3];              // inner cells per dim
+  int ncells;
+  double fixScale[3];     // 2^32 / L_d   (double -> box-wrapped int32)
+  float fixUnit[3];       // L_d / 2^32   (int32 difference -> float length)
+  int4* posq;             // box-wrapped int32 coordinates + type
+  int32_t* pcell;         // reference cell of each sorted particle
+  int32_t* cellStart;     // ncells + 1
+  int32_t* nl;            // K * cap, entry (k, i) at nl[k * cap + i]
+  int32_t* nn;            // neighbour count per particle
+  int K;                  // neighbour capacity
+  long long* ffix;        // 3*cap pair+bond force, int64 2^-32 fixed point (mixed)
+  double* f64;            // 3*cap pair+bond force (FP64 path)
+  double* ftot;           // 3*cap total force after the aftCalcF extensions
+  int64_t idMin;          // dense id map base
+  int idSpan;             // dense id map size
+  int32_t* id2idx;        // idSpan: sorted index of id, -1 if absent
+  int32_t* bondStart;     // idSpan + 1, CSR of bond partners by id - idMin
+  int64_t* bondPartner;   // partner ids
+  uint8_t* langExcl;      // idSpan: 1 if the Langevin thermostat skips this id
+  int32_t* exclStart;     // idSpan + 1, Verlet-list exclusions by id (or null)
+  int64_t* exclIds;
+  const LJPair* lj;       // ntypes*ntypes FP64 table (device)
+  const LJPairF* ljf;     // float copy for the mixed kernel
+  int ntypes;
+  int ljSingle;           // only pair (0,0) is set
+  int ljCapped;           // some pair uses LennardJonesCapped
+  unsigned* err;          // device error word
+  unsigned long long* maxSq;  // max |dx|^2 of the last integrate1, as double bits
+};
+
+struct RebuildScratch {
+  int32_t* cellOf;    // cap: cell of particle (unsorted order)
+  int32_t* slot;      // cap: arrival slot inside its cell
+  int32_t* cellCount; // ncells
+  int32_t* perm;      // cap: sorted position -> old row
+};
+
+// launchers (espp_kernels.cu)
+void launch_fold_bin(const DevView& d, RebuildScratch& s, bool fold, cudaStream_t st);
+void launch_sort_cells(const DevView& d, RebuildScratch& s, cudaStream_t st);
+void launch_gather(const DevView& d, const ParticleArrays& src, const ParticleArrays& dst,
+                   const RebuildScratch& s, cudaStream_t st);
+void launch_id_map(const DevView& d, cudaStream_t st);
+void launch_build_nl(const DevView& d, double cutsq, cudaStream_t st);
+void launch_posq(const DevView& d, cudaStream_t st);
+void launch_forces(const DevView& d, bool mixed, const FENEParams& fene, int tpp,
+                   cudaStream_t st);
+struct IntegrateArgs {
+  int do_i2, do_i1, langevin, capMode, storeFtot, phase, mixed;
+  double dt, pref1, pref2;
+  double cap[3];
+  uint64_t seed;
+  int64_t step;
+};
+void launch_integrate(const DevView& d, const IntegrateArgs& a, cudaStream_t st);
+// maxDist += sqrt(max |dx|^2); flag = maxDist > skinHalf
+void launch_decide(const DevView& d, double* maxDist, int* flag, double skinHalf,
+                   cudaStream_t st);
+// observables: out[0..6] = (scalar, tensor xx yy zz xy xz yz); deterministic reductions
+void launch_lj_observables(const DevView& d, double* partials, int nblocks, double* out,
+                           int energy, cudaStream_t st);
+void launch_fene_observables(const DevView& d, const FENEParams& fene, double* partials,
+                             int nblocks, double* out, int energy, cudaStream_t st);
+void launch_kinetic(const DevView& d, double* partials, int nblocks, double* out,
+                    cudaStream_t st);
+// Verlet pair export: counts per particle (pairs with id_j > id_i), then the pairs.
+void launch_pair_count(const DevView& d, int32_t* counts, cudaStream_t st);
+void launch_pair_write(const DevView& d, const int64_t* offsets, int64_t* out,
+                       cudaStream_t st);
+void launch_bond_maxsq(const DevView& d, double* partials, int nblocks, double* out,
+                       cudaStream_t st);
+
+// float copy of an LJ table for the mixed-precision kernel
+void make_float_table(const LJTable& t, LJPairF* out);
+int observable_blocks(int n);
+
+}  // namespace espp

@@ -1,0 +1,936 @@
+// espp_kernels.cu - sm_100a kernels of the short-range MD step.
+//
+//  re-binning     k_fold_bin -> k_scan_cells -> k_scatter -> k_sort_in_cell -> k_gather
+//                 (storage::DomainDecomposition::decomposeRealParticles, one node)
+//  Verlet list    k_build_nl: exact FP64 pair test in the reference's ghost-shift
+//                 arithmetic, full per-particle list (VerletList::_rebuildUsingBuffers)
+//  forces         k_force_mixed (FP32 on box-wrapped int32 coordinates, int64 2^-32
+//                 fixed-point output) / k_force_fp64 (plain FP64); LJ + FENE fused
+//  integrator     k_integrate: aftCalcF (Langevin, CapForce) + integrate2 of step n +
+//                 integrate1 of step n+1 in one pass over the particle arrays
+//  observables    FP64 energy / virial / kinetic with fixed-order block reductions
+#include <math.h>
+#include <stdint.h>
+
+#include "espp_internal.h"
+
+namespace espp {
+
+void make_float_table(const LJTable& t, LJPairF* f) {
+  for (int k = 0; k < kMaxTypes * kMaxTypes; ++k) {
+    const LJPair& p = t.p[k];
+    f[k].ff1 = (float)p.ff1;
+    f[k].ff2 = (float)p.ff2;
+    f[k].rcsq = p.set ? (float)p.rcsq : -1.0f;
+    f[k].capsq = p.caprad > 0 ? (float)(p.caprad * p.caprad) : -1.0f;
+    f[k].capff = (float)p.capff;
+    f[k].set = p.set;
+  }
+}
+
+namespace {
+
+constexpr int kBlock = 256;
+
+inline int blocks_for(long long n, int b = kBlock) { return (int)((n + b - 1) / b); }
+
+__device__ __forceinline__ int4 fixed_coords(const DevView& d, double x, double y, double z,
+                                             int type) {
+  // box-wrapped int32: the low 32 bits of round(x * 2^32 / L)
+  long long qx = __double2ll_rn(x * d.fixScale[0]);
+  long long qy = __double2ll_rn(y * d.fixScale[1]);
+  long long qz = __double2ll_rn(z * d.fixScale[2]);
+  return make_int4((int)(unsigned)qx, (int)(unsigned)qy, (int)(unsigned)qz, type);
+}
+
+__device__ __forceinline__ float wrapped_diff(int a, int b, float unit) {
+  return (float)(int)((unsigned)a - (unsigned)b) * unit;
+}
+
+__device__ __forceinline__ float fast_rcp(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// ---- Philox4x32-10 (Salmon et al., SC'11) ----------------------------------------
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    if (r > 0) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+    c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+  }
+  return c;
+}
+
+__device__ __forceinline__ void langevin_uniforms(uint64_t seed, int64_t id, int64_t step,
+                                                  int phase, double u[3]) {
+  uint4 c = make_uint4((uint32_t)(uint64_t)id, (uint32_t)((uint64_t)id >> 32),
+                       (uint32_t)(uint64_t)step,
+                       ((uint32_t)((uint64_t)step >> 32) & 0x7FFFFFFFu) |
+                           ((uint32_t)phase << 31));
+  uint4 r = philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  u[0] = ((double)r.x + 0.5) * (1.0 / 4294967296.0);
+  u[1] = ((double)r.y + 0.5) * (1.0 / 4294967296.0);
+  u[2] = ((double)r.z + 0.5) * (1.0 / 4294967296.0);
+}
+
+// ---- re-binning --------------------------------------------------------------------
+
+// OrthorhombicBC::foldCoordinate + CellGrid::mapPositionToCellChecked/Clipped.
+__global__ void k_fold_bin(DevView d, RebuildScratch s, int fold) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n) return;
+  int c[3];
+  bool outside = false;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    double x = d.a.x[(size_t)k * d.cap + i];
+    if (fold) {
+      double q = floor(__dmul_rn(x, d.invL[k]));
+      if (!(fabs(q) < 1.0e9)) {
+        outside = true;
+        q = 0.0;
+      }
+      int tmp = (int)q;
+      d.a.img[(size_t)k * d.cap + i] += tmp;
+      x = __dsub_rn(x, __dmul_rn((double)tmp, d.L[k]));
+      d.a.x[(size_t)k * d.cap + i] = x;
+    }
+    double lpos = x;
+    double t = __dmul_rn(lpos, d.invCellSize[k]);
+    int ck = (t > -2.0e9 && t < 2.0e9) ? (int)t : (t > 0 ? d.nc[k] : -1);
+    if (!(x == x)) {
+      outside = true;
+      ck = 0;
+    }
+    if (lpos < 0.0 && t <= -1.0) ck = -1;  // (int) truncates toward zero
+    if (ck < 0) {
+      if (fold && !(lpos >= -2.220446049250313e-16)) outside = true;
+      ck = 0;
+    } else if (ck >= d.nc[k]) {
+      if (fold && !(x <= d.L[k] + 2.220446049250313e-16)) outside = true;
+      ck = d.nc[k] - 1;
+    }
+    c[k] = ck;
+  }
+  if (outside) atomicOr(d.err, kErrOutside);
+  int cell = c[0] + d.nc[0] * (c[1] + d.nc[1] * c[2]);
+  s.cellOf[i] = cell;
+  s.slot[i] = atomicAdd(&s.cellCount[cell], 1);
+}
+
+// Exclusive scan of the cell counts into cellStart (one block).
+__global__ void k_scan_cells(const int32_t* __restrict__ count, int32_t* __restrict__ start,
+                             int ncells) {
+  __shared__ int32_t sums[1024];
+  int t = threadIdx.x;
+  int chunk = (ncells + blockDim.x - 1) / blockDim.x;
+  int b = t * chunk, e = min(ncells, b + chunk);
+  int acc = 0;
+  for (int c = b; c < e; ++c) acc += count[c];
+  sums[t] = acc;
+  __syncthreads();
+  for (int off = 1; off < (int)blockDim.x; off <<= 1) {
+    int v = t >= off ? sums[t - off] : 0;
+    __syncthreads();
+    sums[t] += v;
+    __syncthreads();
+  }
+  int run = sums[t] - acc;
+  for (int c = b; c < e; ++c) {
+    start[c] = run;
+    run += count[c];
+  }
+  if (t == blockDim.x - 1) start[ncells] = sums[t];
+}
+
+__global__ void k_scatter(DevView d, RebuildScratch s) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n) return;
+  s.perm[d.cellStart[s.cellOf[i]] + s.slot[i]] = i;
+}
+
+// Order inside a cell: by particle id, so the layout is independent of the atomic
+// arrival order above.
+__global__ void k_sort_in_cell(DevView d, RebuildScratch s) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.ncells) return;
+  int b = d.cellStart[c], e = d.cellStart[c + 1];
+  for (int k = b + 1; k < e; ++k) {
+    int v = s.perm[k];
+    int64_t key = d.a.id[v];
+    int m = k - 1;
+    while (m >= b && d.a.id[s.perm[m]] > key) {
+      s.perm[m + 1] = s.perm[m];
+      --m;
+    }
+    s.perm[m + 1] = v;
+  }
+}
+
+__global__ void k_gather(DevView d, ParticleArrays src, ParticleArrays dst, RebuildScratch s) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.n) return;
+  int o = s.perm[k];
+  double p[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    p[c] = src.x[(size_t)c * d.cap + o];
+    dst.x[(size_t)c * d.cap + k] = p[c];
+    dst.v[(size_t)c * d.cap + k] = src.v[(size_t)c * d.cap + o];
+    dst.img[(size_t)c * d.cap + k] = src.img[(size_t)c * d.cap + o];
+  }
+  int ty = src.type[o];
+  dst.id[k] = src.id[o];
+  dst.type[k] = ty;
+  dst.mass[k] = src.mass[o];
+  d.pcell[k] = s.cellOf[o];
+  d.posq[k] = fixed_coords(d, p[0], p[1], p[2], ty);
+}
+
+__global__ void k_id_map(DevView d) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.n) return;
+  int64_t off = d.a.id[k] - d.idMin;
+  if (off < 0 || off >= d.idSpan) {
+    atomicOr(d.err, kErrIdRange);
+    return;
+  }
+  d.id2idx[off] = k;
+}
+
+__global__ void k_posq(DevView d) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.n) return;
+  d.posq[k] = fixed_coords(d, d.a.x[k], d.a.x[(size_t)d.cap + k], d.a.x[2 * (size_t)d.cap + k],
+                           d.a.type[k]);
+}
+
+// ---- Verlet list -------------------------------------------------------------------
+
+__device__ __forceinline__ bool is_excluded(const DevView& d, int64_t a, int64_t b) {
+  if (!d.exclStart) return false;
+  int64_t off = a - d.idMin;
+  int e0 = d.exclStart[off], e1 = d.exclStart[off + 1];
+  for (int e = e0; e < e1; ++e)
+    if (d.exclIds[e] == b) return true;
+  return false;
+}
+
+// One warp per cell; lanes own the cell's particles (32 at a time).  Candidates are
+// the 27 cells of the reference's neighbour stencil; the inclusion test is the
+// reference's d = p1 - (p2 + shift), d.sqr() <= cutsq in FP64 without contraction,
+// where p1 is the particle of the backward cell and shift is the ghost image offset
+// of the forward cell (VerletList.cpp:399-426, DomainDecomposition.cpp:1347-1391).
+__global__ void k_build_nl(DevView d, double cutsq) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= d.ncells) return;
+  const int c = warp;
+  const int cx = c % d.nc[0], cy = (c / d.nc[0]) % d.nc[1], cz = c / (d.nc[0] * d.nc[1]);
+  const int s0 = d.cellStart[c], s1 = d.cellStart[c + 1];
+  const double* X = d.a.x;
+  const double* Y = d.a.x + d.cap;
+  const double* Z = d.a.x + 2 * (size_t)d.cap;
+  for (int base = s0; base < s1; base += 32) {
+    const int i = base + lane;
+    const bool act = i < s1;
+    double xi = 0, yi = 0, zi = 0;
+    int64_t idi = 0;
+    if (act) {
+      xi = X[i];
+      yi = Y[i];
+      zi = Z[i];
+      idi = d.a.id[i];
+    }
+    int cnt = 0;
+    for (int oz = -1; oz <= 1; ++oz)
+      for (int oy = -1; oy <= 1; ++oy)
+        for (int ox = -1; ox <= 1; ++ox) {
+          int ncx = cx + ox, ncy = cy + oy, ncz = cz + oz;
+          int wx = ncx < 0 ? -1 : (ncx >= d.nc[0] ? 1 : 0);
+          int wy = ncy < 0 ? -1 : (ncy >= d.nc[1] ? 1 : 0);
+          int wz = ncz < 0 ? -1 : (ncz >= d.nc[2] ? 1 : 0);
+          ncx -= wx * d.nc[0];
+          ncy -= wy * d.nc[1];
+          ncz -= wz * d.nc[2];
+          const int nb = ncx + d.nc[0] * (ncy + d.nc[1] * ncz);
+          const bool fwd = oz > 0 || (oz == 0 && (oy > 0 || (oy == 0 && ox > 0)));
+          // shift of the forward particle's ghost image
+          const double sx = wx * d.L[0], sy = wy * d.L[1], sz = wz * d.L[2];
+          const int j0 = d.cellStart[nb], j1 = d.cellStart[nb + 1];
+          for (int j = j0; j < j1; ++j) {
+            const double xj = X[j], yj = Y[j], zj = Z[j];
+            double dx, dy, dz;
+            if (fwd) {  // p1 = i, p2 = ghost of j at xj + s
+              dx = __dsub_rn(xi, __dadd_rn(xj, sx));
+              dy = __dsub_rn(yi, __dadd_rn(yj, sy));
+              dz = __dsub_rn(zi, __dadd_rn(zj, sz));
+            } else {  // p1 = j, p2 = ghost of i at xi - s
+              dx = __dsub_rn(xj, __dadd_rn(xi, -sx));
+              dy = __dsub_rn(yj, __dadd_rn(yi, -sy));
+              dz = __dsub_rn(zj, __dadd_rn(zi, -sz));
+            }
+            const double d2 =
+                __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+            if (act && j != i && !(d2 > cutsq)) {
+              if (!is_excluded(d, idi, d.a.id[j])) {
+                if (cnt < d.K) d.nl[(size_t)cnt * d.cap + i] = j;
+                ++cnt;
+              }
+            }
+          }
+        }
+    if (act) {
+      if (cnt > d.K) atomicOr(d.err, kErrNlOverflow);
+      d.nn[i] = min(cnt, d.K);
+    }
+  }
+}
+
+// ---- forces ------------------------------------------------------------------------
+
+__device__ __forceinline__ long long to_fix(float f, unsigned* err) {
+  if (!(fabsf(f) < 1.0e9f)) atomicOr(err, kErrFixOverflow);
+  return __float2ll_rn(f * 4294967296.0f);
+}
+
+// FP32 pair forces on box-wrapped int32 coordinates.  The minimum image is the 32-bit
+// wrap of the coordinate difference.  One thread per particle (TPP threads when >1),
+// FP32 sums along the list, results stored as int64 2^-32 fixed point; partial sums
+// of the TPP threads and the bond term are combined in int64, so the result does not
+// depend on the order in which they are added.
+template <int TPP, bool SINGLE, bool CAPPED, bool FENE>
+__global__ void __launch_bounds__(256) k_force_mixed(DevView d, FENEParams fp) {
+  __shared__ LJPairF sP[kMaxTypes * kMaxTypes];
+  if (!SINGLE) {
+    for (int t = threadIdx.x; t < d.ntypes * d.ntypes; t += blockDim.x) sP[t] = d.ljf[t];
+    __syncthreads();
+  }
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i0 = gt / TPP;
+  const int sub = gt % TPP;
+  if (TPP == 1 && i0 >= d.n) return;
+  // with TPP > 1 every lane stays until the shuffles below
+  const bool act = i0 < d.n;
+  const int i = act ? i0 : 0;
+  const int4 pi = d.posq[i];
+  const float ux = d.fixUnit[0], uy = d.fixUnit[1], uz = d.fixUnit[2];
+  const int cnt = act ? d.nn[i] : 0;
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  LJPairF P = d.ljf[0];
+  const int ntypes = d.ntypes;
+  const int* __restrict__ nl = d.nl;
+  for (int k = sub; k < cnt; k += TPP) {
+    const int j = __ldg(&nl[(size_t)k * d.cap + i]);
+    const int4 pj = __ldg(&d.posq[j]);
+    const float dx = wrapped_diff(pi.x, pj.x, ux);
+    const float dy = wrapped_diff(pi.y, pj.y, uy);
+    const float dz = wrapped_diff(pi.z, pj.z, uz);
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    if (!SINGLE) P = sP[pi.w * ntypes + pj.w];
+    const float ri2 = fast_rcp(r2);
+    const float ri6 = ri2 * ri2 * ri2;
+    float ff = ri6 * (P.ff1 * ri6 - P.ff2) * ri2;
+    if (CAPPED && r2 <= P.capsq) ff = P.capff * rsqrtf(r2);
+    ff = (r2 <= P.rcsq) ? ff : 0.f;
+    fx += dx * ff;
+    fy += dy * ff;
+    fz += dz * ff;
+  }
+  long long Fx = to_fix(fx, d.err), Fy = to_fix(fy, d.err), Fz = to_fix(fz, d.err);
+  if (FENE && sub == 0 && act) {
+    const int64_t off = d.a.id[i] - d.idMin;
+    const int b0 = d.bondStart[off], b1 = d.bondStart[off + 1];
+    float bx = 0.f, by = 0.f, bz = 0.f;
+    const float rmaxsq = (float)fp.rmaxsq, K = (float)fp.K, r0 = (float)fp.r0;
+    for (int b = b0; b < b1; ++b) {
+      const int64_t po = d.bondPartner[b] - d.idMin;
+      const int j = (po >= 0 && po < d.idSpan) ? d.id2idx[po] : -1;
+      if (j < 0) {
+        atomicOr(d.err, kErrBondMissing);
+        continue;
+      }
+      const int4 pj = d.posq[j];
+      const float dx = wrapped_diff(pi.x, pj.x, ux);
+      const float dy = wrapped_diff(pi.y, pj.y, uy);
+      const float dz = wrapped_diff(pi.z, pj.z, uz);
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      if (!(r2 <= (float)fp.rcsq)) continue;
+      float ff;
+      if (fp.r0 > 2.220446049250313e-16) {
+        const float r = sqrtf(r2);
+        ff = -K * (r - r0) / (r * (1.f - ((r - r0) * (r - r0) / rmaxsq)));
+      } else {
+        ff = -K / (1.f - r2 / rmaxsq);
+      }
+      bx += dx * ff;
+      by += dy * ff;
+      bz += dz * ff;
+    }
+    Fx += to_fix(bx, d.err);
+    Fy += to_fix(by, d.err);
+    Fz += to_fix(bz, d.err);
+  }
+  if (TPP > 1) {
+#pragma unroll
+    for (int o = TPP / 2; o > 0; o >>= 1) {
+      Fx += __shfl_xor_sync(0xffffffffu, Fx, o, TPP);
+      Fy += __shfl_xor_sync(0xffffffffu, Fy, o, TPP);
+      Fz += __shfl_xor_sync(0xffffffffu, Fz, o, TPP);
+    }
+  }
+  if (sub == 0 && act) {
+    d.ffix[i] = Fx;
+    d.ffix[(size_t)d.cap + i] = Fy;
+    d.ffix[2 * (size_t)d.cap + i] = Fz;
+  }
+}
+
+__device__ __forceinline__ double min_image(double dx, double L, double halfL) {
+  if (dx < -halfL)
+    dx += L;
+  else if (dx > halfL)
+    dx -= L;
+  return dx;
+}
+
+// Plain FP64 form of the same kernel (reference arithmetic of LennardJones.hpp:137-143
+// and FENE.hpp:97-112 on minimum-image distances).
+template <int TPP, bool SINGLE, bool CAPPED, bool FENE>
+__global__ void __launch_bounds__(256) k_force_fp64(DevView d, FENEParams fp) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i0 = gt / TPP;
+  const int sub = gt % TPP;
+  if (TPP == 1 && i0 >= d.n) return;
+  const bool act = i0 < d.n;
+  const int i = act ? i0 : 0;
+  const double* X = d.a.x;
+  const double* Y = d.a.x + d.cap;
+  const double* Z = d.a.x + 2 * (size_t)d.cap;
+  const double xi = X[i], yi = Y[i], zi = Z[i];
+  const int ti = d.a.type[i];
+  const int cnt = act ? d.nn[i] : 0;
+  double fx = 0, fy = 0, fz = 0;
+  const int ntypes = d.ntypes;
+  for (int k = sub; k < cnt; k += TPP) {
+    const int j = __ldg(&d.nl[(size_t)k * d.cap + i]);
+    const double dx = min_image(xi - __ldg(&X[j]), d.L[0], d.halfL[0]);
+    const double dy = min_image(yi - __ldg(&Y[j]), d.L[1], d.halfL[1]);
+    const double dz = min_image(zi - __ldg(&Z[j]), d.L[2], d.halfL[2]);
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    const LJPair& P = SINGLE ? d.lj[0] : d.lj[ti * ntypes + __ldg(&d.a.type[j])];
+    if (!P.set || r2 > P.rcsq) continue;
+    double ff;
+    if (CAPPED && P.caprad > 0 && !(r2 > P.caprad * P.caprad)) {
+      ff = P.capff / sqrt(r2);
+    } else {
+      const double ri2 = 1.0 / r2;
+      const double ri6 = ri2 * ri2 * ri2;
+      ff = ri6 * (P.ff1 * ri6 - P.ff2) * ri2;
+    }
+    fx += dx * ff;
+    fy += dy * ff;
+    fz += dz * ff;
+  }
+  if (FENE && sub == 0 && act) {
+    const int64_t off = d.a.id[i] - d.idMin;
+    const int b0 = d.bondStart[off], b1 = d.bondStart[off + 1];
+    for (int b = b0; b < b1; ++b) {
+      const int64_t po = d.bondPartner[b] - d.idMin;
+      const int j = (po >= 0 && po < d.idSpan) ? d.id2idx[po] : -1;
+      if (j < 0) {
+        atomicOr(d.err, kErrBondMissing);
+        continue;
+      }
+      const double dx = min_image(xi - X[j], d.L[0], d.halfL[0]);
+      const double dy = min_image(yi - Y[j], d.L[1], d.halfL[1]);
+      const double dz = min_image(zi - Z[j], d.L[2], d.halfL[2]);
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 > fp.rcsq) continue;
+      double ff;
+      if (fp.r0 > 2.220446049250313e-16) {
+        const double r = sqrt(r2);
+        ff = -fp.K * (r - fp.r0) / (r * (1 - ((r - fp.r0) * (r - fp.r0) / fp.rmaxsq)));
+      } else {
+        ff = -fp.K / (1.0 - r2 / fp.rmaxsq);
+      }
+      fx += dx * ff;
+      fy += dy * ff;
+      fz += dz * ff;
+    }
+  }
+  if (TPP > 1) {
+#pragma unroll
+    for (int o = TPP / 2; o > 0; o >>= 1) {
+      fx += __shfl_xor_sync(0xffffffffu, fx, o, TPP);
+      fy += __shfl_xor_sync(0xffffffffu, fy, o, TPP);
+      fz += __shfl_xor_sync(0xffffffffu, fz, o, TPP);
+    }
+  }
+  if (sub == 0 && act) {
+    d.f64[i] = fx;
+    d.f64[(size_t)d.cap + i] = fy;
+    d.f64[2 * (size_t)d.cap + i] = fz;
+  }
+}
+
+// ---- integrator --------------------------------------------------------------------
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// aftCalcF (LangevinThermostat::frictionThermo, CapForce) on the pair force, then
+// integrate2 of this step and integrate1 of the next (VelocityVerlet.cpp:236-305),
+// with the reference's operation order and no FMA contraction.
+template <bool MIXED>
+__global__ void __launch_bounds__(256) k_integrate(DevView d, IntegrateArgs a) {
+  __shared__ double smax[kBlock / 32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double sq = 0.0;
+  if (i < d.n) {
+    const size_t cap = d.cap;
+    const double m = d.a.mass[i];
+    double F[3], v[3], x[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      F[k] = MIXED ? (double)d.ffix[k * cap + i] * kInvFix : d.f64[k * cap + i];
+      v[k] = d.a.v[k * cap + i];
+    }
+    if (a.langevin) {
+      const int64_t id = d.a.id[i];
+      if (!(d.langExcl && d.langExcl[id - d.idMin])) {
+        const double massf = sqrt(m);
+        double u[3];
+        langevin_uniforms(a.seed, id, a.step, a.phase, u);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const double t1 = __dmul_rn(__dmul_rn(a.pref1, v[k]), m);
+          const double t2 = __dmul_rn(__dmul_rn(a.pref2, u[k] - 0.5), massf);
+          F[k] = __dadd_rn(F[k], __dadd_rn(t1, t2));
+        }
+      }
+    }
+    if (a.capMode == 1) {
+      const double capfsq = __dmul_rn(a.cap[0], a.cap[0]);
+      const double fsq =
+          __dadd_rn(__dadd_rn(__dmul_rn(F[0], F[0]), __dmul_rn(F[1], F[1])), __dmul_rn(F[2], F[2]));
+      if (fsq > capfsq) {
+        const double scaling = sqrt(capfsq / fsq);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) F[k] = __dmul_rn(F[k], scaling);
+      }
+    } else if (a.capMode == 2) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        if (F[k] > 0 && F[k] > a.cap[k])
+          F[k] = a.cap[k];
+        else if (F[k] < 0 && F[k] < -a.cap[k])
+          F[k] = -a.cap[k];
+      }
+    }
+    if (a.storeFtot) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) d.ftot[k * cap + i] = F[k];
+    }
+    const double dtfm = __ddiv_rn(__dmul_rn(0.5, a.dt), m);
+    if (a.do_i2) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) v[k] = __dadd_rn(v[k], __dmul_rn(dtfm, F[k]));
+    }
+    if (a.do_i1) {
+      double dp[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        v[k] = __dadd_rn(v[k], __dmul_rn(dtfm, F[k]));
+        dp[k] = __dmul_rn(v[k], a.dt);
+        x[k] = __dadd_rn(d.a.x[k * cap + i], dp[k]);
+        d.a.x[k * cap + i] = x[k];
+      }
+      sq = __dadd_rn(__dadd_rn(__dmul_rn(dp[0], dp[0]), __dmul_rn(dp[1], dp[1])),
+                     __dmul_rn(dp[2], dp[2]));
+      d.posq[i] = fixed_coords(d, x[0], x[1], x[2], d.a.type[i]);
+    }
+    if (a.do_i1 || a.do_i2) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) d.a.v[k * cap + i] = v[k];
+    }
+  }
+  if (a.do_i1) {
+    sq = warp_max(sq);
+    if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = sq;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      double v = threadIdx.x < blockDim.x / 32 ? smax[threadIdx.x] : 0.0;
+      v = warp_max(v);
+      if (threadIdx.x == 0 && v > 0.0)
+        atomicMax(d.maxSq, (unsigned long long)__double_as_longlong(v));
+    }
+  }
+}
+
+__global__ void k_decide(unsigned long long* maxSq, double* maxDist, int* flag,
+                         double skinHalf) {
+  double m = __longlong_as_double((long long)*maxSq);
+  *maxSq = 0ull;
+  double md = __dadd_rn(*maxDist, sqrt(m));
+  int f = md > skinHalf ? 1 : 0;
+  *maxDist = f ? 0.0 : md;
+  *flag = f;
+}
+
+// ---- observables -------------------------------------------------------------------
+
+template <int NV>
+__device__ void block_sum_store(double (&v)[NV], double* partials) {
+  __shared__ double sm[NV][kBlock / 32];
+#pragma unroll
+  for (int c = 0; c < NV; ++c) {
+    double t = v[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if ((threadIdx.x & 31) == 0) sm[c][threadIdx.x >> 5] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int c = 0; c < NV; ++c) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x / 32); ++w) t += sm[c][w];
+      partials[(size_t)blockIdx.x * NV + c] = t;
+    }
+  }
+}
+
+// Fixed-order sum of the block partials (one block) -> out[0..NV)
+template <int NV>
+__global__ void k_sum_partials(const double* __restrict__ partials, int nblocks, double* out) {
+  __shared__ double sm[NV][256];
+  double acc[NV];
+#pragma unroll
+  for (int c = 0; c < NV; ++c) acc[c] = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+#pragma unroll
+    for (int c = 0; c < NV; ++c) acc[c] += partials[(size_t)b * NV + c];
+#pragma unroll
+  for (int c = 0; c < NV; ++c) sm[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int c = 0; c < NV; ++c) {
+      double t = 0.0;
+      for (int w = 0; w < (int)blockDim.x; ++w) t += sm[c][w];
+      out[c] = t;
+    }
+  }
+}
+
+
+// LJ energy (energy=1: E = 4 eps ((sig^2/r^2)^6 - (sig^2/r^2)^3) - shift,
+// LennardJones.hpp:109-114) or virial r.F and its tensor (energy=0,
+// VerletListInteractionTemplate.hpp:274-331) over each listed pair once (j > i).
+__global__ void k_lj_obs(DevView d, int energy, double* partials) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (i < d.n) {
+    const double* X = d.a.x;
+    const double* Y = d.a.x + d.cap;
+    const double* Z = d.a.x + 2 * (size_t)d.cap;
+    const double xi = X[i], yi = Y[i], zi = Z[i];
+    const int ti = d.a.type[i];
+    const int cnt = d.nn[i];
+    for (int k = 0; k < cnt; ++k) {
+      const int j = d.nl[(size_t)k * d.cap + i];
+      if (j < i) continue;
+      const double dx = min_image(xi - X[j], d.L[0], d.halfL[0]);
+      const double dy = min_image(yi - Y[j], d.L[1], d.halfL[1]);
+      const double dz = min_image(zi - Z[j], d.L[2], d.halfL[2]);
+      const double r2 =
+          __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+      const LJPair& P = d.lj[ti * d.ntypes + d.a.type[j]];
+      if (!P.set || r2 > P.rcsq) continue;
+      if (energy) {
+        double ds = r2;
+        if (P.caprad > 0 && !(ds > P.caprad * P.caprad)) ds = P.caprad * P.caprad;
+        const double frac2 = __ddiv_rn(P.ef2, ds);
+        const double frac6 = __dmul_rn(__dmul_rn(frac2, frac2), frac2);
+        acc[0] += __dsub_rn(__dmul_rn(P.ef1, __dsub_rn(__dmul_rn(frac6, frac6), frac6)), P.shift);
+      } else {
+        double ff;
+        if (P.caprad > 0 && !(r2 > P.caprad * P.caprad)) {
+          ff = P.capff / sqrt(r2);
+        } else {
+          const double ri2 = 1.0 / r2;
+          const double ri6 = ri2 * ri2 * ri2;
+          ff = ri6 * (P.ff1 * ri6 - P.ff2) * ri2;
+        }
+        const double f0 = dx * ff, f1 = dy * ff, f2 = dz * ff;
+        acc[0] += dx * f0 + dy * f1 + dz * f2;
+        acc[1] += dx * f0;
+        acc[2] += dy * f1;
+        acc[3] += dz * f2;
+        acc[4] += dx * f1;
+        acc[5] += dx * f2;
+        acc[6] += dy * f2;
+      }
+    }
+  }
+  block_sum_store<7>(acc, partials);
+}
+
+// FENE energy (FENE.hpp:91-95) or virial over each bond once (partner id > own id).
+__global__ void k_fene_obs(DevView d, FENEParams fp, int energy, double* partials) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (i < d.n && fp.on) {
+    const double* X = d.a.x;
+    const double* Y = d.a.x + d.cap;
+    const double* Z = d.a.x + 2 * (size_t)d.cap;
+    const int64_t id = d.a.id[i];
+    const int64_t off = id - d.idMin;
+    const int b0 = d.bondStart[off], b1 = d.bondStart[off + 1];
+    for (int b = b0; b < b1; ++b) {
+      const int64_t pid = d.bondPartner[b];
+      if (pid <= id) continue;
+      const int j = d.id2idx[pid - d.idMin];
+      if (j < 0) continue;
+      const double dx = min_image(X[i] - X[j], d.L[0], d.halfL[0]);
+      const double dy = min_image(Y[i] - Y[j], d.L[1], d.halfL[1]);
+      const double dz = min_image(Z[i] - Z[j], d.L[2], d.halfL[2]);
+      const double r2 =
+          __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+      if (r2 > fp.rcsq) continue;
+      if (energy) {
+        const double q = (sqrt(r2) - fp.r0) / fp.rmax;
+        acc[0] += -0.5 * fp.rmaxsq * fp.K * log(1 - q * q) - fp.shift;
+      } else {
+        double ff;
+        if (fp.r0 > 2.220446049250313e-16) {
+          const double r = sqrt(r2);
+          ff = -fp.K * (r - fp.r0) / (r * (1 - ((r - fp.r0) * (r - fp.r0) / fp.rmaxsq)));
+        } else {
+          ff = -fp.K / (1.0 - r2 / fp.rmaxsq);
+        }
+        const double f0 = dx * ff, f1 = dy * ff, f2 = dz * ff;
+        acc[0] += dx * f0 + dy * f1 + dz * f2;
+        acc[1] += dx * f0;
+        acc[2] += dy * f1;
+        acc[3] += dz * f2;
+        acc[4] += dx * f1;
+        acc[5] += dx * f2;
+        acc[6] += dy * f2;
+      }
+    }
+  }
+  block_sum_store<7>(acc, partials);
+}
+
+// max bond length^2 over all bonds (FixedPairList::getLongtimeMaxBondSqr)
+__global__ void k_bond_maxsq(DevView d, double* partials) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[1] = {0.0};
+  __shared__ double sm[kBlock / 32];
+  if (i < d.n && d.bondStart) {
+    const int64_t off = d.a.id[i] - d.idMin;
+    for (int b = d.bondStart[off]; b < d.bondStart[off + 1]; ++b) {
+      const int j = d.id2idx[d.bondPartner[b] - d.idMin];
+      if (j < 0) continue;
+      double r2 = 0;
+      for (int k = 0; k < 3; ++k) {
+        const double dk = min_image(d.a.x[(size_t)k * d.cap + i] - d.a.x[(size_t)k * d.cap + j],
+                                    d.L[k], d.halfL[k]);
+        r2 += dk * dk;
+      }
+      acc[0] = fmax(acc[0], r2);
+    }
+  }
+  double v = warp_max(acc[0]);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) t = fmax(t, sm[w]);
+    partials[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_max_partials(const double* partials, int nb, double* out) {
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int b = 0; b < nb; ++b) t = fmax(t, partials[b]);
+    *out = t;
+  }
+}
+
+__global__ void k_kinetic(DevView d, double* partials) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[1] = {0.0};
+  if (i < d.n) {
+    const double vx = d.a.v[i], vy = d.a.v[(size_t)d.cap + i], vz = d.a.v[2 * (size_t)d.cap + i];
+    acc[0] = d.a.mass[i] * (vx * vx + vy * vy + vz * vz);
+  }
+  block_sum_store<1>(acc, partials);
+}
+
+__global__ void k_pair_count(DevView d, int32_t* counts) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n) return;
+  const int64_t idi = d.a.id[i];
+  int c = 0;
+  for (int k = 0; k < d.nn[i]; ++k) c += d.a.id[d.nl[(size_t)k * d.cap + i]] > idi;
+  counts[i] = c;
+}
+
+__global__ void k_pair_write(DevView d, const int64_t* offsets, int64_t* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n) return;
+  const int64_t idi = d.a.id[i];
+  int64_t o = offsets[i];
+  for (int k = 0; k < d.nn[i]; ++k) {
+    const int64_t idj = d.a.id[d.nl[(size_t)k * d.cap + i]];
+    if (idj > idi) {
+      out[2 * o] = idi;
+      out[2 * o + 1] = idj;
+      ++o;
+    }
+  }
+}
+
+}  // namespace
+
+// ---- launchers ---------------------------------------------------------------------
+
+void launch_fold_bin(const DevView& d, RebuildScratch& s, bool fold, cudaStream_t st) {
+  cudaMemsetAsync(s.cellCount, 0, sizeof(int32_t) * d.ncells, st);
+  if (d.n > 0) k_fold_bin<<<blocks_for(d.n), kBlock, 0, st>>>(d, s, fold ? 1 : 0);
+}
+
+void launch_sort_cells(const DevView& d, RebuildScratch& s, cudaStream_t st) {
+  k_scan_cells<<<1, 1024, 0, st>>>(s.cellCount, d.cellStart, d.ncells);
+  if (d.n > 0) k_scatter<<<blocks_for(d.n), kBlock, 0, st>>>(d, s);
+  k_sort_in_cell<<<blocks_for(d.ncells), kBlock, 0, st>>>(d, s);
+}
+
+void launch_gather(const DevView& d, const ParticleArrays& src, const ParticleArrays& dst,
+                   const RebuildScratch& s, cudaStream_t st) {
+  if (d.n > 0) k_gather<<<blocks_for(d.n), kBlock, 0, st>>>(d, src, dst, s);
+}
+
+void launch_id_map(const DevView& d, cudaStream_t st) {
+  if (d.n > 0) k_id_map<<<blocks_for(d.n), kBlock, 0, st>>>(d);
+}
+
+void launch_posq(const DevView& d, cudaStream_t st) {
+  if (d.n > 0) k_posq<<<blocks_for(d.n), kBlock, 0, st>>>(d);
+}
+
+void launch_build_nl(const DevView& d, double cutsq, cudaStream_t st) {
+  long long threads = (long long)d.ncells * 32;
+  k_build_nl<<<blocks_for(threads, 128), 128, 0, st>>>(d, cutsq);
+}
+
+template <int TPP, bool MIXED>
+static void force_dispatch(const DevView& d, bool single, bool capped, bool fene,
+                           const FENEParams& fp, cudaStream_t st) {
+  const int grid = blocks_for((long long)d.n * TPP);
+#define ESPP_FORCE_CASE(S, C, F)                                                   \
+  if (single == S && capped == C && fene == F) {                                   \
+    if (MIXED)                                                                     \
+      k_force_mixed<TPP, S, C, F><<<grid, kBlock, 0, st>>>(d, fp);                 \
+    else                                                                           \
+      k_force_fp64<TPP, S, C, F><<<grid, kBlock, 0, st>>>(d, fp);                  \
+    return;                                                                        \
+  }
+  ESPP_FORCE_CASE(true, false, false)
+  ESPP_FORCE_CASE(true, false, true)
+  ESPP_FORCE_CASE(true, true, false)
+  ESPP_FORCE_CASE(true, true, true)
+  ESPP_FORCE_CASE(false, false, false)
+  ESPP_FORCE_CASE(false, false, true)
+  ESPP_FORCE_CASE(false, true, false)
+  ESPP_FORCE_CASE(false, true, true)
+#undef ESPP_FORCE_CASE
+}
+
+void launch_forces(const DevView& d, bool mixed, const FENEParams& fp, int tpp,
+                   cudaStream_t st) {
+  if (d.n == 0) return;
+  const bool fene = fp.on != 0;
+  switch (tpp) {
+    case 2:
+      mixed ? force_dispatch<2, true>(d, d.ljSingle != 0, d.ljCapped != 0, fene, fp, st)
+            : force_dispatch<2, false>(d, d.ljSingle != 0, d.ljCapped != 0, fene, fp, st);
+      break;
+    case 4:
+      mixed ? force_dispatch<4, true>(d, d.ljSingle != 0, d.ljCapped != 0, fene, fp, st)
+            : force_dispatch<4, false>(d, d.ljSingle != 0, d.ljCapped != 0, fene, fp, st);
+      break;
+    case 8:
+      mixed ? force_dispatch<8, true>(d, d.ljSingle != 0, d.ljCapped != 0, fene, fp, st)
+            : force_dispatch<8, false>(d, d.ljSingle != 0, d.ljCapped != 0, fene, fp, st);
+      break;
+    default:
+      mixed ? force_dispatch<1, true>(d, d.ljSingle != 0, d.ljCapped != 0, fene, fp, st)
+            : force_dispatch<1, false>(d, d.ljSingle != 0, d.ljCapped != 0, fene, fp, st);
+  }
+}
+
+
+void launch_integrate(const DevView& d, const IntegrateArgs& a, cudaStream_t st) {
+  if (d.n == 0) return;
+  if (a.mixed)
+    k_integrate<true><<<blocks_for(d.n), kBlock, 0, st>>>(d, a);
+  else
+    k_integrate<false><<<blocks_for(d.n), kBlock, 0, st>>>(d, a);
+}
+
+void launch_decide(const DevView& d, double* maxDist, int* flag, double skinHalf,
+                   cudaStream_t st) {
+  k_decide<<<1, 1, 0, st>>>(d.maxSq, maxDist, flag, skinHalf);
+}
+
+void launch_lj_observables(const DevView& d, double* partials, int nblocks, double* out,
+                           int energy, cudaStream_t st) {
+  k_lj_obs<<<nblocks, kBlock, 0, st>>>(d, energy, partials);
+  k_sum_partials<7><<<1, 256, 0, st>>>(partials, nblocks, out);
+}
+
+void launch_fene_observables(const DevView& d, const FENEParams& fp, double* partials,
+                             int nblocks, double* out, int energy, cudaStream_t st) {
+  k_fene_obs<<<nblocks, kBlock, 0, st>>>(d, fp, energy, partials);
+  k_sum_partials<7><<<1, 256, 0, st>>>(partials, nblocks, out);
+}
+
+void launch_kinetic(const DevView& d, double* partials, int nblocks, double* out,
+                    cudaStream_t st) {
+  k_kinetic<<<nblocks, kBlock, 0, st>>>(d, partials);
+  k_sum_partials<1><<<1, 256, 0, st>>>(partials, nblocks, out);
+}
+
+void launch_bond_maxsq(const DevView& d, double* partials, int nblocks, double* out,
+                       cudaStream_t st) {
+  k_bond_maxsq<<<nblocks, kBlock, 0, st>>>(d, partials);
+  k_max_partials<<<1, 32, 0, st>>>(partials, nblocks, out);
+}
+
+void launch_pair_count(const DevView& d, int32_t* counts, cudaStream_t st) {
+  if (d.n > 0) k_pair_count<<<blocks_for(d.n), kBlock, 0, st>>>(d, counts);
+}
+
+void launch_pair_write(const DevView& d, const int64_t* offsets, int64_t* out,
+                       cudaStream_t st) {
+  if (d.n > 0) k_pair_write<<<blocks_for(d.n), kBlock, 0, st>>>(d, offsets, out);
+}
+
+int observable_blocks(int n) { return blocks_for(n > 0 ? n : 1); }
+
+}  // namespace espp

@@ -1,0 +1,159 @@
+/*
+ * espp_b200.h - C ABI of the B200 short-range MD step (cell binning, Verlet list,
+ * Lennard-Jones / FENE forces, velocity Verlet with Langevin thermostat).
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and returns an
+ * int status: 0 on success, a negative ESPP_E* code on failure.  The text of the last
+ * failure on the calling thread is available through espp_last_error().
+ *
+ * One espp_system is one simulation box with all of its particles resident on one
+ * GPU (the CUDA library, libespp_b200.so).  The same ABI is implemented on the host in
+ * FP64 by the test oracle; the two are compared call for call by the parity tests.
+ *
+ * Each entry point names the ESPResSo++ interface it replaces (paths inside the
+ * espressopp/espressopp source tree).  Arrays of 3-vectors are interleaved
+ * (x0,y0,z0,x1,...).  Particle identity is the 64-bit particle id of the reference.
+ * A handle is not thread safe; calls on one handle must be serialised by the caller.
+ */
+#ifndef ESPP_B200_H
+#define ESPP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define ESPP_API __attribute__((visibility("default")))
+#else
+#define ESPP_API
+#endif
+
+typedef struct espp_system espp_system;
+
+/* status codes */
+#define ESPP_OK 0
+#define ESPP_EINVAL (-1)    /* bad argument (message says which) */
+#define ESPP_ESTATE (-2)    /* call not valid in the current state */
+#define ESPP_ECUDA (-3)     /* CUDA runtime error */
+#define ESPP_ERANGE (-4)    /* value outside the supported range */
+#define ESPP_ENOMEM (-5)    /* allocation failed */
+#define ESPP_EOVERFLOW (-6) /* a fixed-capacity structure overflowed */
+#define ESPP_ETIMEOUT (-7)  /* a bounded device wait gave up */
+#define ESPP_ENAN (-8)      /* non-finite particle coordinate */
+
+/* precision modes */
+#define ESPP_PREC_FP64 0  /* all-FP64 pair forces (plain form) */
+#define ESPP_PREC_MIXED 1 /* FP32 pair forces, int64 2^-32 fixed-point sums, FP64 integrator */
+
+/* interaction kinds for the observable calls */
+#define ESPP_IA_LJ 0   /* VerletListLennardJones */
+#define ESPP_IA_FENE 1 /* FixedPairListFENE */
+
+/* force-capping modes (integrator::CapForce) */
+#define ESPP_CAP_OFF 0
+#define ESPP_CAP_ABS 1       /* |F| <= cap[0] */
+#define ESPP_CAP_COMPONENT 2 /* |F_d| <= cap[d] */
+
+ESPP_API int espp_abi_version(void);
+
+/* Copies the last error message of this thread (NUL terminated, truncated to cap) and
+ * returns its full length. */
+ESPP_API size_t espp_last_error(char* buf, size_t cap);
+
+/* ---- System + bc::OrthorhombicBC + storage::DomainDecomposition -------------------
+ * Replaces System (src/System.cpp:40-105), OrthorhombicBC::setBoxL
+ * (src/bc/OrthorhombicBC.cpp:40-50) and the DomainDecomposition constructor
+ * (src/storage/DomainDecomposition.cpp:70-85) on one node: nodeGrid = (1,1,1),
+ * halfCellInt = 1, cell grid as given (tools/decomp.py:322-342 computes it). */
+ESPP_API int espp_system_create(const double box[3], double skin, const int32_t cell_grid[3],
+                       int32_t precision, uint64_t seed, espp_system** out);
+ESPP_API int espp_system_destroy(espp_system* s);
+/* System::setSkin (src/System.cpp:75-93). */
+ESPP_API int espp_set_skin(espp_system* s, double skin);
+
+/* Storage::addParticle + property setters (src/storage/Storage.cpp:285-313,
+ * src/storage/Storage.py:233-330).  type/mass/vel may be NULL (defaults 0, 1.0, 0). */
+ESPP_API int espp_add_particles(espp_system* s, int64_t n, const int64_t* id, const int32_t* type,
+                       const double* mass, const double* pos, const double* vel);
+/* Storage::decompose (src/storage/Storage.cpp:598-604): fold, re-bin, rebuild lists. */
+ESPP_API int espp_decompose(espp_system* s);
+ESPP_API int espp_num_particles(espp_system* s, int64_t* n);
+/* Storage::lookupRealParticle + Particle accessors (src/Particle.hpp:44-410) for n ids.
+ * Any of pos/vel/force/image may be NULL. */
+ESPP_API int espp_get_particles(espp_system* s, int64_t n, const int64_t* ids, double* pos,
+                       double* vel, double* force, int32_t* image);
+/* Particle setters for existing ids (pos/vel may be NULL). */
+ESPP_API int espp_set_particles(espp_system* s, int64_t n, const int64_t* ids, const double* pos,
+                       const double* vel);
+
+/* ---- VerletList (src/VerletList.cpp:196-270, :274-450) ----------------------------
+ * cutoff is the interaction cutoff; the list holds pairs with |d| <= cutoff + skin.
+ * excl_pairs: nexcl id pairs never listed (VerletList::exclude, :480-485). */
+ESPP_API int espp_vl_create(espp_system* s, double cutoff, int64_t nexcl, const int64_t* excl_pairs);
+ESPP_API int espp_vl_rebuild(espp_system* s);
+/* VerletList::totalSize (:454-462). */
+ESPP_API int espp_vl_size(espp_system* s, int64_t* npairs);
+/* getAllPairs as unordered id pairs, each written (min id, max id), sorted
+ * lexicographically (testsuite/verlet_list_buffer/verlet_list_buffer.py sort_pairs).
+ * Writes at most cap pairs (2*cap int64); *npairs receives the total. */
+ESPP_API int espp_vl_pairs(espp_system* s, int64_t cap, int64_t* pairs, int64_t* npairs);
+ESPP_API int espp_vl_builds(espp_system* s, int64_t* builds);
+
+/* ---- interaction::LennardJones / LennardJonesCapped on the Verlet list -------------
+ * VerletListInteractionTemplate::setPotential (src/interaction/
+ * VerletListInteractionTemplate.hpp:65-78) with LennardJones(eps, sig, rc, shift)
+ * (src/interaction/LennardJones.hpp:56-87).  caprad > 0 selects LennardJonesCapped
+ * (src/interaction/LennardJonesCapped.hpp:80-160).  shift is the final energy shift. */
+ESPP_API int espp_lj_set(espp_system* s, int32_t type1, int32_t type2, double epsilon, double sigma,
+                double cutoff, double shift, double caprad);
+
+/* ---- FixedPairList + interaction::FENE --------------------------------------------
+ * FixedPairList::add (src/FixedPairList.cpp:88-141): pairs are id pairs. */
+ESPP_API int espp_bonds_add(espp_system* s, int64_t n, const int64_t* pairs);
+ESPP_API int espp_bonds_size(espp_system* s, int64_t* n);
+/* FixedPairListFENE(system, fpl, FENE(K, r0, rMax, cutoff, shift))
+ * (src/interaction/FENE.hpp:35-115, src/interaction/FENE.cpp:45-53). */
+ESPP_API int espp_fene_set(espp_system* s, double K, double r0, double rmax, double cutoff,
+                  double shift);
+/* FixedPairList::getLongtimeMaxBondSqr. */
+ESPP_API int espp_bonds_max_sqr(espp_system* s, double* maxsq);
+
+/* ---- integrator::VelocityVerlet + extensions ---------------------------------------
+ * MDIntegrator::setTimeStep (src/integrator/MDIntegrator.cpp:53-60). */
+ESPP_API int espp_integrator_set(espp_system* s, double dt);
+/* MDIntegrator step counter (read / write). */
+ESPP_API int espp_step_get(espp_system* s, int64_t* step);
+ESPP_API int espp_step_set(espp_system* s, int64_t step);
+/* LangevinThermostat gamma/temperature/exclusions (src/integrator/
+ * LangevinThermostat.cpp:41-214).  gamma == 0 and temperature == 0 disables it.  The
+ * noise is Philox4x32-10 keyed on (seed, particle id) with counter (step, phase). */
+ESPP_API int espp_langevin_set(espp_system* s, int32_t enabled, double gamma, double temperature,
+                      int64_t nexcl, const int64_t* excl_ids);
+/* CapForce (src/integrator/CapForce.cpp:34-200). */
+ESPP_API int espp_capforce_set(espp_system* s, int32_t mode, const double cap[3]);
+/* VelocityVerlet::run (src/integrator/VelocityVerlet.cpp:63-169). */
+ESPP_API int espp_run(espp_system* s, int64_t nsteps);
+/* VelocityVerlet::getNumResorts (:246). */
+ESPP_API int espp_num_resorts(espp_system* s, int64_t* n);
+/* VelocityVerlet::loadTimers (:206-218): run, pair, FENE, angle, comm1, comm2, int1,
+ * int2, resort, other (seconds). */
+ESPP_API int espp_timers(espp_system* s, double t[10]);
+
+/* ---- observables (FP64) --------------------------------------------------------
+ * Interaction::computeEnergy / computeVirial / computeVirialTensor
+ * (VerletListInteractionTemplate.hpp:201-331, FixedPairListInteractionTemplate.hpp:
+ * 207+, 400-440).  Tensor order xx, yy, zz, xy, xz, yz (src/Tensor.hpp:125-133). */
+ESPP_API int espp_energy(espp_system* s, int32_t which, double* e);
+ESPP_API int espp_virial(espp_system* s, int32_t which, double* w);
+ESPP_API int espp_virial_tensor(espp_system* s, int32_t which, double w[6]);
+/* sum m v^2 over real particles and their count (analysis/Temperature.hpp:57-125). */
+ESPP_API int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ESPP_B200_H */

@@ -1,0 +1,1048 @@
+// espp_oracle.cpp - TEST INFRASTRUCTURE ONLY.
+//
+// CPU FP64 restatement of ESPResSo++'s short-range MD step, used by the parity tests,
+// smoke() and bench.py's CPU-baseline leg as the checker.  Nothing in the product
+// links or calls this file.  It implements the same C ABI as the CUDA library
+// (include/espp_b200.h), so a test can drive both with identical calls.
+//
+// It follows the reference's data model on one MPI rank: a frame cell grid with one
+// layer of ghost cells, Particle records in per-cell vectors, ghosts refreshed by a
+// shifted copy each step, forces collected back from ghosts, and a half Verlet list of
+// (real, real-or-ghost) particle pointers.  Built with -O2 -std=c++17
+// -ffp-contract=off so that every product and sum rounds as in the reference build
+// (ISO C++17 mode, no FMA contraction).
+//
+// Langevin noise: the reference draws from boost::lagged_fibonacci607 in storage order
+// (src/esutil/RNG.cpp:60-66), which is not reproducible across implementations.  The
+// oracle and the GPU both use Philox4x32-10 (Salmon et al., SC'11) keyed on
+// (seed, particle id) with counter (step, phase), so Langevin runs compare exactly.
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <utility>
+#include <vector>
+
+#include "../include/espp_b200.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+// ---- Philox4x32-10 --------------------------------------------------------------
+struct U4 {
+  uint32_t v[4];
+};
+
+inline void mulhilo(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo) {
+  uint64_t p = (uint64_t)a * (uint64_t)b;
+  hi = (uint32_t)(p >> 32);
+  lo = (uint32_t)p;
+}
+
+U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
+  for (int r = 0; r < 10; ++r) {
+    if (r > 0) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    uint32_t hi0, lo0, hi1, lo1;
+    mulhilo(0xD2511F53u, c.v[0], hi0, lo0);
+    mulhilo(0xCD9E8D57u, c.v[2], hi1, lo1);
+    U4 n;
+    n.v[0] = hi1 ^ c.v[1] ^ k0;
+    n.v[1] = lo1;
+    n.v[2] = hi0 ^ c.v[3] ^ k1;
+    n.v[3] = lo0;
+    c = n;
+  }
+  return c;
+}
+
+// Three uniforms in (0,1) for (seed, id, step, phase).
+void langevin_uniforms(uint64_t seed, int64_t id, int64_t step, int phase, double u[3]) {
+  U4 c;
+  c.v[0] = (uint32_t)((uint64_t)id);
+  c.v[1] = (uint32_t)((uint64_t)id >> 32);
+  c.v[2] = (uint32_t)((uint64_t)step);
+  c.v[3] = ((uint32_t)((uint64_t)step >> 32) & 0x7FFFFFFFu) | ((uint32_t)phase << 31);
+  U4 r = philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  for (int d = 0; d < 3; ++d) u[d] = ((double)r.v[d] + 0.5) * (1.0 / 4294967296.0);
+}
+
+// ---- data model ------------------------------------------------------------------
+struct Particle {
+  int64_t id = 0;
+  int32_t type = 0;
+  double mass = 1.0;
+  double r[3] = {0, 0, 0};
+  double v[3] = {0, 0, 0};
+  double f[3] = {0, 0, 0};
+  int32_t img[3] = {0, 0, 0};
+  bool ghost = false;
+};
+
+struct NeighborCell {
+  int cell;
+  bool useForAllPairs;  // true: neighbour index < own index (not part of the half shell)
+};
+
+struct Cell {
+  std::vector<Particle> p;
+  std::vector<NeighborCell> nbrs;
+};
+
+struct LJParams {
+  bool set = false;
+  double eps = 0, sig = 0, rc = 0, rcsq = 0, shift = 0, caprad = 0;
+  double ff1 = 0, ff2 = 0;
+};
+
+}  // namespace
+
+struct espp_system {
+  double L[3], invL[3], L2[3];
+  double skin;
+  int precision;
+  uint64_t seed;
+  int n[3], F[3];  // inner cells, frame cells (n + 2)
+  double cellSize[3], invCellSize[3];
+  std::vector<Cell> cells;
+  std::vector<int> realCells, ghostCells;
+  std::vector<int> commReals[6], commGhosts[6];
+  std::unordered_map<int64_t, std::pair<int, int>> where;  // id -> (cell, slot) for reals
+
+  // Verlet list
+  bool has_vl = false;
+  double vl_cut = 0, vl_cutVerlet = 0, vl_cutsq = 0;
+  std::set<std::pair<int64_t, int64_t>> exList;
+  std::vector<std::pair<Particle*, Particle*>> vlPairs;
+  int64_t builds = 0;
+  int max_type = 0;
+
+  // potentials
+  std::map<std::pair<int, int>, LJParams> lj;
+  bool fene_on = false;
+  double fK = 0, fr0 = 0, frmax = 0, frmaxsq = 0, frc = 0, frcsq = 0, fshift = 0;
+  std::vector<std::pair<int64_t, int64_t>> bondsGlobal;
+  std::vector<std::pair<Particle*, Particle*>> bondPtrs;
+  double ltMaxBondSqr = 0;
+
+  // integrator
+  double dt = 0.005;
+  int64_t step = 0;
+  double maxDist = 0;
+  bool resortFlag = true;
+  int64_t nResorts = 0;
+  bool lang_on = false;
+  double gamma = 0, temperature = 0, pref1 = 0, pref2 = 0, pref2buffer = 0;
+  std::set<int64_t> langExcl;
+  int capMode = ESPP_CAP_OFF;
+  double cap[3] = {0, 0, 0};
+  int langPhase = 0;
+};
+
+namespace {
+
+const double ROUND_ERROR_PREC = std::numeric_limits<double>::epsilon();
+
+int cellIndex(const espp_system* s, int m, int n, int o) {
+  return m + s->F[0] * (n + s->F[1] * o);
+}
+
+// OrthorhombicBC::foldCoordinate (src/bc/OrthorhombicBC.cpp:144-161).
+void foldCoordinate(const espp_system* s, double* pos, int32_t* img, int dir) {
+  int tmp = static_cast<int>(std::floor(pos[dir] * s->invL[dir]));
+  img[dir] += tmp;
+  pos[dir] -= tmp * s->L[dir];
+}
+
+// CellGrid::mapPositionToCellClipped (src/storage/CellGrid.cpp:87-107), myLeft = 0.
+int mapClipped(const espp_system* s, const double* pos) {
+  int c[3];
+  for (int i = 0; i < 3; ++i) {
+    double lpos = pos[i] - 0.0;
+    c[i] = static_cast<int>(lpos * s->invCellSize[i]) + 1;
+    if (c[i] < 1)
+      c[i] = 1;
+    else if (c[i] >= s->F[i] - 1)
+      c[i] = s->F[i] - 2;
+  }
+  return cellIndex(s, c[0], c[1], c[2]);
+}
+
+// CellGrid::mapPositionToCellChecked (src/storage/CellGrid.cpp:109-145); -1 = noCell.
+int mapChecked(const espp_system* s, const double* pos) {
+  int c[3];
+  for (int i = 0; i < 3; ++i) {
+    double lpos = pos[i] - 0.0;
+    c[i] = static_cast<int>(lpos * s->invCellSize[i]) + 1;
+    if (c[i] < 1) {
+      if (lpos >= -ROUND_ERROR_PREC)
+        c[i] = 1;
+      else
+        return -1;
+    } else if (c[i] >= s->F[i] - 1) {
+      if (pos[i] <= s->L[i] + ROUND_ERROR_PREC)
+        c[i] = s->F[i] - 2;
+      else
+        return -1;
+    }
+  }
+  return cellIndex(s, c[0], c[1], c[2]);
+}
+
+void reindex(espp_system* s) {
+  s->where.clear();
+  for (int ci : s->realCells) {
+    auto& P = s->cells[ci].p;
+    for (size_t k = 0; k < P.size(); ++k) s->where[P[k].id] = {ci, (int)k};
+  }
+}
+
+Particle* lookup(espp_system* s, int64_t id) {
+  auto it = s->where.find(id);
+  if (it == s->where.end()) return nullptr;
+  return &s->cells[it->second.first].p[it->second.second];
+}
+
+// DomainDecomposition::createCellGrid/markCells/initCellInteractions/
+// prepareGhostCommunication (src/storage/DomainDecomposition.cpp:87-170, 325-374,
+// 1243-1308) for nodeGrid (1,1,1) and halfCellInt 1.
+void buildGrid(espp_system* s) {
+  for (int i = 0; i < 3; ++i) {
+    s->F[i] = s->n[i] + 2;
+    s->cellSize[i] = (s->L[i] - 0.0) / double(s->n[i]);
+    s->invCellSize[i] = 1.0 / s->cellSize[i];
+  }
+  s->cells.assign((size_t)s->F[0] * s->F[1] * s->F[2], Cell());
+  s->realCells.clear();
+  s->ghostCells.clear();
+  for (int o = 0; o < s->F[2]; ++o)
+    for (int n = 0; n < s->F[1]; ++n)
+      for (int m = 0; m < s->F[0]; ++m) {
+        bool inner = m >= 1 && m < s->F[0] - 1 && n >= 1 && n < s->F[1] - 1 && o >= 1 &&
+                     o < s->F[2] - 1;
+        (inner ? s->realCells : s->ghostCells).push_back(cellIndex(s, m, n, o));
+      }
+  for (int o = 1; o < s->F[2] - 1; ++o)
+    for (int n = 1; n < s->F[1] - 1; ++n)
+      for (int m = 1; m < s->F[0] - 1; ++m) {
+        int ci = cellIndex(s, m, n, o);
+        for (int p = o - 1; p <= o + 1; ++p)
+          for (int q = n - 1; q <= n + 1; ++q)
+            for (int r = m - 1; r <= m + 1; ++r)
+              if (p != o || q != n || r != m) {
+                int c2 = cellIndex(s, r, q, p);
+                s->cells[ci].nbrs.push_back({c2, c2 < ci});
+              }
+      }
+  // ghost communication cell lists (fillCells order: z outer, y, x inner)
+  auto fill = [&](std::vector<int>& out, const int lb[3], const int rb[3]) {
+    out.clear();
+    for (int o = lb[2]; o < rb[2]; ++o)
+      for (int n = lb[1]; n < rb[1]; ++n)
+        for (int m = lb[0]; m < rb[0]; ++m) out.push_back(cellIndex(s, m, n, o));
+  };
+  for (int coord = 0; coord < 3; ++coord) {
+    int lb[3], rb[3];
+    for (int off = 1; off <= 2; ++off) {
+      int oc = (coord + off) % 3;
+      if (oc < coord) {
+        lb[oc] = 0;
+        rb[oc] = s->F[oc];
+      } else {
+        lb[oc] = 1;
+        rb[oc] = s->F[oc] - 1;
+      }
+    }
+    for (int lr = 0; lr < 2; ++lr) {
+      int dir = 2 * coord + lr;
+      if (lr == 0) {
+        lb[coord] = 1;
+        rb[coord] = 2;
+      } else {
+        lb[coord] = s->F[coord] - 2;
+        rb[coord] = s->F[coord] - 1;
+      }
+      fill(s->commReals[dir], lb, rb);
+      if (lr == 0) {
+        lb[coord] = s->F[coord] - 1;
+        rb[coord] = s->F[coord];
+      } else {
+        lb[coord] = 0;
+        rb[coord] = 1;
+      }
+      fill(s->commGhosts[dir], lb, rb);
+    }
+  }
+}
+
+// DomainDecomposition::doGhostCommunication, local-copy branch (:1347-1391).
+// realToGhosts with full copies (exchangeGhosts) or positions only (updateGhosts);
+// ghost-to-real force collection in reverse direction order.
+void ghostComm(espp_system* s, bool realToGhosts, bool fullCopy) {
+  for (int _coord = 0; _coord < 3; ++_coord) {
+    int coord = realToGhosts ? _coord : (2 - _coord);
+    for (int lr = 0; lr < 2; ++lr) {
+      int dir = 2 * coord + lr;
+      double shift[3] = {0, 0, 0};
+      shift[coord] = (lr == 0 ? 1.0 : -1.0) * s->L[coord];
+      auto& R = s->commReals[dir];
+      auto& G = s->commGhosts[dir];
+      for (size_t i = 0; i < G.size(); ++i) {
+        auto& reals = s->cells[R[i]].p;
+        auto& ghosts = s->cells[G[i]].p;
+        if (realToGhosts) {
+          if (fullCopy) ghosts.resize(reals.size());
+          for (size_t k = 0; k < reals.size(); ++k) {
+            Particle& g = ghosts[k];
+            const Particle& r = reals[k];
+            if (fullCopy) {
+              g = r;
+              g.ghost = true;
+            }
+            for (int d = 0; d < 3; ++d) g.r[d] = r.r[d] + shift[d];
+          }
+        } else {
+          for (size_t k = 0; k < reals.size(); ++k)
+            for (int d = 0; d < 3; ++d) reals[k].f[d] += ghosts[k].f[d];
+        }
+      }
+    }
+  }
+}
+
+bool excluded(const espp_system* s, int64_t a, int64_t b) {
+  return s->exList.count({a, b}) == 1 || s->exList.count({b, a}) == 1;
+}
+
+// VerletList::rebuild + _rebuildUsingBuffers<EXCL, AoS> + checkPair
+// (src/VerletList.cpp:238-270, 274-430, 434-450).
+void vlRebuild(espp_system* s) {
+  s->vl_cutVerlet = s->vl_cut + s->skin;
+  s->vl_cutsq = s->vl_cutVerlet * s->vl_cutVerlet;
+  s->vlPairs.clear();
+  std::vector<Particle*> cp;
+  std::vector<std::array<double, 3>> cpos;
+  for (int ci : s->realCells) {
+    Cell& cell = s->cells[ci];
+    cp.clear();
+    cpos.clear();
+    for (const NeighborCell& nc : cell.nbrs) {
+      if (nc.useForAllPairs) continue;
+      for (Particle& p : s->cells[nc.cell].p) {
+        cp.push_back(&p);
+        cpos.push_back({p.r[0], p.r[1], p.r[2]});
+      }
+    }
+    auto& P = cell.p;
+    for (size_t a = 0; a < P.size(); ++a) {
+      Particle& p1 = P[a];
+      for (size_t b = a + 1; b < P.size(); ++b) {
+        Particle& p2 = P[b];
+        double d0 = p1.r[0] - p2.r[0], d1 = p1.r[1] - p2.r[1], d2 = p1.r[2] - p2.r[2];
+        double dsq = d0 * d0 + d1 * d1 + d2 * d2;
+        if (dsq > s->vl_cutsq) continue;
+        if (excluded(s, p1.id, p2.id)) continue;
+        s->max_type = std::max(s->max_type, std::max(p1.type, p2.type));
+        s->vlPairs.push_back({&p1, &p2});
+      }
+      for (size_t b = 0; b < cp.size(); ++b) {
+        double d0 = p1.r[0] - cpos[b][0], d1 = p1.r[1] - cpos[b][1],
+               d2 = p1.r[2] - cpos[b][2];
+        double dsq = d0 * d0 + d1 * d1 + d2 * d2;
+        if (dsq > s->vl_cutsq) continue;
+        if (excluded(s, p1.id, cp[b]->id)) continue;
+        s->max_type = std::max(s->max_type, std::max(p1.type, cp[b]->type));
+        s->vlPairs.push_back({&p1, cp[b]});
+      }
+    }
+  }
+  s->builds++;
+}
+
+// FixedPairList::onParticlesChanged (src/FixedPairList.cpp:275-315): both ends resolve
+// to the real particle on one rank.
+void bondsRefresh(espp_system* s) {
+  s->bondPtrs.clear();
+  for (auto& b : s->bondsGlobal) {
+    Particle* p1 = lookup(s, b.first);
+    Particle* p2 = lookup(s, b.second);
+    if (p1 && p2) s->bondPtrs.push_back({p1, p2});
+  }
+}
+
+void onParticlesChanged(espp_system* s) {
+  if (s->has_vl) vlRebuild(s);
+  bondsRefresh(s);
+}
+
+// DomainDecomposition::decomposeRealParticles, one-node branch (:1031-1158), then
+// exchangeGhosts and the onParticlesChanged signal (Storage::decompose,
+// src/storage/Storage.cpp:598-604).
+int decompose(espp_system* s) {
+  for (int coord = 0; coord < 3; ++coord) {
+    for (int ci : s->realCells) {
+      auto& P = s->cells[ci].p;
+      for (size_t k = 0; k < P.size(); ++k) {
+        Particle& part = P[k];
+        foldCoordinate(s, part.r, part.img, coord);
+        if (coord == 2) {
+          int sc = mapChecked(s, part.r);
+          if (sc != ci) {
+            if (sc < 0) {
+              return fail(ESPP_ENAN, "particle " + std::to_string(part.id) +
+                                         " has moved to outer space");
+            }
+            s->cells[sc].p.push_back(part);
+            size_t last = P.size() - 1;
+            if (k != last) P[k] = P[last];
+            P.resize(last);
+            --k;
+          }
+        }
+      }
+    }
+  }
+  reindex(s);
+  ghostComm(s, true, true);
+  onParticlesChanged(s);
+  return ESPP_OK;
+}
+
+// Potential::_computeForce + LennardJones::_computeForceRaw / LennardJonesCapped
+// (src/interaction/Potential.hpp:422-431, LennardJones.hpp:137-143,
+// LennardJonesCapped.hpp:140-160).
+bool ljForce(const LJParams& P, const double d[3], double f[3]) {
+  double distSqr = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  if (distSqr > P.rcsq) return false;
+  double ffactor;
+  if (P.caprad > 0 && !(distSqr > P.caprad * P.caprad)) {
+    double frac2 = (P.sig / P.caprad) * (P.sig / P.caprad);
+    double frac6 = frac2 * frac2 * frac2;
+    ffactor = 48.0 * P.eps * frac6 * (frac6 - 0.5) / (P.caprad * std::sqrt(distSqr));
+  } else {
+    double frac2 = 1.0 / distSqr;
+    double frac6 = frac2 * frac2 * frac2;
+    ffactor = frac6 * (P.ff1 * frac6 - P.ff2) * frac2;
+  }
+  for (int k = 0; k < 3; ++k) f[k] = d[k] * ffactor;
+  return true;
+}
+
+// LennardJones::_computeEnergySqrRaw (LennardJones.hpp:109-114) / capped variant.
+double ljEnergyRaw(const LJParams& P, double distSqr) {
+  if (P.caprad > 0 && !(distSqr > P.caprad * P.caprad)) distSqr = P.caprad * P.caprad;
+  double frac2 = P.sig * P.sig / distSqr;
+  double frac6 = frac2 * frac2 * frac2;
+  return 4.0 * P.eps * (frac6 * frac6 - frac6);
+}
+
+double ljEnergy(const LJParams& P, double distSqr) {
+  if (distSqr > P.rcsq) return 0.0;
+  return ljEnergyRaw(P, distSqr) - P.shift;
+}
+
+// OrthorhombicBC::getMinimumImageVectorBox (src/bc/OrthorhombicBC.cpp:86-105).
+void minImageBox(const espp_system* s, const double* a, const double* b, double d[3]) {
+  for (int k = 0; k < 3; ++k) {
+    d[k] = a[k] - b[k];
+    if (d[k] < -s->L2[k])
+      d[k] += s->L[k];
+    else if (d[k] > s->L2[k])
+      d[k] -= s->L[k];
+  }
+}
+
+// FENE::_computeForceRaw / _computeEnergySqrRaw (src/interaction/FENE.hpp:91-112).
+bool feneForce(const espp_system* s, const double d[3], double f[3]) {
+  double distSqr = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  if (distSqr > s->frcsq) return false;
+  double ffactor;
+  if (s->fr0 > ROUND_ERROR_PREC) {
+    double r = std::sqrt(distSqr);
+    ffactor = -s->fK * (r - s->fr0) / (r * (1 - ((r - s->fr0) * (r - s->fr0) / s->frmaxsq)));
+  } else {
+    ffactor = -s->fK / (1.0 - distSqr / s->frmaxsq);
+  }
+  for (int k = 0; k < 3; ++k) f[k] = d[k] * ffactor;
+  return true;
+}
+
+double feneEnergy(const espp_system* s, double distSqr) {
+  if (distSqr > s->frcsq) return 0.0;
+  double e = -0.5 * s->frmaxsq * s->fK *
+             std::log(1 - std::pow((std::sqrt(distSqr) - s->fr0) / s->frmax, 2));
+  return e - s->fshift;
+}
+
+const LJParams* ljFor(const espp_system* s, int t1, int t2) {
+  auto it = s->lj.find({std::min(t1, t2), std::max(t1, t2)});
+  if (it == s->lj.end() || !it->second.set) return nullptr;
+  return &it->second;
+}
+
+// VelocityVerlet::updateForces / calcForces / initForces (:307-371) with
+// VerletListInteractionTemplate::addForces (:116-198), FixedPairList template
+// addForces (:112-205) and the aftCalcF extensions.
+void updateForces(espp_system* s) {
+  ghostComm(s, true, false);
+  for (auto& c : s->cells)
+    for (auto& p : c.p) p.f[0] = p.f[1] = p.f[2] = 0.0;
+  if (s->has_vl) {
+    for (auto& pr : s->vlPairs) {
+      Particle& p1 = *pr.first;
+      Particle& p2 = *pr.second;
+      const LJParams* P = ljFor(s, p1.type, p2.type);
+      if (!P) continue;
+      double d[3] = {p1.r[0] - p2.r[0], p1.r[1] - p2.r[1], p1.r[2] - p2.r[2]};
+      double f[3];
+      if (ljForce(*P, d, f))
+        for (int k = 0; k < 3; ++k) {
+          p1.f[k] += f[k];
+          p2.f[k] -= f[k];
+        }
+    }
+  }
+  if (s->fene_on) {
+    for (auto& pr : s->bondPtrs) {
+      Particle& p1 = *pr.first;
+      Particle& p2 = *pr.second;
+      double d[3];
+      minImageBox(s, p1.r, p2.r, d);
+      double dsq = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+      if (dsq > s->ltMaxBondSqr) s->ltMaxBondSqr = dsq;
+      double f[3];
+      if (feneForce(s, d, f))
+        for (int k = 0; k < 3; ++k) {
+          p1.f[k] += f[k];
+          p2.f[k] -= f[k];
+        }
+    }
+  }
+  ghostComm(s, false, false);
+  // aftCalcF: LangevinThermostat::thermalize (:105-177), then CapForce (at_back).
+  if (s->lang_on) {
+    for (int ci : s->realCells)
+      for (auto& p : s->cells[ci].p) {
+        if (s->langExcl.count(p.id)) continue;
+        double massf = std::sqrt(p.mass);
+        double u[3];
+        langevin_uniforms(s->seed, p.id, s->step, s->langPhase, u);
+        for (int k = 0; k < 3; ++k) {
+          double ranval = u[k] - 0.5;
+          p.f[k] += s->pref1 * p.v[k] * p.mass + s->pref2 * ranval * massf;
+        }
+      }
+  }
+  if (s->capMode == ESPP_CAP_ABS) {
+    double capfsq = s->cap[0] * s->cap[0];
+    for (int ci : s->realCells)
+      for (auto& p : s->cells[ci].p) {
+        double fsq = p.f[0] * p.f[0] + p.f[1] * p.f[1] + p.f[2] * p.f[2];
+        if (fsq > capfsq) {
+          double scaling = std::sqrt(capfsq / fsq);
+          for (int k = 0; k < 3; ++k) p.f[k] *= scaling;
+        }
+      }
+  } else if (s->capMode == ESPP_CAP_COMPONENT) {
+    for (int ci : s->realCells)
+      for (auto& p : s->cells[ci].p)
+        for (int k = 0; k < 3; ++k) {
+          if (p.f[k] > 0 && p.f[k] > s->cap[k])
+            p.f[k] = s->cap[k];
+          else if (p.f[k] < 0 && p.f[k] < -s->cap[k])
+            p.f[k] = -s->cap[k];
+        }
+  }
+}
+
+// VelocityVerlet::integrate1 / integrate2 (:236-305).
+double integrate1(espp_system* s) {
+  double maxSqDist = 0.0;
+  for (int ci : s->realCells)
+    for (auto& p : s->cells[ci].p) {
+      double dtfm = 0.5 * s->dt / p.mass;
+      double sq = 0.0;
+      double dp[3];
+      for (int k = 0; k < 3; ++k) {
+        p.v[k] += dtfm * p.f[k];
+        dp[k] = p.v[k];
+        dp[k] *= s->dt;
+        p.r[k] += dp[k];
+      }
+      sq += dp[0] * dp[0] + dp[1] * dp[1] + dp[2] * dp[2];
+      maxSqDist = std::max(maxSqDist, sq);
+    }
+  return std::sqrt(maxSqDist);
+}
+
+void integrate2(espp_system* s) {
+  double half_dt = 0.5 * s->dt;
+  for (int ci : s->realCells)
+    for (auto& p : s->cells[ci].p) {
+      double dtfm = half_dt / p.mass;
+      for (int k = 0; k < 3; ++k) p.v[k] += dtfm * p.f[k];
+    }
+  s->step++;
+}
+
+// VelocityVerlet::run (:63-169) with the Langevin runInit/recalc hooks (:179-214).
+int run(espp_system* s, int64_t nsteps) {
+  double skinHalf = 0.5 * s->skin;
+  s->nResorts = 0;
+  if (s->lang_on) {
+    s->pref1 = -s->gamma;
+    s->pref2 = std::sqrt(24.0 * s->temperature * s->gamma / s->dt);
+  }
+  if (s->resortFlag) {
+    int rc = decompose(s);
+    if (rc) return rc;
+    s->maxDist = 0.0;
+    s->resortFlag = false;
+  }
+  if (s->lang_on) {
+    s->pref2buffer = s->pref2;
+    s->pref2 *= std::sqrt(3.0);
+  }
+  s->langPhase = 1;
+  updateForces(s);
+  s->langPhase = 0;
+  if (s->lang_on) s->pref2 = s->pref2buffer;
+  for (int64_t i = 0; i < nsteps; ++i) {
+    s->maxDist += integrate1(s);
+    if (s->maxDist > skinHalf) s->resortFlag = true;
+    if (s->resortFlag) {
+      int rc = decompose(s);
+      if (rc) return rc;
+      s->maxDist = 0.0;
+      s->resortFlag = false;
+      s->nResorts++;
+    }
+    updateForces(s);
+    integrate2(s);
+  }
+  return ESPP_OK;
+}
+
+#define CHECK_S(s)                                              \
+  do {                                                          \
+    if (!(s)) return fail(ESPP_EINVAL, "null system handle"); \
+  } while (0)
+
+}  // namespace
+
+extern "C" {
+
+int espp_abi_version(void) { return 1; }
+
+size_t espp_last_error(char* buf, size_t cap) {
+  if (buf && cap) {
+    size_t n = std::min(cap - 1, g_err.size());
+    std::memcpy(buf, g_err.data(), n);
+    buf[n] = 0;
+  }
+  return g_err.size();
+}
+
+int espp_system_create(const double box[3], double skin, const int32_t cell_grid[3],
+                       int32_t precision, uint64_t seed, espp_system** out) {
+  if (!box || !cell_grid || !out) return fail(ESPP_EINVAL, "null argument");
+  for (int i = 0; i < 3; ++i) {
+    if (!(box[i] > 0)) return fail(ESPP_EINVAL, "box lengths must be positive");
+    if (cell_grid[i] <= 0) return fail(ESPP_EINVAL, "cell grid dimensions have to be positive");
+  }
+  espp_system* s = new espp_system();
+  for (int i = 0; i < 3; ++i) {
+    s->L[i] = box[i];
+    s->invL[i] = 1.0 / box[i];
+    s->L2[i] = 0.5 * box[i];
+    s->n[i] = cell_grid[i];
+  }
+  s->skin = skin;
+  s->precision = precision;
+  s->seed = seed;
+  buildGrid(s);
+  *out = s;
+  return ESPP_OK;
+}
+
+int espp_system_destroy(espp_system* s) {
+  delete s;
+  return ESPP_OK;
+}
+
+int espp_set_skin(espp_system* s, double skin) {
+  CHECK_S(s);
+  s->skin = skin;
+  return ESPP_OK;
+}
+
+int espp_add_particles(espp_system* s, int64_t n, const int64_t* id, const int32_t* type,
+                       const double* mass, const double* pos, const double* vel) {
+  CHECK_S(s);
+  if (n < 0 || (n > 0 && (!id || !pos))) return fail(ESPP_EINVAL, "bad particle arrays");
+  for (int64_t i = 0; i < n; ++i) {
+    if (s->where.count(id[i])) return fail(ESPP_EINVAL, "duplicate particle id");
+    Particle p;
+    p.id = id[i];
+    p.type = type ? type[i] : 0;
+    p.mass = mass ? mass[i] : 1.0;
+    for (int k = 0; k < 3; ++k) {
+      p.r[k] = pos[3 * i + k];
+      p.v[k] = vel ? vel[3 * i + k] : 0.0;
+    }
+    for (int k = 0; k < 3; ++k) foldCoordinate(s, p.r, p.img, k);
+    int c = mapClipped(s, p.r);
+    s->cells[c].p.push_back(p);
+    s->where[p.id] = {c, (int)s->cells[c].p.size() - 1};
+  }
+  s->resortFlag = true;
+  return ESPP_OK;
+}
+
+int espp_decompose(espp_system* s) {
+  CHECK_S(s);
+  int rc = decompose(s);
+  if (rc) return rc;
+  s->maxDist = 0.0;
+  s->resortFlag = false;
+  return ESPP_OK;
+}
+
+int espp_num_particles(espp_system* s, int64_t* n) {
+  CHECK_S(s);
+  *n = (int64_t)s->where.size();
+  return ESPP_OK;
+}
+
+int espp_get_particles(espp_system* s, int64_t n, const int64_t* ids, double* pos,
+                       double* vel, double* force, int32_t* image) {
+  CHECK_S(s);
+  for (int64_t i = 0; i < n; ++i) {
+    Particle* p = lookup(s, ids[i]);
+    if (!p) return fail(ESPP_EINVAL, "unknown particle id " + std::to_string(ids[i]));
+    for (int k = 0; k < 3; ++k) {
+      if (pos) pos[3 * i + k] = p->r[k];
+      if (vel) vel[3 * i + k] = p->v[k];
+      if (force) force[3 * i + k] = p->f[k];
+      if (image) image[3 * i + k] = p->img[k];
+    }
+  }
+  return ESPP_OK;
+}
+
+int espp_set_particles(espp_system* s, int64_t n, const int64_t* ids, const double* pos,
+                       const double* vel) {
+  CHECK_S(s);
+  for (int64_t i = 0; i < n; ++i) {
+    Particle* p = lookup(s, ids[i]);
+    if (!p) return fail(ESPP_EINVAL, "unknown particle id " + std::to_string(ids[i]));
+    for (int k = 0; k < 3; ++k) {
+      if (pos) p->r[k] = pos[3 * i + k];
+      if (vel) p->v[k] = vel[3 * i + k];
+    }
+  }
+  if (pos) s->resortFlag = true;
+  return ESPP_OK;
+}
+
+int espp_vl_create(espp_system* s, double cutoff, int64_t nexcl, const int64_t* excl) {
+  CHECK_S(s);
+  s->has_vl = true;
+  s->vl_cut = cutoff;
+  for (int64_t i = 0; i < nexcl; ++i) s->exList.insert({excl[2 * i], excl[2 * i + 1]});
+  vlRebuild(s);
+  return ESPP_OK;
+}
+
+int espp_vl_rebuild(espp_system* s) {
+  CHECK_S(s);
+  if (!s->has_vl) return fail(ESPP_ESTATE, "no Verlet list");
+  vlRebuild(s);
+  return ESPP_OK;
+}
+
+int espp_vl_size(espp_system* s, int64_t* npairs) {
+  CHECK_S(s);
+  *npairs = (int64_t)s->vlPairs.size();
+  return ESPP_OK;
+}
+
+int espp_vl_pairs(espp_system* s, int64_t cap, int64_t* pairs, int64_t* npairs) {
+  CHECK_S(s);
+  std::vector<std::pair<int64_t, int64_t>> v;
+  v.reserve(s->vlPairs.size());
+  for (auto& pr : s->vlPairs) {
+    int64_t a = pr.first->id, b = pr.second->id;
+    v.push_back({std::min(a, b), std::max(a, b)});
+  }
+  std::sort(v.begin(), v.end());
+  *npairs = (int64_t)v.size();
+  for (int64_t i = 0; i < std::min<int64_t>(cap, (int64_t)v.size()); ++i) {
+    pairs[2 * i] = v[i].first;
+    pairs[2 * i + 1] = v[i].second;
+  }
+  return ESPP_OK;
+}
+
+int espp_vl_builds(espp_system* s, int64_t* builds) {
+  CHECK_S(s);
+  *builds = s->builds;
+  return ESPP_OK;
+}
+
+int espp_lj_set(espp_system* s, int32_t t1, int32_t t2, double eps, double sig, double rc,
+                double shift, double caprad) {
+  CHECK_S(s);
+  LJParams P;
+  P.set = true;
+  P.eps = eps;
+  P.sig = sig;
+  P.rc = rc;
+  P.rcsq = rc * rc;
+  P.shift = shift;
+  P.caprad = caprad;
+  double sig2 = sig * sig;
+  double sig6 = sig2 * sig2 * sig2;
+  P.ff1 = 48.0 * eps * sig6 * sig6;
+  P.ff2 = 24.0 * eps * sig6;
+  s->lj[{std::min(t1, t2), std::max(t1, t2)}] = P;
+  return ESPP_OK;
+}
+
+int espp_bonds_add(espp_system* s, int64_t n, const int64_t* pairs) {
+  CHECK_S(s);
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t a = pairs[2 * i], b = pairs[2 * i + 1];
+    if (a > b) std::swap(a, b);
+    if (!lookup(s, a) || !lookup(s, b))
+      return fail(ESPP_EINVAL, "bond partner does not exist");
+    s->bondsGlobal.push_back({a, b});
+  }
+  bondsRefresh(s);
+  return ESPP_OK;
+}
+
+int espp_bonds_size(espp_system* s, int64_t* n) {
+  CHECK_S(s);
+  *n = (int64_t)s->bondsGlobal.size();
+  return ESPP_OK;
+}
+
+int espp_fene_set(espp_system* s, double K, double r0, double rmax, double rc,
+                  double shift) {
+  CHECK_S(s);
+  s->fene_on = true;
+  s->fK = K;
+  s->fr0 = r0;
+  s->frmax = rmax;
+  s->frmaxsq = rmax * rmax;
+  s->frc = rc;
+  s->frcsq = rc * rc;
+  s->fshift = shift;
+  return ESPP_OK;
+}
+
+int espp_bonds_max_sqr(espp_system* s, double* m) {
+  CHECK_S(s);
+  *m = s->ltMaxBondSqr;
+  return ESPP_OK;
+}
+
+int espp_integrator_set(espp_system* s, double dt) {
+  CHECK_S(s);
+  if (dt == 0.0) return fail(ESPP_EINVAL, "Timestep 'dt' must be non-zero!");
+  s->dt = dt;
+  return ESPP_OK;
+}
+
+int espp_step_get(espp_system* s, int64_t* step) {
+  CHECK_S(s);
+  *step = s->step;
+  return ESPP_OK;
+}
+
+int espp_step_set(espp_system* s, int64_t step) {
+  CHECK_S(s);
+  s->step = step;
+  return ESPP_OK;
+}
+
+int espp_langevin_set(espp_system* s, int32_t enabled, double gamma, double T, int64_t nexcl,
+                      const int64_t* excl) {
+  CHECK_S(s);
+  s->lang_on = enabled != 0;
+  s->gamma = gamma;
+  s->temperature = T;
+  s->langExcl.clear();
+  for (int64_t i = 0; i < nexcl; ++i) s->langExcl.insert(excl[i]);
+  return ESPP_OK;
+}
+
+int espp_capforce_set(espp_system* s, int32_t mode, const double cap[3]) {
+  CHECK_S(s);
+  s->capMode = mode;
+  for (int k = 0; k < 3; ++k) s->cap[k] = cap ? cap[k] : 0.0;
+  return ESPP_OK;
+}
+
+int espp_run(espp_system* s, int64_t nsteps) {
+  CHECK_S(s);
+  return run(s, nsteps);
+}
+
+int espp_num_resorts(espp_system* s, int64_t* n) {
+  CHECK_S(s);
+  *n = s->nResorts;
+  return ESPP_OK;
+}
+
+int espp_timers(espp_system* s, double t[10]) {
+  CHECK_S(s);
+  for (int i = 0; i < 10; ++i) t[i] = 0.0;
+  return ESPP_OK;
+}
+
+int espp_energy(espp_system* s, int32_t which, double* e) {
+  CHECK_S(s);
+  double es = 0.0;
+  if (which == ESPP_IA_LJ) {
+    for (auto& pr : s->vlPairs) {
+      const LJParams* P = ljFor(s, pr.first->type, pr.second->type);
+      if (!P) continue;
+      double d[3] = {pr.first->r[0] - pr.second->r[0], pr.first->r[1] - pr.second->r[1],
+                     pr.first->r[2] - pr.second->r[2]};
+      es += ljEnergy(*P, d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    }
+  } else if (which == ESPP_IA_FENE) {
+    if (s->fene_on)
+      for (auto& pr : s->bondPtrs) {
+        double d[3];
+        minImageBox(s, pr.first->r, pr.second->r, d);
+        es += feneEnergy(s, d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      }
+  } else {
+    return fail(ESPP_EINVAL, "unknown interaction kind");
+  }
+  *e = es;
+  return ESPP_OK;
+}
+
+static int virialImpl(espp_system* s, int32_t which, double* wsc, double w6[6]) {
+  double w = 0.0;
+  double t[6] = {0, 0, 0, 0, 0, 0};
+  auto acc = [&](const double d[3], const double f[3]) {
+    w = w + (d[0] * f[0] + d[1] * f[1] + d[2] * f[2]);
+    t[0] += d[0] * f[0];
+    t[1] += d[1] * f[1];
+    t[2] += d[2] * f[2];
+    t[3] += d[0] * f[1];
+    t[4] += d[0] * f[2];
+    t[5] += d[1] * f[2];
+  };
+  if (which == ESPP_IA_LJ) {
+    for (auto& pr : s->vlPairs) {
+      const LJParams* P = ljFor(s, pr.first->type, pr.second->type);
+      if (!P) continue;
+      double d[3] = {pr.first->r[0] - pr.second->r[0], pr.first->r[1] - pr.second->r[1],
+                     pr.first->r[2] - pr.second->r[2]};
+      double f[3];
+      if (ljForce(*P, d, f)) acc(d, f);
+    }
+  } else if (which == ESPP_IA_FENE) {
+    if (s->fene_on)
+      for (auto& pr : s->bondPtrs) {
+        double d[3];
+        minImageBox(s, pr.first->r, pr.second->r, d);
+        double f[3];
+        if (feneForce(s, d, f)) acc(d, f);
+      }
+  } else {
+    return fail(ESPP_EINVAL, "unknown interaction kind");
+  }
+  if (wsc) *wsc = w;
+  if (w6)
+    for (int k = 0; k < 6; ++k) w6[k] = t[k];
+  return ESPP_OK;
+}
+
+int espp_virial(espp_system* s, int32_t which, double* w) {
+  CHECK_S(s);
+  return virialImpl(s, which, w, nullptr);
+}
+
+int espp_virial_tensor(espp_system* s, int32_t which, double w[6]) {
+  CHECK_S(s);
+  return virialImpl(s, which, nullptr, w);
+}
+
+int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n) {
+  CHECK_S(s);
+  double v2 = 0.0;
+  int64_t cnt = 0;
+  for (int ci : s->realCells)
+    for (auto& p : s->cells[ci].p) {
+      v2 += p.mass * (p.v[0] * p.v[0] + p.v[1] * p.v[1] + p.v[2] * p.v[2]);
+      cnt++;
+    }
+  *sum_mv2 = v2;
+  *n = cnt;
+  return ESPP_OK;
+}
+
+// Test hook: Philox outputs, so the tests can pin the generator on known answers.
+int espp_oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  U4 c;
+  for (int i = 0; i < 4; ++i) c.v[i] = ctr[i];
+  U4 r = philox4x32_10(c, key[0], key[1]);
+  for (int i = 0; i < 4; ++i) out[i] = r.v[i];
+  return ESPP_OK;
+}
+
+// Test hooks: the potentials on a distance vector (LennardJones.hpp / FENE.hpp KATs).
+int espp_oracle_lj_eval(double eps, double sig, double rc, double shift, double caprad,
+                        const double d[3], double* e, double f[3]) {
+  LJParams P;
+  P.eps = eps;
+  P.sig = sig;
+  P.rc = rc;
+  P.rcsq = rc * rc;
+  P.shift = shift;
+  P.caprad = caprad;
+  double sig2 = sig * sig, sig6 = sig2 * sig2 * sig2;
+  P.ff1 = 48.0 * eps * sig6 * sig6;
+  P.ff2 = 24.0 * eps * sig6;
+  *e = ljEnergy(P, d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  if (!ljForce(P, d, f)) f[0] = f[1] = f[2] = 0.0;
+  return ESPP_OK;
+}
+
+int espp_oracle_fene_eval(double K, double r0, double rmax, double rc, double shift,
+                          const double d[3], double* e, double f[3]) {
+  espp_system s;
+  s.fK = K;
+  s.fr0 = r0;
+  s.frmax = rmax;
+  s.frmaxsq = rmax * rmax;
+  s.frcsq = rc * rc;
+  s.fshift = shift;
+  *e = feneEnergy(&s, d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  if (!feneForce(&s, d, f)) f[0] = f[1] = f[2] = 0.0;
+  return ESPP_OK;
+}
+
+}  // extern "C"

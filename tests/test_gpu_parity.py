@@ -1,0 +1,98 @@
+"""GPU parity against the FP64 oracle (both driven through the same C ABI)."""
+import math
+
+import numpy as np
+import pytest
+
+from espressopp_b200 import _abi
+from simdriver import (Sim, cell_grid, cuda_lib, lattice, load_lj2048, load_polymer40k,
+                       mb_velocities, oracle_lib)
+
+pytestmark = pytest.mark.gpu
+
+
+def _lj_setup(lib, prec, pid, pos, vel, box, rc=2.5, skin=0.3, shift=None, seed=7):
+    s = Sim(lib, box, skin, cell_grid(box, rc, skin), precision=prec, seed=seed)
+    s.add(pid, pos, vel)
+    s.decompose()
+    s.vl(rc)
+    if shift is None:
+        shift = 4.0 * ((1.0 / rc ** 2) ** 6 - (1.0 / rc ** 2) ** 3)
+    s.lj(0, 0, 1.0, 1.0, rc, shift)
+    return s
+
+
+def _rel_rms(a, b):
+    return math.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2))
+
+
+@pytest.mark.parametrize("prec", [_abi.PREC_FP64, _abi.PREC_MIXED])
+def test_lj2048_pairs_bit_exact(prec):
+    pid, pos, vel, box = load_lj2048()
+    o = _lj_setup(oracle_lib(), _abi.PREC_FP64, pid, pos, vel, box)
+    g = _lj_setup(cuda_lib(), prec, pid, pos, vel, box)
+    po, pg = o.pairs(), g.pairs()
+    assert len(po) == len(pg) == o.vl_size() == g.vl_size()
+    assert np.array_equal(po, pg)
+
+
+def test_lj2048_forces_energy_fp64_and_mixed():
+    pid, pos, vel, box = load_lj2048()
+    o = _lj_setup(oracle_lib(), _abi.PREC_FP64, pid, pos, vel, box)
+    g64 = _lj_setup(cuda_lib(), _abi.PREC_FP64, pid, pos, vel, box)
+    gmx = _lj_setup(cuda_lib(), _abi.PREC_MIXED, pid, pos, vel, box)
+    for s in (o, g64, gmx):
+        s.integrator(0.005)
+        s.run(0)
+    fo = o.particles(pid)[2]
+    f64 = g64.particles(pid)[2]
+    fmx = gmx.particles(pid)[2]
+    assert _rel_rms(f64, fo) < 1e-12
+    assert _rel_rms(fmx, fo) < 1e-5
+    eo = o.energy(_abi.IA_LJ)
+    assert abs(g64.energy(_abi.IA_LJ) - eo) < 1e-10 * abs(eo)
+    assert abs(gmx.energy(_abi.IA_LJ) - eo) < 1e-10 * abs(eo)
+    wo = o.virial(_abi.IA_LJ)
+    assert abs(g64.virial(_abi.IA_LJ) - wo) < 1e-10 * abs(wo)
+    assert np.allclose(g64.virial_tensor(_abi.IA_LJ), o.virial_tensor(_abi.IA_LJ), rtol=1e-9,
+                       atol=1e-9)
+
+
+def test_polymer_melt_golden_step0():
+    pos, bonds, box, gold = load_polymer40k()
+    ids = np.arange(1, len(pos) + 1)
+    for prec in (_abi.PREC_FP64, _abi.PREC_MIXED):
+        s = Sim(cuda_lib(), box, 0.3, cell_grid(box, 1.12, 0.3), precision=prec)
+        s.add(ids, pos)
+        s.decompose()
+        s.vl(1.42)
+        s.lj(0, 0, 1.0, 1.0, 1.12, 0.0)
+        s.bonds(bonds)
+        s.fene(30.0, 0.0, 1.5)
+        assert round(s.energy(_abi.IA_LJ), 3) == gold["epair"]
+        assert round(s.energy(_abi.IA_FENE), 3) == gold["ebond"]
+        P = (s.virial(_abi.IA_LJ) + s.virial(_abi.IA_FENE)) / (3.0 * np.prod(box))
+        assert round(P, 5) == gold["P"]
+
+
+@pytest.mark.parametrize("langevin", [False, True])
+def test_lj_short_run_matches_oracle(langevin):
+    pos, box = lattice(12, 0.8442, 0.05, seed=1)
+    vel = mb_velocities(len(pos), 1.0, seed=2)
+    pid = np.arange(len(pos))
+    sims = [_lj_setup(oracle_lib(), _abi.PREC_FP64, pid, pos, vel, box),
+            _lj_setup(cuda_lib(), _abi.PREC_FP64, pid, pos, vel, box),
+            _lj_setup(cuda_lib(), _abi.PREC_MIXED, pid, pos, vel, box)]
+    for s in sims:
+        s.integrator(0.005)
+        if langevin:
+            s.langevin(1.0, 1.0)
+        s.run(20)
+    ref = sims[0].particles(pid)
+    for s, tol in ((sims[1], 1e-9), (sims[2], 1e-5)):
+        got = s.particles(pid)
+        assert np.max(np.abs(got[0] - ref[0])) < tol
+        assert np.array_equal(got[3], ref[3])
+        assert _rel_rms(got[1], ref[1]) < tol
+        assert s.step() == sims[0].step() == 20
+    assert sims[1].num_resorts() == sims[0].num_resorts()

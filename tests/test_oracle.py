@@ -1,0 +1,177 @@
+"""The FP64 oracle pinned to the reference's own golden values (CPU only).
+
+Sources of the expected numbers (all inside espressopp/espressopp):
+* testsuite/interaction_potentials/unittest/TestFENE.cpp:31-68 (FENE energies, force)
+* testsuite/interaction_potentials/unittest/TestLennardJones.cpp:30-50 and
+  testLennardJones.py (LJ minimum, zero crossing, cutoff)
+* testsuite/interaction_potentials/unittest/testFENE.py (FENE at r0)
+* testsuite/tabulated/result.dat:15-17 (step-0 energies and pressure of the 40 000-bead
+  polymer melt), via tests/golden/polymer_melt_40k.*
+* testsuite/unittest/PTestVerletList.cpp (Verlet list size == brute-force count)
+* Random123 known-answer vectors for Philox4x32-10 (kat_vectors).
+"""
+import ctypes
+import itertools
+import math
+
+import numpy as np
+import pytest
+
+from espressopp_b200 import _abi
+from simdriver import (Sim, cell_grid, lattice, load_lj2048, load_polymer40k, mb_velocities,
+                       oracle_lib)
+
+
+def _lj(eps, sig, rc, shift, d, caprad=0.0):
+    lib = oracle_lib()
+    e = ctypes.c_double()
+    f = (ctypes.c_double * 3)()
+    dd = (ctypes.c_double * 3)(*d)
+    lib.espp_oracle_lj_eval(eps, sig, rc, shift, caprad, dd, ctypes.byref(e), f)
+    return e.value, list(f)
+
+
+def _fene(K, r0, rmax, d, rc=math.inf, shift=0.0):
+    lib = oracle_lib()
+    e = ctypes.c_double()
+    f = (ctypes.c_double * 3)()
+    dd = (ctypes.c_double * 3)(*d)
+    lib.espp_oracle_fene_eval(K, r0, rmax, rc, shift, dd, ctypes.byref(e), f)
+    return e.value, list(f)
+
+
+def test_philox_known_answers():
+    lib = oracle_lib()
+    cases = [
+        ([0, 0, 0, 0], [0, 0], [0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8]),
+        ([0xffffffff] * 4, [0xffffffff] * 2, [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd]),
+        ([0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344], [0xa4093822, 0x299f31d0],
+         [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1]),
+    ]
+    for c, k, want in cases:
+        C = (ctypes.c_uint32 * 4)(*c)
+        K = (ctypes.c_uint32 * 2)(*k)
+        O = (ctypes.c_uint32 * 4)()
+        lib.espp_oracle_philox(C, K, O)
+        assert list(O) == want
+
+
+def test_fene_golden():
+    # TestFENE.cpp: BOOST_CHECK_CLOSE(..., 0.01) is a 0.01 % tolerance
+    for r, want in ((0.97, 18.279), (0.80, 11.296), (1.40, 69.147)):
+        e, _ = _fene(30.0, 0.0, 1.5, (r, 0.0, 0.0))
+        assert e == pytest.approx(want, rel=1e-4)
+    _, f = _fene(30.0, 0.0, 1.5, (0.9, 0.1, 0.1))
+    assert f == pytest.approx([-42.782, -4.7535, -4.7535], rel=1e-4)
+    # testFENE.py: K=1, r0=1, rMax=0.5: E(1) = 0, F(1) = 0
+    e, f = _fene(1.0, 1.0, 0.5, (1.0, 0.0, 0.0))
+    assert e == 0.0 and f == [0.0, 0.0, 0.0]
+
+
+def test_lj_golden():
+    e, f = _lj(1.0, 1.0, math.inf, 0.0, (2 ** (1 / 6), 0, 0))
+    assert e == pytest.approx(-1.0, rel=1e-4)
+    assert abs(f[0]) < 1e-12
+    assert abs(_lj(1.0, 1.0, math.inf, 0.0, (2.5, 0, 0))[0]) < 5.0
+    assert abs(_lj(1.0, 1.0, math.inf, 0.0, (10.0, 0, 0))[0]) < 1.0
+    # cutoff 2: small before, zero after (auto shift = E_raw(rc))
+    sh = 4.0 * ((1 / 4.0) ** 6 - (1 / 4.0) ** 3)
+    assert abs(_lj(1.0, 1.0, 2.0, sh, (1.9999, 0, 0))[0]) < 0.01
+    assert abs(_lj(1.0, 1.0, 2.0, sh, (2.0, 0, 0))[0]) < 0.01
+    assert _lj(1.0, 1.0, 2.0, sh, (10.0, 0, 0))[0] == 0.0
+    # testLennardJones.py: eps = sig = 2
+    assert abs(_lj(2.0, 2.0, math.inf, 0.0, (2.0, 0, 0))[0]) < 1e-12
+    assert _lj(2.0, 2.0, math.inf, 0.0, (2 * 2 ** (1 / 6), 0, 0))[0] == pytest.approx(-2.0)
+
+
+def test_polymer_melt_step0_matches_result_dat():
+    pos, bonds, box, gold = load_polymer40k()
+    s = Sim(oracle_lib(), box, 0.3, cell_grid(box, 1.12, 0.3))
+    s.add(np.arange(1, len(pos) + 1), pos)
+    s.decompose()
+    s.vl(1.42)
+    s.lj(0, 0, 1.0, 1.0, 1.12, 0.0)
+    s.bonds(bonds)
+    s.fene(30.0, 0.0, 1.5)
+    assert round(s.energy(_abi.IA_LJ), 3) == gold["epair"]
+    assert round(s.energy(_abi.IA_FENE), 3) == gold["ebond"]
+    P = (s.virial(_abi.IA_LJ) + s.virial(_abi.IA_FENE)) / (3.0 * np.prod(box))
+    assert round(P, 5) == gold["P"]
+
+
+def _brute_pairs(pos, box, cut):
+    n = len(pos)
+    d = pos[:, None, :] - pos[None, :, :]
+    d -= np.round(d / box) * box
+    r2 = np.sum(d * d, -1)
+    iu = np.triu_indices(n, 1)
+    return int(np.sum(r2[iu] <= cut * cut))
+
+
+def test_verlet_list_complete_vs_brute_force():
+    # PTestVerletList.cpp: random particles, list size == N^2 count
+    rng = np.random.Generator(np.random.PCG64(11))
+    box = np.array([10.0, 11.0, 12.0])
+    pos = rng.uniform(0, 1, size=(216, 3)) * box
+    rc, skin = 1.5, 0.001
+    s = Sim(oracle_lib(), box, skin, cell_grid(box, rc, skin))
+    s.add(np.arange(216), pos)
+    s.decompose()
+    s.vl(rc)
+    assert s.vl_size() == _brute_pairs(pos, box, rc + skin)
+    # and on the 2048-particle LJ fixture
+    pid, p2, _, b2 = load_lj2048()
+    s2 = Sim(oracle_lib(), b2, 0.3, cell_grid(b2, 2.5, 0.3))
+    s2.add(pid, p2)
+    s2.decompose()
+    s2.vl(2.5)
+    folded = p2 - np.floor(p2 / b2) * b2
+    assert s2.vl_size() == _brute_pairs(folded, b2, 2.8)
+
+
+def test_nve_energy_conserved():
+    pos, box = lattice(8, 0.8442, 0.05, seed=1)
+    vel = mb_velocities(len(pos), 1.0, seed=2)
+    s = Sim(oracle_lib(), box, 0.3, cell_grid(box, 2.5, 0.3))
+    s.add(np.arange(len(pos)), pos, vel)
+    s.decompose()
+    s.vl(2.5)
+    s.lj(0, 0, 1.0, 1.0, 2.5, 4.0 * (2.5 ** -12 - 2.5 ** -6))
+    s.integrator(0.002)
+    s.run(0)
+    e0 = s.energy(_abi.IA_LJ) + 0.5 * s.kinetic()[0]
+    s.run(200)
+    e1 = s.energy(_abi.IA_LJ) + 0.5 * s.kinetic()[0]
+    assert abs(e1 - e0) / len(pos) < 2e-4
+    assert s.num_resorts() > 0
+
+
+def test_langevin_thermalises_and_excludes():
+    # testLangevinThermostat.py: an excluded particle keeps its velocity, others move
+    pos, box = lattice(6, 0.5, 0.05, seed=3)
+    n = len(pos)
+    s = Sim(oracle_lib(), box, 0.3, cell_grid(box, 2.5, 0.3), seed=99)
+    s.add(np.arange(n), pos, np.zeros((n, 3)))
+    s.decompose()
+    s.integrator(0.005)
+    s.langevin(1.0, 2.0, excl=[0])
+    s.run(400)
+    _, v, _, _ = s.particles(np.arange(n))
+    assert np.all(v[0] == 0.0)
+    T = np.sum(v[1:] ** 2) / (3 * (n - 1))
+    assert 1.4 < T < 2.6
+
+
+def test_capforce_limits_total_force():
+    pos, box = lattice(6, 1.2, 0.2, seed=5)
+    n = len(pos)
+    s = Sim(oracle_lib(), box, 0.3, cell_grid(box, 1.12246, 0.3))
+    s.add(np.arange(n), pos)
+    s.decompose()
+    s.vl(1.12246)
+    s.lj(0, 0, 1.0, 1.0, 1.12246, 1.0)
+    s.capforce(_abi.CAP_ABS, 5.0)
+    s.integrator(0.001)
+    s.run(0)
+    f = s.particles(np.arange(n))[2]
+    assert np.max(np.linalg.norm(f, axis=1)) <= 5.0 + 1e-12
