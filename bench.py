@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""Benchmark of the short-range MD step: LJ particle-steps/s on one B200.
+
+Workload (the large LJ fluid): N = 160^3 = 4,096,000 particles on a simple-cubic
+lattice at reduced density 0.8442 with uniform jitter +-0.05 sigma (seed 1),
+Maxwell-Boltzmann velocities at T = 1 (seed 2, zero net momentum), LJ eps = sigma = 1,
+rc = 2.5 (auto shift), Verlet skin 0.3, cell grid 60^3, velocity Verlet dt = 0.005, NVE,
+mixed precision (FP32 pair forces on box-wrapped int32 coordinates, int64 2^-32
+fixed-point force sums, FP64 positions / velocities / energies).  Particle data
+(262 MB of positions, velocities and packed coordinates) exceeds the 126 MB L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one velocity-Verlet step (force, aftCalcF, integrate2 + integrate1, and the
+re-sort + Verlet rebuild whenever the accumulated displacement exceeds skin/2).  W
+untimed steps run first; the K timed steps are one espp_run call whose step loop is
+timed by CUDA events on the library's stream (max over ranks).  Under torchrun each
+rank steps its own independent copy of the system on its GPU (replicas, weak scaling).
+
+``--impl reference`` times the CPU restatement of the reference algorithm (the FP64
+oracle; the reference itself cannot be built on this image: it needs Boost, MPI, FFTW
+and HDF5) on all host cores, one independent 32,768-particle sample system per core at
+the same density, cutoff and skin.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+RHO = 0.8442
+RC = 2.5
+SKIN = 0.3
+DT = 0.005
+# neighbours within rc + skin, counted once per pair (half list): (2/3) pi (rc+skin)^3 rho
+N_HALF = 2.0 / 3.0 * math.pi * (RC + SKIN) ** 3 * RHO
+# algorithmic bytes per particle and step, whole step (mixed precision):
+# x r/w 48 + v r/w 48 + int64 F w/r 48 + FP32 packed x w/r 24 + 4 B per half-list pair
+STEP_BYTES = 168.0 + 4.0 * N_HALF
+# force kernel: packed coordinates read 12 + 4 B per half-list pair + int64 F write 24
+FORCE_BYTES = 12.0 + 4.0 * N_HALF + 24.0
+# DRAM bytes per particle of one force-kernel launch measured by ncu
+# (profiles/force_mixed_lj_ncu.txt), scaled from the 32^3 case; None until captured
+FORCE_TRAFFIC_PER_PARTICLE = None
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def lattice(n_side, rho, jitter, seed):
+    N = n_side ** 3
+    L = (N / rho) ** (1.0 / 3.0)
+    a = L / n_side
+    g = (np.arange(n_side) + 0.5) * a
+    pos = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pos += rng.uniform(-jitter, jitter, size=pos.shape)
+    return pos, L
+
+
+def mb_velocities(N, T, seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    v = rng.normal(0.0, math.sqrt(T), size=(N, 3))
+    v *= math.sqrt(T / (np.sum(v * v) / (3 * N)))
+    v -= v.mean(axis=0)
+    return v
+
+
+def make_system(lib, n_side, precision, seed=12345):
+    from espressopp_b200._abi import call, dptr, i32ptr, i64ptr
+    pos, L = lattice(n_side, RHO, 0.05, 1)
+    vel = mb_velocities(len(pos), 1.0, 2)
+    ids = np.arange(len(pos), dtype=np.int64)
+    box = np.array([L, L, L])
+    ncell = int(L / (RC + SKIN))
+    cg = np.array([ncell] * 3, np.int32)
+    h = ctypes.c_void_p()
+    call(lib, "espp_system_create", dptr(box), SKIN, i32ptr(cg), precision, seed, ctypes.byref(h))
+    call(lib, "espp_add_particles", h, len(ids), i64ptr(ids), None, None,
+         dptr(np.ascontiguousarray(pos.reshape(-1))), dptr(np.ascontiguousarray(vel.reshape(-1))))
+    call(lib, "espp_decompose", h)
+    call(lib, "espp_vl_create", h, RC, 0, None)
+    shift = 4.0 * (RC ** -12 - RC ** -6)
+    call(lib, "espp_lj_set", h, 0, 0, 1.0, 1.0, RC, shift, 0.0)
+    call(lib, "espp_integrator_set", h, DT)
+    return h, ids, pos, vel, box, cg
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0}, "fallback"
+
+
+# ---- CPU baseline (the oracle: a restatement of the reference algorithm) ------------
+def _oracle_sample(args):
+    """Steps one 32^3 sample system with the FP64 CPU oracle; returns
+    (particle_steps, seconds).  Runs in its own process."""
+    n_side, steps, budget_s = args
+    sys.path.insert(0, REPO)
+    from espressopp_b200 import _abi
+    lib_path = os.path.join(REPO, "oracle", "_build", "liboracle_espp.so")
+    if not os.path.exists(lib_path):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(REPO, "oracle")])
+    lib = _abi.bind(ctypes.CDLL(lib_path))
+    h, ids, pos, vel, box, cg = make_system(lib, n_side, _abi.PREC_FP64)
+    _abi.call(lib, "espp_run", h, 1)  # decompose + list build outside the timing
+    done = 0
+    t0 = time.perf_counter()
+    while True:
+        _abi.call(lib, "espp_run", h, steps)
+        done += steps
+        el = time.perf_counter() - t0
+        if el >= budget_s:
+            break
+    lib.espp_system_destroy(h)
+    return done * n_side ** 3, el
+
+
+def cpu_baseline(cores, budget_s=12.0, n_side=32, steps=4):
+    import multiprocessing as mp
+    if cores == 1:
+        ps, el = _oracle_sample((n_side, steps, budget_s))
+        return ps / el, 1
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        t0 = time.perf_counter()
+        res = pool.map(_oracle_sample, [(n_side, steps, budget_s)] * cores)
+        wall = time.perf_counter() - t0
+    # aggregate rate over the longest worker's timed span
+    return sum(r[0] for r in res) / max(r[1] for r in res), cores
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    rates = []
+    for _ in range(max(1, args.steps_ref)):
+        r, c = cpu_baseline(cores, budget_s=args.ref_budget)
+        rates.append(r)
+    value = float(np.median(rates))
+    line = {
+        "impl": "reference", "metric": "LJ particle-steps/s", "value": value,
+        "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "LJ fluid 160^3 (rho 0.8442, rc 2.5, skin 0.3, dt 0.005, NVE)",
+                   "sample": "32^3 = 32768-particle systems at the same density, cutoff and skin, "
+                             "one per host core"},
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores,
+                         "kind": "port",
+                         "sample": "%d cores x independent 32768-particle systems, %.0f s each"
+                                   % (cores, args.ref_budget)},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- GPU arm ---------------------------------------------------------------------
+def gpu_arm(args, rank, world, local_rank):
+    import espressopp_b200
+    from espressopp_b200 import _abi
+    from espressopp_b200._abi import call, dptr, i64ptr
+
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist_mod
+        torch.cuda.set_device(local_rank)
+        dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        dist = dist_mod
+
+    lib = espressopp_b200.load_library()
+    call(lib, "espp_select_device", local_rank)
+    prec = _abi.PREC_MIXED if args.precision == "mixed" else _abi.PREC_FP64
+    t_setup = time.perf_counter()
+    h, ids, pos, vel, box, cg = make_system(lib, args.n_side, prec)
+    N = len(ids)
+    log("rank %d: setup %.1f s, N=%d, cells %s" % (rank, time.perf_counter() - t_setup, N,
+                                                   tuple(cg)))
+
+    def barrier():
+        if dist is not None:
+            import torch
+            t = torch.zeros(1, device="cuda")
+            dist.all_reduce(t)
+            torch.cuda.synchronize()
+
+    # warm-up (untimed)
+    call(lib, "espp_run", h, args.warmup)
+
+    # timed region: one run of K steps on the captured step-loop graph; CUDA events on
+    # the library's stream around the step loop
+    call(lib, "espp_set_profiling", h, 0)
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    time.sleep(0.3)
+    barrier()
+    call(lib, "espp_run", h, args.steps)
+    barrier()
+    clocks = sampler.stop()
+    ms = np.zeros(2)
+    call(lib, "espp_last_run_ms", h, dptr(ms))
+    ph_g = np.zeros(4)
+    launches = np.zeros(4, np.int64)
+    call(lib, "espp_profile", h, dptr(ph_g), i64ptr(launches))
+    resorts = ctypes.c_int64()
+    call(lib, "espp_num_resorts", h, ctypes.byref(resorts))
+    loop_ms = float(ms[1])
+    if dist is not None:
+        import torch
+        t = torch.tensor([loop_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        loop_ms = float(t.item())
+
+    # per-kernel device times: the same workload stepped K more steps with every launch
+    # bracketed by CUDA events on the library's stream (host-driven loop)
+    call(lib, "espp_set_profiling", h, 1)
+    call(lib, "espp_run", h, args.steps)
+    ph = np.zeros(4)
+    launches_p = np.zeros(4, np.int64)
+    call(lib, "espp_profile", h, dptr(ph), i64ptr(launches_p))
+    call(lib, "espp_set_profiling", h, 0)
+
+    # end to end through the C ABI with pinned host buffers: state in, K steps, state out
+    import torch
+    pin_pos = torch.empty((N, 3), dtype=torch.float64, pin_memory=True).numpy()
+    pin_vel = torch.empty((N, 3), dtype=torch.float64, pin_memory=True).numpy()
+    pin_ids = torch.empty((N,), dtype=torch.int64, pin_memory=True).numpy()
+    pin_ids[:] = ids
+    call(lib, "espp_get_particles", h, N, i64ptr(pin_ids), dptr(pin_pos), dptr(pin_vel), None,
+         None)
+    barrier()
+    t0 = time.perf_counter()
+    call(lib, "espp_set_particles", h, N, i64ptr(pin_ids), dptr(pin_pos), dptr(pin_vel))
+    call(lib, "espp_run", h, args.steps)
+    call(lib, "espp_get_particles", h, N, i64ptr(pin_ids), dptr(pin_pos), dptr(pin_vel), None,
+         None)
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    lib.espp_system_destroy(h)
+    if rank != 0:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    peaks, peak_kind = measured_peaks()
+    hbm = float(peaks["hbm_gbs"])
+    force_avg_ms = ph[0] / max(1, launches_p[0])
+    achieved = FORCE_BYTES * N / (force_avg_ms * 1e-3) / 1e9
+    step_s = loop_ms * 1e-3 / args.steps
+    value = world * N * args.steps / (loop_ms * 1e-3)
+    cpu_rate, cpu_cores = cpu_baseline(1, budget_s=args.cpu_budget) if world == 1 else (None, 1)
+    traffic = (FORCE_TRAFFIC_PER_PARTICLE * N) if FORCE_TRAFFIC_PER_PARTICLE else None
+    line = {
+        "metric": "LJ particle-steps/s", "value": value, "unit": "particle-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": loop_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+i64 fixed (forces), f64 (integrator)",
+        "data": "synthetic",
+        "config": {"workload": "LJ fluid, %d^3 = %d particles, rho %.4f, rc %.1f, skin %.1f, "
+                               "dt %.3f, NVE, %s" % (args.n_side, N, RHO, RC, SKIN, DT,
+                                                     args.precision),
+                   "cell_grid": list(map(int, cg)), "l2": "inputs larger than L2 (262 MB)",
+                   "parallelism": "replicas x%d" % world if world > 1 else "1 GPU",
+                   "resorts_in_timed_steps": int(resorts.value)},
+        "roofline": {"kernel": "k_force_mixed" if prec else "k_force_fp64", "bound": "hbm",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_kind": peak_kind,
+                     "alg_bytes_per_particle": FORCE_BYTES, "traffic": traffic,
+                     "avg_launch_ms": force_avg_ms},
+        "step_roofline": {"alg_bytes_per_particle_step": STEP_BYTES,
+                          "achieved_gbs": STEP_BYTES * N / step_s / 1e9,
+                          "frac": STEP_BYTES * N / step_s / 1e9 / hbm},
+        "profiled_pass_ms": {"force": ph[0], "integrate": ph[1], "rebuild": ph[2],
+                             "decide": ph[3], "launches": [int(x) for x in launches_p]},
+        "gpu_launches": int(launches.sum()),
+        "clocks": clocks,
+        "e2e": {"value": world * N * args.steps / e2e_s, "unit": "particle-steps/s",
+                "h2d_bytes_per_step": int(N * (48 + 8) / args.steps),
+                "d2h_bytes_per_step": int(N * 48 / args.steps),
+                "note": "pinned host state in (ids, x, v), K steps, state out (x, v) per call"},
+    }
+    if cpu_rate is not None:
+        line["cpu_baseline"] = {"value": cpu_rate, "unit": "particle-steps/s", "cores": cpu_cores,
+                                "kind": "port",
+                                "sample": "one 32768-particle system (same density, rc, skin), "
+                                          "%.0f s of stepping on 1 core" % args.cpu_budget}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--n-side", type=int, default=160)
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--ref-budget", type=float, default=20.0)
+    ap.add_argument("--steps-ref", type=int, default=1)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("at least 3 warm-up steps")
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+    else:
+        gpu_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

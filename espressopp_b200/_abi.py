@@ -47,6 +47,10 @@ PROTOTYPES = {
     "espp_virial": (c_int32, [_P, c_int32, _D]),
     "espp_virial_tensor": (c_int32, [_P, c_int32, _D]),
     "espp_kinetic": (c_int32, [_P, _D, _I64]),
+    "espp_set_profiling": (c_int32, [_P, c_int32]),
+    "espp_profile": (c_int32, [_P, _D, _I64]),
+    "espp_last_run_ms": (c_int32, [_P, _D]),
+    "espp_select_device": (c_int32, [c_int32]),
 }
 
 # status codes (include/espp_b200.h)

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -88,6 +89,25 @@ struct espp_system {
   double* ftot = nullptr;
   RebuildScratch scr{};
   bool binned = false;
+  bool listValid = false;
+
+  // staging for by-id state transfers
+  int stageCap = 0;
+  int64_t* stIds = nullptr;
+  double* stPos = nullptr;
+  double* stVel = nullptr;
+  double* stF = nullptr;
+  int32_t* stImg = nullptr;
+
+  // device-event timing of the run loop
+  bool profiling = false;
+  std::vector<cudaEvent_t> evPool;
+  size_t evUsed = 0;
+  std::vector<std::pair<int, size_t>> evPhase;  // (phase, index of start event)
+  double phaseMs[4] = {0, 0, 0, 0};             // force, integrate, rebuild, other
+  long long phaseLaunches[4] = {0, 0, 0, 0};
+  cudaEvent_t runBeg = nullptr, runLoop = nullptr, runEnd = nullptr;
+  double lastRunMs = 0.0, lastLoopMs = 0.0;
 
   // id-indexed structures
   int64_t idMin = 0;
@@ -102,13 +122,22 @@ struct espp_system {
 
   // device scalars
   unsigned* err = nullptr;
-  unsigned long long* maxSq = nullptr;
-  double* maxDist = nullptr;
-  int* flag = nullptr;
+  DevCounters* ctr = nullptr;     // device
+  DevCounters* hctr = nullptr;    // pinned host mirror
+  ParticleArrays* d_pa = nullptr; // device: [0] current, [1] re-sort target
+  bool paHostValid = true;        // host A/B mirror what d_pa holds
   double* obs = nullptr;
   double* partials = nullptr;
   int partialsCap = 0;
-  int* hflag = nullptr;  // pinned
+
+  // captured step loop (WHILE { decide; IF(re-sort) {...}; force; integrate })
+  bool useGraph = true;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graphExec = nullptr;
+  std::string graphKey;
+  // pre-run snapshot to recover from a Verlet-list overflow inside the graph
+  ParticleArrays snap{};
+  int snapCap = 0;
 
   // Verlet list
   bool has_vl = false;
@@ -143,7 +172,7 @@ struct espp_system {
 
   DevView view() const {
     DevView d{};
-    d.a = A;
+    d.pa = d_pa;
     d.n = n;
     d.cap = cap;
     for (int k = 0; k < 3; ++k) {
@@ -183,7 +212,7 @@ struct espp_system {
       if (lj.p[k].set && lj.p[k].caprad > 0) capped = 1;
     d.ljCapped = capped;
     d.err = err;
-    d.maxSq = maxSq;
+    d.ctr = ctr;
     return d;
   }
 };
@@ -210,6 +239,24 @@ void alloc_particles(ParticleArrays& a, int cap) {
 
 void sync(espp_system* s) { cuda_check(cudaStreamSynchronize(s->st), "stream synchronize"); }
 
+// Host view of which physical buffers are current (the re-sort swaps them on the device).
+void sync_pa(espp_system* s) {
+  if (s->paHostValid) return;
+  ParticleArrays h[2];
+  cuda_check(cudaMemcpyAsync(h, s->d_pa, sizeof(h), cudaMemcpyDeviceToHost, s->st), "arrays");
+  sync(s);
+  s->A = h[0];
+  s->B = h[1];
+  s->paHostValid = true;
+}
+
+void push_pa(espp_system* s) {
+  ParticleArrays h[2] = {s->A, s->B};
+  cuda_check(cudaMemcpyAsync(s->d_pa, h, sizeof(h), cudaMemcpyHostToDevice, s->st), "arrays");
+  sync(s);
+  s->paHostValid = true;
+}
+
 // Host copy of every particle in storage order.
 struct HostParticles {
   std::vector<int64_t> id;
@@ -229,7 +276,7 @@ void copy_soa_down(espp_system* s, std::vector<T>& out, const T* dsrc, int comps
 }
 
 HostParticles download(espp_system* s, bool withForce) {
-  sync(s);
+  sync_pa(s);
   HostParticles h;
   copy_soa_down(s, h.id, s->A.id, 1);
   copy_soa_down(s, h.type, s->A.type, 1);
@@ -269,6 +316,7 @@ void free_buffers(espp_system* s) {
 // Reallocates the per-particle buffers for cap >= n and uploads h.
 void upload(espp_system* s, const HostParticles& h) {
   int n = (int)h.id.size();
+  sync_pa(s);
   if (n > s->cap) {
     free_buffers(s);
     int cap = std::max(n, 32);
@@ -292,6 +340,7 @@ void upload(espp_system* s, const HostParticles& h) {
     dfree(s->nl);
   }
   s->n = n;
+  push_pa(s);
   copy_soa_up(s, s->A.id, h.id, 1);
   copy_soa_up(s, s->A.type, h.type, 1);
   copy_soa_up(s, s->A.mass, h.mass, 1);
@@ -403,13 +452,12 @@ void bin(espp_system* s, bool fold) {
   }
   launch_fold_bin(d, s->scr, fold, s->st);
   launch_sort_cells(d, s->scr, s->st);
-  d = s->view();  // fold updated A in place
-  launch_gather(d, s->A, s->B, s->scr, s->st);
-  std::swap(s->A, s->B);
-  d = s->view();
+  launch_gather(d, s->scr, s->st);  // gathers into pa[1] and swaps on the device
+  s->paHostValid = false;
   launch_id_map(d, s->st);
   cuda_check(cudaGetLastError(), "re-binning kernels");
   s->binned = true;
+  s->listValid = false;
 }
 
 int estimate_K(espp_system* s) {
@@ -444,6 +492,7 @@ void build_list(espp_system* s) {
   }
   check_err(s);
   s->builds++;
+  s->listValid = true;
 }
 
 void decompose(espp_system* s) {
@@ -476,6 +525,7 @@ void upload_lj(espp_system* s) {
 }
 
 void forces(espp_system* s) {
+  if (s->has_vl && s->lj_any && !s->listValid) build_list(s);
   DevView d = s->view();
   if (!s->has_vl || !s->lj_any) d.nn = s->nnZero;  // no pair term: bonds only
   launch_forces(d, s->precision == ESPP_PREC_MIXED, s->fene, s->tpp, s->st);
@@ -500,27 +550,242 @@ double now_s() {
       .count();
 }
 
+// ---- device-event phase timing ---------------------------------------------------
+enum { kPhForce = 0, kPhIntegrate = 1, kPhRebuild = 2, kPhOther = 3 };
+
+cudaEvent_t next_event(espp_system* s) {
+  if (s->evUsed == s->evPool.size()) {
+    cudaEvent_t e;
+    cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+    s->evPool.push_back(e);
+  }
+  return s->evPool[s->evUsed++];
+}
+
+struct PhaseScope {
+  espp_system* s;
+  int ph;
+  size_t idx;
+  PhaseScope(espp_system* s_, int ph_, int launches) : s(s_), ph(ph_) {
+    s->phaseLaunches[ph] += launches;
+    if (!s->profiling) return;
+    idx = s->evUsed;
+    cuda_check(cudaEventRecord(next_event(s), s->st), "event");
+  }
+  ~PhaseScope() {
+    if (!s->profiling) return;
+    if (cudaEventRecord(next_event(s), s->st) == cudaSuccess) s->evPhase.push_back({ph, idx});
+  }
+};
+
+void collect_phases(espp_system* s) {
+  if (!s->profiling) return;
+  sync(s);
+  for (auto& pe : s->evPhase) {
+    float ms = 0.f;
+    cuda_check(cudaEventElapsedTime(&ms, s->evPool[pe.second], s->evPool[pe.second + 1]),
+               "event time");
+    s->phaseMs[pe.first] += ms;
+  }
+  s->evPhase.clear();
+  s->evUsed = 0;
+}
+
+// rebuild = fold/bin (fold_bin, scan, scatter, sort, gather, id map) + Verlet list
+void timed_decompose(espp_system* s) {
+  PhaseScope ps(s, kPhRebuild, 8 + (s->has_vl ? 1 : 0));
+  decompose(s);
+}
+
+void timed_forces(espp_system* s) {
+  PhaseScope ps(s, kPhForce, 1);
+  forces(s);
+}
+
+void timed_integrate(espp_system* s, const IntegrateArgs& a) {
+  PhaseScope ps(s, kPhIntegrate, 1);
+  launch_integrate(s->view(), a, s->st);
+}
+
+void set_counters(espp_system* s, const DevCounters& c) {
+  *s->hctr = c;
+  cuda_check(cudaMemcpyAsync(s->ctr, s->hctr, sizeof(DevCounters), cudaMemcpyHostToDevice, s->st),
+             "counters");
+}
+
+DevCounters get_counters(espp_system* s) {
+  cuda_check(cudaMemcpyAsync(s->hctr, s->ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s->st),
+             "counters");
+  sync(s);
+  return *s->hctr;
+}
+
+void destroy_graph(espp_system* s) {
+  if (s->graphExec) cudaGraphExecDestroy(s->graphExec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  s->graphExec = nullptr;
+  s->graph = nullptr;
+  s->graphKey.clear();
+}
+
+// Everything a captured launch bakes in: kernel arguments and launch shapes.
+std::string graph_key(espp_system* s, const IntegrateArgs& a) {
+  DevView d = s->view();
+  std::string k((const char*)&d, sizeof(d));
+  k.append((const char*)&a, sizeof(a));
+  k.append((const char*)&s->fene, sizeof(s->fene));
+  int extra[4] = {s->tpp, s->has_vl ? 1 : 0, s->lj_any ? 1 : 0, s->precision};
+  k.append((const char*)extra, sizeof(extra));
+  double sk = s->skin + s->vl_cut;
+  k.append((const char*)&sk, sizeof(sk));
+  return k;
+}
+
+// Re-sort + Verlet build launched on st (also used to populate the IF body).
+void launch_rebuild_kernels(espp_system* s, cudaStream_t st) {
+  DevView d = s->view();
+  launch_fold_bin(d, s->scr, true, st);
+  launch_sort_cells(d, s->scr, st);
+  launch_gather(d, s->scr, st);
+  launch_id_map(d, st);
+  if (s->has_vl) {
+    const double cv = s->vl_cut + s->skin;
+    launch_build_nl(d, cv * cv, st);
+  }
+}
+
+void launch_force_kernel(espp_system* s, cudaStream_t st) {
+  DevView d = s->view();
+  if (!s->has_vl || !s->lj_any) d.nn = s->nnZero;
+  launch_forces(d, s->precision == ESPP_PREC_MIXED, s->fene, s->tpp, st);
+}
+
+// WHILE(remaining) { decide; IF(re-sort) { fold, bin, sort, gather, swap, id map, list };
+//                    force; integrate2 + integrate1 }
+void capture_graph(espp_system* s, const IntegrateArgs& ai) {
+  destroy_graph(s);
+  cudaGraph_t g;
+  cuda_check(cudaGraphCreate(&g, 0), "cudaGraphCreate");
+  cudaGraphConditionalHandle hWhile, hIf;
+  cuda_check(cudaGraphConditionalHandleCreate(&hWhile, g, 1, cudaGraphCondAssignDefault),
+             "conditional handle");
+  cudaGraphNodeParams wp = {};
+  wp.type = cudaGraphNodeTypeConditional;
+  wp.conditional.handle = hWhile;
+  wp.conditional.type = cudaGraphCondTypeWhile;
+  wp.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  cuda_check(cudaGraphAddNode(&wnode, g, nullptr, 0, &wp), "while node");
+  cudaGraph_t body = wp.conditional.phGraph_out[0];
+  cuda_check(cudaGraphConditionalHandleCreate(&hIf, body, 0, cudaGraphCondAssignDefault),
+             "conditional handle");
+  cudaStream_t cs;
+  cuda_check(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
+  const double skinHalf = 0.5 * s->skin;
+  // body: decide
+  cuda_check(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal), "capture");
+  launch_decide_graph(s->view(), skinHalf, hIf, hWhile, cs);
+  cudaStreamCaptureStatus st;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  cuda_check(cudaStreamGetCaptureInfo(cs, &st, nullptr, nullptr, &deps, &ndeps), "capture info");
+  cudaGraphNodeParams ip = {};
+  ip.type = cudaGraphNodeTypeConditional;
+  ip.conditional.handle = hIf;
+  ip.conditional.type = cudaGraphCondTypeIf;
+  ip.conditional.size = 1;
+  cudaGraphNode_t inode;
+  cuda_check(cudaGraphAddNode(&inode, body, deps, ndeps, &ip), "if node");
+  cuda_check(cudaStreamUpdateCaptureDependencies(cs, &inode, 1, cudaStreamSetCaptureDependencies),
+             "capture dependencies");
+  launch_force_kernel(s, cs);
+  launch_integrate(s->view(), ai, cs);
+  cudaGraph_t done;
+  cuda_check(cudaStreamEndCapture(cs, &done), "end capture");
+  // IF body: re-sort and list build
+  cudaGraph_t rb = ip.conditional.phGraph_out[0];
+  cuda_check(cudaStreamBeginCaptureToGraph(cs, rb, nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal), "capture");
+  launch_rebuild_kernels(s, cs);
+  cuda_check(cudaStreamEndCapture(cs, &done), "end capture");
+  cudaStreamDestroy(cs);
+  cudaGraphExec_t ex;
+  cuda_check(cudaGraphInstantiate(&ex, g, 0), "cudaGraphInstantiate");
+  s->graph = g;
+  s->graphExec = ex;
+}
+
+void ensure_snapshot(espp_system* s) {
+  if (s->snapCap >= s->cap) return;
+  free_particles(s->snap);
+  alloc_particles(s->snap, s->cap);
+  s->snapCap = s->cap;
+}
+
+void copy_arrays(espp_system* s, const ParticleArrays& dst, const ParticleArrays& src) {
+  const size_t c = s->cap;
+  cuda_check(cudaMemcpyAsync(dst.x, src.x, 3 * c * sizeof(double), cudaMemcpyDeviceToDevice, s->st),
+             "copy");
+  cuda_check(cudaMemcpyAsync(dst.v, src.v, 3 * c * sizeof(double), cudaMemcpyDeviceToDevice, s->st),
+             "copy");
+  cuda_check(cudaMemcpyAsync(dst.id, src.id, c * sizeof(int64_t), cudaMemcpyDeviceToDevice, s->st),
+             "copy");
+  cuda_check(cudaMemcpyAsync(dst.type, src.type, c * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                             s->st), "copy");
+  cuda_check(cudaMemcpyAsync(dst.mass, src.mass, c * sizeof(double), cudaMemcpyDeviceToDevice,
+                             s->st), "copy");
+  cuda_check(cudaMemcpyAsync(dst.img, src.img, 3 * c * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                             s->st), "copy");
+}
+
+int K_high_water(espp_system* s) { return get_counters(s).nnMax; }
+
+// Grows the Verlet capacity ahead of need when the builds came within 10 % of it.
+void maybe_grow_K(espp_system* s) {
+  if (!s->has_vl || s->K == 0) return;
+  int hw = K_high_water(s);
+  if (hw * 10 > s->K * 9) {
+    s->K = (hw * 3 / 2 + 15) / 8 * 8;
+    dfree(s->nl);
+    s->nl = dalloc<int32_t>((size_t)s->K * s->cap);
+    s->listValid = false;
+  }
+}
+
 // VelocityVerlet::run (src/integrator/VelocityVerlet.cpp:63-169).
 void run(espp_system* s, int64_t nsteps) {
   const double t0 = now_s();
   double tResort = 0.0;
   s->nResorts = 0;
   const double skinHalf = 0.5 * s->skin;
+  if (!s->runBeg) {
+    cuda_check(cudaEventCreate(&s->runBeg), "event");
+    cuda_check(cudaEventCreate(&s->runLoop), "event");
+    cuda_check(cudaEventCreate(&s->runEnd), "event");
+  }
+  cuda_check(cudaEventRecord(s->runBeg, s->st), "event");
   if (s->idDirty) rebuild_id_tables(s);
   if (s->resortFlag) {
     double tr = now_s();
-    decompose(s);
-    cuda_check(cudaMemsetAsync(s->maxDist, 0, sizeof(double), s->st), "memset");
+    timed_decompose(s);
+    DevCounters c = get_counters(s);
+    c.maxDist = 0.0;
+    set_counters(s, c);
     s->resortFlag = false;
     tResort += now_s() - tr;
-  } else if (s->has_vl && !s->binned) {
-    build_list(s);
   }
   if (!s->binned) bin(s, false);
-  cuda_check(cudaMemsetAsync(s->maxSq, 0, sizeof(unsigned long long), s->st), "memset");
+  if (s->has_vl && !s->listValid) build_list(s);
+  DevCounters c0 = get_counters(s);
+  c0.maxSq = 0ull;
+  c0.resorts = 0;
+  c0.step = s->step - 1;
+  c0.remaining = nsteps;
+  set_counters(s, c0);
   // start-of-run force (recalc1 = heatUp: pref2 * sqrt(3); recalc2 restores it)
   IntegrateArgs a = integrate_args(s);
-  forces(s);
+  timed_forces(s);
   IntegrateArgs a0 = a;
   a0.pref2 = a.pref2 * std::sqrt(3.0);
   a0.phase = 1;
@@ -528,37 +793,112 @@ void run(espp_system* s, int64_t nsteps) {
   a0.do_i2 = 0;
   a0.do_i1 = nsteps > 0 ? 1 : 0;
   a0.storeFtot = nsteps > 0 ? 0 : 1;
-  launch_integrate(s->view(), a0, s->st);
+  timed_integrate(s, a0);
   cuda_check(cudaGetLastError(), "start-of-run kernels");
-  for (int64_t i = 0; i < nsteps; ++i) {
-    DevView d = s->view();
-    launch_decide(d, s->maxDist, s->flag, skinHalf, s->st);
-    cuda_check(cudaMemcpyAsync(s->hflag, s->flag, sizeof(int), cudaMemcpyDeviceToHost, s->st),
-               "flag");
-    sync(s);
-    if (*s->hflag) {
-      double tr = now_s();
-      decompose(s);
-      s->nResorts++;
-      tResort += now_s() - tr;
+  cuda_check(cudaEventRecord(s->runLoop, s->st), "event");
+  IntegrateArgs ai = a;
+  ai.phase = 0;
+  ai.do_i2 = 1;
+  ai.do_i1 = 1;
+  ai.storeFtot = 0;
+  bool graphDone = false;
+  if (nsteps > 0 && s->useGraph && !s->profiling) {
+    IntegrateArgs ag = ai;
+    ag.fromCounters = 1;
+    ag.step = 0;  // read from the device counters
+    std::string key = graph_key(s, ag);
+    if (!s->graphExec || key != s->graphKey) {
+      capture_graph(s, ag);
+      s->graphKey = key;
     }
-    forces(s);
-    IntegrateArgs ai = a;
-    ai.phase = 0;
-    ai.step = s->step;
-    ai.do_i2 = 1;
-    ai.do_i1 = (i + 1 < nsteps) ? 1 : 0;
-    ai.storeFtot = (i + 1 < nsteps) ? 0 : 1;
-    launch_integrate(s->view(), ai, s->st);
-    cuda_check(cudaGetLastError(), "step kernels");
-    s->step++;
+    sync_pa(s);
+    ensure_snapshot(s);
+    copy_arrays(s, s->snap, s->A);
+    const DevCounters before = c0;
+    const int64_t step0 = s->step;
+    cuda_check(cudaGraphLaunch(s->graphExec, s->st), "cudaGraphLaunch");
+    cuda_check(cudaEventRecord(s->runEnd, s->st), "event");
+    sync(s);
+    unsigned e = read_err(s);
+    if (e & kErrNlOverflow) {
+      // restore the pre-run state, grow the list and redo the run on the host loop
+      cuda_check(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->st), "memset");
+      s->paHostValid = false;
+      sync_pa(s);
+      copy_arrays(s, s->A, s->snap);
+      set_counters(s, before);
+      s->step = step0;
+      s->binned = false;
+      s->K = std::max(s->K * 2, K_high_water(s) + 32);
+      dfree(s->nl);
+      s->nl = dalloc<int32_t>((size_t)s->K * s->cap);
+      s->listValid = false;
+      destroy_graph(s);
+      const bool g = s->useGraph;
+      s->useGraph = false;
+      try {
+        run(s, nsteps);
+      } catch (...) {
+        s->useGraph = g;
+        throw;
+      }
+      s->useGraph = g;
+      return;
+    }
+    DevCounters c = get_counters(s);
+    s->step += nsteps;
+    s->nResorts = c.resorts;
+    s->builds += c.resorts;
+    // kernels launched by the graph: decide + force + integrate per step, and zero,
+    // fold/bin, scan, scatter, in-cell sort, gather, swap, id map (+ list) per re-sort
+    s->phaseLaunches[kPhOther] += nsteps;
+    s->phaseLaunches[kPhForce] += nsteps;
+    s->phaseLaunches[kPhIntegrate] += nsteps;
+    s->phaseLaunches[kPhRebuild] += c.resorts * (8 + (s->has_vl ? 1 : 0));
+    s->paHostValid = false;
+    graphDone = true;
+  }
+  if (!graphDone) {
+    for (int64_t i = 0; i < nsteps; ++i) {
+      {
+        PhaseScope ps(s, kPhOther, 1);
+        launch_decide(s->view(), skinHalf, s->st);
+      }
+      cuda_check(cudaMemcpyAsync(s->hctr, s->ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost,
+                                 s->st), "flag");
+      sync(s);
+      if (s->hctr->flag) {
+        double tr = now_s();
+        timed_decompose(s);
+        s->nResorts++;
+        tResort += now_s() - tr;
+      }
+      timed_forces(s);
+      IntegrateArgs aj = ai;
+      aj.step = s->step;
+      aj.do_i1 = (i + 1 < nsteps) ? 1 : 0;
+      aj.storeFtot = (i + 1 < nsteps) ? 0 : 1;
+      timed_integrate(s, aj);
+      cuda_check(cudaGetLastError(), "step kernels");
+      s->step++;
+    }
+    cuda_check(cudaEventRecord(s->runEnd, s->st), "event");
   }
   sync(s);
   check_err(s);
+  maybe_grow_K(s);
+  float ms = 0.f;
+  cuda_check(cudaEventElapsedTime(&ms, s->runBeg, s->runEnd), "event time");
+  s->lastRunMs = ms;
+  cuda_check(cudaEventElapsedTime(&ms, s->runLoop, s->runEnd), "event time");
+  s->lastLoopMs = ms;
+  collect_phases(s);
   const double t1 = now_s();
   s->timers[0] = t1 - t0;
-  s->timers[8] = tResort;
-  s->timers[9] = s->timers[0] - tResort;
+  s->timers[1] = s->phaseMs[kPhForce] * 1e-3;
+  s->timers[6] = s->phaseMs[kPhIntegrate] * 1e-3;
+  s->timers[8] = graphDone ? s->phaseMs[kPhRebuild] * 1e-3 : tResort;
+  s->timers[9] = s->timers[0] - s->timers[1] - s->timers[6] - s->timers[8];
 }
 
 double* obs_partials(espp_system* s, int& nb) {
@@ -573,9 +913,8 @@ double* obs_partials(espp_system* s, int& nb) {
 
 void prepare_observables(espp_system* s) {
   if (s->idDirty) rebuild_id_tables(s);
-  if (s->resortFlag && !s->binned) bin(s, false);
-  if (s->has_vl && !s->binned) build_list(s);
   if (!s->binned) bin(s, false);
+  if (s->has_vl && !s->listValid) build_list(s);
 }
 
 void observable(espp_system* s, int which, int energy, double out[7]) {
@@ -637,14 +976,24 @@ void destroy(espp_system* s) {
   dfree(s->exclStart);
   dfree(s->exclIds);
   dfree(s->err);
-  dfree(s->maxSq);
-  dfree(s->maxDist);
-  dfree(s->flag);
+  destroy_graph(s);
+  free_particles(s->snap);
+  dfree(s->ctr);
+  dfree(s->d_pa);
   dfree(s->obs);
   dfree(s->partials);
   dfree(s->d_lj);
   dfree(s->d_ljf);
-  if (s->hflag) cudaFreeHost(s->hflag);
+  dfree(s->stIds);
+  dfree(s->stPos);
+  dfree(s->stVel);
+  dfree(s->stF);
+  dfree(s->stImg);
+  for (cudaEvent_t e : s->evPool) cudaEventDestroy(e);
+  if (s->runBeg) cudaEventDestroy(s->runBeg);
+  if (s->runLoop) cudaEventDestroy(s->runLoop);
+  if (s->runEnd) cudaEventDestroy(s->runEnd);
+  if (s->hctr) cudaFreeHost(s->hctr);
   if (s->st) cudaStreamDestroy(s->st);
   delete s;
 }
@@ -696,14 +1045,14 @@ int espp_system_create(const double box[3], double skin, const int32_t cell_grid
     s->scr.cellCount = dalloc<int32_t>(ncells);
     cuda_check(cudaMemset(s->cellStart, 0, sizeof(int32_t) * (ncells + 1)), "memset");
     s->err = dalloc<unsigned>(1);
-    s->maxSq = dalloc<unsigned long long>(1);
-    s->maxDist = dalloc<double>(1);
-    s->flag = dalloc<int>(1);
+    s->ctr = dalloc<DevCounters>(1);
+    s->d_pa = dalloc<ParticleArrays>(2);
     s->obs = dalloc<double>(8);
     cuda_check(cudaMemset(s->err, 0, sizeof(unsigned)), "memset");
-    cuda_check(cudaMemset(s->maxSq, 0, sizeof(unsigned long long)), "memset");
-    cuda_check(cudaMemset(s->maxDist, 0, sizeof(double)), "memset");
-    cuda_check(cudaMallocHost(&s->hflag, sizeof(int)), "pinned flag");
+    cuda_check(cudaMemset(s->ctr, 0, sizeof(DevCounters)), "memset");
+    cuda_check(cudaMemset(s->d_pa, 0, 2 * sizeof(ParticleArrays)), "memset");
+    cuda_check(cudaMallocHost(&s->hctr, sizeof(DevCounters)), "pinned counters");
+    if (const char* g = std::getenv("ESPP_B200_GRAPH")) s->useGraph = std::atoi(g) != 0;
     s->lj.ntypes = 1;
     upload_lj(s.get());
     *out = s.release();
@@ -766,7 +1115,9 @@ int espp_decompose(espp_system* s) {
   return guard([&] {
     checked(s);
     decompose(s);
-    cuda_check(cudaMemsetAsync(s->maxDist, 0, sizeof(double), s->st), "memset");
+    DevCounters c = get_counters(s);
+    c.maxDist = 0.0;
+    set_counters(s, c);
     sync(s);
     s->resortFlag = false;
   });
@@ -776,24 +1127,57 @@ int espp_num_particles(espp_system* s, int64_t* n) {
   return guard([&] { *n = checked(s)->n; });
 }
 
+void ensure_stage(espp_system* s, int64_t n) {
+  if (n <= s->stageCap) return;
+  dfree(s->stIds);
+  dfree(s->stPos);
+  dfree(s->stVel);
+  dfree(s->stF);
+  dfree(s->stImg);
+  int cap = (int)std::max<int64_t>(n, 1024);
+  s->stIds = dalloc<int64_t>(cap);
+  s->stPos = dalloc<double>(3 * (size_t)cap);
+  s->stVel = dalloc<double>(3 * (size_t)cap);
+  s->stF = dalloc<double>(3 * (size_t)cap);
+  s->stImg = dalloc<int32_t>(3 * (size_t)cap);
+  s->stageCap = cap;
+}
+
+// id map valid and current particle order fixed
+void ensure_id_map(espp_system* s) {
+  if (s->idDirty) rebuild_id_tables(s);
+  if (!s->binned) bin(s, false);
+}
+
 int espp_get_particles(espp_system* s, int64_t n, const int64_t* ids, double* pos,
                        double* vel, double* force, int32_t* image) {
   return guard([&] {
     checked(s);
-    HostParticles h = download(s, true);
-    std::unordered_map<int64_t, int> where;
-    where.reserve(h.id.size());
-    for (size_t k = 0; k < h.id.size(); ++k) where[h.id[k]] = (int)k;
-    for (int64_t i = 0; i < n; ++i) {
-      auto it = where.find(ids[i]);
-      if (it == where.end()) raise(ESPP_EINVAL, "unknown particle id " + std::to_string(ids[i]));
-      const int k = it->second;
-      for (int c = 0; c < 3; ++c) {
-        if (pos) pos[3 * i + c] = h.x[3 * k + c];
-        if (vel) vel[3 * i + c] = h.v[3 * k + c];
-        if (force) force[3 * i + c] = h.f[3 * k + c];
-        if (image) image[3 * i + c] = h.img[3 * k + c];
-      }
+    if (n <= 0) return;
+    if (!ids) raise(ESPP_EINVAL, "null id array");
+    ensure_id_map(s);
+    ensure_stage(s, n);
+    cuda_check(cudaMemcpyAsync(s->stIds, ids, sizeof(int64_t) * n, cudaMemcpyHostToDevice,
+                               s->st), "upload ids");
+    launch_get_by_id(s->view(), (int)n, s->stIds, pos ? s->stPos : nullptr,
+                     vel ? s->stVel : nullptr, force ? s->stF : nullptr,
+                     image ? s->stImg : nullptr, s->st);
+    if (pos)
+      cuda_check(cudaMemcpyAsync(pos, s->stPos, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost,
+                                 s->st), "download");
+    if (vel)
+      cuda_check(cudaMemcpyAsync(vel, s->stVel, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost,
+                                 s->st), "download");
+    if (force)
+      cuda_check(cudaMemcpyAsync(force, s->stF, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost,
+                                 s->st), "download");
+    if (image)
+      cuda_check(cudaMemcpyAsync(image, s->stImg, sizeof(int32_t) * 3 * n,
+                                 cudaMemcpyDeviceToHost, s->st), "download");
+    unsigned e = read_err(s);
+    if (e & kErrIdRange) {
+      cuda_check(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->st), "memset");
+      raise(ESPP_EINVAL, "unknown particle id");
     }
   });
 }
@@ -802,25 +1186,59 @@ int espp_set_particles(espp_system* s, int64_t n, const int64_t* ids, const doub
                        const double* vel) {
   return guard([&] {
     checked(s);
-    HostParticles h = download(s, true);
-    std::unordered_map<int64_t, int> where;
-    for (size_t k = 0; k < h.id.size(); ++k) where[h.id[k]] = (int)k;
-    for (int64_t i = 0; i < n; ++i) {
-      auto it = where.find(ids[i]);
-      if (it == where.end()) raise(ESPP_EINVAL, "unknown particle id " + std::to_string(ids[i]));
-      for (int c = 0; c < 3; ++c) {
-        if (pos) h.x[3 * it->second + c] = pos[3 * i + c];
-        if (vel) h.v[3 * it->second + c] = vel[3 * i + c];
-      }
+    if (n <= 0) return;
+    if (!ids) raise(ESPP_EINVAL, "null id array");
+    ensure_id_map(s);
+    ensure_stage(s, n);
+    cuda_check(cudaMemcpyAsync(s->stIds, ids, sizeof(int64_t) * n, cudaMemcpyHostToDevice,
+                               s->st), "upload ids");
+    if (pos)
+      cuda_check(cudaMemcpyAsync(s->stPos, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice,
+                                 s->st), "upload");
+    if (vel)
+      cuda_check(cudaMemcpyAsync(s->stVel, vel, sizeof(double) * 3 * n, cudaMemcpyHostToDevice,
+                                 s->st), "upload");
+    launch_set_by_id(s->view(), (int)n, s->stIds, pos ? s->stPos : nullptr,
+                     vel ? s->stVel : nullptr, s->st);
+    unsigned e = read_err(s);
+    if (e & kErrIdRange) {
+      cuda_check(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->st), "memset");
+      raise(ESPP_EINVAL, "unknown particle id");
     }
-    bool keepBinned = s->binned && !pos;
-    upload(s, h);
-    if (keepBinned) {
-      // same order as before: the cell structure and lists are still valid
-      s->binned = true;
-    }
+    // new positions: the reference re-sorts before the next force evaluation
     if (pos) s->resortFlag = true;
   });
+}
+
+int espp_set_profiling(espp_system* s, int32_t on) {
+  return guard([&] {
+    checked(s)->profiling = on != 0;
+    for (int k = 0; k < 4; ++k) {
+      s->phaseMs[k] = 0.0;
+      s->phaseLaunches[k] = 0;
+    }
+  });
+}
+
+int espp_profile(espp_system* s, double ms[4], int64_t launches[4]) {
+  return guard([&] {
+    checked(s);
+    for (int k = 0; k < 4; ++k) {
+      if (ms) ms[k] = s->phaseMs[k];
+      if (launches) launches[k] = s->phaseLaunches[k];
+    }
+  });
+}
+
+int espp_last_run_ms(espp_system* s, double ms[2]) {
+  return guard([&] {
+    ms[0] = checked(s)->lastRunMs;
+    ms[1] = s->lastLoopMs;
+  });
+}
+
+int espp_select_device(int32_t device) {
+  return guard([&] { cuda_check(cudaSetDevice(device), "cudaSetDevice"); });
 }
 
 int espp_vl_create(espp_system* s, double cutoff, int64_t nexcl, const int64_t* excl) {

@@ -60,9 +60,20 @@ struct ParticleArrays {
   int32_t* img;  // 3*cap
 };
 
+// Step-loop state kept on the device so that a captured CUDA graph can run the loop.
+struct DevCounters {
+  unsigned long long maxSq;  // max |dx|^2 of the last integrate1, as double bits
+  double maxDist;            // accumulated max displacement since the last re-sort
+  long long step;            // step whose force is being computed (Langevin counter)
+  long long remaining;       // loop steps left after the current one
+  long long resorts;         // re-sorts done in this run
+  int flag;                  // re-sort needed this step
+  int nnMax;                 // largest neighbour count seen by the Verlet builds
+};
+
 // Pointers and scalars every kernel needs; passed by value.
 struct DevView {
-  ParticleArrays a;       // current arrays
+  ParticleArrays* pa;     // device: pa[0] current arrays, pa[1] target of the re-sort
   int n;                  // particles
   int cap;                // allocated rows
   double L[3], invL[3], halfL[3];
@@ -94,7 +105,7 @@ struct DevView {
   int ljSingle;           // only pair (0,0) is set
   int ljCapped;           // some pair uses LennardJonesCapped
   unsigned* err;          // device error word
-  unsigned long long* maxSq;  // max |dx|^2 of the last integrate1, as double bits
+  DevCounters* ctr;       // step-loop state
 };
 
 struct RebuildScratch {
@@ -107,8 +118,7 @@ struct RebuildScratch {
 // launchers (espp_kernels.cu)
 void launch_fold_bin(const DevView& d, RebuildScratch& s, bool fold, cudaStream_t st);
 void launch_sort_cells(const DevView& d, RebuildScratch& s, cudaStream_t st);
-void launch_gather(const DevView& d, const ParticleArrays& src, const ParticleArrays& dst,
-                   const RebuildScratch& s, cudaStream_t st);
+void launch_gather(const DevView& d, const RebuildScratch& s, cudaStream_t st);
 void launch_id_map(const DevView& d, cudaStream_t st);
 void launch_build_nl(const DevView& d, double cutsq, cudaStream_t st);
 void launch_posq(const DevView& d, cudaStream_t st);
@@ -116,6 +126,7 @@ void launch_forces(const DevView& d, bool mixed, const FENEParams& fene, int tpp
                    cudaStream_t st);
 struct IntegrateArgs {
   int do_i2, do_i1, langevin, capMode, storeFtot, phase, mixed;
+  int fromCounters;  // step from ctr->step; final step (i2 only, store F) when remaining==0
   double dt, pref1, pref2;
   double cap[3];
   uint64_t seed;
@@ -123,8 +134,10 @@ struct IntegrateArgs {
 };
 void launch_integrate(const DevView& d, const IntegrateArgs& a, cudaStream_t st);
 // maxDist += sqrt(max |dx|^2); flag = maxDist > skinHalf
-void launch_decide(const DevView& d, double* maxDist, int* flag, double skinHalf,
-                   cudaStream_t st);
+void launch_decide(const DevView& d, double skinHalf, cudaStream_t st);
+// graph form: also advances ctr->step / ctr->remaining and sets the conditionals
+void launch_decide_graph(const DevView& d, double skinHalf, cudaGraphConditionalHandle hIf,
+                         cudaGraphConditionalHandle hWhile, cudaStream_t st);
 // observables: out[0..6] = (scalar, tensor xx yy zz xy xz yz); deterministic reductions
 void launch_lj_observables(const DevView& d, double* partials, int nblocks, double* out,
                            int energy, cudaStream_t st);
@@ -142,5 +155,9 @@ void launch_bond_maxsq(const DevView& d, double* partials, int nblocks, double* 
 // float copy of an LJ table for the mixed-precision kernel
 void make_float_table(const LJTable& t, LJPairF* out);
 int observable_blocks(int n);
+void launch_set_by_id(const DevView& d, int n, const int64_t* ids, const double* pos,
+                      const double* vel, cudaStream_t st);
+void launch_get_by_id(const DevView& d, int n, const int64_t* ids, double* pos, double* vel,
+                      double* force, int32_t* img, cudaStream_t st);
 
 }  // namespace espp

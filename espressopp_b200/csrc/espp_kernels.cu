@@ -84,13 +84,14 @@ __device__ __forceinline__ void langevin_uniforms(uint64_t seed, int64_t id, int
 
 // OrthorhombicBC::foldCoordinate + CellGrid::mapPositionToCellChecked/Clipped.
 __global__ void k_fold_bin(DevView d, RebuildScratch s, int fold) {
+  const ParticleArrays a = d.pa[0];
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.n) return;
   int c[3];
   bool outside = false;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    double x = d.a.x[(size_t)k * d.cap + i];
+    double x = a.x[(size_t)k * d.cap + i];
     if (fold) {
       double q = floor(__dmul_rn(x, d.invL[k]));
       if (!(fabs(q) < 1.0e9)) {
@@ -98,9 +99,9 @@ __global__ void k_fold_bin(DevView d, RebuildScratch s, int fold) {
         q = 0.0;
       }
       int tmp = (int)q;
-      d.a.img[(size_t)k * d.cap + i] += tmp;
+      a.img[(size_t)k * d.cap + i] += tmp;
       x = __dsub_rn(x, __dmul_rn((double)tmp, d.L[k]));
-      d.a.x[(size_t)k * d.cap + i] = x;
+      a.x[(size_t)k * d.cap + i] = x;
     }
     double lpos = x;
     double t = __dmul_rn(lpos, d.invCellSize[k]);
@@ -159,14 +160,15 @@ __global__ void k_scatter(DevView d, RebuildScratch s) {
 // Order inside a cell: by particle id, so the layout is independent of the atomic
 // arrival order above.
 __global__ void k_sort_in_cell(DevView d, RebuildScratch s) {
+  const ParticleArrays a = d.pa[0];
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.ncells) return;
   int b = d.cellStart[c], e = d.cellStart[c + 1];
   for (int k = b + 1; k < e; ++k) {
     int v = s.perm[k];
-    int64_t key = d.a.id[v];
+    int64_t key = a.id[v];
     int m = k - 1;
-    while (m >= b && d.a.id[s.perm[m]] > key) {
+    while (m >= b && a.id[s.perm[m]] > key) {
       s.perm[m + 1] = s.perm[m];
       --m;
     }
@@ -174,7 +176,8 @@ __global__ void k_sort_in_cell(DevView d, RebuildScratch s) {
   }
 }
 
-__global__ void k_gather(DevView d, ParticleArrays src, ParticleArrays dst, RebuildScratch s) {
+__global__ void k_gather(DevView d, RebuildScratch s) {
+  const ParticleArrays src = d.pa[0], dst = d.pa[1];
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= d.n) return;
   int o = s.perm[k];
@@ -195,9 +198,10 @@ __global__ void k_gather(DevView d, ParticleArrays src, ParticleArrays dst, Rebu
 }
 
 __global__ void k_id_map(DevView d) {
+  const ParticleArrays a = d.pa[0];
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= d.n) return;
-  int64_t off = d.a.id[k] - d.idMin;
+  int64_t off = a.id[k] - d.idMin;
   if (off < 0 || off >= d.idSpan) {
     atomicOr(d.err, kErrIdRange);
     return;
@@ -206,10 +210,11 @@ __global__ void k_id_map(DevView d) {
 }
 
 __global__ void k_posq(DevView d) {
+  const ParticleArrays a = d.pa[0];
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= d.n) return;
-  d.posq[k] = fixed_coords(d, d.a.x[k], d.a.x[(size_t)d.cap + k], d.a.x[2 * (size_t)d.cap + k],
-                           d.a.type[k]);
+  d.posq[k] = fixed_coords(d, a.x[k], a.x[(size_t)d.cap + k], a.x[2 * (size_t)d.cap + k],
+                           a.type[k]);
 }
 
 // ---- Verlet list -------------------------------------------------------------------
@@ -229,15 +234,16 @@ __device__ __forceinline__ bool is_excluded(const DevView& d, int64_t a, int64_t
 // where p1 is the particle of the backward cell and shift is the ghost image offset
 // of the forward cell (VerletList.cpp:399-426, DomainDecomposition.cpp:1347-1391).
 __global__ void k_build_nl(DevView d, double cutsq) {
+  const ParticleArrays a = d.pa[0];
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (warp >= d.ncells) return;
   const int c = warp;
   const int cx = c % d.nc[0], cy = (c / d.nc[0]) % d.nc[1], cz = c / (d.nc[0] * d.nc[1]);
   const int s0 = d.cellStart[c], s1 = d.cellStart[c + 1];
-  const double* X = d.a.x;
-  const double* Y = d.a.x + d.cap;
-  const double* Z = d.a.x + 2 * (size_t)d.cap;
+  const double* X = a.x;
+  const double* Y = a.x + d.cap;
+  const double* Z = a.x + 2 * (size_t)d.cap;
   for (int base = s0; base < s1; base += 32) {
     const int i = base + lane;
     const bool act = i < s1;
@@ -247,7 +253,7 @@ __global__ void k_build_nl(DevView d, double cutsq) {
       xi = X[i];
       yi = Y[i];
       zi = Z[i];
-      idi = d.a.id[i];
+      idi = a.id[i];
     }
     int cnt = 0;
     for (int oz = -1; oz <= 1; ++oz)
@@ -280,7 +286,7 @@ __global__ void k_build_nl(DevView d, double cutsq) {
             const double d2 =
                 __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
             if (act && j != i && !(d2 > cutsq)) {
-              if (!is_excluded(d, idi, d.a.id[j])) {
+              if (!is_excluded(d, idi, a.id[j])) {
                 if (cnt < d.K) d.nl[(size_t)cnt * d.cap + i] = j;
                 ++cnt;
               }
@@ -291,6 +297,8 @@ __global__ void k_build_nl(DevView d, double cutsq) {
       if (cnt > d.K) atomicOr(d.err, kErrNlOverflow);
       d.nn[i] = min(cnt, d.K);
     }
+    const int wmax = __reduce_max_sync(0xffffffffu, act ? cnt : 0);
+    if (lane == 0 && wmax > 0) atomicMax(&d.ctr->nnMax, wmax);
   }
 }
 
@@ -308,6 +316,7 @@ __device__ __forceinline__ long long to_fix(float f, unsigned* err) {
 // depend on the order in which they are added.
 template <int TPP, bool SINGLE, bool CAPPED, bool FENE>
 __global__ void __launch_bounds__(256) k_force_mixed(DevView d, FENEParams fp) {
+  const ParticleArrays a = d.pa[0];
   __shared__ LJPairF sP[kMaxTypes * kMaxTypes];
   if (!SINGLE) {
     for (int t = threadIdx.x; t < d.ntypes * d.ntypes; t += blockDim.x) sP[t] = d.ljf[t];
@@ -346,7 +355,7 @@ __global__ void __launch_bounds__(256) k_force_mixed(DevView d, FENEParams fp) {
   }
   long long Fx = to_fix(fx, d.err), Fy = to_fix(fy, d.err), Fz = to_fix(fz, d.err);
   if (FENE && sub == 0 && act) {
-    const int64_t off = d.a.id[i] - d.idMin;
+    const int64_t off = a.id[i] - d.idMin;
     const int b0 = d.bondStart[off], b1 = d.bondStart[off + 1];
     float bx = 0.f, by = 0.f, bz = 0.f;
     const float rmaxsq = (float)fp.rmaxsq, K = (float)fp.K, r0 = (float)fp.r0;
@@ -405,17 +414,18 @@ __device__ __forceinline__ double min_image(double dx, double L, double halfL) {
 // and FENE.hpp:97-112 on minimum-image distances).
 template <int TPP, bool SINGLE, bool CAPPED, bool FENE>
 __global__ void __launch_bounds__(256) k_force_fp64(DevView d, FENEParams fp) {
+  const ParticleArrays a = d.pa[0];
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int i0 = gt / TPP;
   const int sub = gt % TPP;
   if (TPP == 1 && i0 >= d.n) return;
   const bool act = i0 < d.n;
   const int i = act ? i0 : 0;
-  const double* X = d.a.x;
-  const double* Y = d.a.x + d.cap;
-  const double* Z = d.a.x + 2 * (size_t)d.cap;
+  const double* X = a.x;
+  const double* Y = a.x + d.cap;
+  const double* Z = a.x + 2 * (size_t)d.cap;
   const double xi = X[i], yi = Y[i], zi = Z[i];
-  const int ti = d.a.type[i];
+  const int ti = a.type[i];
   const int cnt = act ? d.nn[i] : 0;
   double fx = 0, fy = 0, fz = 0;
   const int ntypes = d.ntypes;
@@ -425,7 +435,7 @@ __global__ void __launch_bounds__(256) k_force_fp64(DevView d, FENEParams fp) {
     const double dy = min_image(yi - __ldg(&Y[j]), d.L[1], d.halfL[1]);
     const double dz = min_image(zi - __ldg(&Z[j]), d.L[2], d.halfL[2]);
     const double r2 = dx * dx + dy * dy + dz * dz;
-    const LJPair& P = SINGLE ? d.lj[0] : d.lj[ti * ntypes + __ldg(&d.a.type[j])];
+    const LJPair& P = SINGLE ? d.lj[0] : d.lj[ti * ntypes + __ldg(&a.type[j])];
     if (!P.set || r2 > P.rcsq) continue;
     double ff;
     if (CAPPED && P.caprad > 0 && !(r2 > P.caprad * P.caprad)) {
@@ -440,7 +450,7 @@ __global__ void __launch_bounds__(256) k_force_fp64(DevView d, FENEParams fp) {
     fz += dz * ff;
   }
   if (FENE && sub == 0 && act) {
-    const int64_t off = d.a.id[i] - d.idMin;
+    const int64_t off = a.id[i] - d.idMin;
     const int b0 = d.bondStart[off], b1 = d.bondStart[off + 1];
     for (int b = b0; b < b1; ++b) {
       const int64_t po = d.bondPartner[b] - d.idMin;
@@ -494,20 +504,28 @@ __device__ __forceinline__ double warp_max(double v) {
 // with the reference's operation order and no FMA contraction.
 template <bool MIXED>
 __global__ void __launch_bounds__(256) k_integrate(DevView d, IntegrateArgs a) {
+  const ParticleArrays P = d.pa[0];
   __shared__ double smax[kBlock / 32];
+  if (a.fromCounters) {  // uniform over the grid: written by the decide kernel before
+    a.step = d.ctr->step;
+    if (d.ctr->remaining == 0) {
+      a.do_i1 = 0;
+      a.storeFtot = 1;
+    }
+  }
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double sq = 0.0;
   if (i < d.n) {
     const size_t cap = d.cap;
-    const double m = d.a.mass[i];
+    const double m = P.mass[i];
     double F[3], v[3], x[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       F[k] = MIXED ? (double)d.ffix[k * cap + i] * kInvFix : d.f64[k * cap + i];
-      v[k] = d.a.v[k * cap + i];
+      v[k] = P.v[k * cap + i];
     }
     if (a.langevin) {
-      const int64_t id = d.a.id[i];
+      const int64_t id = P.id[i];
       if (!(d.langExcl && d.langExcl[id - d.idMin])) {
         const double massf = sqrt(m);
         double u[3];
@@ -553,16 +571,16 @@ __global__ void __launch_bounds__(256) k_integrate(DevView d, IntegrateArgs a) {
       for (int k = 0; k < 3; ++k) {
         v[k] = __dadd_rn(v[k], __dmul_rn(dtfm, F[k]));
         dp[k] = __dmul_rn(v[k], a.dt);
-        x[k] = __dadd_rn(d.a.x[k * cap + i], dp[k]);
-        d.a.x[k * cap + i] = x[k];
+        x[k] = __dadd_rn(P.x[k * cap + i], dp[k]);
+        P.x[k * cap + i] = x[k];
       }
       sq = __dadd_rn(__dadd_rn(__dmul_rn(dp[0], dp[0]), __dmul_rn(dp[1], dp[1])),
                      __dmul_rn(dp[2], dp[2]));
-      d.posq[i] = fixed_coords(d, x[0], x[1], x[2], d.a.type[i]);
+      d.posq[i] = fixed_coords(d, x[0], x[1], x[2], P.type[i]);
     }
     if (a.do_i1 || a.do_i2) {
 #pragma unroll
-      for (int k = 0; k < 3; ++k) d.a.v[k * cap + i] = v[k];
+      for (int k = 0; k < 3; ++k) P.v[k * cap + i] = v[k];
     }
   }
   if (a.do_i1) {
@@ -573,19 +591,45 @@ __global__ void __launch_bounds__(256) k_integrate(DevView d, IntegrateArgs a) {
       double v = threadIdx.x < blockDim.x / 32 ? smax[threadIdx.x] : 0.0;
       v = warp_max(v);
       if (threadIdx.x == 0 && v > 0.0)
-        atomicMax(d.maxSq, (unsigned long long)__double_as_longlong(v));
+        atomicMax(&d.ctr->maxSq, (unsigned long long)__double_as_longlong(v));
     }
   }
 }
 
-__global__ void k_decide(unsigned long long* maxSq, double* maxDist, int* flag,
-                         double skinHalf) {
-  double m = __longlong_as_double((long long)*maxSq);
-  *maxSq = 0ull;
-  double md = __dadd_rn(*maxDist, sqrt(m));
-  int f = md > skinHalf ? 1 : 0;
-  *maxDist = f ? 0.0 : md;
-  *flag = f;
+__device__ __forceinline__ int decide_core(DevCounters* c, double skinHalf) {
+  const double m = __longlong_as_double((long long)c->maxSq);
+  c->maxSq = 0ull;
+  const double md = __dadd_rn(c->maxDist, sqrt(m));
+  const int f = md > skinHalf ? 1 : 0;
+  c->maxDist = f ? 0.0 : md;
+  c->flag = f;
+  c->resorts += f;
+  return f;
+}
+
+__global__ void k_decide(DevCounters* c, double skinHalf) { decide_core(c, skinHalf); }
+
+// First node of the captured step loop: advance the step, decide on the re-sort and
+// set the IF (re-sort) and WHILE (more steps) conditionals.
+__global__ void k_decide_graph(DevCounters* c, double skinHalf, cudaGraphConditionalHandle hIf,
+                               cudaGraphConditionalHandle hWhile) {
+  c->step += 1;
+  const long long rem = c->remaining - 1;
+  c->remaining = rem;
+  const int f = decide_core(c, skinHalf);
+  cudaGraphSetConditional(hIf, f ? 1u : 0u);
+  cudaGraphSetConditional(hWhile, rem > 0 ? 1u : 0u);
+}
+
+__global__ void k_zero_i32(int32_t* p, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = 0;
+}
+
+__global__ void k_swap_arrays(ParticleArrays* pa) {
+  const ParticleArrays t = pa[0];
+  pa[0] = pa[1];
+  pa[1] = t;
 }
 
 // ---- observables -------------------------------------------------------------------
@@ -639,14 +683,15 @@ __global__ void k_sum_partials(const double* __restrict__ partials, int nblocks,
 // LennardJones.hpp:109-114) or virial r.F and its tensor (energy=0,
 // VerletListInteractionTemplate.hpp:274-331) over each listed pair once (j > i).
 __global__ void k_lj_obs(DevView d, int energy, double* partials) {
+  const ParticleArrays a = d.pa[0];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   if (i < d.n) {
-    const double* X = d.a.x;
-    const double* Y = d.a.x + d.cap;
-    const double* Z = d.a.x + 2 * (size_t)d.cap;
+    const double* X = a.x;
+    const double* Y = a.x + d.cap;
+    const double* Z = a.x + 2 * (size_t)d.cap;
     const double xi = X[i], yi = Y[i], zi = Z[i];
-    const int ti = d.a.type[i];
+    const int ti = a.type[i];
     const int cnt = d.nn[i];
     for (int k = 0; k < cnt; ++k) {
       const int j = d.nl[(size_t)k * d.cap + i];
@@ -656,7 +701,7 @@ __global__ void k_lj_obs(DevView d, int energy, double* partials) {
       const double dz = min_image(zi - Z[j], d.L[2], d.halfL[2]);
       const double r2 =
           __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-      const LJPair& P = d.lj[ti * d.ntypes + d.a.type[j]];
+      const LJPair& P = d.lj[ti * d.ntypes + a.type[j]];
       if (!P.set || r2 > P.rcsq) continue;
       if (energy) {
         double ds = r2;
@@ -689,13 +734,14 @@ __global__ void k_lj_obs(DevView d, int energy, double* partials) {
 
 // FENE energy (FENE.hpp:91-95) or virial over each bond once (partner id > own id).
 __global__ void k_fene_obs(DevView d, FENEParams fp, int energy, double* partials) {
+  const ParticleArrays a = d.pa[0];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   if (i < d.n && fp.on) {
-    const double* X = d.a.x;
-    const double* Y = d.a.x + d.cap;
-    const double* Z = d.a.x + 2 * (size_t)d.cap;
-    const int64_t id = d.a.id[i];
+    const double* X = a.x;
+    const double* Y = a.x + d.cap;
+    const double* Z = a.x + 2 * (size_t)d.cap;
+    const int64_t id = a.id[i];
     const int64_t off = id - d.idMin;
     const int b0 = d.bondStart[off], b1 = d.bondStart[off + 1];
     for (int b = b0; b < b1; ++b) {
@@ -736,17 +782,18 @@ __global__ void k_fene_obs(DevView d, FENEParams fp, int energy, double* partial
 
 // max bond length^2 over all bonds (FixedPairList::getLongtimeMaxBondSqr)
 __global__ void k_bond_maxsq(DevView d, double* partials) {
+  const ParticleArrays a = d.pa[0];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[1] = {0.0};
   __shared__ double sm[kBlock / 32];
   if (i < d.n && d.bondStart) {
-    const int64_t off = d.a.id[i] - d.idMin;
+    const int64_t off = a.id[i] - d.idMin;
     for (int b = d.bondStart[off]; b < d.bondStart[off + 1]; ++b) {
       const int j = d.id2idx[d.bondPartner[b] - d.idMin];
       if (j < 0) continue;
       double r2 = 0;
       for (int k = 0; k < 3; ++k) {
-        const double dk = min_image(d.a.x[(size_t)k * d.cap + i] - d.a.x[(size_t)k * d.cap + j],
+        const double dk = min_image(a.x[(size_t)k * d.cap + i] - a.x[(size_t)k * d.cap + j],
                                     d.L[k], d.halfL[k]);
         r2 += dk * dk;
       }
@@ -772,31 +819,34 @@ __global__ void k_max_partials(const double* partials, int nb, double* out) {
 }
 
 __global__ void k_kinetic(DevView d, double* partials) {
+  const ParticleArrays a = d.pa[0];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[1] = {0.0};
   if (i < d.n) {
-    const double vx = d.a.v[i], vy = d.a.v[(size_t)d.cap + i], vz = d.a.v[2 * (size_t)d.cap + i];
-    acc[0] = d.a.mass[i] * (vx * vx + vy * vy + vz * vz);
+    const double vx = a.v[i], vy = a.v[(size_t)d.cap + i], vz = a.v[2 * (size_t)d.cap + i];
+    acc[0] = a.mass[i] * (vx * vx + vy * vy + vz * vz);
   }
   block_sum_store<1>(acc, partials);
 }
 
 __global__ void k_pair_count(DevView d, int32_t* counts) {
+  const ParticleArrays a = d.pa[0];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.n) return;
-  const int64_t idi = d.a.id[i];
+  const int64_t idi = a.id[i];
   int c = 0;
-  for (int k = 0; k < d.nn[i]; ++k) c += d.a.id[d.nl[(size_t)k * d.cap + i]] > idi;
+  for (int k = 0; k < d.nn[i]; ++k) c += a.id[d.nl[(size_t)k * d.cap + i]] > idi;
   counts[i] = c;
 }
 
 __global__ void k_pair_write(DevView d, const int64_t* offsets, int64_t* out) {
+  const ParticleArrays a = d.pa[0];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.n) return;
-  const int64_t idi = d.a.id[i];
+  const int64_t idi = a.id[i];
   int64_t o = offsets[i];
   for (int k = 0; k < d.nn[i]; ++k) {
-    const int64_t idj = d.a.id[d.nl[(size_t)k * d.cap + i]];
+    const int64_t idj = a.id[d.nl[(size_t)k * d.cap + i]];
     if (idj > idi) {
       out[2 * o] = idi;
       out[2 * o + 1] = idj;
@@ -805,12 +855,54 @@ __global__ void k_pair_write(DevView d, const int64_t* offsets, int64_t* out) {
   }
 }
 
+
+// Particle state by id through the dense id map: scatter host rows into the sorted
+// arrays / gather them back out (Storage::lookupRealParticle on the device).
+__global__ void k_set_by_id(DevView d, int n, const int64_t* ids, const double* pos,
+                            const double* vel) {
+  const ParticleArrays a = d.pa[0];
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int64_t off = ids[r] - d.idMin;
+  const int k = (off >= 0 && off < d.idSpan) ? d.id2idx[off] : -1;
+  if (k < 0) {
+    atomicOr(d.err, kErrIdRange);
+    return;
+  }
+  for (int c = 0; c < 3; ++c) {
+    if (pos) a.x[(size_t)c * d.cap + k] = pos[3 * (size_t)r + c];
+    if (vel) a.v[(size_t)c * d.cap + k] = vel[3 * (size_t)r + c];
+  }
+  if (pos)
+    d.posq[k] = fixed_coords(d, a.x[k], a.x[(size_t)d.cap + k], a.x[2 * (size_t)d.cap + k],
+                             a.type[k]);
+}
+
+__global__ void k_get_by_id(DevView d, int n, const int64_t* ids, double* pos, double* vel,
+                            double* force, int32_t* img) {
+  const ParticleArrays a = d.pa[0];
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int64_t off = ids[r] - d.idMin;
+  const int k = (off >= 0 && off < d.idSpan) ? d.id2idx[off] : -1;
+  if (k < 0) {
+    atomicOr(d.err, kErrIdRange);
+    return;
+  }
+  for (int c = 0; c < 3; ++c) {
+    if (pos) pos[3 * (size_t)r + c] = a.x[(size_t)c * d.cap + k];
+    if (vel) vel[3 * (size_t)r + c] = a.v[(size_t)c * d.cap + k];
+    if (force) force[3 * (size_t)r + c] = d.ftot[(size_t)c * d.cap + k];
+    if (img) img[3 * (size_t)r + c] = a.img[(size_t)c * d.cap + k];
+  }
+}
+
 }  // namespace
 
 // ---- launchers ---------------------------------------------------------------------
 
 void launch_fold_bin(const DevView& d, RebuildScratch& s, bool fold, cudaStream_t st) {
-  cudaMemsetAsync(s.cellCount, 0, sizeof(int32_t) * d.ncells, st);
+  k_zero_i32<<<blocks_for(d.ncells), kBlock, 0, st>>>(s.cellCount, d.ncells);
   if (d.n > 0) k_fold_bin<<<blocks_for(d.n), kBlock, 0, st>>>(d, s, fold ? 1 : 0);
 }
 
@@ -820,9 +912,9 @@ void launch_sort_cells(const DevView& d, RebuildScratch& s, cudaStream_t st) {
   k_sort_in_cell<<<blocks_for(d.ncells), kBlock, 0, st>>>(d, s);
 }
 
-void launch_gather(const DevView& d, const ParticleArrays& src, const ParticleArrays& dst,
-                   const RebuildScratch& s, cudaStream_t st) {
-  if (d.n > 0) k_gather<<<blocks_for(d.n), kBlock, 0, st>>>(d, src, dst, s);
+void launch_gather(const DevView& d, const RebuildScratch& s, cudaStream_t st) {
+  if (d.n > 0) k_gather<<<blocks_for(d.n), kBlock, 0, st>>>(d, s);
+  k_swap_arrays<<<1, 1, 0, st>>>(d.pa);
 }
 
 void launch_id_map(const DevView& d, cudaStream_t st) {
@@ -893,9 +985,13 @@ void launch_integrate(const DevView& d, const IntegrateArgs& a, cudaStream_t st)
     k_integrate<false><<<blocks_for(d.n), kBlock, 0, st>>>(d, a);
 }
 
-void launch_decide(const DevView& d, double* maxDist, int* flag, double skinHalf,
-                   cudaStream_t st) {
-  k_decide<<<1, 1, 0, st>>>(d.maxSq, maxDist, flag, skinHalf);
+void launch_decide(const DevView& d, double skinHalf, cudaStream_t st) {
+  k_decide<<<1, 1, 0, st>>>(d.ctr, skinHalf);
+}
+
+void launch_decide_graph(const DevView& d, double skinHalf, cudaGraphConditionalHandle hIf,
+                         cudaGraphConditionalHandle hWhile, cudaStream_t st) {
+  k_decide_graph<<<1, 1, 0, st>>>(d.ctr, skinHalf, hIf, hWhile);
 }
 
 void launch_lj_observables(const DevView& d, double* partials, int nblocks, double* out,
@@ -932,5 +1028,15 @@ void launch_pair_write(const DevView& d, const int64_t* offsets, int64_t* out,
 }
 
 int observable_blocks(int n) { return blocks_for(n > 0 ? n : 1); }
+
+void launch_set_by_id(const DevView& d, int n, const int64_t* ids, const double* pos,
+                      const double* vel, cudaStream_t st) {
+  if (n > 0) k_set_by_id<<<blocks_for(n), kBlock, 0, st>>>(d, n, ids, pos, vel);
+}
+
+void launch_get_by_id(const DevView& d, int n, const int64_t* ids, double* pos, double* vel,
+                      double* force, int32_t* img, cudaStream_t st) {
+  if (n > 0) k_get_by_id<<<blocks_for(n), kBlock, 0, st>>>(d, n, ids, pos, vel, force, img);
+}
 
 }  // namespace espp

@@ -152,6 +152,20 @@ ESPP_API int espp_virial_tensor(espp_system* s, int32_t which, double w[6]);
 /* sum m v^2 over real particles and their count (analysis/Temperature.hpp:57-125). */
 ESPP_API int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n);
 
+/* ---- measurement ---------------------------------------------------------------
+ * No reference counterpart (the reference times phases with esutil::WallTimer,
+ * VelocityVerlet.cpp:171-232).  With profiling on, run() brackets each phase with
+ * CUDA events on the system's stream: ms[0] pair/bond force kernel, ms[1] integrator
+ * kernel, ms[2] re-sort + Verlet build, ms[3] rebuild decision; launches[] counts the
+ * kernels each phase launched.  espp_set_profiling resets the sums. */
+ESPP_API int espp_set_profiling(espp_system* s, int32_t on);
+ESPP_API int espp_profile(espp_system* s, double ms[4], int64_t launches[4]);
+/* Device time of the last espp_run on the system's stream (ms): ms[0] whole call,
+ * ms[1] the step loop after the start-of-run force evaluation. */
+ESPP_API int espp_last_run_ms(espp_system* s, double ms[2]);
+/* Selects the CUDA device for systems created afterwards on the calling thread. */
+ESPP_API int espp_select_device(int32_t device);
+
 #ifdef __cplusplus
 }
 #endif

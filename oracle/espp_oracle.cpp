@@ -1004,6 +1004,28 @@ int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n) {
   return ESPP_OK;
 }
 
+int espp_set_profiling(espp_system* s, int32_t) {
+  CHECK_S(s);
+  return ESPP_OK;
+}
+
+int espp_profile(espp_system* s, double ms[4], int64_t launches[4]) {
+  CHECK_S(s);
+  for (int k = 0; k < 4; ++k) {
+    if (ms) ms[k] = 0.0;
+    if (launches) launches[k] = 0;
+  }
+  return ESPP_OK;
+}
+
+int espp_last_run_ms(espp_system* s, double ms[2]) {
+  CHECK_S(s);
+  ms[0] = ms[1] = 0.0;
+  return ESPP_OK;
+}
+
+int espp_select_device(int32_t) { return ESPP_OK; }
+
 // Test hook: Philox outputs, so the tests can pin the generator on known answers.
 int espp_oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
   U4 c;
