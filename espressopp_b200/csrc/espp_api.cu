@@ -16,6 +16,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <unordered_map>
@@ -1000,6 +1001,40 @@ void destroy(espp_system* s) {
 
 }  // namespace
 
+namespace {
+
+// ---- allocation-free energy ------------------------------------------------------
+// Scratch of espp_energy_noalloc: slots [0, 8) take the final sums, slots [8, ...) one
+// row of 7 partial sums per reduction block (256 particles).  Statically sized, so
+// the call never allocates; every GPU that loads this library holds these 1.8 MB
+// until the process exits.
+constexpr int kNoAllocMaxBlocks = 32768;
+constexpr long long kNoAllocMaxParticles = (long long)kNoAllocMaxBlocks * 256;
+static __device__ __align__(256) double g_noalloc_scratch[8 + 7 * kNoAllocMaxBlocks];
+
+// Device address of g_noalloc_scratch per device, looked up once with that device
+// current (the host-side name of the array is only a stand-in, not a device address).
+std::mutex g_noalloc_mutex;
+double* g_noalloc_addr[256] = {nullptr};
+
+double* noalloc_scratch(int device) {
+  if (device < 0 || device >= 256) raise(ESPP_ERANGE, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_addr[device]) {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) {
+      cudaGetLastError();
+      raise(ESPP_ECUDA, std::string("cudaGetSymbolAddress of the energy scratch failed: ") +
+                            cudaGetErrorString(e));
+    }
+    g_noalloc_addr[device] = (double*)ptr;
+  }
+  return g_noalloc_addr[device];
+}
+
+}  // namespace
+
 extern "C" {
 
 int espp_abi_version(void) { return 1; }
@@ -1502,6 +1537,42 @@ int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n) {
     double* part = obs_partials(s, nb);
     launch_kinetic(s->view(), part, nb, s->obs, s->st);
     cuda_check(cudaMemcpyAsync(sum_mv2, s->obs, sizeof(double), cudaMemcpyDeviceToHost, s->st),
+               "download");
+    sync(s);
+  });
+}
+
+int espp_energy_noalloc(espp_system* s, int32_t which, double* e) {
+  return guard([&] {
+    checked(s);
+    if (!e) raise(ESPP_EINVAL, "null output pointer");
+    if (which != ESPP_IA_LJ && which != ESPP_IA_FENE)
+      raise(ESPP_EINVAL, "unknown interaction kind");
+    if (s->n > kNoAllocMaxParticles)
+      raise(ESPP_ERANGE, "espp_energy_noalloc handles at most 8388608 particles (its static "
+                         "scratch holds 32768 reduction blocks of 256); use espp_energy");
+    // everything the reduction reads must already exist: this call builds nothing
+    if (s->idDirty || !s->binned || (which == ESPP_IA_LJ && s->has_vl && s->lj_any &&
+                                     !s->listValid))
+      raise(ESPP_ESTATE, "espp_energy_noalloc needs particles sorted and the Verlet list "
+                         "built (call espp_decompose, espp_run or espp_energy first)");
+    double* scratch = noalloc_scratch(s->device);
+    *e = 0.0;
+    if (s->n == 0) return;
+    if (which == ESPP_IA_LJ && (!s->has_vl || !s->lj_any)) return;
+    if (which == ESPP_IA_FENE && !s->fene.on) return;
+    // every slot read below is written first: each block stores its own partial row and
+    // the final kernel overwrites the 7 result slots, so nothing needs clearing
+    const int nb = observable_blocks(s->n);
+    double* partials = scratch + 8;
+    double* out = scratch;
+    DevView d = s->view();
+    if (which == ESPP_IA_LJ)
+      launch_lj_observables(d, partials, nb, out, 1, s->st);
+    else
+      launch_fene_observables(d, s->fene, partials, nb, out, 1, s->st);
+    cuda_check(cudaGetLastError(), "energy kernels");
+    cuda_check(cudaMemcpyAsync(e, out, sizeof(double), cudaMemcpyDeviceToHost, s->st),
                "download");
     sync(s);
   });

@@ -152,6 +152,25 @@ ESPP_API int espp_virial_tensor(espp_system* s, int32_t which, double w[6]);
 /* sum m v^2 over real particles and their count (analysis/Temperature.hpp:57-125). */
 ESPP_API int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n);
 
+/* Same result as espp_energy (identical kernels and reduction order), but the call
+ * allocates no device memory: the per-block partial sums live in a statically sized
+ * array inside the library instead of a buffer obtained with cudaMalloc.  No
+ * counterpart exists in the reference.  It is meant for callers that may not allocate
+ * GPU memory themselves or have a library do it for them: hosts whose device memory
+ * is owned by another allocator (a framework's pool or caching allocator, or a fixed
+ * memory budget), and time-critical loops where a first-use cudaMalloc or cudaFree
+ * would synchronise the device.
+ *   - Limit: at most 8,388,608 particles (32768 reduction blocks of 256); more gives
+ *     ESPP_ERANGE.  The static array (1.8 MB) is held on every GPU that loads the
+ *     library until the process exits.
+ *   - The system must be ready: particles sorted and, for ESPP_IA_LJ, the Verlet list
+ *     built (after espp_decompose, espp_run or espp_energy); otherwise ESPP_ESTATE.
+ *   - The first call on a device looks up the array's device address with that device
+ *     current; make that first call before any stream capture on that device.
+ *   - All calls share the one array, which keeps the last call's contents; calls that
+ *     overlap on the GPU (two systems on different streams or threads) race. */
+ESPP_API int espp_energy_noalloc(espp_system* s, int32_t which, double* e);
+
 /* ---- measurement ---------------------------------------------------------------
  * No reference counterpart (the reference times phases with esutil::WallTimer,
  * VelocityVerlet.cpp:171-232).  With profiling on, run() brackets each phase with

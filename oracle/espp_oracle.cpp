@@ -1004,6 +1004,10 @@ int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n) {
   return ESPP_OK;
 }
 
+int espp_energy_noalloc(espp_system* s, int32_t which, double* e) {
+  return espp_energy(s, which, e);
+}
+
 int espp_set_profiling(espp_system* s, int32_t) {
   CHECK_S(s);
   return ESPP_OK;
