@@ -249,8 +249,13 @@ def gpu_arm(args, rank, world, local_rank):
             dist.all_reduce(t)
             torch.cuda.synchronize()
 
-    # warm-up (untimed)
+    # warm-up (untimed), then pick threads per particle for the force kernel
     call(lib, "espp_run", h, args.warmup)
+    tpp = ctypes.c_int32()
+    tune_ms = np.zeros(4)
+    call(lib, "espp_autotune", h, ctypes.byref(tpp), dptr(tune_ms))
+    log("rank %d: autotune tpp=%d (1,2,4,8 -> %s ms)" % (rank, tpp.value,
+                                                        np.round(tune_ms, 4).tolist()))
 
     # timed region: one run of K steps on the captured step-loop graph; CUDA events on
     # the library's stream around the step loop
@@ -264,8 +269,8 @@ def gpu_arm(args, rank, world, local_rank):
     clocks = sampler.stop()
     ms = np.zeros(2)
     call(lib, "espp_last_run_ms", h, dptr(ms))
-    ph_g = np.zeros(4)
-    launches = np.zeros(4, np.int64)
+    ph_g = np.zeros(8)
+    launches = np.zeros(8, np.int64)
     call(lib, "espp_profile", h, dptr(ph_g), i64ptr(launches))
     resorts = ctypes.c_int64()
     call(lib, "espp_num_resorts", h, ctypes.byref(resorts))
@@ -280,8 +285,8 @@ def gpu_arm(args, rank, world, local_rank):
     # bracketed by CUDA events on the library's stream (host-driven loop)
     call(lib, "espp_set_profiling", h, 1)
     call(lib, "espp_run", h, args.steps)
-    ph = np.zeros(4)
-    launches_p = np.zeros(4, np.int64)
+    ph = np.zeros(8)
+    launches_p = np.zeros(8, np.int64)
     call(lib, "espp_profile", h, dptr(ph), i64ptr(launches_p))
     call(lib, "espp_set_profiling", h, 0)
 
@@ -332,7 +337,9 @@ def gpu_arm(args, rank, world, local_rank):
                                                      args.precision),
                    "cell_grid": list(map(int, cg)), "l2": "inputs larger than L2 (262 MB)",
                    "parallelism": "replicas x%d" % world if world > 1 else "1 GPU",
-                   "resorts_in_timed_steps": int(resorts.value)},
+                   "resorts_in_timed_steps": int(resorts.value),
+                   "threads_per_particle": int(tpp.value),
+                   "autotune_force_ms": {str(c): float(t) for c, t in zip((1, 2, 4, 8), tune_ms)}},
         "roofline": {"kernel": "k_force_mixed" if prec else "k_force_fp64", "bound": "hbm",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": peak_kind,
@@ -341,8 +348,9 @@ def gpu_arm(args, rank, world, local_rank):
         "step_roofline": {"alg_bytes_per_particle_step": STEP_BYTES,
                           "achieved_gbs": STEP_BYTES * N / step_s / 1e9,
                           "frac": STEP_BYTES * N / step_s / 1e9 / hbm},
-        "profiled_pass_ms": {"force": ph[0], "integrate": ph[1], "rebuild": ph[2],
-                             "decide": ph[3], "launches": [int(x) for x in launches_p]},
+        "profiled_pass_ms": {"force": ph[0], "integrate": ph[1], "resort": ph[2],
+                             "decide": ph[3], "verlet_build": ph[4],
+                             "launches": [int(x) for x in launches_p[:5]]},
         "gpu_launches": int(launches.sum()),
         "clocks": clocks,
         "e2e": {"value": world * N * args.steps / e2e_s, "unit": "particle-steps/s",

@@ -52,6 +52,8 @@ PROTOTYPES = {
     "espp_profile": (c_int32, [_P, _D, _I64]),
     "espp_last_run_ms": (c_int32, [_P, _D]),
     "espp_select_device": (c_int32, [c_int32]),
+    "espp_set_tpp": (c_int32, [_P, c_int32]),
+    "espp_autotune": (c_int32, [_P, _I32, _D]),
 }
 
 # status codes (include/espp_b200.h)

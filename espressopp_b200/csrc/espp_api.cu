@@ -79,6 +79,7 @@ struct espp_system {
   int n = 0, cap = 0;
   ParticleArrays A{}, B{};
   int4* posq = nullptr;
+  float4* xrel = nullptr;
   int32_t* pcell = nullptr;
   int32_t* cellStart = nullptr;
   int32_t* nl = nullptr;
@@ -91,6 +92,7 @@ struct espp_system {
   RebuildScratch scr{};
   bool binned = false;
   bool listValid = false;
+  bool xrelFresh = false;  // xrel written by the last gather from the current positions
 
   // staging for by-id state transfers
   int stageCap = 0;
@@ -105,8 +107,8 @@ struct espp_system {
   std::vector<cudaEvent_t> evPool;
   size_t evUsed = 0;
   std::vector<std::pair<int, size_t>> evPhase;  // (phase, index of start event)
-  double phaseMs[4] = {0, 0, 0, 0};             // force, integrate, rebuild, other
-  long long phaseLaunches[4] = {0, 0, 0, 0};
+  double phaseMs[8] = {0};                      // force, integrate, re-sort, decide, list
+  long long phaseLaunches[8] = {0};
   cudaEvent_t runBeg = nullptr, runLoop = nullptr, runEnd = nullptr;
   double lastRunMs = 0.0, lastLoopMs = 0.0;
 
@@ -188,6 +190,7 @@ struct espp_system {
     }
     d.ncells = nc[0] * nc[1] * nc[2];
     d.posq = posq;
+    d.xrel = xrel;
     d.pcell = pcell;
     d.cellStart = cellStart;
     d.nl = nl;
@@ -302,6 +305,7 @@ void free_buffers(espp_system* s) {
   free_particles(s->A);
   free_particles(s->B);
   dfree(s->posq);
+  dfree(s->xrel);
   dfree(s->pcell);
   dfree(s->nl);
   dfree(s->nn);
@@ -326,6 +330,7 @@ void upload(espp_system* s, const HostParticles& h) {
     alloc_particles(s->A, cap);
     alloc_particles(s->B, cap);
     s->posq = dalloc<int4>(cap);
+    s->xrel = dalloc<float4>(cap);
     s->pcell = dalloc<int32_t>(cap);
     s->nn = dalloc<int32_t>(cap);
     s->nnZero = dalloc<int32_t>(cap);
@@ -455,6 +460,7 @@ void bin(espp_system* s, bool fold) {
   launch_sort_cells(d, s->scr, s->st);
   launch_gather(d, s->scr, s->st);  // gathers into pa[1] and swaps on the device
   s->paHostValid = false;
+  s->xrelFresh = true;
   launch_id_map(d, s->st);
   cuda_check(cudaGetLastError(), "re-binning kernels");
   s->binned = true;
@@ -480,6 +486,8 @@ void build_list(espp_system* s) {
     dfree(s->nl);
     s->nl = dalloc<int32_t>((size_t)s->K * s->cap);
   }
+  if (!s->xrelFresh) launch_xrel(s->view(), s->st);
+  s->xrelFresh = false;
   for (int attempt = 0; attempt < 6; ++attempt) {
     DevView d = s->view();
     launch_build_nl(d, cutsq, s->st);
@@ -552,7 +560,7 @@ double now_s() {
 }
 
 // ---- device-event phase timing ---------------------------------------------------
-enum { kPhForce = 0, kPhIntegrate = 1, kPhRebuild = 2, kPhOther = 3 };
+enum { kPhForce = 0, kPhIntegrate = 1, kPhRebuild = 2, kPhOther = 3, kPhList = 4, kNumPh = 8 };
 
 cudaEvent_t next_event(espp_system* s) {
   if (s->evUsed == s->evPool.size()) {
@@ -594,8 +602,13 @@ void collect_phases(espp_system* s) {
 
 // rebuild = fold/bin (fold_bin, scan, scatter, sort, gather, id map) + Verlet list
 void timed_decompose(espp_system* s) {
-  PhaseScope ps(s, kPhRebuild, 8 + (s->has_vl ? 1 : 0));
-  decompose(s);
+  {
+    PhaseScope ps(s, kPhRebuild, 10);
+    bin(s, true);
+  }
+  check_err(s);
+  PhaseScope ps(s, kPhList, s->has_vl ? 1 : 0);
+  build_list(s);
 }
 
 void timed_forces(espp_system* s) {
@@ -830,7 +843,7 @@ void run(espp_system* s, int64_t nsteps) {
       set_counters(s, before);
       s->step = step0;
       s->binned = false;
-      s->K = std::max(s->K * 2, K_high_water(s) + 32);
+      s->K = (std::max(s->K * 2, K_high_water(s) + 32) + 7) / 8 * 8;  // multiple of 8
       dfree(s->nl);
       s->nl = dalloc<int32_t>((size_t)s->K * s->cap);
       s->listValid = false;
@@ -855,7 +868,8 @@ void run(espp_system* s, int64_t nsteps) {
     s->phaseLaunches[kPhOther] += nsteps;
     s->phaseLaunches[kPhForce] += nsteps;
     s->phaseLaunches[kPhIntegrate] += nsteps;
-    s->phaseLaunches[kPhRebuild] += c.resorts * (8 + (s->has_vl ? 1 : 0));
+    s->phaseLaunches[kPhRebuild] += c.resorts * 10;
+    s->phaseLaunches[kPhList] += s->has_vl ? c.resorts : 0;
     s->paHostValid = false;
     graphDone = true;
   }
@@ -898,7 +912,7 @@ void run(espp_system* s, int64_t nsteps) {
   s->timers[0] = t1 - t0;
   s->timers[1] = s->phaseMs[kPhForce] * 1e-3;
   s->timers[6] = s->phaseMs[kPhIntegrate] * 1e-3;
-  s->timers[8] = graphDone ? s->phaseMs[kPhRebuild] * 1e-3 : tResort;
+  s->timers[8] = graphDone ? (s->phaseMs[kPhRebuild] + s->phaseMs[kPhList]) * 1e-3 : tResort;
   s->timers[9] = s->timers[0] - s->timers[1] - s->timers[6] - s->timers[8];
 }
 
@@ -970,6 +984,7 @@ void destroy(espp_system* s) {
   free_buffers(s);
   dfree(s->cellStart);
   dfree(s->scr.cellCount);
+  dfree(s->scr.tileSum);
   dfree(s->id2idx);
   dfree(s->bondStart);
   dfree(s->bondPartner);
@@ -1078,6 +1093,7 @@ int espp_system_create(const double box[3], double skin, const int32_t cell_grid
     if (ncells > (1LL << 30)) raise(ESPP_ERANGE, "cell grid too large");
     s->cellStart = dalloc<int32_t>(ncells + 1);
     s->scr.cellCount = dalloc<int32_t>(ncells);
+    s->scr.tileSum = dalloc<int32_t>(scan_tiles((int)ncells) + 1);
     cuda_check(cudaMemset(s->cellStart, 0, sizeof(int32_t) * (ncells + 1)), "memset");
     s->err = dalloc<unsigned>(1);
     s->ctr = dalloc<DevCounters>(1);
@@ -1088,6 +1104,10 @@ int espp_system_create(const double box[3], double skin, const int32_t cell_grid
     cuda_check(cudaMemset(s->d_pa, 0, 2 * sizeof(ParticleArrays)), "memset");
     cuda_check(cudaMallocHost(&s->hctr, sizeof(DevCounters)), "pinned counters");
     if (const char* g = std::getenv("ESPP_B200_GRAPH")) s->useGraph = std::atoi(g) != 0;
+    if (const char* t = std::getenv("ESPP_B200_TPP")) {
+      const int v = std::atoi(t);
+      if (v == 1 || v == 2 || v == 4 || v == 8) s->tpp = v;
+    }
     s->lj.ntypes = 1;
     upload_lj(s.get());
     *out = s.release();
@@ -1248,17 +1268,17 @@ int espp_set_particles(espp_system* s, int64_t n, const int64_t* ids, const doub
 int espp_set_profiling(espp_system* s, int32_t on) {
   return guard([&] {
     checked(s)->profiling = on != 0;
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < kNumPh; ++k) {
       s->phaseMs[k] = 0.0;
       s->phaseLaunches[k] = 0;
     }
   });
 }
 
-int espp_profile(espp_system* s, double ms[4], int64_t launches[4]) {
+int espp_profile(espp_system* s, double ms[8], int64_t launches[8]) {
   return guard([&] {
     checked(s);
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < kNumPh; ++k) {
       if (ms) ms[k] = s->phaseMs[k];
       if (launches) launches[k] = s->phaseLaunches[k];
     }
@@ -1539,6 +1559,52 @@ int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n) {
     cuda_check(cudaMemcpyAsync(sum_mv2, s->obs, sizeof(double), cudaMemcpyDeviceToHost, s->st),
                "download");
     sync(s);
+  });
+}
+
+int espp_set_tpp(espp_system* s, int32_t tpp) {
+  return guard([&] {
+    checked(s);
+    if (tpp != 1 && tpp != 2 && tpp != 4 && tpp != 8)
+      raise(ESPP_EINVAL, "threads per particle must be 1, 2, 4 or 8");
+    s->tpp = tpp;
+  });
+}
+
+int espp_autotune(espp_system* s, int32_t* best_tpp, double ms[4]) {
+  return guard([&] {
+    checked(s);
+    if (s->idDirty) rebuild_id_tables(s);
+    if (!s->binned) bin(s, false);
+    if (s->has_vl && !s->listValid) build_list(s);
+    const int cand[4] = {1, 2, 4, 8};
+    const int old = s->tpp;
+    cudaEvent_t e0, e1;
+    cuda_check(cudaEventCreate(&e0), "event");
+    cuda_check(cudaEventCreate(&e1), "event");
+    double best = 1e300;
+    int pick = old;
+    for (int c = 0; c < 4; ++c) {
+      s->tpp = cand[c];
+      launch_force_kernel(s, s->st);  // warm
+      cuda_check(cudaEventRecord(e0, s->st), "event");
+      for (int r = 0; r < 3; ++r) launch_force_kernel(s, s->st);
+      cuda_check(cudaEventRecord(e1, s->st), "event");
+      sync(s);
+      float t = 0.f;
+      cuda_check(cudaEventElapsedTime(&t, e0, e1), "event time");
+      if (ms) ms[c] = t / 3.0;
+      if (t < best) {
+        best = t;
+        pick = cand[c];
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cuda_check(cudaGetLastError(), "autotune");
+    check_err(s);
+    s->tpp = pick;
+    if (best_tpp) *best_tpp = pick;
   });
 }
 

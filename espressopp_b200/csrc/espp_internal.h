@@ -83,6 +83,7 @@ struct DevView {
   double fixScale[3];     // 2^32 / L_d   (double -> box-wrapped int32)
   float fixUnit[3];       // L_d / 2^32   (int32 difference -> float length)
   int4* posq;             // box-wrapped int32 coordinates + type
+  float4* xrel;           // FP32 position relative to its cell origin at the last re-sort
   int32_t* pcell;         // reference cell of each sorted particle
   int32_t* cellStart;     // ncells + 1
   int32_t* nl;            // K * cap, entry (k, i) at nl[k * cap + i]
@@ -113,6 +114,7 @@ struct RebuildScratch {
   int32_t* slot;      // cap: arrival slot inside its cell
   int32_t* cellCount; // ncells
   int32_t* perm;      // cap: sorted position -> old row
+  int32_t* tileSum;   // scan_tiles(ncells): per-tile sums / offsets of the cell scan
 };
 
 // launchers (espp_kernels.cu)
@@ -122,6 +124,7 @@ void launch_gather(const DevView& d, const RebuildScratch& s, cudaStream_t st);
 void launch_id_map(const DevView& d, cudaStream_t st);
 void launch_build_nl(const DevView& d, double cutsq, cudaStream_t st);
 void launch_posq(const DevView& d, cudaStream_t st);
+void launch_xrel(const DevView& d, cudaStream_t st);
 void launch_forces(const DevView& d, bool mixed, const FENEParams& fene, int tpp,
                    cudaStream_t st);
 struct IntegrateArgs {
@@ -155,6 +158,7 @@ void launch_bond_maxsq(const DevView& d, double* partials, int nblocks, double* 
 // float copy of an LJ table for the mixed-precision kernel
 void make_float_table(const LJTable& t, LJPairF* out);
 int observable_blocks(int n);
+int scan_tiles(int ncells);
 void launch_set_by_id(const DevView& d, int n, const int64_t* ids, const double* pos,
                       const double* vel, cudaStream_t st);
 void launch_get_by_id(const DevView& d, int n, const int64_t* ids, double* pos, double* vel,

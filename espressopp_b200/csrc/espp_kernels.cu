@@ -126,29 +126,85 @@ __global__ void k_fold_bin(DevView d, RebuildScratch s, int fold) {
   s.slot[i] = atomicAdd(&s.cellCount[cell], 1);
 }
 
-// Exclusive scan of the cell counts into cellStart (one block).
-__global__ void k_scan_cells(const int32_t* __restrict__ count, int32_t* __restrict__ start,
-                             int ncells) {
-  __shared__ int32_t sums[1024];
-  int t = threadIdx.x;
-  int chunk = (ncells + blockDim.x - 1) / blockDim.x;
-  int b = t * chunk, e = min(ncells, b + chunk);
-  int acc = 0;
-  for (int c = b; c < e; ++c) acc += count[c];
-  sums[t] = acc;
+// Exclusive scan of the cell counts into cellStart, in three passes: block sums, a
+// scan of the block sums (one block), then each block's scan plus its offset.
+constexpr int kScanBlock = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanBlock * kScanItems;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* sm, int& total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += t;
+  }
+  if (lane == 31) sm[w] = x;
   __syncthreads();
-  for (int off = 1; off < (int)blockDim.x; off <<= 1) {
-    int v = t >= off ? sums[t - off] : 0;
-    __syncthreads();
-    sums[t] += v;
-    __syncthreads();
+  if (w == 0) {
+    int y = lane < (int)(blockDim.x >> 5) ? sm[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, y, o);
+      if (lane >= o) y += t;
+    }
+    sm[lane] = y;
   }
-  int run = sums[t] - acc;
-  for (int c = b; c < e; ++c) {
-    start[c] = run;
-    run += count[c];
+  __syncthreads();
+  total = sm[(blockDim.x >> 5) - 1];
+  const int excl = x - v + (w > 0 ? sm[w - 1] : 0);
+  __syncthreads();
+  return excl;
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_scan_tiles(const int32_t* __restrict__ count,
+                                                            int n, int32_t* __restrict__ tile_sum) {
+  __shared__ int sm[32];
+  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  int v = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) v += (base + k < n) ? count[base + k] : 0;
+  int total;
+  block_exclusive_scan(v, sm, total);
+  if (threadIdx.x == 0) tile_sum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_scan_tile_sums(int32_t* __restrict__ tile_sum,
+                                                                int ntiles) {
+  __shared__ int sm[32];
+  int carry = 0;
+  for (int b = 0; b < ntiles; b += kScanBlock) {
+    const int t = b + (int)threadIdx.x;
+    const int v = t < ntiles ? tile_sum[t] : 0;
+    int total;
+    const int e = block_exclusive_scan(v, sm, total);
+    if (t < ntiles) tile_sum[t] = carry + e;
+    carry += total;
   }
-  if (t == blockDim.x - 1) start[ncells] = sums[t];
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_scan_apply(const int32_t* __restrict__ count,
+                                                            int n,
+                                                            const int32_t* __restrict__ tile_off,
+                                                            int32_t* __restrict__ start) {
+  __shared__ int sm[32];
+  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  int c[kScanItems];
+  int v = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    c[k] = (base + k < n) ? count[base + k] : 0;
+    v += c[k];
+  }
+  int total;
+  int run = block_exclusive_scan(v, sm, total) + tile_off[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (base + k < n) start[base + k] = run;
+    run += c[k];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) start[n] = run;
 }
 
 __global__ void k_scatter(DevView d, RebuildScratch s) {
@@ -158,21 +214,40 @@ __global__ void k_scatter(DevView d, RebuildScratch s) {
 }
 
 // Order inside a cell: by particle id, so the layout is independent of the atomic
-// arrival order above.
+// arrival order above.  One warp per cell: each lane takes one particle and its rank
+// among the cell's ids is its new slot (cells with more than 32 particles are sorted
+// by insertion on lane 0).
 __global__ void k_sort_in_cell(DevView d, RebuildScratch s) {
   const ParticleArrays a = d.pa[0];
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (c >= d.ncells) return;
-  int b = d.cellStart[c], e = d.cellStart[c + 1];
-  for (int k = b + 1; k < e; ++k) {
-    int v = s.perm[k];
-    int64_t key = a.id[v];
-    int m = k - 1;
-    while (m >= b && a.id[s.perm[m]] > key) {
-      s.perm[m + 1] = s.perm[m];
-      --m;
+  const int b = d.cellStart[c], e = d.cellStart[c + 1];
+  const int n = e - b;
+  if (n <= 1) return;
+  if (n <= 32) {
+    const int v = lane < n ? s.perm[b + lane] : 0;
+    const int64_t key = lane < n ? a.id[v] : INT64_MAX;
+    int rank = 0;
+    for (int m = 0; m < n; ++m) {
+      const int64_t km = __shfl_sync(0xffffffffu, key, m);
+      rank += km < key;
     }
-    s.perm[m + 1] = v;
+    __syncwarp();
+    if (lane < n) s.perm[b + rank] = v;
+    return;
+  }
+  if (lane == 0) {
+    for (int k = b + 1; k < e; ++k) {
+      const int v = s.perm[k];
+      const int64_t key = a.id[v];
+      int m = k - 1;
+      while (m >= b && a.id[s.perm[m]] > key) {
+        s.perm[m + 1] = s.perm[m];
+        --m;
+      }
+      s.perm[m + 1] = v;
+    }
   }
 }
 
@@ -193,8 +268,12 @@ __global__ void k_gather(DevView d, RebuildScratch s) {
   dst.id[k] = src.id[o];
   dst.type[k] = ty;
   dst.mass[k] = src.mass[o];
-  d.pcell[k] = s.cellOf[o];
+  const int cell = s.cellOf[o];
+  d.pcell[k] = cell;
   d.posq[k] = fixed_coords(d, p[0], p[1], p[2], ty);
+  const int cx = cell % d.nc[0], cy = (cell / d.nc[0]) % d.nc[1], cz = cell / (d.nc[0] * d.nc[1]);
+  d.xrel[k] = make_float4((float)(p[0] - cx * d.cellSize[0]), (float)(p[1] - cy * d.cellSize[1]),
+                          (float)(p[2] - cz * d.cellSize[2]), 0.f);
 }
 
 __global__ void k_id_map(DevView d) {
@@ -217,6 +296,19 @@ __global__ void k_posq(DevView d) {
                            a.type[k]);
 }
 
+// Cell-relative FP32 positions from the current coordinates and the cells of the last
+// re-sort (a Verlet rebuild without re-binning, VerletList::rebuild on stale cells).
+__global__ void k_xrel(DevView d) {
+  const ParticleArrays a = d.pa[0];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.n) return;
+  const int cell = d.pcell[k];
+  const int cx = cell % d.nc[0], cy = (cell / d.nc[0]) % d.nc[1], cz = cell / (d.nc[0] * d.nc[1]);
+  d.xrel[k] = make_float4((float)(a.x[k] - cx * d.cellSize[0]),
+                          (float)(a.x[(size_t)d.cap + k] - cy * d.cellSize[1]),
+                          (float)(a.x[2 * (size_t)d.cap + k] - cz * d.cellSize[2]), 0.f);
+}
+
 // ---- Verlet list -------------------------------------------------------------------
 
 __device__ __forceinline__ bool is_excluded(const DevView& d, int64_t a, int64_t b) {
@@ -228,77 +320,189 @@ __device__ __forceinline__ bool is_excluded(const DevView& d, int64_t a, int64_t
   return false;
 }
 
-// One warp per cell; lanes own the cell's particles (32 at a time).  Candidates are
-// the 27 cells of the reference's neighbour stencil; the inclusion test is the
-// reference's d = p1 - (p2 + shift), d.sqr() <= cutsq in FP64 without contraction,
-// where p1 is the particle of the backward cell and shift is the ghost image offset
-// of the forward cell (VerletList.cpp:399-426, DomainDecomposition.cpp:1347-1391).
-__global__ void k_build_nl(DevView d, double cutsq) {
+// The reference's FP64 inclusion test for one candidate pair (rarely reached: only
+// candidates whose FP32 distance lies within the 2e-5 band around the cutoff).
+__device__ __noinline__ bool exact_pair_test(const double* __restrict__ x, size_t cap, int i,
+                                             int j, bool fwd, double sx, double sy, double sz,
+                                             double cutsq) {
+  const double xi = x[i], yi = x[cap + i], zi = x[2 * cap + i];
+  const double xj = x[j], yj = x[cap + j], zj = x[2 * cap + j];
+  double ex, ey, ez;
+  if (fwd) {  // p1 = i, p2 = ghost of j at xj + s
+    ex = __dsub_rn(xi, __dadd_rn(xj, sx));
+    ey = __dsub_rn(yi, __dadd_rn(yj, sy));
+    ez = __dsub_rn(zi, __dadd_rn(zj, sz));
+  } else {  // p1 = j, p2 = ghost of i at xi - s
+    ex = __dsub_rn(xj, __dadd_rn(xi, -sx));
+    ey = __dsub_rn(yj, __dadd_rn(yi, -sy));
+    ez = __dsub_rn(zj, __dadd_rn(zi, -sz));
+  }
+  const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+  return !(d2 > cutsq);
+}
+
+// One warp per cell, in two phases per group of up to 32 particles of the cell.
+//  A: the lanes hold candidates: for each of the 9 rows (oy, oz) of the reference's
+//     27-cell stencil, the particles of the row's three x-cells are taken 32 at a time
+//     (one "chunk"), and every particle i of the group is tested against the whole chunk
+//     in FP32 on cell-relative coordinates.  One ballot per (i, chunk) gives a 32-bit
+//     mask of the candidates inside the cutoff, a second one the candidates within a
+//     relative band of 2e-5 around it; both go to shared memory.
+//  B: the lanes hold the group's particles: each lane walks its masks in chunk order,
+//     settles borderline bits with the reference's own FP64 arithmetic (exact_pair_test)
+//     and appends the partners in bit order.
+// Each list is therefore the reference's pair set (VerletList.cpp:274-450) in a
+// deterministic order (row, chunk, lane).
+constexpr int kMaxChunks = 24;  // chunks per batch of the two phases
+
+template <bool EXCL>
+__global__ void __launch_bounds__(128) k_build_nl(DevView d, double cutsq) {
   const ParticleArrays a = d.pa[0];
-  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
+  __shared__ float4 s_xi[4][32];
+  __shared__ unsigned s_in[4][kMaxChunks][32];
+  __shared__ unsigned s_bd[4][kMaxChunks][32];
+  __shared__ int s_row[4][9][8];  // st0, ct0, st1, ct1, st2, ct2, first chunk, chunks
+  const int wib = threadIdx.x >> 5;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (warp >= d.ncells) return;
   const int c = warp;
   const int cx = c % d.nc[0], cy = (c / d.nc[0]) % d.nc[1], cz = c / (d.nc[0] * d.nc[1]);
   const int s0 = d.cellStart[c], s1 = d.cellStart[c + 1];
-  const double* X = a.x;
-  const double* Y = a.x + d.cap;
-  const double* Z = a.x + 2 * (size_t)d.cap;
-  for (int base = s0; base < s1; base += 32) {
-    const int i = base + lane;
-    const bool act = i < s1;
-    double xi = 0, yi = 0, zi = 0;
-    int64_t idi = 0;
-    if (act) {
-      xi = X[i];
-      yi = Y[i];
-      zi = Z[i];
-      idi = a.id[i];
+  if (s0 == s1) return;
+  const float lo = (float)(cutsq * (1.0 - 2e-5)), hi = (float)(cutsq * (1.0 + 2e-5));
+  const float hx = (float)d.cellSize[0], hy = (float)d.cellSize[1], hz = (float)d.cellSize[2];
+  const float4* __restrict__ xr = d.xrel;
+  const int cxm = cx == 0 ? d.nc[0] - 1 : cx - 1;
+  const int cxp = cx == d.nc[0] - 1 ? 0 : cx + 1;
+  // the 9 rows of the stencil: three x-cells each, as (start, count) segments
+  if (lane < 9) {
+    const int oz = lane / 3 - 1, oy = lane % 3 - 1;
+    int ncy = cy + oy, ncz = cz + oz;
+    ncy += ncy < 0 ? d.nc[1] : (ncy >= d.nc[1] ? -d.nc[1] : 0);
+    ncz += ncz < 0 ? d.nc[2] : (ncz >= d.nc[2] ? -d.nc[2] : 0);
+    const int rb = d.nc[0] * (ncy + d.nc[1] * ncz);
+    const int st0 = d.cellStart[rb + cxm], st1 = d.cellStart[rb + cx], st2 = d.cellStart[rb + cxp];
+    const int ct0 = d.cellStart[rb + cxm + 1] - st0, ct1 = d.cellStart[rb + cx + 1] - st1;
+    const int ct2 = d.cellStart[rb + cxp + 1] - st2;
+    s_row[wib][lane][0] = st0;
+    s_row[wib][lane][1] = ct0;
+    s_row[wib][lane][2] = st1;
+    s_row[wib][lane][3] = ct1;
+    s_row[wib][lane][4] = st2;
+    s_row[wib][lane][5] = ct2;
+    s_row[wib][lane][7] = (ct0 + ct1 + ct2 + 31) >> 5;
+  }
+  __syncwarp();
+  int nchunks = 0;
+  if (lane == 0)
+    for (int r = 0; r < 9; ++r) {
+      s_row[wib][r][6] = nchunks;
+      nchunks += s_row[wib][r][7];
     }
+  nchunks = __shfl_sync(0xffffffffu, nchunks, 0);
+  __syncwarp();
+  for (int g = s0; g < s1; g += 32) {
+    const int ni = min(32, s1 - g);
+    if (lane < ni) s_xi[wib][lane] = xr[g + lane];
+    const int i = g + lane;
+    const int64_t idi = (EXCL && lane < ni) ? a.id[i] : 0;
     int cnt = 0;
-    for (int oz = -1; oz <= 1; ++oz)
-      for (int oy = -1; oy <= 1; ++oy)
-        for (int ox = -1; ox <= 1; ++ox) {
-          int ncx = cx + ox, ncy = cy + oy, ncz = cz + oz;
-          int wx = ncx < 0 ? -1 : (ncx >= d.nc[0] ? 1 : 0);
-          int wy = ncy < 0 ? -1 : (ncy >= d.nc[1] ? 1 : 0);
-          int wz = ncz < 0 ? -1 : (ncz >= d.nc[2] ? 1 : 0);
-          ncx -= wx * d.nc[0];
-          ncy -= wy * d.nc[1];
-          ncz -= wz * d.nc[2];
-          const int nb = ncx + d.nc[0] * (ncy + d.nc[1] * ncz);
-          const bool fwd = oz > 0 || (oz == 0 && (oy > 0 || (oy == 0 && ox > 0)));
-          // shift of the forward particle's ghost image
-          const double sx = wx * d.L[0], sy = wy * d.L[1], sz = wz * d.L[2];
-          const int j0 = d.cellStart[nb], j1 = d.cellStart[nb + 1];
-          for (int j = j0; j < j1; ++j) {
-            const double xj = X[j], yj = Y[j], zj = Z[j];
-            double dx, dy, dz;
-            if (fwd) {  // p1 = i, p2 = ghost of j at xj + s
-              dx = __dsub_rn(xi, __dadd_rn(xj, sx));
-              dy = __dsub_rn(yi, __dadd_rn(yj, sy));
-              dz = __dsub_rn(zi, __dadd_rn(zj, sz));
-            } else {  // p1 = j, p2 = ghost of i at xi - s
-              dx = __dsub_rn(xj, __dadd_rn(xi, -sx));
-              dy = __dsub_rn(yj, __dadd_rn(yi, -sy));
-              dz = __dsub_rn(zj, __dadd_rn(zi, -sz));
-            }
-            const double d2 =
-                __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-            if (act && j != i && !(d2 > cutsq)) {
-              if (!is_excluded(d, idi, a.id[j])) {
-                if (cnt < d.K) d.nl[(size_t)cnt * d.cap + i] = j;
-                ++cnt;
-              }
-            }
+    int* out = d.nl + i;
+    const size_t stride = d.cap;
+    __syncwarp();
+    int r = 0;  // row of the first chunk of the batch
+    for (int qb = 0; qb < nchunks; qb += kMaxChunks) {
+      const int nq = min(kMaxChunks, nchunks - qb);
+      // ---- phase A: masks for chunks qb .. qb + nq
+      int rr = r;
+      for (int q = 0; q < nq; ++q) {
+        while (qb + q >= s_row[wib][rr][6] + s_row[wib][rr][7]) ++rr;
+        const int cb = (qb + q - s_row[wib][rr][6]) << 5;
+        const int oz = rr / 3 - 1, oy = rr % 3 - 1;
+        const int st0 = s_row[wib][rr][0], ct0 = s_row[wib][rr][1];
+        const int st1 = s_row[wib][rr][2], ct1 = s_row[wib][rr][3];
+        const int st2 = s_row[wib][rr][4], ct2 = s_row[wib][rr][5];
+        const int t = cb + lane;
+        const bool validj = t < ct0 + ct1 + ct2;
+        const int seg = t < ct0 ? 0 : (t < ct0 + ct1 ? 1 : 2);
+        const int j = !validj ? -1 : (seg == 0 ? st0 + t : (seg == 1 ? st1 + t - ct0 : st2 + t - ct0 - ct1));
+        float4 rj = validj ? xr[j] : make_float4(1e30f, 1e30f, 1e30f, 0.f);
+        rj.x += (seg - 1) * hx;
+        rj.y += oy * hy;
+        rj.z += oz * hz;
+        for (int m = 0; m < ni; ++m) {
+          const float4 ri = s_xi[wib][m];
+          const float dx = ri.x - rj.x, dy = ri.y - rj.y, dz = ri.z - rj.z;
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          const bool self = j == g + m;
+          const unsigned bin = __ballot_sync(0xffffffffu, r2 < lo && !self);
+          const unsigned bbd = __ballot_sync(0xffffffffu, r2 >= lo && r2 <= hi && !self);
+          if (lane == m) {
+            s_in[wib][q][m] = bin;
+            s_bd[wib][q][m] = bbd;
           }
         }
-    if (act) {
-      if (cnt > d.K) atomicOr(d.err, kErrNlOverflow);
-      d.nn[i] = min(cnt, d.K);
+      }
+      __syncwarp();
+      // ---- phase B: each lane appends its partners of these chunks in bit order
+      if (lane < ni) {
+        rr = r;
+        for (int q = 0; q < nq; ++q) {
+          while (qb + q >= s_row[wib][rr][6] + s_row[wib][rr][7]) ++rr;
+          unsigned m_in = s_in[wib][q][lane];
+          const unsigned m_bd = s_bd[wib][q][lane];
+          if (!(m_in | m_bd)) continue;
+          const int cb = (qb + q - s_row[wib][rr][6]) << 5;
+          const int st0 = s_row[wib][rr][0], ct0 = s_row[wib][rr][1];
+          const int st1 = s_row[wib][rr][2], ct1 = s_row[wib][rr][3];
+          const int st2 = s_row[wib][rr][4];
+          if (__builtin_expect(m_bd != 0u, 0)) {
+            const int oz = rr / 3 - 1, oy = rr % 3 - 1;
+            const int ncy = cy + oy, ncz = cz + oz;
+            const int wy = ncy < 0 ? -1 : (ncy >= d.nc[1] ? 1 : 0);
+            const int wz = ncz < 0 ? -1 : (ncz >= d.nc[2] ? 1 : 0);
+            unsigned b = m_bd;
+            while (b) {
+              const int bit = __ffs(b) - 1;
+              b &= b - 1;
+              const int t = cb + bit;
+              const int seg = t < ct0 ? 0 : (t < ct0 + ct1 ? 1 : 2);
+              const int ox = seg - 1;
+              const int j = seg == 0 ? st0 + t : (seg == 1 ? st1 + t - ct0 : st2 + t - ct0 - ct1);
+              const int wx = seg == 0 ? (cx == 0 ? -1 : 0) : (seg == 2 ? (cx == d.nc[0] - 1 ? 1 : 0) : 0);
+              const bool fwd = oz > 0 || (oz == 0 && (oy > 0 || (oy == 0 && ox > 0)));
+              if (exact_pair_test(a.x, d.cap, i, j, fwd, wx * d.L[0], wy * d.L[1], wz * d.L[2],
+                                  cutsq))
+                m_in |= 1u << bit;
+            }
+          }
+          while (m_in) {
+            const int bit = __ffs(m_in) - 1;
+            m_in &= m_in - 1;
+            const int t = cb + bit;
+            const int j = t < ct0 ? st0 + t : (t < ct0 + ct1 ? st1 + t - ct0 : st2 + t - ct0 - ct1);
+            if (EXCL && is_excluded(d, idi, a.id[j])) continue;
+            if (cnt < d.K) *out = j;
+            out += stride;
+            ++cnt;
+          }
+        }
+      }
+      r = rr;
+      __syncwarp();
     }
-    const int wmax = __reduce_max_sync(0xffffffffu, act ? cnt : 0);
+    if (lane < ni) {
+      if (cnt > d.K) atomicOr(d.err, kErrNlOverflow);
+      const int cc = min(cnt, d.K);
+      d.nn[i] = cc;
+      // pad to a multiple of 8 with the particle itself (r^2 = 0, masked by the force
+      // kernels) so that batches of 8 need no bounds checks; K is a multiple of 8
+      for (int k = cc; k < ((cc + 7) & ~7); ++k) d.nl[(size_t)k * stride + i] = i;
+    }
+    const int wmax = __reduce_max_sync(0xffffffffu, lane < ni ? cnt : 0);
     if (lane == 0 && wmax > 0) atomicMax(&d.ctr->nnMax, wmax);
+    __syncwarp();
   }
 }
 
@@ -335,23 +539,94 @@ __global__ void __launch_bounds__(256) k_force_mixed(DevView d, FENEParams fp) {
   float fx = 0.f, fy = 0.f, fz = 0.f;
   LJPairF P = d.ljf[0];
   const int ntypes = d.ntypes;
-  const int* __restrict__ nl = d.nl;
-  for (int k = sub; k < cnt; k += TPP) {
-    const int j = __ldg(&nl[(size_t)k * d.cap + i]);
-    const int4 pj = __ldg(&d.posq[j]);
-    const float dx = wrapped_diff(pi.x, pj.x, ux);
-    const float dy = wrapped_diff(pi.y, pj.y, uy);
-    const float dz = wrapped_diff(pi.z, pj.z, uz);
-    const float r2 = dx * dx + dy * dy + dz * dz;
-    if (!SINGLE) P = sP[pi.w * ntypes + pj.w];
-    const float ri2 = fast_rcp(r2);
-    const float ri6 = ri2 * ri2 * ri2;
-    float ff = ri6 * (P.ff1 * ri6 - P.ff2) * ri2;
-    if (CAPPED && r2 <= P.capsq) ff = P.capff * rsqrtf(r2);
-    ff = (r2 <= P.rcsq) ? ff : 0.f;
-    fx += dx * ff;
-    fy += dy * ff;
-    fz += dz * ff;
+  const int* __restrict__ nl = d.nl + i;
+  const size_t cap = d.cap;
+  constexpr int U = 8;
+  if (TPP == 1) {
+    // Lists are padded to a multiple of 8 with the particle itself (r^2 = 0, masked), so
+    // each batch of 8 entries is read without bounds checks.  The next batch's entries
+    // are loaded before the current batch's coordinates are used, so list loads,
+    // coordinate gathers and arithmetic overlap; the sum order is the list order.
+    const int padded = (cnt + 7) & ~7;
+    const size_t stride = cap;
+    const int* q = nl;
+    int jn[U];
+    if (padded > 0) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) jn[u] = __ldcs(q + u * stride);
+    }
+    for (int k = 0; k < padded; k += U) {
+      int4 pj[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) pj[u] = __ldg(&d.posq[jn[u]]);
+      q += U * stride;
+      if (k + U < padded) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) jn[u] = __ldcs(q + u * stride);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const float dx = wrapped_diff(pi.x, pj[u].x, ux);
+        const float dy = wrapped_diff(pi.y, pj[u].y, uy);
+        const float dz = wrapped_diff(pi.z, pj[u].z, uz);
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (!SINGLE) P = sP[pi.w * ntypes + pj[u].w];
+        const float ri2 = fast_rcp(r2);
+        const float ri6 = ri2 * ri2 * ri2;
+        float ff = ri6 * (P.ff1 * ri6 - P.ff2) * ri2;
+        if (CAPPED && r2 <= P.capsq) ff = P.capff * rsqrtf(r2);
+        ff = (r2 > 0.f && r2 <= P.rcsq) ? ff : 0.f;
+        fx += dx * ff;
+        fy += dy * ff;
+        fz += dz * ff;
+      }
+    }
+  } else {
+    // Entries (k, i) are read as a stream (evict-first) in batches of U per thread; the
+    // next batch's entries are loaded before the current batch's coordinates are used, so
+    // list loads, coordinate gathers and arithmetic overlap.  Slots past the end of the
+    // list read the particle itself and are masked out, so every batch has the same shape
+    // and the sum order is the list order.
+    int jn[U];
+  #pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int kk = sub + u * TPP;
+      jn[u] = kk < cnt ? __ldcs(nl + (size_t)kk * cap) : i;
+    }
+    for (int k = sub; k < cnt; k += U * TPP) {
+      int j[U];
+      bool valid[U];
+  #pragma unroll
+      for (int u = 0; u < U; ++u) {
+        j[u] = jn[u];
+        valid[u] = k + u * TPP < cnt;
+      }
+      int4 pj[U];
+  #pragma unroll
+      for (int u = 0; u < U; ++u) pj[u] = __ldg(&d.posq[j[u]]);
+      const int kn = k + U * TPP;
+  #pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int kk = kn + u * TPP;
+        jn[u] = kk < cnt ? __ldcs(nl + (size_t)kk * cap) : i;
+      }
+  #pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const float dx = wrapped_diff(pi.x, pj[u].x, ux);
+        const float dy = wrapped_diff(pi.y, pj[u].y, uy);
+        const float dz = wrapped_diff(pi.z, pj[u].z, uz);
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (!SINGLE) P = sP[pi.w * ntypes + pj[u].w];
+        const float ri2 = fast_rcp(r2);
+        const float ri6 = ri2 * ri2 * ri2;
+        float ff = ri6 * (P.ff1 * ri6 - P.ff2) * ri2;
+        if (CAPPED && r2 <= P.capsq) ff = P.capff * rsqrtf(r2);
+        ff = (valid[u] && r2 <= P.rcsq) ? ff : 0.f;
+        fx += dx * ff;
+        fy += dy * ff;
+        fz += dz * ff;
+      }
+    }
   }
   long long Fx = to_fix(fx, d.err), Fy = to_fix(fy, d.err), Fz = to_fix(fz, d.err);
   if (FENE && sub == 0 && act) {
@@ -429,14 +704,15 @@ __global__ void __launch_bounds__(256) k_force_fp64(DevView d, FENEParams fp) {
   const int cnt = act ? d.nn[i] : 0;
   double fx = 0, fy = 0, fz = 0;
   const int ntypes = d.ntypes;
-  for (int k = sub; k < cnt; k += TPP) {
-    const int j = __ldg(&d.nl[(size_t)k * d.cap + i]);
-    const double dx = min_image(xi - __ldg(&X[j]), d.L[0], d.halfL[0]);
-    const double dy = min_image(yi - __ldg(&Y[j]), d.L[1], d.halfL[1]);
-    const double dz = min_image(zi - __ldg(&Z[j]), d.L[2], d.halfL[2]);
+  const int* __restrict__ nl = d.nl + i;
+  const size_t cap = d.cap;
+  auto pair = [&](int j, double xj, double yj, double zj) {
+    const double dx = min_image(xi - xj, d.L[0], d.halfL[0]);
+    const double dy = min_image(yi - yj, d.L[1], d.halfL[1]);
+    const double dz = min_image(zi - zj, d.L[2], d.halfL[2]);
     const double r2 = dx * dx + dy * dy + dz * dz;
     const LJPair& P = SINGLE ? d.lj[0] : d.lj[ti * ntypes + __ldg(&a.type[j])];
-    if (!P.set || r2 > P.rcsq) continue;
+    if (!P.set || r2 > P.rcsq) return;
     double ff;
     if (CAPPED && P.caprad > 0 && !(r2 > P.caprad * P.caprad)) {
       ff = P.capff / sqrt(r2);
@@ -448,6 +724,26 @@ __global__ void __launch_bounds__(256) k_force_fp64(DevView d, FENEParams fp) {
     fx += dx * ff;
     fy += dy * ff;
     fz += dz * ff;
+  };
+  constexpr int U = 4;
+  int k = sub;
+  for (; k + (U - 1) * TPP < cnt; k += U * TPP) {
+    int j[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) j[u] = __ldcs(nl + (size_t)(k + u * TPP) * cap);
+    double xj[U], yj[U], zj[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      xj[u] = __ldg(&X[j[u]]);
+      yj[u] = __ldg(&Y[j[u]]);
+      zj[u] = __ldg(&Z[j[u]]);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) pair(j[u], xj[u], yj[u], zj[u]);
+  }
+  for (; k < cnt; k += TPP) {
+    const int j = __ldcs(nl + (size_t)k * cap);
+    pair(j, __ldg(&X[j]), __ldg(&Y[j]), __ldg(&Z[j]));
   }
   if (FENE && sub == 0 && act) {
     const int64_t off = a.id[i] - d.idMin;
@@ -907,10 +1203,15 @@ void launch_fold_bin(const DevView& d, RebuildScratch& s, bool fold, cudaStream_
 }
 
 void launch_sort_cells(const DevView& d, RebuildScratch& s, cudaStream_t st) {
-  k_scan_cells<<<1, 1024, 0, st>>>(s.cellCount, d.cellStart, d.ncells);
+  const int ntiles = (d.ncells + kScanTile - 1) / kScanTile;
+  k_scan_tiles<<<ntiles, kScanBlock, 0, st>>>(s.cellCount, d.ncells, s.tileSum);
+  k_scan_tile_sums<<<1, kScanBlock, 0, st>>>(s.tileSum, ntiles);
+  k_scan_apply<<<ntiles, kScanBlock, 0, st>>>(s.cellCount, d.ncells, s.tileSum, d.cellStart);
   if (d.n > 0) k_scatter<<<blocks_for(d.n), kBlock, 0, st>>>(d, s);
-  k_sort_in_cell<<<blocks_for(d.ncells), kBlock, 0, st>>>(d, s);
+  k_sort_in_cell<<<blocks_for((long long)d.ncells * 32), kBlock, 0, st>>>(d, s);
 }
+
+int scan_tiles(int ncells) { return (ncells + kScanTile - 1) / kScanTile; }
 
 void launch_gather(const DevView& d, const RebuildScratch& s, cudaStream_t st) {
   if (d.n > 0) k_gather<<<blocks_for(d.n), kBlock, 0, st>>>(d, s);
@@ -921,13 +1222,20 @@ void launch_id_map(const DevView& d, cudaStream_t st) {
   if (d.n > 0) k_id_map<<<blocks_for(d.n), kBlock, 0, st>>>(d);
 }
 
+void launch_xrel(const DevView& d, cudaStream_t st) {
+  if (d.n > 0) k_xrel<<<blocks_for(d.n), kBlock, 0, st>>>(d);
+}
+
 void launch_posq(const DevView& d, cudaStream_t st) {
   if (d.n > 0) k_posq<<<blocks_for(d.n), kBlock, 0, st>>>(d);
 }
 
 void launch_build_nl(const DevView& d, double cutsq, cudaStream_t st) {
   long long threads = (long long)d.ncells * 32;
-  k_build_nl<<<blocks_for(threads, 128), 128, 0, st>>>(d, cutsq);
+  if (d.exclStart)
+    k_build_nl<true><<<blocks_for(threads, 128), 128, 0, st>>>(d, cutsq);
+  else
+    k_build_nl<false><<<blocks_for(threads, 128), 128, 0, st>>>(d, cutsq);
 }
 
 template <int TPP, bool MIXED>

@@ -173,12 +173,23 @@ ESPP_API int espp_energy_noalloc(espp_system* s, int32_t which, double* e);
 
 /* ---- measurement ---------------------------------------------------------------
  * No reference counterpart (the reference times phases with esutil::WallTimer,
- * VelocityVerlet.cpp:171-232).  With profiling on, run() brackets each phase with
- * CUDA events on the system's stream: ms[0] pair/bond force kernel, ms[1] integrator
- * kernel, ms[2] re-sort + Verlet build, ms[3] rebuild decision; launches[] counts the
- * kernels each phase launched.  espp_set_profiling resets the sums. */
+ * VelocityVerlet.cpp:171-232).  With profiling on, run() steps on the host-driven loop
+ * and brackets each phase with CUDA events on the system's stream: ms[0] pair/bond
+ * force kernel, ms[1] integrator kernel, ms[2] re-sort (fold, bin, sort, gather),
+ * ms[3] rebuild decision, ms[4] Verlet build, ms[5..7] unused; launches[] counts the
+ * kernels of each phase (also without profiling).  espp_set_profiling resets both. */
 ESPP_API int espp_set_profiling(espp_system* s, int32_t on);
-ESPP_API int espp_profile(espp_system* s, double ms[4], int64_t launches[4]);
+ESPP_API int espp_profile(espp_system* s, double ms[8], int64_t launches[8]);
+/* Threads per particle of the force kernel (1, 2, 4 or 8; default 4, or the
+ * environment variable ESPP_B200_TPP).  The FP32 partial sums of the threads are combined
+ * in int64 fixed point, so the value changes the rounding of the mixed-precision forces
+ * (within the 1e-5 error budget) but not their determinism for a fixed setting.
+ * No reference counterpart (tuning of the GPU kernel). */
+ESPP_API int espp_set_tpp(espp_system* s, int32_t tpp);
+/* Times the force kernel on the current particle state for 1, 2, 4 and 8 threads per
+ * particle (3 launches each, CUDA events), keeps the fastest and returns it; ms[c] (may
+ * be NULL) receives the mean launch time of candidate c. */
+ESPP_API int espp_autotune(espp_system* s, int32_t* best_tpp, double ms[4]);
 /* Device time of the last espp_run on the system's stream (ms): ms[0] whole call,
  * ms[1] the step loop after the start-of-run force evaluation. */
 ESPP_API int espp_last_run_ms(espp_system* s, double ms[2]);

@@ -1013,9 +1013,9 @@ int espp_set_profiling(espp_system* s, int32_t) {
   return ESPP_OK;
 }
 
-int espp_profile(espp_system* s, double ms[4], int64_t launches[4]) {
+int espp_profile(espp_system* s, double ms[8], int64_t launches[8]) {
   CHECK_S(s);
-  for (int k = 0; k < 4; ++k) {
+  for (int k = 0; k < 8; ++k) {
     if (ms) ms[k] = 0.0;
     if (launches) launches[k] = 0;
   }
@@ -1029,6 +1029,19 @@ int espp_last_run_ms(espp_system* s, double ms[2]) {
 }
 
 int espp_select_device(int32_t) { return ESPP_OK; }
+
+int espp_set_tpp(espp_system* s, int32_t) {
+  CHECK_S(s);
+  return ESPP_OK;
+}
+
+int espp_autotune(espp_system* s, int32_t* best, double ms[4]) {
+  CHECK_S(s);
+  if (best) *best = 1;
+  if (ms)
+    for (int k = 0; k < 4; ++k) ms[k] = 0.0;
+  return ESPP_OK;
+}
 
 // Test hook: Philox outputs, so the tests can pin the generator on known answers.
 int espp_oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {

@@ -120,3 +120,41 @@ def test_graph_loop_matches_host_loop(prec, monkeypatch):
     assert sims[0].num_resorts() == sims[1].num_resorts()
     assert sims[0].builds() == sims[1].builds() > 2
     assert sims[0].step() == sims[1].step() == 67
+
+
+@pytest.mark.parametrize("tpp", [1, 2, 4, 8])
+def test_mixed_forces_every_threads_per_particle(tpp):
+    pid, pos, vel, box = load_lj2048()
+    o = _lj_setup(oracle_lib(), _abi.PREC_FP64, pid, pos, vel, box)
+    o.integrator(0.005)
+    o.run(0)
+    fo = o.particles(pid)[2]
+    got = []
+    for _ in range(2):
+        g = _lj_setup(cuda_lib(), _abi.PREC_MIXED, pid, pos, vel, box)
+        _abi.call(g.lib, "espp_set_tpp", g.h, tpp)
+        g.integrator(0.005)
+        g.run(0)
+        got.append(g.particles(pid)[2])
+    assert np.array_equal(got[0], got[1])  # deterministic for a fixed setting
+    assert _rel_rms(got[0], fo) < 1e-5
+
+
+@pytest.mark.parametrize("prec", [_abi.PREC_FP64, _abi.PREC_MIXED])
+def test_large_cells_pairs_and_forces(prec):
+    """3x3x3 cells of ~76 particles: the Verlet build walks the cell in groups of 32 and
+    the in-cell sort takes its fallback path; the pair set stays the reference's."""
+    pid, pos, vel, box = load_lj2048()
+    sims = []
+    for lib, p in ((oracle_lib(), _abi.PREC_FP64), (cuda_lib(), prec)):
+        s = Sim(lib, box, 0.3, [3, 3, 3], precision=p)
+        s.add(pid, pos, vel)
+        s.decompose()
+        s.vl(2.5)
+        s.lj(0, 0, 1.0, 1.0, 2.5, 4.0 * (2.5 ** -12 - 2.5 ** -6))
+        s.integrator(0.005)
+        s.run(10)
+        sims.append(s)
+    assert np.array_equal(sims[0].pairs(), sims[1].pairs())
+    ro, rg = sims[0].particles(pid), sims[1].particles(pid)
+    assert np.max(np.abs(rg[0] - ro[0])) < (1e-9 if prec == _abi.PREC_FP64 else 1e-5)
