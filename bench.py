@@ -251,11 +251,22 @@ def gpu_arm(args, rank, world, local_rank):
 
     # warm-up (untimed), then pick threads per particle for the force kernel
     call(lib, "espp_run", h, args.warmup)
-    tpp = ctypes.c_int32()
+    tpp = ctypes.c_int32(args.tpp)
     tune_ms = np.zeros(4)
-    call(lib, "espp_autotune", h, ctypes.byref(tpp), dptr(tune_ms))
+    if args.tpp:
+        call(lib, "espp_set_tpp", h, args.tpp)
+    else:
+        call(lib, "espp_autotune", h, ctypes.byref(tpp), dptr(tune_ms))
     log("rank %d: autotune tpp=%d (1,2,4,8 -> %s ms)" % (rank, tpp.value,
                                                         np.round(tune_ms, 4).tolist()))
+
+    def total_energy(hh):
+        e = ctypes.c_double()
+        call(lib, "espp_energy", hh, 0, ctypes.byref(e))
+        v2 = ctypes.c_double()
+        nn = ctypes.c_int64()
+        call(lib, "espp_kinetic", hh, ctypes.byref(v2), ctypes.byref(nn))
+        return e.value + 0.5 * v2.value
 
     # timed region: one run of K steps on the captured step-loop graph; CUDA events on
     # the library's stream around the step loop
@@ -280,6 +291,7 @@ def gpu_arm(args, rank, world, local_rank):
         t = torch.tensor([loop_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         loop_ms = float(t.item())
+
 
     # per-kernel device times: the same workload stepped K more steps with every launch
     # bracketed by CUDA events on the library's stream (host-driven loop)
@@ -311,6 +323,53 @@ def gpu_arm(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
 
+    # mixed vs all-FP64 GPU on the same positions: force error and step throughput
+    cmp = {}
+    if prec == _abi.PREC_MIXED and not args.no_fp64:
+        h64 = make_system(lib, args.n_side, _abi.PREC_FP64)[0]
+        call(lib, "espp_set_particles", h64, N, i64ptr(pin_ids), dptr(pin_pos), dptr(pin_vel))
+        call(lib, "espp_run", h64, 0)
+        call(lib, "espp_run", h, 0)
+        f32 = np.zeros((N, 3))
+        f64 = np.zeros((N, 3))
+        call(lib, "espp_get_particles", h, N, i64ptr(pin_ids), None, None, dptr(f32), None)
+        call(lib, "espp_get_particles", h64, N, i64ptr(pin_ids), None, None, dptr(f64), None)
+        df = f32 - f64
+        rel_rms = float(np.sqrt(np.sum(df * df) / np.sum(f64 * f64)))
+        rel_max = float(np.max(np.linalg.norm(df, axis=1)) /
+                        np.sqrt(np.mean(np.sum(f64 * f64, axis=1))))
+        call(lib, "espp_run", h64, args.warmup)
+        tpp64 = ctypes.c_int32()
+        call(lib, "espp_autotune", h64, ctypes.byref(tpp64), None)
+        # both precisions step the same K NVE steps from the same state
+        call(lib, "espp_set_particles", h64, N, i64ptr(pin_ids), dptr(pin_pos), dptr(pin_vel))
+        call(lib, "espp_set_particles", h, N, i64ptr(pin_ids), dptr(pin_pos), dptr(pin_vel))
+        call(lib, "espp_run", h64, 0)
+        call(lib, "espp_run", h, 0)
+        e64_before = total_energy(h64)
+        e32_before = total_energy(h)
+        barrier()
+        call(lib, "espp_run", h64, args.steps)
+        barrier()
+        call(lib, "espp_run", h, args.steps)
+        drift64 = (total_energy(h64) - e64_before) / N / (args.steps * DT)
+        drift32 = (total_energy(h) - e32_before) / N / (args.steps * DT)
+        ms64 = np.zeros(2)
+        call(lib, "espp_last_run_ms", h64, dptr(ms64))
+        loop64 = float(ms64[1])
+        if dist is not None:
+            t = torch.tensor([loop64], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            loop64 = float(t.item())
+        lib.espp_system_destroy(h64)
+        cmp = {"force_rel_rms_err": rel_rms, "force_rel_max_err": rel_max,
+               "fp64_value": world * N * args.steps / (loop64 * 1e-3),
+               "fp64_ms_per_step": loop64 / args.steps,
+               "mixed_over_fp64": loop64 / loop_ms,
+               "fp64_threads_per_particle": int(tpp64.value),
+               "same_segment_nve_drift_per_particle_per_tau": {"mixed": drift32, "fp64": drift64,
+                                                               "e0_per_particle": e64_before / N}}
+
     lib.espp_system_destroy(h)
     if rank != 0:
         if dist is not None:
@@ -330,7 +389,10 @@ def gpu_arm(args, rank, world, local_rank):
         "metric": "LJ particle-steps/s", "value": value, "unit": "particle-steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": loop_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32+i64 fixed (forces), f64 (integrator)",
+        "vs_baseline": None, "dtype": "f32" if prec else "f64",
+        "dtype_detail": "pair forces f32 on int32 box-wrapped coordinates, int64 2^-32 "
+                        "fixed-point force sums, f64 positions/velocities/energies"
+                        if prec else "all f64",
         "data": "synthetic",
         "config": {"workload": "LJ fluid, %d^3 = %d particles, rho %.4f, rc %.1f, skin %.1f, "
                                "dt %.3f, NVE, %s" % (args.n_side, N, RHO, RC, SKIN, DT,
@@ -352,6 +414,10 @@ def gpu_arm(args, rank, world, local_rank):
                              "decide": ph[3], "verlet_build": ph[4],
                              "launches": [int(x) for x in launches_p[:5]]},
         "gpu_launches": int(launches.sum()),
+        "accuracy": dict(cmp, note="forces of the mixed and the all-FP64 kernel on identical "
+                                   "positions; drift = (E_after - E_before) / N / (K dt) with "
+                                   "both precisions stepping the same K NVE steps from the "
+                                   "same state"),
         "clocks": clocks,
         "e2e": {"value": world * N * args.steps / e2e_s, "unit": "particle-steps/s",
                 "h2d_bytes_per_step": int(N * (48 + 8) / args.steps),
@@ -380,6 +446,9 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--ref-budget", type=float, default=20.0)
     ap.add_argument("--steps-ref", type=int, default=1)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the all-FP64 comparison")
+    ap.add_argument("--tpp", type=int, default=0, choices=[0, 1, 2, 4, 8],
+                    help="threads per particle of the force kernel (0: autotune)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")

@@ -53,6 +53,13 @@ __device__ __forceinline__ float fast_rcp(float x) {
   return r;
 }
 
+// Verlet list layout: each particle's entries in blocks of 8 contiguous ints, block b of
+// particle i at ints [(b * cap + i) * 8, +8).  A thread reads a whole block with two
+// 16-byte loads and a warp of consecutive particles reads 1 KB of contiguous memory.
+__device__ __forceinline__ size_t nl_index(int k, int i, size_t cap) {
+  return (((size_t)(k >> 3) * cap + (size_t)i) << 3) + (size_t)(k & 7);
+}
+
 // ---- Philox4x32-10 (Salmon et al., SC'11) ----------------------------------------
 __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
 #pragma unroll
@@ -408,8 +415,7 @@ __global__ void __launch_bounds__(128) k_build_nl(DevView d, double cutsq) {
     const int i = g + lane;
     const int64_t idi = (EXCL && lane < ni) ? a.id[i] : 0;
     int cnt = 0;
-    int* out = d.nl + i;
-    const size_t stride = d.cap;
+    const size_t cap = d.cap;
     __syncwarp();
     int r = 0;  // row of the first chunk of the batch
     for (int qb = 0; qb < nchunks; qb += kMaxChunks) {
@@ -483,8 +489,7 @@ __global__ void __launch_bounds__(128) k_build_nl(DevView d, double cutsq) {
             const int t = cb + bit;
             const int j = t < ct0 ? st0 + t : (t < ct0 + ct1 ? st1 + t - ct0 : st2 + t - ct0 - ct1);
             if (EXCL && is_excluded(d, idi, a.id[j])) continue;
-            if (cnt < d.K) *out = j;
-            out += stride;
+            if (cnt < d.K) d.nl[nl_index(cnt, i, cap)] = j;
             ++cnt;
           }
         }
@@ -498,7 +503,7 @@ __global__ void __launch_bounds__(128) k_build_nl(DevView d, double cutsq) {
       d.nn[i] = cc;
       // pad to a multiple of 8 with the particle itself (r^2 = 0, masked by the force
       // kernels) so that batches of 8 need no bounds checks; K is a multiple of 8
-      for (int k = cc; k < ((cc + 7) & ~7); ++k) d.nl[(size_t)k * stride + i] = i;
+      for (int k = cc; k < ((cc + 7) & ~7); ++k) d.nl[nl_index(k, i, cap)] = i;
     }
     const int wmax = __reduce_max_sync(0xffffffffu, lane < ni ? cnt : 0);
     if (lane == 0 && wmax > 0) atomicMax(&d.ctr->nnMax, wmax);
@@ -539,94 +544,64 @@ __global__ void __launch_bounds__(256) k_force_mixed(DevView d, FENEParams fp) {
   float fx = 0.f, fy = 0.f, fz = 0.f;
   LJPairF P = d.ljf[0];
   const int ntypes = d.ntypes;
-  const int* __restrict__ nl = d.nl + i;
   const size_t cap = d.cap;
-  constexpr int U = 8;
+  auto pair = [&](const int4 pj) {
+    const float dx = wrapped_diff(pi.x, pj.x, ux);
+    const float dy = wrapped_diff(pi.y, pj.y, uy);
+    const float dz = wrapped_diff(pi.z, pj.z, uz);
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    if (!SINGLE) P = sP[pi.w * ntypes + pj.w];
+    const float ri2 = fast_rcp(r2);
+    const float ri6 = ri2 * ri2 * ri2;
+    float ff = ri6 * (P.ff1 * ri6 - P.ff2) * ri2;
+    if (CAPPED && r2 <= P.capsq) ff = P.capff * rsqrtf(r2);
+    // padding entries are the particle itself: r^2 = 0
+    ff = (r2 > 0.f && r2 <= P.rcsq) ? ff : 0.f;
+    fx += dx * ff;
+    fy += dy * ff;
+    fz += dz * ff;
+  };
   if (TPP == 1) {
-    // Lists are padded to a multiple of 8 with the particle itself (r^2 = 0, masked), so
-    // each batch of 8 entries is read without bounds checks.  The next batch's entries
-    // are loaded before the current batch's coordinates are used, so list loads,
-    // coordinate gathers and arithmetic overlap; the sum order is the list order.
-    const int padded = (cnt + 7) & ~7;
-    const size_t stride = cap;
-    const int* q = nl;
-    int jn[U];
-    if (padded > 0) {
-#pragma unroll
-      for (int u = 0; u < U; ++u) jn[u] = __ldcs(q + u * stride);
+    // The list is padded to a multiple of 8 (with the particle itself), so it is read in
+    // whole blocks of 8: two 16-byte streaming loads per block.  The next block is loaded
+    // before the current block's coordinates are used, so list loads, coordinate gathers
+    // and arithmetic overlap; the sum order is the list order.
+    const int nblk = (cnt + 7) >> 3;
+    const int4* blk = reinterpret_cast<const int4*>(d.nl) + (size_t)i * 2;
+    const size_t bstride = cap * 2;
+    int4 ja = make_int4(i, i, i, i), jb = ja;
+    if (nblk > 0) {
+      ja = __ldcs(blk);
+      jb = __ldcs(blk + 1);
     }
-    for (int k = 0; k < padded; k += U) {
-      int4 pj[U];
+    for (int b = 0; b < nblk; ++b) {
+      const int j[8] = {ja.x, ja.y, ja.z, ja.w, jb.x, jb.y, jb.z, jb.w};
+      int4 pj[8];
 #pragma unroll
-      for (int u = 0; u < U; ++u) pj[u] = __ldg(&d.posq[jn[u]]);
-      q += U * stride;
-      if (k + U < padded) {
-#pragma unroll
-        for (int u = 0; u < U; ++u) jn[u] = __ldcs(q + u * stride);
+      for (int u = 0; u < 8; ++u) pj[u] = __ldg(&d.posq[j[u]]);
+      blk += bstride;
+      if (b + 1 < nblk) {
+        ja = __ldcs(blk);
+        jb = __ldcs(blk + 1);
       }
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const float dx = wrapped_diff(pi.x, pj[u].x, ux);
-        const float dy = wrapped_diff(pi.y, pj[u].y, uy);
-        const float dz = wrapped_diff(pi.z, pj[u].z, uz);
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        if (!SINGLE) P = sP[pi.w * ntypes + pj[u].w];
-        const float ri2 = fast_rcp(r2);
-        const float ri6 = ri2 * ri2 * ri2;
-        float ff = ri6 * (P.ff1 * ri6 - P.ff2) * ri2;
-        if (CAPPED && r2 <= P.capsq) ff = P.capff * rsqrtf(r2);
-        ff = (r2 > 0.f && r2 <= P.rcsq) ? ff : 0.f;
-        fx += dx * ff;
-        fy += dy * ff;
-        fz += dz * ff;
-      }
+      for (int u = 0; u < 8; ++u) pair(pj[u]);
     }
   } else {
-    // Entries (k, i) are read as a stream (evict-first) in batches of U per thread; the
-    // next batch's entries are loaded before the current batch's coordinates are used, so
-    // list loads, coordinate gathers and arithmetic overlap.  Slots past the end of the
-    // list read the particle itself and are masked out, so every batch has the same shape
-    // and the sum order is the list order.
-    int jn[U];
-  #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int kk = sub + u * TPP;
-      jn[u] = kk < cnt ? __ldcs(nl + (size_t)kk * cap) : i;
-    }
-    for (int k = sub; k < cnt; k += U * TPP) {
+    // thread sub of particle i takes entries sub, sub + TPP, ...
+    constexpr int U = 4;
+    int k = sub;
+    for (; k + (U - 1) * TPP < cnt; k += U * TPP) {
       int j[U];
-      bool valid[U];
-  #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        j[u] = jn[u];
-        valid[u] = k + u * TPP < cnt;
-      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) j[u] = __ldcs(d.nl + nl_index(k + u * TPP, i, cap));
       int4 pj[U];
-  #pragma unroll
+#pragma unroll
       for (int u = 0; u < U; ++u) pj[u] = __ldg(&d.posq[j[u]]);
-      const int kn = k + U * TPP;
-  #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int kk = kn + u * TPP;
-        jn[u] = kk < cnt ? __ldcs(nl + (size_t)kk * cap) : i;
-      }
-  #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const float dx = wrapped_diff(pi.x, pj[u].x, ux);
-        const float dy = wrapped_diff(pi.y, pj[u].y, uy);
-        const float dz = wrapped_diff(pi.z, pj[u].z, uz);
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        if (!SINGLE) P = sP[pi.w * ntypes + pj[u].w];
-        const float ri2 = fast_rcp(r2);
-        const float ri6 = ri2 * ri2 * ri2;
-        float ff = ri6 * (P.ff1 * ri6 - P.ff2) * ri2;
-        if (CAPPED && r2 <= P.capsq) ff = P.capff * rsqrtf(r2);
-        ff = (valid[u] && r2 <= P.rcsq) ? ff : 0.f;
-        fx += dx * ff;
-        fy += dy * ff;
-        fz += dz * ff;
-      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) pair(pj[u]);
     }
+    for (; k < cnt; k += TPP) pair(__ldg(&d.posq[__ldcs(d.nl + nl_index(k, i, cap))]));
   }
   long long Fx = to_fix(fx, d.err), Fy = to_fix(fy, d.err), Fz = to_fix(fz, d.err);
   if (FENE && sub == 0 && act) {
@@ -704,7 +679,6 @@ __global__ void __launch_bounds__(256) k_force_fp64(DevView d, FENEParams fp) {
   const int cnt = act ? d.nn[i] : 0;
   double fx = 0, fy = 0, fz = 0;
   const int ntypes = d.ntypes;
-  const int* __restrict__ nl = d.nl + i;
   const size_t cap = d.cap;
   auto pair = [&](int j, double xj, double yj, double zj) {
     const double dx = min_image(xi - xj, d.L[0], d.halfL[0]);
@@ -712,7 +686,7 @@ __global__ void __launch_bounds__(256) k_force_fp64(DevView d, FENEParams fp) {
     const double dz = min_image(zi - zj, d.L[2], d.halfL[2]);
     const double r2 = dx * dx + dy * dy + dz * dz;
     const LJPair& P = SINGLE ? d.lj[0] : d.lj[ti * ntypes + __ldg(&a.type[j])];
-    if (!P.set || r2 > P.rcsq) return;
+    if (!P.set || !(r2 > 0.0) || r2 > P.rcsq) return;  // padding: the particle itself
     double ff;
     if (CAPPED && P.caprad > 0 && !(r2 > P.caprad * P.caprad)) {
       ff = P.capff / sqrt(r2);
@@ -725,25 +699,31 @@ __global__ void __launch_bounds__(256) k_force_fp64(DevView d, FENEParams fp) {
     fy += dy * ff;
     fz += dz * ff;
   };
-  constexpr int U = 4;
-  int k = sub;
-  for (; k + (U - 1) * TPP < cnt; k += U * TPP) {
-    int j[U];
+  if (TPP == 1) {
+    const int nblk = (cnt + 7) >> 3;
+    const int4* blk = reinterpret_cast<const int4*>(d.nl) + (size_t)i * 2;
+    const size_t bstride = cap * 2;
+    for (int b = 0; b < nblk; ++b, blk += bstride) {
 #pragma unroll
-    for (int u = 0; u < U; ++u) j[u] = __ldcs(nl + (size_t)(k + u * TPP) * cap);
-    double xj[U], yj[U], zj[U];
+      for (int h = 0; h < 2; ++h) {
+        const int4 jj = __ldcs(blk + h);
+        const int j[4] = {jj.x, jj.y, jj.z, jj.w};
+        double xj[4], yj[4], zj[4];
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      xj[u] = __ldg(&X[j[u]]);
-      yj[u] = __ldg(&Y[j[u]]);
-      zj[u] = __ldg(&Z[j[u]]);
+        for (int u = 0; u < 4; ++u) {
+          xj[u] = __ldg(&X[j[u]]);
+          yj[u] = __ldg(&Y[j[u]]);
+          zj[u] = __ldg(&Z[j[u]]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) pair(j[u], xj[u], yj[u], zj[u]);
+      }
     }
-#pragma unroll
-    for (int u = 0; u < U; ++u) pair(j[u], xj[u], yj[u], zj[u]);
-  }
-  for (; k < cnt; k += TPP) {
-    const int j = __ldcs(nl + (size_t)k * cap);
-    pair(j, __ldg(&X[j]), __ldg(&Y[j]), __ldg(&Z[j]));
+  } else {
+    for (int k = sub; k < cnt; k += TPP) {
+      const int j = __ldcs(d.nl + nl_index(k, i, cap));
+      pair(j, __ldg(&X[j]), __ldg(&Y[j]), __ldg(&Z[j]));
+    }
   }
   if (FENE && sub == 0 && act) {
     const int64_t off = a.id[i] - d.idMin;
@@ -990,7 +970,7 @@ __global__ void k_lj_obs(DevView d, int energy, double* partials) {
     const int ti = a.type[i];
     const int cnt = d.nn[i];
     for (int k = 0; k < cnt; ++k) {
-      const int j = d.nl[(size_t)k * d.cap + i];
+      const int j = d.nl[nl_index(k, i, d.cap)];
       if (j < i) continue;
       const double dx = min_image(xi - X[j], d.L[0], d.halfL[0]);
       const double dy = min_image(yi - Y[j], d.L[1], d.halfL[1]);
@@ -1131,7 +1111,7 @@ __global__ void k_pair_count(DevView d, int32_t* counts) {
   if (i >= d.n) return;
   const int64_t idi = a.id[i];
   int c = 0;
-  for (int k = 0; k < d.nn[i]; ++k) c += a.id[d.nl[(size_t)k * d.cap + i]] > idi;
+  for (int k = 0; k < d.nn[i]; ++k) c += a.id[d.nl[nl_index(k, i, d.cap)]] > idi;
   counts[i] = c;
 }
 
@@ -1142,7 +1122,7 @@ __global__ void k_pair_write(DevView d, const int64_t* offsets, int64_t* out) {
   const int64_t idi = a.id[i];
   int64_t o = offsets[i];
   for (int k = 0; k < d.nn[i]; ++k) {
-    const int64_t idj = a.id[d.nl[(size_t)k * d.cap + i]];
+    const int64_t idj = a.id[d.nl[nl_index(k, i, d.cap)]];
     if (idj > idi) {
       out[2 * o] = idi;
       out[2 * o + 1] = idj;
