@@ -48,9 +48,10 @@ N_HALF = 2.0 / 3.0 * math.pi * (RC + SKIN) ** 3 * RHO
 STEP_BYTES = 168.0 + 4.0 * N_HALF
 # force kernel: packed coordinates read 12 + 4 B per half-list pair + int64 F write 24
 FORCE_BYTES = 12.0 + 4.0 * N_HALF + 24.0
-# DRAM bytes per particle of one force-kernel launch measured by ncu
-# (profiles/force_mixed_lj_ncu.txt), scaled from the 32^3 case; None until captured
-FORCE_TRAFFIC_PER_PARTICLE = None
+# DRAM bytes (read + write) per particle of one force-kernel launch, measured by ncu on
+# the 1,000,000-particle case (profiles/force_mixed_lj_1M_ncu.txt: 345.0 MB + 5.6 MB);
+# traffic grows in proportion to the particle count at fixed density
+FORCE_TRAFFIC_PER_PARTICLE = 350.6
 
 
 def log(*a):
@@ -384,7 +385,7 @@ def gpu_arm(args, rank, world, local_rank):
     step_s = loop_ms * 1e-3 / args.steps
     value = world * N * args.steps / (loop_ms * 1e-3)
     cpu_rate, cpu_cores = cpu_baseline(1, budget_s=args.cpu_budget) if world == 1 else (None, 1)
-    traffic = (FORCE_TRAFFIC_PER_PARTICLE * N) if FORCE_TRAFFIC_PER_PARTICLE else None
+    traffic = (FORCE_TRAFFIC_PER_PARTICLE * N) if (FORCE_TRAFFIC_PER_PARTICLE and prec) else None
     line = {
         "metric": "LJ particle-steps/s", "value": value, "unit": "particle-steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
