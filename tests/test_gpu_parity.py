@@ -158,3 +158,87 @@ def test_large_cells_pairs_and_forces(prec):
     assert np.array_equal(sims[0].pairs(), sims[1].pairs())
     ro, rg = sims[0].particles(pid), sims[1].particles(pid)
     assert np.max(np.abs(rg[0] - ro[0])) < (1e-9 if prec == _abi.PREC_FP64 else 1e-5)
+
+
+@pytest.mark.parametrize("prec", [_abi.PREC_FP64, _abi.PREC_MIXED])
+def test_polymer_melt_langevin_run_matches_oracle(prec):
+    """40 000-bead ring melt: WCA (rc 1.12, shift 0) + FENE + Langevin, 15 steps."""
+    pos, bonds, box, gold = load_polymer40k()
+    ids = np.arange(1, len(pos) + 1)
+    sims = []
+    for lib, p in ((oracle_lib(), _abi.PREC_FP64), (cuda_lib(), prec)):
+        s = Sim(lib, box, 0.3, cell_grid(box, 1.12, 0.3), precision=p, seed=54321)
+        s.add(ids, pos)
+        s.decompose()
+        s.vl(1.42)
+        s.lj(0, 0, 1.0, 1.0, 1.12, 0.0)
+        s.bonds(bonds)
+        s.fene(30.0, 0.0, 1.5)
+        s.integrator(0.01)
+        s.langevin(1.0, 1.0)
+        s.run(15)
+        sims.append(s)
+    ro, rg = sims[0].particles(ids), sims[1].particles(ids)
+    tol = 1e-9 if prec == _abi.PREC_FP64 else 2e-5
+    assert np.max(np.abs(rg[0] - ro[0])) < tol
+    assert np.array_equal(rg[3], ro[3])
+    for which in (_abi.IA_LJ, _abi.IA_FENE):
+        eo, eg = sims[0].energy(which), sims[1].energy(which)
+        assert abs(eg - eo) < (1e-9 if prec == _abi.PREC_FP64 else 1e-5) * abs(eo)
+
+
+def test_multitype_lj_with_exclusions():
+    pid, pos, vel, box = load_lj2048()
+    types = (pid % 3).astype(np.int32)
+    excl = np.array([[int(pid[k]), int(pid[k + 1])] for k in range(0, 400, 2)])
+    sims = []
+    for lib, p in ((oracle_lib(), _abi.PREC_FP64), (cuda_lib(), _abi.PREC_FP64),
+                   (cuda_lib(), _abi.PREC_MIXED)):
+        s = Sim(lib, box, 0.3, cell_grid(box, 2.5, 0.3), precision=p)
+        s.add(pid, pos, vel, types=types)
+        s.decompose()
+        s.vl(2.5, excl=excl)
+        s.lj(0, 0, 1.0, 1.0, 2.5, 0.0)
+        s.lj(0, 1, 1.5, 0.9, 2.2, 0.0)
+        s.lj(1, 1, 0.7, 1.1, 2.5, 0.0)
+        s.lj(2, 2, 1.2, 1.0, 2.0, 0.0)
+        # pairs (0,2) and (1,2) left unset: no interaction, as in the reference's table
+        s.integrator(0.005)
+        s.run(5)
+        sims.append(s)
+    for s in sims[1:]:
+        assert np.array_equal(s.pairs(), sims[0].pairs())
+    ex = set(map(tuple, np.sort(excl, axis=1)))
+    assert not ex & set(map(tuple, sims[0].pairs()))
+    ro = sims[0].particles(pid)
+    assert np.max(np.abs(sims[1].particles(pid)[0] - ro[0])) < 1e-9
+    assert np.max(np.abs(sims[2].particles(pid)[0] - ro[0])) < 1e-5
+    eo = sims[0].energy(_abi.IA_LJ)
+    assert abs(sims[1].energy(_abi.IA_LJ) - eo) < 1e-9 * abs(eo)
+
+
+@pytest.mark.parametrize("mode,cap", [(_abi.CAP_ABS, 20.0), (_abi.CAP_COMPONENT, [15.0, 10.0, 5.0])])
+def test_capforce_and_capped_lj(mode, cap):
+    pos, box = lattice(10, 1.1, 0.25, seed=7)   # dense, overlapping start
+    pid = np.arange(len(pos))
+    sims = []
+    for lib, p in ((oracle_lib(), _abi.PREC_FP64), (cuda_lib(), _abi.PREC_FP64),
+                   (cuda_lib(), _abi.PREC_MIXED)):
+        s = Sim(lib, box, 0.3, cell_grid(box, 2 ** (1 / 6), 0.3), precision=p)
+        s.add(pid, pos)
+        s.decompose()
+        s.vl(2 ** (1 / 6))
+        s.lj(0, 0, 1.0, 1.0, 2 ** (1 / 6), 1.0, caprad=0.9)
+        s.capforce(mode, cap)
+        s.integrator(0.002)
+        s.langevin(0.5, 1.0)
+        s.run(10)
+        sims.append(s)
+    ro = sims[0].particles(pid)
+    assert np.max(np.abs(sims[1].particles(pid)[0] - ro[0])) < 1e-9
+    assert np.max(np.abs(sims[2].particles(pid)[0] - ro[0])) < 1e-5
+    f = sims[1].particles(pid)[2]
+    if mode == _abi.CAP_ABS:
+        assert np.max(np.linalg.norm(f, axis=1)) <= cap * (1 + 1e-12)
+    else:
+        assert np.all(np.abs(f) <= np.array(cap) * (1 + 1e-12))
