@@ -436,12 +436,132 @@ def gpu_arm(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+# ---- batched parallel-tempering replicas ------------------------------------------
+def replicas_arm(args, rank, world, local_rank):
+    """64 LJ replicas, N ~ U{2000..64000} (seed 4), rho 0.8442, rc 2.5, skin 0.3,
+    T_r = 0.7 (2.0/0.7)^(r/63), Langevin gamma 1, dt 0.005, Metropolis exchange between
+    neighbours every 100 steps (ParallelTempering.exchange rule).  Times K steps of all
+    replicas with one graph launch per 100-step segment against the same steps run
+    replica by replica (espp_run each), wall clock around the calls."""
+    import espressopp_b200
+    from espressopp_b200 import _abi
+    from espressopp_b200._abi import call, dptr, i32ptr, i64ptr
+    from espressopp_b200.parallel_tempering import exchange_decisions
+    lib = espressopp_b200.load_library()
+    call(lib, "espp_select_device", local_rank)
+    R = 64
+    rng = np.random.Generator(np.random.PCG64(4))
+    sizes = rng.integers(2000, 64001, size=R)
+    temps = [0.7 * (2.0 / 0.7) ** (r / (R - 1)) for r in range(R)]
+
+    def make(r, prec):
+        N = int(sizes[r])
+        L = (N / RHO) ** (1.0 / 3.0)
+        a = int(math.ceil(N ** (1.0 / 3.0)))
+        sp = L / a
+        g = (np.arange(a) + 0.5) * sp
+        grid = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)[:N]
+        pr = np.random.Generator(np.random.PCG64(1000 + r))
+        pos = grid + pr.uniform(-0.05, 0.05, size=grid.shape)
+        vel = mb_velocities(N, temps[r], 2000 + r)
+        h = ctypes.c_void_p()
+        box = np.array([L, L, L])
+        cg = np.array([int(L / (RC + SKIN))] * 3, np.int32)
+        call(lib, "espp_system_create", dptr(box), SKIN, i32ptr(cg), prec, 77 + r, ctypes.byref(h))
+        ids = np.arange(N, dtype=np.int64)
+        call(lib, "espp_add_particles", h, N, i64ptr(ids), None, None,
+             dptr(np.ascontiguousarray(pos.reshape(-1))), dptr(np.ascontiguousarray(vel.reshape(-1))))
+        call(lib, "espp_decompose", h)
+        call(lib, "espp_vl_create", h, RC, 0, None)
+        call(lib, "espp_lj_set", h, 0, 0, 1.0, 1.0, RC, 4.0 * (RC ** -12 - RC ** -6), 0.0)
+        call(lib, "espp_integrator_set", h, DT)
+        call(lib, "espp_set_tpp", h, 1)
+        return h
+
+    prec = _abi.PREC_MIXED if args.precision == "mixed" else _abi.PREC_FP64
+    T = list(temps)
+
+    def set_T(hs):
+        for r, h in enumerate(hs):
+            call(lib, "espp_langevin_set", h, 1, 1.0, T[r], 0, None)
+
+    def exchange(hs, oddeven, urng):
+        e = []
+        kin = []
+        for h in hs:
+            v = ctypes.c_double()
+            call(lib, "espp_energy", h, 0, ctypes.byref(v))
+            e.append(v.value)
+            k2 = ctypes.c_double()
+            nn = ctypes.c_int64()
+            call(lib, "espp_kinetic", h, ctypes.byref(k2), ctypes.byref(nn))
+            kin.append(k2.value / (3.0 * nn.value))
+        dec = exchange_decisions(e, kin, [int(x) for x in sizes], oddeven, urng.random)
+        for m, n, _, _, ok in dec:
+            if ok:
+                T[m], T[n] = T[n], T[m]
+        return sum(ok for *_, ok in dec)
+
+    import random
+    total = int(sizes.sum())
+    segments = max(1, args.steps // 100)
+    seg = args.steps // segments
+    out = {}
+    for mode in ("sequential", "batched"):
+        T[:] = temps
+        hs = [make(r, prec) for r in range(R)]
+        set_T(hs)
+        b = None
+        if mode == "batched":
+            arr = (ctypes.c_void_p * R)(*[h.value for h in hs])
+            b = ctypes.c_void_p()
+            call(lib, "espp_batch_create", arr, R, ctypes.byref(b))
+        urng = random.Random(335977)
+
+        def step_all(n):
+            if b is not None:
+                call(lib, "espp_batch_run", b, n)
+            else:
+                for h in hs:
+                    call(lib, "espp_run", h, n)
+
+        step_all(args.warmup)
+        swaps = 0
+        t0 = time.perf_counter()
+        for k in range(segments):
+            step_all(seg)
+            swaps += exchange(hs, k % 2, urng)
+            set_T(hs)
+        el = time.perf_counter() - t0
+        out[mode] = {"seconds": el, "value": total * seg * segments / el, "swaps": swaps}
+        if b is not None:
+            lib.espp_batch_destroy(b)
+        for h in hs:
+            lib.espp_system_destroy(h)
+    if rank == 0:
+        line = {"metric": "PT replica particle-steps/s, 64 LJ replicas on 1 B200",
+                "value": out["batched"]["value"], "unit": "particle-steps/s", "n_gpus": world,
+                "steps": seg * segments, "warmup": args.warmup, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec else "f64",
+                "data": "synthetic",
+                "config": {"workload": "64 LJ replicas, N ~ U{2000..64000} (seed 4), total %d "
+                                       "particles, rho 0.8442, rc 2.5, skin 0.3, Langevin gamma 1, "
+                                       "T 0.7..2.0 geometric, dt 0.005, exchange every %d steps"
+                                       % (total, seg),
+                           "timing": "wall clock around the run calls and exchanges"},
+                "batched": out["batched"], "sequential": out["sequential"],
+                "batched_over_sequential": out["batched"]["value"] / out["sequential"]["value"]}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="lj", choices=["lj", "replicas"],
+                    help="lj: the 4,096,000-particle fluid (default); replicas: 64 PT replicas")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--n-side", type=int, default=160)
     ap.add_argument("--cpu-budget", type=float, default=12.0)
@@ -458,6 +578,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         reference_arm(args, rank, world)
+    elif args.workload == "replicas":
+        replicas_arm(args, rank, world, local_rank)
     else:
         gpu_arm(args, rank, world, local_rank)
 

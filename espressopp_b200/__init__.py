@@ -15,7 +15,8 @@ from .core import (FixedPairList, Int3D, Real3D, System, Tensor, VerletList,  # 
                    infinity, set_default_precision)
 from . import analysis, bc, esutil, integrator, interaction, storage, tools  # noqa: F401
 from . import standard_system  # noqa: F401
+from .parallel_tempering import ParallelTempering  # noqa: F401
 
 __all__ = ["System", "VerletList", "FixedPairList", "Real3D", "Int3D", "Tensor", "analysis",
            "bc", "esutil", "integrator", "interaction", "storage", "tools", "standard_system",
-           "set_default_precision", "load_library", "infinity"]
+           "set_default_precision", "load_library", "infinity", "ParallelTempering"]

@@ -674,12 +674,10 @@ void launch_force_kernel(espp_system* s, cudaStream_t st) {
   launch_forces(d, s->precision == ESPP_PREC_MIXED, s->fene, s->tpp, st);
 }
 
+// Adds to graph g one WHILE node (no dependencies) running the step loop of s:
 // WHILE(remaining) { decide; IF(re-sort) { fold, bin, sort, gather, swap, id map, list };
 //                    force; integrate2 + integrate1 }
-void capture_graph(espp_system* s, const IntegrateArgs& ai) {
-  destroy_graph(s);
-  cudaGraph_t g;
-  cuda_check(cudaGraphCreate(&g, 0), "cudaGraphCreate");
+void add_step_loop(espp_system* s, cudaGraph_t g, const IntegrateArgs& ai) {
   cudaGraphConditionalHandle hWhile, hIf;
   cuda_check(cudaGraphConditionalHandleCreate(&hWhile, g, 1, cudaGraphCondAssignDefault),
              "conditional handle");
@@ -724,6 +722,13 @@ void capture_graph(espp_system* s, const IntegrateArgs& ai) {
   launch_rebuild_kernels(s, cs);
   cuda_check(cudaStreamEndCapture(cs, &done), "end capture");
   cudaStreamDestroy(cs);
+}
+
+void capture_graph(espp_system* s, const IntegrateArgs& ai) {
+  destroy_graph(s);
+  cudaGraph_t g;
+  cuda_check(cudaGraphCreate(&g, 0), "cudaGraphCreate");
+  add_step_loop(s, g, ai);
   cudaGraphExec_t ex;
   cuda_check(cudaGraphInstantiate(&ex, g, 0), "cudaGraphInstantiate");
   s->graph = g;
@@ -767,12 +772,12 @@ void maybe_grow_K(espp_system* s) {
   }
 }
 
-// VelocityVerlet::run (src/integrator/VelocityVerlet.cpp:63-169).
-void run(espp_system* s, int64_t nsteps) {
-  const double t0 = now_s();
-  double tResort = 0.0;
+// Everything of VelocityVerlet::run before the step loop (src/integrator/
+// VelocityVerlet.cpp:63-103): re-sort if flagged, lists, device counters, and the
+// start-of-run force with the Langevin heat-up factor followed by integrate1 of step 0.
+// Returns the integrate arguments of the loop.
+IntegrateArgs run_prologue(espp_system* s, int64_t nsteps, double& tResort) {
   s->nResorts = 0;
-  const double skinHalf = 0.5 * s->skin;
   if (!s->runBeg) {
     cuda_check(cudaEventCreate(&s->runBeg), "event");
     cuda_check(cudaEventCreate(&s->runLoop), "event");
@@ -791,14 +796,16 @@ void run(espp_system* s, int64_t nsteps) {
   }
   if (!s->binned) bin(s, false);
   if (s->has_vl && !s->listValid) build_list(s);
+  IntegrateArgs a = integrate_args(s);
   DevCounters c0 = get_counters(s);
   c0.maxSq = 0ull;
   c0.resorts = 0;
   c0.step = s->step - 1;
   c0.remaining = nsteps;
+  c0.pref1 = a.pref1;
+  c0.pref2 = a.pref2;
   set_counters(s, c0);
   // start-of-run force (recalc1 = heatUp: pref2 * sqrt(3); recalc2 restores it)
-  IntegrateArgs a = integrate_args(s);
   timed_forces(s);
   IntegrateArgs a0 = a;
   a0.pref2 = a.pref2 * std::sqrt(3.0);
@@ -815,90 +822,65 @@ void run(espp_system* s, int64_t nsteps) {
   ai.do_i2 = 1;
   ai.do_i1 = 1;
   ai.storeFtot = 0;
-  bool graphDone = false;
-  if (nsteps > 0 && s->useGraph && !s->profiling) {
-    IntegrateArgs ag = ai;
-    ag.fromCounters = 1;
-    ag.step = 0;  // read from the device counters
-    std::string key = graph_key(s, ag);
-    if (!s->graphExec || key != s->graphKey) {
-      capture_graph(s, ag);
-      s->graphKey = key;
+  return ai;
+}
+
+// Arguments baked into a captured step loop: step and Langevin prefactors come from
+// the device counters.
+IntegrateArgs graph_args(const IntegrateArgs& ai) {
+  IntegrateArgs ag = ai;
+  ag.fromCounters = 1;
+  ag.step = 0;
+  ag.pref1 = 0.0;
+  ag.pref2 = 0.0;
+  return ag;
+}
+
+void run_host_loop(espp_system* s, int64_t nsteps, const IntegrateArgs& ai, double& tResort) {
+  const double skinHalf = 0.5 * s->skin;
+  for (int64_t i = 0; i < nsteps; ++i) {
+    {
+      PhaseScope ps(s, kPhOther, 1);
+      launch_decide(s->view(), skinHalf, s->st);
     }
-    sync_pa(s);
-    ensure_snapshot(s);
-    copy_arrays(s, s->snap, s->A);
-    const DevCounters before = c0;
-    const int64_t step0 = s->step;
-    cuda_check(cudaGraphLaunch(s->graphExec, s->st), "cudaGraphLaunch");
-    cuda_check(cudaEventRecord(s->runEnd, s->st), "event");
+    cuda_check(cudaMemcpyAsync(s->hctr, s->ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost,
+                               s->st), "flag");
     sync(s);
-    unsigned e = read_err(s);
-    if (e & kErrNlOverflow) {
-      // restore the pre-run state, grow the list and redo the run on the host loop
-      cuda_check(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->st), "memset");
-      s->paHostValid = false;
-      sync_pa(s);
-      copy_arrays(s, s->A, s->snap);
-      set_counters(s, before);
-      s->step = step0;
-      s->binned = false;
-      s->K = (std::max(s->K * 2, K_high_water(s) + 32) + 7) / 8 * 8;  // multiple of 8
-      dfree(s->nl);
-      s->nl = dalloc<int32_t>((size_t)s->K * s->cap);
-      s->listValid = false;
-      destroy_graph(s);
-      const bool g = s->useGraph;
-      s->useGraph = false;
-      try {
-        run(s, nsteps);
-      } catch (...) {
-        s->useGraph = g;
-        throw;
-      }
-      s->useGraph = g;
-      return;
+    if (s->hctr->flag) {
+      double tr = now_s();
+      timed_decompose(s);
+      s->nResorts++;
+      tResort += now_s() - tr;
     }
-    DevCounters c = get_counters(s);
-    s->step += nsteps;
-    s->nResorts = c.resorts;
-    s->builds += c.resorts;
-    // kernels launched by the graph: decide + force + integrate per step, and zero,
-    // fold/bin, scan, scatter, in-cell sort, gather, swap, id map (+ list) per re-sort
-    s->phaseLaunches[kPhOther] += nsteps;
-    s->phaseLaunches[kPhForce] += nsteps;
-    s->phaseLaunches[kPhIntegrate] += nsteps;
-    s->phaseLaunches[kPhRebuild] += c.resorts * 10;
-    s->phaseLaunches[kPhList] += s->has_vl ? c.resorts : 0;
-    s->paHostValid = false;
-    graphDone = true;
+    timed_forces(s);
+    IntegrateArgs aj = ai;
+    aj.step = s->step;
+    aj.do_i1 = (i + 1 < nsteps) ? 1 : 0;
+    aj.storeFtot = (i + 1 < nsteps) ? 0 : 1;
+    timed_integrate(s, aj);
+    cuda_check(cudaGetLastError(), "step kernels");
+    s->step++;
   }
-  if (!graphDone) {
-    for (int64_t i = 0; i < nsteps; ++i) {
-      {
-        PhaseScope ps(s, kPhOther, 1);
-        launch_decide(s->view(), skinHalf, s->st);
-      }
-      cuda_check(cudaMemcpyAsync(s->hctr, s->ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost,
-                                 s->st), "flag");
-      sync(s);
-      if (s->hctr->flag) {
-        double tr = now_s();
-        timed_decompose(s);
-        s->nResorts++;
-        tResort += now_s() - tr;
-      }
-      timed_forces(s);
-      IntegrateArgs aj = ai;
-      aj.step = s->step;
-      aj.do_i1 = (i + 1 < nsteps) ? 1 : 0;
-      aj.storeFtot = (i + 1 < nsteps) ? 0 : 1;
-      timed_integrate(s, aj);
-      cuda_check(cudaGetLastError(), "step kernels");
-      s->step++;
-    }
-    cuda_check(cudaEventRecord(s->runEnd, s->st), "event");
-  }
+  cuda_check(cudaEventRecord(s->runEnd, s->st), "event");
+}
+
+// Bookkeeping after a graph-run step loop of nsteps.
+void graph_loop_done(espp_system* s, int64_t nsteps) {
+  DevCounters c = get_counters(s);
+  s->step += nsteps;
+  s->nResorts = c.resorts;
+  s->builds += c.resorts;
+  // kernels launched by the graph: decide + force + integrate per step, and zero,
+  // fold/bin, scan (3), scatter, in-cell sort, gather, swap, id map (+ list) per re-sort
+  s->phaseLaunches[kPhOther] += nsteps;
+  s->phaseLaunches[kPhForce] += nsteps;
+  s->phaseLaunches[kPhIntegrate] += nsteps;
+  s->phaseLaunches[kPhRebuild] += c.resorts * 10;
+  s->phaseLaunches[kPhList] += s->has_vl ? c.resorts : 0;
+  s->paHostValid = false;
+}
+
+void run_epilogue(espp_system* s, double t0, double tResort, bool graphDone) {
   sync(s);
   check_err(s);
   maybe_grow_K(s);
@@ -914,6 +896,158 @@ void run(espp_system* s, int64_t nsteps) {
   s->timers[6] = s->phaseMs[kPhIntegrate] * 1e-3;
   s->timers[8] = graphDone ? (s->phaseMs[kPhRebuild] + s->phaseMs[kPhList]) * 1e-3 : tResort;
   s->timers[9] = s->timers[0] - s->timers[1] - s->timers[6] - s->timers[8];
+}
+
+// State at the start of a graph run, kept so that a Verlet-list overflow inside the
+// graph can be undone: particle arrays (copied on the device) and the host counters.
+struct RunSnapshot {
+  DevCounters ctr;
+  int64_t step, builds;
+  bool resortFlag;
+};
+
+RunSnapshot take_snapshot(espp_system* s) {
+  sync_pa(s);
+  ensure_snapshot(s);
+  copy_arrays(s, s->snap, s->A);
+  RunSnapshot r;
+  r.ctr = get_counters(s);
+  r.step = s->step;
+  r.builds = s->builds;
+  r.resortFlag = s->resortFlag;
+  return r;
+}
+
+// Restores the state saved before a graph run whose Verlet list overflowed and grows the
+// list capacity (the caller then redoes the run on the host loop).
+void recover_overflow(espp_system* s, const RunSnapshot& r) {
+  cuda_check(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->st), "memset");
+  s->paHostValid = false;
+  sync_pa(s);
+  copy_arrays(s, s->A, s->snap);
+  set_counters(s, r.ctr);
+  s->step = r.step;
+  s->builds = r.builds;
+  s->resortFlag = r.resortFlag;
+  s->binned = false;
+  s->K = (std::max(s->K * 2, K_high_water(s) + 32) + 7) / 8 * 8;  // multiple of 8
+  dfree(s->nl);
+  s->nl = dalloc<int32_t>((size_t)s->K * s->cap);
+  s->listValid = false;
+  destroy_graph(s);
+}
+
+void run_host(espp_system* s, int64_t nsteps);
+
+// VelocityVerlet::run (src/integrator/VelocityVerlet.cpp:63-169).
+void run(espp_system* s, int64_t nsteps) {
+  if (!(nsteps > 0 && s->useGraph && !s->profiling)) {
+    run_host(s, nsteps);
+    return;
+  }
+  const double t0 = now_s();
+  double tResort = 0.0;
+  RunSnapshot snap = take_snapshot(s);
+  IntegrateArgs ai = run_prologue(s, nsteps, tResort);
+  IntegrateArgs ag = graph_args(ai);
+  std::string key = graph_key(s, ag);
+  if (!s->graphExec || key != s->graphKey) {
+    capture_graph(s, ag);
+    s->graphKey = key;
+  }
+  cuda_check(cudaGraphLaunch(s->graphExec, s->st), "cudaGraphLaunch");
+  cuda_check(cudaEventRecord(s->runEnd, s->st), "event");
+  sync(s);
+  if (read_err(s) & kErrNlOverflow) {
+    // back to the state before the run, a larger list, and the run again on the host loop
+    recover_overflow(s, snap);
+    run_host(s, nsteps);
+    return;
+  }
+  graph_loop_done(s, nsteps);
+  run_epilogue(s, t0, tResort, true);
+}
+
+void run_host(espp_system* s, int64_t nsteps) {
+  const double t0 = now_s();
+  double tResort = 0.0;
+  IntegrateArgs ai = run_prologue(s, nsteps, tResort);
+  run_host_loop(s, nsteps, ai, tResort);
+  run_epilogue(s, t0, tResort, false);
+}
+
+}  // namespace
+
+// Many independent systems stepped by one graph launch: one WHILE branch per system, no
+// dependencies between the branches, so the GPU runs the replicas' kernels concurrently
+// and each keeps its own re-sort schedule (ParallelTempering / MultiSystem,
+// src/ParallelTempering.py:78-203, src/MultiSystem.py:105-125).
+struct espp_batch {
+  std::vector<espp_system*> sys;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ex = nullptr;
+  std::string key;
+  cudaEvent_t beg = nullptr, end = nullptr;
+  std::vector<cudaEvent_t> ready;
+  double lastMs = 0.0;
+};
+
+namespace {
+
+void batch_destroy_graph(espp_batch* b) {
+  if (b->ex) cudaGraphExecDestroy(b->ex);
+  if (b->g) cudaGraphDestroy(b->g);
+  b->ex = nullptr;
+  b->g = nullptr;
+  b->key.clear();
+}
+
+void batch_run(espp_batch* b, int64_t nsteps) {
+  if (nsteps <= 0) {
+    for (espp_system* s : b->sys) run(s, nsteps);
+    return;
+  }
+  const size_t R = b->sys.size();
+  const double t0 = now_s();
+  std::vector<RunSnapshot> snaps(R);
+  std::vector<double> tRes(R, 0.0);
+  std::vector<IntegrateArgs> ags(R);
+  std::string key;
+  for (size_t r = 0; r < R; ++r) {
+    espp_system* s = b->sys[r];
+    snaps[r] = take_snapshot(s);
+    ags[r] = graph_args(run_prologue(s, nsteps, tRes[r]));
+    key += graph_key(s, ags[r]);
+    cuda_check(cudaEventRecord(b->ready[r], s->st), "event");
+    cuda_check(cudaStreamWaitEvent(b->st, b->ready[r], 0), "stream wait");
+  }
+  if (!b->ex || key != b->key) {
+    batch_destroy_graph(b);
+    cuda_check(cudaGraphCreate(&b->g, 0), "cudaGraphCreate");
+    for (size_t r = 0; r < R; ++r) add_step_loop(b->sys[r], b->g, ags[r]);
+    cuda_check(cudaGraphInstantiate(&b->ex, b->g, 0), "cudaGraphInstantiate");
+    b->key = key;
+  }
+  cuda_check(cudaEventRecord(b->beg, b->st), "event");
+  cuda_check(cudaGraphLaunch(b->ex, b->st), "cudaGraphLaunch");
+  cuda_check(cudaEventRecord(b->end, b->st), "event");
+  for (size_t r = 0; r < R; ++r) cuda_check(cudaEventRecord(b->sys[r]->runEnd, b->st), "event");
+  cuda_check(cudaStreamSynchronize(b->st), "stream synchronize");
+  float ms = 0.f;
+  cuda_check(cudaEventElapsedTime(&ms, b->beg, b->end), "event time");
+  b->lastMs = ms;
+  for (size_t r = 0; r < R; ++r) {
+    espp_system* s = b->sys[r];
+    if (read_err(s) & kErrNlOverflow) {
+      recover_overflow(s, snaps[r]);
+      run_host(s, nsteps);
+      continue;
+    }
+    graph_loop_done(s, nsteps);
+    run_epilogue(s, t0, tRes[r], true);
+  }
 }
 
 double* obs_partials(espp_system* s, int& nb) {
@@ -1605,6 +1739,61 @@ int espp_autotune(espp_system* s, int32_t* best_tpp, double ms[4]) {
     check_err(s);
     s->tpp = pick;
     if (best_tpp) *best_tpp = pick;
+  });
+}
+
+int espp_batch_create(espp_system* const* systems, int32_t n, espp_batch** out) {
+  return guard([&] {
+    if (!systems || !out || n <= 0) raise(ESPP_EINVAL, "need at least one system");
+    std::unique_ptr<espp_batch> b(new espp_batch());
+    for (int32_t k = 0; k < n; ++k) {
+      if (!systems[k]) raise(ESPP_EINVAL, "null system handle");
+      if (k > 0 && systems[k]->device != systems[0]->device)
+        raise(ESPP_EINVAL, "all systems of a batch must live on the same device");
+      for (int32_t m = 0; m < k; ++m)
+        if (systems[m] == systems[k]) raise(ESPP_EINVAL, "a system appears twice in the batch");
+      b->sys.push_back(systems[k]);
+    }
+    b->device = systems[0]->device;
+    cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
+    cuda_check(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking), "stream");
+    cuda_check(cudaEventCreate(&b->beg), "event");
+    cuda_check(cudaEventCreate(&b->end), "event");
+    b->ready.resize(n);
+    for (auto& e : b->ready) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    *out = b.release();
+  });
+}
+
+int espp_batch_destroy(espp_batch* b) {
+  return guard([&] {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->st) cudaStreamSynchronize(b->st);
+    batch_destroy_graph(b);
+    for (auto& e : b->ready) cudaEventDestroy(e);
+    if (b->beg) cudaEventDestroy(b->beg);
+    if (b->end) cudaEventDestroy(b->end);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+  });
+}
+
+int espp_batch_run(espp_batch* b, int64_t nsteps) {
+  return guard([&] {
+    if (!b) raise(ESPP_EINVAL, "null batch handle");
+    if (nsteps < 0) raise(ESPP_EINVAL, "negative step count");
+    cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
+    for (espp_system* s : b->sys)
+      if (s->profiling) raise(ESPP_ESTATE, "profiling is on for a system of the batch");
+    batch_run(b, nsteps);
+  });
+}
+
+int espp_batch_last_run_ms(espp_batch* b, double* ms) {
+  return guard([&] {
+    if (!b) raise(ESPP_EINVAL, "null batch handle");
+    *ms = b->lastMs;
   });
 }
 

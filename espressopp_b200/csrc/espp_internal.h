@@ -69,6 +69,7 @@ struct DevCounters {
   long long resorts;         // re-sorts done in this run
   int flag;                  // re-sort needed this step
   int nnMax;                 // largest neighbour count seen by the Verlet builds
+  double pref1, pref2;       // Langevin prefactors of the step loop (-gamma, sqrt(24 T gamma/dt))
 };
 
 // Pointers and scalars every kernel needs; passed by value.

@@ -784,6 +784,8 @@ __global__ void __launch_bounds__(256) k_integrate(DevView d, IntegrateArgs a) {
   __shared__ double smax[kBlock / 32];
   if (a.fromCounters) {  // uniform over the grid: written by the decide kernel before
     a.step = d.ctr->step;
+    a.pref1 = d.ctr->pref1;
+    a.pref2 = d.ctr->pref2;
     if (d.ctr->remaining == 0) {
       a.do_i1 = 0;
       a.storeFtot = 1;

@@ -142,6 +142,20 @@ ESPP_API int espp_num_resorts(espp_system* s, int64_t* n);
  * int2, resort, other (seconds). */
 ESPP_API int espp_timers(espp_system* s, double t[10]);
 
+/* ---- batched replicas -------------------------------------------------------------
+ * MultiSystem / ParallelTempering on one GPU (src/MultiSystem.py:105-125,
+ * src/ParallelTempering.py:78-203): n independent systems on the same device stepped by
+ * one graph launch that holds one step loop per system, with no dependencies between
+ * them, so the replicas run concurrently and each keeps its own re-sort schedule.  The
+ * systems stay owned by the caller and must outlive the batch; results per system are
+ * identical to espp_run on that system alone. */
+typedef struct espp_batch espp_batch;
+ESPP_API int espp_batch_create(espp_system* const* systems, int32_t n, espp_batch** out);
+ESPP_API int espp_batch_destroy(espp_batch* b);
+ESPP_API int espp_batch_run(espp_batch* b, int64_t nsteps);
+/* Device time of the last espp_batch_run's graph launch (ms). */
+ESPP_API int espp_batch_last_run_ms(espp_batch* b, double* ms);
+
 /* ---- observables (FP64) --------------------------------------------------------
  * Interaction::computeEnergy / computeVirial / computeVirialTensor
  * (VerletListInteractionTemplate.hpp:201-331, FixedPairListInteractionTemplate.hpp:

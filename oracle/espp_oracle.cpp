@@ -1043,6 +1043,36 @@ int espp_autotune(espp_system* s, int32_t* best, double ms[4]) {
   return ESPP_OK;
 }
 
+struct espp_batch {
+  std::vector<espp_system*> sys;
+};
+
+int espp_batch_create(espp_system* const* systems, int32_t n, espp_batch** out) {
+  if (!systems || !out || n <= 0) return fail(ESPP_EINVAL, "need at least one system");
+  espp_batch* b = new espp_batch();
+  b->sys.assign(systems, systems + n);
+  *out = b;
+  return ESPP_OK;
+}
+
+int espp_batch_destroy(espp_batch* b) {
+  delete b;
+  return ESPP_OK;
+}
+
+int espp_batch_run(espp_batch* b, int64_t nsteps) {
+  for (espp_system* s : b->sys) {
+    int rc = run(s, nsteps);
+    if (rc) return rc;
+  }
+  return ESPP_OK;
+}
+
+int espp_batch_last_run_ms(espp_batch*, double* ms) {
+  *ms = 0.0;
+  return ESPP_OK;
+}
+
 // Test hook: Philox outputs, so the tests can pin the generator on known answers.
 int espp_oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
   U4 c;

@@ -242,3 +242,90 @@ def test_capforce_and_capped_lj(mode, cap):
         assert np.max(np.linalg.norm(f, axis=1)) <= cap * (1 + 1e-12)
     else:
         assert np.all(np.abs(f) <= np.array(cap) * (1 + 1e-12))
+
+
+def _replica(lib, n_side, rho, T, seed, prec):
+    pos, box = lattice(n_side, rho, 0.05, seed=seed)
+    vel = mb_velocities(len(pos), T, seed=seed + 100)
+    s = _lj_setup(lib, prec, np.arange(len(pos)), pos, vel, box, seed=seed)
+    s.integrator(0.005)
+    s.langevin(1.0, T)
+    return s
+
+
+@pytest.mark.parametrize("prec", [_abi.PREC_FP64, _abi.PREC_MIXED])
+def test_batch_run_matches_individual_runs(prec):
+    """One graph launch stepping 4 replicas of different sizes and temperatures gives
+    each replica exactly the trajectory of espp_run on it alone."""
+    import ctypes
+    specs = [(9, 0.8442, 0.8, 1), (12, 0.8442, 1.2, 2), (14, 0.8, 1.6, 3), (10, 0.85, 2.0, 4)]
+    lib = cuda_lib()
+    solo = [_replica(lib, *sp, prec) for sp in specs]
+    for s in solo:
+        s.run(40)
+        s.run(25)
+    rep = [_replica(lib, *sp, prec) for sp in specs]
+    arr = (ctypes.c_void_p * len(rep))(*[s.h.value for s in rep])
+    b = ctypes.c_void_p()
+    _abi.call(lib, "espp_batch_create", arr, len(rep), ctypes.byref(b))
+    try:
+        _abi.call(lib, "espp_batch_run", b, 40)
+        _abi.call(lib, "espp_batch_run", b, 25)
+    finally:
+        lib.espp_batch_destroy(b)
+    for a, c, sp in zip(solo, rep, specs):
+        ids = np.arange(sp[0] ** 3)
+        pa, pc = a.particles(ids), c.particles(ids)
+        for k in range(4):
+            assert np.array_equal(pa[k], pc[k])
+        assert a.num_resorts() == c.num_resorts() and a.step() == c.step() == 65
+        assert a.builds() == c.builds()
+
+
+def test_parallel_tempering_api_runs_and_exchanges():
+    import random
+    import espressopp_b200 as espressopp
+    pt = espressopp.ParallelTempering(NumberOfSystems=4, RNG=random.Random(7))
+    for i in range(pt.getNumberOfSystems()):
+        pt.startDefiningSystem(i)
+        x, y, z, Lx, Ly, Lz = espressopp.tools.lattice.createCubic(1000 + 200 * i, 0.8442,
+                                                                    perfect=False)
+        system = espressopp.System()
+        system.rng = espressopp.esutil.RNG(100 + i)
+        system.bc = espressopp.bc.OrthorhombicBC(system.rng, (Lx, Ly, Lz))
+        system.skin = 0.3
+        cg = espressopp.tools.decomp.cellGrid((Lx, Ly, Lz), (1, 1, 1), 2.5, 0.3)
+        system.storage = espressopp.storage.DomainDecomposition(system, (1, 1, 1), cg)
+        system.storage.addParticles([[k, espressopp.Real3D(x[k], y[k], z[k])]
+                                     for k in range(len(x))], "id", "pos")
+        system.storage.decompose()
+        vl = espressopp.VerletList(system, cutoff=2.5)
+        lj = espressopp.interaction.VerletListLennardJones(vl)
+        lj.setPotential(0, 0, espressopp.interaction.LennardJones(1.0, 1.0, 2.5, 0.0))
+        system.addInteraction(lj)
+        integ = espressopp.integrator.VelocityVerlet(system)
+        integ.dt = 0.005
+        lang = espressopp.integrator.LangevinThermostat(system)
+        lang.gamma = 1.0
+        lang.temperature = 0.7 + 0.4 * i
+        integ.addExtension(lang)
+        pt.setIntegrator(integ, lang)
+        pt.setAnalysisE(lj)
+        pt.setAnalysisT(espressopp.analysis.Temperature(system))
+        pt.setAnalysisNPart(espressopp.analysis.NPart(system))
+        pt.endDefiningSystem(i)
+    for _ in range(3):
+        pt.run(50)
+        before = [th.temperature for th in pt._thermostat]
+        measured = pt._multisystem.runAnalysisTemperature()
+        decisions = pt.exchange()
+        assert len(decisions) >= 1
+        # the reference gives each exchanged thermostat the other replica's measured T
+        for m, n, _, _, ok in decisions:
+            if ok:
+                assert pt._thermostat[n].temperature == pytest.approx(measured[m], rel=1e-12)
+                assert pt._thermostat[m].temperature == pytest.approx(measured[n], rel=1e-12)
+            else:
+                assert pt._thermostat[n].temperature == before[n]
+    temps = pt._multisystem.runAnalysisTemperature()
+    assert all(0.05 < t < 10.0 for t in temps)
