@@ -437,18 +437,27 @@ __global__ void __launch_bounds__(128) k_build_nl(DevView d, double cutsq) {
         rj.x += (seg - 1) * hx;
         rj.y += oy * hy;
         rj.z += oz * hz;
-        for (int m = 0; m < ni; ++m) {
-          const float4 ri = s_xi[wib][m];
-          const float dx = ri.x - rj.x, dy = ri.y - rj.y, dz = ri.z - rj.z;
-          const float r2 = dx * dx + dy * dy + dz * dz;
-          const bool self = j == g + m;
-          const unsigned bin = __ballot_sync(0xffffffffu, r2 < lo && !self);
-          const unsigned bbd = __ballot_sync(0xffffffffu, r2 >= lo && r2 <= hi && !self);
-          if (lane == m) {
-            s_in[wib][q][m] = bin;
-            s_bd[wib][q][m] = bbd;
-          }
+        // two particles per iteration (independent chains); lane m keeps the masks of
+        // particle m in registers and stores them once per chunk
+        unsigned my_in = 0u, my_bd = 0u;
+        const int jl = j - g;  // candidate index relative to the group (self test)
+        for (int m = 0; m < ni; m += 2) {
+          const int m1 = min(m + 1, ni - 1);
+          const float4 ra = s_xi[wib][m];
+          const float4 rb = s_xi[wib][m1];
+          const float ax = ra.x - rj.x, ay = ra.y - rj.y, az = ra.z - rj.z;
+          const float bx = rb.x - rj.x, by = rb.y - rj.y, bz = rb.z - rj.z;
+          const float a2 = ax * ax + ay * ay + az * az;
+          const float b2 = bx * bx + by * by + bz * bz;
+          const unsigned ina = __ballot_sync(0xffffffffu, a2 < lo && jl != m);
+          const unsigned bda = __ballot_sync(0xffffffffu, a2 >= lo && a2 <= hi && jl != m);
+          const unsigned inb = __ballot_sync(0xffffffffu, b2 < lo && jl != m1);
+          const unsigned bdb = __ballot_sync(0xffffffffu, b2 >= lo && b2 <= hi && jl != m1);
+          my_in = lane == m ? ina : (lane == m1 ? inb : my_in);
+          my_bd = lane == m ? bda : (lane == m1 ? bdb : my_bd);
         }
+        s_in[wib][q][lane] = my_in;
+        s_bd[wib][q][lane] = my_bd;
       }
       __syncwarp();
       // ---- phase B: each lane appends its partners of these chunks in bit order
