@@ -348,26 +348,113 @@ __device__ __noinline__ bool exact_pair_test(const double* __restrict__ x, size_
   return !(d2 > cutsq);
 }
 
-// One warp per cell, in two phases per group of up to 32 particles of the cell.
-//  A: the lanes hold candidates: for each of the 9 rows (oy, oz) of the reference's
-//     27-cell stencil, the particles of the row's three x-cells are taken 32 at a time
-//     (one "chunk"), and every particle i of the group is tested against the whole chunk
-//     in FP32 on cell-relative coordinates.  One ballot per (i, chunk) gives a 32-bit
-//     mask of the candidates inside the cutoff, a second one the candidates within a
-//     relative band of 2e-5 around it; both go to shared memory.
-//  B: the lanes hold the group's particles: each lane walks its masks in chunk order,
-//     settles borderline bits with the reference's own FP64 arithmetic (exact_pair_test)
-//     and appends the partners in bit order.
-// Each list is therefore the reference's pair set (VerletList.cpp:274-450) in a
-// deterministic order (row, chunk, lane).
-constexpr int kMaxChunks = 24;  // chunks per batch of the two phases
+// Packed FP32 pairs (sm_100 f32x2 arithmetic): two particles' coordinates in one 64-bit
+// register, low half first.
+__device__ __forceinline__ unsigned long long f2_pack(float lo, float hi) {
+  return ((unsigned long long)__float_as_uint(hi) << 32) | __float_as_uint(lo);
+}
+__device__ __forceinline__ unsigned long long f2_sub(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b,
+                                                     unsigned long long c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
 
+// Squared FP32 distances of two group particles (packed xi, yi, zi) to one candidate
+// (packed twice in cx, cy, cz), packed the same way.  The fast test and the borderline
+// pass both call this, so a candidate is classified the same way by both.
+__device__ __forceinline__ unsigned long long pair_r2(const float2* __restrict__ sp,
+                                                      unsigned long long cx,
+                                                      unsigned long long cy,
+                                                      unsigned long long cz) {
+  const float2 px = sp[0], py = sp[1], pz = sp[2];
+  const unsigned long long dx = f2_sub(f2_pack(px.x, px.y), cx);
+  const unsigned long long dy = f2_sub(f2_pack(py.x, py.y), cy);
+  const unsigned long long dz = f2_sub(f2_pack(pz.x, pz.y), cz);
+  return f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
+}
+__device__ __forceinline__ float f2_lo(unsigned long long v) { return __uint_as_float((unsigned)v); }
+__device__ __forceinline__ float f2_hi(unsigned long long v) {
+  return __uint_as_float((unsigned)(v >> 32));
+}
+
+// Appends candidate j (held by this lane) to the list of the particle whose first block
+// starts at nl_i when `in` is set: the lanes of one ballot write consecutive slots in
+// lane order.
+__device__ __forceinline__ void nl_append(int* __restrict__ nl_i, unsigned cap8, int K, int cnt,
+                                          unsigned mask, bool in, int j) {
+  const int k = cnt + __popc(mask & ((1u << (threadIdx.x & 31)) - 1u));
+  if (in && k < K) nl_i[(size_t)(unsigned)(k >> 3) * cap8 + (unsigned)(k & 7)] = j;
+}
+
+// The fast tests of one chunk against the group, four group members per step (two
+// packed pairs, independent chains).  SELF: the chunk may hold group members (centre
+// row), so the candidate equal to the tested particle is skipped.  Returns whether any
+// candidate came near the cutoff (a superset of the borderline band).
+template <bool SELF, bool EXCL>
+__device__ __forceinline__ bool chunk_fast(const DevView& d, const float2 (*sxp)[3],
+                                           const int64_t* sid, int ni, int* __restrict__ nlg,
+                                           unsigned cap8, int K, int j, int jl, int64_t idj,
+                                           unsigned long long cxx, unsigned long long cyy,
+                                           unsigned long long czz, float lo,
+                                           unsigned long long mid2, float hw, int (&cnt)[32]) {
+  bool band = false;
+#pragma unroll
+  for (int p4 = 0; p4 < 8; ++p4) {
+    if (4 * p4 >= ni) break;
+    const unsigned long long r01 = pair_r2(sxp[2 * p4], cxx, cyy, czz);
+    const unsigned long long r23 = pair_r2(sxp[2 * p4 + 1], cxx, cyy, czz);
+    const unsigned long long t01 = f2_sub(r01, mid2), t23 = f2_sub(r23, mid2);
+    band |= (fabsf(f2_lo(t01)) <= hw) | (fabsf(f2_hi(t01)) <= hw) |
+            (fabsf(f2_lo(t23)) <= hw) | (fabsf(f2_hi(t23)) <= hw);
+    const float r2[4] = {f2_lo(r01), f2_hi(r01), f2_lo(r23), f2_hi(r23)};
+    bool in[4];
+    unsigned m[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      in[u] = r2[u] < lo && (!SELF || jl != 4 * p4 + u);
+      if (EXCL && in[u] && is_excluded(d, sid[4 * p4 + u], idj)) in[u] = false;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) m[u] = __ballot_sync(0xffffffffu, in[u]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      nl_append(nlg + 8 * (4 * p4 + u), cap8, K, cnt[4 * p4 + u], m[u], in[u], j);
+      cnt[4 * p4 + u] += __popc(m[u]);
+    }
+  }
+  return band;
+}
+
+// One warp per cell and group of up to 32 of its particles.  The lanes hold candidates:
+// for each of the 9 rows (oy, oz) of the reference's 27-cell stencil the particles of
+// the row's three x-cells are taken 32 at a time (a "chunk").  Every group particle is
+// tested against the chunk in FP32 on cell-relative coordinates, two group particles
+// per packed f32x2 operation; one ballot per (particle, chunk) gives the candidates
+// inside the cutoff, and those lanes write their index straight into the particle's
+// list at the slot the ballot's prefix count gives.  Candidates within a relative band
+// of 2e-5 around the cutoff are left out of that ballot; a chunk that has any is
+// revisited and those are decided by the reference's own FP64 arithmetic
+// (exact_pair_test) and appended after the chunk's other partners.
+// Each list is therefore the reference's pair set (VerletList.cpp:274-450) in a
+// deterministic order.  The group's list counts live in registers (warp-uniform),
+// unrolled over the 32 possible group members.
 template <bool EXCL>
 __global__ void __launch_bounds__(128) k_build_nl(DevView d, double cutsq) {
   const ParticleArrays a = d.pa[0];
-  __shared__ float4 s_xi[4][32];
-  __shared__ unsigned s_in[4][kMaxChunks][32];
-  __shared__ unsigned s_bd[4][kMaxChunks][32];
+  __shared__ float2 s_xp[4][16][3];  // group particles (2p, 2p+1): x pair, y pair, z pair
+  __shared__ int64_t s_id[4][32];
+  __shared__ int s_cnt[4][32];
   __shared__ int s_row[4][9][8];  // st0, ct0, st1, ct1, st2, ct2, first chunk, chunks
   const int wib = threadIdx.x >> 5;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -378,11 +465,17 @@ __global__ void __launch_bounds__(128) k_build_nl(DevView d, double cutsq) {
   const int s0 = d.cellStart[c], s1 = d.cellStart[c + 1];
   if (s0 == s1) return;
   const float lo = (float)(cutsq * (1.0 - 2e-5)), hi = (float)(cutsq * (1.0 + 2e-5));
+  // the fast path's trigger for the borderline pass: |r2 - mid| <= hw, 1.5 x wider than
+  // the band [lo, hi] so that rounding of r2 - mid cannot hide a borderline candidate
+  const float mid = (float)cutsq, hw = (float)(cutsq * 3e-5);
+  const unsigned long long mid2 = f2_pack(mid, mid);
   const float hx = (float)d.cellSize[0], hy = (float)d.cellSize[1], hz = (float)d.cellSize[2];
   const float4* __restrict__ xr = d.xrel;
+  const int K = d.K;
+  const unsigned cap8 = (unsigned)d.cap << 3;
+  int* __restrict__ nl = d.nl;
   const int cxm = cx == 0 ? d.nc[0] - 1 : cx - 1;
   const int cxp = cx == d.nc[0] - 1 ? 0 : cx + 1;
-  // the 9 rows of the stencil: three x-cells each, as (start, count) segments
   if (lane < 9) {
     const int oz = lane / 3 - 1, oy = lane % 3 - 1;
     int ncy = cy + oy, ncz = cz + oz;
@@ -411,110 +504,92 @@ __global__ void __launch_bounds__(128) k_build_nl(DevView d, double cutsq) {
   __syncwarp();
   for (int g = s0; g < s1; g += 32) {
     const int ni = min(32, s1 - g);
-    if (lane < ni) s_xi[wib][lane] = xr[g + lane];
-    const int i = g + lane;
-    const int64_t idi = (EXCL && lane < ni) ? a.id[i] : 0;
-    int cnt = 0;
-    const size_t cap = d.cap;
-    __syncwarp();
-    int r = 0;  // row of the first chunk of the batch
-    for (int qb = 0; qb < nchunks; qb += kMaxChunks) {
-      const int nq = min(kMaxChunks, nchunks - qb);
-      // ---- phase A: masks for chunks qb .. qb + nq
-      int rr = r;
-      for (int q = 0; q < nq; ++q) {
-        while (qb + q >= s_row[wib][rr][6] + s_row[wib][rr][7]) ++rr;
-        const int cb = (qb + q - s_row[wib][rr][6]) << 5;
-        const int oz = rr / 3 - 1, oy = rr % 3 - 1;
-        const int st0 = s_row[wib][rr][0], ct0 = s_row[wib][rr][1];
-        const int st1 = s_row[wib][rr][2], ct1 = s_row[wib][rr][3];
-        const int st2 = s_row[wib][rr][4], ct2 = s_row[wib][rr][5];
-        const int t = cb + lane;
-        const bool validj = t < ct0 + ct1 + ct2;
-        const int seg = t < ct0 ? 0 : (t < ct0 + ct1 ? 1 : 2);
-        const int j = !validj ? -1 : (seg == 0 ? st0 + t : (seg == 1 ? st1 + t - ct0 : st2 + t - ct0 - ct1));
-        float4 rj = validj ? xr[j] : make_float4(1e30f, 1e30f, 1e30f, 0.f);
-        rj.x += (seg - 1) * hx;
-        rj.y += oy * hy;
-        rj.z += oz * hz;
-        // two particles per iteration (independent chains); lane m keeps the masks of
-        // particle m in registers and stores them once per chunk
-        unsigned my_in = 0u, my_bd = 0u;
-        const int jl = j - g;  // candidate index relative to the group (self test)
-        for (int m = 0; m < ni; m += 2) {
-          const int m1 = min(m + 1, ni - 1);
-          const float4 ra = s_xi[wib][m];
-          const float4 rb = s_xi[wib][m1];
-          const float ax = ra.x - rj.x, ay = ra.y - rj.y, az = ra.z - rj.z;
-          const float bx = rb.x - rj.x, by = rb.y - rj.y, bz = rb.z - rj.z;
-          const float a2 = ax * ax + ay * ay + az * az;
-          const float b2 = bx * bx + by * by + bz * bz;
-          const unsigned ina = __ballot_sync(0xffffffffu, a2 < lo && jl != m);
-          const unsigned bda = __ballot_sync(0xffffffffu, a2 >= lo && a2 <= hi && jl != m);
-          const unsigned inb = __ballot_sync(0xffffffffu, b2 < lo && jl != m1);
-          const unsigned bdb = __ballot_sync(0xffffffffu, b2 >= lo && b2 <= hi && jl != m1);
-          my_in = lane == m ? ina : (lane == m1 ? inb : my_in);
-          my_bd = lane == m ? bda : (lane == m1 ? bdb : my_bd);
-        }
-        s_in[wib][q][lane] = my_in;
-        s_bd[wib][q][lane] = my_bd;
-      }
-      __syncwarp();
-      // ---- phase B: each lane appends its partners of these chunks in bit order
-      if (lane < ni) {
-        rr = r;
-        for (int q = 0; q < nq; ++q) {
-          while (qb + q >= s_row[wib][rr][6] + s_row[wib][rr][7]) ++rr;
-          unsigned m_in = s_in[wib][q][lane];
-          const unsigned m_bd = s_bd[wib][q][lane];
-          if (!(m_in | m_bd)) continue;
-          const int cb = (qb + q - s_row[wib][rr][6]) << 5;
-          const int st0 = s_row[wib][rr][0], ct0 = s_row[wib][rr][1];
-          const int st1 = s_row[wib][rr][2], ct1 = s_row[wib][rr][3];
-          const int st2 = s_row[wib][rr][4];
-          if (__builtin_expect(m_bd != 0u, 0)) {
-            const int oz = rr / 3 - 1, oy = rr % 3 - 1;
-            const int ncy = cy + oy, ncz = cz + oz;
-            const int wy = ncy < 0 ? -1 : (ncy >= d.nc[1] ? 1 : 0);
-            const int wz = ncz < 0 ? -1 : (ncz >= d.nc[2] ? 1 : 0);
-            unsigned b = m_bd;
-            while (b) {
-              const int bit = __ffs(b) - 1;
-              b &= b - 1;
-              const int t = cb + bit;
-              const int seg = t < ct0 ? 0 : (t < ct0 + ct1 ? 1 : 2);
-              const int ox = seg - 1;
-              const int j = seg == 0 ? st0 + t : (seg == 1 ? st1 + t - ct0 : st2 + t - ct0 - ct1);
-              const int wx = seg == 0 ? (cx == 0 ? -1 : 0) : (seg == 2 ? (cx == d.nc[0] - 1 ? 1 : 0) : 0);
-              const bool fwd = oz > 0 || (oz == 0 && (oy > 0 || (oy == 0 && ox > 0)));
-              if (exact_pair_test(a.x, d.cap, i, j, fwd, wx * d.L[0], wy * d.L[1], wz * d.L[2],
-                                  cutsq))
-                m_in |= 1u << bit;
-            }
-          }
-          while (m_in) {
-            const int bit = __ffs(m_in) - 1;
-            m_in &= m_in - 1;
-            const int t = cb + bit;
-            const int j = t < ct0 ? st0 + t : (t < ct0 + ct1 ? st1 + t - ct0 : st2 + t - ct0 - ct1);
-            if (EXCL && is_excluded(d, idi, a.id[j])) continue;
-            if (cnt < d.K) d.nl[nl_index(cnt, i, cap)] = j;
-            ++cnt;
-          }
-        }
-      }
-      r = rr;
-      __syncwarp();
+    {
+      const float4 r = lane < ni ? xr[g + lane] : make_float4(1e18f, 1e18f, 1e18f, 0.f);
+      float* sp = reinterpret_cast<float*>(&s_xp[wib][lane >> 1][0]) + (lane & 1);
+      sp[0] = r.x;
+      sp[2] = r.y;
+      sp[4] = r.z;
+      if (EXCL) s_id[wib][lane] = lane < ni ? a.id[g + lane] : -1;
     }
+    __syncwarp();
+    int cnt[32];
+#pragma unroll
+    for (int m = 0; m < 32; ++m) cnt[m] = 0;
+    int rr = 0;
+    for (int q = 0; q < nchunks; ++q) {
+      while (q >= s_row[wib][rr][6] + s_row[wib][rr][7]) ++rr;
+      const int cb = (q - s_row[wib][rr][6]) << 5;
+      const int oz = rr / 3 - 1, oy = rr % 3 - 1;
+      const int st0 = s_row[wib][rr][0], ct0 = s_row[wib][rr][1];
+      const int st1 = s_row[wib][rr][2], ct1 = s_row[wib][rr][3];
+      const int st2 = s_row[wib][rr][4], ct2 = s_row[wib][rr][5];
+      const int t = cb + lane;
+      const bool validj = t < ct0 + ct1 + ct2;
+      const int seg = t < ct0 ? 0 : (t < ct0 + ct1 ? 1 : 2);
+      const int j = !validj ? -1 : (seg == 0 ? st0 + t : (seg == 1 ? st1 + t - ct0 : st2 + t - ct0 - ct1));
+      // invalid lanes sit at -1e18 and padding group members at +1e18: no pair among
+      // them comes near the cutoff, and no square overflows FP32
+      float4 rj = validj ? xr[j] : make_float4(-1e18f, -1e18f, -1e18f, 0.f);
+      rj.x += (seg - 1) * hx;
+      rj.y += oy * hy;
+      rj.z += oz * hz;
+      const unsigned long long cxx = f2_pack(rj.x, rj.x), cyy = f2_pack(rj.y, rj.y);
+      const unsigned long long czz = f2_pack(rj.z, rj.z);
+      const int jl = j - g;  // the group member this candidate is, if any (self test)
+      const int64_t idj = (EXCL && validj) ? a.id[j] : -2;
+      int* __restrict__ nlg = nl + ((size_t)g << 3);
+      const bool band =
+          (oy == 0 && oz == 0)
+              ? chunk_fast<true, EXCL>(d, s_xp[wib], s_id[wib], ni, nlg, cap8, K, j, jl, idj,
+                                       cxx, cyy, czz, lo, mid2, hw, cnt)
+              : chunk_fast<false, EXCL>(d, s_xp[wib], s_id[wib], ni, nlg, cap8, K, j, jl, idj,
+                                        cxx, cyy, czz, lo, mid2, hw, cnt);
+      if (__builtin_expect(__any_sync(0xffffffffu, band), 0)) {
+        // borderline candidates of this chunk: the reference's FP64 test decides
+#pragma unroll
+        for (int m = 0; m < 32; ++m)
+          if (lane == m) s_cnt[wib][m] = cnt[m];
+        __syncwarp();
+        const int ncy = cy + oy, ncz = cz + oz;
+        const int wy = ncy < 0 ? -1 : (ncy >= d.nc[1] ? 1 : 0);
+        const int wz = ncz < 0 ? -1 : (ncz >= d.nc[2] ? 1 : 0);
+        const int ox = seg - 1;
+        const int wx = seg == 0 ? (cx == 0 ? -1 : 0) : (seg == 2 ? (cx == d.nc[0] - 1 ? 1 : 0) : 0);
+        const bool fwd = oz > 0 || (oz == 0 && (oy > 0 || (oy == 0 && ox > 0)));
+        for (int m = 0; m < ni; ++m) {
+          const unsigned long long rp = pair_r2(s_xp[wib][m >> 1], cxx, cyy, czz);
+          const float r2 = (m & 1) ? f2_hi(rp) : f2_lo(rp);
+          const bool bd = r2 >= lo && r2 <= hi && jl != m;
+          if (!__any_sync(0xffffffffu, bd)) continue;
+          bool in = bd && exact_pair_test(a.x, d.cap, g + m, j, fwd, wx * d.L[0], wy * d.L[1],
+                                          wz * d.L[2], cutsq);
+          if (EXCL && in && is_excluded(d, s_id[wib][m], idj)) in = false;
+          const unsigned mm = __ballot_sync(0xffffffffu, in);
+          const int c0 = s_cnt[wib][m];
+          nl_append(nlg + 8 * m, cap8, K, c0, mm, in, j);
+          __syncwarp();
+          if (lane == 0) s_cnt[wib][m] = c0 + __popc(mm);
+          __syncwarp();
+        }
+#pragma unroll
+        for (int m = 0; m < 32; ++m) cnt[m] = s_cnt[wib][m];
+        __syncwarp();
+      }
+    }
+    int my = 0;
+#pragma unroll
+    for (int m = 0; m < 32; ++m) my = lane == m ? cnt[m] : my;
     if (lane < ni) {
-      if (cnt > d.K) atomicOr(d.err, kErrNlOverflow);
-      const int cc = min(cnt, d.K);
+      const int i = g + lane;
+      if (my > K) atomicOr(d.err, kErrNlOverflow);
+      const int cc = min(my, K);
       d.nn[i] = cc;
       // pad to a multiple of 8 with the particle itself (r^2 = 0, masked by the force
       // kernels) so that batches of 8 need no bounds checks; K is a multiple of 8
-      for (int k = cc; k < ((cc + 7) & ~7); ++k) d.nl[nl_index(k, i, cap)] = i;
+      for (int k = cc; k < ((cc + 7) & ~7); ++k) nl[nl_index(k, i, d.cap)] = i;
     }
-    const int wmax = __reduce_max_sync(0xffffffffu, lane < ni ? cnt : 0);
+    const int wmax = __reduce_max_sync(0xffffffffu, lane < ni ? my : 0);
     if (lane == 0 && wmax > 0) atomicMax(&d.ctr->nnMax, wmax);
     __syncwarp();
   }
