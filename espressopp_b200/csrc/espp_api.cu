@@ -18,6 +18,7 @@
 #include <memory>
 #include <mutex>
 #include <new>
+#include <cstdio>
 #include <string>
 #include <unordered_map>
 #include <utility>
@@ -25,6 +26,7 @@
 
 #include "../../include/espp_b200.h"
 #include "espp_internal.h"
+#include "espp_tab.h"
 
 using namespace espp;
 
@@ -155,6 +157,19 @@ struct espp_system {
   bool lj_any = false;
   FENEParams fene{};
   std::vector<std::pair<int64_t, int64_t>> bonds;
+  // interaction::Tabulated: specifications by slot (type pair key t1*kMaxTypes+t2 with
+  // t1 <= t2, or kTabBondKey for the fixed pair list), built into one coefficient array
+  struct TabSpec {
+    int itype;
+    std::vector<double> r, e, f;
+    double rc, shift;
+  };
+  std::map<int, TabSpec> tabSpecs;
+  TabDesc* d_tabs = nullptr;
+  double* d_tabCoef = nullptr;
+  int32_t* d_tabPair = nullptr;
+  int tabNT = 0;
+  int tabBond = -1;
 
   // integrator
   double dt = 0.005;
@@ -215,6 +230,11 @@ struct espp_system {
     for (int k = 0; k < kMaxTypes * kMaxTypes; ++k)
       if (lj.p[k].set && lj.p[k].caprad > 0) capped = 1;
     d.ljCapped = capped;
+    d.tabs = d_tabs;
+    d.tabCoef = d_tabCoef;
+    d.tabPair = d_tabPair;
+    d.tabNT = tabNT;
+    d.tabBond = tabBond;
     d.err = err;
     d.ctr = ctr;
     return d;
@@ -533,11 +553,75 @@ void upload_lj(espp_system* s) {
   s->lj.single = (nt == 1 && compact[0].set) ? 1 : 0;
 }
 
-void forces(espp_system* s) {
-  if (s->has_vl && s->lj_any && !s->listValid) build_list(s);
+constexpr int kTabBondKey = -1;
+
+// Builds every table of the system into one coefficient array and uploads it with the
+// descriptors and the type-pair map.
+void upload_tabs(espp_system* s) {
+  std::vector<TabDesc> descs;
+  std::vector<double> coef;
+  int nt = 0;
+  for (auto& kv : s->tabSpecs)
+    if (kv.first != kTabBondKey) nt = std::max(nt, kv.first % kMaxTypes + 1);
+  nt = nt > 0 ? std::max(nt, s->maxType + 1) : 0;
+  std::vector<int32_t> pairMap((size_t)nt * nt, -1);
+  int bondIdx = -1;
+  for (auto& kv : s->tabSpecs) {
+    const espp_system::TabSpec& t = kv.second;
+    TabDesc desc;
+    const char* msg = build_table(t.itype, (int)t.r.size(), t.r.data(), t.e.data(),
+                                  t.f.data(), desc, coef);
+    if (msg) raise(ESPP_EINVAL, msg);
+    desc.rcsq = t.rc * t.rc;
+    desc.shift = t.shift;
+    const int idx = (int)descs.size();
+    descs.push_back(desc);
+    if (kv.first == kTabBondKey) {
+      bondIdx = idx;
+    } else {
+      const int t1 = kv.first / kMaxTypes, t2 = kv.first % kMaxTypes;
+      pairMap[(size_t)t1 * nt + t2] = idx;
+      pairMap[(size_t)t2 * nt + t1] = idx;
+    }
+  }
+  dfree(s->d_tabs);
+  dfree(s->d_tabCoef);
+  dfree(s->d_tabPair);
+  if (!descs.empty()) {
+    s->d_tabs = dalloc<TabDesc>(descs.size());
+    s->d_tabCoef = dalloc<double>(coef.size());
+    cuda_check(cudaMemcpy(s->d_tabs, descs.data(), sizeof(TabDesc) * descs.size(),
+                          cudaMemcpyHostToDevice), "upload");
+    cuda_check(cudaMemcpy(s->d_tabCoef, coef.data(), sizeof(double) * coef.size(),
+                          cudaMemcpyHostToDevice), "upload");
+  }
+  if (nt > 0) {
+    s->d_tabPair = dalloc<int32_t>(pairMap.size());
+    cuda_check(cudaMemcpy(s->d_tabPair, pairMap.data(), sizeof(int32_t) * pairMap.size(),
+                          cudaMemcpyHostToDevice), "upload");
+  }
+  s->tabNT = nt;
+  s->tabBond = bondIdx;
+}
+
+// whether a pair interaction runs on the Verlet list
+bool pair_any(const espp_system* s) { return s->lj_any || s->tabNT > 0; }
+
+// Main pair + FENE kernel (list counts zeroed when no LJ pair is set), then the
+// tabulated pair and bond forces added to its output.
+void launch_all_forces(espp_system* s, cudaStream_t st) {
   DevView d = s->view();
-  if (!s->has_vl || !s->lj_any) d.nn = s->nnZero;  // no pair term: bonds only
-  launch_forces(d, s->precision == ESPP_PREC_MIXED, s->fene, s->tpp, s->st);
+  const bool mixed = s->precision == ESPP_PREC_MIXED;
+  DevView dm = d;
+  if (!s->has_vl || !s->lj_any) dm.nn = s->nnZero;  // no LJ term: bonds only
+  launch_forces(dm, mixed, s->fene, s->tpp, st);
+  if (!s->has_vl) d.tabNT = 0;
+  launch_force_tab(d, mixed, st);
+}
+
+void forces(espp_system* s) {
+  if (s->has_vl && pair_any(s) && !s->listValid) build_list(s);
+  launch_all_forces(s, s->st);
 }
 
 
@@ -668,11 +752,7 @@ void launch_rebuild_kernels(espp_system* s, cudaStream_t st) {
   }
 }
 
-void launch_force_kernel(espp_system* s, cudaStream_t st) {
-  DevView d = s->view();
-  if (!s->has_vl || !s->lj_any) d.nn = s->nnZero;
-  launch_forces(d, s->precision == ESPP_PREC_MIXED, s->fene, s->tpp, st);
-}
+void launch_force_kernel(espp_system* s, cudaStream_t st) { launch_all_forces(s, st); }
 
 // Adds to graph g one WHILE node (no dependencies) running the step loop of s:
 // WHILE(remaining) { decide; IF(re-sort) { fold, bin, sort, gather, swap, id map, list };
@@ -1079,6 +1159,12 @@ void observable(espp_system* s, int which, int energy, double out[7]) {
   } else if (which == ESPP_IA_FENE) {
     if (!s->fene.on) return;
     launch_fene_observables(d, s->fene, part, nb, s->obs, energy, s->st);
+  } else if (which == ESPP_IA_TAB_PAIR) {
+    if (!s->has_vl || s->tabNT == 0) return;
+    launch_tab_observables(d, 0, part, nb, s->obs, energy, s->st);
+  } else if (which == ESPP_IA_TAB_BOND) {
+    if (s->tabBond < 0) return;
+    launch_tab_observables(d, 1, part, nb, s->obs, energy, s->st);
   } else {
     raise(ESPP_EINVAL, "unknown interaction kind");
   }
@@ -1134,6 +1220,9 @@ void destroy(espp_system* s) {
   dfree(s->partials);
   dfree(s->d_lj);
   dfree(s->d_ljf);
+  dfree(s->d_tabs);
+  dfree(s->d_tabCoef);
+  dfree(s->d_tabPair);
   dfree(s->stIds);
   dfree(s->stPos);
   dfree(s->stVel);
@@ -1583,6 +1672,86 @@ int espp_fene_set(espp_system* s, double K, double r0, double rmax, double rc, d
     s->fene.rmaxsq = rmax * rmax;
     s->fene.rcsq = rc * rc;
     s->fene.shift = shift;
+  });
+}
+
+int espp_tab_read(const char* path, int64_t cap, double* r, double* energy, double* force,
+                  int64_t* n) {
+  return guard([&] {
+    if (!path || !n) raise(ESPP_EINVAL, "null argument");
+    // InterpolationLinear::readFile: fgets + sscanf("%lg %lg %lg"), other lines skipped
+    FILE* fp = std::fopen(path, "r");
+    if (!fp) raise(ESPP_EINVAL, std::string("could not open file ") + path);
+    char line[1024];
+    int64_t cnt = 0;
+    while (std::fgets(line, sizeof(line), fp)) {
+      double a, b, c;
+      if (std::sscanf(line, "%lg %lg %lg", &a, &b, &c) < 3) continue;
+      if (cnt < cap) {
+        if (r) r[cnt] = a;
+        if (energy) energy[cnt] = b;
+        if (force) force[cnt] = c;
+      }
+      ++cnt;
+    }
+    std::fclose(fp);
+    *n = cnt;
+    if (cnt < 2) raise(ESPP_EINVAL, "illegal file for tabulated potential");
+  });
+}
+
+int espp_tab_eval(int32_t itype, int64_t n, const double* r, const double* e, const double* f,
+                  int64_t m, const double* x, double* energy, double* force) {
+  return guard([&] {
+    if (!r || !e || !f || (m > 0 && !x)) raise(ESPP_EINVAL, "null argument");
+    if (n > 0x7fffffff) raise(ESPP_ERANGE, "table too long");
+    TabDesc t;
+    std::vector<double> coef;
+    if (const char* msg = build_table(itype, (int)n, r, e, f, t, coef)) raise(ESPP_EINVAL, msg);
+    for (int64_t k = 0; k < m; ++k) {
+      if (energy) energy[k] = tab_value(t, coef.data(), false, x[k]);
+      if (force) force[k] = tab_value(t, coef.data(), true, x[k]);
+    }
+  });
+}
+
+namespace {
+void set_tab(espp_system* s, int key, int32_t itype, int64_t n, const double* r,
+             const double* e, const double* f, double rc, double shift) {
+  if (!r || !e || !f) raise(ESPP_EINVAL, "null table");
+  if (n > 0x7fffffff) raise(ESPP_ERANGE, "table too long");
+  espp_system::TabSpec t;
+  t.itype = itype;
+  t.r.assign(r, r + n);
+  t.e.assign(e, e + n);
+  t.f.assign(f, f + n);
+  t.rc = rc;
+  t.shift = shift;
+  TabDesc probe;
+  std::vector<double> coef;
+  if (const char* msg = build_table(itype, (int)n, r, e, f, probe, coef)) raise(ESPP_EINVAL, msg);
+  s->tabSpecs[key] = std::move(t);
+  upload_tabs(s);
+}
+}  // namespace
+
+int espp_tab_pair_set(espp_system* s, int32_t t1, int32_t t2, int32_t itype, int64_t n,
+                      const double* r, const double* e, const double* f, double rc,
+                      double shift) {
+  return guard([&] {
+    checked(s);
+    if (t1 < 0 || t2 < 0 || t1 >= kMaxTypes || t2 >= kMaxTypes)
+      raise(ESPP_ERANGE, "particle type out of range");
+    if (t1 > t2) std::swap(t1, t2);
+    set_tab(s, t1 * kMaxTypes + t2, itype, n, r, e, f, rc, shift);
+  });
+}
+
+int espp_tab_bond_set(espp_system* s, int32_t itype, int64_t n, const double* r,
+                      const double* e, const double* f, double rc, double shift) {
+  return guard([&] {
+    checked(s);
+    set_tab(s, kTabBondKey, itype, n, r, e, f, rc, shift);
   });
 }
 

@@ -73,6 +73,19 @@ struct DevCounters {
 };
 
 // Pointers and scalars every kernel needs; passed by value.
+// One interpolation table of interaction::Tabulated (InterpolationLinear / Akima / Cubic)
+// with the potential's cutoff and shift.  Coefficients live in one double array:
+// r[n] at off_r; energy and force coefficient arrays at off_e / off_f, laid out per
+// interpolation type: linear a[n], b[n]; Akima p0[n], p1[n], p2[n], p3[n]; cubic y[n],
+// y2[n] (value and second derivative of the spline).
+struct TabDesc {
+  int itype;
+  int n;
+  int off_r, off_e, off_f;
+  double inner, invdelta, deltasq6;
+  double rcsq, shift;
+};
+
 struct DevView {
   ParticleArrays* pa;     // device: pa[0] current arrays, pa[1] target of the re-sort
   int n;                  // particles
@@ -87,7 +100,7 @@ struct DevView {
   float4* xrel;           // FP32 position relative to its cell origin at the last re-sort
   int32_t* pcell;         // reference cell of each sorted particle
   int32_t* cellStart;     // ncells + 1
-  int32_t* nl;            // K * cap, entry (k, i) at nl[k * cap + i]
+  int32_t* nl;            // K * cap, blocks of 8: entry (k, i) at ((k/8)*cap + i)*8 + k%8
   int32_t* nn;            // neighbour count per particle
   int K;                  // neighbour capacity
   long long* ffix;        // 3*cap pair+bond force, int64 2^-32 fixed point (mixed)
@@ -106,6 +119,11 @@ struct DevView {
   int ntypes;
   int ljSingle;           // only pair (0,0) is set
   int ljCapped;           // some pair uses LennardJonesCapped
+  const TabDesc* tabs;    // tabulated potentials (device), coefficients in tabCoef
+  const double* tabCoef;
+  const int32_t* tabPair; // tabNT*tabNT: table of the type pair on the Verlet list, -1 none
+  int tabNT;              // 0: no tabulated pair interaction
+  int tabBond;            // table of the fixed pair list, -1 none
   unsigned* err;          // device error word
   DevCounters* ctr;       // step-loop state
 };
@@ -147,6 +165,10 @@ void launch_lj_observables(const DevView& d, double* partials, int nblocks, doub
                            int energy, cudaStream_t st);
 void launch_fene_observables(const DevView& d, const FENEParams& fene, double* partials,
                              int nblocks, double* out, int energy, cudaStream_t st);
+// tabulated pair and bond forces, added to the main kernel's output
+void launch_force_tab(const DevView& d, bool mixed, cudaStream_t st);
+void launch_tab_observables(const DevView& d, int bond, double* partials, int nblocks,
+                            double* out, int energy, cudaStream_t st);
 void launch_kinetic(const DevView& d, double* partials, int nblocks, double* out,
                     cudaStream_t st);
 // Verlet pair export: counts per particle (pairs with id_j > id_i), then the pairs.

@@ -13,6 +13,7 @@
 #include <stdint.h>
 
 #include "espp_internal.h"
+#include "espp_tab.h"
 
 namespace espp {
 
@@ -1180,6 +1181,135 @@ __global__ void k_max_partials(const double* partials, int nb, double* out) {
   }
 }
 
+// ---- interaction::Tabulated ---------------------------------------------------------
+
+__device__ __forceinline__ long long to_fix_d(double f, unsigned* err) {
+  if (!(fabs(f) < 1.0e9)) atomicOr(err, kErrFixOverflow);
+  return __double2ll_rn(f * 4294967296.0);
+}
+
+// Distance vector i - j under the minimum image, and its square in the reference's
+// order ((dx dx + dy dy) + dz dz).
+__device__ __forceinline__ double tab_dist(const DevView& d, const double* X, int i, int j,
+                                           double& dx, double& dy, double& dz) {
+  const size_t c = d.cap;
+  dx = min_image(X[i] - X[j], d.L[0], d.halfL[0]);
+  dy = min_image(X[c + i] - X[c + j], d.L[1], d.halfL[1]);
+  dz = min_image(X[2 * c + i] - X[2 * c + j], d.L[2], d.halfL[2]);
+  return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+// Tabulated pair forces over the Verlet list (VerletListTabulated: force = dist *
+// getForce(r) / r below the cutoff, Tabulated.hpp:99-115) and tabulated bond forces
+// over the fixed pair list (FixedPairListTabulated), added to the forces the main pair
+// kernel wrote.  One thread per particle; FP64 distances and table arithmetic in both
+// precision modes (the mixed mode adds the sum as int64 2^-32 fixed point).
+template <bool MIXED>
+__global__ void k_force_tab(DevView d) {
+  const ParticleArrays a = d.pa[0];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n) return;
+  const double* X = a.x;
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  auto add = [&](int t, int j) {
+    const TabDesc& T = d.tabs[t];
+    double dx, dy, dz;
+    const double r2 = tab_dist(d, X, i, j, dx, dy, dz);
+    if (r2 > T.rcsq) return;
+    const double r = sqrt(r2);
+    const double ff = tab_value(T, d.tabCoef, true, r) / r;
+    fx += dx * ff;
+    fy += dy * ff;
+    fz += dz * ff;
+  };
+  if (d.tabNT > 0) {
+    const int ti = a.type[i];
+    const int cnt = d.nn[i];
+    for (int k = 0; k < cnt; ++k) {
+      const int j = d.nl[nl_index(k, i, d.cap)];
+      const int tj = a.type[j];
+      if (ti >= d.tabNT || tj >= d.tabNT) continue;
+      const int t = d.tabPair[ti * d.tabNT + tj];
+      if (t >= 0) add(t, j);
+    }
+  }
+  if (d.tabBond >= 0 && d.bondStart) {
+    const int64_t off = a.id[i] - d.idMin;
+    for (int b = d.bondStart[off]; b < d.bondStart[off + 1]; ++b) {
+      const int64_t po = d.bondPartner[b] - d.idMin;
+      const int j = (po >= 0 && po < d.idSpan) ? d.id2idx[po] : -1;
+      if (j < 0) {
+        atomicOr(d.err, kErrBondMissing);
+        continue;
+      }
+      add(d.tabBond, j);
+    }
+  }
+  const size_t c = d.cap;
+  if (MIXED) {
+    d.ffix[i] += to_fix_d(fx, d.err);
+    d.ffix[c + i] += to_fix_d(fy, d.err);
+    d.ffix[2 * c + i] += to_fix_d(fz, d.err);
+  } else {
+    d.f64[i] += fx;
+    d.f64[c + i] += fy;
+    d.f64[2 * c + i] += fz;
+  }
+}
+
+// Energy (getEnergy(r) - shift below the cutoff) or virial and its tensor of the
+// tabulated pair interaction (bond = 0, each Verlet pair once) or the tabulated bonds
+// (bond = 1, each bond once).
+__global__ void k_tab_obs(DevView d, int bond, int energy, double* partials) {
+  const ParticleArrays a = d.pa[0];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  auto add = [&](int t, int j) {
+    const TabDesc& T = d.tabs[t];
+    double dx, dy, dz;
+    const double r2 = tab_dist(d, a.x, i, j, dx, dy, dz);
+    if (r2 > T.rcsq) return;
+    const double r = sqrt(r2);
+    if (energy) {
+      acc[0] += tab_value(T, d.tabCoef, false, r) - T.shift;
+    } else {
+      const double ff = tab_value(T, d.tabCoef, true, r) / r;
+      const double f0 = dx * ff, f1 = dy * ff, f2 = dz * ff;
+      acc[0] += dx * f0 + dy * f1 + dz * f2;
+      acc[1] += dx * f0;
+      acc[2] += dy * f1;
+      acc[3] += dz * f2;
+      acc[4] += dx * f1;
+      acc[5] += dx * f2;
+      acc[6] += dy * f2;
+    }
+  };
+  if (i < d.n) {
+    if (!bond && d.tabNT > 0) {
+      const int ti = a.type[i];
+      const int cnt = d.nn[i];
+      for (int k = 0; k < cnt; ++k) {
+        const int j = d.nl[nl_index(k, i, d.cap)];
+        if (j < i) continue;
+        const int tj = a.type[j];
+        if (ti >= d.tabNT || tj >= d.tabNT) continue;
+        const int t = d.tabPair[ti * d.tabNT + tj];
+        if (t >= 0) add(t, j);
+      }
+    } else if (bond && d.tabBond >= 0 && d.bondStart) {
+      const int64_t id = a.id[i];
+      const int64_t off = id - d.idMin;
+      for (int b = d.bondStart[off]; b < d.bondStart[off + 1]; ++b) {
+        const int64_t pid = d.bondPartner[b];
+        if (pid <= id) continue;
+        const int j = d.id2idx[pid - d.idMin];
+        if (j >= 0) add(d.tabBond, j);
+      }
+    }
+  }
+  block_sum_store<7>(acc, partials);
+}
+
 __global__ void k_kinetic(DevView d, double* partials) {
   const ParticleArrays a = d.pa[0];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1377,6 +1507,20 @@ void launch_lj_observables(const DevView& d, double* partials, int nblocks, doub
 void launch_fene_observables(const DevView& d, const FENEParams& fp, double* partials,
                              int nblocks, double* out, int energy, cudaStream_t st) {
   k_fene_obs<<<nblocks, kBlock, 0, st>>>(d, fp, energy, partials);
+  k_sum_partials<7><<<1, 256, 0, st>>>(partials, nblocks, out);
+}
+
+void launch_force_tab(const DevView& d, bool mixed, cudaStream_t st) {
+  if (d.n == 0 || (d.tabNT == 0 && d.tabBond < 0)) return;
+  if (mixed)
+    k_force_tab<true><<<blocks_for(d.n), kBlock, 0, st>>>(d);
+  else
+    k_force_tab<false><<<blocks_for(d.n), kBlock, 0, st>>>(d);
+}
+
+void launch_tab_observables(const DevView& d, int bond, double* partials, int nblocks,
+                            double* out, int energy, cudaStream_t st) {
+  k_tab_obs<<<nblocks, kBlock, 0, st>>>(d, bond, energy, partials);
   k_sum_partials<7><<<1, 256, 0, st>>>(partials, nblocks, out);
 }
 

@@ -297,3 +297,128 @@ class FixedPairListFENE(Interaction):
             return
         p = self._pot
         call(st._lib, "espp_fene_set", st._h, p.K, p.r0, p.rMax, p.cutoff, p.shift)
+
+
+class Tabulated(Potential):
+    """interaction.Tabulated(itype, filename, cutoff=infinity) (Tabulated.py:610-615 and
+    921-926, Tabulated.hpp:43-115, Tabulated.cpp:45-67): energy and force interpolated from a table
+    file of (r, energy, force) lines; itype 1 linear, 2 Akima, 3 cubic spline.  The file is
+    read and the table evaluated by the library, with the reference's parsing and
+    interpolation arithmetic."""
+
+    def __init__(self, itype, filename, cutoff=infinity):
+        import numpy as np
+        from ._lib import load_library
+        self._lib = load_library()
+        self._itype = int(itype)
+        self._filename = str(filename)
+        n = ctypes.c_int64()
+        path = self._filename.encode()
+        call(self._lib, "espp_tab_read", path, 0, None, None, None, ctypes.byref(n))
+        self._r, self._e, self._f = np.zeros(n.value), np.zeros(n.value), np.zeros(n.value)
+        call(self._lib, "espp_tab_read", path, n.value, dptr(self._r), dptr(self._e),
+             dptr(self._f), ctypes.byref(n))
+        Potential.__init__(self, cutoff, 0.0)
+
+    @property
+    def filename(self):
+        return self._filename
+
+    @property
+    def itype(self):
+        return self._itype
+
+    def _eval(self, r, force):
+        x = ctypes.c_double(r)
+        out = ctypes.c_double()
+        call(self._lib, "espp_tab_eval", self._itype, len(self._r), dptr(self._r),
+             dptr(self._e), dptr(self._f), 1, ctypes.byref(x),
+             None if force else ctypes.byref(out), ctypes.byref(out) if force else None)
+        return out.value
+
+    def _energy_raw(self, ds):
+        return self._eval(math.sqrt(ds), False)
+
+    def _ffactor(self, ds):
+        r = math.sqrt(ds)
+        return self._eval(r, True) / r
+
+    def _table(self):
+        return (self._itype, len(self._r), dptr(self._r), dptr(self._e), dptr(self._f))
+
+
+class VerletListTabulated(Interaction):
+    """interaction.VerletListTabulated(vl) (Tabulated.py:816-829, Tabulated.cpp:85-95)."""
+
+    kind = _abi.IA_TAB_PAIR
+
+    def __init__(self, vl):
+        Interaction.__init__(self)
+        self._vl = vl
+        self._pots = {}
+
+    def setPotential(self, type1, type2, potential):
+        if not isinstance(potential, Tabulated):
+            raise TypeError("potential type does not match the interaction")
+        self._pots[(int(type1), int(type2))] = potential
+        self._pots[(int(type2), int(type1))] = potential
+        if self._system is not None:
+            self._push()
+            self._system.maxCutoff = max(self._system.maxCutoff, self.getMaxCutoff())
+
+    def getPotential(self, type1, type2):
+        return self._pots.get((int(type1), int(type2)))
+
+    def getVerletList(self):
+        return self._vl
+
+    getVerletListLocal = getVerletList
+
+    def getMaxCutoff(self):
+        return max([p.cutoff for p in self._pots.values()] or [0.0])
+
+    def _push(self):
+        st = self._handle()
+        if self._vl.system.storage is not st:
+            raise RuntimeError("Verlet list belongs to another system")
+        for (t1, t2), p in self._pots.items():
+            if t1 > t2:
+                continue
+            call(st._lib, "espp_tab_pair_set", st._h, t1, t2, *p._table(), p.cutoff, p.shift)
+
+
+class FixedPairListTabulated(Interaction):
+    """interaction.FixedPairListTabulated(system, fpl, potential) (Tabulated.py:841-851,
+    Tabulated.cpp:147-158)."""
+
+    kind = _abi.IA_TAB_BOND
+
+    def __init__(self, system, fpl, potential=None):
+        Interaction.__init__(self)
+        self._fpl = fpl
+        self._pot = potential
+        self._pending_system = system
+
+    def setPotential(self, potential):
+        self._pot = potential
+        if self._system is not None:
+            self._push()
+
+    def getPotential(self):
+        return self._pot
+
+    def setFixedPairList(self, fpl):
+        self._fpl = fpl
+
+    def getFixedPairList(self):
+        return self._fpl
+
+    def getMaxCutoff(self):
+        return 0.0 if self._pot is None or math.isinf(self._pot.cutoff) else self._pot.cutoff
+
+    def _push(self):
+        st = self._handle()
+        if self._pot is None:
+            return
+        p = self._pot
+        call(st._lib, "espp_tab_bond_set", st._h, *p._table(), p.cutoff, p.shift)

@@ -51,6 +51,13 @@ typedef struct espp_system espp_system;
 /* interaction kinds for the observable calls */
 #define ESPP_IA_LJ 0   /* VerletListLennardJones */
 #define ESPP_IA_FENE 1 /* FixedPairListFENE */
+#define ESPP_IA_TAB_PAIR 2 /* VerletListTabulated */
+#define ESPP_IA_TAB_BOND 3 /* FixedPairListTabulated */
+
+/* interpolation types of interaction::Tabulated (src/interaction/Tabulated.cpp:49-67) */
+#define ESPP_TAB_LINEAR 1
+#define ESPP_TAB_AKIMA 2
+#define ESPP_TAB_CUBIC 3
 
 /* force-capping modes (integrator::CapForce) */
 #define ESPP_CAP_OFF 0
@@ -120,6 +127,35 @@ ESPP_API int espp_fene_set(espp_system* s, double K, double r0, double rmax, dou
                   double shift);
 /* FixedPairList::getLongtimeMaxBondSqr. */
 ESPP_API int espp_bonds_max_sqr(espp_system* s, double* maxsq);
+
+/* ---- interaction::Tabulated -----------------------------------------------------------
+ * Table files as InterpolationLinear/Akima/Cubic::readFile read them
+ * (src/interaction/InterpolationLinear.cpp readFile; same in the Akima and Cubic
+ * variants): every line whose first three fields parse as numbers (sscanf "%lg %lg %lg")
+ * is one entry (r, energy, force); other lines are skipped.  Writes at most cap
+ * entries, *n receives the count.  Fewer than 2 entries is ESPP_EINVAL ("illegal file
+ * for tabulated potential"), an unreadable file ESPP_EINVAL. */
+ESPP_API int espp_tab_read(const char* path, int64_t cap, double* r, double* energy,
+                           double* force, int64_t* n);
+/* Interpolation::getEnergy / getForce (src/interaction/InterpolationLinear.hpp,
+ * InterpolationAkima.hpp, InterpolationCubic.hpp) of the table (r, e, f) of n entries at
+ * m distances x, on the host: the scalar evaluation behind Tabulated's computeEnergy /
+ * computeForce.  Either output may be NULL. */
+ESPP_API int espp_tab_eval(int32_t itype, int64_t n, const double* r, const double* e,
+                           const double* f, int64_t m, const double* x, double* energy,
+                           double* force);
+/* VerletListTabulated::setPotential(type1, type2, Tabulated(itype, table, cutoff))
+ * (src/interaction/Tabulated.cpp:85-95, Tabulated.hpp:43-115): the pair interacts through
+ * the table on the system's Verlet list.  shift is the final energy shift (0 unless the
+ * caller sets one).  Replaces an earlier table of the same type pair. */
+ESPP_API int espp_tab_pair_set(espp_system* s, int32_t type1, int32_t type2, int32_t itype,
+                               int64_t n, const double* r, const double* e, const double* f,
+                               double cutoff, double shift);
+/* FixedPairListTabulated(system, fpl, Tabulated(itype, table, cutoff))
+ * (src/interaction/Tabulated.cpp:147-158): the bonds of the system's fixed pair list
+ * interact through the table (in addition to FENE when that is set too). */
+ESPP_API int espp_tab_bond_set(espp_system* s, int32_t itype, int64_t n, const double* r,
+                               const double* e, const double* f, double cutoff, double shift);
 
 /* ---- integrator::VelocityVerlet + extensions ---------------------------------------
  * MDIntegrator::setTimeStep (src/integrator/MDIntegrator.cpp:53-60). */

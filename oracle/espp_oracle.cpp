@@ -20,7 +20,9 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
+#include <memory>
 #include <limits>
 #include <map>
 #include <set>
@@ -110,6 +112,213 @@ struct LJParams {
   double ff1 = 0, ff2 = 0;
 };
 
+// ---- interaction::Tabulated tables (restated from the reference) --------------------
+// InterpolationLinear / InterpolationAkima / InterpolationCubic
+// (src/interaction/Interpolation*.{hpp,cpp}), built from (radius, energy, force) arrays
+// instead of a file.  Where the reference evaluates with index N-1 it reads coefficient
+// slots it never wrote (or element N for cubic splines); here the last interval is used
+// instead, as in the CUDA library.
+struct Interp {
+  int itype = 0, N = 0;
+  double inner = 0, outer = 0, delta = 0, invdelta = 0, deltasq6 = 0;
+  std::vector<double> radius, energy, force;
+  std::vector<double> ae, be, af, bf;                    // linear
+  std::vector<double> p0e, p1e, p2e, p3e, p0f, p1f, p2f, p3f;  // Akima
+  std::vector<double> energy2, force2;                   // cubic
+
+  int index(double r) const {
+    int idx;
+    double q = (r - inner) * invdelta;
+    if (q < 0.0)
+      idx = 0;  // static_cast<int> of (-1, 0) is 0; below that the reference clamps to 0
+    else if (q >= (double)N)
+      idx = N - 1;
+    else
+      idx = static_cast<int>(q);
+    return std::min(idx, N - 2);
+  }
+  // InterpolationLinear.cpp spline
+  static void linear(const double* x, const double* y, int N, std::vector<double>& a,
+                     std::vector<double>& b) {
+    a.assign(N, 0.0);
+    b.assign(N, 0.0);
+    for (int i = 0; i < N - 1; i++) {
+      a[i] = (y[i + 1] - y[i]) / (x[i + 1] - x[i]);
+      b[i] = y[i] - a[i] * x[i];
+    }
+  }
+  // InterpolationAkima.hpp getSlope
+  static double getSlope(double m1, double m2, double m3, double m4) {
+    if ((m1 == m2) && (m3 == m4)) return (m2 + m3) / 2.0;
+    return (std::fabs(m4 - m3) * m2 + std::fabs(m2 - m1) * m3) /
+           (std::fabs(m4 - m3) + std::fabs(m2 - m1));
+  }
+  // InterpolationAkima.cpp spline
+  static void akima(const double* x, const double* y, int N, std::vector<double>& p0,
+                    std::vector<double>& p1, std::vector<double>& p2, std::vector<double>& p3) {
+    double m1, m2, m3, m4, m5;
+    double temp, g0, g1, g2, x1, x2, y1, y2, x4, x5, y4, y5;
+    std::vector<double> t(N);
+    p0.assign(N, 0.0);
+    p1.assign(N, 0.0);
+    p2.assign(N, 0.0);
+    p3.assign(N, 0.0);
+    temp = (x[1] - x[0]) / (x[2] - x[0]);
+    temp = temp * temp;
+    g0 = y[0];
+    g1 = ((y[1] - y[0]) - temp * (y[2] - y[0])) / ((x[1] - x[0]) - temp * (x[2] - x[0]));
+    g2 = ((y[2] - y[0]) - g1 * (x[2] - x[0])) / ((x[2] - x[0]) * (x[2] - x[0]));
+    x1 = x[0] - (x[2] - x[0]);
+    x2 = x[1] - (x[2] - x[0]);
+    y1 = g0 + g1 * (x1 - x[0]) + g2 * (x1 - x[0]) * (x1 - x[0]);
+    y2 = g0 + g1 * (x2 - x[0]) + g2 * (x2 - x[0]) * (x2 - x[0]);
+    m1 = (y2 - y1) / (x2 - x1);
+    m2 = (y[0] - y2) / (x[0] - x2);
+    m3 = (y[1] - y[0]) / (x[1] - x[0]);
+    m4 = (y[2] - y[1]) / (x[2] - x[1]);
+    t[0] = getSlope(m1, m2, m3, m4);
+    m5 = (y[3] - y[2]) / (x[3] - x[2]);
+    t[1] = getSlope(m2, m3, m4, m5);
+    temp = (x[N - 2] - x[N - 1]) / (x[N - 3] - x[N - 1]);
+    temp = temp * temp;
+    g0 = y[N - 1];
+    g1 = ((y[N - 2] - y[N - 1]) - temp * (y[N - 3] - y[N - 1])) /
+         ((x[N - 2] - x[N - 1]) - temp * (x[N - 3] - x[N - 1]));
+    g2 = ((y[N - 3] - y[N - 1]) - g1 * (x[N - 3] - x[N - 1])) /
+         ((x[N - 3] - x[N - 1]) * (x[N - 3] - x[N - 1]));
+    x4 = x[N - 2] + (x[N - 1] - x[N - 3]);
+    x5 = x[N - 1] + (x[N - 1] - x[N - 3]);
+    y4 = g0 + g1 * (x4 - x[N - 1]) + g2 * (x4 - x[N - 1]) * (x4 - x[N - 1]);
+    y5 = g0 + g1 * (x5 - x[N - 1]) + g2 * (x5 - x[N - 1]) * (x5 - x[N - 1]);
+    m1 = (y[N - 3] - y[N - 4]) / (x[N - 3] - x[N - 4]);
+    m2 = (y[N - 2] - y[N - 3]) / (x[N - 2] - x[N - 3]);
+    m3 = (y[N - 1] - y[N - 2]) / (x[N - 1] - x[N - 2]);
+    m4 = (y4 - y[N - 1]) / (x4 - x[N - 1]);
+    m5 = (y5 - y4) / (x5 - x4);
+    t[N - 2] = getSlope(m1, m2, m3, m4);
+    t[N - 1] = getSlope(m2, m3, m4, m5);
+    for (int i = 2; i < N - 2; i++) {
+      m1 = (y[i - 1] - y[i - 2]) / (x[i - 1] - x[i - 2]);
+      m2 = (y[i] - y[i - 1]) / (x[i] - x[i - 1]);
+      m3 = (y[i + 1] - y[i]) / (x[i + 1] - x[i]);
+      m4 = (y[i + 2] - y[i + 1]) / (x[i + 2] - x[i + 1]);
+      t[i] = getSlope(m1, m2, m3, m4);
+    }
+    for (int i = 0; i < N - 1; i++) {
+      p0[i] = y[i];
+      p1[i] = t[i];
+      p2[i] = (3.0 * (y[i + 1] - y[i]) / (x[i + 1] - x[i]) - 2.0 * t[i] - t[i + 1]) /
+              (x[i + 1] - x[i]);
+      p3[i] = (t[i] + t[i + 1] - 2.0 * (y[i + 1] - y[i]) / (x[i + 1] - x[i])) /
+              ((x[i + 1] - x[i]) * (x[i + 1] - x[i]));
+    }
+  }
+  // InterpolationCubic.cpp spline
+  static void cubic(const double* x, const double* y, int n, double yp1, double ypn,
+                    std::vector<double>& y2) {
+    y2.assign(n, 0.0);
+    std::vector<double> u(n);
+    if (yp1 > 0.99e30) {
+      y2[0] = 0.0;
+      u[0] = 0.0;
+    } else {
+      y2[0] = -0.5;
+      u[0] = (3.0 / (x[1] - x[0])) * ((y[1] - y[0]) / (x[1] - x[0]) - yp1);
+    }
+    for (int i = 1; i < n - 1; i++) {
+      double sig = (x[i] - x[i - 1]) / (x[i + 1] - x[i - 1]);
+      double p = sig * y2[i - 1] + 2.0;
+      y2[i] = (sig - 1.0) / p;
+      u[i] = (y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1]);
+      u[i] = (6.0 * u[i] / (x[i + 1] - x[i - 1]) - sig * u[i - 1]) / p;
+    }
+    double qn, un;
+    if (ypn > 0.99e30) {
+      qn = 0.0;
+      un = 0.0;
+    } else {
+      qn = 0.5;
+      un = (3.0 / (x[n - 1] - x[n - 2])) * (ypn - (y[n - 1] - y[n - 2]) / (x[n - 1] - x[n - 2]));
+    }
+    y2[n - 1] = (un - qn * u[n - 2]) / (qn * y2[n - 2] + 1.0);
+    for (int k = n - 2; k >= 0; k--) y2[k] = y2[k] * y2[k + 1] + u[k];
+  }
+  // readRaw of the three classes, from arrays
+  std::string build(int it, int n, const double* r, const double* e, const double* f) {
+    if (it < 1 || it > 3) return "interpolation type must be 1, 2 or 3";
+    if (n < 2) return "illegal file for tabulated potential";
+    if (it == 2 && n < 4) return "Akima interpolation needs at least 4 table entries";
+    itype = it;
+    N = n;
+    radius.assign(r, r + n);
+    energy.assign(e, e + n);
+    force.assign(f, f + n);
+    delta = radius[1] - radius[0];
+    if (delta <= 0.0) return "illegal distance for entries";
+    inner = radius[0];
+    outer = radius[N - 1];
+    delta = (outer - inner) / (N - 1);
+    invdelta = 1.0 / delta;
+    deltasq6 = delta * delta / 6.0;
+    if (itype == 1) {
+      linear(r, e, N, ae, be);
+      linear(r, f, N, af, bf);
+    } else if (itype == 2) {
+      akima(r, e, N, p0e, p1e, p2e, p3e);
+      akima(r, f, N, p0f, p1f, p2f, p3f);
+    } else {
+      cubic(r, e, N, -force[0], -force[N - 1], energy2);
+      double yp1 = (force[1] - force[0]) / (radius[1] - radius[0]);
+      double ypN = (force[N - 1] - force[N - 2]) / (radius[N - 1] - radius[N - 2]);
+      cubic(r, f, N, yp1, ypN, force2);
+    }
+    return "";
+  }
+  double eval(double r, bool isForce) const {
+    int index = this->index(r);
+    if (itype == 1) {  // InterpolationLinear.hpp splineInterpolation
+      const std::vector<double>& a = isForce ? af : ae;
+      const std::vector<double>& b = isForce ? bf : be;
+      return a[index] * r + b[index];
+    }
+    if (itype == 2) {  // InterpolationAkima.hpp splineInterpolation (z*z stored in an int)
+      const std::vector<double>& p0 = isForce ? p0f : p0e;
+      const std::vector<double>& p1 = isForce ? p1f : p1e;
+      const std::vector<double>& p2 = isForce ? p2f : p2e;
+      const std::vector<double>& p3 = isForce ? p3f : p3e;
+      double z = r - radius[index];
+      int zz2 = z * z;
+      return p0[index] + p1[index] * z + p2[index] * zz2 + p3[index] * zz2 * z;
+    }
+    // InterpolationCubic.hpp splineInterpolation
+    const std::vector<double>& fn = isForce ? force : energy;
+    const std::vector<double>& fn2 = isForce ? force2 : energy2;
+    double b = (r - radius[index]) * invdelta;
+    double a = 1.0 - b;
+    return a * fn[index] + b * fn[index + 1] +
+           ((a * a * a - a) * fn2[index] + (b * b * b - b) * fn2[index + 1]) * deltasq6;
+  }
+};
+
+// interaction::Tabulated (src/interaction/Tabulated.hpp:43-115)
+struct TabPot {
+  std::shared_ptr<Interp> table;
+  double cutoffSqr = 0, shift = 0;
+  bool force(const double dist[3], double f[3]) const {
+    double distSqr = dist[0] * dist[0] + dist[1] * dist[1] + dist[2] * dist[2];
+    if (distSqr > cutoffSqr) return false;
+    double distrt = std::sqrt(distSqr);
+    double ffactor = table->eval(distrt, true);
+    ffactor /= distrt;
+    for (int k = 0; k < 3; ++k) f[k] = dist[k] * ffactor;
+    return true;
+  }
+  double energy(double distSqr) const {
+    if (distSqr > cutoffSqr) return 0.0;
+    return table->eval(std::sqrt(distSqr), false) - shift;
+  }
+};
+
 }  // namespace
 
 struct espp_system {
@@ -139,6 +348,9 @@ struct espp_system {
   std::vector<std::pair<int64_t, int64_t>> bondsGlobal;
   std::vector<std::pair<Particle*, Particle*>> bondPtrs;
   double ltMaxBondSqr = 0;
+  std::map<std::pair<int, int>, TabPot> tabPair;
+  bool tabBondOn = false;
+  TabPot tabBond;
 
   // integrator
   double dt = 0.005;
@@ -533,6 +745,38 @@ void updateForces(espp_system* s) {
         }
     }
   }
+  // VerletListTabulated then FixedPairListTabulated (interactions added after LJ/FENE)
+  if (s->has_vl && !s->tabPair.empty()) {
+    for (auto& pr : s->vlPairs) {
+      Particle& p1 = *pr.first;
+      Particle& p2 = *pr.second;
+      auto it = s->tabPair.find({std::min(p1.type, p2.type), std::max(p1.type, p2.type)});
+      if (it == s->tabPair.end()) continue;
+      double d[3] = {p1.r[0] - p2.r[0], p1.r[1] - p2.r[1], p1.r[2] - p2.r[2]};
+      double f[3];
+      if (it->second.force(d, f))
+        for (int k = 0; k < 3; ++k) {
+          p1.f[k] += f[k];
+          p2.f[k] -= f[k];
+        }
+    }
+  }
+  if (s->tabBondOn) {
+    for (auto& pr : s->bondPtrs) {
+      Particle& p1 = *pr.first;
+      Particle& p2 = *pr.second;
+      double d[3];
+      minImageBox(s, p1.r, p2.r, d);
+      double dsq = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+      if (dsq > s->ltMaxBondSqr) s->ltMaxBondSqr = dsq;
+      double f[3];
+      if (s->tabBond.force(d, f))
+        for (int k = 0; k < 3; ++k) {
+          p1.f[k] += f[k];
+          p2.f[k] -= f[k];
+        }
+    }
+  }
   ghostComm(s, false, false);
   // aftCalcF: LangevinThermostat::thermalize (:105-177), then CapForce (at_back).
   if (s->lang_on) {
@@ -863,6 +1107,73 @@ int espp_bonds_max_sqr(espp_system* s, double* m) {
   return ESPP_OK;
 }
 
+// InterpolationLinear.cpp readFile: fgets + sscanf("%lg %lg %lg")
+int espp_tab_read(const char* path, int64_t cap, double* r, double* energy, double* force,
+                  int64_t* n) {
+  if (!path || !n) return fail(ESPP_EINVAL, "null argument");
+  FILE* fp = fopen(path, "r");
+  if (fp == NULL) return fail(ESPP_EINVAL, std::string("could not open file ") + path);
+  char line[1024];
+  int64_t N = 0;
+  double rr, e, f;
+  while (1) {
+    if (fgets(line, 1024, fp) == NULL) break;
+    int k = sscanf(line, "%lg %lg %lg", &rr, &e, &f);
+    if (k < 3) continue;
+    if (N < cap) {
+      if (r) r[N] = rr;
+      if (energy) energy[N] = e;
+      if (force) force[N] = f;
+    }
+    N++;
+  }
+  fclose(fp);
+  *n = N;
+  if (N < 2) return fail(ESPP_EINVAL, "illegal file for tabulated potential");
+  return ESPP_OK;
+}
+
+int espp_tab_eval(int32_t itype, int64_t n, const double* r, const double* e, const double* f,
+                  int64_t m, const double* x, double* energy, double* force) {
+  if (!r || !e || !f || (m > 0 && !x)) return fail(ESPP_EINVAL, "null argument");
+  Interp t;
+  std::string msg = t.build(itype, (int)n, r, e, f);
+  if (!msg.empty()) return fail(ESPP_EINVAL, msg);
+  for (int64_t k = 0; k < m; ++k) {
+    if (energy) energy[k] = t.eval(x[k], false);
+    if (force) force[k] = t.eval(x[k], true);
+  }
+  return ESPP_OK;
+}
+
+int espp_tab_pair_set(espp_system* s, int32_t t1, int32_t t2, int32_t itype, int64_t n,
+                      const double* r, const double* e, const double* f, double rc,
+                      double shift) {
+  CHECK_S(s);
+  auto t = std::make_shared<Interp>();
+  std::string msg = t->build(itype, (int)n, r, e, f);
+  if (!msg.empty()) return fail(ESPP_EINVAL, msg);
+  TabPot p;
+  p.table = t;
+  p.cutoffSqr = rc * rc;
+  p.shift = shift;
+  s->tabPair[{std::min(t1, t2), std::max(t1, t2)}] = p;
+  return ESPP_OK;
+}
+
+int espp_tab_bond_set(espp_system* s, int32_t itype, int64_t n, const double* r,
+                      const double* e, const double* f, double rc, double shift) {
+  CHECK_S(s);
+  auto t = std::make_shared<Interp>();
+  std::string msg = t->build(itype, (int)n, r, e, f);
+  if (!msg.empty()) return fail(ESPP_EINVAL, msg);
+  s->tabBond.table = t;
+  s->tabBond.cutoffSqr = rc * rc;
+  s->tabBond.shift = shift;
+  s->tabBondOn = true;
+  return ESPP_OK;
+}
+
 int espp_integrator_set(espp_system* s, double dt) {
   CHECK_S(s);
   if (dt == 0.0) return fail(ESPP_EINVAL, "Timestep 'dt' must be non-zero!");
@@ -935,6 +1246,23 @@ int espp_energy(espp_system* s, int32_t which, double* e) {
         minImageBox(s, pr.first->r, pr.second->r, d);
         es += feneEnergy(s, d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
       }
+  } else if (which == ESPP_IA_TAB_PAIR) {
+    if (s->has_vl)
+      for (auto& pr : s->vlPairs) {
+        auto it = s->tabPair.find({std::min(pr.first->type, pr.second->type),
+                                   std::max(pr.first->type, pr.second->type)});
+        if (it == s->tabPair.end()) continue;
+        double d[3] = {pr.first->r[0] - pr.second->r[0], pr.first->r[1] - pr.second->r[1],
+                       pr.first->r[2] - pr.second->r[2]};
+        es += it->second.energy(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      }
+  } else if (which == ESPP_IA_TAB_BOND) {
+    if (s->tabBondOn)
+      for (auto& pr : s->bondPtrs) {
+        double d[3];
+        minImageBox(s, pr.first->r, pr.second->r, d);
+        es += s->tabBond.energy(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      }
   } else {
     return fail(ESPP_EINVAL, "unknown interaction kind");
   }
@@ -970,6 +1298,25 @@ static int virialImpl(espp_system* s, int32_t which, double* wsc, double w6[6]) 
         minImageBox(s, pr.first->r, pr.second->r, d);
         double f[3];
         if (feneForce(s, d, f)) acc(d, f);
+      }
+  } else if (which == ESPP_IA_TAB_PAIR) {
+    if (s->has_vl)
+      for (auto& pr : s->vlPairs) {
+        auto it = s->tabPair.find({std::min(pr.first->type, pr.second->type),
+                                   std::max(pr.first->type, pr.second->type)});
+        if (it == s->tabPair.end()) continue;
+        double d[3] = {pr.first->r[0] - pr.second->r[0], pr.first->r[1] - pr.second->r[1],
+                       pr.first->r[2] - pr.second->r[2]};
+        double f[3];
+        if (it->second.force(d, f)) acc(d, f);
+      }
+  } else if (which == ESPP_IA_TAB_BOND) {
+    if (s->tabBondOn)
+      for (auto& pr : s->bondPtrs) {
+        double d[3];
+        minImageBox(s, pr.first->r, pr.second->r, d);
+        double f[3];
+        if (s->tabBond.force(d, f)) acc(d, f);
       }
   } else {
     return fail(ESPP_EINVAL, "unknown interaction kind");

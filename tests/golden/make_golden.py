@@ -119,6 +119,18 @@ def main(ref_root):
                   "verlet_cutoff": 1.42, "skin": 0.3, "cell_grid": "decomp.cellGrid(rc=1.12)"},
         "printed_decimals": {"epair": 3, "ebond": 3, "P": 5},
     }
+    # the same configuration with Tabulated(itype=2) tables written by the test script
+    # (testsuite/tabulated/polymer_melt_tabulated.py writeTabFile: "%15.8g" x 3, N=257;
+    # LJ r in [0.01, 1.12], FENE r in [0.0001, 1.49])
+    start = [i for i, l in enumerate(lines) if "with tabulated" in l and "without" not in l][0]
+    row = [l for l in lines[start:] if l.split() and l.split()[0] == "0"][0].split()
+    golden["tabulated"] = {
+        "source": "testsuite/tabulated/result.dat (simulation with tabulated potentials)",
+        "P": float(row[2]), "Pxy": float(row[3]), "epair": float(row[6]),
+        "ebond": float(row[7]),
+        "tables": {"itype": 2, "N": 257, "format": "%15.8g %15.8g %15.8g\\n",
+                   "lj": [0.01, 1.12], "fene": [0.0001, 1.49]},
+    }
     with open(os.path.join(HERE, "polymer_melt_40k.json"), "w") as f:
         json.dump(golden, f, indent=1)
     print("wrote fixtures to", HERE)

@@ -210,3 +210,38 @@ def mb_velocities(N, T, seed):
     v *= math.sqrt(T / (2.0 * ek / (3 * N)))
     v -= v.mean(axis=0)
     return v
+
+
+def write_tab_file(pot, path, N, low, high, body=2):
+    """Table file as testsuite/tabulated/polymer_melt_tabulated.py writeTabFile writes it:
+    N equidistant r in [low, high], one "%15.8g %15.8g %15.8g" line (r, energy, force)."""
+    delta = (high - low) / (N - 1)
+    with open(path, "w") as out:
+        for i in range(N):
+            r = low + i * delta
+            energy = pot.computeEnergy(r)
+            force = pot.computeForce((r, 0.0, 0.0))[0]
+            out.write("%15.8g %15.8g %15.8g\n" % (r, energy, force))
+
+
+def read_tab(lib, path):
+    """(r, e, f) arrays of a table file read through espp_tab_read of lib."""
+    n = ctypes.c_int64()
+    call(lib, "espp_tab_read", path.encode(), 0, None, None, None, ctypes.byref(n))
+    r, e, f = np.zeros(n.value), np.zeros(n.value), np.zeros(n.value)
+    call(lib, "espp_tab_read", path.encode(), n.value, dptr(r), dptr(e), dptr(f),
+         ctypes.byref(n))
+    return r, e, f
+
+
+def polymer_tab_tables(tmpdir, lib):
+    """The Akima tables of testsuite/tabulated/polymer_melt_tabulated.py (LJ eps=sig=1
+    rc=1.12 shift 0 on [0.01, 1.12]; FENE K=30 r0=0 rMax=1.5 on [0.0001, 1.49]; N=257)."""
+    from espressopp_b200 import interaction
+    lj = interaction.LennardJones(epsilon=1.0, sigma=1.0, shift=False, cutoff=1.12)
+    fene = interaction.FENE(K=30.0, r0=0.0, rMax=1.5)
+    plj = os.path.join(str(tmpdir), "pot-lj.txt")
+    pfene = os.path.join(str(tmpdir), "pot-fene.txt")
+    write_tab_file(lj, plj, N=257, low=0.01, high=lj.cutoff)
+    write_tab_file(fene, pfene, N=257, low=0.0001, high=1.49)
+    return read_tab(lib, plj), read_tab(lib, pfene), plj, pfene
