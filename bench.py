@@ -269,6 +269,7 @@ def gpu_arm(args, rank, world, local_rank):
         call(lib, "espp_kinetic", hh, ctypes.byref(v2), ctypes.byref(nn))
         return e.value + 0.5 * v2.value
 
+    log("rank %d: timed run" % rank)
     # timed region: one run of K steps on the captured step-loop graph; CUDA events on
     # the library's stream around the step loop
     call(lib, "espp_set_profiling", h, 0)
@@ -294,6 +295,7 @@ def gpu_arm(args, rank, world, local_rank):
         loop_ms = float(t.item())
 
 
+    log("rank %d: profiled pass" % rank)
     # per-kernel device times: the same workload stepped K more steps with every launch
     # bracketed by CUDA events on the library's stream (host-driven loop)
     call(lib, "espp_set_profiling", h, 1)
@@ -303,6 +305,7 @@ def gpu_arm(args, rank, world, local_rank):
     call(lib, "espp_profile", h, dptr(ph), i64ptr(launches_p))
     call(lib, "espp_set_profiling", h, 0)
 
+    log("rank %d: end-to-end pass" % rank)
     # end to end through the C ABI with pinned host buffers: state in, K steps, state out
     import torch
     pin_pos = torch.empty((N, 3), dtype=torch.float64, pin_memory=True).numpy()
@@ -324,6 +327,7 @@ def gpu_arm(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
 
+    log("rank %d: FP64 comparison" % rank)
     # mixed vs all-FP64 GPU on the same positions: force error and step throughput
     cmp = {}
     if prec == _abi.PREC_MIXED and not args.no_fp64:
@@ -372,6 +376,7 @@ def gpu_arm(args, rank, world, local_rank):
                                                                "e0_per_particle": e64_before / N}}
 
     lib.espp_system_destroy(h)
+    configs = small_configs(lib) if (rank == 0 and world == 1 and not args.no_configs) else None
     if rank != 0:
         if dist is not None:
             dist.barrier()
@@ -420,6 +425,7 @@ def gpu_arm(args, rank, world, local_rank):
                                    "both precisions stepping the same K NVE steps from the "
                                    "same state"),
         "clocks": clocks,
+        "other_configs": configs,
         "e2e": {"value": world * N * args.steps / e2e_s, "unit": "particle-steps/s",
                 "h2d_bytes_per_step": int(N * (48 + 8) / args.steps),
                 "d2h_bytes_per_step": int(N * 48 / args.steps),
@@ -434,6 +440,83 @@ def gpu_arm(args, rank, world, local_rank):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ---- the smaller configurations of the benchmark spec ------------------------------
+def kg_melt_config(lib, prec, nchains=200, nbeads=200, cap_steps=1000, steps=9000):
+    """Kremer-Grest melt: nchains x nbeads beads at density 0.85 (random walks, bond 0.97,
+    overlaps < 0.8 rejected; tools.topology.polymer_melt, seed 3), WCA (rc 2^(1/6), auto
+    shift) + FENE (K 30, R0 1.5), dt 0.01, Langevin gamma 0.5 T 1.  The first cap_steps
+    steps cap the pair force (LennardJonesCapped, caprad 0.9) so that the growth overlaps
+    relax while FENE keeps every bond below R0 (a cap on the total force would let bonds
+    stretch past R0, where FENE turns repulsive); then `steps` more with plain WCA.
+    Returns device-timed throughput and end-state observables."""
+    from espressopp_b200._abi import call, dptr, i32ptr, i64ptr
+    from espressopp_b200.tools import topology
+    pos, bonds, L = topology.polymer_melt(nchains, nbeads, 0.85, seed=3)
+    rc = 2.0 ** (1.0 / 6.0)
+    box = np.array([L, L, L])
+    cg = np.array([int(L / (rc + SKIN))] * 3, np.int32)
+    ids = np.arange(1, len(pos) + 1, dtype=np.int64)
+    h = ctypes.c_void_p()
+    call(lib, "espp_system_create", dptr(box), SKIN, i32ptr(cg), prec, 77, ctypes.byref(h))
+    call(lib, "espp_add_particles", h, len(ids), i64ptr(ids), None, None,
+         dptr(np.ascontiguousarray(pos.reshape(-1))), None)
+    call(lib, "espp_decompose", h)
+    call(lib, "espp_vl_create", h, rc, 0, None)
+    shift = 4.0 * (rc ** -12 - rc ** -6)
+    call(lib, "espp_lj_set", h, 0, 0, 1.0, 1.0, rc, shift, 0.9)
+    b = np.ascontiguousarray(bonds.reshape(-1))
+    call(lib, "espp_bonds_add", h, len(bonds), i64ptr(b))
+    call(lib, "espp_fene_set", h, 30.0, 0.0, 1.5, math.inf, 0.0)
+    call(lib, "espp_integrator_set", h, 0.01)
+    call(lib, "espp_langevin_set", h, 1, 0.5, 1.0, 0, None)
+    ms = np.zeros(2)
+    call(lib, "espp_run", h, cap_steps)
+    call(lib, "espp_last_run_ms", h, dptr(ms))
+    t_cap = float(ms[1])
+    call(lib, "espp_lj_set", h, 0, 0, 1.0, 1.0, rc, shift, 0.0)
+    call(lib, "espp_run", h, steps)
+    call(lib, "espp_last_run_ms", h, dptr(ms))
+    t_run = float(ms[1])
+    v2 = ctypes.c_double()
+    nn = ctypes.c_int64()
+    call(lib, "espp_kinetic", h, ctypes.byref(v2), ctypes.byref(nn))
+    e = ctypes.c_double()
+    call(lib, "espp_energy", h, 1, ctypes.byref(e))
+    mx = ctypes.c_double()
+    call(lib, "espp_bonds_max_sqr", h, ctypes.byref(mx))
+    lib.espp_system_destroy(h)
+    n = len(ids)
+    return {"value": n * (cap_steps + steps) / ((t_cap + t_run) * 1e-3),
+            "ms_per_step": (t_cap + t_run) / (cap_steps + steps),
+            "ms_per_step_capped": t_cap / cap_steps, "T_end": v2.value / (3 * n),
+            "fene_energy_per_bond": e.value / len(bonds), "max_bond": math.sqrt(mx.value)}
+
+
+def lj32k_config(lib, prec, steps=1000):
+    """LJ fluid 32^3 = 32,768 particles (the reference's CPU-runnable case): rho 0.8442,
+    rc 2.5, skin 0.3, dt 0.005, Langevin gamma 1 T 1, 1000 steps."""
+    from espressopp_b200._abi import call, dptr
+    h = make_system(lib, 32, prec)[0]
+    call(lib, "espp_langevin_set", h, 1, 1.0, 1.0, 0, None)
+    call(lib, "espp_run", h, steps)
+    ms = np.zeros(2)
+    call(lib, "espp_last_run_ms", h, dptr(ms))
+    lib.espp_system_destroy(h)
+    return {"value": 32768 * steps / (ms[1] * 1e-3), "ms_per_step": float(ms[1]) / steps}
+
+
+def small_configs(lib):
+    from espressopp_b200 import _abi
+    out = {}
+    for name, prec in (("fp64", _abi.PREC_FP64), ("mixed", _abi.PREC_MIXED)):
+        log("configs: Kremer-Grest melt, " + name)
+        out["kg_melt_40k_" + name] = kg_melt_config(lib, prec)
+        log("configs: 32k LJ, " + name)
+        out["lj_32k_" + name] = lj32k_config(lib, prec)
+    out["unit"] = "particle-steps/s (device-timed step loop)"
+    return out
 
 
 # ---- batched parallel-tempering replicas ------------------------------------------
@@ -568,6 +651,8 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=20.0)
     ap.add_argument("--steps-ref", type=int, default=1)
     ap.add_argument("--no-fp64", action="store_true", help="skip the all-FP64 comparison")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the Kremer-Grest melt and 32k LJ configurations")
     ap.add_argument("--tpp", type=int, default=0, choices=[0, 1, 2, 4, 8],
                     help="threads per particle of the force kernel (0: autotune)")
     args = ap.parse_args()

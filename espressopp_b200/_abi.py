@@ -52,6 +52,7 @@ PROTOTYPES = {
     "espp_virial": (c_int32, [_P, c_int32, _D]),
     "espp_virial_tensor": (c_int32, [_P, c_int32, _D]),
     "espp_kinetic": (c_int32, [_P, _D, _I64]),
+    "espp_rdf": (c_int32, [_P, c_int32, _D]),
     "espp_energy_noalloc": (c_int32, [_P, c_int32, _D]),
     "espp_set_profiling": (c_int32, [_P, c_int32]),
     "espp_profile": (c_int32, [_P, _D, _I64]),

@@ -1,5 +1,6 @@
 """Observables (src/analysis/Temperature.hpp:57-125, Pressure.cpp:41-119,
-PressureTensor.hpp:51-80, NPart).  Reductions run on the GPU in FP64."""
+PressureTensor.hpp:51-80, RadialDistrF.cpp:47-150, NPart).  Reductions run on the GPU in
+FP64."""
 import ctypes
 
 import numpy as np
@@ -72,3 +73,18 @@ class PressureTensor(_Observable):
             w += np.asarray(ia.computeVirialTensor())
         L = self.system.bc.boxL
         return Tensor((vv + w) / (L[0] * L[1] * L[2]))
+
+
+class RadialDistrF(_Observable):
+    """analysis.RadialDistrF(system) (RadialDistrF.py:45-60, RadialDistrF.cpp:47-150):
+    compute(rdfN) returns the radial distribution function of the current configuration
+    in rdfN bins up to half the y edge of the box, computed on the GPU over all pairs."""
+
+    print_progress = False
+
+    def compute(self, rdfN):
+        st = self._st()
+        out = np.zeros(int(rdfN))
+        call(st._lib, "espp_rdf", st._h, int(rdfN), out.ctypes.data_as(
+            ctypes.POINTER(ctypes.c_double)))
+        return list(out)

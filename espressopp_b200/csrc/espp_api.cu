@@ -1865,6 +1865,40 @@ int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n) {
   });
 }
 
+int espp_rdf(espp_system* s, int32_t rdfN, double* out) {
+  return guard([&] {
+    checked(s);
+    if (rdfN <= 0 || !out) raise(ESPP_EINVAL, "rdfN must be positive");
+    if (s->idDirty) rebuild_id_tables(s);
+    if (!s->binned) bin(s, false);
+    // dr from half the y edge, as the reference does (RadialDistrF.cpp:59-60)
+    const double dr = (s->L[1] / 2.) / (double)rdfN;
+    unsigned long long* hist = dalloc<unsigned long long>(rdfN);
+    std::vector<unsigned long long> h(rdfN);
+    try {
+      cuda_check(cudaMemsetAsync(hist, 0, sizeof(unsigned long long) * rdfN, s->st), "memset");
+      launch_rdf(s->view(), rdfN, dr, hist, s->st);
+      cuda_check(cudaGetLastError(), "rdf kernel");
+      cuda_check(cudaMemcpyAsync(h.data(), hist, sizeof(unsigned long long) * rdfN,
+                                 cudaMemcpyDeviceToHost, s->st), "download");
+      sync(s);
+    } catch (...) {
+      dfree(hist);
+      throw;
+    }
+    dfree(hist);
+    // normalisation (RadialDistrF.cpp:136-146): the factor is formed in long double
+    const int num_part = s->n;
+    const double rho = (double)num_part / (s->L[0] * s->L[1] * s->L[2]);
+    const double factor = 2.0 * 3.141592653589793238462643383279502884L * dr * rho *
+                          (double)1 * (double)num_part;
+    for (int i = 0; i < rdfN; i++) {
+      const double radius = (i + 0.5) * dr;
+      out[i] = (double)h[i] / (factor * (radius * radius + dr * dr / 12.0));
+    }
+  });
+}
+
 int espp_set_tpp(espp_system* s, int32_t tpp) {
   return guard([&] {
     checked(s);

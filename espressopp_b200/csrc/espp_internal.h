@@ -165,6 +165,9 @@ void launch_lj_observables(const DevView& d, double* partials, int nblocks, doub
                            int energy, cudaStream_t st);
 void launch_fene_observables(const DevView& d, const FENEParams& fene, double* partials,
                              int nblocks, double* out, int energy, cudaStream_t st);
+// pair-distance histogram (integer counts, accumulated into hist) for RadialDistrF
+void launch_rdf(const DevView& d, int rdfN, double dr, unsigned long long* hist,
+                cudaStream_t st);
 // tabulated pair and bond forces, added to the main kernel's output
 void launch_force_tab(const DevView& d, bool mixed, cudaStream_t st);
 void launch_tab_observables(const DevView& d, int bond, double* partials, int nblocks,

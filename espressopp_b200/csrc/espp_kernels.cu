@@ -1181,6 +1181,76 @@ __global__ void k_max_partials(const double* partials, int nb, double* out) {
   }
 }
 
+// ---- analysis::RadialDistrF -----------------------------------------------------------
+
+constexpr int kRdfTile = 256;
+
+// Pair-distance histogram over all pairs i < j (RadialDistrF.cpp:104-129): the distance is
+// the FP64 minimum image (one shift per axis, the reference's two comparisons), its bin
+// static_cast<int>(|d| / dr), counted when below rdfN.  One block per pair of 256-particle
+// tiles (upper triangle, decoded from the linear block index); counts are integers, so the
+// histogram does not depend on the order of the additions.  SMEM: per-block histogram in
+// shared memory (rdfN bins), flushed with one global atomic per non-empty bin.
+template <bool SMEM>
+__global__ void __launch_bounds__(kRdfTile) k_rdf(DevView d, int rdfN, int ntiles, double dr,
+                                                  unsigned long long* hist) {
+  extern __shared__ unsigned s_hist[];
+  __shared__ double sx[kRdfTile], sy[kRdfTile], sz[kRdfTile];
+  // linear block index -> (bi, bj), bj >= bi, rows of the upper triangle in order
+  const long long k = blockIdx.x;
+  const double T = 2.0 * ntiles + 1.0;
+  long long bi = (long long)((T - sqrt(T * T - 8.0 * (double)k)) * 0.5);
+  auto row_start = [&](long long r) { return r * ntiles - r * (r - 1) / 2; };
+  while (bi > 0 && row_start(bi) > k) --bi;
+  while (bi + 1 < ntiles && row_start(bi + 1) <= k) ++bi;
+  const long long bj = bi + (k - row_start(bi));
+  const ParticleArrays a = d.pa[0];
+  const double* X = a.x;
+  const size_t c = d.cap;
+  if (SMEM)
+    for (int b = threadIdx.x; b < rdfN; b += blockDim.x) s_hist[b] = 0u;
+  const long long j0 = bj * kRdfTile;
+  {
+    const long long j = j0 + threadIdx.x;
+    if (j < d.n) {
+      sx[threadIdx.x] = X[j];
+      sy[threadIdx.x] = X[c + j];
+      sz[threadIdx.x] = X[2 * c + j];
+    }
+  }
+  __syncthreads();
+  const long long i = bi * kRdfTile + threadIdx.x;
+  const int jn = (int)min((long long)kRdfTile, (long long)d.n - j0);
+  if (i < d.n) {
+    const double xi = X[i], yi = X[c + i], zi = X[2 * c + i];
+    const double Lx = d.L[0], Ly = d.L[1], Lz = d.L[2];
+    const double hx = d.halfL[0], hy = d.halfL[1], hz = d.halfL[2];
+    for (int t = bi == bj ? threadIdx.x + 1 : 0; t < jn; ++t) {
+      double dx = xi - sx[t], dy = yi - sy[t], dz = zi - sz[t];
+      if (dx < -hx) dx += Lx;
+      if (dx > hx) dx -= Lx;
+      if (dy < -hy) dy += Ly;
+      if (dy > hy) dy -= Ly;
+      if (dz < -hz) dz += Lz;
+      if (dz > hz) dz -= Lz;
+      const double r =
+          sqrt(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+      const int bin = (int)(r / dr);
+      if (bin < rdfN) {
+        if (SMEM)
+          atomicAdd(&s_hist[bin], 1u);
+        else
+          atomicAdd(&hist[bin], 1ull);
+      }
+    }
+  }
+  if (SMEM) {
+    __syncthreads();
+    for (int b = threadIdx.x; b < rdfN; b += blockDim.x)
+      if (s_hist[b]) atomicAdd(&hist[b], (unsigned long long)s_hist[b]);
+  }
+}
+
 // ---- interaction::Tabulated ---------------------------------------------------------
 
 __device__ __forceinline__ long long to_fix_d(double f, unsigned* err) {
@@ -1508,6 +1578,19 @@ void launch_fene_observables(const DevView& d, const FENEParams& fp, double* par
                              int nblocks, double* out, int energy, cudaStream_t st) {
   k_fene_obs<<<nblocks, kBlock, 0, st>>>(d, fp, energy, partials);
   k_sum_partials<7><<<1, 256, 0, st>>>(partials, nblocks, out);
+}
+
+void launch_rdf(const DevView& d, int rdfN, double dr, unsigned long long* hist,
+                cudaStream_t st) {
+  if (d.n < 2) return;
+  const long long ntiles = (d.n + kRdfTile - 1) / kRdfTile;
+  const long long nblocks = ntiles * (ntiles + 1) / 2;
+  constexpr int kSmemBins = 10 * 1024;  // 40 KB of shared counts (+6 KB of tile)
+  if (rdfN <= kSmemBins)
+    k_rdf<true><<<(unsigned)nblocks, kRdfTile, sizeof(unsigned) * rdfN, st>>>(
+        d, rdfN, (int)ntiles, dr, hist);
+  else
+    k_rdf<false><<<(unsigned)nblocks, kRdfTile, 0, st>>>(d, rdfN, (int)ntiles, dr, hist);
 }
 
 void launch_force_tab(const DevView& d, bool mixed, cudaStream_t st) {

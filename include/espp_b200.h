@@ -202,6 +202,11 @@ ESPP_API int espp_virial_tensor(espp_system* s, int32_t which, double w[6]);
 /* sum m v^2 over real particles and their count (analysis/Temperature.hpp:57-125). */
 ESPP_API int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n);
 
+/* analysis::RadialDistrF::computeArray(rdfN) (src/analysis/RadialDistrF.cpp:47-150): histogram
+ * of all pair distances (minimum image) in rdfN bins of width dr = L_y / (2 rdfN), each
+ * bin divided by 2 pi dr rho N ((i + 1/2)^2 dr^2 + dr^2 / 12).  out receives rdfN values. */
+ESPP_API int espp_rdf(espp_system* s, int32_t rdfN, double* out);
+
 /* Same result as espp_energy (identical kernels and reduction order), but the call
  * allocates no device memory: the per-block partial sums live in a statically sized
  * array inside the library instead of a buffer obtained with cudaMalloc.  No

@@ -1337,6 +1337,47 @@ int espp_virial_tensor(espp_system* s, int32_t which, double w[6]) {
   return virialImpl(s, which, nullptr, w);
 }
 
+// RadialDistrF::computeArray (src/analysis/RadialDistrF.cpp:47-150), one rank, one
+// configuration: particles numbered in id order, all pairs i < j.
+int espp_rdf(espp_system* s, int32_t rdfN, double* out) {
+  CHECK_S(s);
+  if (rdfN <= 0 || !out) return fail(ESPP_EINVAL, "rdfN must be positive");
+  double Li[3] = {s->L[0], s->L[1], s->L[2]};
+  double Li_half[3] = {Li[0] / 2., Li[1] / 2., Li[2] / 2.};
+  std::vector<double> histogram(rdfN, 0.0);
+  double dr = Li_half[1] / (double)rdfN;
+  std::map<size_t, std::array<double, 3>> conf;
+  for (int ci : s->realCells)
+    for (auto& p : s->cells[ci].p) conf[(size_t)p.id] = {p.r[0], p.r[1], p.r[2]};
+  std::vector<std::array<double, 3>> config;
+  for (auto& kv : conf) config.push_back(kv.second);
+  int num_part = (int)config.size();
+  for (int i = 0; i < num_part; i++) {
+    const std::array<double, 3>& coordP1 = config[i];
+    for (int j = i + 1; j < num_part; j++) {
+      const std::array<double, 3>& coordP2 = config[j];
+      double distVector[3] = {coordP1[0] - coordP2[0], coordP1[1] - coordP2[1],
+                              coordP1[2] - coordP2[2]};
+      for (int ii = 0; ii < 3; ii++) {
+        if (distVector[ii] < -Li_half[ii]) distVector[ii] += Li[ii];
+        if (distVector[ii] > Li_half[ii]) distVector[ii] -= Li[ii];
+      }
+      double abs = std::sqrt(distVector[0] * distVector[0] + distVector[1] * distVector[1] +
+                             distVector[2] * distVector[2]);
+      int bin = (int)(abs / dr);
+      if (bin < rdfN) histogram[bin] += 1.0;
+    }
+  }
+  int nconfigs = 1;
+  double rho = (double)num_part / (Li[0] * Li[1] * Li[2]);
+  double factor = 2.0 * M_PIl * dr * rho * (double)nconfigs * (double)num_part;
+  for (int i = 0; i < rdfN; i++) {
+    double radius = (i + 0.5) * dr;
+    out[i] = histogram[i] / (factor * (radius * radius + dr * dr / 12.0));
+  }
+  return ESPP_OK;
+}
+
 int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n) {
   CHECK_S(s);
   double v2 = 0.0;

@@ -329,3 +329,26 @@ def test_parallel_tempering_api_runs_and_exchanges():
                 assert pt._thermostat[n].temperature == before[n]
     temps = pt._multisystem.runAnalysisTemperature()
     assert all(0.05 < t < 10.0 for t in temps)
+
+
+@pytest.mark.parametrize("rdfN", [100, 1000, 20000])
+def test_rdf_matches_oracle_bitwise(rdfN):
+    """RadialDistrF: integer pair counts per bin are identical, so the normalised arrays
+    are bitwise equal (RadialDistrF.cpp:47-150); the 20000-bin case uses global counts."""
+    pid, pos, vel, box = load_lj2048()
+    o = _lj_setup(oracle_lib(), _abi.PREC_FP64, pid, pos, vel, box)
+    g = _lj_setup(cuda_lib(), _abi.PREC_FP64, pid, pos, vel, box)
+    ho, hg = np.zeros(rdfN), np.zeros(rdfN)
+    _abi.call(o.lib, "espp_rdf", o.h, rdfN, _abi.dptr(ho))
+    _abi.call(g.lib, "espp_rdf", g.h, rdfN, _abi.dptr(hg))
+    assert np.array_equal(ho, hg)
+    # after a run the trajectories agree to ~1e-12, so at most a few pairs change bins
+    for s in (o, g):
+        s.integrator(0.005)
+        s.run(40)
+    _abi.call(o.lib, "espp_rdf", o.h, rdfN, _abi.dptr(ho))
+    _abi.call(g.lib, "espp_rdf", g.h, rdfN, _abi.dptr(hg))
+    dr = box[1] / 2 / rdfN
+    r = (np.arange(rdfN) + 0.5) * dr
+    one_pair = 1.0 / (2 * np.pi * dr * len(pid) ** 2 / np.prod(box) * (r * r + dr * dr / 12))
+    assert np.sum(np.abs(ho - hg) / one_pair) <= 4.0

@@ -204,3 +204,19 @@ def test_tabulated_polymer_melt_step0_matches_result_dat(tmp_path):
     # the tabulated virial is held to the analytic one within the interpolation error.
     P = (s.virial(_abi.IA_TAB_PAIR) + s.virial(_abi.IA_TAB_BOND)) / (3.0 * np.prod(box))
     assert abs(P - gold["P"]) < 0.02
+
+
+def test_rdf_of_lj_fluid_is_normalised():
+    """RadialDistrF on the 2048-particle LJ fixture: zero inside the core, first peak near
+    2^(1/6), and g(r) -> 1 at long range (RadialDistrF.cpp:136-146 normalisation)."""
+    pid, pos, _, box = load_lj2048()
+    s = Sim(oracle_lib(), box, 0.3, cell_grid(box, 2.5, 0.3))
+    s.add(pid, pos)
+    s.decompose()
+    g = np.zeros(100)
+    _abi.call(oracle_lib(), "espp_rdf", s.h, 100, _abi.dptr(g))
+    dr = box[1] / 2 / 100
+    r = (np.arange(100) + 0.5) * dr
+    assert np.all(g[r < 0.8] == 0.0)
+    assert 1.0 < r[np.argmax(g)] < 1.25 and g.max() > 2.0
+    assert abs(np.mean(g[(r > 4.5) & (r < 6.5)]) - 1.0) < 0.05
