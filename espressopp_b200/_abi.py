@@ -53,6 +53,16 @@ PROTOTYPES = {
     "espp_virial_tensor": (c_int32, [_P, c_int32, _D]),
     "espp_kinetic": (c_int32, [_P, _D, _I64]),
     "espp_rdf": (c_int32, [_P, c_int32, _D]),
+    "espp_mlp_create": (c_int32, [c_double, c_double, POINTER(c_void_p)]),
+    "espp_mlp_destroy": (c_int32, [_P]),
+    "espp_mlp_num_params": (c_int32, [_I64]),
+    "espp_mlp_set_params": (c_int32, [_P, c_int64, _D]),
+    "espp_mlp_get_params": (c_int32, [_P, c_int64, _D]),
+    "espp_mlp_set_norm": (c_int32, [_P, _D, _D]),
+    "espp_mlp_attach": (c_int32, [_P, _P]),
+    "espp_mlp_descriptors": (c_int32, [_P, c_int64, _I64, _D]),
+    "espp_mlp_fm_grad": (c_int32, [_P, c_int64, _I64, _D, _D, _D]),
+    "espp_mlp_adam_step": (c_int32, [_P, c_double, c_double, c_double, c_double, c_double]),
     "espp_energy_noalloc": (c_int32, [_P, c_int32, _D]),
     "espp_set_profiling": (c_int32, [_P, c_int32]),
     "espp_profile": (c_int32, [_P, _D, _I64]),
@@ -74,6 +84,7 @@ IA_LJ = 0
 IA_FENE = 1
 IA_TAB_PAIR = 2
 IA_TAB_BOND = 3
+IA_MLP = 4
 TAB_LINEAR, TAB_AKIMA, TAB_CUBIC = 1, 2, 3
 CAP_OFF, CAP_ABS, CAP_COMPONENT = 0, 1, 2
 

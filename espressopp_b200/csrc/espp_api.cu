@@ -27,6 +27,7 @@
 #include "../../include/espp_b200.h"
 #include "espp_internal.h"
 #include "espp_tab.h"
+#include "espp_mlp.h"
 
 using namespace espp;
 
@@ -170,6 +171,17 @@ struct espp_system {
   int32_t* d_tabPair = nullptr;
   int tabNT = 0;
   int tabBond = -1;
+  // learned CG potential (not owned) and its per-particle scratch
+  espp_mlp* mlp = nullptr;
+  int mlpCap = 0;
+  float* mlpG = nullptr;
+  float* mlpD = nullptr;
+  float* mlpE = nullptr;
+  float* mlpF = nullptr;    // force-matching: model force, error adjoint, tangent
+  float* mlpErr = nullptr;
+  float* mlpTan = nullptr;
+  float* mlpPart = nullptr;
+  double* mlpFref = nullptr;
 
   // integrator
   double dt = 0.005;
@@ -235,6 +247,11 @@ struct espp_system {
     d.tabPair = d_tabPair;
     d.tabNT = tabNT;
     d.tabBond = tabBond;
+    d.mlp = mlp_view(mlp);
+    d.mlp.G = mlpG;
+    d.mlp.D = mlpD;
+    d.mlp.E = mlpE;
+    d.mlp.on = (mlp && has_vl) ? 1 : 0;
     d.err = err;
     d.ctr = ctr;
     return d;
@@ -339,6 +356,8 @@ void free_buffers(espp_system* s) {
 }
 
 // Reallocates the per-particle buffers for cap >= n and uploads h.
+void ensure_mlp_scratch(espp_system* s);
+
 void upload(espp_system* s, const HostParticles& h) {
   int n = (int)h.id.size();
   sync_pa(s);
@@ -379,6 +398,7 @@ void upload(espp_system* s, const HostParticles& h) {
   cuda_check(cudaMemset(s->ffix, 0, sizeof(long long) * 3 * s->cap), "memset");
   cuda_check(cudaMemset(s->f64, 0, sizeof(double) * 3 * s->cap), "memset");
   s->binned = false;
+  ensure_mlp_scratch(s);
 }
 
 // Dense id map, bond and exclusion CSRs indexed by id - idMin.
@@ -605,7 +625,30 @@ void upload_tabs(espp_system* s) {
 }
 
 // whether a pair interaction runs on the Verlet list
-bool pair_any(const espp_system* s) { return s->lj_any || s->tabNT > 0; }
+bool pair_any(const espp_system* s) { return s->lj_any || s->tabNT > 0 || s->mlp; }
+
+// per-particle buffers of the learned potential, sized to the particle capacity
+void ensure_mlp_scratch(espp_system* s) {
+  if (!s->mlp || s->mlpCap >= s->cap) return;
+  const size_t c = (size_t)std::max(s->cap, 1);
+  dfree(s->mlpG);
+  dfree(s->mlpD);
+  dfree(s->mlpE);
+  dfree(s->mlpF);
+  dfree(s->mlpErr);
+  dfree(s->mlpTan);
+  dfree(s->mlpPart);
+  dfree(s->mlpFref);
+  s->mlpG = dalloc<float>(c * kMlpK);
+  s->mlpD = dalloc<float>(c * kMlpK);
+  s->mlpE = dalloc<float>(c);
+  s->mlpF = dalloc<float>(c * 3);
+  s->mlpErr = dalloc<float>(c * 3);
+  s->mlpTan = dalloc<float>(c * kMlpK);
+  s->mlpPart = dalloc<float>((size_t)mlp_grad_blocks((int)c) * kMlpParams);
+  s->mlpFref = dalloc<double>(c * 3);
+  s->mlpCap = s->cap;
+}
 
 // Main pair + FENE kernel (list counts zeroed when no LJ pair is set), then the
 // tabulated pair and bond forces added to its output.
@@ -617,6 +660,7 @@ void launch_all_forces(espp_system* s, cudaStream_t st) {
   launch_forces(dm, mixed, s->fene, s->tpp, st);
   if (!s->has_vl) d.tabNT = 0;
   launch_force_tab(d, mixed, st);
+  if (d.mlp.on) launch_mlp_forces(d, mixed, nullptr, st);
 }
 
 void forces(espp_system* s) {
@@ -1165,6 +1209,11 @@ void observable(espp_system* s, int which, int energy, double out[7]) {
   } else if (which == ESPP_IA_TAB_BOND) {
     if (s->tabBond < 0) return;
     launch_tab_observables(d, 1, part, nb, s->obs, energy, s->st);
+  } else if (which == ESPP_IA_MLP) {
+    if (!d.mlp.on) return;
+    if (!energy) raise(ESPP_EINVAL, "the virial of the learned potential is not available");
+    launch_mlp_energy_terms(d, s->st);
+    launch_sum_site_energy(d, part, nb, s->obs, s->st);
   } else {
     raise(ESPP_EINVAL, "unknown interaction kind");
   }
@@ -1223,6 +1272,14 @@ void destroy(espp_system* s) {
   dfree(s->d_tabs);
   dfree(s->d_tabCoef);
   dfree(s->d_tabPair);
+  dfree(s->mlpG);
+  dfree(s->mlpD);
+  dfree(s->mlpE);
+  dfree(s->mlpF);
+  dfree(s->mlpErr);
+  dfree(s->mlpTan);
+  dfree(s->mlpPart);
+  dfree(s->mlpFref);
   dfree(s->stIds);
   dfree(s->stPos);
   dfree(s->stVel);
@@ -1862,6 +1919,175 @@ int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n) {
     cuda_check(cudaMemcpyAsync(sum_mv2, s->obs, sizeof(double), cudaMemcpyDeviceToHost, s->st),
                "download");
     sync(s);
+  });
+}
+
+int espp_mlp_create(double rc, double r0, espp_mlp** out) {
+  return guard([&] {
+    if (!out) raise(ESPP_EINVAL, "null output pointer");
+    if (!(rc > r0) || r0 < 0) raise(ESPP_EINVAL, "the basis needs 0 <= r0 < rc");
+    auto m = std::make_unique<espp_mlp>();
+    cuda_check(cudaGetDevice(&m->device), "cudaGetDevice");
+    m->rc = rc;
+    m->r0 = r0;
+    m->theta = dalloc<float>(kMlpParams);
+    m->grad = dalloc<float>(kMlpParams);
+    m->adam_m = dalloc<float>(kMlpParams);
+    m->adam_v = dalloc<float>(kMlpParams);
+    m->shift = dalloc<float>(kMlpK);
+    m->scale = dalloc<float>(kMlpK);
+    for (float* p : {m->theta, m->grad, m->adam_m, m->adam_v})
+      cuda_check(cudaMemset(p, 0, sizeof(float) * kMlpParams), "memset");
+    std::vector<float> zero(kMlpK, 0.f), one(kMlpK, 1.f);
+    cuda_check(cudaMemcpy(m->shift, zero.data(), sizeof(float) * kMlpK, cudaMemcpyHostToDevice),
+               "upload");
+    cuda_check(cudaMemcpy(m->scale, one.data(), sizeof(float) * kMlpK, cudaMemcpyHostToDevice),
+               "upload");
+    *out = m.release();
+  });
+}
+
+int espp_mlp_destroy(espp_mlp* m) {
+  return guard([&] {
+    if (!m) return;
+    cudaSetDevice(m->device);
+    for (float* p : {m->theta, m->grad, m->adam_m, m->adam_v, m->shift, m->scale})
+      if (p) cudaFree(p);
+    delete m;
+  });
+}
+
+int espp_mlp_num_params(int64_t* n) {
+  return guard([&] {
+    if (!n) raise(ESPP_EINVAL, "null output pointer");
+    *n = kMlpParams;
+  });
+}
+
+int espp_mlp_set_params(espp_mlp* m, int64_t n, const double* theta) {
+  return guard([&] {
+    if (!m || !theta) raise(ESPP_EINVAL, "null argument");
+    if (n != kMlpParams) raise(ESPP_EINVAL, "wrong number of parameters");
+    cuda_check(cudaSetDevice(m->device), "cudaSetDevice");
+    std::vector<float> h(theta, theta + n);
+    cuda_check(cudaMemcpy(m->theta, h.data(), sizeof(float) * n, cudaMemcpyHostToDevice),
+               "upload");
+  });
+}
+
+int espp_mlp_get_params(espp_mlp* m, int64_t n, double* theta) {
+  return guard([&] {
+    if (!m || !theta) raise(ESPP_EINVAL, "null argument");
+    if (n != kMlpParams) raise(ESPP_EINVAL, "wrong number of parameters");
+    cuda_check(cudaSetDevice(m->device), "cudaSetDevice");
+    std::vector<float> h(n);
+    cuda_check(cudaMemcpy(h.data(), m->theta, sizeof(float) * n, cudaMemcpyDeviceToHost),
+               "download");
+    for (int64_t q = 0; q < n; ++q) theta[q] = h[q];
+  });
+}
+
+int espp_mlp_set_norm(espp_mlp* m, const double* shift, const double* scale) {
+  return guard([&] {
+    if (!m || !shift || !scale) raise(ESPP_EINVAL, "null argument");
+    cuda_check(cudaSetDevice(m->device), "cudaSetDevice");
+    std::vector<float> a(shift, shift + kMlpK), b(scale, scale + kMlpK);
+    cuda_check(cudaMemcpy(m->shift, a.data(), sizeof(float) * kMlpK, cudaMemcpyHostToDevice),
+               "upload");
+    cuda_check(cudaMemcpy(m->scale, b.data(), sizeof(float) * kMlpK, cudaMemcpyHostToDevice),
+               "upload");
+  });
+}
+
+int espp_mlp_attach(espp_system* s, espp_mlp* m) {
+  return guard([&] {
+    checked(s);
+    if (m && m->device != s->device) raise(ESPP_EINVAL, "model and system on different devices");
+    if (m && s->has_vl && s->vl_cut < m->rc)
+      raise(ESPP_ERANGE, "Verlet-list cutoff below the model's cutoff");
+    s->mlp = m;
+    s->mlpCap = 0;
+    ensure_mlp_scratch(s);
+  });
+}
+
+int espp_mlp_descriptors(espp_system* s, int64_t n, const int64_t* ids, double* G) {
+  return guard([&] {
+    checked(s);
+    if (!s->mlp || !s->has_vl) raise(ESPP_ESTATE, "no learned potential on a Verlet list");
+    prepare_observables(s);
+    DevView d = s->view();
+    launch_mlp_energy_terms(d, s->st);
+    sync_pa(s);
+    std::vector<float> g((size_t)s->n * kMlpK);
+    std::vector<int64_t> sid(s->n);
+    cuda_check(cudaMemcpyAsync(g.data(), s->mlpG, sizeof(float) * g.size(),
+                               cudaMemcpyDeviceToHost, s->st), "download");
+    cuda_check(cudaMemcpyAsync(sid.data(), s->A.id, sizeof(int64_t) * s->n,
+                               cudaMemcpyDeviceToHost, s->st), "download");
+    sync(s);
+    std::unordered_map<int64_t, int> where;
+    where.reserve(s->n * 2);
+    for (int i = 0; i < s->n; ++i) where[sid[i]] = i;
+    for (int64_t k = 0; k < n; ++k) {
+      auto it = where.find(ids[k]);
+      if (it == where.end()) raise(ESPP_EINVAL, "particle id not present");
+      for (int q = 0; q < kMlpK; ++q) G[k * kMlpK + q] = g[(size_t)it->second * kMlpK + q];
+    }
+  });
+}
+
+int espp_mlp_fm_grad(espp_system* s, int64_t n, const int64_t* ids, const double* fref,
+                     double* loss, double* grad) {
+  return guard([&] {
+    checked(s);
+    if (!s->mlp || !s->has_vl) raise(ESPP_ESTATE, "no learned potential on a Verlet list");
+    if (n != s->n) raise(ESPP_EINVAL, "reference forces must cover every particle");
+    prepare_observables(s);
+    ensure_stage(s, n);
+    DevView d = s->view();
+    cuda_check(cudaMemcpyAsync(s->stIds, ids, sizeof(int64_t) * n, cudaMemcpyHostToDevice, s->st),
+               "upload");
+    cuda_check(cudaMemcpyAsync(s->stPos, fref, sizeof(double) * 3 * n, cudaMemcpyHostToDevice,
+                               s->st), "upload");
+    launch_scatter3_by_id(d, (int)n, s->stIds, s->stPos, s->mlpFref, s->st);
+    std::vector<float> g0;
+    if (grad) {
+      g0.resize(kMlpParams);
+      cuda_check(cudaMemcpyAsync(g0.data(), s->mlp->grad, sizeof(float) * kMlpParams,
+                                 cudaMemcpyDeviceToHost, s->st), "download");
+    }
+    launch_mlp_forces(d, false, s->mlpF, s->st);
+    int nb;
+    double* part = obs_partials(s, nb);
+    launch_mlp_fm_grad(d, s->mlpF, s->mlpFref, s->mlpErr, s->mlpTan, s->mlpPart,
+                       mlp_grad_blocks(s->n), s->mlp->grad, part, nb, s->obs, s->st);
+    cuda_check(cudaGetLastError(), "force-matching kernels");
+    double l = 0.0;
+    cuda_check(cudaMemcpyAsync(&l, s->obs, sizeof(double), cudaMemcpyDeviceToHost, s->st),
+               "download");
+    std::vector<float> g1;
+    if (grad) {
+      g1.resize(kMlpParams);
+      cuda_check(cudaMemcpyAsync(g1.data(), s->mlp->grad, sizeof(float) * kMlpParams,
+                                 cudaMemcpyDeviceToHost, s->st), "download");
+    }
+    sync(s);
+    check_err(s);
+    if (loss) *loss = l;
+    if (grad)
+      for (int q = 0; q < kMlpParams; ++q) grad[q] = (double)g1[q] - (double)g0[q];
+  });
+}
+
+int espp_mlp_adam_step(espp_mlp* m, double lr, double beta1, double beta2, double eps,
+                       double gscale) {
+  return guard([&] {
+    if (!m) raise(ESPP_EINVAL, "null model");
+    cuda_check(cudaSetDevice(m->device), "cudaSetDevice");
+    launch_mlp_adam(m, lr, beta1, beta2, eps, gscale, 0);
+    cuda_check(cudaGetLastError(), "adam kernel");
+    cuda_check(cudaDeviceSynchronize(), "adam");
   });
 }
 

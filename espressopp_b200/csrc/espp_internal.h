@@ -11,6 +11,15 @@ constexpr int kMaxTypes = 8;
 constexpr double kFix = 4294967296.0;        // 2^32: fixed-point force scale
 constexpr double kInvFix = 1.0 / 4294967296.0;
 
+#ifdef __CUDACC__
+// Verlet list layout: each particle's entries in blocks of 8 contiguous ints, block b of
+// particle i at ints [(b * cap + i) * 8, +8).  A thread reads a whole block with two
+// 16-byte loads and a warp of consecutive particles reads 1 KB of contiguous memory.
+__host__ __device__ __forceinline__ size_t nl_index(int k, int i, size_t cap) {
+  return (((size_t)(k >> 3) * cap + (size_t)i) << 3) + (size_t)(k & 7);
+}
+#endif
+
 // device error word bits
 enum : unsigned {
   kErrNlOverflow = 1u << 0,    // a particle has more Verlet neighbours than the capacity
@@ -73,6 +82,23 @@ struct DevCounters {
 };
 
 // Pointers and scalars every kernel needs; passed by value.
+// Learned coarse-grained pair potential (per-site radial-basis descriptor -> MLP ->
+// site energy), device view.  K = 16 basis functions, H = 64 hidden units.
+constexpr int kMlpK = 16;
+constexpr int kMlpH = 64;
+constexpr int kMlpParams = kMlpH * kMlpK + kMlpH + kMlpH * kMlpH + kMlpH + kMlpH + 1;
+struct MlpDev {
+  float rc, gamma;        // g_k(r) = exp(-gamma (r - mu_k)^2) fc(r), fc = (cos(pi r/rc) + 1)/2
+  float r0, dmu;          // mu_k = r0 + k dmu
+  const float* theta;     // W1[H][K], b1[H], W2[H][H], b2[H], w3[H], b3
+  const float* shift;     // K: x = (G - shift) * scale feeds the network
+  const float* scale;
+  float* G;               // per particle: descriptor (cap x K)
+  float* D;               // per particle: dE/dG (cap x K)
+  float* E;               // per particle: site energy (cap)
+  int on;
+};
+
 // One interpolation table of interaction::Tabulated (InterpolationLinear / Akima / Cubic)
 // with the potential's cutoff and shift.  Coefficients live in one double array:
 // r[n] at off_r; energy and force coefficient arrays at off_e / off_f, laid out per
@@ -124,6 +150,7 @@ struct DevView {
   const int32_t* tabPair; // tabNT*tabNT: table of the type pair on the Verlet list, -1 none
   int tabNT;              // 0: no tabulated pair interaction
   int tabBond;            // table of the fixed pair list, -1 none
+  MlpDev mlp;             // learned CG pair potential on the Verlet list (mlp.on)
   unsigned* err;          // device error word
   DevCounters* ctr;       // step-loop state
 };

@@ -54,12 +54,6 @@ __device__ __forceinline__ float fast_rcp(float x) {
   return r;
 }
 
-// Verlet list layout: each particle's entries in blocks of 8 contiguous ints, block b of
-// particle i at ints [(b * cap + i) * 8, +8).  A thread reads a whole block with two
-// 16-byte loads and a warp of consecutive particles reads 1 KB of contiguous memory.
-__device__ __forceinline__ size_t nl_index(int k, int i, size_t cap) {
-  return (((size_t)(k >> 3) * cap + (size_t)i) << 3) + (size_t)(k & 7);
-}
 
 // ---- Philox4x32-10 (Salmon et al., SC'11) ----------------------------------------
 __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {

@@ -1,0 +1,489 @@
+// Learned coarse-grained pair potential: descriptor, site network, forces, and the
+// force-matching gradient on the GPU.  Model and training scheme: espp_mlp.h.
+#include <math.h>
+#include <stdint.h>
+
+#include "espp_mlp.h"
+
+namespace espp {
+
+namespace {
+
+constexpr int K = kMlpK;
+constexpr int H = kMlpH;
+constexpr int kOffB1 = H * K;
+constexpr int kOffW2 = kOffB1 + H;
+constexpr int kOffB2 = kOffW2 + H * H;
+constexpr int kOffW3 = kOffB2 + H;
+constexpr int kOffB3 = kOffW3 + H;
+constexpr int kSiteTile = 16;  // sites per tile of the site kernel
+constexpr int kGradTile = 8;   // sites per tile of the gradient kernel
+constexpr int kGradBlocks = 296;
+
+__device__ __forceinline__ double mimg(double dx, double L, double hL) {
+  return dx < -hL ? dx + L : (dx > hL ? dx - L : dx);
+}
+
+__device__ __forceinline__ float sigm(float z) { return 1.0f / (1.0f + expf(-z)); }
+__device__ __forceinline__ float silu(float z) { return z * sigm(z); }
+__device__ __forceinline__ float silu1(float z) {
+  const float s = sigm(z);
+  return s * (1.0f + z * (1.0f - s));
+}
+__device__ __forceinline__ float silu2(float z) {
+  const float s = sigm(z);
+  return s * (1.0f - s) * (2.0f + z * (1.0f - 2.0f * s));
+}
+
+// Pair vector d = x_i - x_j (minimum image, FP64) and r^2.
+__device__ __forceinline__ double pair_d(const DevView& d, const double* X, int i, int j,
+                                         float& dx, float& dy, float& dz) {
+  const size_t c = d.cap;
+  const double ex = mimg(X[i] - X[j], d.L[0], d.halfL[0]);
+  const double ey = mimg(X[c + i] - X[c + j], d.L[1], d.halfL[1]);
+  const double ez = mimg(X[2 * c + i] - X[2 * c + j], d.L[2], d.halfL[2]);
+  dx = (float)ex;
+  dy = (float)ey;
+  dz = (float)ez;
+  return ex * ex + ey * ey + ez * ez;
+}
+
+// basis values g[k] (gp == nullptr) or derivatives gp[k] = dg_k/dr at distance r < rc
+__device__ __forceinline__ void rbf(const MlpDev& m, float r, float* g, float* gp) {
+  float sn, cs;
+  sincospif(r / m.rc, &sn, &cs);
+  const float fc = 0.5f * (cs + 1.0f);
+  const float dfc = -0.5f * 3.14159265358979f / m.rc * sn;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const float t = r - (m.r0 + k * m.dmu);
+    const float e = expf(-m.gamma * t * t);
+    if (g) g[k] = e * fc;
+    if (gp) gp[k] = e * (dfc - 2.0f * m.gamma * t * fc);
+  }
+}
+
+// G_i = sum_j g(r_ij) over the list partners within rc.
+__global__ void k_mlp_desc(DevView d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n) return;
+  const MlpDev m = d.mlp;
+  const double* X = d.pa[0].x;
+  const double rc2 = (double)m.rc * (double)m.rc;
+  float G[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) G[k] = 0.f;
+  const int cnt = d.nn[i];
+  for (int q = 0; q < cnt; ++q) {
+    const int j = d.nl[nl_index(q, i, d.cap)];
+    float dx, dy, dz;
+    const double r2 = pair_d(d, X, i, j, dx, dy, dz);
+    if (!(r2 < rc2) || j == i) continue;
+    float g[K];
+    rbf(m, sqrtf((float)r2), g, nullptr);
+#pragma unroll
+    for (int k = 0; k < K; ++k) G[k] += g[k];
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) m.G[(size_t)i * K + k] = G[k];
+}
+
+// Site network on CUDA cores: block of H threads (one per hidden unit), tiles of
+// kSiteTile sites.  E_i and D_i = dE_i/dG_i.
+__global__ void __launch_bounds__(H) k_mlp_site(MlpDev m, int n) {
+  __shared__ float sW1[H][K + 1];
+  __shared__ float sW2[H][H + 1];
+  __shared__ float sx[kSiteTile][K];
+  __shared__ float sz1[kSiteTile][H];
+  __shared__ float sh1[kSiteTile][H];
+  __shared__ float sd2[kSiteTile][H];
+  __shared__ float sd1[kSiteTile][H + 1];
+  __shared__ float sred[kSiteTile][2];
+  const int t = threadIdx.x;
+  const float* th = m.theta;
+  for (int e = t; e < H * K; e += H) sW1[e / K][e % K] = th[e];
+  for (int e = t; e < H * H; e += H) sW2[e / H][e % H] = th[kOffW2 + e];
+  const float b1 = th[kOffB1 + t], b2 = th[kOffB2 + t], w3 = th[kOffW3 + t], b3 = th[kOffB3];
+  __syncthreads();
+  for (int s0 = blockIdx.x * kSiteTile; s0 < n; s0 += gridDim.x * kSiteTile) {
+    for (int e = t; e < kSiteTile * K; e += H) {
+      const int s = e / K, k = e % K, i = s0 + s;
+      sx[s][k] = i < n ? (m.G[(size_t)i * K + k] - m.shift[k]) * m.scale[k] : 0.f;
+    }
+    __syncthreads();
+    for (int s = 0; s < kSiteTile; ++s) {
+      float z = b1;
+#pragma unroll
+      for (int k = 0; k < K; ++k) z += sW1[t][k] * sx[s][k];
+      sz1[s][t] = z;
+      sh1[s][t] = silu(z);
+    }
+    __syncthreads();
+    for (int s = 0; s < kSiteTile; ++s) {
+      float z = b2;
+#pragma unroll 16
+      for (int u = 0; u < H; ++u) z += sW2[t][u] * sh1[s][u];
+      float e = w3 * silu(z);
+      sd2[s][t] = w3 * silu1(z);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+      if ((t & 31) == 0) sred[s][t >> 5] = e;
+    }
+    __syncthreads();
+    for (int s = t; s < kSiteTile; s += H) {
+      const int i = s0 + s;
+      if (i < n) m.E[i] = b3 + sred[s][0] + sred[s][1];
+    }
+    for (int s = 0; s < kSiteTile; ++s) {
+      float g = 0.f;
+#pragma unroll 16
+      for (int v = 0; v < H; ++v) g += sW2[v][t] * sd2[s][v];
+      sd1[s][t] = g * silu1(sz1[s][t]);
+    }
+    __syncthreads();
+    for (int e = t; e < kSiteTile * K; e += H) {
+      const int s = e / K, k = e % K, i = s0 + s;
+      float g = 0.f;
+#pragma unroll 16
+      for (int u = 0; u < H; ++u) g += sW1[u][k] * sd1[s][u];
+      if (i < n) m.D[(size_t)i * K + k] = g * m.scale[k];
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ long long mlp_fix(float f, unsigned* err) {
+  if (!(fabsf(f) < 1.0e9f)) atomicOr(err, kErrFixOverflow);
+  return __float2ll_rn(f * 4294967296.0f);
+}
+
+// F_i = -sum_j phi_ij d_ij / r_ij, phi_ij = sum_k (D_ik + D_jk) g'_k(r_ij).
+template <bool MIXED>
+__global__ void k_mlp_force(DevView d, float* fout) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n) return;
+  const MlpDev m = d.mlp;
+  const double* X = d.pa[0].x;
+  const double rc2 = (double)m.rc * (double)m.rc;
+  float Di[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) Di[k] = m.D[(size_t)i * K + k];
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  const int cnt = d.nn[i];
+  for (int q = 0; q < cnt; ++q) {
+    const int j = d.nl[nl_index(q, i, d.cap)];
+    float dx, dy, dz;
+    const double r2 = pair_d(d, X, i, j, dx, dy, dz);
+    if (!(r2 < rc2) || j == i) continue;
+    const float r = sqrtf((float)r2);
+    float gp[K];
+    rbf(m, r, nullptr, gp);
+    const float4* Dj = reinterpret_cast<const float4*>(m.D + (size_t)j * K);
+    float phi = 0.f;
+#pragma unroll
+    for (int k4 = 0; k4 < K / 4; ++k4) {
+      const float4 v = Dj[k4];
+      phi += (Di[4 * k4] + v.x) * gp[4 * k4] + (Di[4 * k4 + 1] + v.y) * gp[4 * k4 + 1] +
+             (Di[4 * k4 + 2] + v.z) * gp[4 * k4 + 2] + (Di[4 * k4 + 3] + v.w) * gp[4 * k4 + 3];
+    }
+    const float s = phi / r;
+    fx -= s * dx;
+    fy -= s * dy;
+    fz -= s * dz;
+  }
+  const size_t c = d.cap;
+  if (fout) {
+    fout[3 * (size_t)i] = fx;
+    fout[3 * (size_t)i + 1] = fy;
+    fout[3 * (size_t)i + 2] = fz;
+  } else if (MIXED) {
+    d.ffix[i] += mlp_fix(fx, d.err);
+    d.ffix[c + i] += mlp_fix(fy, d.err);
+    d.ffix[2 * c + i] += mlp_fix(fz, d.err);
+  } else {
+    d.f64[i] += fx;
+    d.f64[c + i] += fy;
+    d.f64[2 * c + i] += fz;
+  }
+}
+
+template <int NB>
+__device__ void block_sum_d(double v, double* out) {
+  __shared__ double sm[NB / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < NB / 32; ++w) t += sm[w];
+    *out = t;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_site_energy(DevView d, double* partials) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  block_sum_d<256>(i < d.n ? (double)d.mlp.E[i] : 0.0, partials + blockIdx.x);
+}
+
+__global__ void k_sum_blocks(const double* partials, int nb, double* out) {
+  __shared__ double sm[256];
+  double t = 0.0;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) t += partials[b];
+  sm[threadIdx.x] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)blockDim.x; ++w) s += sm[w];
+    *out = s;
+  }
+}
+
+// force-error adjoint e = dL/dF = 2 (F - Fref) / (3 n) and the squared-error partials
+__global__ void __launch_bounds__(256) k_mlp_fm_err(int n, const float* fm, const double* fref,
+                                                    float* err, double* partials) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double sq = 0.0;
+  if (i < n) {
+    const double inv = 1.0 / (3.0 * n);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double df = (double)fm[3 * (size_t)i + c] - fref[3 * (size_t)i + c];
+      sq += df * df * inv;
+      err[3 * (size_t)i + c] = (float)(2.0 * df * inv);
+    }
+  }
+  block_sum_d<256>(sq, partials + blockIdx.x);
+}
+
+// tangent of the site networks: xdot_i[k] = -scale[k] sum_j g'_k(r_ij) (e_i - e_j).d_ij/r_ij
+__global__ void k_mlp_vpass(DevView d, const float* err, float* tangent) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n) return;
+  const MlpDev m = d.mlp;
+  const double* X = d.pa[0].x;
+  const double rc2 = (double)m.rc * (double)m.rc;
+  const float ex = err[3 * (size_t)i], ey = err[3 * (size_t)i + 1], ez = err[3 * (size_t)i + 2];
+  float v[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = 0.f;
+  const int cnt = d.nn[i];
+  for (int q = 0; q < cnt; ++q) {
+    const int j = d.nl[nl_index(q, i, d.cap)];
+    float dx, dy, dz;
+    const double r2 = pair_d(d, X, i, j, dx, dy, dz);
+    if (!(r2 < rc2) || j == i) continue;
+    const float r = sqrtf((float)r2);
+    float gp[K];
+    rbf(m, r, nullptr, gp);
+    const float proj = ((ex - err[3 * (size_t)j]) * dx + (ey - err[3 * (size_t)j + 1]) * dy +
+                        (ez - err[3 * (size_t)j + 2]) * dz) / r;
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] += gp[k] * proj;
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) tangent[(size_t)i * K + k] = -v[k] * m.scale[k];
+}
+
+// Weight gradient of sum_i d/dt E_i(x_i + t xdot_i) at t = 0 (forward-over-reverse):
+// tangents zdot1 = W1 xdot, hdot1 = silu'(z1) zdot1, zdot2 = W2 hdot1, Edot = w3.silu'(z2)
+// zdot2, then reverse mode through both chains.  Per-block partial gradients (one row of
+// each weight matrix per thread), reduced by k_mlp_reduce in block order.
+__global__ void __launch_bounds__(H) k_mlp_site_grad(MlpDev m, int n, const float* tangent,
+                                                     float* partials) {
+  __shared__ float sW1[H][K + 1];
+  __shared__ float sW2[H][H + 1];
+  __shared__ float sx[kGradTile][K], sxd[kGradTile][K];
+  __shared__ float sh1[kGradTile][H], shd1[kGradTile][H];
+  __shared__ float saz2[kGradTile][H], sazd2[kGradTile][H];
+  const int t = threadIdx.x;
+  const float* th = m.theta;
+  for (int e = t; e < H * K; e += H) sW1[e / K][e % K] = th[e];
+  for (int e = t; e < H * H; e += H) sW2[e / H][e % H] = th[kOffW2 + e];
+  const float b1 = th[kOffB1 + t], b2 = th[kOffB2 + t], w3 = th[kOffW3 + t];
+  float gW1[K], gW2[H];
+#pragma unroll
+  for (int k = 0; k < K; ++k) gW1[k] = 0.f;
+#pragma unroll
+  for (int u = 0; u < H; ++u) gW2[u] = 0.f;
+  float gb1 = 0.f, gb2 = 0.f, gw3 = 0.f;
+  float z1r[kGradTile], zd1r[kGradTile];
+  __syncthreads();
+  for (int s0 = blockIdx.x * kGradTile; s0 < n; s0 += gridDim.x * kGradTile) {
+    for (int e = t; e < kGradTile * K; e += H) {
+      const int s = e / K, k = e % K, i = s0 + s;
+      sx[s][k] = i < n ? (m.G[(size_t)i * K + k] - m.shift[k]) * m.scale[k] : 0.f;
+      sxd[s][k] = i < n ? tangent[(size_t)i * K + k] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < kGradTile; ++s) {
+      float z = b1, zd = 0.f;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        z += sW1[t][k] * sx[s][k];
+        zd += sW1[t][k] * sxd[s][k];
+      }
+      z1r[s] = z;
+      zd1r[s] = zd;
+      sh1[s][t] = silu(z);
+      shd1[s][t] = silu1(z) * zd;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < kGradTile; ++s) {
+      float z = b2, zd = 0.f;
+#pragma unroll 16
+      for (int u = 0; u < H; ++u) {
+        z += sW2[t][u] * sh1[s][u];
+        zd += sW2[t][u] * shd1[s][u];
+      }
+      const float s1 = silu1(z);
+      gw3 += s1 * zd;
+      const float azd2 = w3 * s1;
+      const float az2 = w3 * zd * silu2(z);
+      gb2 += az2;
+#pragma unroll
+      for (int u = 0; u < H; ++u) gW2[u] += az2 * sh1[s][u] + azd2 * shd1[s][u];
+      saz2[s][t] = az2;
+      sazd2[s][t] = azd2;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < kGradTile; ++s) {
+      float ah1 = 0.f, ahd1 = 0.f;
+#pragma unroll 16
+      for (int v = 0; v < H; ++v) {
+        ah1 += sW2[v][t] * saz2[s][v];
+        ahd1 += sW2[v][t] * sazd2[s][v];
+      }
+      const float s1 = silu1(z1r[s]);
+      const float azd1 = ahd1 * s1;
+      const float az1 = ah1 * s1 + ahd1 * zd1r[s] * silu2(z1r[s]);
+      gb1 += az1;
+#pragma unroll
+      for (int k = 0; k < K; ++k) gW1[k] += az1 * sx[s][k] + azd1 * sxd[s][k];
+    }
+    __syncthreads();
+  }
+  float* p = partials + (size_t)blockIdx.x * kMlpParams;
+#pragma unroll
+  for (int k = 0; k < K; ++k) p[t * K + k] = gW1[k];
+  p[kOffB1 + t] = gb1;
+#pragma unroll
+  for (int u = 0; u < H; ++u) p[kOffW2 + t * H + u] = gW2[u];
+  p[kOffB2 + t] = gb2;
+  p[kOffW3 + t] = gw3;
+  if (t == 0) p[kOffB3] = 0.f;
+}
+
+__global__ void k_mlp_reduce(const float* partials, int nb, float* grad) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= kMlpParams) return;
+  double s = 0.0;
+  for (int b = 0; b < nb; ++b) s += partials[(size_t)b * kMlpParams + q];
+  grad[q] += (float)s;
+}
+
+__global__ void k_mlp_adam(float* theta, float* mm, float* vv, float* grad, float lr, float b1,
+                           float b2, float eps, float c1, float c2, float gscale) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= kMlpParams) return;
+  const float g = grad[q] * gscale;
+  mm[q] = b1 * mm[q] + (1.f - b1) * g;
+  vv[q] = b2 * vv[q] + (1.f - b2) * g * g;
+  theta[q] -= lr * (mm[q] / c1) / (sqrtf(vv[q] / c2) + eps);
+  grad[q] = 0.f;
+}
+
+}  // namespace
+
+MlpDev mlp_view(const espp_mlp* m) {
+  MlpDev v{};
+  if (!m) return v;
+  v.rc = (float)m->rc;
+  v.r0 = (float)m->r0;
+  v.dmu = (float)((m->rc - m->r0) / (K - 1));
+  v.gamma = (float)(1.0 / (2.0 * (double)v.dmu * (double)v.dmu));
+  v.theta = m->theta;
+  v.shift = m->shift;
+  v.scale = m->scale;
+  v.on = 1;
+  return v;
+}
+
+int mlp_grad_blocks(int n) {
+  const int tiles = (n + kGradTile - 1) / kGradTile;
+  return tiles < kGradBlocks ? (tiles > 0 ? tiles : 1) : kGradBlocks;
+}
+
+void launch_mlp_energy_terms(const DevView& d, cudaStream_t st) {
+  if (d.n == 0) return;
+  k_mlp_desc<<<(d.n + 255) / 256, 256, 0, st>>>(d);
+  const int tiles = (d.n + kSiteTile - 1) / kSiteTile;
+  k_mlp_site<<<tiles < 1184 ? tiles : 1184, H, 0, st>>>(d.mlp, d.n);
+}
+
+void launch_mlp_forces(const DevView& d, bool mixed, float* fout, cudaStream_t st) {
+  if (d.n == 0 || !d.mlp.on) return;
+  launch_mlp_energy_terms(d, st);
+  if (mixed)
+    k_mlp_force<true><<<(d.n + 255) / 256, 256, 0, st>>>(d, fout);
+  else
+    k_mlp_force<false><<<(d.n + 255) / 256, 256, 0, st>>>(d, fout);
+}
+
+void launch_sum_site_energy(const DevView& d, double* partials, int nblocks, double* out,
+                            cudaStream_t st) {
+  k_site_energy<<<nblocks, 256, 0, st>>>(d, partials);
+  k_sum_blocks<<<1, 256, 0, st>>>(partials, nblocks, out);
+}
+
+void launch_mlp_fm_grad(const DevView& d, const float* fmodel, const double* fref, float* err,
+                        float* tangent, float* partials, int npart_blocks, float* grad,
+                        double* loss_partials, int nloss_blocks, double* loss_out,
+                        cudaStream_t st) {
+  k_mlp_fm_err<<<nloss_blocks, 256, 0, st>>>(d.n, fmodel, fref, err, loss_partials);
+  k_sum_blocks<<<1, 256, 0, st>>>(loss_partials, nloss_blocks, loss_out);
+  k_mlp_vpass<<<(d.n + 255) / 256, 256, 0, st>>>(d, err, tangent);
+  k_mlp_site_grad<<<npart_blocks, H, 0, st>>>(d.mlp, d.n, tangent, partials);
+  k_mlp_reduce<<<(kMlpParams + 255) / 256, 256, 0, st>>>(partials, npart_blocks, grad);
+}
+
+void launch_mlp_adam(espp_mlp* m, double lr, double beta1, double beta2, double eps,
+                     double gscale, cudaStream_t st) {
+  m->adam_t += 1;
+  const float c1 = (float)(1.0 - std::pow(beta1, (double)m->adam_t));
+  const float c2 = (float)(1.0 - std::pow(beta2, (double)m->adam_t));
+  k_mlp_adam<<<(kMlpParams + 255) / 256, 256, 0, st>>>(m->theta, m->adam_m, m->adam_v, m->grad,
+                                                       (float)lr, (float)beta1, (float)beta2,
+                                                       (float)eps, c1, c2, (float)gscale);
+}
+
+}  // namespace espp
+
+namespace espp {
+namespace {
+__global__ void k_scatter3_by_id(int n, const int64_t* ids, const double* vals, int64_t idMin,
+                                 int idSpan, const int32_t* id2idx, double* out, unsigned* err) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int64_t o = ids[k] - idMin;
+  const int i = (o >= 0 && o < idSpan) ? id2idx[o] : -1;
+  if (i < 0) {
+    atomicOr(err, kErrIdRange);
+    return;
+  }
+  out[3 * (size_t)i] = vals[3 * (size_t)k];
+  out[3 * (size_t)i + 1] = vals[3 * (size_t)k + 1];
+  out[3 * (size_t)i + 2] = vals[3 * (size_t)k + 2];
+}
+}  // namespace
+
+void launch_scatter3_by_id(const DevView& d, int n, const int64_t* ids, const double* vals,
+                           double* out, cudaStream_t st) {
+  if (n > 0)
+    k_scatter3_by_id<<<(n + 255) / 256, 256, 0, st>>>(n, ids, vals, d.idMin, d.idSpan, d.id2idx,
+                                                      out, d.err);
+}
+}  // namespace espp

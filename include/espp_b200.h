@@ -53,6 +53,7 @@ typedef struct espp_system espp_system;
 #define ESPP_IA_FENE 1 /* FixedPairListFENE */
 #define ESPP_IA_TAB_PAIR 2 /* VerletListTabulated */
 #define ESPP_IA_TAB_BOND 3 /* FixedPairListTabulated */
+#define ESPP_IA_MLP 4      /* learned coarse-grained pair potential (espp_mlp_*) */
 
 /* interpolation types of interaction::Tabulated (src/interaction/Tabulated.cpp:49-67) */
 #define ESPP_TAB_LINEAR 1
@@ -206,6 +207,39 @@ ESPP_API int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n);
  * of all pair distances (minimum image) in rdfN bins of width dr = L_y / (2 rdfN), each
  * bin divided by 2 pi dr rho N ((i + 1/2)^2 dr^2 + dr^2 / 12).  out receives rdfN values. */
 ESPP_API int espp_rdf(espp_system* s, int32_t rdfN, double* out);
+
+/* ---- learned coarse-grained potential -------------------------------------------------
+ * No counterpart in the reference: a many-body pair potential for coarse-grained sites,
+ * with interaction::Tabulated as its fallback.  Per particle i a descriptor of 16
+ * Gaussian radial basis functions over the Verlet-list partners within rc,
+ *   G_i[k] = sum_j exp(-(r_ij - mu_k)^2 / (2 w^2)) (cos(pi r_ij / rc) + 1) / 2,
+ *   mu_k = r0 + k w, w = (rc - r0) / 15,
+ * normalised as x_i = (G_i - shift) * scale, feeds an MLP 16-64-64-1 with SiLU
+ * activations giving the site energy E_i; E = sum_i E_i and F = -grad E.  Parameters
+ * (espp_mlp_num_params of them, in the order W1[64][16], b1[64], W2[64][64], b2[64],
+ * w3[64], b3) live on the device.  Training is by force matching: espp_mlp_fm_grad
+ * evaluates the mean squared force-component error of one configuration against
+ * reference forces and adds its gradient to the model's accumulator;
+ * espp_mlp_adam_step applies Adam (gradient times gscale) and clears the accumulator. */
+typedef struct espp_mlp espp_mlp;
+ESPP_API int espp_mlp_create(double rc, double r0, espp_mlp** out);
+ESPP_API int espp_mlp_destroy(espp_mlp* m);
+ESPP_API int espp_mlp_num_params(int64_t* n);
+ESPP_API int espp_mlp_set_params(espp_mlp* m, int64_t n, const double* theta);
+ESPP_API int espp_mlp_get_params(espp_mlp* m, int64_t n, double* theta);
+ESPP_API int espp_mlp_set_norm(espp_mlp* m, const double shift[16], const double scale[16]);
+/* Adds the model as an interaction of s on its Verlet list (cutoff >= rc); NULL removes
+ * it.  The model is not owned by the system and must outlive the attachment. */
+ESPP_API int espp_mlp_attach(espp_system* s, espp_mlp* m);
+/* Descriptors G (16 per particle) of the particles ids, in that order. */
+ESPP_API int espp_mlp_descriptors(espp_system* s, int64_t n, const int64_t* ids, double* G);
+/* Loss and gradient on the current configuration against reference forces fref (3 per
+ * particle, given in the order of ids, every particle once).  grad (optional) receives
+ * this configuration's gradient; the model accumulator receives it too. */
+ESPP_API int espp_mlp_fm_grad(espp_system* s, int64_t n, const int64_t* ids,
+                              const double* fref, double* loss, double* grad);
+ESPP_API int espp_mlp_adam_step(espp_mlp* m, double lr, double beta1, double beta2, double eps,
+                                double gscale);
 
 /* Same result as espp_energy (identical kernels and reduction order), but the call
  * allocates no device memory: the per-block partial sums live in a statically sized

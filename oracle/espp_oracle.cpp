@@ -321,6 +321,32 @@ struct TabPot {
 
 }  // namespace
 
+// ---- learned coarse-grained potential (the model of include/espp_b200.h) in FP64 -----
+struct espp_mlp {
+  static constexpr int K = 16, H = 64;
+  static constexpr int NP = H * K + H + H * H + H + H + 1;
+  double rc = 3.0, r0 = 0.0;
+  std::vector<double> theta = std::vector<double>(NP, 0.0);
+  std::vector<double> grad = std::vector<double>(NP, 0.0);
+  std::vector<double> am = std::vector<double>(NP, 0.0), av = std::vector<double>(NP, 0.0);
+  double shift[16] = {0}, scale[16] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+  long long t = 0;
+  double dmu() const { return (rc - r0) / (K - 1); }
+  double gamma() const { return 1.0 / (2.0 * dmu() * dmu()); }
+  // g_k(r) and dg_k/dr
+  void rbf(double r, double* g, double* gp) const {
+    const double pi = 3.14159265358979323846;
+    const double fc = 0.5 * (std::cos(pi * r / rc) + 1.0);
+    const double dfc = -0.5 * pi / rc * std::sin(pi * r / rc);
+    for (int k = 0; k < K; ++k) {
+      const double tt = r - (r0 + k * dmu());
+      const double e = std::exp(-gamma() * tt * tt);
+      if (g) g[k] = e * fc;
+      if (gp) gp[k] = e * (dfc - 2.0 * gamma() * tt * fc);
+    }
+  }
+};
+
 struct espp_system {
   double L[3], invL[3], L2[3];
   double skin;
@@ -364,6 +390,7 @@ struct espp_system {
   int capMode = ESPP_CAP_OFF;
   double cap[3] = {0, 0, 0};
   int langPhase = 0;
+  espp_mlp* mlp = nullptr;
 };
 
 namespace {
@@ -707,6 +734,183 @@ const LJParams* ljFor(const espp_system* s, int t1, int t2) {
   return &it->second;
 }
 
+// The learned potential on the Verlet pairs within rc: descriptors, site networks,
+// forces, and (with fref) the force-matching loss and weight gradient.
+struct MlpPair {
+  int a, b;
+  double d[3], r;
+};
+struct MlpEval {
+  std::vector<Particle*> part;
+  std::unordered_map<int64_t, int> idx;
+  std::vector<MlpPair> pairs;
+  std::vector<std::array<double, 16>> G, D;
+  std::vector<double> E;
+  std::vector<std::array<double, 3>> F;
+};
+
+double mlp_sig(double z) { return 1.0 / (1.0 + std::exp(-z)); }
+double mlp_silu(double z) { return z * mlp_sig(z); }
+double mlp_silu1(double z) {
+  double sg = mlp_sig(z);
+  return sg * (1.0 + z * (1.0 - sg));
+}
+double mlp_silu2(double z) {
+  double sg = mlp_sig(z);
+  return sg * (1.0 - sg) * (2.0 + z * (1.0 - 2.0 * sg));
+}
+
+void mlpEvaluate(espp_system* s, MlpEval& ev) {
+  const espp_mlp& m = *s->mlp;
+  const int K = espp_mlp::K, H = espp_mlp::H;
+  const double* th = m.theta.data();
+  const double *W1 = th, *b1 = th + H * K, *W2 = b1 + H, *b2 = W2 + H * H, *w3 = b2 + H,
+               b3 = w3[H];
+  for (int ci : s->realCells)
+    for (auto& p : s->cells[ci].p) {
+      ev.idx[p.id] = (int)ev.part.size();
+      ev.part.push_back(&p);
+    }
+  const int n = (int)ev.part.size();
+  for (auto& pr : s->vlPairs) {
+    MlpPair q;
+    for (int k = 0; k < 3; ++k) q.d[k] = pr.first->r[k] - pr.second->r[k];
+    double r2 = q.d[0] * q.d[0] + q.d[1] * q.d[1] + q.d[2] * q.d[2];
+    if (!(r2 < m.rc * m.rc) || pr.first->id == pr.second->id) continue;
+    q.r = std::sqrt(r2);
+    q.a = ev.idx[pr.first->id];
+    q.b = ev.idx[pr.second->id];
+    ev.pairs.push_back(q);
+  }
+  ev.G.assign(n, {});
+  ev.D.assign(n, {});
+  ev.E.assign(n, 0.0);
+  ev.F.assign(n, {});
+  for (auto& q : ev.pairs) {
+    double g[16];
+    m.rbf(q.r, g, nullptr);
+    for (int k = 0; k < K; ++k) {
+      ev.G[q.a][k] += g[k];
+      ev.G[q.b][k] += g[k];
+    }
+  }
+  for (int i = 0; i < n; ++i) {
+    double x[16], z1[64], h1[64], d2[64], d1[64];
+    for (int k = 0; k < K; ++k) x[k] = (ev.G[i][k] - m.shift[k]) * m.scale[k];
+    for (int t = 0; t < H; ++t) {
+      double z = b1[t];
+      for (int k = 0; k < K; ++k) z += W1[t * K + k] * x[k];
+      z1[t] = z;
+      h1[t] = mlp_silu(z);
+    }
+    double e = b3;
+    for (int t = 0; t < H; ++t) {
+      double z = b2[t];
+      for (int u = 0; u < H; ++u) z += W2[t * H + u] * h1[u];
+      e += w3[t] * mlp_silu(z);
+      d2[t] = w3[t] * mlp_silu1(z);
+    }
+    ev.E[i] = e;
+    for (int u = 0; u < H; ++u) {
+      double g = 0.0;
+      for (int t = 0; t < H; ++t) g += W2[t * H + u] * d2[t];
+      d1[u] = g * mlp_silu1(z1[u]);
+    }
+    for (int k = 0; k < K; ++k) {
+      double g = 0.0;
+      for (int u = 0; u < H; ++u) g += W1[u * K + k] * d1[u];
+      ev.D[i][k] = g * m.scale[k];
+    }
+  }
+  for (auto& q : ev.pairs) {
+    double gp[16];
+    m.rbf(q.r, nullptr, gp);
+    double phi = 0.0;
+    for (int k = 0; k < K; ++k) phi += (ev.D[q.a][k] + ev.D[q.b][k]) * gp[k];
+    for (int c = 0; c < 3; ++c) {
+      ev.F[q.a][c] -= phi * q.d[c] / q.r;
+      ev.F[q.b][c] += phi * q.d[c] / q.r;
+    }
+  }
+}
+
+// Mean squared force-component error against fref (by particle index of ev) and its
+// gradient, from the tangent xdot_i = -scale * sum_j g'(r_ij) (e_i - e_j).d_ij / r_ij and
+// reverse mode through the site networks' tangent chains.
+double mlpFmGrad(espp_system* s, MlpEval& ev, const std::vector<std::array<double, 3>>& fref,
+                 std::vector<double>& grad) {
+  const espp_mlp& m = *s->mlp;
+  const int K = espp_mlp::K, H = espp_mlp::H;
+  const double* th = m.theta.data();
+  const double *W1 = th, *b1 = th + H * K, *W2 = b1 + H, *b2 = W2 + H * H, *w3 = b2 + H;
+  const int n = (int)ev.part.size();
+  double loss = 0.0;
+  std::vector<std::array<double, 3>> err(n);
+  for (int i = 0; i < n; ++i)
+    for (int c = 0; c < 3; ++c) {
+      double df = ev.F[i][c] - fref[i][c];
+      loss += df * df / (3.0 * n);
+      err[i][c] = 2.0 * df / (3.0 * n);
+    }
+  std::vector<std::array<double, 16>> v(n);
+  for (auto& q : ev.pairs) {
+    double gp[16];
+    m.rbf(q.r, nullptr, gp);
+    double proj = 0.0;
+    for (int c = 0; c < 3; ++c) proj += (err[q.a][c] - err[q.b][c]) * q.d[c] / q.r;
+    for (int k = 0; k < K; ++k) {
+      v[q.a][k] += gp[k] * proj;
+      v[q.b][k] += gp[k] * proj;
+    }
+  }
+  grad.assign(espp_mlp::NP, 0.0);
+  double *gW1 = grad.data(), *gb1 = gW1 + H * K, *gW2 = gb1 + H, *gb2 = gW2 + H * H,
+         *gw3 = gb2 + H;
+  for (int i = 0; i < n; ++i) {
+    double x[16], xd[16], z1[64], zd1[64], h1[64], hd1[64], az2[64], azd2[64];
+    for (int k = 0; k < K; ++k) {
+      x[k] = (ev.G[i][k] - m.shift[k]) * m.scale[k];
+      xd[k] = -v[i][k] * m.scale[k];
+    }
+    for (int t = 0; t < H; ++t) {
+      double z = b1[t], zd = 0.0;
+      for (int k = 0; k < K; ++k) {
+        z += W1[t * K + k] * x[k];
+        zd += W1[t * K + k] * xd[k];
+      }
+      z1[t] = z;
+      zd1[t] = zd;
+      h1[t] = mlp_silu(z);
+      hd1[t] = mlp_silu1(z) * zd;
+    }
+    for (int t = 0; t < H; ++t) {
+      double z = b2[t], zd = 0.0;
+      for (int u = 0; u < H; ++u) {
+        z += W2[t * H + u] * h1[u];
+        zd += W2[t * H + u] * hd1[u];
+      }
+      gw3[t] += mlp_silu1(z) * zd;
+      azd2[t] = w3[t] * mlp_silu1(z);
+      az2[t] = w3[t] * zd * mlp_silu2(z);
+      gb2[t] += az2[t];
+      for (int u = 0; u < H; ++u) gW2[t * H + u] += az2[t] * h1[u] + azd2[t] * hd1[u];
+    }
+    for (int u = 0; u < H; ++u) {
+      double ah1 = 0.0, ahd1 = 0.0;
+      for (int t = 0; t < H; ++t) {
+        ah1 += W2[t * H + u] * az2[t];
+        ahd1 += W2[t * H + u] * azd2[t];
+      }
+      const double s1 = mlp_silu1(z1[u]);
+      const double azd1 = ahd1 * s1;
+      const double az1 = ah1 * s1 + ahd1 * zd1[u] * mlp_silu2(z1[u]);
+      gb1[u] += az1;
+      for (int k = 0; k < K; ++k) gW1[u * K + k] += az1 * x[k] + azd1 * xd[k];
+    }
+  }
+  return loss;
+}
+
 // VelocityVerlet::updateForces / calcForces / initForces (:307-371) with
 // VerletListInteractionTemplate::addForces (:116-198), FixedPairList template
 // addForces (:112-205) and the aftCalcF extensions.
@@ -778,6 +982,12 @@ void updateForces(espp_system* s) {
     }
   }
   ghostComm(s, false, false);
+  if (s->mlp && s->has_vl) {
+    MlpEval ev;
+    mlpEvaluate(s, ev);
+    for (size_t i = 0; i < ev.part.size(); ++i)
+      for (int c = 0; c < 3; ++c) ev.part[i]->f[c] += ev.F[i][c];
+  }
   // aftCalcF: LangevinThermostat::thermalize (:105-177), then CapForce (at_back).
   if (s->lang_on) {
     for (int ci : s->realCells)
@@ -1211,6 +1421,107 @@ int espp_capforce_set(espp_system* s, int32_t mode, const double cap[3]) {
   return ESPP_OK;
 }
 
+int espp_mlp_create(double rc, double r0, espp_mlp** out) {
+  if (!out) return fail(ESPP_EINVAL, "null output pointer");
+  if (!(rc > r0) || r0 < 0) return fail(ESPP_EINVAL, "the basis needs 0 <= r0 < rc");
+  espp_mlp* m = new espp_mlp();
+  m->rc = rc;
+  m->r0 = r0;
+  *out = m;
+  return ESPP_OK;
+}
+
+int espp_mlp_destroy(espp_mlp* m) {
+  delete m;
+  return ESPP_OK;
+}
+
+int espp_mlp_num_params(int64_t* n) {
+  *n = espp_mlp::NP;
+  return ESPP_OK;
+}
+
+int espp_mlp_set_params(espp_mlp* m, int64_t n, const double* theta) {
+  if (!m || n != espp_mlp::NP) return fail(ESPP_EINVAL, "wrong number of parameters");
+  m->theta.assign(theta, theta + n);
+  return ESPP_OK;
+}
+
+int espp_mlp_get_params(espp_mlp* m, int64_t n, double* theta) {
+  if (!m || n != espp_mlp::NP) return fail(ESPP_EINVAL, "wrong number of parameters");
+  std::copy(m->theta.begin(), m->theta.end(), theta);
+  return ESPP_OK;
+}
+
+int espp_mlp_set_norm(espp_mlp* m, const double* shift, const double* scale) {
+  if (!m) return fail(ESPP_EINVAL, "null model");
+  for (int k = 0; k < espp_mlp::K; ++k) {
+    m->shift[k] = shift[k];
+    m->scale[k] = scale[k];
+  }
+  return ESPP_OK;
+}
+
+int espp_mlp_attach(espp_system* s, espp_mlp* m) {
+  CHECK_S(s);
+  if (m && s->has_vl && s->vl_cut < m->rc)
+    return fail(ESPP_ERANGE, "Verlet-list cutoff below the model's cutoff");
+  s->mlp = m;
+  return ESPP_OK;
+}
+
+int espp_mlp_descriptors(espp_system* s, int64_t n, const int64_t* ids, double* G) {
+  CHECK_S(s);
+  if (!s->mlp || !s->has_vl) return fail(ESPP_ESTATE, "no learned potential on a Verlet list");
+  ghostComm(s, true, false);
+  MlpEval ev;
+  mlpEvaluate(s, ev);
+  for (int64_t k = 0; k < n; ++k) {
+    auto it = ev.idx.find(ids[k]);
+    if (it == ev.idx.end()) return fail(ESPP_EINVAL, "particle id not present");
+    for (int q = 0; q < espp_mlp::K; ++q) G[k * espp_mlp::K + q] = ev.G[it->second][q];
+  }
+  return ESPP_OK;
+}
+
+int espp_mlp_fm_grad(espp_system* s, int64_t n, const int64_t* ids, const double* fref,
+                     double* loss, double* grad) {
+  CHECK_S(s);
+  if (!s->mlp || !s->has_vl) return fail(ESPP_ESTATE, "no learned potential on a Verlet list");
+  ghostComm(s, true, false);
+  MlpEval ev;
+  mlpEvaluate(s, ev);
+  if (n != (int64_t)ev.part.size())
+    return fail(ESPP_EINVAL, "reference forces must cover every particle");
+  std::vector<std::array<double, 3>> fr(n);
+  for (int64_t k = 0; k < n; ++k) {
+    auto it = ev.idx.find(ids[k]);
+    if (it == ev.idx.end()) return fail(ESPP_EINVAL, "particle id not present");
+    for (int c = 0; c < 3; ++c) fr[it->second][c] = fref[3 * k + c];
+  }
+  std::vector<double> g;
+  double l = mlpFmGrad(s, ev, fr, g);
+  for (int q = 0; q < espp_mlp::NP; ++q) s->mlp->grad[q] += g[q];
+  if (loss) *loss = l;
+  if (grad) std::copy(g.begin(), g.end(), grad);
+  return ESPP_OK;
+}
+
+int espp_mlp_adam_step(espp_mlp* m, double lr, double beta1, double beta2, double eps,
+                       double gscale) {
+  if (!m) return fail(ESPP_EINVAL, "null model");
+  m->t += 1;
+  double c1 = 1.0 - std::pow(beta1, (double)m->t), c2 = 1.0 - std::pow(beta2, (double)m->t);
+  for (int q = 0; q < espp_mlp::NP; ++q) {
+    double g = m->grad[q] * gscale;
+    m->am[q] = beta1 * m->am[q] + (1 - beta1) * g;
+    m->av[q] = beta2 * m->av[q] + (1 - beta2) * g * g;
+    m->theta[q] -= lr * (m->am[q] / c1) / (std::sqrt(m->av[q] / c2) + eps);
+    m->grad[q] = 0.0;
+  }
+  return ESPP_OK;
+}
+
 int espp_run(espp_system* s, int64_t nsteps) {
   CHECK_S(s);
   return run(s, nsteps);
@@ -1263,6 +1574,13 @@ int espp_energy(espp_system* s, int32_t which, double* e) {
         minImageBox(s, pr.first->r, pr.second->r, d);
         es += s->tabBond.energy(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
       }
+  } else if (which == ESPP_IA_MLP) {
+    if (s->mlp && s->has_vl) {
+      ghostComm(s, true, false);
+      MlpEval ev;
+      mlpEvaluate(s, ev);
+      for (double e : ev.E) es += e;
+    }
   } else {
     return fail(ESPP_EINVAL, "unknown interaction kind");
   }
