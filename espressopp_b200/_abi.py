@@ -53,6 +53,7 @@ PROTOTYPES = {
     "espp_virial_tensor": (c_int32, [_P, c_int32, _D]),
     "espp_kinetic": (c_int32, [_P, _D, _I64]),
     "espp_rdf": (c_int32, [_P, c_int32, _D]),
+    "espp_force_acc": (c_int32, [_P, c_int32, c_int64, _I64, _D]),
     "espp_mlp_create": (c_int32, [c_double, c_double, POINTER(c_void_p)]),
     "espp_mlp_destroy": (c_int32, [_P]),
     "espp_mlp_num_params": (c_int32, [_I64]),

@@ -182,6 +182,9 @@ struct espp_system {
   float* mlpTan = nullptr;
   float* mlpPart = nullptr;
   double* mlpFref = nullptr;
+  // sums of total forces by particle id (espp_force_acc)
+  double* facc = nullptr;
+  int faccSpan = 0;
 
   // integrator
   double dt = 0.005;
@@ -1280,6 +1283,7 @@ void destroy(espp_system* s) {
   dfree(s->mlpTan);
   dfree(s->mlpPart);
   dfree(s->mlpFref);
+  dfree(s->facc);
   dfree(s->stIds);
   dfree(s->stPos);
   dfree(s->stVel);
@@ -1919,6 +1923,41 @@ int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n) {
     cuda_check(cudaMemcpyAsync(sum_mv2, s->obs, sizeof(double), cudaMemcpyDeviceToHost, s->st),
                "download");
     sync(s);
+  });
+}
+
+int espp_force_acc(espp_system* s, int32_t op, int64_t n, const int64_t* ids, double* out) {
+  return guard([&] {
+    checked(s);
+    ensure_id_map(s);
+    if (!s->facc || s->faccSpan != s->idSpan) {
+      dfree(s->facc);
+      s->facc = dalloc<double>(3 * (size_t)std::max(s->idSpan, 1));
+      s->faccSpan = s->idSpan;
+      op = 0;
+      cuda_check(cudaMemsetAsync(s->facc, 0, sizeof(double) * 3 * std::max(s->idSpan, 1),
+                                 s->st), "memset");
+    }
+    if (op == 0) {
+      cuda_check(cudaMemsetAsync(s->facc, 0, sizeof(double) * 3 * std::max(s->idSpan, 1),
+                                 s->st), "memset");
+    } else if (op == 1) {
+      launch_force_acc_add(s->view(), s->facc, s->st);
+    } else if (op == 2) {
+      if (n <= 0) return;
+      if (!ids || !out) raise(ESPP_EINVAL, "null argument");
+      ensure_stage(s, n);
+      cuda_check(cudaMemcpyAsync(s->stIds, ids, sizeof(int64_t) * n, cudaMemcpyHostToDevice,
+                                 s->st), "upload");
+      launch_force_acc_read(s->view(), (int)n, s->stIds, s->facc, s->stF, s->st);
+      cuda_check(cudaMemcpyAsync(out, s->stF, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost,
+                                 s->st), "download");
+      sync(s);
+      check_err(s);
+    } else {
+      raise(ESPP_EINVAL, "op must be 0 (clear), 1 (add) or 2 (read)");
+    }
+    cuda_check(cudaGetLastError(), "force accumulator");
   });
 }
 

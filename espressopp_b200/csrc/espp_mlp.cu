@@ -487,3 +487,37 @@ void launch_scatter3_by_id(const DevView& d, int n, const int64_t* ids, const do
                                                       out, d.err);
 }
 }  // namespace espp
+
+namespace espp {
+namespace {
+// acc[3 (id - idMin) + c] += total force of that particle
+__global__ void k_force_acc_add(DevView d, double* acc) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.n) return;
+  const int64_t off = d.pa[0].id[k] - d.idMin;
+  if (off < 0 || off >= d.idSpan) return;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) acc[3 * off + c] += d.ftot[(size_t)c * d.cap + k];
+}
+__global__ void k_force_acc_read(DevView d, int n, const int64_t* ids, const double* acc,
+                                 double* out) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int64_t off = ids[r] - d.idMin;
+  if (off < 0 || off >= d.idSpan) {
+    atomicOr(d.err, kErrIdRange);
+    return;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) out[3 * (size_t)r + c] = acc[3 * off + c];
+}
+}  // namespace
+
+void launch_force_acc_add(const DevView& d, double* acc, cudaStream_t st) {
+  if (d.n > 0) k_force_acc_add<<<(d.n + 255) / 256, 256, 0, st>>>(d, acc);
+}
+void launch_force_acc_read(const DevView& d, int n, const int64_t* ids, const double* acc,
+                           double* out, cudaStream_t st) {
+  if (n > 0) k_force_acc_read<<<(n + 255) / 256, 256, 0, st>>>(d, n, ids, acc, out);
+}
+}  // namespace espp

@@ -45,6 +45,10 @@ void launch_mlp_adam(espp_mlp* m, double lr, double beta1, double beta2, double 
                      double gscale, cudaStream_t st);
 void launch_sum_site_energy(const DevView& d, double* partials, int nblocks, double* out,
                             cudaStream_t st);
+// force accumulator by particle id (espp_force_acc)
+void launch_force_acc_add(const DevView& d, double* acc, cudaStream_t st);
+void launch_force_acc_read(const DevView& d, int n, const int64_t* ids, const double* acc,
+                           double* out, cudaStream_t st);
 // out[3 id2idx[ids[k]] + c] = vals[3 k + c]
 void launch_scatter3_by_id(const DevView& d, int n, const int64_t* ids, const double* vals,
                            double* out, cudaStream_t st);

@@ -68,8 +68,9 @@ def polymerRW(pid, startpos, numberOfMonomers, bondlength, return_angles=False,
 
 def polymer_melt(nchains, nbeads, density, bondlen=0.97, mindist=0.8, seed=3, tries=64):
     """Kremer-Grest melt of nchains x nbeads beads at bead density `density` in a cubic
-    periodic box.  Returns (positions (N, 3) in [0, L), bonds (M, 2) of 1-based ids
-    numbered chain by chain, box length L).  Seeded: numpy PCG64(seed)."""
+    periodic box.  Returns (positions (N, 3), unwrapped along each chain so that bonded
+    beads are one bond length apart, bonds (M, 2) of 1-based ids numbered chain by chain,
+    box length L).  Seeded: numpy PCG64(seed)."""
     N = nchains * nbeads
     L = (N / density) ** (1.0 / 3.0)
     rng = np.random.Generator(np.random.PCG64(seed))
@@ -78,11 +79,13 @@ def polymer_melt(nchains, nbeads, density, bondlen=0.97, mindist=0.8, seed=3, tr
     ncell = max(3, int(L / (bondlen + mindist)))
     csz = L / ncell
     grid = {}
-    pos = np.empty((N, 3))
+    pos = np.empty((N, 3))    # wrapped into the box, for the neighbour search
+    unw = np.empty((N, 3))    # unwrapped along the chains
     md2 = mindist * mindist
 
     def cell_of(p):
-        return (int(p[0] / csz) % ncell, int(p[1] / csz) % ncell, int(p[2] / csz) % ncell)
+        return (math.floor(p[0] / csz) % ncell, math.floor(p[1] / csz) % ncell,
+                math.floor(p[2] / csz) % ncell)
 
     def near(p):
         cx, cy, cz = cell_of(p)
@@ -104,6 +107,7 @@ def polymer_melt(nchains, nbeads, density, bondlen=0.97, mindist=0.8, seed=3, tr
         return np.min(np.einsum("ijk,ijk->ij", d, d), axis=1)
 
     def place(k, p):
+        unw[k] = p
         p = p - L * np.floor(p / L)
         pos[k] = p
         grid.setdefault(cell_of(p), []).append(k)
@@ -117,7 +121,7 @@ def polymer_melt(nchains, nbeads, density, bondlen=0.97, mindist=0.8, seed=3, tr
         place(k, start)
         k += 1
         for _ in range(nbeads - 1):
-            prev = pos[k - 1].copy()
+            prev = unw[k - 1].copy()
             nb = near(prev)
             best_c, best_d = None, -1.0
             for _ in range(0, tries, 8):
@@ -135,4 +139,4 @@ def polymer_melt(nchains, nbeads, density, bondlen=0.97, mindist=0.8, seed=3, tr
             k += 1
     ids = np.arange(1, N + 1).reshape(nchains, nbeads)
     bonds = np.stack([ids[:, :-1].reshape(-1), ids[:, 1:].reshape(-1)], 1)
-    return pos, bonds.astype(np.int64), L
+    return unw, bonds.astype(np.int64), L

@@ -208,6 +208,14 @@ ESPP_API int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n);
  * bin divided by 2 pi dr rho N ((i + 1/2)^2 dr^2 + dr^2 / 12).  out receives rdfN values. */
 ESPP_API int espp_rdf(espp_system* s, int32_t rdfN, double* out);
 
+/* Sums of the total force (the force espp_get_particles reports) by particle id, kept on
+ * the device across runs and re-sorts: op 0 clears the sums, op 1 adds the current total
+ * forces, op 2 copies the sums of the particles ids (3 per particle) to out.  Serves
+ * time averages of forces, e.g. mapped forces over a window of steps.  No counterpart in
+ * the reference. */
+ESPP_API int espp_force_acc(espp_system* s, int32_t op, int64_t n, const int64_t* ids,
+                            double* out);
+
 /* ---- learned coarse-grained potential -------------------------------------------------
  * No counterpart in the reference: a many-body pair potential for coarse-grained sites,
  * with interaction::Tabulated as its fallback.  Per particle i a descriptor of 16

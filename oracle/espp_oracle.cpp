@@ -391,6 +391,7 @@ struct espp_system {
   double cap[3] = {0, 0, 0};
   int langPhase = 0;
   espp_mlp* mlp = nullptr;
+  std::unordered_map<int64_t, std::array<double, 3>> facc;
 };
 
 namespace {
@@ -1418,6 +1419,27 @@ int espp_capforce_set(espp_system* s, int32_t mode, const double cap[3]) {
   CHECK_S(s);
   s->capMode = mode;
   for (int k = 0; k < 3; ++k) s->cap[k] = cap ? cap[k] : 0.0;
+  return ESPP_OK;
+}
+
+int espp_force_acc(espp_system* s, int32_t op, int64_t n, const int64_t* ids, double* out) {
+  CHECK_S(s);
+  if (op == 0) {
+    s->facc.clear();
+  } else if (op == 1) {
+    for (int ci : s->realCells)
+      for (auto& p : s->cells[ci].p) {
+        auto& a = s->facc[p.id];
+        for (int c = 0; c < 3; ++c) a[c] += p.f[c];
+      }
+  } else if (op == 2) {
+    for (int64_t k = 0; k < n; ++k) {
+      auto it = s->facc.find(ids[k]);
+      for (int c = 0; c < 3; ++c) out[3 * k + c] = it == s->facc.end() ? 0.0 : it->second[c];
+    }
+  } else {
+    return fail(ESPP_EINVAL, "op must be 0 (clear), 1 (add) or 2 (read)");
+  }
   return ESPP_OK;
 }
 
