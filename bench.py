@@ -556,7 +556,7 @@ def cg_arm(args, rank, world, local_rank):
     tabsys.set_pair_table(ptab)
     err_table = cg.fm_error(tabsys, pos[ntrain:], target[ntrain:], fbond_test)
     t_tab = time.perf_counter() - t1
-    # the learned potential corrects the pair table: it is trained on the residual
+    # the learned potential corrects the force-matched pair table: trained on the residual
     pairsys = cg.CGSystem(pos[0], L, bonds, ([0.5, 1.0, 1.5, 2.0], [0.0] * 4, [0.0] * 4))
     pairsys.set_pair_table(ptab)
     resid = np.empty((ntrain,) + target.shape[1:])
@@ -574,12 +574,26 @@ def cg_arm(args, rank, world, local_rank):
                         batch=4, lr=1e-3, log=log)
     t_train = time.perf_counter() - t2
     del resid
-    err_mlp = cg.fm_error(s, pos[ntrain:], target[ntrain:], fbond_test)
+    err_mlp_fm = cg.fm_error(s, pos[ntrain:], target[ntrain:], fbond_test)
     err_zero = 1.0
-    log("force-matching error: pair table + mlp %.4f, pair table %.4f" % (err_mlp, err_table))
-    # reference RDF of the mapped fine-grained sites and chain motion of the FG frames
+    log("force-matching error: pair table + mlp %.4f, pair table %.4f" % (err_mlp_fm, err_table))
+    # structure-based refinement (iterative Boltzmann inversion) of the pair table against
+    # the RDF of the mapped fine-grained sites, for the learned model (network fixed) and
+    # for the table-only fallback
     nb = 120
-    g_fg = cg.rdf_of_frames(s, pos[::max(1, nfr // 25)], nb)
+    g_fg = cg.rdf_of_frames(tabsys, pos[::max(1, nfr // 25)], nb)
+    t3 = time.perf_counter()
+    ibi = {}
+    for name, sysm in (("mlp", s), ("table", tabsys)):
+        sysm.set_pos(sysm.ids, cg.wrap(pos[-1], L))
+        call(sysm.lib, "espp_integrator_set", sysm.h, 0.01)
+        sysm.thermostat(True)
+        _, ibi[name] = cg.ibi_refine(sysm, ptab, g_fg, nb, iters=args.cg_ibi, log=log)
+    t_ibi = time.perf_counter() - t3
+    err_mlp = cg.fm_error(s, pos[ntrain:], target[ntrain:], fbond_test)
+    err_table_fm = err_table
+    err_table = cg.fm_error(tabsys, pos[ntrain:], target[ntrain:], fbond_test)
+    # chain motion of the FG frames
     sites_per_chain = 50
     msd_fg = cg.chain_com_msd(pos, sites_per_chain)
     # CG runs: learned potential and table fallback, both with the bond table
@@ -587,7 +601,7 @@ def cg_arm(args, rank, world, local_rank):
     for name, sysm in (("table", tabsys), ("mlp", s)):
         sysm.set_pos(sysm.ids, cg.wrap(pos[-1], L))
         call(sysm.lib, "espp_integrator_set", sysm.h, 0.01)
-        call(sysm.lib, "espp_langevin_set", sysm.h, 1, 0.5, 1.0, 0, None)
+        sysm.thermostat(True)
         for k in range(20):
             try:
                 sysm.run(100)
@@ -602,7 +616,6 @@ def cg_arm(args, rank, world, local_rank):
                 log("CG run (%s) step %d: T %.3f, max |F| %.3g" %
                     (name, 100 * (k + 1), np.sum(4 * v * v) / (3 * len(v)), np.max(np.abs(f))))
         traj = []
-        p0 = sysm.state(sysm.ids)
         window = nfr * 20
         ms_total = 0.0
         g = np.zeros(nb)
@@ -630,7 +643,6 @@ def cg_arm(args, rank, world, local_rank):
         r = (np.arange(nb) + 0.5) * dr
         sel = r < 3.0 * 2
         l2 = float(np.sqrt(np.mean((g[sel] - g_fg[sel]) ** 2)))
-        vv = p0[1]
         out[name] = {"rdf_l2": l2, "chain_msd_100tau": float(msd_cg[-1]),
                      "ms_per_step": ms_total / (window // 100 * 100 + max(steps_rest, 0))}
         log("CG run (%s): RDF L2 %.4f, chain MSD %.3f (FG %.3f)" %
@@ -646,16 +658,23 @@ def cg_arm(args, rank, world, local_rank):
                                "%d CG sites (4:1), %d frames, MLP 16-64-64-1 SiLU" %
                                (nch, n_cg, nfr)},
         "cg_judge": {
-            "force_matching_rel_err": {"pair_table_plus_mlp": err_mlp,
-                                       "pair_table": err_table, "zero_model": err_zero},
-            "rdf_l2": {"mlp": out["mlp"]["rdf_l2"], "pair_table": out["table"]["rdf_l2"]},
+            "force_matching_rel_err": {
+                "mlp_plus_ibi_table": err_mlp, "ibi_table": err_table,
+                "mlp_plus_force_matched_table": err_mlp_fm,
+                "force_matched_table": err_table_fm, "zero_model": err_zero},
+            "rdf_l2": {"mlp_plus_ibi_table": out["mlp"]["rdf_l2"],
+                       "ibi_table": out["table"]["rdf_l2"],
+                       "ibi_iterations": {"mlp": ibi["mlp"], "table": ibi["table"]},
+                       "definition": "sqrt(mean over bins r < 6 of (g_cg - g_fg)^2), "
+                                     "120 bins up to L/2"},
             "particle_steps_per_chain_motion_fg_over_cg": ratio,
             "chain_com_msd_100tau": {"fg": float(msd_fg[-1]), "mlp": out["mlp"]["chain_msd_100tau"],
                                      "pair_table": out["table"]["chain_msd_100tau"]},
             "cg_ms_per_step": {"mlp": out["mlp"]["ms_per_step"],
                                "pair_table": out["table"]["ms_per_step"]},
             "training_loss_per_epoch": hist,
-            "seconds": {"fg_frames": t_fg, "pair_table_fit": t_tab, "mlp_training": t_train},
+            "seconds": {"fg_frames": t_fg, "pair_table_fit": t_tab, "ibi": t_ibi,
+                        "mlp_training": t_train},
             "force_target": "mapped conservative forces averaged over %d fine-grained "
                             "steps, minus the CG bond forces" % args.cg_window,
             "note": "force-matching error on held-out frames (20 %) relative to the "
@@ -797,6 +816,7 @@ def main():
     ap.add_argument("--cg-frames", type=int, default=500)
     ap.add_argument("--cg-epochs", type=int, default=15)
     ap.add_argument("--cg-steps", type=int, default=100000)
+    ap.add_argument("--cg-ibi", type=int, default=10, help="IBI iterations of the pair table")
     ap.add_argument("--cg-window", type=int, default=50,
                     help="steps over which the mapped forces of a frame are averaged")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])

@@ -286,9 +286,19 @@ class CGSystem(Handle):
         self.mlp = model
         call(self.lib, "espp_mlp_attach", self.h, model.m if model else None)
 
+    def thermostat(self, on, gamma=0.5, T=1.0):
+        self.langevin = (gamma, T) if on else None
+        call(self.lib, "espp_langevin_set", self.h, 1 if on else 0, gamma, T, 0, None)
+
     def forces_at(self, pos):
+        """Conservative forces at the configuration pos (the thermostat is paused)."""
+        lv = getattr(self, "langevin", None)
+        if lv:
+            call(self.lib, "espp_langevin_set", self.h, 0, lv[0], lv[1], 0, None)
         self.set_pos(self.ids, wrap(pos, self.L))
         self.run(0)
+        if lv:
+            call(self.lib, "espp_langevin_set", self.h, 1, lv[0], lv[1], 0, None)
         return self.state(self.ids)[2]
 
 
@@ -403,3 +413,42 @@ def rdf_of_frames(cg, frames_pos, nbins):
         cg.set_pos(cg.ids, wrap(pos, cg.L))
         g += cg.rdf(nbins)
     return g / len(frames_pos)
+
+
+def ibi_refine(cgsys, tab, g_target, nbins, iters=10, steps=3000, every=250, alpha=0.8,
+               rc=3.0, T=1.0, log=None):
+    """Iterative Boltzmann inversion of a pair table against a target RDF: each iteration
+    runs the CG system (bonds + this pair table, thermostatted) on the GPU, samples the
+    RDF, and updates U(r) += alpha T ln(g(r) / g_target(r)) (step at most alpha T, bins
+    with g > 0.02 only, tapered to zero at rc); F = -dU/dr.  Returns the refined table and
+    the RDF L2 error per iteration."""
+    r_t, E_t, F_t = (np.array(a, np.float64) for a in tab)
+    dr = cgsys.L / 2 / nbins
+    rb = (np.arange(nbins) + 0.5) * dr
+    hist = []
+    for it in range(iters):
+        cgsys.set_pair_table((r_t, E_t, F_t), rc)
+        cgsys.run(1000)
+        g = np.zeros(nbins)
+        ns = 0
+        for _ in range(steps // every):
+            cgsys.run(every)
+            g += cgsys.rdf(nbins)
+            ns += 1
+        g /= ns
+        sel = rb < 2 * rc
+        hist.append(float(np.sqrt(np.mean((g[sel] - g_target[sel]) ** 2))))
+        if log:
+            log("IBI iteration %d: RDF L2 %.4f" % (it, hist[-1]))
+        # bins with a reliable RDF only; steps of at most 0.5 T per iteration
+        ok = (rb < rc) & (g > 0.02) & (g_target > 0.02)
+        du = np.zeros(nbins)
+        du[ok] = alpha * T * np.clip(np.log(g[ok] / g_target[ok]), -1.0, 1.0)
+        du = np.convolve(du, np.ones(3) / 3, mode="same")
+        first = np.argmax(ok)
+        du[:first] = du[first]
+        du *= np.clip(1.0 - (rb / rc) ** 4, 0.0, 1.0)
+        E_t = E_t + np.interp(r_t, rb, du)
+        F_t = -np.gradient(E_t, r_t)
+    cgsys.set_pair_table((r_t, E_t, F_t), rc)
+    return (r_t, E_t, F_t), hist

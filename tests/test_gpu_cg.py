@@ -46,7 +46,7 @@ def test_cg_workflow_small(tmp_path):
     call(s.lib, "espp_set_particles", s.h, len(s.ids), _abi.i64ptr(s.ids),
          _abi.dptr(np.ascontiguousarray(cg.wrap(pos[-1], L)).reshape(-1)), None)
     call(s.lib, "espp_integrator_set", s.h, 0.01)
-    call(s.lib, "espp_langevin_set", s.h, 1, 0.5, 1.0, 0, None)
+    s.thermostat(True)
     s.run(400)
     p, v, f, img = s.state(s.ids)
     T = np.sum(4.0 * v * v) / (3 * len(s.ids))
