@@ -56,6 +56,7 @@ PROTOTYPES = {
     "espp_force_acc": (c_int32, [_P, c_int32, c_int64, _I64, _D]),
     "espp_mlp_create": (c_int32, [c_double, c_double, POINTER(c_void_p)]),
     "espp_mlp_destroy": (c_int32, [_P]),
+    "espp_mlp_set_mode": (c_int32, [_P, c_int32]),
     "espp_mlp_num_params": (c_int32, [_I64]),
     "espp_mlp_set_params": (c_int32, [_P, c_int64, _D]),
     "espp_mlp_get_params": (c_int32, [_P, c_int64, _D]),

@@ -487,6 +487,7 @@ void check_err(espp_system* s) {
   if (e & kErrBondMissing) raise(ESPP_ESTATE, "bond partner not present");
   if (e & kErrIdRange) raise(ESPP_ESTATE, "particle id outside the id map");
   if (e & kErrNlOverflow) raise(ESPP_EOVERFLOW, "Verlet list capacity exceeded");
+  if (e & kErrTimeout) raise(ESPP_ETIMEOUT, "a bounded wait inside a kernel ran out");
 }
 
 // Re-sort the particles by cell (fold = Storage::decompose semantics).
@@ -1969,6 +1970,7 @@ int espp_mlp_create(double rc, double r0, espp_mlp** out) {
     cuda_check(cudaGetDevice(&m->device), "cudaGetDevice");
     m->rc = rc;
     m->r0 = r0;
+    if (const char* e = std::getenv("ESPP_B200_MLP_TC")) m->tensor_cores = std::atoi(e) ? 1 : 0;
     m->theta = dalloc<float>(kMlpParams);
     m->grad = dalloc<float>(kMlpParams);
     m->adam_m = dalloc<float>(kMlpParams);
@@ -1983,6 +1985,13 @@ int espp_mlp_create(double rc, double r0, espp_mlp** out) {
     cuda_check(cudaMemcpy(m->scale, one.data(), sizeof(float) * kMlpK, cudaMemcpyHostToDevice),
                "upload");
     *out = m.release();
+  });
+}
+
+int espp_mlp_set_mode(espp_mlp* m, int32_t tensor_cores) {
+  return guard([&] {
+    if (!m) raise(ESPP_EINVAL, "null model");
+    m->tensor_cores = tensor_cores ? 1 : 0;
   });
 }
 

@@ -27,6 +27,7 @@ enum : unsigned {
   kErrOutside = 1u << 2,       // non-finite or out-of-grid coordinate at re-binning
   kErrBondMissing = 1u << 3,   // bond partner id not present
   kErrIdRange = 1u << 4,       // particle id outside the dense id map
+  kErrTimeout = 1u << 5,       // a bounded wait inside a kernel ran out
 };
 
 // Lennard-Jones parameters of one type pair (LennardJones.hpp:79-87 preset()).
@@ -97,6 +98,7 @@ struct MlpDev {
   float* D;               // per particle: dE/dG (cap x K)
   float* E;               // per particle: site energy (cap)
   int on;
+  int tc;                 // site network on the tensor cores (BF16) instead of FP32
 };
 
 // One interpolation table of interaction::Tabulated (InterpolationLinear / Akima / Cubic)

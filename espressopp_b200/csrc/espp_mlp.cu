@@ -1,5 +1,6 @@
 // Learned coarse-grained pair potential: descriptor, site network, forces, and the
 // force-matching gradient on the GPU.  Model and training scheme: espp_mlp.h.
+#include <cuda_bf16.h>
 #include <math.h>
 #include <stdint.h>
 
@@ -409,6 +410,7 @@ MlpDev mlp_view(const espp_mlp* m) {
   v.shift = m->shift;
   v.scale = m->scale;
   v.on = 1;
+  v.tc = m->tensor_cores;
   return v;
 }
 
@@ -417,11 +419,17 @@ int mlp_grad_blocks(int n) {
   return tiles < kGradBlocks ? (tiles > 0 ? tiles : 1) : kGradBlocks;
 }
 
+void launch_mlp_site_tc(const DevView& d, cudaStream_t st);
+
 void launch_mlp_energy_terms(const DevView& d, cudaStream_t st) {
   if (d.n == 0) return;
   k_mlp_desc<<<(d.n + 255) / 256, 256, 0, st>>>(d);
-  const int tiles = (d.n + kSiteTile - 1) / kSiteTile;
-  k_mlp_site<<<tiles < 1184 ? tiles : 1184, H, 0, st>>>(d.mlp, d.n);
+  if (d.mlp.tc) {
+    launch_mlp_site_tc(d, st);
+  } else {
+    const int tiles = (d.n + kSiteTile - 1) / kSiteTile;
+    k_mlp_site<<<tiles < 1184 ? tiles : 1184, H, 0, st>>>(d.mlp, d.n);
+  }
 }
 
 void launch_mlp_forces(const DevView& d, bool mixed, float* fout, cudaStream_t st) {
@@ -520,4 +528,349 @@ void launch_force_acc_read(const DevView& d, int n, const int64_t* ids, const do
                            double* out, cudaStream_t st) {
   if (n > 0) k_force_acc_read<<<(n + 255) / 256, 256, 0, st>>>(d, n, ids, acc, out);
 }
+}  // namespace espp
+
+// ---- site network on the tensor cores (tcgen05, BF16 operands, FP32 accumulators) ----
+//
+// One CTA of 128 threads per tile of 128 sites, persistent over tiles.  The four
+// products of a tile run as tcgen05.mma (cta_group::1, kind::f16, M = 128) with A and B
+// in shared memory (K-major, no swizzle) and the accumulators in tensor memory:
+//   Z1 = X  W1^T  (N = 64, K = 16)     -> H1 = silu(Z1 + b1)
+//   Z2 = H1 W2^T  (N = 64, K = 64)     -> E = w3.silu(Z2 + b2) + b3, P2 = w3 * silu'(Z2 + b2)
+//   G1 = P2 W2    (N = 64, K = 64)     -> P1 = G1 * silu'(Z1 + b1)
+//   DX = P1 W1    (N = 16, K = 64)     -> D = DX * scale
+// Thread t of the CTA owns site row t: TMEM lane t, read back with tcgen05.ld 32x32b.
+// Operand layout ("canonical K-major, no swizzle"): core matrices of 8 rows x 16 bytes,
+// row r, k-chunk c (8 elements) at byte ((c * R/8 + r/8) * 8 + r%8) * 16 for R rows:
+// SBO (next 8-row group) = 128 B, LBO (next k-chunk) = R * 16 B.
+namespace espp {
+namespace {
+
+constexpr int kTcRows = 128;
+constexpr int kTcCols = 256;              // TMEM columns: Z1 0, Z2 64, G1 128, DX 192
+constexpr long long kTcSpin = 1ll << 26;  // bounded mbarrier wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// byte offset of element (r, k) in a canonical K-major operand of R rows
+__device__ __forceinline__ int canon_off(int r, int k, int R) {
+  return (((k >> 3) * (R >> 3) + (r >> 3)) * 8 + (r & 7)) * 16 + (k & 7) * 2;
+}
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, int R) {
+  const uint64_t lbo = (uint64_t)(R * 16) >> 4, sbo = 128 >> 4;
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | (lbo << 16) | (sbo << 32) | (1ull << 46);
+}
+
+// kind::f16 instruction descriptor: BF16 x BF16 -> F32, K-major A and B, M = 128
+__host__ __device__ constexpr uint32_t umma_idesc(int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(kTcRows >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                     int accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u),
+        "r"(0u));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
+  for (long long it = 0; it < kTcSpin; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// writes 64 values of row r (8 k-chunks of 16 bytes) into a canonical 128-row operand
+__device__ __forceinline__ void store_row64(uint8_t* base, int r, const float* v) {
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    uint4 q;
+    q.x = pack_bf16(v[8 * c + 0], v[8 * c + 1]);
+    q.y = pack_bf16(v[8 * c + 2], v[8 * c + 3]);
+    q.z = pack_bf16(v[8 * c + 4], v[8 * c + 5]);
+    q.w = pack_bf16(v[8 * c + 6], v[8 * c + 7]);
+    *reinterpret_cast<uint4*>(base + canon_off(r, 8 * c, kTcRows)) = q;
+  }
+}
+
+struct TcSmem {
+  alignas(128) uint8_t P[kTcRows * H * 2];  // X (first 4 KB), then H1, then P1
+  alignas(128) uint8_t Q[kTcRows * H * 2];  // P2
+  alignas(128) uint8_t W1[H * K * 2];       // B of Z1: W1 [64 x 16]
+  alignas(128) uint8_t W2[H * H * 2];       // B of Z2: W2 [64 x 64]
+  alignas(128) uint8_t W2T[H * H * 2];      // B of G1: W2^T
+  alignas(128) uint8_t W1T[K * H * 2];      // B of DX: W1^T [16 x 64]
+  float b1[H], b2[H], w3[H], scale[K], shift[K];
+  alignas(8) unsigned long long mbar;
+  uint32_t tmem;
+  int abort;
+};
+
+__global__ void __launch_bounds__(kTcRows) k_mlp_site_tc(MlpDev m, int n, unsigned* err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  TcSmem& S = *reinterpret_cast<TcSmem*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int t = threadIdx.x;
+  const int warp = t >> 5;
+  const float* th = m.theta;
+  // weights as BF16 operands
+  for (int e = t; e < H * K; e += kTcRows) {
+    const int o = e / K, k = e % K;  // W1[o][k]
+    const __nv_bfloat16 v = __float2bfloat16_rn(th[e]);
+    *reinterpret_cast<__nv_bfloat16*>(S.W1 + canon_off(o, k, H)) = v;
+    *reinterpret_cast<__nv_bfloat16*>(S.W1T + canon_off(k, o, K)) = v;
+  }
+  for (int e = t; e < H * H; e += kTcRows) {
+    const int o = e / H, u = e % H;  // W2[o][u]
+    const __nv_bfloat16 v = __float2bfloat16_rn(th[kOffW2 + e]);
+    *reinterpret_cast<__nv_bfloat16*>(S.W2 + canon_off(o, u, H)) = v;
+    *reinterpret_cast<__nv_bfloat16*>(S.W2T + canon_off(u, o, H)) = v;
+  }
+  if (t < H) {
+    S.b1[t] = th[kOffB1 + t];
+    S.b2[t] = th[kOffB2 + t];
+    S.w3[t] = th[kOffW3 + t];
+  }
+  if (t < K) {
+    S.scale[t] = m.scale[t];
+    S.shift[t] = m.shift[t];
+  }
+  const float b3 = th[kOffB3];
+  const uint32_t mbar = smem_u32(&S.mbar);
+  if (t == 0) {
+    S.abort = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&S.tmem)),
+                 "r"(kTcCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = S.tmem;
+  const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's lanes
+  const uint32_t aP = smem_u32(S.P), aQ = smem_u32(S.Q);
+  const uint32_t aW1 = smem_u32(S.W1), aW2 = smem_u32(S.W2), aW2T = smem_u32(S.W2T),
+                 aW1T = smem_u32(S.W1T);
+  uint32_t phase = 0;
+  auto wait_mma = [&]() {
+    if (!mbar_wait(mbar, phase)) {
+      S.abort = 1;
+      atomicOr(err, kErrTimeout);
+    }
+    phase ^= 1u;
+    tc_fence_after();
+  };
+  for (int s0 = blockIdx.x * kTcRows; s0 < n; s0 += gridDim.x * kTcRows) {
+    const int i = s0 + t;
+    // X tile: 16 normalised descriptor values of site row t (zeros past n)
+    {
+      float x[16];
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        x[k] = i < n ? (m.G[(size_t)i * K + k] - S.shift[k]) * S.scale[k] : 0.f;
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        uint4 q;
+        q.x = pack_bf16(x[8 * c + 0], x[8 * c + 1]);
+        q.y = pack_bf16(x[8 * c + 2], x[8 * c + 3]);
+        q.z = pack_bf16(x[8 * c + 4], x[8 * c + 5]);
+        q.w = pack_bf16(x[8 * c + 6], x[8 * c + 7]);
+        *reinterpret_cast<uint4*>(S.P + canon_off(t, 8 * c, kTcRows)) = q;
+      }
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (S.abort) break;
+    if (t == 0) {
+      tc_fence_after();
+      umma(tmem + 0, umma_desc(aP, kTcRows), umma_desc(aW1, H), umma_idesc(H), 0);
+      umma_commit(mbar);
+    }
+    wait_mma();
+    // H1 = silu(Z1 + b1)
+    {
+      float v[H];
+#pragma unroll
+      for (int q = 0; q < H / 16; ++q) tmem_ld16(tl + 0 + 16 * q, v + 16 * q);
+      tmem_wait_ld();
+#pragma unroll
+      for (int u = 0; u < H; ++u) v[u] = silu(v[u] + S.b1[u]);
+      store_row64(S.P, t, v);
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (S.abort) break;
+    if (t == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (int kb = 0; kb < H / 16; ++kb)
+        umma(tmem + 64, umma_desc(aP + kb * 2 * kTcRows * 16, kTcRows),
+             umma_desc(aW2 + kb * 2 * H * 16, H), umma_idesc(H), kb > 0);
+      umma_commit(mbar);
+    }
+    wait_mma();
+    // E and P2 = w3 * silu'(Z2 + b2)
+    {
+      float v[H];
+#pragma unroll
+      for (int q = 0; q < H / 16; ++q) tmem_ld16(tl + 64 + 16 * q, v + 16 * q);
+      tmem_wait_ld();
+      float e = b3;
+#pragma unroll
+      for (int u = 0; u < H; ++u) {
+        const float z = v[u] + S.b2[u];
+        e += S.w3[u] * silu(z);
+        v[u] = S.w3[u] * silu1(z);
+      }
+      if (i < n) m.E[i] = e;
+      store_row64(S.Q, t, v);
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (S.abort) break;
+    if (t == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (int kb = 0; kb < H / 16; ++kb)
+        umma(tmem + 128, umma_desc(aQ + kb * 2 * kTcRows * 16, kTcRows),
+             umma_desc(aW2T + kb * 2 * H * 16, H), umma_idesc(H), kb > 0);
+      umma_commit(mbar);
+    }
+    wait_mma();
+    // P1 = G1 * silu'(Z1 + b1)
+    {
+      float g[H], z[H];
+#pragma unroll
+      for (int q = 0; q < H / 16; ++q) {
+        tmem_ld16(tl + 128 + 16 * q, g + 16 * q);
+        tmem_ld16(tl + 0 + 16 * q, z + 16 * q);
+      }
+      tmem_wait_ld();
+#pragma unroll
+      for (int u = 0; u < H; ++u) g[u] *= silu1(z[u] + S.b1[u]);
+      store_row64(S.P, t, g);
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (S.abort) break;
+    if (t == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (int kb = 0; kb < H / 16; ++kb)
+        umma(tmem + 192, umma_desc(aP + kb * 2 * kTcRows * 16, kTcRows),
+             umma_desc(aW1T + kb * 2 * K * 16, K), umma_idesc(K), kb > 0);
+      umma_commit(mbar);
+    }
+    wait_mma();
+    {
+      float dx[16];
+      tmem_ld16(tl + 192, dx);
+      tmem_wait_ld();
+      if (i < n) {
+        float4* o = reinterpret_cast<float4*>(m.D + (size_t)i * K);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          o[q] = make_float4(dx[4 * q] * S.scale[4 * q], dx[4 * q + 1] * S.scale[4 * q + 1],
+                             dx[4 * q + 2] * S.scale[4 * q + 2],
+                             dx[4 * q + 3] * S.scale[4 * q + 3]);
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+  tc_fence_before();
+  __syncthreads();
+  // after a timed-out wait, give the outstanding product its own bounded wait before the
+  // tensor memory is released
+  if (S.abort && t == 0) mbar_wait(mbar, phase);
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTcCols));
+  }
+}
+
+}  // namespace
+
+size_t mlp_tc_smem() { return sizeof(TcSmem) + 1024; }
+
+void launch_mlp_site_tc(const DevView& d, cudaStream_t st) {
+  static int nsm[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  dev &= 63;
+  if (!nsm[dev]) {
+    cudaFuncSetAttribute(k_mlp_site_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)mlp_tc_smem());
+    cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
+    if (nsm[dev] <= 0) nsm[dev] = 148;
+  }
+  const int tiles = (d.n + kTcRows - 1) / kTcRows;
+  const int grid = tiles < 2 * nsm[dev] ? tiles : 2 * nsm[dev];
+  if (grid > 0) k_mlp_site_tc<<<grid, kTcRows, mlp_tc_smem(), st>>>(d.mlp, d.n, d.err);
+}
+
 }  // namespace espp

@@ -24,6 +24,7 @@ struct espp_mlp {
   float* shift = nullptr;   // kMlpK
   float* scale = nullptr;
   long long adam_t = 0;
+  int tensor_cores = 1;     // site network: 1 BF16 tcgen05, 0 FP32 CUDA cores
 };
 
 namespace espp {

@@ -1458,6 +1458,8 @@ int espp_mlp_destroy(espp_mlp* m) {
   return ESPP_OK;
 }
 
+int espp_mlp_set_mode(espp_mlp* m, int32_t) { return m ? ESPP_OK : fail(ESPP_EINVAL, "null model"); }
+
 int espp_mlp_num_params(int64_t* n) {
   *n = espp_mlp::NP;
   return ESPP_OK;

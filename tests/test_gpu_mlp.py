@@ -96,3 +96,31 @@ def test_mlp_training_lowers_the_loss_and_md_runs():
     e1 = s.energy(_abi.IA_MLP) + 0.5 * s.kinetic()[0]
     assert math.isfinite(e1) and abs(e1 - e0) / 400 < 1e-3
     _abi.call(lib, "espp_mlp_destroy", m)
+
+
+def test_mlp_tensor_core_site_network_matches_fp32():
+    """BF16 tcgen05 site network against the FP32 CUDA-core one on the same configuration
+    (1,000 sites: eight 128-site tiles, the last one partial) and against the oracle."""
+    lib = cuda_lib()
+    s, pos, box = cg_system(lib, n=1000, seed=8)
+    o, _, _ = cg_system(oracle_lib(), n=1000, seed=8)
+    m, _ = make_model(lib, seed=9)
+    mo, _ = make_model(oracle_lib(), seed=9)
+    _abi.call(lib, "espp_mlp_attach", s.h, m)
+    _abi.call(o.lib, "espp_mlp_attach", o.h, mo)
+    ids = np.arange(1, 1001)
+    res = {}
+    for mode in (0, 1):
+        _abi.call(lib, "espp_mlp_set_mode", m, mode)
+        s.integrator(0.002)
+        s.run(0)
+        res[mode] = (s.energy(_abi.IA_MLP), s.particles(ids)[2])
+    o.integrator(0.002)
+    o.run(0)
+    eo, fo = o.energy(_abi.IA_MLP), o.particles(ids)[2]
+    assert abs(res[0][0] - eo) < 1e-5 * abs(eo)
+    # BF16 operands: a few 1e-3 relative in energy and forces
+    assert abs(res[1][0] - eo) < 2e-2 * abs(eo)
+    assert _rel(res[1][1], fo) < 3e-2
+    assert _rel(res[1][1], res[0][1]) < 3e-2
+    _abi.call(lib, "espp_mlp_destroy", m)

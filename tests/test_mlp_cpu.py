@@ -24,6 +24,7 @@ def make_model(lib, seed=1, rc=3.0):
     shift = np.full(16, 0.5)
     scale = np.full(16, 0.8)
     _abi.call(lib, "espp_mlp_set_norm", m, _abi.dptr(shift), _abi.dptr(scale))
+    _abi.call(lib, "espp_mlp_set_mode", m, 0)  # FP32 site network: strict parity checks
     return m, theta
 
 
