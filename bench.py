@@ -685,6 +685,46 @@ def cg_arm(args, rank, world, local_rank):
     model.close()
 
 
+# ---- learned potential: force evaluation micro-benchmark --------------------------
+def mlp_arm(args, rank, world, local_rank):
+    """Device time of the learned potential's force pass (descriptor, site network,
+    pair forces) on a CG-like configuration: --mlp-sites sites at density 0.2125 on a
+    jittered lattice, seeded random weights, NVE steps of a CG system that holds only the
+    learned potential; site network on the tensor cores (BF16) and on CUDA cores (FP32)."""
+    from espressopp_b200 import cg
+    from espressopp_b200._abi import call, dptr
+    if rank != 0:
+        return
+    n_side = int(round(args.mlp_sites ** (1.0 / 3.0)))
+    pos, L = lattice(n_side, 0.2125, 0.3, 7)
+    n = len(pos)
+    zero = ([0.5, 1.0, 1.5, 2.0], [0.0] * 4, [0.0] * 4)
+    out = {}
+    for mode, name in ((1, "tensor_cores_bf16"), (0, "cuda_cores_fp32")):
+        sysm = cg.CGSystem(pos, L, np.zeros((0, 2), np.int64), zero)
+        model = cg.MLPModel(seed=5)
+        call(model.lib, "espp_mlp_set_mode", model.m, mode)
+        model.set_norm(np.full(16, 0.5), np.full(16, 1.0))
+        sysm.attach(model)
+        call(sysm.lib, "espp_integrator_set", sysm.h, 0.005)
+        sysm.run(args.warmup)
+        sysm.run(args.steps)
+        ms = np.zeros(2)
+        call(sysm.lib, "espp_last_run_ms", sysm.h, dptr(ms))
+        out[name] = {"ms_per_step": ms[1] / args.steps,
+                     "site_steps_per_s": n * args.steps / (ms[1] * 1e-3)}
+        sysm.close()
+        model.close()
+    line = {"metric": "learned-potential site-steps/s", "unit": "particle-steps/s",
+            "value": out["tensor_cores_bf16"]["site_steps_per_s"], "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "data": "synthetic",
+            "config": {"workload": "learned CG potential force pass, %d sites, rc 3.0, "
+                                   "16 basis functions, MLP 16-64-64-1" % n},
+            "modes": out}
+    print(json.dumps(line), flush=True)
+
+
 # ---- batched parallel-tempering replicas ------------------------------------------
 def replicas_arm(args, rank, world, local_rank):
     """64 LJ replicas, N ~ U{2000..64000} (seed 4), rho 0.8442, rc 2.5, skin 0.3,
@@ -809,9 +849,11 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="lj", choices=["lj", "replicas", "cg"],
+    ap.add_argument("--workload", default="lj", choices=["lj", "replicas", "cg", "mlp"],
                     help="lj: the 4,096,000-particle fluid (default); replicas: 64 PT "
-                         "replicas; cg: the learned coarse-grained potential")
+                         "replicas; cg: the learned coarse-grained potential; mlp: its "
+                         "force pass alone")
+    ap.add_argument("--mlp-sites", type=int, default=50000)
     ap.add_argument("--cg-chains", type=int, default=1000)
     ap.add_argument("--cg-frames", type=int, default=500)
     ap.add_argument("--cg-epochs", type=int, default=15)
@@ -841,6 +883,8 @@ def main():
         replicas_arm(args, rank, world, local_rank)
     elif args.workload == "cg":
         cg_arm(args, rank, world, local_rank)
+    elif args.workload == "mlp":
+        mlp_arm(args, rank, world, local_rank)
     else:
         gpu_arm(args, rank, world, local_rank)
 
