@@ -11,12 +11,13 @@ and standard_system.  Particles live on the GPU (libespp_b200.so, C ABI in
 include/espp_b200.h); there is no CPU fallback.
 """
 from ._lib import LIBRARY_PATH, load_library  # noqa: F401
-from .core import (FixedPairList, Int3D, Real3D, System, Tensor, VerletList,  # noqa: F401
-                   infinity, set_default_precision)
+from .core import (FixedPairList, FixedTripleList, Int3D, Real3D, System,  # noqa: F401
+                   Tensor, VerletList, infinity, set_default_precision)
 from . import analysis, bc, esutil, integrator, interaction, storage, tools  # noqa: F401
 from . import standard_system  # noqa: F401
 from .parallel_tempering import ParallelTempering  # noqa: F401
 
-__all__ = ["System", "VerletList", "FixedPairList", "Real3D", "Int3D", "Tensor", "analysis",
+__all__ = ["System", "VerletList", "FixedPairList", "FixedTripleList", "Real3D", "Int3D",
+           "Tensor", "analysis",
            "bc", "esutil", "integrator", "interaction", "storage", "tools", "standard_system",
            "set_default_precision", "load_library", "infinity", "ParallelTempering"]

@@ -35,6 +35,9 @@ PROTOTYPES = {
     "espp_bonds_size": (c_int32, [_P, _I64]),
     "espp_fene_set": (c_int32, [_P, c_double, c_double, c_double, c_double, c_double]),
     "espp_bonds_max_sqr": (c_int32, [_P, _D]),
+    "espp_triples_add": (c_int32, [_P, c_int64, _I64]),
+    "espp_triples_size": (c_int32, [_P, _I64]),
+    "espp_cosine_set": (c_int32, [_P, c_double, c_double]),
     "espp_tab_read": (c_int32, [c_char_p, c_int64, _D, _D, _D, _I64]),
     "espp_tab_eval": (c_int32, [c_int32, c_int64, _D, _D, _D, c_int64, _D, _D, _D]),
     "espp_tab_pair_set": (c_int32, [_P, c_int32, c_int32, c_int32, c_int64, _D, _D, _D,
@@ -87,6 +90,7 @@ IA_FENE = 1
 IA_TAB_PAIR = 2
 IA_TAB_BOND = 3
 IA_MLP = 4
+IA_COSINE = 5
 TAB_LINEAR, TAB_AKIMA, TAB_CUBIC = 1, 2, 3
 CAP_OFF, CAP_ABS, CAP_COMPONENT = 0, 1, 2
 

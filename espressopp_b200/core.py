@@ -493,3 +493,32 @@ class FixedPairList:
 
     def getLongtimeMaxBond(self):
         return math.sqrt(self.getLongtimeMaxBondSqr())
+
+
+class FixedTripleList:
+    """FixedTripleList(storage) (src/FixedTripleList.py:60-125): angle triples (pid1, pid2,
+    pid3) with pid2 the centre."""
+
+    def __init__(self, storage):
+        self.storage = storage
+        self._triples = []
+
+    def add(self, pid1, pid2, pid3):
+        self.addTriples([(pid1, pid2, pid3)])
+        return True
+
+    def addTriples(self, triplelist):
+        t = np.ascontiguousarray([(int(a), int(b), int(c)) for a, b, c in triplelist],
+                                 np.int64).reshape(-1)
+        if len(t) == 0:
+            return
+        call(self.storage._lib, "espp_triples_add", self.storage._h, len(t) // 3, i64ptr(t))
+        self._triples.extend((int(a), int(b), int(c)) for a, b, c in triplelist)
+
+    def getTriples(self):
+        return [list(self._triples)]
+
+    def size(self):
+        return len(self._triples)
+
+    totalSize = size

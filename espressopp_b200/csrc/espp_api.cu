@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
@@ -158,6 +159,13 @@ struct espp_system {
   bool lj_any = false;
   FENEParams fene{};
   std::vector<std::pair<int64_t, int64_t>> bonds;
+  // FixedTripleList + Cosine
+  std::vector<std::array<int64_t, 3>> triples;
+  CosineParams cosine{};
+  int64_t* d_triples = nullptr;
+  int32_t* tripStart = nullptr;
+  int32_t* tripEntry = nullptr;
+  double* tripF = nullptr;
   // interaction::Tabulated: specifications by slot (type pair key t1*kMaxTypes+t2 with
   // t1 <= t2, or kTabBondKey for the fixed pair list), built into one coefficient array
   struct TabSpec {
@@ -255,6 +263,12 @@ struct espp_system {
     d.mlp.D = mlpD;
     d.mlp.E = mlpE;
     d.mlp.on = (mlp && has_vl) ? 1 : 0;
+    d.triples = d_triples;
+    d.ntriples = (int)triples.size();
+    d.tripStart = tripStart;
+    d.tripEntry = tripEntry;
+    d.tripF = tripF;
+    d.cosine = cosine;
     d.err = err;
     d.ctr = ctr;
     return d;
@@ -459,6 +473,38 @@ void rebuild_id_tables(espp_system* s) {
         e.second - s->idMin < span)
       ex.push_back(e);
   if (!ex.empty()) csr(ex, s->exclStart, s->exclIds);
+  // triples: ids and, per particle, the triples it belongs to with its role
+  dfree(s->d_triples);
+  dfree(s->tripStart);
+  dfree(s->tripEntry);
+  dfree(s->tripF);
+  if (!s->triples.empty()) {
+    const size_t nt = s->triples.size();
+    std::vector<int64_t> ids(3 * nt);
+    std::vector<int32_t> start(span + 1, 0);
+    for (size_t t = 0; t < nt; ++t)
+      for (int q = 0; q < 3; ++q) {
+        const int64_t id = s->triples[t][q];
+        if (id < s->idMin || id - s->idMin >= span) raise(ESPP_EINVAL, "triple member does not exist");
+        ids[3 * t + q] = id;
+        start[id - s->idMin + 1]++;
+      }
+    for (int64_t k = 0; k < span; ++k) start[k + 1] += start[k];
+    std::vector<int32_t> entry(3 * nt);
+    std::vector<int32_t> fill(start.begin(), start.end() - 1);
+    for (size_t t = 0; t < nt; ++t)
+      for (int q = 0; q < 3; ++q) entry[fill[s->triples[t][q] - s->idMin]++] = (int32_t)(t * 4 + q);
+    s->d_triples = dalloc<int64_t>(ids.size());
+    s->tripStart = dalloc<int32_t>(span + 1);
+    s->tripEntry = dalloc<int32_t>(entry.size());
+    s->tripF = dalloc<double>(6 * nt);
+    cuda_check(cudaMemcpy(s->d_triples, ids.data(), sizeof(int64_t) * ids.size(),
+                          cudaMemcpyHostToDevice), "upload");
+    cuda_check(cudaMemcpy(s->tripStart, start.data(), sizeof(int32_t) * (span + 1),
+                          cudaMemcpyHostToDevice), "upload");
+    cuda_check(cudaMemcpy(s->tripEntry, entry.data(), sizeof(int32_t) * entry.size(),
+                          cudaMemcpyHostToDevice), "upload");
+  }
   std::vector<uint8_t> le(span, 0);
   for (int64_t id : s->langExclIds)
     if (id >= s->idMin && id - s->idMin < span) le[id - s->idMin] = 1;
@@ -665,6 +711,7 @@ void launch_all_forces(espp_system* s, cudaStream_t st) {
   if (!s->has_vl) d.tabNT = 0;
   launch_force_tab(d, mixed, st);
   if (d.mlp.on) launch_mlp_forces(d, mixed, nullptr, st);
+  launch_angle_forces(d, mixed, st);
 }
 
 void forces(espp_system* s) {
@@ -1213,6 +1260,9 @@ void observable(espp_system* s, int which, int energy, double out[7]) {
   } else if (which == ESPP_IA_TAB_BOND) {
     if (s->tabBond < 0) return;
     launch_tab_observables(d, 1, part, nb, s->obs, energy, s->st);
+  } else if (which == ESPP_IA_COSINE) {
+    if (s->triples.empty() || !s->cosine.on) return;
+    launch_angle_observables(d, part, nb, s->obs, energy, s->st);
   } else if (which == ESPP_IA_MLP) {
     if (!d.mlp.on) return;
     if (!energy) raise(ESPP_EINVAL, "the virial of the learned potential is not available");
@@ -1285,6 +1335,10 @@ void destroy(espp_system* s) {
   dfree(s->mlpPart);
   dfree(s->mlpFref);
   dfree(s->facc);
+  dfree(s->d_triples);
+  dfree(s->tripStart);
+  dfree(s->tripEntry);
+  dfree(s->tripF);
   dfree(s->stIds);
   dfree(s->stPos);
   dfree(s->stVel);
@@ -1734,6 +1788,37 @@ int espp_fene_set(espp_system* s, double K, double r0, double rmax, double rc, d
     s->fene.rmaxsq = rmax * rmax;
     s->fene.rcsq = rc * rc;
     s->fene.shift = shift;
+  });
+}
+
+int espp_triples_add(espp_system* s, int64_t n, const int64_t* triples) {
+  return guard([&] {
+    checked(s);
+    if (n > 0 && !triples) raise(ESPP_EINVAL, "null triple array");
+    std::unordered_map<int64_t, int> have;
+    for (int64_t id : s->allIds) have[id] = 1;
+    for (int64_t t = 0; t < n; ++t) {
+      std::array<int64_t, 3> tr = {triples[3 * t], triples[3 * t + 1], triples[3 * t + 2]};
+      for (int64_t id : tr)
+        if (!have.count(id)) raise(ESPP_EINVAL, "triple member does not exist");
+      s->triples.push_back(tr);
+    }
+    s->idDirty = true;
+  });
+}
+
+int espp_triples_size(espp_system* s, int64_t* n) {
+  return guard([&] { *n = (int64_t)checked(s)->triples.size(); });
+}
+
+int espp_cosine_set(espp_system* s, double K, double theta0) {
+  return guard([&] {
+    checked(s);
+    s->cosine.on = 1;
+    s->cosine.K = K;
+    s->cosine.theta0 = theta0;
+    s->cosine.Kcos_theta0 = K * std::cos(theta0);
+    s->cosine.Ksin_theta0 = K * std::sin(theta0);
   });
 }
 

@@ -59,6 +59,13 @@ struct FENEParams {
   double K, r0, rmax, rmaxsq, rcsq, shift;
 };
 
+// interaction::Cosine on a FixedTripleList (src/interaction/Cosine.hpp:38-125):
+// E = K (1 + cos(theta - theta0)).
+struct CosineParams {
+  int on;
+  double K, theta0, Kcos_theta0, Ksin_theta0;
+};
+
 // Per-particle arrays in cell-sorted order.  Two copies exist; the re-sort gathers
 // from one into the other and swaps.
 struct ParticleArrays {
@@ -153,6 +160,12 @@ struct DevView {
   int tabNT;              // 0: no tabulated pair interaction
   int tabBond;            // table of the fixed pair list, -1 none
   MlpDev mlp;             // learned CG pair potential on the Verlet list (mlp.on)
+  const int64_t* triples; // 3 * ntriples ids (p1, p2 centre, p3)
+  int ntriples;
+  const int32_t* tripStart; // idSpan + 1: CSR of the triples a particle belongs to, by id
+  const int32_t* tripEntry; // triple index * 4 + role (0 p1, 1 centre, 2 p3)
+  double* tripF;          // 6 * ntriples: force12, force32 of each triple
+  CosineParams cosine;
   unsigned* err;          // device error word
   DevCounters* ctr;       // step-loop state
 };
@@ -197,6 +210,10 @@ void launch_fene_observables(const DevView& d, const FENEParams& fene, double* p
 // pair-distance histogram (integer counts, accumulated into hist) for RadialDistrF
 void launch_rdf(const DevView& d, int rdfN, double dr, unsigned long long* hist,
                 cudaStream_t st);
+// angular forces (per triple, then gathered per particle) added to the force output
+void launch_angle_forces(const DevView& d, bool mixed, cudaStream_t st);
+void launch_angle_observables(const DevView& d, double* partials, int nblocks, double* out,
+                              int energy, cudaStream_t st);
 // tabulated pair and bond forces, added to the main kernel's output
 void launch_force_tab(const DevView& d, bool mixed, cudaStream_t st);
 void launch_tab_observables(const DevView& d, int bond, double* partials, int nblocks,

@@ -667,20 +667,29 @@ __global__ void __launch_bounds__(256) k_force_mixed(DevView d, FENEParams fp) {
       for (int u = 0; u < 8; ++u) pair(pj[u]);
     }
   } else {
-    // thread sub of particle i takes entries sub, sub + TPP, ...
-    constexpr int U = 4;
-    int k = sub;
-    for (; k + (U - 1) * TPP < cnt; k += U * TPP) {
-      int j[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) j[u] = __ldcs(d.nl + nl_index(k + u * TPP, i, cap));
-      int4 pj[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) pj[u] = __ldg(&d.posq[j[u]]);
-#pragma unroll
-      for (int u = 0; u < U; ++u) pair(pj[u]);
+    // thread sub of particle i takes the blocks sub, sub + TPP, ... (8 entries each, two
+    // 16-byte loads); TPP threads per particle keep TPP list blocks in flight per particle
+    const int nblk = (cnt + 7) >> 3;
+    const int4* blk = reinterpret_cast<const int4*>(d.nl) + ((size_t)sub * cap + i) * 2;
+    const size_t bstride = cap * 2 * TPP;
+    int4 ja = make_int4(i, i, i, i), jb = ja;
+    if (sub < nblk) {
+      ja = __ldcs(blk);
+      jb = __ldcs(blk + 1);
     }
-    for (; k < cnt; k += TPP) pair(__ldg(&d.posq[__ldcs(d.nl + nl_index(k, i, cap))]));
+    for (int b = sub; b < nblk; b += TPP) {
+      const int j[8] = {ja.x, ja.y, ja.z, ja.w, jb.x, jb.y, jb.z, jb.w};
+      int4 pj[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) pj[u] = __ldg(&d.posq[j[u]]);
+      blk += bstride;
+      if (b + TPP < nblk) {
+        ja = __ldcs(blk);
+        jb = __ldcs(blk + 1);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) pair(pj[u]);
+    }
   }
   long long Fx = to_fix(fx, d.err), Fy = to_fix(fy, d.err), Fz = to_fix(fz, d.err);
   if (FENE && sub == 0 && act) {
@@ -778,11 +787,13 @@ __global__ void __launch_bounds__(256) k_force_fp64(DevView d, FENEParams fp) {
     fy += dy * ff;
     fz += dz * ff;
   };
-  if (TPP == 1) {
+  {
+    // thread sub of particle i takes the blocks sub, sub + TPP, ... (8 entries each, read
+    // as two 16-byte loads)
     const int nblk = (cnt + 7) >> 3;
-    const int4* blk = reinterpret_cast<const int4*>(d.nl) + (size_t)i * 2;
-    const size_t bstride = cap * 2;
-    for (int b = 0; b < nblk; ++b, blk += bstride) {
+    const int4* blk = reinterpret_cast<const int4*>(d.nl) + ((size_t)sub * cap + i) * 2;
+    const size_t bstride = cap * 2 * TPP;
+    for (int b = sub; b < nblk; b += TPP, blk += bstride) {
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int4 jj = __ldcs(blk + h);
@@ -797,11 +808,6 @@ __global__ void __launch_bounds__(256) k_force_fp64(DevView d, FENEParams fp) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) pair(j[u], xj[u], yj[u], zj[u]);
       }
-    }
-  } else {
-    for (int k = sub; k < cnt; k += TPP) {
-      const int j = __ldcs(d.nl + nl_index(k, i, cap));
-      pair(j, __ldg(&X[j]), __ldg(&Y[j]), __ldg(&Z[j]));
     }
   }
   if (FENE && sub == 0 && act) {
@@ -1245,12 +1251,150 @@ __global__ void __launch_bounds__(kRdfTile) k_rdf(DevView d, int rdfN, int ntile
   }
 }
 
-// ---- interaction::Tabulated ---------------------------------------------------------
-
 __device__ __forceinline__ long long to_fix_d(double f, unsigned* err) {
   if (!(fabs(f) < 1.0e9)) atomicOr(err, kErrFixOverflow);
   return __double2ll_rn(f * 4294967296.0);
 }
+
+// ---- interaction::Cosine on a FixedTripleList ---------------------------------------
+
+__device__ __forceinline__ double mimg_box(double d, double L, double hL) {
+  // OrthorhombicBC::getMinimumImageVectorBox (src/bc/OrthorhombicBC.cpp:86-105)
+  if (d < -hL)
+    d += L;
+  else if (d > hL)
+    d -= L;
+  return d;
+}
+
+__device__ __forceinline__ bool triple_dists(const DevView& d, int t, double* d12, double* d32) {
+  const ParticleArrays a = d.pa[0];
+  int k[3];
+  for (int q = 0; q < 3; ++q) {
+    const int64_t o = d.triples[3 * (size_t)t + q] - d.idMin;
+    k[q] = (o >= 0 && o < d.idSpan) ? d.id2idx[o] : -1;
+    if (k[q] < 0) return false;
+  }
+  const size_t c = d.cap;
+  for (int q = 0; q < 3; ++q) {
+    const double p2 = a.x[q * c + k[1]];
+    d12[q] = mimg_box(a.x[q * c + k[0]] - p2, d.L[q], d.halfL[q]);
+    d32[q] = mimg_box(a.x[q * c + k[2]] - p2, d.L[q], d.halfL[q]);
+  }
+  return true;
+}
+
+// Cosine::_computeForceRaw (Cosine.hpp:79-119) in the reference's operation order.
+__device__ __forceinline__ void cosine_force(const CosineParams& P, const double* d12,
+                                             const double* d32, double* f12, double* f32) {
+  const double SMALL_EPSILON = 1.0E-9;
+  const double d12sq = __dadd_rn(__dadd_rn(__dmul_rn(d12[0], d12[0]), __dmul_rn(d12[1], d12[1])),
+                                 __dmul_rn(d12[2], d12[2]));
+  const double d32sq = __dadd_rn(__dadd_rn(__dmul_rn(d32[0], d32[0]), __dmul_rn(d32[1], d32[1])),
+                                 __dmul_rn(d32[2], d32[2]));
+  const double m12 = sqrt(d12sq), m32 = sqrt(d32sq);
+  const double dot = __dadd_rn(__dadd_rn(__dmul_rn(d12[0], d32[0]), __dmul_rn(d12[1], d32[1])),
+                               __dmul_rn(d12[2], d32[2]));
+  double c = dot / __dmul_rn(m12, m32);
+  if (c < -1.0) c = -1.0;
+  if (c > 1.0) c = 1.0;
+  const double sn = sqrt(__dsub_rn(1.0, __dmul_rn(c, c)));
+  const double a11 = c / d12sq, a12 = -1.0 / __dmul_rn(m12, m32), a22 = c / d32sq;
+  if (sn > SMALL_EPSILON) {
+    const double pre = __dsub_rn(P.Kcos_theta0, __dmul_rn(P.Ksin_theta0, c) / sn);
+    for (int q = 0; q < 3; ++q) {
+      f12[q] = __dmul_rn(pre, __dadd_rn(__dmul_rn(a11, d12[q]), __dmul_rn(a12, d32[q])));
+      f32[q] = __dmul_rn(pre, __dadd_rn(__dmul_rn(a22, d32[q]), __dmul_rn(a12, d12[q])));
+    }
+  } else {
+    for (int q = 0; q < 3; ++q) f12[q] = f32[q] = 0.0;
+  }
+}
+
+// per triple: force12 and force32 into tripF
+__global__ void k_angle_forces(DevView d) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.ntriples) return;
+  double d12[3], d32[3], f12[3] = {0, 0, 0}, f32[3] = {0, 0, 0};
+  if (triple_dists(d, t, d12, d32))
+    cosine_force(d.cosine, d12, d32, f12, f32);
+  else
+    atomicOr(d.err, kErrBondMissing);
+  for (int q = 0; q < 3; ++q) {
+    d.tripF[6 * (size_t)t + q] = f12[q];
+    d.tripF[6 * (size_t)t + 3 + q] = f32[q];
+  }
+}
+
+// per particle: p1 += force12, centre -= force12 + force32, p3 += force32
+// (FixedTripleListInteractionTemplate::addForces, :183-201), in the order of the
+// particle's triple list
+template <bool MIXED>
+__global__ void k_angle_gather(DevView d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n) return;
+  const int64_t off = d.pa[0].id[i] - d.idMin;
+  double f[3] = {0, 0, 0};
+  for (int e = d.tripStart[off]; e < d.tripStart[off + 1]; ++e) {
+    const int t = d.tripEntry[e] >> 2, role = d.tripEntry[e] & 3;
+    const double* F = d.tripF + 6 * (size_t)t;
+    for (int q = 0; q < 3; ++q)
+      f[q] += role == 0 ? F[q] : (role == 2 ? F[3 + q] : -(F[q] + F[3 + q]));
+  }
+  const size_t c = d.cap;
+  for (int q = 0; q < 3; ++q) {
+    if (MIXED)
+      d.ffix[q * c + i] += to_fix_d(f[q], d.err);
+    else
+      d.f64[q * c + i] += f[q];
+  }
+}
+
+// Energy (FixedTripleListInteractionTemplate::computeEnergy :205-275: minimum image by
+// rounding, theta = acos(cos), Cosine::_computeEnergyRaw) or virial d12.f12 + d32.f32.
+__global__ void k_angle_obs(DevView d, int energy, double* partials) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (t < d.ntriples) {
+    double d12[3], d32[3];
+    if (triple_dists(d, t, d12, d32)) {
+      if (energy) {
+        // getMinimumImageVector: subtract round(d / L) L
+        const ParticleArrays a = d.pa[0];
+        for (int q = 0; q < 3; ++q) {
+          const int k0 = d.id2idx[d.triples[3 * (size_t)t] - d.idMin];
+          const int k1 = d.id2idx[d.triples[3 * (size_t)t + 1] - d.idMin];
+          const int k2 = d.id2idx[d.triples[3 * (size_t)t + 2] - d.idMin];
+          const size_t c = d.cap;
+          const double e12 = a.x[q * c + k0] - a.x[q * c + k1];
+          const double e32 = a.x[q * c + k2] - a.x[q * c + k1];
+          d12[q] = e12 - round(e12 * d.invL[q]) * d.L[q];
+          d32[q] = e32 - round(e32 * d.invL[q]) * d.L[q];
+        }
+        const double s12 = d12[0] * d12[0] + d12[1] * d12[1] + d12[2] * d12[2];
+        const double s32 = d32[0] * d32[0] + d32[1] * d32[1] + d32[2] * d32[2];
+        const double cth = (d12[0] * d32[0] + d12[1] * d32[1] + d12[2] * d32[2]) /
+                           (sqrt(s12) * sqrt(s32));
+        acc[0] = d.cosine.K * (1.0 + cos(acos(cth) - d.cosine.theta0));
+      } else {
+        double f12[3], f32[3];
+        cosine_force(d.cosine, d12, d32, f12, f32);
+        acc[0] = d12[0] * f12[0] + d12[1] * f12[1] + d12[2] * f12[2] + d32[0] * f32[0] +
+                 d32[1] * f32[1] + d32[2] * f32[2];
+        acc[1] = d12[0] * f12[0] + d32[0] * f32[0];
+        acc[2] = d12[1] * f12[1] + d32[1] * f32[1];
+        acc[3] = d12[2] * f12[2] + d32[2] * f32[2];
+        acc[4] = d12[0] * f12[1] + d32[0] * f32[1];
+        acc[5] = d12[0] * f12[2] + d32[0] * f32[2];
+        acc[6] = d12[1] * f12[2] + d32[1] * f32[2];
+      }
+    }
+  }
+  block_sum_store<7>(acc, partials);
+}
+
+// ---- interaction::Tabulated ---------------------------------------------------------
+
 
 // Distance vector i - j under the minimum image, and its square in the reference's
 // order ((dx dx + dy dy) + dz dz).
@@ -1585,6 +1729,21 @@ void launch_rdf(const DevView& d, int rdfN, double dr, unsigned long long* hist,
         d, rdfN, (int)ntiles, dr, hist);
   else
     k_rdf<false><<<(unsigned)nblocks, kRdfTile, 0, st>>>(d, rdfN, (int)ntiles, dr, hist);
+}
+
+void launch_angle_forces(const DevView& d, bool mixed, cudaStream_t st) {
+  if (d.n == 0 || d.ntriples == 0 || !d.cosine.on) return;
+  k_angle_forces<<<blocks_for(d.ntriples), kBlock, 0, st>>>(d);
+  if (mixed)
+    k_angle_gather<true><<<blocks_for(d.n), kBlock, 0, st>>>(d);
+  else
+    k_angle_gather<false><<<blocks_for(d.n), kBlock, 0, st>>>(d);
+}
+
+void launch_angle_observables(const DevView& d, double* partials, int nblocks, double* out,
+                              int energy, cudaStream_t st) {
+  k_angle_obs<<<nblocks, kBlock, 0, st>>>(d, energy, partials);
+  k_sum_partials<7><<<1, 256, 0, st>>>(partials, nblocks, out);
 }
 
 void launch_force_tab(const DevView& d, bool mixed, cudaStream_t st) {

@@ -422,3 +422,54 @@ class FixedPairListTabulated(Interaction):
             return
         p = self._pot
         call(st._lib, "espp_tab_bond_set", st._h, *p._table(), p.cutoff, p.shift)
+
+
+class Cosine:
+    """interaction.Cosine(K=1.0, theta0=0.0) (Cosine.py:59-64, Cosine.hpp:38-125):
+    E(theta) = K (1 + cos(theta - theta0))."""
+
+    def __init__(self, K=1.0, theta0=0.0):
+        self.K = float(K)
+        self.theta0 = float(theta0)
+
+    def computeEnergy(self, theta):
+        return self.K * (1.0 + math.cos(float(theta) - self.theta0))
+
+    def computeForce(self, theta):
+        # AngularPotential computeForce(theta) of Cosine returns K (Cosine.hpp:121)
+        return self.K
+
+
+class FixedTripleListCosine(Interaction):
+    """interaction.FixedTripleListCosine(system, ftl, potential) (Cosine.py:66-95,
+    FixedTripleListInteractionTemplate.hpp:46-333)."""
+
+    kind = _abi.IA_COSINE
+
+    def __init__(self, system, ftl, potential=None):
+        Interaction.__init__(self)
+        self._ftl = ftl
+        self._pot = potential
+        self._pending_system = system
+
+    def setPotential(self, potential):
+        self._pot = potential
+        if self._system is not None:
+            self._push()
+
+    def getPotential(self):
+        return self._pot
+
+    def getFixedTripleList(self):
+        return self._ftl
+
+    def getMaxCutoff(self):
+        return 0.0
+
+    def bondType(self):
+        return 3  # Angular
+
+    def _push(self):
+        st = self._handle()
+        if self._pot is not None:
+            call(st._lib, "espp_cosine_set", st._h, self._pot.K, self._pot.theta0)

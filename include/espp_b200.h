@@ -54,6 +54,7 @@ typedef struct espp_system espp_system;
 #define ESPP_IA_TAB_PAIR 2 /* VerletListTabulated */
 #define ESPP_IA_TAB_BOND 3 /* FixedPairListTabulated */
 #define ESPP_IA_MLP 4      /* learned coarse-grained pair potential (espp_mlp_*) */
+#define ESPP_IA_COSINE 5   /* FixedTripleListCosine */
 
 /* interpolation types of interaction::Tabulated (src/interaction/Tabulated.cpp:49-67) */
 #define ESPP_TAB_LINEAR 1
@@ -128,6 +129,15 @@ ESPP_API int espp_fene_set(espp_system* s, double K, double r0, double rmax, dou
                   double shift);
 /* FixedPairList::getLongtimeMaxBondSqr. */
 ESPP_API int espp_bonds_max_sqr(espp_system* s, double* maxsq);
+
+/* ---- FixedTripleList + interaction::Cosine ---------------------------------------------
+ * FixedTripleList::add (src/FixedTripleList.cpp): triples of ids (p1, p2, p3), p2 the
+ * centre.  FixedTripleListCosine(system, ftl, Cosine(K, theta0))
+ * (src/interaction/Cosine.hpp:38-125, FixedTripleListInteractionTemplate.hpp:121-333):
+ * E = K (1 + cos(theta - theta0)). */
+ESPP_API int espp_triples_add(espp_system* s, int64_t n, const int64_t* triples);
+ESPP_API int espp_triples_size(espp_system* s, int64_t* n);
+ESPP_API int espp_cosine_set(espp_system* s, double K, double theta0);
 
 /* ---- interaction::Tabulated -----------------------------------------------------------
  * Table files as InterpolationLinear/Akima/Cubic::readFile read them

@@ -374,6 +374,9 @@ struct espp_system {
   std::vector<std::pair<int64_t, int64_t>> bondsGlobal;
   std::vector<std::pair<Particle*, Particle*>> bondPtrs;
   double ltMaxBondSqr = 0;
+  std::vector<std::array<int64_t, 3>> triplesGlobal;
+  bool cos_on = false;
+  double cK = 0, cTheta0 = 0, cKcos = 0, cKsin = 0;
   std::map<std::pair<int, int>, TabPot> tabPair;
   bool tabBondOn = false;
   TabPot tabBond;
@@ -707,6 +710,41 @@ void minImageBox(const espp_system* s, const double* a, const double* b, double 
   }
 }
 
+// OrthorhombicBC::getMinimumImageVector (src/bc/OrthorhombicBC.cpp:73-83).
+void minImageRound(const espp_system* s, const double* a, const double* b, double d[3]) {
+  for (int k = 0; k < 3; ++k) {
+    d[k] = a[k] - b[k];
+    d[k] -= std::round(d[k] * s->invL[k]) * s->L[k];
+  }
+}
+
+// Cosine::_computeForceRaw (src/interaction/Cosine.hpp:79-119).
+void cosineForce(const espp_system* s, const double d12[3], const double d32[3], double f12[3],
+                 double f32[3]) {
+  const double SMALL_EPSILON = 1.0E-9;
+  double dist12_sqr = d12[0] * d12[0] + d12[1] * d12[1] + d12[2] * d12[2];
+  double dist32_sqr = d32[0] * d32[0] + d32[1] * d32[1] + d32[2] * d32[2];
+  double dist12_magn = std::sqrt(dist12_sqr);
+  double dist32_magn = std::sqrt(dist32_sqr);
+  double cos_theta = (d12[0] * d32[0] + d12[1] * d32[1] + d12[2] * d32[2]) /
+                     (dist12_magn * dist32_magn);
+  if (cos_theta < -1.0) cos_theta = -1.0;
+  if (cos_theta > 1.0) cos_theta = 1.0;
+  double sin_theta = std::sqrt(1.0 - cos_theta * cos_theta);
+  double a11 = cos_theta / dist12_sqr;
+  double a12 = -1.0 / (dist12_magn * dist32_magn);
+  double a22 = cos_theta / dist32_sqr;
+  if (sin_theta > SMALL_EPSILON) {
+    double pre = s->cKcos - s->cKsin * cos_theta / sin_theta;
+    for (int k = 0; k < 3; ++k) {
+      f12[k] = pre * (a11 * d12[k] + a12 * d32[k]);
+      f32[k] = pre * (a22 * d32[k] + a12 * d12[k]);
+    }
+  } else {
+    for (int k = 0; k < 3; ++k) f12[k] = f32[k] = 0.0;
+  }
+}
+
 // FENE::_computeForceRaw / _computeEnergySqrRaw (src/interaction/FENE.hpp:91-112).
 bool feneForce(const espp_system* s, const double d[3], double f[3]) {
   double distSqr = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
@@ -980,6 +1018,24 @@ void updateForces(espp_system* s) {
           p1.f[k] += f[k];
           p2.f[k] -= f[k];
         }
+    }
+  }
+  // FixedTripleListCosine (FixedTripleListInteractionTemplate::addForces :183-201)
+  if (s->cos_on) {
+    for (auto& tr : s->triplesGlobal) {
+      Particle* p1 = lookup(s, tr[0]);
+      Particle* p2 = lookup(s, tr[1]);
+      Particle* p3 = lookup(s, tr[2]);
+      if (!p1 || !p2 || !p3) continue;
+      double d12[3], d32[3], f12[3], f32[3];
+      minImageBox(s, p1->r, p2->r, d12);
+      minImageBox(s, p3->r, p2->r, d32);
+      cosineForce(s, d12, d32, f12, f32);
+      for (int k = 0; k < 3; ++k) {
+        p1->f[k] += f12[k];
+        p2->f[k] -= f12[k] + f32[k];
+        p3->f[k] += f32[k];
+      }
     }
   }
   ghostComm(s, false, false);
@@ -1318,6 +1374,33 @@ int espp_bonds_max_sqr(espp_system* s, double* m) {
   return ESPP_OK;
 }
 
+int espp_triples_add(espp_system* s, int64_t n, const int64_t* triples) {
+  CHECK_S(s);
+  for (int64_t t = 0; t < n; ++t) {
+    std::array<int64_t, 3> tr = {triples[3 * t], triples[3 * t + 1], triples[3 * t + 2]};
+    for (int64_t id : tr)
+      if (!lookup(s, id)) return fail(ESPP_EINVAL, "triple member does not exist");
+    s->triplesGlobal.push_back(tr);
+  }
+  return ESPP_OK;
+}
+
+int espp_triples_size(espp_system* s, int64_t* n) {
+  CHECK_S(s);
+  *n = (int64_t)s->triplesGlobal.size();
+  return ESPP_OK;
+}
+
+int espp_cosine_set(espp_system* s, double K, double theta0) {
+  CHECK_S(s);
+  s->cos_on = true;
+  s->cK = K;
+  s->cTheta0 = theta0;
+  s->cKcos = K * std::cos(theta0);
+  s->cKsin = K * std::sin(theta0);
+  return ESPP_OK;
+}
+
 // InterpolationLinear.cpp readFile: fgets + sscanf("%lg %lg %lg")
 int espp_tab_read(const char* path, int64_t cap, double* r, double* energy, double* force,
                   int64_t* n) {
@@ -1598,6 +1681,22 @@ int espp_energy(espp_system* s, int32_t which, double* e) {
         minImageBox(s, pr.first->r, pr.second->r, d);
         es += s->tabBond.energy(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
       }
+  } else if (which == ESPP_IA_COSINE) {
+    if (s->cos_on)
+      for (auto& tr : s->triplesGlobal) {
+        Particle* p1 = lookup(s, tr[0]);
+        Particle* p2 = lookup(s, tr[1]);
+        Particle* p3 = lookup(s, tr[2]);
+        if (!p1 || !p2 || !p3) continue;
+        double d12[3], d32[3];
+        minImageRound(s, p1->r, p2->r, d12);
+        minImageRound(s, p3->r, p2->r, d32);
+        double s12 = d12[0] * d12[0] + d12[1] * d12[1] + d12[2] * d12[2];
+        double s32 = d32[0] * d32[0] + d32[1] * d32[1] + d32[2] * d32[2];
+        double c = (d12[0] * d32[0] + d12[1] * d32[1] + d12[2] * d32[2]) /
+                   (std::sqrt(s12) * std::sqrt(s32));
+        es += s->cK * (1.0 + std::cos(std::acos(c) - s->cTheta0));
+      }
   } else if (which == ESPP_IA_MLP) {
     if (s->mlp && s->has_vl) {
       ghostComm(s, true, false);
@@ -1640,6 +1739,20 @@ static int virialImpl(espp_system* s, int32_t which, double* wsc, double w6[6]) 
         minImageBox(s, pr.first->r, pr.second->r, d);
         double f[3];
         if (feneForce(s, d, f)) acc(d, f);
+      }
+  } else if (which == ESPP_IA_COSINE) {
+    if (s->cos_on)
+      for (auto& tr : s->triplesGlobal) {
+        Particle* p1 = lookup(s, tr[0]);
+        Particle* p2 = lookup(s, tr[1]);
+        Particle* p3 = lookup(s, tr[2]);
+        if (!p1 || !p2 || !p3) continue;
+        double d12[3], d32[3], f12[3], f32[3];
+        minImageBox(s, p1->r, p2->r, d12);
+        minImageBox(s, p3->r, p2->r, d32);
+        cosineForce(s, d12, d32, f12, f32);
+        acc(d12, f12);
+        acc(d32, f32);
       }
   } else if (which == ESPP_IA_TAB_PAIR) {
     if (s->has_vl)

@@ -94,6 +94,13 @@ class Sim:
     def fene(self, K=30.0, r0=0.0, rmax=1.5, rc=math.inf, shift=0.0):
         call(self.lib, "espp_fene_set", self.h, K, r0, rmax, rc, shift)
 
+    def triples(self, trip):
+        t = np.ascontiguousarray(trip, np.int64).reshape(-1)
+        call(self.lib, "espp_triples_add", self.h, len(t) // 3, i64ptr(t))
+
+    def cosine(self, K=1.5, theta0=3.1415926):
+        call(self.lib, "espp_cosine_set", self.h, K, theta0)
+
     def integrator(self, dt):
         call(self.lib, "espp_integrator_set", self.h, float(dt))
 
@@ -179,12 +186,14 @@ def load_lj2048():
     return z["pid"], z["pos"], z["vel"], z["box"]
 
 
-def load_polymer40k():
+def load_polymer40k(angles=False):
     import json
     z = np.load(os.path.join(GOLDEN, "polymer_melt_40k.npz"))
     pos = z["pos_milli"].astype(np.float64) / 1000.0
     with open(os.path.join(GOLDEN, "polymer_melt_40k.json")) as f:
         gold = json.load(f)
+    if angles:
+        return pos, z["bonds"].astype(np.int64), z["box"], gold, z["angles"].astype(np.int64)
     return pos, z["bonds"].astype(np.int64), z["box"], gold
 
 

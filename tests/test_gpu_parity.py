@@ -352,3 +352,38 @@ def test_rdf_matches_oracle_bitwise(rdfN):
     r = (np.arange(rdfN) + 0.5) * dr
     one_pair = 1.0 / (2 * np.pi * dr * len(pid) ** 2 / np.prod(box) * (r * r + dr * dr / 12))
     assert np.sum(np.abs(ho - hg) / one_pair) <= 4.0
+
+
+@pytest.mark.parametrize("prec", [_abi.PREC_FP64, _abi.PREC_MIXED])
+def test_polymer_melt_with_angles_matches_oracle(prec):
+    """FixedTripleListCosine with LJ and FENE on the 40 000-bead melt: the result.dat
+    eangle at step 0, forces against the oracle, and a short Langevin run."""
+    pos, bonds, box, gold, angles = load_polymer40k(angles=True)
+    ids = np.arange(1, len(pos) + 1)
+    sims = []
+    for lib, p in ((oracle_lib(), _abi.PREC_FP64), (cuda_lib(), prec)):
+        s = Sim(lib, box, 0.3, cell_grid(box, 1.12, 0.3), precision=p, seed=3)
+        s.add(ids, pos)
+        s.decompose()
+        s.vl(1.42)
+        s.lj(0, 0, 1.0, 1.0, 1.12, 0.0)
+        s.bonds(bonds)
+        s.fene(30.0, 0.0, 1.5)
+        s.triples(angles)
+        s.cosine(1.5, 3.1415926)
+        sims.append(s)
+    o, g = sims
+    # result.dat prints sum K (1 - cos(theta - theta0)) = 2 K N - sum K (1 + cos(...))
+    assert round(2 * 1.5 * len(angles) - g.energy(_abi.IA_COSINE), 3) == gold["eangle"]
+    assert abs(g.energy(_abi.IA_COSINE) - o.energy(_abi.IA_COSINE)) < 1e-9 * gold["eangle"]
+    for s in sims:
+        s.integrator(0.002)
+        s.run(0)
+    tol = 1e-12 if prec == _abi.PREC_FP64 else 1e-5
+    assert _rel_rms(g.particles(ids)[2], o.particles(ids)[2]) < tol
+    for s in sims:
+        s.langevin(1.0, 1.0)
+        s.run(20)
+    ref = o.particles(ids)
+    got = g.particles(ids)
+    assert np.max(np.abs(got[0] - ref[0])) < (1e-9 if prec == _abi.PREC_FP64 else 1e-4)

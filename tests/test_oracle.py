@@ -220,3 +220,22 @@ def test_rdf_of_lj_fluid_is_normalised():
     assert np.all(g[r < 0.8] == 0.0)
     assert 1.0 < r[np.argmax(g)] < 1.25 and g.max() > 2.0
     assert abs(np.mean(g[(r > 4.5) & (r < 6.5)]) - 1.0) < 0.05
+
+
+def test_polymer_melt_step0_angle_energy_matches_result_dat():
+    """testsuite/tabulated/result.dat step 0: eangle 32301.755 of FixedTripleListCosine
+    (Cosine K=1.5, theta0=3.1415926) on the 40 000 angles of polymer_melt.start.
+    The printed value is sum K (1 - cos(theta - theta0)) (to the printed digits:
+    32301.7548), the form of an earlier Cosine; the current source has K (1 + cos(theta -
+    theta0)) (src/interaction/Cosine.hpp:74), which the oracle follows.  The two sum to
+    2 K per angle, so the oracle's energy pins the same angles: 2 K N - E = 32301.755."""
+    pos, bonds, box, gold, angles = load_polymer40k(angles=True)
+    s = Sim(oracle_lib(), box, 0.3, cell_grid(box, 1.12, 0.3))
+    s.add(np.arange(1, len(pos) + 1), pos)
+    s.decompose()
+    s.triples(angles)
+    s.cosine(1.5, 3.1415926)
+    e = s.energy(_abi.IA_COSINE)
+    assert round(2 * 1.5 * len(angles) - e, 3) == gold["eangle"]
+    # the angular virial vanishes: d12.F12 + d32.F32 = 0 for any angular force
+    assert abs(s.virial(_abi.IA_COSINE)) < 1e-6
