@@ -2,18 +2,25 @@
 //
 //  re-binning     k_fold_bin -> k_scan_cells -> k_scatter -> k_sort_in_cell -> k_gather
 //                 (storage::DomainDecomposition::decomposeRealParticles, one node)
-//  Verlet list    k_build_nl: exact FP64 pair test in the reference's ghost-shift
-//                 arithmetic, full per-particle list (VerletList::_rebuildUsingBuffers)
+//  Verlet list    k_build_nl_lane (k_build_nl_tc: tcgen05 distance prefilter, opt-in):
+//                 FP32 test with the reference's FP64 ghost-shift arithmetic near the
+//                 cutoff, full per-particle list (VerletList::_rebuildUsingBuffers)
 //  forces         k_force_mixed (FP32 on box-wrapped int32 coordinates, int64 2^-32
 //                 fixed-point output) / k_force_fp64 (plain FP64); LJ + FENE fused
 //  integrator     k_integrate: aftCalcF (Langevin, CapForce) + integrate2 of step n +
 //                 integrate1 of step n+1 in one pass over the particle arrays
 //  observables    FP64 energy / virial / kinetic with fixed-order block reductions
 #include <math.h>
+#include <stddef.h>
 #include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <cuda_fp16.h>
 
 #include "espp_internal.h"
 #include "espp_tab.h"
+#include "espp_tc.h"
 
 namespace espp {
 
@@ -324,9 +331,9 @@ __device__ __forceinline__ bool is_excluded(const DevView& d, int64_t a, int64_t
 
 // The reference's FP64 inclusion test for one candidate pair (rarely reached: only
 // candidates whose FP32 distance lies within the 2e-5 band around the cutoff).
-__device__ __noinline__ bool exact_pair_test(const double* __restrict__ x, size_t cap, int i,
-                                             int j, bool fwd, double sx, double sy, double sz,
-                                             double cutsq) {
+__device__ __forceinline__ bool exact_pair_test_inl(const double* __restrict__ x, size_t cap,
+                                                   int i, int j, bool fwd, double sx, double sy,
+                                                   double sz, double cutsq) {
   const double xi = x[i], yi = x[cap + i], zi = x[2 * cap + i];
   const double xj = x[j], yj = x[cap + j], zj = x[2 * cap + j];
   double ex, ey, ez;
@@ -341,6 +348,11 @@ __device__ __noinline__ bool exact_pair_test(const double* __restrict__ x, size_
   }
   const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
   return !(d2 > cutsq);
+}
+__device__ __noinline__ bool exact_pair_test(const double* __restrict__ x, size_t cap, int i,
+                                             int j, bool fwd, double sx, double sy, double sz,
+                                             double cutsq) {
+  return exact_pair_test_inl(x, cap, i, j, fwd, sx, sy, sz, cutsq);
 }
 
 // Packed FP32 pairs (sm_100 f32x2 arithmetic): two particles' coordinates in one 64-bit
@@ -365,92 +377,91 @@ __device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsig
   return r;
 }
 
-// Squared FP32 distances of two group particles (packed xi, yi, zi) to one candidate
-// (packed twice in cx, cy, cz), packed the same way.  The fast test and the borderline
-// pass both call this, so a candidate is classified the same way by both.
-__device__ __forceinline__ unsigned long long pair_r2(const float2* __restrict__ sp,
-                                                      unsigned long long cx,
-                                                      unsigned long long cy,
-                                                      unsigned long long cz) {
-  const float2 px = sp[0], py = sp[1], pz = sp[2];
-  const unsigned long long dx = f2_sub(f2_pack(px.x, px.y), cx);
-  const unsigned long long dy = f2_sub(f2_pack(py.x, py.y), cy);
-  const unsigned long long dz = f2_sub(f2_pack(pz.x, pz.y), cz);
-  return f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
-}
 __device__ __forceinline__ float f2_lo(unsigned long long v) { return __uint_as_float((unsigned)v); }
 __device__ __forceinline__ float f2_hi(unsigned long long v) {
   return __uint_as_float((unsigned)(v >> 32));
 }
 
-// Appends candidate j (held by this lane) to the list of the particle whose first block
-// starts at nl_i when `in` is set: the lanes of one ballot write consecutive slots in
-// lane order.
-__device__ __forceinline__ void nl_append(int* __restrict__ nl_i, unsigned cap8, int K, int cnt,
-                                          unsigned mask, bool in, int j) {
-  const int k = cnt + __popc(mask & ((1u << (threadIdx.x & 31)) - 1u));
-  if (in && k < K) nl_i[(size_t)(unsigned)(k >> 3) * cap8 + (unsigned)(k & 7)] = j;
-}
+// ---- Verlet build, particle-per-lane form ------------------------------------------
+// One warp per cell and group of up to 32 of its particles; lane l holds particle g + l.
+// The candidates of each stencil row (the row's three x-cells) are staged 32 at a time
+// ("chunk") in shared memory, shifted into the cell's frame, and every lane tests all
+// of them against its particle, two candidates per packed f32x2 operation.  A lane
+// appends its partners to its own staging row and writes every full block of 8 to the
+// list with two 16-byte stores, so the list is written in whole sectors.  Candidates
+// within the relative 2e-5 band around the cutoff are decided, after the chunk's other
+// partners, by the reference's FP64 arithmetic (exact_pair_test), as in the ballot
+// form above; the pair set is the reference's (VerletList.cpp:274-450) and each list
+// is in a fixed order.
+constexpr int kBuildWarps = 4;
+constexpr int kStageLd = 44;  // staging row: <= 7 carried + <= 32 appended; 11 x 16 B
 
-// The fast tests of one chunk against the group, four group members per step (two
-// packed pairs, independent chains).  SELF: the chunk may hold group members (centre
-// row), so the candidate equal to the tested particle is skipped.  Returns whether any
-// candidate came near the cutoff (a superset of the borderline band).
+struct BuildChunk {
+  float x[32], y[32], z[32];
+  int j[32];
+  int64_t id[32];
+};
+
+// Fast tests of one chunk (nv valid candidates) against the lane's particle.  Returns
+// whether any candidate came near the cutoff (a superset of the borderline band).
 template <bool SELF, bool EXCL>
-__device__ __forceinline__ bool chunk_fast(const DevView& d, const float2 (*sxp)[3],
-                                           const int64_t* sid, int ni, int* __restrict__ nlg,
-                                           unsigned cap8, int K, int j, int jl, int64_t idj,
-                                           unsigned long long cxx, unsigned long long cyy,
-                                           unsigned long long czz, float lo,
-                                           unsigned long long mid2, float hw, int (&cnt)[32]) {
+__device__ __forceinline__ bool chunk_scan(const DevView& d, const BuildChunk& c, int nv,
+                                           unsigned long long xi2, unsigned long long yi2,
+                                           unsigned long long zi2, int i, int64_t idi,
+                                           float lo, unsigned long long mid2, float hw,
+                                           int* __restrict__ srow, int& pend) {
   bool band = false;
 #pragma unroll
-  for (int p4 = 0; p4 < 8; ++p4) {
-    if (4 * p4 >= ni) break;
-    const unsigned long long r01 = pair_r2(sxp[2 * p4], cxx, cyy, czz);
-    const unsigned long long r23 = pair_r2(sxp[2 * p4 + 1], cxx, cyy, czz);
-    const unsigned long long t01 = f2_sub(r01, mid2), t23 = f2_sub(r23, mid2);
-    band |= (fabsf(f2_lo(t01)) <= hw) | (fabsf(f2_hi(t01)) <= hw) |
-            (fabsf(f2_lo(t23)) <= hw) | (fabsf(f2_hi(t23)) <= hw);
-    const float r2[4] = {f2_lo(r01), f2_hi(r01), f2_lo(r23), f2_hi(r23)};
-    bool in[4];
-    unsigned m[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      in[u] = r2[u] < lo && (!SELF || jl != 4 * p4 + u);
-      if (EXCL && in[u] && is_excluded(d, sid[4 * p4 + u], idj)) in[u] = false;
+  for (int m = 0; m < 32; m += 2) {
+    if (m >= nv) break;
+    const unsigned long long cx = *reinterpret_cast<const unsigned long long*>(&c.x[m]);
+    const unsigned long long cy = *reinterpret_cast<const unsigned long long*>(&c.y[m]);
+    const unsigned long long cz = *reinterpret_cast<const unsigned long long*>(&c.z[m]);
+    const int2 jj = *reinterpret_cast<const int2*>(&c.j[m]);
+    const unsigned long long dx = f2_sub(xi2, cx), dy = f2_sub(yi2, cy), dz = f2_sub(zi2, cz);
+    const unsigned long long r2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
+    const unsigned long long t = f2_sub(r2, mid2);
+    band |= (fabsf(f2_lo(t)) <= hw) | (fabsf(f2_hi(t)) <= hw);
+    bool ina = f2_lo(r2) < lo, inb = f2_hi(r2) < lo;
+    if (SELF) {
+      ina &= jj.x != i;
+      inb &= jj.y != i;
     }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) m[u] = __ballot_sync(0xffffffffu, in[u]);
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      nl_append(nlg + 8 * (4 * p4 + u), cap8, K, cnt[4 * p4 + u], m[u], in[u], j);
-      cnt[4 * p4 + u] += __popc(m[u]);
+    if (EXCL) {
+      if (ina && is_excluded(d, idi, c.id[m])) ina = false;
+      if (inb && is_excluded(d, idi, c.id[m + 1])) inb = false;
     }
+    if (ina) srow[pend++] = jj.x;
+    if (inb) srow[pend++] = jj.y;
   }
   return band;
 }
 
-// One warp per cell and group of up to 32 of its particles.  The lanes hold candidates:
-// for each of the 9 rows (oy, oz) of the reference's 27-cell stencil the particles of
-// the row's three x-cells are taken 32 at a time (a "chunk").  Every group particle is
-// tested against the chunk in FP32 on cell-relative coordinates, two group particles
-// per packed f32x2 operation; one ballot per (particle, chunk) gives the candidates
-// inside the cutoff, and those lanes write their index straight into the particle's
-// list at the slot the ballot's prefix count gives.  Candidates within a relative band
-// of 2e-5 around the cutoff are left out of that ballot; a chunk that has any is
-// revisited and those are decided by the reference's own FP64 arithmetic
-// (exact_pair_test) and appended after the chunk's other partners.
-// Each list is therefore the reference's pair set (VerletList.cpp:274-450) in a
-// deterministic order.  The group's list counts live in registers (warp-uniform),
-// unrolled over the 32 possible group members.
+// Writes the lane's full blocks of 8 to its list and keeps the remainder in front.
+__device__ __forceinline__ void stage_flush(int* __restrict__ srow, int& pend, int& blk,
+                                            int* __restrict__ nl, int i, size_t cap, int kb) {
+  const int nb = pend >> 3;
+  if (nb == 0) return;
+  for (int b = 0; b < nb; ++b, ++blk) {
+    const int4 v0 = *reinterpret_cast<const int4*>(&srow[8 * b]);
+    const int4 v1 = *reinterpret_cast<const int4*>(&srow[8 * b + 4]);
+    if (blk < kb) {
+      int4* dst = reinterpret_cast<int4*>(nl + nl_index(8 * blk, i, cap));
+      dst[0] = v0;
+      dst[1] = v1;
+    }
+  }
+  const int rem = pend & 7;
+  for (int k = 0; k < rem; ++k) srow[k] = srow[8 * nb + k];
+  pend = rem;
+}
+
 template <bool EXCL>
-__global__ void __launch_bounds__(128) k_build_nl(DevView d, double cutsq) {
+__global__ void __launch_bounds__(kBuildWarps * 32) k_build_nl_lane(DevView d, double cutsq) {
   const ParticleArrays a = d.pa[0];
-  __shared__ float2 s_xp[4][16][3];  // group particles (2p, 2p+1): x pair, y pair, z pair
-  __shared__ int64_t s_id[4][32];
-  __shared__ int s_cnt[4][32];
-  __shared__ int s_row[4][9][8];  // st0, ct0, st1, ct1, st2, ct2, first chunk, chunks
+  __shared__ __align__(16) int s_stage[kBuildWarps][32 * kStageLd];
+  __shared__ __align__(16) BuildChunk s_chunk[kBuildWarps];
+  __shared__ int s_row[kBuildWarps][9][6];  // st0, ct0, st1, ct1, st2, ct2
   const int wib = threadIdx.x >> 5;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -460,15 +471,15 @@ __global__ void __launch_bounds__(128) k_build_nl(DevView d, double cutsq) {
   const int s0 = d.cellStart[c], s1 = d.cellStart[c + 1];
   if (s0 == s1) return;
   const float lo = (float)(cutsq * (1.0 - 2e-5)), hi = (float)(cutsq * (1.0 + 2e-5));
-  // the fast path's trigger for the borderline pass: |r2 - mid| <= hw, 1.5 x wider than
-  // the band [lo, hi] so that rounding of r2 - mid cannot hide a borderline candidate
   const float mid = (float)cutsq, hw = (float)(cutsq * 3e-5);
   const unsigned long long mid2 = f2_pack(mid, mid);
   const float hx = (float)d.cellSize[0], hy = (float)d.cellSize[1], hz = (float)d.cellSize[2];
   const float4* __restrict__ xr = d.xrel;
   const int K = d.K;
-  const unsigned cap8 = (unsigned)d.cap << 3;
+  const size_t cap = d.cap;
   int* __restrict__ nl = d.nl;
+  BuildChunk& ch = s_chunk[wib];
+  int* __restrict__ srow = &s_stage[wib][lane * kStageLd];
   const int cxm = cx == 0 ? d.nc[0] - 1 : cx - 1;
   const int cxp = cx == d.nc[0] - 1 ? 0 : cx + 1;
   if (lane < 9) {
@@ -478,115 +489,395 @@ __global__ void __launch_bounds__(128) k_build_nl(DevView d, double cutsq) {
     ncz += ncz < 0 ? d.nc[2] : (ncz >= d.nc[2] ? -d.nc[2] : 0);
     const int rb = d.nc[0] * (ncy + d.nc[1] * ncz);
     const int st0 = d.cellStart[rb + cxm], st1 = d.cellStart[rb + cx], st2 = d.cellStart[rb + cxp];
-    const int ct0 = d.cellStart[rb + cxm + 1] - st0, ct1 = d.cellStart[rb + cx + 1] - st1;
-    const int ct2 = d.cellStart[rb + cxp + 1] - st2;
     s_row[wib][lane][0] = st0;
-    s_row[wib][lane][1] = ct0;
+    s_row[wib][lane][1] = d.cellStart[rb + cxm + 1] - st0;
     s_row[wib][lane][2] = st1;
-    s_row[wib][lane][3] = ct1;
+    s_row[wib][lane][3] = d.cellStart[rb + cx + 1] - st1;
     s_row[wib][lane][4] = st2;
-    s_row[wib][lane][5] = ct2;
-    s_row[wib][lane][7] = (ct0 + ct1 + ct2 + 31) >> 5;
+    s_row[wib][lane][5] = d.cellStart[rb + cxp + 1] - st2;
   }
-  __syncwarp();
-  int nchunks = 0;
-  if (lane == 0)
-    for (int r = 0; r < 9; ++r) {
-      s_row[wib][r][6] = nchunks;
-      nchunks += s_row[wib][r][7];
-    }
-  nchunks = __shfl_sync(0xffffffffu, nchunks, 0);
   __syncwarp();
   for (int g = s0; g < s1; g += 32) {
     const int ni = min(32, s1 - g);
-    {
-      const float4 r = lane < ni ? xr[g + lane] : make_float4(1e18f, 1e18f, 1e18f, 0.f);
-      float* sp = reinterpret_cast<float*>(&s_xp[wib][lane >> 1][0]) + (lane & 1);
-      sp[0] = r.x;
-      sp[2] = r.y;
-      sp[4] = r.z;
-      if (EXCL) s_id[wib][lane] = lane < ni ? a.id[g + lane] : -1;
-    }
-    __syncwarp();
-    int cnt[32];
-#pragma unroll
-    for (int m = 0; m < 32; ++m) cnt[m] = 0;
-    int rr = 0;
-    for (int q = 0; q < nchunks; ++q) {
-      while (q >= s_row[wib][rr][6] + s_row[wib][rr][7]) ++rr;
-      const int cb = (q - s_row[wib][rr][6]) << 5;
+    const bool own = lane < ni;
+    const int i = own ? g + lane : g;
+    // padding lanes sit at +1e18 and invalid candidates at -1e18: no pair among them
+    // comes near the cutoff, and no square overflows FP32
+    const float4 ri = own ? xr[i] : make_float4(1e18f, 1e18f, 1e18f, 0.f);
+    const unsigned long long xi2 = f2_pack(ri.x, ri.x), yi2 = f2_pack(ri.y, ri.y);
+    const unsigned long long zi2 = f2_pack(ri.z, ri.z);
+    const int64_t idi = (EXCL && own) ? a.id[i] : -3;
+    int pend = 0, blk = 0;
+    for (int rr = 0; rr < 9; ++rr) {
       const int oz = rr / 3 - 1, oy = rr % 3 - 1;
       const int st0 = s_row[wib][rr][0], ct0 = s_row[wib][rr][1];
       const int st1 = s_row[wib][rr][2], ct1 = s_row[wib][rr][3];
       const int st2 = s_row[wib][rr][4], ct2 = s_row[wib][rr][5];
-      const int t = cb + lane;
-      const bool validj = t < ct0 + ct1 + ct2;
-      const int seg = t < ct0 ? 0 : (t < ct0 + ct1 ? 1 : 2);
-      const int j = !validj ? -1 : (seg == 0 ? st0 + t : (seg == 1 ? st1 + t - ct0 : st2 + t - ct0 - ct1));
-      // invalid lanes sit at -1e18 and padding group members at +1e18: no pair among
-      // them comes near the cutoff, and no square overflows FP32
-      float4 rj = validj ? xr[j] : make_float4(-1e18f, -1e18f, -1e18f, 0.f);
-      rj.x += (seg - 1) * hx;
-      rj.y += oy * hy;
-      rj.z += oz * hz;
-      const unsigned long long cxx = f2_pack(rj.x, rj.x), cyy = f2_pack(rj.y, rj.y);
-      const unsigned long long czz = f2_pack(rj.z, rj.z);
-      const int jl = j - g;  // the group member this candidate is, if any (self test)
-      const int64_t idj = (EXCL && validj) ? a.id[j] : -2;
-      int* __restrict__ nlg = nl + ((size_t)g << 3);
-      const bool band =
-          (oy == 0 && oz == 0)
-              ? chunk_fast<true, EXCL>(d, s_xp[wib], s_id[wib], ni, nlg, cap8, K, j, jl, idj,
-                                       cxx, cyy, czz, lo, mid2, hw, cnt)
-              : chunk_fast<false, EXCL>(d, s_xp[wib], s_id[wib], ni, nlg, cap8, K, j, jl, idj,
-                                        cxx, cyy, czz, lo, mid2, hw, cnt);
-      if (__builtin_expect(__any_sync(0xffffffffu, band), 0)) {
-        // borderline candidates of this chunk: the reference's FP64 test decides
-#pragma unroll
-        for (int m = 0; m < 32; ++m)
-          if (lane == m) s_cnt[wib][m] = cnt[m];
-        __syncwarp();
-        const int ncy = cy + oy, ncz = cz + oz;
-        const int wy = ncy < 0 ? -1 : (ncy >= d.nc[1] ? 1 : 0);
-        const int wz = ncz < 0 ? -1 : (ncz >= d.nc[2] ? 1 : 0);
-        const int ox = seg - 1;
-        const int wx = seg == 0 ? (cx == 0 ? -1 : 0) : (seg == 2 ? (cx == d.nc[0] - 1 ? 1 : 0) : 0);
-        const bool fwd = oz > 0 || (oz == 0 && (oy > 0 || (oy == 0 && ox > 0)));
-        for (int m = 0; m < ni; ++m) {
-          const unsigned long long rp = pair_r2(s_xp[wib][m >> 1], cxx, cyy, czz);
-          const float r2 = (m & 1) ? f2_hi(rp) : f2_lo(rp);
-          const bool bd = r2 >= lo && r2 <= hi && jl != m;
-          if (!__any_sync(0xffffffffu, bd)) continue;
-          bool in = bd && exact_pair_test(a.x, d.cap, g + m, j, fwd, wx * d.L[0], wy * d.L[1],
-                                          wz * d.L[2], cutsq);
-          if (EXCL && in && is_excluded(d, s_id[wib][m], idj)) in = false;
-          const unsigned mm = __ballot_sync(0xffffffffu, in);
-          const int c0 = s_cnt[wib][m];
-          nl_append(nlg + 8 * m, cap8, K, c0, mm, in, j);
-          __syncwarp();
-          if (lane == 0) s_cnt[wib][m] = c0 + __popc(mm);
-          __syncwarp();
+      const int nrow = ct0 + ct1 + ct2;
+      for (int cb = 0; cb < nrow; cb += 32) {
+        const int nv = min(32, nrow - cb);
+        {
+          const int t = cb + lane;
+          const bool validj = t < nrow;
+          const int seg = t < ct0 ? 0 : (t < ct0 + ct1 ? 1 : 2);
+          const int j = !validj ? -1
+                                : (seg == 0 ? st0 + t : (seg == 1 ? st1 + t - ct0 : st2 + t - ct0 - ct1));
+          float4 rj = validj ? xr[j] : make_float4(-1e18f, -1e18f, -1e18f, 0.f);
+          ch.x[lane] = rj.x + (seg - 1) * hx;
+          ch.y[lane] = rj.y + oy * hy;
+          ch.z[lane] = rj.z + oz * hz;
+          ch.j[lane] = j;
+          if (EXCL) ch.id[lane] = validj ? a.id[j] : -2;
         }
-#pragma unroll
-        for (int m = 0; m < 32; ++m) cnt[m] = s_cnt[wib][m];
+        __syncwarp();
+        const bool band =
+            rr == 4 ? chunk_scan<true, EXCL>(d, ch, nv, xi2, yi2, zi2, i, idi, lo, mid2, hw, srow, pend)
+                    : chunk_scan<false, EXCL>(d, ch, nv, xi2, yi2, zi2, i, idi, lo, mid2, hw, srow,
+                                              pend);
+        if (__builtin_expect(__any_sync(0xffffffffu, band), 0) && own) {
+          // borderline candidates of this chunk: the reference's FP64 test decides
+          const int ncy = cy + oy, ncz = cz + oz;
+          const int wy = ncy < 0 ? -1 : (ncy >= d.nc[1] ? 1 : 0);
+          const int wz = ncz < 0 ? -1 : (ncz >= d.nc[2] ? 1 : 0);
+          for (int m = 0; m < nv; ++m) {
+            const unsigned long long dx = f2_sub(xi2, f2_pack(ch.x[m], ch.x[m]));
+            const unsigned long long dy = f2_sub(yi2, f2_pack(ch.y[m], ch.y[m]));
+            const unsigned long long dz = f2_sub(zi2, f2_pack(ch.z[m], ch.z[m]));
+            const float r2 = f2_lo(f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx))));
+            const int j = ch.j[m];
+            if (!(r2 >= lo && r2 <= hi) || j == i) continue;
+            const int t = cb + m;
+            const int seg = t < ct0 ? 0 : (t < ct0 + ct1 ? 1 : 2);
+            const int ox = seg - 1;
+            const int wx = seg == 0 ? (cx == 0 ? -1 : 0) : (seg == 2 ? (cx == d.nc[0] - 1 ? 1 : 0) : 0);
+            const bool fwd = oz > 0 || (oz == 0 && (oy > 0 || (oy == 0 && ox > 0)));
+            bool in = exact_pair_test(a.x, d.cap, i, j, fwd, wx * d.L[0], wy * d.L[1], wz * d.L[2],
+                                      cutsq);
+            if (EXCL && in && is_excluded(d, idi, ch.id[m])) in = false;
+            if (in) srow[pend++] = j;
+          }
+        }
+        stage_flush(srow, pend, blk, nl, i, cap, K >> 3);
         __syncwarp();
       }
     }
-    int my = 0;
-#pragma unroll
-    for (int m = 0; m < 32; ++m) my = lane == m ? cnt[m] : my;
-    if (lane < ni) {
-      const int i = g + lane;
-      if (my > K) atomicOr(d.err, kErrNlOverflow);
-      const int cc = min(my, K);
-      d.nn[i] = cc;
+    const int total = blk * 8 + pend;
+    if (own) {
+      if (total > K) atomicOr(d.err, kErrNlOverflow);
+      d.nn[i] = min(total, K);
       // pad to a multiple of 8 with the particle itself (r^2 = 0, masked by the force
       // kernels) so that batches of 8 need no bounds checks; K is a multiple of 8
-      for (int k = cc; k < ((cc + 7) & ~7); ++k) nl[nl_index(k, i, d.cap)] = i;
+      if (pend > 0) {
+        for (int k = pend; k < 8; ++k) srow[k] = i;
+        pend = 8;
+        stage_flush(srow, pend, blk, nl, i, cap, K >> 3);
+      }
     }
-    const int wmax = __reduce_max_sync(0xffffffffu, lane < ni ? my : 0);
+    const int wmax = __reduce_max_sync(0xffffffffu, own ? total : 0);
     if (lane == 0 && wmax > 0) atomicMax(&d.ctr->nnMax, wmax);
     __syncwarp();
+  }
+}
+
+// ---- Verlet build with a tensor-core distance prefilter ----------------------------
+// Tiles of whole cells of one x-row of the cell grid (at most 128 particles, at most
+// kTbMaxCells cells; a cell with more particles is split into tiles of 128).  The
+// tile's candidates are the particles of its 9 stencil rows over the x-cells from one
+// before to one after the tile ("columns"), enumerated column-major.  Chunks of 128
+// candidates are staged in shared memory and one tcgen05.mma (kind::f16, M = N = 128,
+// K = 16, FP32 accumulators in TMEM) gives for every (tile particle, candidate) slot
+//   D = |x_i|^2 + |x_j|^2 - 2 x_i.x_j - thr,   thr = 1.02 (rc+skin)^2 + 0.05,
+// with the coordinates in a frame centred on the tile and each coordinate carried as an
+// FP16 pair (hi + lo: 22 significant bits); the neglected lo*lo products and the FP32
+// accumulation leave an error far below the margin in thr.  Thread t reads its row of D
+// with tcgen05.ld and collects the sign bits; only those candidates (about 1.02 times
+// the neighbours) are tested exactly, in FP32, with the same borderline band and FP64
+// decision (exact_pair_test) as the other build forms, and against the 27-cell stencil
+// of the particle's own cell.  The pair set is therefore the reference's
+// (VerletList.cpp:274-450); each list is in a fixed order (column-major candidates).
+constexpr int kTbRows = 128;                    // tile particles (MMA M)
+constexpr int kTbN = 128;                       // candidates per chunk (MMA N, TMEM columns)
+constexpr int kTbMaxCells = 32;                 // cells per tile
+constexpr int kTbMaxW = kTbMaxCells + 2;        // candidate columns
+constexpr int kTbSegs = 9 * kTbMaxW;            // (column, stencil row) segments
+constexpr int kTbSmem = 50 * 1024;              // dynamic shared memory: at most 4 CTAs / SM
+
+struct TbSmem {
+  alignas(128) uint8_t A[kTbRows * 32];          // tile particles: 16 FP16 terms each
+  alignas(128) uint8_t B[2][kTbN * 32];          // candidates: 16 FP16 terms each
+  float4 cand[2][kTbN];                          // x, y, z in the tile frame; j as bits
+  int cseg[2][kTbN];                             // segment (column * 9 + row) of each
+  int cw[2][2];                                  // first and last column of the chunk
+  int segStart[kTbSegs];
+  int segPre[kTbSegs + 1];
+  alignas(16) int stage[kTbRows * kStageLd];  // rows read and written as 16-byte vectors
+  alignas(8) unsigned long long mbar;
+  uint32_t tmem;
+  int abort;
+};
+static_assert(sizeof(TbSmem) + 128 <= kTbSmem, "tile build shared memory");
+static_assert(offsetof(TbSmem, stage) % 16 == 0 && (kStageLd * 4) % 16 == 0,
+              "staging rows are accessed as 16-byte vectors");
+static_assert(offsetof(TbSmem, cand) % 16 == 0, "candidates are read as 16-byte vectors");
+
+__device__ __forceinline__ uint32_t pack_h2(float a, float b) {
+  const __half2 h = __floats2half2_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+__device__ __forceinline__ void split_h(float v, float& hi, float& lo) {
+  hi = __half2float(__float2half_rn(v));
+  lo = v - hi;
+}
+
+template <bool EXCL>
+__global__ void __launch_bounds__(kTbRows, 4) k_build_nl_tc(DevView d, double cutsq) {
+  extern __shared__ __align__(128) uint8_t tb_raw[];
+  TbSmem& S = *reinterpret_cast<TbSmem*>(((uintptr_t)tb_raw + 127) & ~(uintptr_t)127);
+  const ParticleArrays a = d.pa[0];
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int nx = d.nc[0], ny = d.nc[1], nz = d.nc[2];
+  const float lo = (float)(cutsq * (1.0 - 2e-5)), hi = (float)(cutsq * (1.0 + 2e-5));
+  const float thr = (float)(cutsq * 1.02 + 0.05);
+  const float hx = (float)d.cellSize[0], hy = (float)d.cellSize[1], hz = (float)d.cellSize[2];
+  const float4* __restrict__ xr = d.xrel;
+  const int* __restrict__ cs = d.cellStart;
+  const int K = d.K;
+  const size_t cap = d.cap;
+  int* __restrict__ nl = d.nl;
+  int* __restrict__ srow = &S.stage[t * kStageLd];
+  const uint32_t mbar = tc::smem_u32(&S.mbar);
+  if (t == 0) {
+    S.abort = 0;
+    tc::mbar_init(mbar);
+  }
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tmem), kTbN);
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = S.tmem;
+  const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
+  const uint32_t idesc = tc::idesc_f16(kTbRows, kTbN, false);
+  const uint64_t dA = tc::desc(tc::smem_u32(S.A), kTbRows);
+  uint32_t phase = 0;
+  bool abort = false;
+  int nmax = 0;
+  for (int row = blockIdx.x; row < ny * nz && !abort; row += gridDim.x) {
+    const int cy = row % ny, cz = row / ny;
+    const int rb = nx * row;
+    for (int ca = 0; ca < nx && !abort;) {
+      // the tile: cells ca..cb of this row, together at most 128 particles (or one cell)
+      int cb = ca;
+      while (cb + 1 < nx && cb + 1 - ca < kTbMaxCells && cs[rb + cb + 2] - cs[rb + ca] <= kTbRows)
+        ++cb;
+      const int p0 = cs[rb + ca], p1 = cs[rb + cb + 1];
+      if (p0 == p1) {
+        ca = cb + 1;
+        continue;
+      }
+      const int c0 = ca - 1, W = cb - ca + 3;
+      const float wc = 0.5f * (float)W;
+      // candidate segments (column w, stencil row rr), column-major
+      __syncthreads();  // the previous tile's readers of the segment table are done
+      for (int s = t; s < 9 * W; s += kTbRows) {
+        const int w = s / 9, rr = s % 9;
+        const int oz = rr / 3 - 1, oy = rr % 3 - 1;
+        int ncy = cy + oy, ncz = cz + oz;
+        ncy += ncy < 0 ? ny : (ncy >= ny ? -ny : 0);
+        ncz += ncz < 0 ? nz : (ncz >= nz ? -nz : 0);
+        int ncx = (c0 + w) % nx;
+        ncx += ncx < 0 ? nx : 0;
+        const int cell = ncx + nx * (ncy + ny * ncz);
+        S.segStart[s] = cs[cell];
+        S.segPre[s] = cs[cell + 1] - cs[cell];
+      }
+      __syncthreads();
+      if (warp == 0) {
+        int run = 0;
+        for (int base = 0; base < 9 * W; base += 32) {
+          const int s = base + lane;
+          const int c = s < 9 * W ? S.segPre[s] : 0;
+          int incl = c;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
+          }
+          if (s < 9 * W) S.segPre[s] = run + incl - c;
+          run += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (lane == 0) S.segPre[9 * W] = run;
+      }
+      __syncthreads();
+      const int ncand = S.segPre[9 * W];
+      const int nchunks = (ncand + kTbN - 1) / kTbN;
+      for (int s0 = p0; s0 < p1 && !abort; s0 += kTbRows) {
+        __syncthreads();  // the previous sub-tile's readers of the chunk buffers are done
+        const int ni = min(kTbRows, p1 - s0);
+        const bool own = t < ni;
+        const int i = own ? s0 + t : s0;
+        // this particle in the tile frame, and its column
+        const float4 ri = xr[i];
+        const int wi = d.pcell[i] % nx - c0;
+        const float xi = ri.x + ((float)wi - wc) * hx, yi = ri.y - 0.5f * hy, zi = ri.z - 0.5f * hz;
+        {
+          float xh, xl, yh, yl, zh, zl, sh, sl;
+          split_h(xi, xh, xl);
+          split_h(yi, yh, yl);
+          split_h(zi, zh, zl);
+          split_h(xi * xi + yi * yi + zi * zi, sh, sl);
+          uint4 q0, q1;
+          if (own) {
+            q0 = make_uint4(pack_h2(xh, xl), pack_h2(xh, yh), pack_h2(yl, yh), pack_h2(zh, zl));
+            q1 = make_uint4(pack_h2(zh, sh), pack_h2(sl, 1.f), pack_h2(1.f, 0.f), 0u);
+          } else {
+            q0 = make_uint4(0u, 0u, 0u, 0u);
+            q1 = q0;
+          }
+          *reinterpret_cast<uint4*>(S.A + tc::canon_off(t, 0, kTbRows)) = q0;
+          *reinterpret_cast<uint4*>(S.A + tc::canon_off(t, 8, kTbRows)) = q1;
+        }
+        const int64_t idi = (EXCL && own) ? a.id[i] : -3;
+        // column range of this warp's particles (for skipping far chunks)
+        const int wlo = __reduce_min_sync(0xffffffffu, own ? wi : 1 << 20);
+        const int whi = __reduce_max_sync(0xffffffffu, own ? wi : -(1 << 20));
+        int pend = 0, blk = 0;
+        for (int q = 0; q < nchunks; ++q) {
+          const int buf = q & 1;
+          // stage candidate q * 128 + t
+          {
+            const int n = q * kTbN + t;
+            uint4 q0 = make_uint4(0u, 0u, 0u, 0u), q1 = q0;
+            int sg = -1;
+            if (n < ncand) {
+              int lo_s = 0, hi_s = 9 * W - 1;  // largest s with segPre[s] <= n
+              while (lo_s < hi_s) {
+                const int mid = (lo_s + hi_s + 1) >> 1;
+                if (S.segPre[mid] <= n) lo_s = mid;
+                else hi_s = mid - 1;
+              }
+              sg = lo_s;
+              const int w = sg / 9, rr = sg % 9;
+              const int j = S.segStart[sg] + (n - S.segPre[sg]);
+              const float4 rj = xr[j];
+              const float fx = rj.x + ((float)w - wc) * hx;
+              const float fy = rj.y + ((float)(rr % 3 - 1) - 0.5f) * hy;
+              const float fz = rj.z + ((float)(rr / 3 - 1) - 0.5f) * hz;
+              S.cand[buf][t] = make_float4(fx, fy, fz, __int_as_float(j));
+              float xh, xl, yh, yl, zh, zl, th, tlw;
+              split_h(-2.f * fx, xh, xl);
+              split_h(-2.f * fy, yh, yl);
+              split_h(-2.f * fz, zh, zl);
+              split_h(fx * fx + fy * fy + fz * fz - thr, th, tlw);
+              q0 = make_uint4(pack_h2(xh, xh), pack_h2(xl, yh), pack_h2(yh, yl), pack_h2(zh, zh));
+              q1 = make_uint4(pack_h2(zl, 1.f), pack_h2(1.f, th), pack_h2(tlw, 0.f), 0u);
+            } else {
+              // no candidate: D = 60000 > 0
+              q1 = make_uint4(0u, pack_h2(0.f, 60000.f), 0u, 0u);
+            }
+            S.cseg[buf][t] = sg;
+            *reinterpret_cast<uint4*>(S.B[buf] + tc::canon_off(t, 0, kTbN)) = q0;
+            *reinterpret_cast<uint4*>(S.B[buf] + tc::canon_off(t, 8, kTbN)) = q1;
+            if (t == 0) S.cw[buf][0] = sg / 9;
+            const int last = min(kTbN, ncand - q * kTbN) - 1;
+            if (t == last) S.cw[buf][1] = sg / 9;
+          }
+          tc::fence_async_smem();
+          tc::fence_before();
+          __syncthreads();
+          tc::fence_after();
+          if (S.abort) {
+            abort = true;
+            break;
+          }
+          if (t == 0) {
+            tc::mma_f16(tmem, dA, tc::desc(tc::smem_u32(S.B[buf]), kTbN), idesc, 0);
+            tc::commit(mbar);
+          }
+          if (!tc::mbar_wait(mbar, phase)) {
+            S.abort = 1;
+            atomicOr(d.err, kErrTimeout);
+          }
+          phase ^= 1u;
+          tc::fence_after();
+          // warps whose particles are more than one column away from the whole chunk
+          // skip it (all its candidates are outside their stencils)
+          if (whi >= 0 && S.cw[buf][1] >= wlo - 1 && S.cw[buf][0] <= whi + 1) {
+#pragma unroll 1
+            for (int h = 0; h < kTbN / 32; ++h) {
+              uint32_t v[32];
+              tc::tmem_ld32(tl + 32 * h, v);
+              tc::wait_ld();
+              uint32_t m = 0;
+#pragma unroll
+              for (int k = 0; k < 32; ++k) m = __funnelshift_l(v[k], m, 1);
+              m = own ? __brev(m) : 0u;
+              while (m) {
+                const int b = __ffs(m) - 1;
+                m &= m - 1;
+                const int n = 32 * h + b;
+                const int sg = S.cseg[buf][n];
+                const int w = sg / 9;
+                const int ox = w - wi;
+                if (ox < -1 || ox > 1) continue;
+                const float4 c = S.cand[buf][n];
+                const int j = __float_as_int(c.w);
+                if (j == i) continue;
+                const float dx = xi - c.x, dy = yi - c.y, dz = zi - c.z;
+                const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+                bool in;
+                if (r2 < lo) {
+                  in = true;
+                } else if (r2 > hi) {
+                  in = false;
+                } else {
+                  const int rr = sg % 9;
+                  const int oz = rr / 3 - 1, oy = rr % 3 - 1;
+                  const int cxi = wi + c0;
+                  const int wx = cxi + ox < 0 ? -1 : (cxi + ox >= nx ? 1 : 0);
+                  const int ncy = cy + oy, ncz = cz + oz;
+                  const int wy = ncy < 0 ? -1 : (ncy >= ny ? 1 : 0);
+                  const int wz = ncz < 0 ? -1 : (ncz >= nz ? 1 : 0);
+                  const bool fwd = oz > 0 || (oz == 0 && (oy > 0 || (oy == 0 && ox > 0)));
+                  in = exact_pair_test_inl(a.x, d.cap, i, j, fwd, wx * d.L[0], wy * d.L[1],
+                                       wz * d.L[2], cutsq);
+                }
+                if (EXCL && in && is_excluded(d, idi, a.id[j])) in = false;
+                if (in) srow[pend++] = j;
+              }
+              if (pend >= 8) stage_flush(srow, pend, blk, nl, i, cap, K >> 3);
+            }
+          }
+          tc::fence_before();
+        }
+        if (abort) break;
+        const int total = blk * 8 + pend;
+        if (own) {
+          if (total > K) atomicOr(d.err, kErrNlOverflow);
+          d.nn[i] = min(total, K);
+          // pad to a multiple of 8 with the particle itself (r^2 = 0, masked by the
+          // force kernels) so that batches of 8 need no bounds checks
+          if (pend > 0) {
+            for (int k = pend; k < 8; ++k) srow[k] = i;
+            pend = 8;
+            stage_flush(srow, pend, blk, nl, i, cap, K >> 3);
+          }
+          nmax = max(nmax, total);
+        }
+      }
+      ca = cb + 1;
+    }
+  }
+  const int wmax = __reduce_max_sync(0xffffffffu, nmax);
+  if (lane == 0 && wmax > 0) atomicMax(&d.ctr->nnMax, wmax);
+  tc::fence_before();
+  __syncthreads();
+  // after a timed-out wait, give the outstanding product its own bounded wait before the
+  // tensor memory is released
+  if (S.abort && t == 0) tc::mbar_wait(mbar, phase);
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after();
+    tc::tmem_dealloc(tmem, kTbN);
   }
 }
 
@@ -1634,12 +1925,38 @@ void launch_posq(const DevView& d, cudaStream_t st) {
   if (d.n > 0) k_posq<<<blocks_for(d.n), kBlock, 0, st>>>(d);
 }
 
+// The particle-per-lane form is the default; ESPP_B200_BUILD=tc selects the form with the
+// tensor-core prefilter (same pair set, slower on the LJ benchmark: its survivor pass is
+// latency-bound).
 void launch_build_nl(const DevView& d, double cutsq, cudaStream_t st) {
-  long long threads = (long long)d.ncells * 32;
+  const char* form = getenv("ESPP_B200_BUILD");
+  // the tensor-core form keeps every tile-frame coordinate well inside the FP16 range
+  const bool tcok = d.nc[0] >= 3 && (0.5 * kTbMaxW + 1.0) * d.cellSize[0] <= 100.0 &&
+                    2.0 * d.cellSize[1] <= 100.0 && 2.0 * d.cellSize[2] <= 100.0;
+  if (form && !strcmp(form, "tc") && tcok) {
+    static int nsm[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    dev &= 63;
+    if (!nsm[dev]) {
+      cudaFuncSetAttribute(k_build_nl_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmem);
+      cudaFuncSetAttribute(k_build_nl_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmem);
+      cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
+      if (nsm[dev] <= 0) nsm[dev] = 148;
+    }
+    const int rows = d.nc[1] * d.nc[2];
+    const int grid = rows < 4 * nsm[dev] ? rows : 4 * nsm[dev];
+    if (d.exclStart)
+      k_build_nl_tc<true><<<grid, kTbRows, kTbSmem, st>>>(d, cutsq);
+    else
+      k_build_nl_tc<false><<<grid, kTbRows, kTbSmem, st>>>(d, cutsq);
+    return;
+  }
+  const int nb = blocks_for((long long)d.ncells * 32, kBuildWarps * 32);
   if (d.exclStart)
-    k_build_nl<true><<<blocks_for(threads, 128), 128, 0, st>>>(d, cutsq);
+    k_build_nl_lane<true><<<nb, kBuildWarps * 32, 0, st>>>(d, cutsq);
   else
-    k_build_nl<false><<<blocks_for(threads, 128), 128, 0, st>>>(d, cutsq);
+    k_build_nl_lane<false><<<nb, kBuildWarps * 32, 0, st>>>(d, cutsq);
 }
 
 template <int TPP, bool MIXED>

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include "espp_mlp.h"
+#include "espp_tc.h"
 
 namespace espp {
 
@@ -548,85 +549,23 @@ namespace {
 
 constexpr int kTcRows = 128;
 constexpr int kTcCols = 256;              // TMEM columns: Z1 0, Z2 64, G1 128, DX 192
-constexpr long long kTcSpin = 1ll << 26;  // bounded mbarrier wait
+using tc::canon_off;
+using tc::fence_async_smem;
+using tc::mbar_wait;
+using tc::smem_u32;
+using tc::tmem_ld16;
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-// byte offset of element (r, k) in a canonical K-major operand of R rows
-__device__ __forceinline__ int canon_off(int r, int k, int R) {
-  return (((k >> 3) * (R >> 3) + (r >> 3)) * 8 + (r & 7)) * 16 + (k & 7) * 2;
-}
-
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, int R) {
-  const uint64_t lbo = (uint64_t)(R * 16) >> 4, sbo = 128 >> 4;
-  return (uint64_t)((saddr >> 4) & 0x3FFF) | (lbo << 16) | (sbo << 32) | (1ull << 46);
-}
-
-// kind::f16 instruction descriptor: BF16 x BF16 -> F32, K-major A and B, M = 128
-__host__ __device__ constexpr uint32_t umma_idesc(int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
-         ((uint32_t)(kTcRows >> 4) << 24);
-}
-
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, int R) { return tc::desc(saddr, R); }
+// BF16 x BF16 -> F32, K-major A and B, M = 128
+__host__ __device__ constexpr uint32_t umma_idesc(int N) { return tc::idesc_f16(kTcRows, N, true); }
 __device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
                                      int accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
-      :
-      : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u),
-        "r"(0u));
+  tc::mma_f16(tmem_d, da, db, idesc, accumulate);
 }
-
-__device__ __forceinline__ void umma_commit(uint32_t mbar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
-      : "memory");
-}
-
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
-  for (long long it = 0; it < kTcSpin; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(mbar), "r"(phase)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-      "%11, %12, %13, %14, %15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-#pragma unroll
-  for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
-}
-
-__device__ __forceinline__ void tmem_wait_ld() {
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void fence_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
+__device__ __forceinline__ void umma_commit(uint32_t mbar) { tc::commit(mbar); }
+__device__ __forceinline__ void tmem_wait_ld() { tc::wait_ld(); }
+__device__ __forceinline__ void tc_fence_before() { tc::fence_before(); }
+__device__ __forceinline__ void tc_fence_after() { tc::fence_after(); }
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
   const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
