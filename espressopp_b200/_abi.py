@@ -56,6 +56,15 @@ PROTOTYPES = {
     "espp_virial_tensor": (c_int32, [_P, c_int32, _D]),
     "espp_kinetic": (c_int32, [_P, _D, _I64]),
     "espp_rdf": (c_int32, [_P, c_int32, _D]),
+    "espp_confs_create": (c_int32, [_P, c_int32, c_int64, _I64, POINTER(c_void_p)]),
+    "espp_confs_destroy": (c_int32, [_P]),
+    "espp_confs_gather": (c_int32, [_P]),
+    "espp_confs_push": (c_int32, [_P, _D]),
+    "espp_confs_size": (c_int32, [_P, _I32]),
+    "espp_confs_clear": (c_int32, [_P]),
+    "espp_confs_get": (c_int32, [_P, c_int32, _D]),
+    "espp_msd": (c_int32, [_P, _D]),
+    "espp_msd_chain_com": (c_int32, [_P, c_int32, _D]),
     "espp_force_acc": (c_int32, [_P, c_int32, c_int64, _I64, _D]),
     "espp_mlp_create": (c_int32, [c_double, c_double, POINTER(c_void_p)]),
     "espp_mlp_destroy": (c_int32, [_P]),
@@ -93,6 +102,7 @@ IA_MLP = 4
 IA_COSINE = 5
 TAB_LINEAR, TAB_AKIMA, TAB_CUBIC = 1, 2, 3
 CAP_OFF, CAP_ABS, CAP_COMPONENT = 0, 1, 2
+CONF_POSITION, CONF_VELOCITY, CONF_UNFOLDED = 0, 1, 2
 
 
 def bind(lib, extra=None):

@@ -1,6 +1,6 @@
 """Observables (src/analysis/Temperature.hpp:57-125, Pressure.cpp:41-119,
-PressureTensor.hpp:51-80, RadialDistrF.cpp:47-150, NPart).  Reductions run on the GPU in
-FP64."""
+PressureTensor.hpp:51-80, RadialDistrF.cpp:47-150, NPart, ConfigsParticleDecomp.cpp,
+MeanSquareDispl.cpp).  Reductions run on the GPU in FP64."""
 import ctypes
 
 import numpy as np
@@ -88,3 +88,156 @@ class RadialDistrF(_Observable):
         call(st._lib, "espp_rdf", st._h, int(rdfN), out.ctypes.data_as(
             ctypes.POINTER(ctypes.c_double)))
         return list(out)
+
+
+class Configuration:
+    """One snapshot (analysis/Configuration.cpp:103-240): values by particle id."""
+
+    def __init__(self, ids, xyz):
+        self._ids = [int(i) for i in ids]
+        self._index = {pid: k for k, pid in enumerate(self._ids)}
+        self._xyz = np.asarray(xyz, np.float64).reshape(-1, 3)
+
+    def getCoordinates(self, pid):
+        return tuple(float(v) for v in self._xyz[self._index[int(pid)]])
+
+    __getitem__ = getCoordinates
+
+    def getIds(self):
+        return list(self._ids)
+
+    def __iter__(self):
+        return iter(self._ids)
+
+    @property
+    def size(self):
+        return len(self._ids)
+
+
+class ConfigsParticleDecomp(_Observable):
+    """analysis.ConfigsParticleDecomp(system[, chainlength, start_pid])
+    (ConfigsParticleDecomp.py:40-90, ConfigsParticleDecomp.hpp:61-230): a list of
+    snapshots of the particles present at construction (or, with chainlength, of the ids
+    start_pid .. start_pid + N - 1), held on the GPU.  key selects what a snapshot holds:
+    "position", "velocity" or "unfolded" (position + image * box)."""
+
+    key = "position"
+    _KEYS = {"position": 0, "velocity": 1, "unfolded": 2}
+
+    def __init__(self, system, chainlength=None, start_pid=0):
+        super().__init__(system)
+        st = self._st()
+        if self.key not in self._KEYS:
+            raise RuntimeError("Error. Key %s is unknown. Use position, unfolded or velocity."
+                               % self.key)
+        n = st.getNRealParticles()
+        if chainlength is None:
+            ids = st.getRealParticleIDs()
+        else:
+            if n % int(chainlength) != 0:
+                print("chainlength does not match total number of particles\n"
+                      "chainlength: %d\n num_of_part %d\n" % (chainlength, n))
+            ids = list(range(int(start_pid), int(start_pid) + n))
+        self.chainlength = None if chainlength is None else int(chainlength)
+        self.start_pid = int(start_pid)
+        self.num_of_part = n
+        self._ids = np.ascontiguousarray(ids, np.int64)
+        self._lib = st._lib
+        h = ctypes.c_void_p()
+        call(self._lib, "espp_confs_create", st._h, self._KEYS[self.key], len(self._ids),
+             self._ids.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), ctypes.byref(h))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.espp_confs_destroy(h)
+            self._h = None
+
+    def gather(self):
+        call(self._lib, "espp_confs_gather", self._h)
+
+    def gatherFromFile(self, filename):
+        """Reads "id type x y z" lines after two header lines (ConfigsParticleDecomp.cpp:144-206)."""
+        try:
+            with open(filename) as f:
+                lines = f.read().splitlines()[2:]
+        except OSError:
+            raise RuntimeError("Unable to open file %s" % filename)
+        conf = {}
+        for line in lines:
+            parts = line.split()
+            if len(parts) >= 5:
+                conf[int(parts[0])] = (float(parts[2]), float(parts[3]), float(parts[4]))
+        print("read %d particles from file %s" % (len(conf), filename))
+        if len(conf) != self.num_of_part:
+            raise RuntimeError("Number of read particles does not match the number of particles "
+                               "of the system (which is %d)" % self.num_of_part)
+        xyz = np.array([conf[int(pid)] for pid in self._ids], np.float64).reshape(-1)
+        call(self._lib, "espp_confs_push", self._h,
+             xyz.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+
+    def clear(self):
+        call(self._lib, "espp_confs_clear", self._h)
+
+    @property
+    def size(self):
+        m = ctypes.c_int32()
+        call(self._lib, "espp_confs_size", self._h, ctypes.byref(m))
+        return m.value
+
+    def __getitem__(self, m):
+        out = np.zeros(3 * len(self._ids))
+        call(self._lib, "espp_confs_get", self._h, int(m),
+             out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return Configuration(self._ids, out)
+
+    def all(self):
+        return [self[m] for m in range(self.size)]
+
+    def __iter__(self):
+        return iter(self.all())
+
+    def compute(self):
+        raise NotImplementedError("compute() is defined by the derived analyses")
+
+
+class MeanSquareDispl(ConfigsParticleDecomp):
+    """analysis.MeanSquareDispl(system[, chainlength, start_pid]) (MeanSquareDispl.py:50-80,
+    MeanSquareDispl.cpp): snapshots of unfolded positions; compute() returns, for every lag
+    m, the mean over snapshot pairs and particles of |r(t) - r(t+m)|^2 / 6; computeG3() the
+    same for the centres of mass of the chains relative to their snapshot's mean.  The lag
+    sums run on the GPU in FP64."""
+
+    key = "unfolded"
+
+    def __init__(self, system, chainlength=None, start_pid=0):
+        super().__init__(system, chainlength, start_pid)
+        self.print_progress = True
+
+    def _progress_done(self):
+        print("calculation progress (mean square displacement): 100%")
+
+    def compute(self):
+        out = np.zeros(self.size)
+        call(self._lib, "espp_msd", self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        self._progress_done()
+        return list(out)
+
+    def computeG2(self):
+        print("Sorry. Computation of G2 does not work correctly.", end="")
+        print("Update ESPResSO++ when it is repaired. ")
+        return []
+
+    def computeG3(self):
+        if self.chainlength is None:
+            raise RuntimeError("computeG3 needs the chainlength given at construction")
+        out = np.zeros(self.size)
+        call(self._lib, "espp_msd_chain_com", self._h, self.chainlength,
+             out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        self._progress_done()
+        return list(out)
+
+    def strange(self):
+        print(1)
+        return 1

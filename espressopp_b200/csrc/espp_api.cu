@@ -2258,6 +2258,186 @@ int espp_rdf(espp_system* s, int32_t rdfN, double* out) {
   });
 }
 
+// ---- snapshots of tracked particles, mean-square displacement ----------------------
+
+struct espp_confs {
+  espp_system* s = nullptr;
+  int key = 0;
+  int64_t n = 0;
+  int64_t* ids = nullptr;    // device, tracked ids in order
+  double* snap = nullptr;    // device, M snapshots of 3 n doubles
+  int M = 0, capM = 0;
+};
+
+namespace espp {
+namespace {
+void confs_reserve(espp_confs* c, int M) {
+  if (M <= c->capM) return;
+  const int cap = std::max(M, std::max(8, 2 * c->capM));
+  double* nb = dalloc<double>((size_t)cap * 3 * std::max<int64_t>(c->n, 1));
+  if (c->M > 0)
+    cuda_check(cudaMemcpyAsync(nb, c->snap, sizeof(double) * 3 * (size_t)c->n * c->M,
+                               cudaMemcpyDeviceToDevice, c->s->st), "copy");
+  sync(c->s);
+  dfree(c->snap);
+  c->snap = nb;
+  c->capM = cap;
+}
+// per-lag sums from the per-block partials, in block order
+void msd_finish(espp_confs* c, int64_t n, const double* dsnap, double* Z) {
+  const int M = c->M;
+  const int nb = msd_blocks(n);
+  double* part = dalloc<double>((size_t)M * nb);
+  std::vector<double> h((size_t)M * nb);
+  try {
+    launch_msd(dsnap, n, M, part, c->s->st);
+    cuda_check(cudaGetLastError(), "msd kernel");
+    cuda_check(cudaMemcpyAsync(h.data(), part, sizeof(double) * h.size(), cudaMemcpyDeviceToHost,
+                               c->s->st), "download");
+    sync(c->s);
+  } catch (...) {
+    dfree(part);
+    throw;
+  }
+  dfree(part);
+  for (int m = 0; m < M; ++m) {
+    double z = 0.0;
+    for (int b = 0; b < nb; ++b) z += h[(size_t)m * nb + b];
+    Z[m] = z;
+  }
+}
+}  // namespace
+}  // namespace espp
+
+int espp_confs_create(espp_system* s, int32_t key, int64_t n, const int64_t* ids,
+                      espp_confs** out) {
+  return guard([&] {
+    checked(s);
+    if (!out) raise(ESPP_EINVAL, "null output pointer");
+    if (key < ESPP_CONF_POSITION || key > ESPP_CONF_UNFOLDED)
+      raise(ESPP_EINVAL, "Error. Key is unknown. Use position, unfolded or velocity.");
+    if (n < 0 || (n > 0 && !ids)) raise(ESPP_EINVAL, "bad id list");
+    auto c = std::make_unique<espp_confs>();
+    c->s = s;
+    c->key = key;
+    c->n = n;
+    if (n > 0) {
+      c->ids = dalloc<int64_t>((size_t)n);
+      cuda_check(cudaMemcpyAsync(c->ids, ids, sizeof(int64_t) * n, cudaMemcpyHostToDevice, s->st),
+                 "upload");
+      sync(s);
+    }
+    *out = c.release();
+  });
+}
+
+int espp_confs_destroy(espp_confs* c) {
+  return guard([&] {
+    if (!c) return;
+    dfree(c->ids);
+    dfree(c->snap);
+    delete c;
+  });
+}
+
+int espp_confs_gather(espp_confs* c) {
+  return guard([&] {
+    if (!c) raise(ESPP_EINVAL, "null handle");
+    espp_system* s = c->s;
+    checked(s);
+    ensure_id_map(s);
+    confs_reserve(c, c->M + 1);
+    launch_conf_gather(s->view(), c->ids, c->n, c->key, c->snap + (size_t)c->M * 3 * c->n, s->st);
+    cuda_check(cudaGetLastError(), "gather kernel");
+    sync(s);
+    check_err(s);
+    ++c->M;
+  });
+}
+
+int espp_confs_push(espp_confs* c, const double* xyz) {
+  return guard([&] {
+    if (!c) raise(ESPP_EINVAL, "null handle");
+    if (c->n > 0 && !xyz) raise(ESPP_EINVAL, "null argument");
+    confs_reserve(c, c->M + 1);
+    if (c->n > 0)
+      cuda_check(cudaMemcpyAsync(c->snap + (size_t)c->M * 3 * c->n, xyz, sizeof(double) * 3 * c->n,
+                                 cudaMemcpyHostToDevice, c->s->st), "upload");
+    sync(c->s);
+    ++c->M;
+  });
+}
+
+int espp_confs_size(espp_confs* c, int32_t* m) {
+  return guard([&] {
+    if (!c || !m) raise(ESPP_EINVAL, "null argument");
+    *m = c->M;
+  });
+}
+
+int espp_confs_clear(espp_confs* c) {
+  return guard([&] {
+    if (!c) raise(ESPP_EINVAL, "null handle");
+    c->M = 0;
+  });
+}
+
+int espp_confs_get(espp_confs* c, int32_t m, double* xyz) {
+  return guard([&] {
+    if (!c || !xyz) raise(ESPP_EINVAL, "null argument");
+    if (m < 0 || m >= c->M) raise(ESPP_ERANGE, "Error. Velocities::get <out-of-range>");
+    if (c->n > 0)
+      cuda_check(cudaMemcpyAsync(xyz, c->snap + (size_t)m * 3 * c->n, sizeof(double) * 3 * c->n,
+                                 cudaMemcpyDeviceToHost, c->s->st), "download");
+    sync(c->s);
+  });
+}
+
+int espp_msd(espp_confs* c, double* out) {
+  return guard([&] {
+    if (!c || !out) raise(ESPP_EINVAL, "null argument");
+    const int M = c->M;
+    if (M == 0) return;
+    std::vector<double> Z(M);
+    msd_finish(c, c->n, c->snap, Z.data());
+    // MeanSquareDispl.cpp:127-137: divide by the number of pairs of snapshots, then by 6 N
+    const double inv_coef = 1.0 / (6.0 * (double)c->n);
+    for (int m = 0; m < M; ++m) {
+      Z[m] /= (double)(M - m);
+      out[m] = Z[m] * inv_coef;
+    }
+  });
+}
+
+int espp_msd_chain_com(espp_confs* c, int32_t chainlength, double* out) {
+  return guard([&] {
+    if (!c || !out) raise(ESPP_EINVAL, "null argument");
+    if (chainlength <= 0) raise(ESPP_EINVAL, "chainlength must be positive");
+    const int M = c->M;
+    const int64_t nch = c->n / chainlength;
+    if (M == 0) return;
+    if (nch == 0) raise(ESPP_EINVAL, "no complete chain among the tracked particles");
+    double* com = dalloc<double>((size_t)M * 3 * nch);
+    std::vector<double> Z(M);
+    try {
+      launch_chain_com(c->snap, c->n, M, chainlength, nch, com, c->s->st);
+      cuda_check(cudaGetLastError(), "chain centre kernels");
+      // the centres relative to their snapshot mean are the items of the same lag sums
+      espp_confs tmp;
+      tmp.s = c->s;
+      tmp.M = M;
+      msd_finish(&tmp, nch, com, Z.data());
+    } catch (...) {
+      dfree(com);
+      throw;
+    }
+    dfree(com);
+    // MeanSquareDispl.cpp:419-425
+    const double inv_coef = 1.0 / (6.0 * (double)nch);
+    for (int m = 0; m < M; ++m) out[m] = inv_coef * Z[m] / (double)(M - m);
+  });
+}
+
 int espp_set_tpp(espp_system* s, int32_t tpp) {
   return guard([&] {
     checked(s);

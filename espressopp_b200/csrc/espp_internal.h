@@ -208,6 +208,12 @@ void launch_lj_observables(const DevView& d, double* partials, int nblocks, doub
 void launch_fene_observables(const DevView& d, const FENEParams& fene, double* partials,
                              int nblocks, double* out, int energy, cudaStream_t st);
 // pair-distance histogram (integer counts, accumulated into hist) for RadialDistrF
+void launch_conf_gather(const DevView& d, const int64_t* ids, int64_t n, int key, double* dst,
+                        cudaStream_t st);
+int msd_blocks(int64_t n);
+void launch_msd(const double* snap, int64_t n, int M, double* partial, cudaStream_t st);
+void launch_chain_com(const double* snap, int64_t n, int M, int L, int64_t nch, double* com,
+                      cudaStream_t st);
 void launch_rdf(const DevView& d, int rdfN, double dr, unsigned long long* hist,
                 cudaStream_t st);
 // angular forces (per triple, then gathered per particle) added to the force output

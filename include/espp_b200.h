@@ -218,6 +218,37 @@ ESPP_API int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n);
  * bin divided by 2 pi dr rho N ((i + 1/2)^2 dr^2 + dr^2 / 12).  out receives rdfN values. */
 ESPP_API int espp_rdf(espp_system* s, int32_t rdfN, double* out);
 
+/* Snapshots of tracked particles kept on the device: analysis::ConfigsParticleDecomp
+ * (src/analysis/ConfigsParticleDecomp.hpp:61-230, ConfigsParticleDecomp.cpp:43-206) and its
+ * MeanSquareDispl (src/analysis/MeanSquareDispl.cpp).  A snapshot holds, for each tracked id
+ * in the order given at creation (ascending, as the reference's id map iterates), the
+ * position, the velocity or the unfolded position x + image * L (ESPP_CONF_*).  The handle
+ * refers to its system and must be destroyed before it. */
+typedef struct espp_confs espp_confs;
+#define ESPP_CONF_POSITION 0
+#define ESPP_CONF_VELOCITY 1
+#define ESPP_CONF_UNFOLDED 2
+ESPP_API int espp_confs_create(espp_system* s, int32_t key, int64_t n, const int64_t* ids,
+                               espp_confs** out);
+ESPP_API int espp_confs_destroy(espp_confs* c);
+/* ConfigsParticleDecomp::gather (ConfigsParticleDecomp.cpp:70-142): appends the current
+ * state.  ESPP_ESTATE if a tracked id is not in the system. */
+ESPP_API int espp_confs_gather(espp_confs* c);
+/* Appends a snapshot given by the caller (gatherFromFile, :144-206): 3 n values x y z per
+ * tracked id, in the tracked order. */
+ESPP_API int espp_confs_push(espp_confs* c, const double* xyz);
+ESPP_API int espp_confs_size(espp_confs* c, int32_t* m);
+ESPP_API int espp_confs_clear(espp_confs* c);
+/* Snapshot m as 3 n values (ConfigsParticleDecomp::getConf); ESPP_ERANGE if m is outside. */
+ESPP_API int espp_confs_get(espp_confs* c, int32_t m, double* xyz);
+/* MeanSquareDispl::compute (MeanSquareDispl.cpp:42-141) over the M snapshots:
+ * out[m] = (sum_{t < M-m} sum_i |r_i(t) - r_i(t+m)|^2 / (M - m)) / (6 N), m = 0 .. M-1. */
+ESPP_API int espp_msd(espp_confs* c, double* out);
+/* MeanSquareDispl::computeG3 (MeanSquareDispl.cpp:248-430): the same over the centres of
+ * mass of chains of chainlength consecutive tracked particles, each taken relative to the
+ * mean of that snapshot's chain centres; out[m] = (sum / (6 C)) / (M - m) for C chains. */
+ESPP_API int espp_msd_chain_com(espp_confs* c, int32_t chainlength, double* out);
+
 /* Sums of the total force (the force espp_get_particles reports) by particle id, kept on
  * the device across runs and re-sorts: op 0 clears the sums, op 1 adds the current total
  * forces, op 2 copies the sums of the particles ids (3 per particle) to out.  Serves

@@ -1794,6 +1794,164 @@ int espp_virial_tensor(espp_system* s, int32_t which, double w[6]) {
 
 // RadialDistrF::computeArray (src/analysis/RadialDistrF.cpp:47-150), one rank, one
 // configuration: particles numbered in id order, all pairs i < j.
+// ---- ConfigsParticleDecomp / MeanSquareDispl (src/analysis/ConfigsParticleDecomp.cpp,
+// src/analysis/MeanSquareDispl.cpp) -----------------------------------------------------
+}  // extern "C"
+
+struct espp_confs {
+  espp_system* s = nullptr;
+  int key = 0;
+  std::vector<int64_t> ids;                       // tracked ids, ascending
+  std::vector<std::vector<double>> confs;         // per snapshot: x y z per tracked id
+};
+
+extern "C" {
+
+int espp_confs_create(espp_system* s, int32_t key, int64_t n, const int64_t* ids,
+                      espp_confs** out) {
+  CHECK_S(s);
+  if (!out) return fail(ESPP_EINVAL, "null output pointer");
+  if (key < ESPP_CONF_POSITION || key > ESPP_CONF_UNFOLDED)
+    return fail(ESPP_EINVAL, "Error. Key is unknown. Use position, unfolded or velocity.");
+  if (n < 0 || (n > 0 && !ids)) return fail(ESPP_EINVAL, "bad id list");
+  auto* c = new espp_confs();
+  c->s = s;
+  c->key = key;
+  c->ids.assign(ids, ids + n);
+  *out = c;
+  return ESPP_OK;
+}
+
+int espp_confs_destroy(espp_confs* c) {
+  delete c;
+  return ESPP_OK;
+}
+
+// ConfigsParticleDecomp::gather (ConfigsParticleDecomp.cpp:70-142): property of each id,
+// "unfolded" = pos[i] + img[i] * Li[i]
+int espp_confs_gather(espp_confs* c) {
+  if (!c) return fail(ESPP_EINVAL, "null handle");
+  espp_system* s = c->s;
+  std::vector<double> conf(3 * c->ids.size());
+  for (size_t k = 0; k < c->ids.size(); ++k) {
+    Particle* p = lookup(s, c->ids[k]);
+    if (!p) return fail(ESPP_ESTATE, "particle id outside the id map");
+    for (int i = 0; i < 3; ++i) {
+      double v;
+      if (c->key == ESPP_CONF_VELOCITY)
+        v = p->v[i];
+      else if (c->key == ESPP_CONF_UNFOLDED)
+        v = p->r[i] + p->img[i] * s->L[i];
+      else
+        v = p->r[i];
+      conf[3 * k + i] = v;
+    }
+  }
+  c->confs.push_back(std::move(conf));
+  return ESPP_OK;
+}
+
+int espp_confs_push(espp_confs* c, const double* xyz) {
+  if (!c) return fail(ESPP_EINVAL, "null handle");
+  if (!c->ids.empty() && !xyz) return fail(ESPP_EINVAL, "null argument");
+  c->confs.emplace_back(xyz, xyz + 3 * c->ids.size());
+  return ESPP_OK;
+}
+
+int espp_confs_size(espp_confs* c, int32_t* m) {
+  if (!c || !m) return fail(ESPP_EINVAL, "null argument");
+  *m = (int32_t)c->confs.size();
+  return ESPP_OK;
+}
+
+int espp_confs_clear(espp_confs* c) {
+  if (!c) return fail(ESPP_EINVAL, "null handle");
+  c->confs.clear();
+  return ESPP_OK;
+}
+
+int espp_confs_get(espp_confs* c, int32_t m, double* xyz) {
+  if (!c || !xyz) return fail(ESPP_EINVAL, "null argument");
+  if (m < 0 || m >= (int32_t)c->confs.size())
+    return fail(ESPP_ERANGE, "Error. Velocities::get <out-of-range>");
+  std::copy(c->confs[m].begin(), c->confs[m].end(), xyz);
+  return ESPP_OK;
+}
+
+// MeanSquareDispl::compute (MeanSquareDispl.cpp:42-141), one rank: Z[m] accumulates
+// delta.sqr() over n < M - m and the ids in order; then Z[m] /= (M - m); Z[m] *= 1/(6 N)
+int espp_msd(espp_confs* c, double* out) {
+  if (!c || !out) return fail(ESPP_EINVAL, "null argument");
+  const int M = (int)c->confs.size();
+  const size_t N = c->ids.size();
+  std::vector<double> Z(M, 0.0);
+  for (int m = 0; m < M; m++) {
+    Z[m] = 0.0;
+    for (int n = 0; n < M - m; n++)
+      for (size_t i = 0; i < N; ++i) {
+        const double* pos1 = &c->confs[n + m][3 * i];
+        const double* pos2 = &c->confs[n][3 * i];
+        const double d[3] = {pos2[0] - pos1[0], pos2[1] - pos1[1], pos2[2] - pos1[2]};
+        Z[m] += d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+      }
+  }
+  for (int m = 0; m < M; m++) Z[m] /= (double)(M - m);
+  const double inv_coef = 1.0 / (6.0 * (double)N);
+  for (int m = 0; m < M; m++) out[m] = Z[m] * inv_coef;
+  return ESPP_OK;
+}
+
+// MeanSquareDispl::computeG3 (MeanSquareDispl.cpp:248-430), one rank: chain centres of
+// chainlength consecutive ids, the snapshot's mean chain centre subtracted
+int espp_msd_chain_com(espp_confs* c, int32_t chainlength, double* out) {
+  if (!c || !out) return fail(ESPP_EINVAL, "null argument");
+  if (chainlength <= 0) return fail(ESPP_EINVAL, "chainlength must be positive");
+  const int M = (int)c->confs.size();
+  const size_t N = c->ids.size();
+  const int num_chains = (int)(N / chainlength);
+  if (M == 0) return ESPP_OK;
+  if (num_chains == 0) return fail(ESPP_EINVAL, "no complete chain among the tracked particles");
+  std::vector<std::vector<std::array<double, 3>>> chainCOM(M);
+  std::vector<std::array<double, 3>> sysCOM(M);
+  for (int m = 0; m < M; m++) {
+    double posCOM[3] = {0, 0, 0}, mass = 0.0, sys[3] = {0, 0, 0};
+    int part_count = 0, chain_count = 0;
+    for (size_t e = 0; e < N; ++e) {
+      const double* pos = &c->confs[m][3 * e];
+      for (int i = 0; i < 3; ++i) posCOM[i] += pos[i];
+      mass += 1;
+      part_count += 1;
+      if (part_count == chainlength) {
+        std::array<double, 3> com = {posCOM[0] / mass, posCOM[1] / mass, posCOM[2] / mass};
+        chainCOM[m].push_back(com);
+        for (int i = 0; i < 3; ++i) sys[i] += com[i];
+        chain_count += 1;
+        part_count = 0;
+        posCOM[0] = posCOM[1] = posCOM[2] = 0.0;
+        mass = 0;
+      }
+    }
+    for (int i = 0; i < 3; ++i) sysCOM[m][i] = sys[i] / chain_count;
+  }
+  std::vector<double> Z(M, 0.0);
+  for (int m = 0; m < M; m++) {
+    Z[m] = 0.0;
+    for (int n = 0; n < M - m; n++)
+      for (int cid = 0; cid < (int)chainCOM[0].size(); cid++) {
+        double d[3];
+        for (int i = 0; i < 3; ++i) {
+          const double pos1 = chainCOM[n + m][cid][i] - sysCOM[n + m][i];
+          const double pos2 = chainCOM[n][cid][i] - sysCOM[n][i];
+          d[i] = pos2 - pos1;
+        }
+        Z[m] += d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+      }
+  }
+  const double inv_coef = 1.0 / (6.0 * num_chains);
+  for (int m = 0; m < M; m++) out[m] = inv_coef * Z[m] / (double)(M - m);
+  return ESPP_OK;
+}
+
 int espp_rdf(espp_system* s, int32_t rdfN, double* out) {
   CHECK_S(s);
   if (rdfN <= 0 || !out) return fail(ESPP_EINVAL, "rdfN must be positive");

@@ -175,6 +175,78 @@ class Sim:
         call(self.lib, "espp_vl_pairs", self.h, n, i64ptr(out), ctypes.byref(got))
         return out[:got.value]
 
+    def confs(self, key, ids):
+        ids = np.ascontiguousarray(ids, np.int64)
+        h = ctypes.c_void_p()
+        call(self.lib, "espp_confs_create", self.h, int(key), len(ids), i64ptr(ids),
+             ctypes.byref(h))
+        return Confs(self.lib, h, len(ids))
+
+
+class Confs:
+    """Snapshot list (espp_confs_*) of one system, for the MSD tests."""
+
+    def __init__(self, lib, h, n):
+        self.lib, self.h, self.n = lib, h, n
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.lib.espp_confs_destroy(self.h)
+                self.h = ctypes.c_void_p()
+        except Exception:
+            pass
+
+    def gather(self):
+        call(self.lib, "espp_confs_gather", self.h)
+
+    def push(self, xyz):
+        xyz = np.ascontiguousarray(xyz, np.float64).reshape(-1)
+        call(self.lib, "espp_confs_push", self.h, dptr(xyz))
+
+    def size(self):
+        m = ctypes.c_int32()
+        call(self.lib, "espp_confs_size", self.h, ctypes.byref(m))
+        return m.value
+
+    def get(self, m):
+        out = np.zeros((self.n, 3))
+        call(self.lib, "espp_confs_get", self.h, int(m), dptr(out))
+        return out
+
+    def msd(self):
+        out = np.zeros(self.size())
+        call(self.lib, "espp_msd", self.h, dptr(out))
+        return out
+
+    def msd_chain(self, chainlength):
+        out = np.zeros(self.size())
+        call(self.lib, "espp_msd_chain_com", self.h, int(chainlength), dptr(out))
+        return out
+
+
+def msd_reference(snaps):
+    """MeanSquareDispl::compute (MeanSquareDispl.cpp:89-137) on snapshots (M, N, 3)."""
+    M, N = snaps.shape[0], snaps.shape[1]
+    out = np.zeros(M)
+    for m in range(M):
+        z = sum(np.sum((snaps[t] - snaps[t + m]) ** 2) for t in range(M - m))
+        out[m] = z / (M - m) / (6.0 * N)
+    return out
+
+
+def msd_chain_reference(snaps, chainlength):
+    """MeanSquareDispl::computeG3 (MeanSquareDispl.cpp:312-425) on snapshots (M, N, 3)."""
+    M, N = snaps.shape[0], snaps.shape[1]
+    nch = N // chainlength
+    com = snaps[:, :nch * chainlength].reshape(M, nch, chainlength, 3).mean(axis=2)
+    rel = com - com.mean(axis=1, keepdims=True)
+    out = np.zeros(M)
+    for m in range(M):
+        z = sum(np.sum((rel[t] - rel[t + m]) ** 2) for t in range(M - m))
+        out[m] = z / (6.0 * nch) / (M - m)
+    return out
+
 
 def cell_grid(box, rc, skin, half_cell_int=1):
     """tools.decomp.cellGrid (src/tools/decomp.py:322-342) for nodeGrid (1,1,1)."""

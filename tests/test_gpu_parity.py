@@ -6,7 +6,7 @@ import pytest
 
 from espressopp_b200 import _abi
 from simdriver import (Sim, cell_grid, cuda_lib, lattice, load_lj2048, load_polymer40k,
-                       mb_velocities, oracle_lib)
+                       mb_velocities, msd_chain_reference, msd_reference, oracle_lib)
 
 pytestmark = pytest.mark.gpu
 
@@ -354,6 +354,73 @@ def test_parallel_tempering_api_runs_and_exchanges():
                 assert pt._thermostat[n].temperature == before[n]
     temps = pt._multisystem.runAnalysisTemperature()
     assert all(0.05 < t < 10.0 for t in temps)
+
+
+def test_msd_matches_oracle():
+    """MeanSquareDispl::compute / computeG3 on the GPU against the oracle on the same
+    snapshots (FP64, only the summation order differs), and GPU snapshots of the same
+    Langevin run against the oracle's (ConfigsParticleDecomp.cpp:70-142)."""
+    from test_oracle import _lj2048_msd_run
+    so, co, pid, box = _lj2048_msd_run(oracle_lib())
+    sg, cg_, _, _ = _lj2048_msd_run(cuda_lib())
+    snaps_o = np.array([co.get(m) for m in range(co.size())])
+    snaps_g = np.array([cg_.get(m) for m in range(cg_.size())])
+    assert snaps_g.shape == snaps_o.shape
+    assert np.max(np.abs(snaps_g - snaps_o)) < 1e-8
+    # the same snapshots pushed into a GPU list: only the reduction order differs
+    pg = sg.confs(_abi.CONF_UNFOLDED, pid)
+    for m in range(len(snaps_o)):
+        pg.push(snaps_o[m])
+    assert np.allclose(pg.msd(), co.msd(), rtol=1e-12, atol=0)
+    for L in (1, 16, 100):
+        assert np.allclose(pg.msd_chain(L), co.msd_chain(L), rtol=1e-10, atol=1e-15)
+    assert np.allclose(cg_.msd(), co.msd(), rtol=1e-6)
+    pos, vel, _, img = sg.particles(pid)
+    cg_.gather()
+    assert np.array_equal(cg_.get(cg_.size() - 1), pos + img * np.asarray(box))
+    cv = sg.confs(_abi.CONF_VELOCITY, pid)
+    cv.gather()
+    assert np.array_equal(cv.get(0), vel)
+    bad = sg.confs(_abi.CONF_POSITION, np.array([10 ** 6], np.int64))
+    with pytest.raises(RuntimeError, match="id"):
+        bad.gather()
+
+
+def test_msd_python_api():
+    """analysis.MeanSquareDispl through the Python mirror on a small LJ fluid."""
+    import espressopp_b200 as espressopp
+    x, y, z, Lx, Ly, Lz = espressopp.tools.lattice.createCubic(1000, 0.8442, perfect=False)
+    system = espressopp.System()
+    system.rng = espressopp.esutil.RNG(5)
+    system.bc = espressopp.bc.OrthorhombicBC(system.rng, (Lx, Ly, Lz))
+    system.skin = 0.3
+    cgrid = espressopp.tools.decomp.cellGrid((Lx, Ly, Lz), (1, 1, 1), 2.5, 0.3)
+    system.storage = espressopp.storage.DomainDecomposition(system, (1, 1, 1), cgrid)
+    system.storage.addParticles([[k, espressopp.Real3D(x[k], y[k], z[k])]
+                                 for k in range(len(x))], "id", "pos")
+    system.storage.decompose()
+    vl = espressopp.VerletList(system, cutoff=2.5)
+    lj = espressopp.interaction.VerletListLennardJones(vl)
+    lj.setPotential(0, 0, espressopp.interaction.LennardJones(1.0, 1.0, 2.5))
+    system.addInteraction(lj)
+    integ = espressopp.integrator.VelocityVerlet(system)
+    integ.dt = 0.005
+    lang = espressopp.integrator.LangevinThermostat(system)
+    lang.gamma = 1.0
+    lang.temperature = 1.0
+    integ.addExtension(lang)
+    msd = espressopp.analysis.MeanSquareDispl(system, chainlength=10)
+    for _ in range(5):
+        msd.gather()
+        integ.run(20)
+    assert msd.size == 5
+    snaps = np.array([[msd[m].getCoordinates(pid) for pid in range(1000)] for m in range(5)])
+    got = msd.compute()
+    assert np.allclose(got, msd_reference(snaps), rtol=1e-12, atol=0)
+    assert np.allclose(msd.computeG3(), msd_chain_reference(snaps, 10), rtol=1e-10, atol=1e-15)
+    assert msd.computeG2() == []
+    msd.clear()
+    assert msd.size == 0
 
 
 @pytest.mark.parametrize("rdfN", [100, 1000, 20000])

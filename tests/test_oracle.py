@@ -19,7 +19,7 @@ import pytest
 
 from espressopp_b200 import _abi
 from simdriver import (Sim, cell_grid, lattice, load_lj2048, load_polymer40k, mb_velocities,
-                       oracle_lib)
+                       msd_chain_reference, msd_reference, oracle_lib)
 
 
 def _lj(eps, sig, rc, shift, d, caprad=0.0):
@@ -220,6 +220,49 @@ def test_rdf_of_lj_fluid_is_normalised():
     assert np.all(g[r < 0.8] == 0.0)
     assert 1.0 < r[np.argmax(g)] < 1.25 and g.max() > 2.0
     assert abs(np.mean(g[(r > 4.5) & (r < 6.5)]) - 1.0) < 0.05
+
+
+def _lj2048_msd_run(lib, prec=_abi.PREC_FP64, nsnap=6, every=20, key=_abi.CONF_UNFOLDED):
+    pid, pos, vel, box = load_lj2048()
+    s = Sim(lib, box, 0.3, cell_grid(box, 2.5, 0.3), precision=prec, seed=11)
+    s.add(pid, pos, vel)
+    s.decompose()
+    s.vl(2.5)
+    s.lj(0, 0, 1.0, 1.0, 2.5, 4.0 * (2.5 ** -12 - 2.5 ** -6))
+    s.integrator(0.005)
+    s.langevin(1.0, 1.0)
+    c = s.confs(key, pid)
+    for _ in range(nsnap):
+        c.gather()
+        s.run(every)
+    return s, c, pid, box
+
+
+def test_msd_oracle_matches_direct_evaluation():
+    """MeanSquareDispl::compute / computeG3 of the oracle against a direct numpy evaluation
+    of the reference's sums on the same snapshots, and the "unfolded" key against
+    position + image * box of the same particles (ConfigsParticleDecomp.cpp:70-142)."""
+    s, c, pid, box = _lj2048_msd_run(oracle_lib())
+    assert c.size() == 6
+    snaps = np.array([c.get(m) for m in range(6)])
+    got = c.msd()
+    want = msd_reference(snaps)
+    assert got[0] == 0.0
+    assert np.allclose(got, want, rtol=1e-12, atol=0)
+    assert np.all(np.diff(got) > 0)  # displacement grows with the lag in a liquid
+    for L in (1, 16, 100):
+        assert np.allclose(c.msd_chain(L), msd_chain_reference(snaps, L), rtol=1e-10, atol=1e-15)
+    pos, _, _, img = s.particles(pid)
+    c.gather()
+    last = c.get(6)
+    assert np.array_equal(last, pos + img * np.asarray(box))
+    with pytest.raises(RuntimeError, match="out-of-range"):
+        c.get(7)
+    call = _abi.call
+    call(oracle_lib(), "espp_confs_clear", c.h)
+    assert c.size() == 0
+    c.push(snaps[2])
+    assert np.array_equal(c.get(0), snaps[2])
 
 
 def test_polymer_melt_step0_angle_energy_matches_result_dat():
