@@ -222,10 +222,30 @@ __global__ void k_scatter(DevView d, RebuildScratch s) {
   s.perm[d.cellStart[s.cellOf[i]] + s.slot[i]] = i;
 }
 
-// Order inside a cell: by particle id, so the layout is independent of the atomic
-// arrival order above.  One warp per cell: each lane takes one particle and its rank
-// among the cell's ids is its new slot (cells with more than 32 particles are sorted
-// by insertion on lane 0).
+// Order inside a cell: by the Morton code of the particle's 8 x 8 x 8 sub-cell, then by
+// id.  The layout is independent of the atomic arrival order above, and consecutive
+// particles (the lanes of a force warp) sit close together, so their neighbour lists
+// overlap and their coordinate gathers share cache lines.  One warp per cell: each lane
+// takes one particle and its rank among the cell's keys is its new slot (cells with
+// more than 32 particles are sorted by insertion on lane 0).
+__device__ __forceinline__ unsigned spread3(unsigned v) {  // bits b2 b1 b0 -> b2..b1..b0
+  return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4);
+}
+__device__ __forceinline__ uint64_t in_cell_key(const DevView& d, const ParticleArrays& a, int v,
+                                                int c) {
+  const int cx = c % d.nc[0], cy = (c / d.nc[0]) % d.nc[1], cz = c / (d.nc[0] * d.nc[1]);
+  const int cc[3] = {cx, cy, cz};
+  unsigned q[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const double f = (a.x[(size_t)i * d.cap + v] - cc[i] * d.cellSize[i]) * d.invCellSize[i];
+    const int b = (int)(f * 8.0);
+    q[i] = (unsigned)(b < 0 ? 0 : (b > 7 ? 7 : b));
+  }
+  const uint64_t morton = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
+  return (morton << 54) | (uint64_t)(a.id[v] - d.idMin);
+}
+
 __global__ void k_sort_in_cell(DevView d, RebuildScratch s) {
   const ParticleArrays a = d.pa[0];
   const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -236,10 +256,10 @@ __global__ void k_sort_in_cell(DevView d, RebuildScratch s) {
   if (n <= 1) return;
   if (n <= 32) {
     const int v = lane < n ? s.perm[b + lane] : 0;
-    const int64_t key = lane < n ? a.id[v] : INT64_MAX;
+    const uint64_t key = lane < n ? in_cell_key(d, a, v, c) : UINT64_MAX;
     int rank = 0;
     for (int m = 0; m < n; ++m) {
-      const int64_t km = __shfl_sync(0xffffffffu, key, m);
+      const uint64_t km = __shfl_sync(0xffffffffu, key, m);
       rank += km < key;
     }
     __syncwarp();
@@ -249,9 +269,9 @@ __global__ void k_sort_in_cell(DevView d, RebuildScratch s) {
   if (lane == 0) {
     for (int k = b + 1; k < e; ++k) {
       const int v = s.perm[k];
-      const int64_t key = a.id[v];
+      const uint64_t key = in_cell_key(d, a, v, c);
       int m = k - 1;
-      while (m >= b && a.id[s.perm[m]] > key) {
+      while (m >= b && in_cell_key(d, a, s.perm[m], c) > key) {
         s.perm[m + 1] = s.perm[m];
         --m;
       }
