@@ -858,7 +858,7 @@ def main():
     ap.add_argument("--cg-frames", type=int, default=500)
     ap.add_argument("--cg-epochs", type=int, default=15)
     ap.add_argument("--cg-steps", type=int, default=100000)
-    ap.add_argument("--cg-ibi", type=int, default=10, help="IBI iterations of the pair table")
+    ap.add_argument("--cg-ibi", type=int, default=20, help="IBI iterations of the pair table")
     ap.add_argument("--cg-window", type=int, default=50,
                     help="steps over which the mapped forces of a frame are averaged")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])

@@ -420,12 +420,15 @@ def ibi_refine(cgsys, tab, g_target, nbins, iters=10, steps=3000, every=250, alp
     """Iterative Boltzmann inversion of a pair table against a target RDF: each iteration
     runs the CG system (bonds + this pair table, thermostatted) on the GPU, samples the
     RDF, and updates U(r) += alpha T ln(g(r) / g_target(r)) (step at most alpha T, bins
-    with g > 0.02 only, tapered to zero at rc); F = -dU/dr.  Returns the refined table and
-    the RDF L2 error per iteration."""
+    with g > 0.02 only, tapered to zero at rc); F = -dU/dr.  An iteration whose RDF error
+    is larger than the best so far goes back to the best table and halves alpha, and the
+    best table is the one returned.  Returns the refined table and the RDF L2 error per
+    iteration."""
     r_t, E_t, F_t = (np.array(a, np.float64) for a in tab)
     dr = cgsys.L / 2 / nbins
     rb = (np.arange(nbins) + 0.5) * dr
     hist = []
+    best = (np.inf, E_t.copy(), None)
     for it in range(iters):
         cgsys.set_pair_table((r_t, E_t, F_t), rc)
         cgsys.run(1000)
@@ -439,7 +442,14 @@ def ibi_refine(cgsys, tab, g_target, nbins, iters=10, steps=3000, every=250, alp
         sel = rb < 2 * rc
         hist.append(float(np.sqrt(np.mean((g[sel] - g_target[sel]) ** 2))))
         if log:
-            log("IBI iteration %d: RDF L2 %.4f" % (it, hist[-1]))
+            log("IBI iteration %d: RDF L2 %.4f (alpha %.3f)" % (it, hist[-1], alpha))
+        if hist[-1] < best[0]:
+            best = (hist[-1], E_t.copy(), g.copy())
+        else:
+            # overshoot: step again from the best table with half the step
+            alpha *= 0.5
+            E_t = best[1].copy()
+            g = best[2]
         # bins with a reliable RDF only; steps of at most 0.5 T per iteration
         ok = (rb < rc) & (g > 0.02) & (g_target > 0.02)
         du = np.zeros(nbins)
@@ -450,5 +460,7 @@ def ibi_refine(cgsys, tab, g_target, nbins, iters=10, steps=3000, every=250, alp
         du *= np.clip(1.0 - (rb / rc) ** 4, 0.0, 1.0)
         E_t = E_t + np.interp(r_t, rb, du)
         F_t = -np.gradient(E_t, r_t)
+    E_t = best[1]
+    F_t = -np.gradient(E_t, r_t)
     cgsys.set_pair_table((r_t, E_t, F_t), rc)
     return (r_t, E_t, F_t), hist
