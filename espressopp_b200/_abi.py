@@ -43,6 +43,7 @@ PROTOTYPES = {
     "espp_tab_pair_set": (c_int32, [_P, c_int32, c_int32, c_int32, c_int64, _D, _D, _D,
                                     c_double, c_double]),
     "espp_tab_bond_set": (c_int32, [_P, c_int32, c_int64, _D, _D, _D, c_double, c_double]),
+    "espp_tab_angle_set": (c_int32, [_P, c_int32, c_int64, _D, _D, _D]),
     "espp_integrator_set": (c_int32, [_P, c_double]),
     "espp_step_get": (c_int32, [_P, _I64]),
     "espp_step_set": (c_int32, [_P, c_int64]),
@@ -100,6 +101,7 @@ IA_TAB_PAIR = 2
 IA_TAB_BOND = 3
 IA_MLP = 4
 IA_COSINE = 5
+IA_TAB_ANGLE = 6
 TAB_LINEAR, TAB_AKIMA, TAB_CUBIC = 1, 2, 3
 CAP_OFF, CAP_ABS, CAP_COMPONENT = 0, 1, 2
 CONF_POSITION, CONF_VELOCITY, CONF_UNFOLDED = 0, 1, 2

@@ -179,6 +179,7 @@ struct espp_system {
   int32_t* d_tabPair = nullptr;
   int tabNT = 0;
   int tabBond = -1;
+  int tabAngle = -1;
   // learned CG potential (not owned) and its per-particle scratch
   espp_mlp* mlp = nullptr;
   int mlpCap = 0;
@@ -258,6 +259,7 @@ struct espp_system {
     d.tabPair = d_tabPair;
     d.tabNT = tabNT;
     d.tabBond = tabBond;
+    d.tabAngle = tabAngle;
     d.mlp = mlp_view(mlp);
     d.mlp.G = mlpG;
     d.mlp.D = mlpD;
@@ -624,6 +626,7 @@ void upload_lj(espp_system* s) {
 }
 
 constexpr int kTabBondKey = -1;
+constexpr int kTabAngleKey = -2;
 
 // Builds every table of the system into one coefficient array and uploads it with the
 // descriptors and the type-pair map.
@@ -632,10 +635,10 @@ void upload_tabs(espp_system* s) {
   std::vector<double> coef;
   int nt = 0;
   for (auto& kv : s->tabSpecs)
-    if (kv.first != kTabBondKey) nt = std::max(nt, kv.first % kMaxTypes + 1);
+    if (kv.first >= 0) nt = std::max(nt, kv.first % kMaxTypes + 1);
   nt = nt > 0 ? std::max(nt, s->maxType + 1) : 0;
   std::vector<int32_t> pairMap((size_t)nt * nt, -1);
-  int bondIdx = -1;
+  int bondIdx = -1, angleIdx = -1;
   for (auto& kv : s->tabSpecs) {
     const espp_system::TabSpec& t = kv.second;
     TabDesc desc;
@@ -648,6 +651,8 @@ void upload_tabs(espp_system* s) {
     descs.push_back(desc);
     if (kv.first == kTabBondKey) {
       bondIdx = idx;
+    } else if (kv.first == kTabAngleKey) {
+      angleIdx = idx;
     } else {
       const int t1 = kv.first / kMaxTypes, t2 = kv.first % kMaxTypes;
       pairMap[(size_t)t1 * nt + t2] = idx;
@@ -672,6 +677,7 @@ void upload_tabs(espp_system* s) {
   }
   s->tabNT = nt;
   s->tabBond = bondIdx;
+  s->tabAngle = angleIdx;
 }
 
 // whether a pair interaction runs on the Verlet list
@@ -1262,7 +1268,10 @@ void observable(espp_system* s, int which, int energy, double out[7]) {
     launch_tab_observables(d, 1, part, nb, s->obs, energy, s->st);
   } else if (which == ESPP_IA_COSINE) {
     if (s->triples.empty() || !s->cosine.on) return;
-    launch_angle_observables(d, part, nb, s->obs, energy, s->st);
+    launch_angle_observables(d, part, nb, s->obs, energy, 0, s->st);
+  } else if (which == ESPP_IA_TAB_ANGLE) {
+    if (s->triples.empty() || s->tabAngle < 0) return;
+    launch_angle_observables(d, part, nb, s->obs, energy, 1, s->st);
   } else if (which == ESPP_IA_MLP) {
     if (!d.mlp.on) return;
     if (!energy) raise(ESPP_EINVAL, "the virial of the learned potential is not available");
@@ -1899,6 +1908,14 @@ int espp_tab_bond_set(espp_system* s, int32_t itype, int64_t n, const double* r,
   return guard([&] {
     checked(s);
     set_tab(s, kTabBondKey, itype, n, r, e, f, rc, shift);
+  });
+}
+
+int espp_tab_angle_set(espp_system* s, int32_t itype, int64_t n, const double* theta,
+                       const double* e, const double* f) {
+  return guard([&] {
+    checked(s);
+    set_tab(s, kTabAngleKey, itype, n, theta, e, f, INFINITY, 0.0);
   });
 }
 

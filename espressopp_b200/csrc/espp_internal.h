@@ -159,6 +159,7 @@ struct DevView {
   const int32_t* tabPair; // tabNT*tabNT: table of the type pair on the Verlet list, -1 none
   int tabNT;              // 0: no tabulated pair interaction
   int tabBond;            // table of the fixed pair list, -1 none
+  int tabAngle;           // TabulatedAngular table of the fixed triple list, -1 none
   MlpDev mlp;             // learned CG pair potential on the Verlet list (mlp.on)
   const int64_t* triples; // 3 * ntriples ids (p1, p2 centre, p3)
   int ntriples;
@@ -218,8 +219,9 @@ void launch_rdf(const DevView& d, int rdfN, double dr, unsigned long long* hist,
                 cudaStream_t st);
 // angular forces (per triple, then gathered per particle) added to the force output
 void launch_angle_forces(const DevView& d, bool mixed, cudaStream_t st);
+// kind 0: interaction::Cosine, 1: TabulatedAngular
 void launch_angle_observables(const DevView& d, double* partials, int nblocks, double* out,
-                              int energy, cudaStream_t st);
+                              int energy, int kind, cudaStream_t st);
 // tabulated pair and bond forces, added to the main kernel's output
 void launch_force_tab(const DevView& d, bool mixed, cudaStream_t st);
 void launch_tab_observables(const DevView& d, int bond, double* partials, int nblocks,

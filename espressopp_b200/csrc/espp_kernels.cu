@@ -1623,14 +1623,47 @@ __device__ __forceinline__ void cosine_force(const CosineParams& P, const double
 }
 
 // per triple: force12 and force32 into tripF
+// TabulatedAngular::_computeForceRaw (TabulatedAngular.hpp:88-113) in the reference's
+// operation order (no clamp of cos(theta), as there).
+__device__ __forceinline__ void tab_angle_force(const DevView& d, const double* d12,
+                                                const double* d32, double* f12, double* f32) {
+  const double d12sq = __dadd_rn(__dadd_rn(__dmul_rn(d12[0], d12[0]), __dmul_rn(d12[1], d12[1])),
+                                 __dmul_rn(d12[2], d12[2]));
+  const double d32sq = __dadd_rn(__dadd_rn(__dmul_rn(d32[0], d32[0]), __dmul_rn(d32[1], d32[1])),
+                                 __dmul_rn(d32[2], d32[2]));
+  const double d1232 = __dmul_rn(sqrt(d12sq), sqrt(d32sq));
+  const double dot = __dadd_rn(__dadd_rn(__dmul_rn(d12[0], d32[0]), __dmul_rn(d12[1], d32[1])),
+                               __dmul_rn(d12[2], d32[2]));
+  const double c = __ddiv_rn(dot, d1232);
+  double a = tab_value(d.tabs[d.tabAngle], d.tabCoef, true, acos(c));
+  a = __dmul_rn(a, __ddiv_rn(1.0, sqrt(__dsub_rn(1.0, __dmul_rn(c, c)))));
+  const double a11 = __ddiv_rn(__dmul_rn(a, c), d12sq);
+  const double a12 = __ddiv_rn(-a, d1232);
+  const double a22 = __ddiv_rn(__dmul_rn(a, c), d32sq);
+  for (int q = 0; q < 3; ++q) {
+    f12[q] = __dadd_rn(__dmul_rn(a11, d12[q]), __dmul_rn(a12, d32[q]));
+    f32[q] = __dadd_rn(__dmul_rn(a22, d32[q]), __dmul_rn(a12, d12[q]));
+  }
+}
+
+// per triple: force12, force32 of Cosine and/or TabulatedAngular (summed when both act)
 __global__ void k_angle_forces(DevView d) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= d.ntriples) return;
   double d12[3], d32[3], f12[3] = {0, 0, 0}, f32[3] = {0, 0, 0};
-  if (triple_dists(d, t, d12, d32))
-    cosine_force(d.cosine, d12, d32, f12, f32);
-  else
+  if (triple_dists(d, t, d12, d32)) {
+    if (d.cosine.on) cosine_force(d.cosine, d12, d32, f12, f32);
+    if (d.tabAngle >= 0) {
+      double g12[3], g32[3];
+      tab_angle_force(d, d12, d32, g12, g32);
+      for (int q = 0; q < 3; ++q) {
+        f12[q] = d.cosine.on ? f12[q] + g12[q] : g12[q];
+        f32[q] = d.cosine.on ? f32[q] + g32[q] : g32[q];
+      }
+    }
+  } else {
     atomicOr(d.err, kErrBondMissing);
+  }
   for (int q = 0; q < 3; ++q) {
     d.tripF[6 * (size_t)t + q] = f12[q];
     d.tripF[6 * (size_t)t + 3 + q] = f32[q];
@@ -1662,8 +1695,9 @@ __global__ void k_angle_gather(DevView d) {
 }
 
 // Energy (FixedTripleListInteractionTemplate::computeEnergy :205-275: minimum image by
-// rounding, theta = acos(cos), Cosine::_computeEnergyRaw) or virial d12.f12 + d32.f32.
-__global__ void k_angle_obs(DevView d, int energy, double* partials) {
+// rounding, theta = acos(cos), then Cosine::_computeEnergyRaw (kind 0) or the table's
+// getEnergy (kind 1)) or virial d12.f12 + d32.f32.
+__global__ void k_angle_obs(DevView d, int energy, int kind, double* partials) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   if (t < d.ntriples) {
@@ -1686,10 +1720,14 @@ __global__ void k_angle_obs(DevView d, int energy, double* partials) {
         const double s32 = d32[0] * d32[0] + d32[1] * d32[1] + d32[2] * d32[2];
         const double cth = (d12[0] * d32[0] + d12[1] * d32[1] + d12[2] * d32[2]) /
                            (sqrt(s12) * sqrt(s32));
-        acc[0] = d.cosine.K * (1.0 + cos(acos(cth) - d.cosine.theta0));
+        acc[0] = kind == 0 ? d.cosine.K * (1.0 + cos(acos(cth) - d.cosine.theta0))
+                           : tab_value(d.tabs[d.tabAngle], d.tabCoef, false, acos(cth));
       } else {
         double f12[3], f32[3];
-        cosine_force(d.cosine, d12, d32, f12, f32);
+        if (kind == 0)
+          cosine_force(d.cosine, d12, d32, f12, f32);
+        else
+          tab_angle_force(d, d12, d32, f12, f32);
         acc[0] = d12[0] * f12[0] + d12[1] * f12[1] + d12[2] * f12[2] + d32[0] * f32[0] +
                  d32[1] * f32[1] + d32[2] * f32[2];
         acc[1] = d12[0] * f12[0] + d32[0] * f32[0];
@@ -2069,7 +2107,7 @@ void launch_rdf(const DevView& d, int rdfN, double dr, unsigned long long* hist,
 }
 
 void launch_angle_forces(const DevView& d, bool mixed, cudaStream_t st) {
-  if (d.n == 0 || d.ntriples == 0 || !d.cosine.on) return;
+  if (d.n == 0 || d.ntriples == 0 || (!d.cosine.on && d.tabAngle < 0)) return;
   k_angle_forces<<<blocks_for(d.ntriples), kBlock, 0, st>>>(d);
   if (mixed)
     k_angle_gather<true><<<blocks_for(d.n), kBlock, 0, st>>>(d);
@@ -2078,8 +2116,8 @@ void launch_angle_forces(const DevView& d, bool mixed, cudaStream_t st) {
 }
 
 void launch_angle_observables(const DevView& d, double* partials, int nblocks, double* out,
-                              int energy, cudaStream_t st) {
-  k_angle_obs<<<nblocks, kBlock, 0, st>>>(d, energy, partials);
+                              int energy, int kind, cudaStream_t st) {
+  k_angle_obs<<<nblocks, kBlock, 0, st>>>(d, energy, kind, partials);
   k_sum_partials<7><<<1, 256, 0, st>>>(partials, nblocks, out);
 }
 

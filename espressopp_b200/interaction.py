@@ -473,3 +473,54 @@ class FixedTripleListCosine(Interaction):
         st = self._handle()
         if self._pot is not None:
             call(st._lib, "espp_cosine_set", st._h, self._pot.K, self._pot.theta0)
+
+
+class TabulatedAngular(Tabulated):
+    """interaction.TabulatedAngular(itype, filename, cutoff=infinity) (TabulatedAngular.py,
+    TabulatedAngular.hpp:36-113, TabulatedAngular.cpp:40-64): E(theta) and f = -dE/dtheta
+    interpolated from a table file of (theta, energy, force) lines; itype 1 linear, 2 Akima,
+    3 cubic spline."""
+
+    def computeEnergy(self, theta):
+        return self._eval(float(theta), False)
+
+    def computeForce(self, theta):
+        return self._eval(float(theta), True)
+
+
+class FixedTripleListTabulatedAngular(Interaction):
+    """interaction.FixedTripleListTabulatedAngular(system, ftl, potential)
+    (TabulatedAngular.cpp:82-88, FixedTripleListInteractionTemplate.hpp:46-333)."""
+
+    kind = _abi.IA_TAB_ANGLE
+
+    def __init__(self, system, ftl, potential=None):
+        Interaction.__init__(self)
+        self._ftl = ftl
+        self._pot = potential
+        self._pending_system = system
+
+    def setPotential(self, potential):
+        self._pot = potential
+        if self._system is not None:
+            self._push()
+
+    def getPotential(self):
+        return self._pot
+
+    def setFixedTripleList(self, ftl):
+        self._ftl = ftl
+
+    def getFixedTripleList(self):
+        return self._ftl
+
+    def getMaxCutoff(self):
+        return 0.0
+
+    def bondType(self):
+        return 3  # Angular
+
+    def _push(self):
+        st = self._handle()
+        if self._pot is not None:
+            call(st._lib, "espp_tab_angle_set", st._h, *self._pot._table())

@@ -55,6 +55,7 @@ typedef struct espp_system espp_system;
 #define ESPP_IA_TAB_BOND 3 /* FixedPairListTabulated */
 #define ESPP_IA_MLP 4      /* learned coarse-grained pair potential (espp_mlp_*) */
 #define ESPP_IA_COSINE 5   /* FixedTripleListCosine */
+#define ESPP_IA_TAB_ANGLE 6 /* FixedTripleListTabulatedAngular */
 
 /* interpolation types of interaction::Tabulated (src/interaction/Tabulated.cpp:49-67) */
 #define ESPP_TAB_LINEAR 1
@@ -167,6 +168,14 @@ ESPP_API int espp_tab_pair_set(espp_system* s, int32_t type1, int32_t type2, int
  * interact through the table (in addition to FENE when that is set too). */
 ESPP_API int espp_tab_bond_set(espp_system* s, int32_t itype, int64_t n, const double* r,
                                const double* e, const double* f, double cutoff, double shift);
+/* FixedTripleListTabulatedAngular(system, ftl, TabulatedAngular(itype, table))
+ * (src/interaction/TabulatedAngular.hpp:75-113): the triples of the system's fixed triple
+ * list interact through E(theta) of the table (theta in radians, f = -dE/dtheta), with
+ * force12 = a11 d12 + a12 d32, force32 = a22 d32 + a12 d12, a = f(acos c) / sqrt(1 - c^2),
+ * a11 = a c / |d12|^2, a12 = -a / (|d12| |d32|), a22 = a c / |d32|^2.  Replaces an
+ * earlier angle table; acts in addition to interaction::Cosine when that is set too. */
+ESPP_API int espp_tab_angle_set(espp_system* s, int32_t itype, int64_t n, const double* theta,
+                                const double* e, const double* f);
 
 /* ---- integrator::VelocityVerlet + extensions ---------------------------------------
  * MDIntegrator::setTimeStep (src/integrator/MDIntegrator.cpp:53-60). */

@@ -380,6 +380,7 @@ struct espp_system {
   std::map<std::pair<int, int>, TabPot> tabPair;
   bool tabBondOn = false;
   TabPot tabBond;
+  std::shared_ptr<Interp> tabAngle;  // TabulatedAngular of the fixed triple list
 
   // integrator
   double dt = 0.005;
@@ -745,6 +746,24 @@ void cosineForce(const espp_system* s, const double d12[3], const double d32[3],
   }
 }
 
+// TabulatedAngular::_computeForceRaw (src/interaction/TabulatedAngular.hpp:88-113).
+void tabAngleForce(const espp_system* s, const double d12[3], const double d32[3],
+                   double f12[3], double f32[3]) {
+  double dist12_sqr = d12[0] * d12[0] + d12[1] * d12[1] + d12[2] * d12[2];
+  double dist32_sqr = d32[0] * d32[0] + d32[1] * d32[1] + d32[2] * d32[2];
+  double dist1232 = std::sqrt(dist12_sqr) * std::sqrt(dist32_sqr);
+  double cos_theta = (d12[0] * d32[0] + d12[1] * d32[1] + d12[2] * d32[2]) / dist1232;
+  double a = s->tabAngle->eval(std::acos(cos_theta), true);
+  a *= 1.0 / (std::sqrt(1.0 - cos_theta * cos_theta));
+  double a11 = a * cos_theta / dist12_sqr;
+  double a12 = -a / dist1232;
+  double a22 = a * cos_theta / dist32_sqr;
+  for (int k = 0; k < 3; ++k) {
+    f12[k] = a11 * d12[k] + a12 * d32[k];
+    f32[k] = a22 * d32[k] + a12 * d12[k];
+  }
+}
+
 // FENE::_computeForceRaw / _computeEnergySqrRaw (src/interaction/FENE.hpp:91-112).
 bool feneForce(const espp_system* s, const double d[3], double f[3]) {
   double distSqr = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
@@ -1020,8 +1039,10 @@ void updateForces(espp_system* s) {
         }
     }
   }
-  // FixedTripleListCosine (FixedTripleListInteractionTemplate::addForces :183-201)
-  if (s->cos_on) {
+  // FixedTripleListCosine / FixedTripleListTabulatedAngular
+  // (FixedTripleListInteractionTemplate::addForces :183-201), one interaction after the other
+  for (int kind = 0; kind < 2; ++kind) {
+    if (kind == 0 ? !s->cos_on : !s->tabAngle) continue;
     for (auto& tr : s->triplesGlobal) {
       Particle* p1 = lookup(s, tr[0]);
       Particle* p2 = lookup(s, tr[1]);
@@ -1030,7 +1051,10 @@ void updateForces(espp_system* s) {
       double d12[3], d32[3], f12[3], f32[3];
       minImageBox(s, p1->r, p2->r, d12);
       minImageBox(s, p3->r, p2->r, d32);
-      cosineForce(s, d12, d32, f12, f32);
+      if (kind == 0)
+        cosineForce(s, d12, d32, f12, f32);
+      else
+        tabAngleForce(s, d12, d32, f12, f32);
       for (int k = 0; k < 3; ++k) {
         p1->f[k] += f12[k];
         p2->f[k] -= f12[k] + f32[k];
@@ -1468,6 +1492,17 @@ int espp_tab_bond_set(espp_system* s, int32_t itype, int64_t n, const double* r,
   return ESPP_OK;
 }
 
+int espp_tab_angle_set(espp_system* s, int32_t itype, int64_t n, const double* theta,
+                       const double* e, const double* f) {
+  CHECK_S(s);
+  if (!theta || !e || !f) return fail(ESPP_EINVAL, "null table");
+  auto t = std::make_shared<Interp>();
+  std::string msg = t->build(itype, (int)n, theta, e, f);
+  if (!msg.empty()) return fail(ESPP_EINVAL, msg);
+  s->tabAngle = t;
+  return ESPP_OK;
+}
+
 int espp_integrator_set(espp_system* s, double dt) {
   CHECK_S(s);
   if (dt == 0.0) return fail(ESPP_EINVAL, "Timestep 'dt' must be non-zero!");
@@ -1697,6 +1732,22 @@ int espp_energy(espp_system* s, int32_t which, double* e) {
                    (std::sqrt(s12) * std::sqrt(s32));
         es += s->cK * (1.0 + std::cos(std::acos(c) - s->cTheta0));
       }
+  } else if (which == ESPP_IA_TAB_ANGLE) {
+    if (s->tabAngle)
+      for (auto& tr : s->triplesGlobal) {
+        Particle* p1 = lookup(s, tr[0]);
+        Particle* p2 = lookup(s, tr[1]);
+        Particle* p3 = lookup(s, tr[2]);
+        if (!p1 || !p2 || !p3) continue;
+        double d12[3], d32[3];
+        minImageRound(s, p1->r, p2->r, d12);
+        minImageRound(s, p3->r, p2->r, d32);
+        double s12 = d12[0] * d12[0] + d12[1] * d12[1] + d12[2] * d12[2];
+        double s32 = d32[0] * d32[0] + d32[1] * d32[1] + d32[2] * d32[2];
+        double c = (d12[0] * d32[0] + d12[1] * d32[1] + d12[2] * d32[2]) /
+                   (std::sqrt(s12) * std::sqrt(s32));
+        es += s->tabAngle->eval(std::acos(c), false);
+      }
   } else if (which == ESPP_IA_MLP) {
     if (s->mlp && s->has_vl) {
       ghostComm(s, true, false);
@@ -1751,6 +1802,20 @@ static int virialImpl(espp_system* s, int32_t which, double* wsc, double w6[6]) 
         minImageBox(s, p1->r, p2->r, d12);
         minImageBox(s, p3->r, p2->r, d32);
         cosineForce(s, d12, d32, f12, f32);
+        acc(d12, f12);
+        acc(d32, f32);
+      }
+  } else if (which == ESPP_IA_TAB_ANGLE) {
+    if (s->tabAngle)
+      for (auto& tr : s->triplesGlobal) {
+        Particle* p1 = lookup(s, tr[0]);
+        Particle* p2 = lookup(s, tr[1]);
+        Particle* p3 = lookup(s, tr[2]);
+        if (!p1 || !p2 || !p3) continue;
+        double d12[3], d32[3], f12[3], f32[3];
+        minImageBox(s, p1->r, p2->r, d12);
+        minImageBox(s, p3->r, p2->r, d32);
+        tabAngleForce(s, d12, d32, f12, f32);
         acc(d12, f12);
         acc(d32, f32);
       }

@@ -101,6 +101,11 @@ class Sim:
     def cosine(self, K=1.5, theta0=3.1415926):
         call(self.lib, "espp_cosine_set", self.h, K, theta0)
 
+    def tab_angle(self, itype, theta, e, f):
+        th, ee, ff = (np.ascontiguousarray(a, np.float64) for a in (theta, e, f))
+        call(self.lib, "espp_tab_angle_set", self.h, int(itype), len(th), dptr(th), dptr(ee),
+             dptr(ff))
+
     def integrator(self, dt):
         call(self.lib, "espp_integrator_set", self.h, float(dt))
 
@@ -223,6 +228,12 @@ class Confs:
         out = np.zeros(self.size())
         call(self.lib, "espp_msd_chain_com", self.h, int(chainlength), dptr(out))
         return out
+
+
+def cosine_angle_table(K=1.5, theta0=3.1415926, n=4001):
+    """E(theta) = K (1 + cos(theta - theta0)) and f = -dE/dtheta on [0, pi]."""
+    th = np.linspace(0.0, math.pi, n)
+    return th, K * (1.0 + np.cos(th - theta0)), K * np.sin(th - theta0)
 
 
 def msd_reference(snaps):

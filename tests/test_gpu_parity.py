@@ -5,8 +5,9 @@ import numpy as np
 import pytest
 
 from espressopp_b200 import _abi
-from simdriver import (Sim, cell_grid, cuda_lib, lattice, load_lj2048, load_polymer40k,
-                       mb_velocities, msd_chain_reference, msd_reference, oracle_lib)
+from simdriver import (Sim, cell_grid, cosine_angle_table, cuda_lib, lattice, load_lj2048,
+                       load_polymer40k, mb_velocities, msd_chain_reference, msd_reference,
+                       oracle_lib)
 
 pytestmark = pytest.mark.gpu
 
@@ -354,6 +355,42 @@ def test_parallel_tempering_api_runs_and_exchanges():
                 assert pt._thermostat[n].temperature == before[n]
     temps = pt._multisystem.runAnalysisTemperature()
     assert all(0.05 < t < 10.0 for t in temps)
+
+
+@pytest.mark.parametrize("prec", [_abi.PREC_FP64, _abi.PREC_MIXED])
+def test_tabulated_angular_matches_oracle(prec, tmp_path):
+    """FixedTripleListTabulatedAngular on the 40 000-bead melt (an Akima table of a bent
+    angle potential, with Cosine acting too): energy, virial and forces against the oracle,
+    then a short Langevin run; the Python classes read the same table from a file."""
+    from test_oracle import _melt_with_angles
+    th = np.linspace(0.0, math.pi, 181)
+    e = 2.0 * (np.cos(th) - np.cos(2.0)) ** 2
+    f = 4.0 * (np.cos(th) - np.cos(2.0)) * np.sin(th)
+    sims = [_melt_with_angles(lib, p, cosine=True, table=(2, th, e, f))[0]
+            for lib, p in ((oracle_lib(), _abi.PREC_FP64), (cuda_lib(), prec))]
+    o, g = sims
+    ids = np.arange(1, 40001)
+    eo = o.energy(_abi.IA_TAB_ANGLE)
+    assert abs(g.energy(_abi.IA_TAB_ANGLE) - eo) < 1e-9 * abs(eo)
+    wo = o.virial(_abi.IA_TAB_ANGLE)
+    assert abs(g.virial(_abi.IA_TAB_ANGLE) - wo) < 1e-9 * abs(eo)
+    for s in sims:
+        s.run(0)
+    tol = 1e-12 if prec == _abi.PREC_FP64 else 1e-5
+    assert _rel_rms(g.particles(ids)[2], o.particles(ids)[2]) < tol
+    for s in sims:
+        s.langevin(1.0, 1.0)
+        s.run(20)
+    assert np.max(np.abs(g.particles(ids)[0] - o.particles(ids)[0])) < (
+        1e-9 if prec == _abi.PREC_FP64 else 1e-4)
+    import espressopp_b200 as espressopp
+    path = tmp_path / "angle.tab"
+    with open(path, "w") as fh:
+        for a, b, c in zip(th, e, f):
+            fh.write("%.17g %.17g %.17g\n" % (a, b, c))
+    pot = espressopp.interaction.TabulatedAngular(2, str(path))
+    assert pot.computeEnergy(1.3) == pytest.approx(2.0 * (math.cos(1.3) - math.cos(2.0)) ** 2,
+                                                   rel=1e-3)
 
 
 def test_msd_matches_oracle():

@@ -18,8 +18,8 @@ import numpy as np
 import pytest
 
 from espressopp_b200 import _abi
-from simdriver import (Sim, cell_grid, lattice, load_lj2048, load_polymer40k, mb_velocities,
-                       msd_chain_reference, msd_reference, oracle_lib)
+from simdriver import (Sim, cell_grid, cosine_angle_table, lattice, load_lj2048, load_polymer40k,
+                       mb_velocities, msd_chain_reference, msd_reference, oracle_lib)
 
 
 def _lj(eps, sig, rc, shift, d, caprad=0.0):
@@ -220,6 +220,46 @@ def test_rdf_of_lj_fluid_is_normalised():
     assert np.all(g[r < 0.8] == 0.0)
     assert 1.0 < r[np.argmax(g)] < 1.25 and g.max() > 2.0
     assert abs(np.mean(g[(r > 4.5) & (r < 6.5)]) - 1.0) < 0.05
+
+
+def _melt_with_angles(lib, prec=_abi.PREC_FP64, cosine=True, table=None):
+    pos, bonds, box, gold, angles = load_polymer40k(angles=True)
+    ids = np.arange(1, len(pos) + 1)
+    s = Sim(lib, box, 0.3, cell_grid(box, 1.12, 0.3), precision=prec, seed=3)
+    s.add(ids, pos)
+    s.decompose()
+    s.vl(1.42)
+    s.lj(0, 0, 1.0, 1.0, 1.12, 0.0)
+    s.bonds(bonds)
+    s.fene(30.0, 0.0, 1.5)
+    s.triples(angles)
+    if cosine:
+        s.cosine(1.5, 3.1415926)
+    if table is not None:
+        s.tab_angle(*table)
+    s.integrator(0.002)
+    return s, ids
+
+
+def test_tabulated_angular_reproduces_cosine():
+    """TabulatedAngular (TabulatedAngular.hpp:75-113) with a cubic table of the Cosine
+    potential gives Cosine's energy, virial and forces on the 40 000 angles of the melt to
+    the interpolation accuracy; both together add up."""
+    c, ids = _melt_with_angles(oracle_lib(), cosine=True)
+    t, _ = _melt_with_angles(oracle_lib(), cosine=False, table=(3,) + cosine_angle_table())
+    both, _ = _melt_with_angles(oracle_lib(), cosine=True, table=(3,) + cosine_angle_table())
+    ec, et = c.energy(_abi.IA_COSINE), t.energy(_abi.IA_TAB_ANGLE)
+    assert abs(et - ec) < 1e-9 * abs(ec)
+    assert abs(t.virial(_abi.IA_TAB_ANGLE) - c.virial(_abi.IA_COSINE)) < 1e-6 * abs(ec)
+    for s in (c, t, both):
+        s.run(0)
+    fc, ft, fb = c.particles(ids)[2], t.particles(ids)[2], both.particles(ids)[2]
+    assert np.max(np.abs(ft - fc)) < 1e-6 * np.max(np.abs(fc))
+    # with both interactions the angle part of the force is twice the Cosine one
+    base, _ = _melt_with_angles(oracle_lib(), cosine=False)
+    base.run(0)
+    fn = base.particles(ids)[2]
+    assert np.max(np.abs((fb - fn) - 2 * (fc - fn))) < 1e-6 * np.max(np.abs(fc - fn))
 
 
 def _lj2048_msd_run(lib, prec=_abi.PREC_FP64, nsnap=6, every=20, key=_abi.CONF_UNFOLDED):
