@@ -540,8 +540,11 @@ def cg_arm(args, rank, world, local_rank):
     log("fine-grained frames: %d x %d sites in %.1f s" % (nfr, pos.shape[1], t_fg))
     ntrain = int(0.8 * nfr)
     tab = cg.boltzmann_bond_table(cg.bond_lengths(pos, bonds))
-    # non-bonded target: mapped force minus the CG bond force
+    triples = cg.angle_triples(bonds)
+    atab = cg.boltzmann_angle_table(cg.angles_of(pos[:ntrain], triples))
+    # non-bonded target: mapped force minus the CG bond and angle forces
     bondsys = cg.CGSystem(pos[0], L, bonds, tab)
+    bondsys.set_angle_table(triples, atab)
     fbond_test = np.zeros((nfr - ntrain,) + pos.shape[1:])
     for k in range(nfr):
         fb = bondsys.forces_at(pos[k])
@@ -551,19 +554,25 @@ def cg_arm(args, rank, world, local_rank):
     bondsys.close()
     target = frc
     t1 = time.perf_counter()
-    ptab = cg.pair_fm_table(pos[:min(ntrain, 10)], target[:min(ntrain, 10)], L)
-    tabsys = cg.CGSystem(pos[0], L, bonds, tab)
+    # non-bonded terms act between sites that are not bonded to each other (excluding the
+    # 1-3 pairs as well measured worse: RDF L2 0.034 against 0.024)
+    excl = np.asarray(bonds, np.int64).reshape(-1, 2)
+    ptab = cg.pair_fm_table(pos[:min(ntrain, 10)], target[:min(ntrain, 10)], L, exclude=excl)
+    tabsys = cg.CGSystem(pos[0], L, bonds, tab, exclude=excl)
+    tabsys.set_angle_table(triples, atab)
     tabsys.set_pair_table(ptab)
     err_table = cg.fm_error(tabsys, pos[ntrain:], target[ntrain:], fbond_test)
     t_tab = time.perf_counter() - t1
     # the learned potential corrects the force-matched pair table: trained on the residual
-    pairsys = cg.CGSystem(pos[0], L, bonds, ([0.5, 1.0, 1.5, 2.0], [0.0] * 4, [0.0] * 4))
+    pairsys = cg.CGSystem(pos[0], L, bonds, ([0.5, 1.0, 1.5, 2.0], [0.0] * 4, [0.0] * 4),
+                          exclude=excl)
     pairsys.set_pair_table(ptab)
     resid = np.empty((ntrain,) + target.shape[1:])
     for k in range(ntrain):
         resid[k] = target[k] - pairsys.forces_at(pos[k])
     pairsys.close()
-    s = cg.CGSystem(pos[0], L, bonds, tab)
+    s = cg.CGSystem(pos[0], L, bonds, tab, exclude=excl)
+    s.set_angle_table(triples, atab)
     s.set_pair_table(ptab)
     model = cg.MLPModel(seed=3)
     s.attach(model)

@@ -209,17 +209,75 @@ def boltzmann_bond_table(lengths, T=1.0, n=400, rmin=0.05, rmax=8.0, path=None):
     return r, U, F
 
 
-def pair_fm_table(frames_pos, frames_f, L, rc=3.0, nknots=50, wall=100.0, path=None):
+def angle_triples(cg_bonds):
+    """Triples (a, b, c) of consecutive sites of a chain: bonds (a, b) and (b, c)."""
+    bs = {(int(a), int(b)) for a, b in np.asarray(cg_bonds).reshape(-1, 2)}
+    return np.array([(a, b, b + 1) for a, b in sorted(bs) if b == a + 1 and (b, b + 1) in bs],
+                    np.int64).reshape(-1, 3)
+
+
+def angles_of(pos_unwrapped, triples):
+    """Bending angles theta (radians) of the triples in every frame (frames, N, 3)."""
+    p = np.asarray(pos_unwrapped)
+    t = np.asarray(triples) - 1
+    d12 = p[:, t[:, 0]] - p[:, t[:, 1]]
+    d32 = p[:, t[:, 2]] - p[:, t[:, 1]]
+    c = np.sum(d12 * d32, -1) / np.sqrt(np.sum(d12 * d12, -1) * np.sum(d32 * d32, -1))
+    return np.arccos(np.clip(c, -1.0, 1.0)).reshape(-1)
+
+
+def boltzmann_angle_table(thetas, T=1.0, n=721, nbins=90, stiff=20.0, path=None):
+    """Angle potential U(theta) = -T ln(P(theta) / sin(theta)) from the angle histogram,
+    smoothed; below the sampled range a stiff quadratic wall, and near theta = pi the
+    quadratic through the last sampled bins, so that U is flat at pi and the tabulated
+    angular force f / sin(theta) stays finite there.  Returns (theta, E, f = -dE/dtheta)."""
+    hist, edges = np.histogram(thetas, bins=nbins, range=(0.0, math.pi), density=True)
+    tc = 0.5 * (edges[1:] + edges[:-1])
+    ok = hist > 0.002 * hist.max()
+    u = np.full(nbins, np.nan)
+    u[ok] = -T * np.log(hist[ok] / np.sin(tc[ok]))
+    first = int(np.argmax(ok))
+    th = np.linspace(0.0, math.pi, n)
+    U = np.interp(th, tc[ok], u[ok])
+    lo = tc[first]
+    U = np.where(th < lo, U[np.searchsorted(th, lo)] + stiff * (lo - th) ** 2, U)
+    # flat at pi: even quadratic in (pi - theta) fitted to the last sampled bins
+    tail = ok & (tc > math.pi - 0.6)
+    if np.count_nonzero(tail) >= 3:
+        x = (math.pi - tc[tail]) ** 2
+        c1, c0 = np.polyfit(x, u[tail], 1)
+        near = th > math.pi - 0.3
+        w = np.clip((th - (math.pi - 0.3)) / 0.3, 0.0, 1.0)
+        U = np.where(near, (1 - w) * U + w * (c0 + c1 * (math.pi - th) ** 2), U)
+    U = np.convolve(np.pad(U, 4, mode="edge"), np.ones(9) / 9, mode="valid")
+    U -= U.min()
+    F = -np.gradient(U, th)
+    F[-1] = 0.0
+    if path:
+        write_table(path, th, U, F)
+    return th, U, F
+
+
+def pair_fm_table(frames_pos, frames_f, L, rc=3.0, nknots=50, wall=100.0, path=None,
+                  exclude=None):
     """Force-matched radial pair force f(r): hat functions on nknots points from the
     closest sampled separation to rc, fitted by regularised linear least squares to the
-    target forces; below the sampled range a repulsive wall (slope `wall`).
-    The fallback of the learned potential, and its prior.  Returns the table (r, E, F)
-    with E = integral of f from r to rc."""
+    target forces; below the sampled range a repulsive wall (slope `wall`).  Pairs of
+    `exclude` (site id pairs, e.g. the bonds) take no part.  The fallback of the learned
+    potential, and its prior.  Returns the table (r, E, F) with E = integral of f from r
+    to rc."""
     from scipy.spatial import cKDTree
+    ex = None
+    if exclude is not None and len(exclude):
+        e = np.sort(np.asarray(exclude, np.int64).reshape(-1, 2) - 1, axis=1)
+        ex = set(map(tuple, e.tolist()))
     pair_sets = []
     for pos in frames_pos:
         p = wrap(pos, L)
         pairs = cKDTree(p, boxsize=L).query_pairs(rc, output_type="ndarray")
+        if ex is not None:
+            keep = np.array([(int(a), int(b)) not in ex for a, b in pairs], bool)
+            pairs = pairs[keep]
         d = p[pairs[:, 0]] - p[pairs[:, 1]]
         d -= L * np.round(d / L)
         pair_sets.append((pairs, d, np.sqrt(np.sum(d * d, 1))))
@@ -260,12 +318,16 @@ class CGSystem(Handle):
     potential or the pair-table fallback on a Verlet list of cutoff rc."""
 
     def __init__(self, pos, L, cg_bonds, bond_tab, mass=4.0, rc=3.0, precision=_abi.PREC_MIXED,
-                 seed=5, lib=None):
+                 seed=5, lib=None, exclude=None):
         Handle.__init__(self, [L, L, L], SKIN, rc, precision, seed=seed, lib=lib)
         self.L = L
         self.ids = np.arange(1, len(pos) + 1, dtype=np.int64)
         self.add(self.ids, wrap(pos, L), mass=mass)
-        call(self.lib, "espp_vl_create", self.h, rc, 0, None)
+        if exclude is not None and len(exclude):
+            ex = np.ascontiguousarray(exclude, np.int64).reshape(-1)
+            call(self.lib, "espp_vl_create", self.h, rc, len(ex) // 2, i64ptr(ex))
+        else:
+            call(self.lib, "espp_vl_create", self.h, rc, 0, None)
         b = np.ascontiguousarray(cg_bonds, np.int64).reshape(-1)
         call(self.lib, "espp_bonds_add", self.h, len(b) // 2, i64ptr(b))
         self.set_bond_table(bond_tab)
@@ -276,6 +338,13 @@ class CGSystem(Handle):
         r, e, f = (np.ascontiguousarray(a, np.float64) for a in tab)
         call(self.lib, "espp_tab_bond_set", self.h, 1, len(r), dptr(r), dptr(e), dptr(f),
              math.inf, 0.0)
+
+    def set_angle_table(self, triples, tab):
+        """FixedTripleListTabulatedAngular on the triples (linear interpolation)."""
+        t = np.ascontiguousarray(triples, np.int64).reshape(-1)
+        call(self.lib, "espp_triples_add", self.h, len(t) // 3, i64ptr(t))
+        th, e, f = (np.ascontiguousarray(a, np.float64) for a in tab)
+        call(self.lib, "espp_tab_angle_set", self.h, 1, len(th), dptr(th), dptr(e), dptr(f))
 
     def set_pair_table(self, tab, rc=3.0):
         r, e, f = (np.ascontiguousarray(a, np.float64) for a in tab)

@@ -37,6 +37,11 @@ def test_cg_workflow_small(tmp_path):
     assert err_table < 1.05
     resid = np.array([t - pair_only.forces_at(p) for p, t in zip(pos, target)])
     s = cg.CGSystem(pos[0], L, bonds, tab)
+    triples = cg.angle_triples(bonds)
+    assert len(triples) == 24 * (10 - 2)
+    atab = cg.boltzmann_angle_table(cg.angles_of(pos, triples))
+    assert np.all(np.isfinite(atab[1])) and atab[2][-1] == 0.0
+    s.set_angle_table(triples, atab)
     s.set_pair_table(ptab)
     model = cg.MLPModel(seed=3)
     s.attach(model)
