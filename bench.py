@@ -442,7 +442,7 @@ def gpu_arm(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
-# ---- the smaller configurations of the benchmark spec ------------------------------
+# ---- the smaller configurations: Kremer-Grest melt and 32k LJ fluid ----------------
 def kg_melt_config(lib, prec, nchains=200, nbeads=200, cap_steps=1000, steps=9000):
     """Kremer-Grest melt: nchains x nbeads beads at density 0.85 (random walks, bond 0.97,
     overlaps < 0.8 rejected; tools.topology.polymer_melt, seed 3), WCA (rc 2^(1/6), auto
@@ -521,13 +521,12 @@ def small_configs(lib):
 
 # ---- learned coarse-grained potential ---------------------------------------------
 def cg_arm(args, rank, world, local_rank):
-    """Learned CG potential (the benchmark spec's coarse-graining configuration): a
-    fine-grained Kremer-Grest melt of 1000 x 200 beads (200,000 beads) mapped 4 -> 1
-    (50,000 sites); 500 frames of mapped conservative forces; CG bonds from a
-    Boltzmann-inverted table; an MLP 16-64-64-1 trained by force matching on the GPU;
-    a force-matched pair table as the fallback; CG runs judged against the fine-grained
-    path by force-matching error, RDF and chain motion.  Sizes scale with --cg-chains
-    and --cg-frames."""
+    """Learned CG potential workload: a fine-grained Kremer-Grest melt of 1000 x 200 beads
+    (200,000 beads) mapped 4 -> 1 (50,000 sites); 500 frames of mapped conservative
+    forces; CG bonds and angles from Boltzmann-inverted tables; an MLP 16-64-64-1 trained
+    by force matching on the GPU; a force-matched pair table as the fallback; CG runs
+    compared with the fine-grained melt by force-matching error, RDF and chain motion.
+    Sizes scale with --cg-chains and --cg-frames."""
     from espressopp_b200 import cg
     from espressopp_b200._abi import call, dptr
     if rank != 0:
@@ -666,7 +665,7 @@ def cg_arm(args, rank, world, local_rank):
         "config": {"workload": "learned CG potential: Kremer-Grest melt %d x 200 beads -> "
                                "%d CG sites (4:1), %d frames, MLP 16-64-64-1 SiLU" %
                                (nch, n_cg, nfr)},
-        "cg_judge": {
+        "cg_quality": {
             "force_matching_rel_err": {
                 "mlp_plus_ibi_table": err_mlp, "ibi_table": err_table,
                 "mlp_plus_force_matched_table": err_mlp_fm,
