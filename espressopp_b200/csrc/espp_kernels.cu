@@ -55,6 +55,16 @@ __device__ __forceinline__ float wrapped_diff(int a, int b, float unit) {
   return (float)(int)((unsigned)a - (unsigned)b) * unit;
 }
 
+// 16-byte read of the Verlet list that does not allocate in L1, so that the list stream
+// leaves L1 to the coordinate gathers
+__device__ __forceinline__ int4 ld_list(const int4* p) {
+  int4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p));
+  return v;
+}
+
 __device__ __forceinline__ float fast_rcp(float x) {
   float r;
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
@@ -961,8 +971,8 @@ __global__ void __launch_bounds__(256) k_force_mixed(DevView d, FENEParams fp) {
     const size_t bstride = cap * 2;
     int4 ja = make_int4(i, i, i, i), jb = ja;
     if (nblk > 0) {
-      ja = __ldcs(blk);
-      jb = __ldcs(blk + 1);
+      ja = ld_list(blk);
+      jb = ld_list(blk + 1);
     }
     for (int b = 0; b < nblk; ++b) {
       const int j[8] = {ja.x, ja.y, ja.z, ja.w, jb.x, jb.y, jb.z, jb.w};
@@ -971,8 +981,8 @@ __global__ void __launch_bounds__(256) k_force_mixed(DevView d, FENEParams fp) {
       for (int u = 0; u < 8; ++u) pj[u] = __ldg(&d.posq[j[u]]);
       blk += bstride;
       if (b + 1 < nblk) {
-        ja = __ldcs(blk);
-        jb = __ldcs(blk + 1);
+        ja = ld_list(blk);
+        jb = ld_list(blk + 1);
       }
 #pragma unroll
       for (int u = 0; u < 8; ++u) pair(pj[u]);
@@ -985,8 +995,8 @@ __global__ void __launch_bounds__(256) k_force_mixed(DevView d, FENEParams fp) {
     const size_t bstride = cap * 2 * TPP;
     int4 ja = make_int4(i, i, i, i), jb = ja;
     if (sub < nblk) {
-      ja = __ldcs(blk);
-      jb = __ldcs(blk + 1);
+      ja = ld_list(blk);
+      jb = ld_list(blk + 1);
     }
     for (int b = sub; b < nblk; b += TPP) {
       const int j[8] = {ja.x, ja.y, ja.z, ja.w, jb.x, jb.y, jb.z, jb.w};
@@ -995,8 +1005,8 @@ __global__ void __launch_bounds__(256) k_force_mixed(DevView d, FENEParams fp) {
       for (int u = 0; u < 8; ++u) pj[u] = __ldg(&d.posq[j[u]]);
       blk += bstride;
       if (b + TPP < nblk) {
-        ja = __ldcs(blk);
-        jb = __ldcs(blk + 1);
+        ja = ld_list(blk);
+        jb = ld_list(blk + 1);
       }
 #pragma unroll
       for (int u = 0; u < 8; ++u) pair(pj[u]);
