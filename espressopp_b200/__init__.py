@@ -13,7 +13,7 @@ include/espp_b200.h); there is no CPU fallback.
 from ._lib import LIBRARY_PATH, load_library  # noqa: F401
 from .core import (FixedPairList, FixedTripleList, Int3D, Real3D, System,  # noqa: F401
                    Tensor, VerletList, infinity, set_default_precision)
-from . import analysis, bc, esutil, integrator, interaction, storage, tools  # noqa: F401
+from . import analysis, bc, esutil, integrator, interaction, io, storage, tools  # noqa: F401
 from . import standard_system  # noqa: F401
 from .parallel_tempering import ParallelTempering  # noqa: F401
 
