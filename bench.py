@@ -49,9 +49,9 @@ STEP_BYTES = 168.0 + 4.0 * N_HALF
 # force kernel: packed coordinates read 12 + 4 B per half-list pair + int64 F write 24
 FORCE_BYTES = 12.0 + 4.0 * N_HALF + 24.0
 # DRAM bytes (read + write) per particle of one force-kernel launch, measured by ncu on
-# the 1,000,000-particle case (profiles/force_mixed_lj_1M_ncu.txt: 345.0 MB + 5.6 MB);
+# the 1,000,000-particle case (profiles/force_mixed_lj_1M_ncu.txt: 345.0 MB + 6.7 MB);
 # traffic grows in proportion to the particle count at fixed density
-FORCE_TRAFFIC_PER_PARTICLE = 350.6
+FORCE_TRAFFIC_PER_PARTICLE = 351.7
 
 
 def log(*a):

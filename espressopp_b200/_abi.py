@@ -56,6 +56,7 @@ PROTOTYPES = {
     "espp_virial": (c_int32, [_P, c_int32, _D]),
     "espp_virial_tensor": (c_int32, [_P, c_int32, _D]),
     "espp_kinetic": (c_int32, [_P, _D, _I64]),
+    "espp_kinetic_tensor": (c_int32, [_P, _D]),
     "espp_rdf": (c_int32, [_P, c_int32, _D]),
     "espp_confs_create": (c_int32, [_P, c_int32, c_int64, _I64, POINTER(c_void_p)]),
     "espp_confs_destroy": (c_int32, [_P]),

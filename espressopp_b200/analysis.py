@@ -54,20 +54,14 @@ class Pressure(_Observable):
 
 
 class PressureTensor(_Observable):
-    """P_ab = (sum m v_a v_b + W_ab) / V; kinetic part from the particle velocities."""
+    """P_ab = (sum m v_a v_b + W_ab) / V (PressureTensor.hpp:51-80); the kinetic sum and
+    the virials are reduced on the GPU."""
 
     def compute(self):
         st = self._st()
-        _, pos, vel, _, _ = st.getAll()
-        masses = np.array([st._masses[i] for i in sorted(st._types)])
         vv = np.zeros(6)
-        mv = vel * masses[:, None]
-        vv[0] = np.sum(mv[:, 0] * vel[:, 0])
-        vv[1] = np.sum(mv[:, 1] * vel[:, 1])
-        vv[2] = np.sum(mv[:, 2] * vel[:, 2])
-        vv[3] = np.sum(mv[:, 0] * vel[:, 1])
-        vv[4] = np.sum(mv[:, 0] * vel[:, 2])
-        vv[5] = np.sum(mv[:, 1] * vel[:, 2])
+        call(st._lib, "espp_kinetic_tensor", st._h,
+             vv.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
         w = np.zeros(6)
         for ia in self.system.shortRangeInteractions:
             w += np.asarray(ia.computeVirialTensor())

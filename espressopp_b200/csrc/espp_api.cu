@@ -2029,6 +2029,21 @@ int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n) {
   });
 }
 
+int espp_kinetic_tensor(espp_system* s, double out[6]) {
+  return guard([&] {
+    checked(s);
+    if (!out) raise(ESPP_EINVAL, "null output pointer");
+    for (int k = 0; k < 6; ++k) out[k] = 0.0;
+    if (s->n == 0) return;
+    int nb;
+    double* part = obs_partials(s, nb);
+    launch_kinetic_tensor(s->view(), part, nb, s->obs, s->st);
+    cuda_check(cudaMemcpyAsync(out, s->obs, 6 * sizeof(double), cudaMemcpyDeviceToHost, s->st),
+               "download");
+    sync(s);
+  });
+}
+
 int espp_force_acc(espp_system* s, int32_t op, int64_t n, const int64_t* ids, double* out) {
   return guard([&] {
     checked(s);

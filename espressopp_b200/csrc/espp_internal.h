@@ -228,6 +228,8 @@ void launch_tab_observables(const DevView& d, int bond, double* partials, int nb
                             double* out, int energy, cudaStream_t st);
 void launch_kinetic(const DevView& d, double* partials, int nblocks, double* out,
                     cudaStream_t st);
+void launch_kinetic_tensor(const DevView& d, double* partials, int nblocks, double* out,
+                           cudaStream_t st);
 // Verlet pair export: counts per particle (pairs with id_j > id_i), then the pairs.
 void launch_pair_count(const DevView& d, int32_t* counts, cudaStream_t st);
 void launch_pair_write(const DevView& d, const int64_t* offsets, int64_t* out,

@@ -1888,6 +1888,24 @@ __global__ void k_kinetic(DevView d, double* partials) {
   block_sum_store<1>(acc, partials);
 }
 
+// mass * Tensor(v, v) of each particle: (xx, yy, zz, xy, xz, yz), m (v_a v_b)
+__global__ void k_kinetic_tensor(DevView d, double* partials) {
+  const ParticleArrays a = d.pa[0];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  if (i < d.n) {
+    const double v[3] = {a.v[i], a.v[(size_t)d.cap + i], a.v[2 * (size_t)d.cap + i]};
+    const double m = a.mass[i];
+    acc[0] = __dmul_rn(m, __dmul_rn(v[0], v[0]));
+    acc[1] = __dmul_rn(m, __dmul_rn(v[1], v[1]));
+    acc[2] = __dmul_rn(m, __dmul_rn(v[2], v[2]));
+    acc[3] = __dmul_rn(m, __dmul_rn(v[0], v[1]));
+    acc[4] = __dmul_rn(m, __dmul_rn(v[0], v[2]));
+    acc[5] = __dmul_rn(m, __dmul_rn(v[1], v[2]));
+  }
+  block_sum_store<6>(acc, partials);
+}
+
 __global__ void k_pair_count(DevView d, int32_t* counts) {
   const ParticleArrays a = d.pa[0];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2149,6 +2167,12 @@ void launch_kinetic(const DevView& d, double* partials, int nblocks, double* out
                     cudaStream_t st) {
   k_kinetic<<<nblocks, kBlock, 0, st>>>(d, partials);
   k_sum_partials<1><<<1, 256, 0, st>>>(partials, nblocks, out);
+}
+
+void launch_kinetic_tensor(const DevView& d, double* partials, int nblocks, double* out,
+                           cudaStream_t st) {
+  k_kinetic_tensor<<<nblocks, kBlock, 0, st>>>(d, partials);
+  k_sum_partials<6><<<1, 256, 0, st>>>(partials, nblocks, out);
 }
 
 void launch_bond_maxsq(const DevView& d, double* partials, int nblocks, double* out,

@@ -221,6 +221,9 @@ ESPP_API int espp_virial(espp_system* s, int32_t which, double* w);
 ESPP_API int espp_virial_tensor(espp_system* s, int32_t which, double w[6]);
 /* sum m v^2 over real particles and their count (analysis/Temperature.hpp:57-125). */
 ESPP_API int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n);
+/* sum over real particles of mass * Tensor(v, v) (analysis/PressureTensor.hpp:60-70):
+ * out = (xx, yy, zz, xy, xz, yz), each m (v_a v_b). */
+ESPP_API int espp_kinetic_tensor(espp_system* s, double out[6]);
 
 /* analysis::RadialDistrF::computeArray(rdfN) (src/analysis/RadialDistrF.cpp:47-150): histogram
  * of all pair distances (minimum image) in rdfN bins of width dr = L_y / (2 rdfN), each

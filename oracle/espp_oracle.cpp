@@ -2056,6 +2056,23 @@ int espp_rdf(espp_system* s, int32_t rdfN, double* out) {
   return ESPP_OK;
 }
 
+// PressureTensor::computeRaw's kinetic part (src/analysis/PressureTensor.hpp:60-70):
+// vvLocal += mass * Tensor(vel, vel) over the real particles
+int espp_kinetic_tensor(espp_system* s, double out[6]) {
+  CHECK_S(s);
+  if (!out) return fail(ESPP_EINVAL, "null output pointer");
+  double t[6] = {0, 0, 0, 0, 0, 0};
+  for (int ci : s->realCells)
+    for (auto& p : s->cells[ci].p) {
+      const double* v = p.v;
+      const double vv[6] = {v[0] * v[0], v[1] * v[1], v[2] * v[2],
+                            v[0] * v[1], v[0] * v[2], v[1] * v[2]};
+      for (int k = 0; k < 6; ++k) t[k] += p.mass * vv[k];
+    }
+  for (int k = 0; k < 6; ++k) out[k] = t[k];
+  return ESPP_OK;
+}
+
 int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n) {
   CHECK_S(s);
   double v2 = 0.0;

@@ -393,6 +393,21 @@ def test_tabulated_angular_matches_oracle(prec, tmp_path):
                                                    rel=1e-3)
 
 
+def test_kinetic_tensor_matches_oracle():
+    """sum of mass * Tensor(v, v) (PressureTensor.hpp:60-70) on the GPU against the oracle;
+    its trace is the kinetic sum of Temperature."""
+    pid, pos, vel, box = load_lj2048()
+    outs = []
+    for lib in (oracle_lib(), cuda_lib()):
+        s = _lj_setup(lib, _abi.PREC_FP64, pid, pos, vel, box)
+        t = np.zeros(6)
+        _abi.call(lib, "espp_kinetic_tensor", s.h, _abi.dptr(t))
+        outs.append((t, s.kinetic()))
+    (to, ko), (tg, kg) = outs
+    assert np.allclose(tg, to, rtol=1e-12, atol=1e-12 * np.abs(to).max())
+    assert abs(tg[:3].sum() - kg[0]) < 1e-12 * kg[0]
+
+
 def test_msd_matches_oracle():
     """MeanSquareDispl::compute / computeG3 on the GPU against the oracle on the same
     snapshots (FP64, only the summation order differs), and GPU snapshots of the same
