@@ -592,11 +592,14 @@ def cg_arm(args, rank, world, local_rank):
     g_fg = cg.rdf_of_frames(tabsys, pos[::max(1, nfr // 25)], nb)
     t3 = time.perf_counter()
     ibi = {}
+    g_cg = {}
+    blen = cg.bond_lengths(pos[:ntrain], bonds)
     for name, sysm in (("mlp", s), ("table", tabsys)):
         sysm.set_pos(sysm.ids, cg.wrap(pos[-1], L))
         call(sysm.lib, "espp_integrator_set", sysm.h, 0.01)
         sysm.thermostat(True)
-        _, ibi[name] = cg.ibi_refine(sysm, ptab, g_fg, nb, iters=args.cg_ibi, log=log)
+        _, ibi[name], g_cg[name] = cg.ibi_refine(sysm, ptab, g_fg, nb, iters=args.cg_ibi,
+                                                 log=log, bonded=(bonds, tab, blen))
     t_ibi = time.perf_counter() - t3
     err_mlp = cg.fm_error(s, pos[ntrain:], target[ntrain:], fbond_test)
     err_table_fm = err_table
@@ -673,6 +676,11 @@ def cg_arm(args, rank, world, local_rank):
             "rdf_l2": {"mlp_plus_ibi_table": out["mlp"]["rdf_l2"],
                        "ibi_table": out["table"]["rdf_l2"],
                        "ibi_iterations": {"mlp": ibi["mlp"], "table": ibi["table"]},
+                       "curves": {"r": [round(float(x), 4) for x in (np.arange(nb) + 0.5) *
+                                        (L / 2 / nb)],
+                                  "fg": [round(float(x), 5) for x in g_fg],
+                                  "mlp": [round(float(x), 5) for x in g_cg["mlp"]],
+                                  "table": [round(float(x), 5) for x in g_cg["table"]]},
                        "definition": "sqrt(mean over bins r < 6 of (g_cg - g_fg)^2), "
                                      "120 bins up to L/2"},
             "particle_steps_per_chain_motion_fg_over_cg": ratio,

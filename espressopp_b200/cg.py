@@ -485,51 +485,90 @@ def rdf_of_frames(cg, frames_pos, nbins):
 
 
 def ibi_refine(cgsys, tab, g_target, nbins, iters=10, steps=3000, every=250, alpha=0.8,
-               rc=3.0, T=1.0, log=None):
+               rc=3.0, T=1.0, log=None, bonded=None):
     """Iterative Boltzmann inversion of a pair table against a target RDF: each iteration
     runs the CG system (bonds + this pair table, thermostatted) on the GPU, samples the
     RDF, and updates U(r) += alpha T ln(g(r) / g_target(r)) (step at most alpha T, bins
-    with g > 0.02 only, tapered to zero at rc); F = -dU/dr.  An iteration whose RDF error
-    is larger than the best so far goes back to the best table and halves alpha, and the
-    best table is the one returned.  Returns the refined table and the RDF L2 error per
-    iteration."""
+    where either RDF is sampled, tapered to zero at rc); F = -dU/dr.  An iteration whose RDF error
+    is larger than the best so far goes back to the best tables and halves alpha, and the
+    best tables are the ones returned.
+    bonded = (bonds, bond table, target bond lengths): the bond table is refined in the
+    same way against the bond-length distribution of the target (U_b += alpha T
+    ln(P(r) / P_target(r)) over the sampled range).
+    Returns the refined pair table, the RDF L2 error per iteration, and the last sampled
+    RDF of the best tables."""
     r_t, E_t, F_t = (np.array(a, np.float64) for a in tab)
     dr = cgsys.L / 2 / nbins
     rb = (np.arange(nbins) + 0.5) * dr
     hist = []
-    best = (np.inf, E_t.copy(), None)
+    if bonded is not None:
+        bonds, btab, blen = bonded
+        rbt, Ebt, _ = (np.array(a, np.float64) for a in btab)
+        lo, hi = np.percentile(blen, [0.5, 99.5])
+        bedges = np.linspace(lo, hi, 41)
+        pb_target, _ = np.histogram(blen, bins=bedges, density=True)
+        bc = 0.5 * (bedges[1:] + bedges[:-1])
+        bidx = np.asarray(bonds, np.int64).reshape(-1, 2) - 1
+    best = (np.inf, E_t.copy(), None, None if bonded is None else Ebt.copy(), None)
     for it in range(iters):
         cgsys.set_pair_table((r_t, E_t, F_t), rc)
+        if bonded is not None:
+            cgsys.set_bond_table((rbt, Ebt, -np.gradient(Ebt, rbt)))
         cgsys.run(1000)
         g = np.zeros(nbins)
+        lens = []
         ns = 0
         for _ in range(steps // every):
             cgsys.run(every)
             g += cgsys.rdf(nbins)
+            if bonded is not None:
+                p = cgsys.state(cgsys.ids)[0]
+                d = p[bidx[:, 0]] - p[bidx[:, 1]]
+                d -= cgsys.L * np.round(d / cgsys.L)
+                lens.append(np.sqrt(np.sum(d * d, 1)))
             ns += 1
         g /= ns
+        pb = None
+        if bonded is not None:
+            pb, _ = np.histogram(np.concatenate(lens), bins=bedges, density=True)
         sel = rb < 2 * rc
         hist.append(float(np.sqrt(np.mean((g[sel] - g_target[sel]) ** 2))))
         if log:
             log("IBI iteration %d: RDF L2 %.4f (alpha %.3f)" % (it, hist[-1], alpha))
         if hist[-1] < best[0]:
-            best = (hist[-1], E_t.copy(), g.copy())
+            best = (hist[-1], E_t.copy(), g.copy(), None if bonded is None else Ebt.copy(), pb)
         else:
-            # overshoot: step again from the best table with half the step
+            # overshoot: step again from the best tables with half the step
             alpha *= 0.5
             E_t = best[1].copy()
             g = best[2]
-        # bins with a reliable RDF only; steps of at most 0.5 T per iteration
-        ok = (rb < rc) & (g > 0.02) & (g_target > 0.02)
+            if bonded is not None:
+                Ebt = best[3].copy()
+                pb = best[4]
+        # bins where either RDF is sampled (the core too, where the CG sites come closer
+        # than the mapped ones); steps of at most alpha T per iteration
+        ok = (rb < rc) & ((g > 0.002) | (g_target > 0.002))
         du = np.zeros(nbins)
-        du[ok] = alpha * T * np.clip(np.log(g[ok] / g_target[ok]), -1.0, 1.0)
+        du[ok] = alpha * T * np.clip(
+            np.log(np.maximum(g[ok], 1e-4) / np.maximum(g_target[ok], 1e-4)), -1.0, 1.0)
         du = np.convolve(du, np.ones(3) / 3, mode="same")
         first = np.argmax(ok)
         du[:first] = du[first]
         du *= np.clip(1.0 - (rb / rc) ** 4, 0.0, 1.0)
         E_t = E_t + np.interp(r_t, rb, du)
         F_t = -np.gradient(E_t, r_t)
+        if bonded is not None:
+            okb = (pb > 0.01 * pb_target.max()) & (pb_target > 0.01 * pb_target.max())
+            dub = np.zeros_like(bc)
+            dub[okb] = alpha * T * np.clip(np.log(pb[okb] / pb_target[okb]), -1.0, 1.0)
+            dub = np.convolve(dub, np.ones(3) / 3, mode="same")
+            # over the sampled range; outside it the end values (a constant shift keeps the
+            # continuation's force)
+            if okb.any():
+                Ebt = Ebt + np.interp(rbt, bc[okb], dub[okb])
     E_t = best[1]
     F_t = -np.gradient(E_t, r_t)
     cgsys.set_pair_table((r_t, E_t, F_t), rc)
-    return (r_t, E_t, F_t), hist
+    if bonded is not None:
+        cgsys.set_bond_table((rbt, best[3], -np.gradient(best[3], rbt)))
+    return (r_t, E_t, F_t), hist, best[2]
