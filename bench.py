@@ -46,6 +46,9 @@ N_HALF = 2.0 / 3.0 * math.pi * (RC + SKIN) ** 3 * RHO
 # algorithmic bytes per particle and step, whole step (mixed precision):
 # x r/w 48 + v r/w 48 + int64 F w/r 48 + FP32 packed x w/r 24 + 4 B per half-list pair
 STEP_BYTES = 168.0 + 4.0 * N_HALF
+# algorithmic FLOPs per particle-step: 24 per half-list pair (3 sub, 5 for r^2, 1 rcp,
+# 2 for r^6, 4 for the force factor, 3 for F, 6 accumulate)
+STEP_FLOPS = 24.0 * N_HALF
 # force kernel: packed coordinates read 12 + 4 B per half-list pair + int64 F write 24
 FORCE_BYTES = 12.0 + 4.0 * N_HALF + 24.0
 # DRAM bytes (read + write) per particle of one force-kernel launch, measured by ncu on
@@ -385,6 +388,8 @@ def gpu_arm(args, rank, world, local_rank):
 
     peaks, peak_kind = measured_peaks()
     hbm = float(peaks["hbm_gbs"])
+    fp32 = ctypes.c_double()
+    call(lib, "espp_fp32_peak", ctypes.byref(fp32))
     force_avg_ms = ph[0] / max(1, launches_p[0])
     achieved = FORCE_BYTES * N / (force_avg_ms * 1e-3) / 1e9
     step_s = loop_ms * 1e-3 / args.steps
@@ -416,6 +421,12 @@ def gpu_arm(args, rank, world, local_rank):
         "step_roofline": {"alg_bytes_per_particle_step": STEP_BYTES,
                           "achieved_gbs": STEP_BYTES * N / step_s / 1e9,
                           "frac": STEP_BYTES * N / step_s / 1e9 / hbm},
+        "step_flop_roofline": {"alg_flops_per_particle_step": STEP_FLOPS,
+                               "achieved_tflops": STEP_FLOPS * N / step_s / 1e12,
+                               "peak_tflops": fp32.value,
+                               "frac": (STEP_FLOPS * N / step_s / 1e12 / fp32.value
+                                        if fp32.value > 0 else None),
+                               "peak_kind": "measured FP32 FMA throughput (probe kernel)"},
         "profiled_pass_ms": {"force": ph[0], "integrate": ph[1], "resort": ph[2],
                              "decide": ph[3], "verlet_build": ph[4],
                              "launches": [int(x) for x in launches_p[:5]]},

@@ -85,6 +85,7 @@ PROTOTYPES = {
     "espp_last_run_ms": (c_int32, [_P, _D]),
     "espp_select_device": (c_int32, [c_int32]),
     "espp_set_tpp": (c_int32, [_P, c_int32]),
+    "espp_fp32_peak": (c_int32, [_D]),
     "espp_batch_create": (c_int32, [POINTER(c_void_p), c_int32, POINTER(c_void_p)]),
     "espp_batch_destroy": (c_int32, [_P]),
     "espp_batch_run": (c_int32, [_P, c_int64]),

@@ -2470,6 +2470,17 @@ int espp_msd_chain_com(espp_confs* c, int32_t chainlength, double* out) {
   });
 }
 
+int espp_fp32_peak(double* tflops) {
+  return guard([&] {
+    if (!tflops) raise(ESPP_EINVAL, "null output pointer");
+    int dev = 0, nsm = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    cuda_check(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "attribute");
+    *tflops = measure_fp32_tflops(nsm, 0);
+    cuda_check(cudaGetLastError(), "fp32 probe");
+  });
+}
+
 int espp_set_tpp(espp_system* s, int32_t tpp) {
   return guard([&] {
     checked(s);

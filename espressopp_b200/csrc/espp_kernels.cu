@@ -1976,6 +1976,40 @@ __global__ void k_get_by_id(DevView d, int n, const int64_t* ids, double* pos, d
 
 }  // namespace
 
+// ---- FP32 throughput probe (the FLOP side of the step's roofline) ---------------------
+// Eight independent FMA chains per thread, scalar or packed f32x2; the result is kept live
+// by a store that never happens for finite inputs.
+template <bool PACKED>
+__global__ void __launch_bounds__(256) k_fma_probe(float* out, int iters) {
+  const float b = 1.0000001f, c = 1.0e-7f;
+  if (PACKED) {
+    unsigned long long a[8];
+    const unsigned long long bb = f2_pack(b, b), cc = f2_pack(c, c);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a[q] = f2_pack(threadIdx.x * 1e-3f + q, q * 0.5f);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) a[q] = f2_fma(a[q], bb, cc);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s += f2_lo(a[q]) + f2_hi(a[q]);
+    if (s == -1.0f) out[blockIdx.x] = s;
+  } else {
+    float a[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a[q] = threadIdx.x * 1e-3f + q;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) a[q] = fmaf(a[q], b, c);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s += a[q];
+    if (s == -1.0f) out[blockIdx.x] = s;
+  }
+}
+
 // ---- launchers ---------------------------------------------------------------------
 
 void launch_fold_bin(const DevView& d, RebuildScratch& s, bool fold, cudaStream_t st) {
@@ -2066,6 +2100,35 @@ static void force_dispatch(const DevView& d, bool single, bool capped, bool fene
   ESPP_FORCE_CASE(false, true, false)
   ESPP_FORCE_CASE(false, true, true)
 #undef ESPP_FORCE_CASE
+}
+
+double measure_fp32_tflops(int nsm, cudaStream_t st) {
+  const int blocks = nsm * 8, threads = 256, iters = 8192;
+  float* out = nullptr;
+  cudaMalloc(&out, sizeof(float) * blocks);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  double best = 0.0;
+  for (int packed = 0; packed < 2; ++packed) {
+    for (int rep = 0; rep < 3; ++rep) {
+      cudaEventRecord(e0, st);
+      if (packed)
+        k_fma_probe<true><<<blocks, threads, 0, st>>>(out, iters);
+      else
+        k_fma_probe<false><<<blocks, threads, 0, st>>>(out, iters);
+      cudaEventRecord(e1, st);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      const double flops = 2.0 * (packed ? 16.0 : 8.0) * iters * (double)blocks * threads;
+      if (ms > 0.f && rep > 0) best = fmax(best, flops / (ms * 1e-3) / 1e12);
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  return best;
 }
 
 void launch_forces(const DevView& d, bool mixed, const FENEParams& fp, int tpp,

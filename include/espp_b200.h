@@ -339,6 +339,11 @@ ESPP_API int espp_profile(espp_system* s, double ms[8], int64_t launches[8]);
  * (within the 1e-5 error budget) but not their determinism for a fixed setting.
  * No reference counterpart (tuning of the GPU kernel). */
 ESPP_API int espp_set_tpp(espp_system* s, int32_t tpp);
+
+/* Sustained FP32 FMA throughput of the current device in TFLOP/s (a probe kernel of
+ * independent scalar and packed f32x2 FMA chains, the higher of the two), for the FLOP
+ * side of the step's roofline.  No reference counterpart. */
+ESPP_API int espp_fp32_peak(double* tflops);
 /* Times the force kernel on the current particle state for 1, 2, 4 and 8 threads per
  * particle (3 launches each, CUDA events), keeps the fastest and returns it; ms[c] (may
  * be NULL) receives the mean launch time of candidate c. */

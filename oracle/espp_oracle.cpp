@@ -2118,6 +2118,13 @@ int espp_set_tpp(espp_system* s, int32_t) {
   return ESPP_OK;
 }
 
+// no device: the CPU restatement reports no FP32 peak
+int espp_fp32_peak(double* tflops) {
+  if (!tflops) return fail(ESPP_EINVAL, "null output pointer");
+  *tflops = 0.0;
+  return ESPP_OK;
+}
+
 int espp_autotune(espp_system* s, int32_t* best, double ms[4]) {
   CHECK_S(s);
   if (best) *best = 1;

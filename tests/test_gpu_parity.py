@@ -1,4 +1,5 @@
 """GPU parity against the FP64 oracle (both driven through the same C ABI)."""
+import ctypes
 import math
 
 import numpy as np
@@ -531,3 +532,11 @@ def test_polymer_melt_with_angles_matches_oracle(prec):
     ref = o.particles(ids)
     got = g.particles(ids)
     assert np.max(np.abs(got[0] - ref[0])) < (1e-9 if prec == _abi.PREC_FP64 else 1e-4)
+
+
+def test_fp32_probe_reports_a_plausible_peak():
+    """The FP32 FMA probe behind the FLOP side of the roofline: a B200 sustains tens of
+    TFLOP/s (148 SMs x 128 lanes x 2 FLOP x ~1.9 GHz = 72 TFLOP/s scalar)."""
+    t = ctypes.c_double()
+    _abi.call(cuda_lib(), "espp_fp32_peak", ctypes.byref(t))
+    assert 20.0 < t.value < 400.0
