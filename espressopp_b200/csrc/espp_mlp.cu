@@ -27,6 +27,13 @@ __device__ __forceinline__ double mimg(double dx, double L, double hL) {
 }
 
 __device__ __forceinline__ float sigm(float z) { return 1.0f / (1.0f + expf(-z)); }
+// fast forms for the BF16 tensor-core network (operand rounding dominates their error)
+__device__ __forceinline__ float sigm_fast(float z) { return __fdividef(1.0f, 1.0f + __expf(-z)); }
+__device__ __forceinline__ float silu_fast(float z) { return z * sigm_fast(z); }
+__device__ __forceinline__ float silu1_fast(float z) {
+  const float s = sigm_fast(z);
+  return s * (1.0f + z * (1.0f - s));
+}
 __device__ __forceinline__ float silu(float z) { return z * sigm(z); }
 __device__ __forceinline__ float silu1(float z) {
   const float s = sigm(z);
@@ -692,7 +699,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_site_tc(MlpDev m, int n, unsign
       for (int q = 0; q < H / 16; ++q) tmem_ld16(tl + 0 + 16 * q, v + 16 * q);
       tmem_wait_ld();
 #pragma unroll
-      for (int u = 0; u < H; ++u) v[u] = silu(v[u] + S.b1[u]);
+      for (int u = 0; u < H; ++u) v[u] = silu_fast(v[u] + S.b1[u]);
       store_row64(S.P, t, v);
     }
     fence_async_smem();
@@ -718,8 +725,8 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_site_tc(MlpDev m, int n, unsign
 #pragma unroll
       for (int u = 0; u < H; ++u) {
         const float z = v[u] + S.b2[u];
-        e += S.w3[u] * silu(z);
-        v[u] = S.w3[u] * silu1(z);
+        e += S.w3[u] * silu_fast(z);
+        v[u] = S.w3[u] * silu1_fast(z);
       }
       if (i < n) m.E[i] = e;
       store_row64(S.Q, t, v);
@@ -747,7 +754,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_site_tc(MlpDev m, int n, unsign
       }
       tmem_wait_ld();
 #pragma unroll
-      for (int u = 0; u < H; ++u) g[u] *= silu1(z[u] + S.b1[u]);
+      for (int u = 0; u < H; ++u) g[u] *= silu1_fast(z[u] + S.b1[u]);
       store_row64(S.P, t, g);
     }
     fence_async_smem();
