@@ -419,10 +419,11 @@ __device__ __forceinline__ float f2_hi(unsigned long long v) {
 // of them against its particle, two candidates per packed f32x2 operation.  A lane
 // appends its partners to its own staging row and writes every full block of 8 to the
 // list with two 16-byte stores, so the list is written in whole sectors.  Candidates
-// within the relative 2e-5 band around the cutoff are decided, after the chunk's other
-// partners, by the reference's FP64 arithmetic (exact_pair_test), as in the ballot
-// form above; the pair set is the reference's (VerletList.cpp:274-450) and each list
-// is in a fixed order.
+// are tested in FP32 on cell-relative coordinates; those within the relative 2e-5 band
+// around (rc + skin)^2 are decided, after the chunk's other partners, by the reference's
+// FP64 arithmetic (exact_pair_test: d = p1 - (p2 + ghost shift), ((dx dx + dy dy) + dz dz),
+// Particle.hpp:93-98, DomainDecomposition.cpp:1347-1391).  The pair set is therefore the
+// reference's (VerletList.cpp:274-450), and each list is in a fixed order.
 constexpr int kBuildWarps = 4;
 constexpr int kStageLd = 44;  // staging row: <= 7 carried + <= 32 appended; 11 x 16 B
 
