@@ -57,7 +57,10 @@ __device__ __forceinline__ double pair_d(const DevView& d, const double* X, int 
   return ex * ex + ey * ey + ez * ez;
 }
 
-// basis values g[k] (gp == nullptr) or derivatives gp[k] = dg_k/dr at distance r < rc
+// basis values g[k] (gp == nullptr) or derivatives gp[k] = dg_k/dr at distance r < rc;
+// FAST takes the fast exponential (for the BF16 tensor-core network, whose operand
+// rounding dominates the error)
+template <bool FAST = false>
 __device__ __forceinline__ void rbf(const MlpDev& m, float r, float* g, float* gp) {
   float sn, cs;
   sincospif(r / m.rc, &sn, &cs);
@@ -66,13 +69,14 @@ __device__ __forceinline__ void rbf(const MlpDev& m, float r, float* g, float* g
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const float t = r - (m.r0 + k * m.dmu);
-    const float e = expf(-m.gamma * t * t);
+    const float e = FAST ? __expf(-m.gamma * t * t) : expf(-m.gamma * t * t);
     if (g) g[k] = e * fc;
     if (gp) gp[k] = e * (dfc - 2.0f * m.gamma * t * fc);
   }
 }
 
 // G_i = sum_j g(r_ij) over the list partners within rc.
+template <bool FAST>
 __global__ void k_mlp_desc(DevView d) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.n) return;
@@ -89,7 +93,7 @@ __global__ void k_mlp_desc(DevView d) {
     const double r2 = pair_d(d, X, i, j, dx, dy, dz);
     if (!(r2 < rc2) || j == i) continue;
     float g[K];
-    rbf(m, sqrtf((float)r2), g, nullptr);
+    rbf<FAST>(m, sqrtf((float)r2), g, nullptr);
 #pragma unroll
     for (int k = 0; k < K; ++k) G[k] += g[k];
   }
@@ -167,7 +171,7 @@ __device__ __forceinline__ long long mlp_fix(float f, unsigned* err) {
 }
 
 // F_i = -sum_j phi_ij d_ij / r_ij, phi_ij = sum_k (D_ik + D_jk) g'_k(r_ij).
-template <bool MIXED>
+template <bool MIXED, bool FAST>
 __global__ void k_mlp_force(DevView d, float* fout) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.n) return;
@@ -186,7 +190,7 @@ __global__ void k_mlp_force(DevView d, float* fout) {
     if (!(r2 < rc2) || j == i) continue;
     const float r = sqrtf((float)r2);
     float gp[K];
-    rbf(m, r, nullptr, gp);
+    rbf<FAST>(m, r, nullptr, gp);
     const float4* Dj = reinterpret_cast<const float4*>(m.D + (size_t)j * K);
     float phi = 0.f;
 #pragma unroll
@@ -431,7 +435,10 @@ void launch_mlp_site_tc(const DevView& d, cudaStream_t st);
 
 void launch_mlp_energy_terms(const DevView& d, cudaStream_t st) {
   if (d.n == 0) return;
-  k_mlp_desc<<<(d.n + 255) / 256, 256, 0, st>>>(d);
+  if (d.mlp.tc)
+    k_mlp_desc<true><<<(d.n + 255) / 256, 256, 0, st>>>(d);
+  else
+    k_mlp_desc<false><<<(d.n + 255) / 256, 256, 0, st>>>(d);
   if (d.mlp.tc) {
     launch_mlp_site_tc(d, st);
   } else {
@@ -443,10 +450,13 @@ void launch_mlp_energy_terms(const DevView& d, cudaStream_t st) {
 void launch_mlp_forces(const DevView& d, bool mixed, float* fout, cudaStream_t st) {
   if (d.n == 0 || !d.mlp.on) return;
   launch_mlp_energy_terms(d, st);
+  const unsigned nb = (d.n + 255) / 256;
   if (mixed)
-    k_mlp_force<true><<<(d.n + 255) / 256, 256, 0, st>>>(d, fout);
+    d.mlp.tc ? k_mlp_force<true, true><<<nb, 256, 0, st>>>(d, fout)
+             : k_mlp_force<true, false><<<nb, 256, 0, st>>>(d, fout);
   else
-    k_mlp_force<false><<<(d.n + 255) / 256, 256, 0, st>>>(d, fout);
+    d.mlp.tc ? k_mlp_force<false, true><<<nb, 256, 0, st>>>(d, fout)
+             : k_mlp_force<false, false><<<nb, 256, 0, st>>>(d, fout);
 }
 
 void launch_sum_site_energy(const DevView& d, double* partials, int nblocks, double* out,
