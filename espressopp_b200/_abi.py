@@ -86,6 +86,7 @@ PROTOTYPES = {
     "espp_select_device": (c_int32, [c_int32]),
     "espp_set_tpp": (c_int32, [_P, c_int32]),
     "espp_fp32_peak": (c_int32, [_D]),
+    "espp_selftest_bounded_wait": (c_int32, [_P, c_int64, _D]),
     "espp_batch_create": (c_int32, [POINTER(c_void_p), c_int32, POINTER(c_void_p)]),
     "espp_batch_destroy": (c_int32, [_P]),
     "espp_batch_run": (c_int32, [_P, c_int64]),

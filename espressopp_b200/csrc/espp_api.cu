@@ -1100,22 +1100,31 @@ RunSnapshot take_snapshot(espp_system* s) {
 }
 
 // Restores the state saved before a graph run whose Verlet list overflowed and grows the
-// list capacity (the caller then redoes the run on the host loop).
+// list capacity (the caller then redoes the run on the host loop).  The list is rebuilt
+// at the restored positions without counting a build: the accumulated displacement is
+// restored too, so re-sorts and builds fall on the same steps as in a run that never
+// overflowed, and the new list holds every pair the old one held within the cutoff
+// until the next re-sort.
 void recover_overflow(espp_system* s, const RunSnapshot& r) {
+  const int hw = K_high_water(s);  // the graph's largest count, before the restore
   cuda_check(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->st), "memset");
   s->paHostValid = false;
   sync_pa(s);
   copy_arrays(s, s->A, s->snap);
   set_counters(s, r.ctr);
   s->step = r.step;
-  s->builds = r.builds;
   s->resortFlag = r.resortFlag;
   s->binned = false;
-  s->K = (std::max(s->K * 2, K_high_water(s) + 32) + 7) / 8 * 8;  // multiple of 8
+  s->K = (std::max(s->K * 2, hw + 32) + 7) / 8 * 8;  // multiple of 8
   dfree(s->nl);
   s->nl = dalloc<int32_t>((size_t)s->K * s->cap);
   s->listValid = false;
   destroy_graph(s);
+  if (!s->resortFlag) {
+    bin(s, false);
+    build_list(s);
+  }
+  s->builds = r.builds;
 }
 
 void run_host(espp_system* s, int64_t nsteps);
@@ -2041,6 +2050,26 @@ int espp_kinetic_tensor(espp_system* s, double out[6]) {
     cuda_check(cudaMemcpyAsync(out, s->obs, 6 * sizeof(double), cudaMemcpyDeviceToHost, s->st),
                "download");
     sync(s);
+  });
+}
+
+int espp_selftest_bounded_wait(espp_system* s, int64_t spins, double* ns) {
+  return guard([&] {
+    checked(s);
+    if (!(spins >= 1 && spins <= (int64_t)1 << 20))
+      raise(ESPP_ERANGE, "spins must lie in [1, 2^20]");
+    unsigned long long* d_out = dalloc<unsigned long long>(2);
+    unsigned long long h[2] = {0, 0};
+    launch_wait_selftest(s->err, (long long)spins, d_out, s->st);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h, d_out, sizeof(h), cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    dfree(d_out);
+    cuda_check(e, "bounded-wait self-test");
+    if (ns) *ns = (double)h[0];
+    check_err(s);
+    if (h[1] == 0) raise(ESPP_ESTATE, "an mbarrier phase completed with no arrival");
   });
 }
 

@@ -199,6 +199,8 @@ struct IntegrateArgs {
 };
 // sustained FP32 FMA throughput of the device (TFLOP/s), scalar or packed, whichever is higher
 double measure_fp32_tflops(int nsm, cudaStream_t st);
+void launch_wait_selftest(unsigned* err, long long spins, unsigned long long* out,
+                          cudaStream_t st);
 void launch_integrate(const DevView& d, const IntegrateArgs& a, cudaStream_t st);
 // maxDist += sqrt(max |dx|^2); flag = maxDist > skinHalf
 void launch_decide(const DevView& d, double skinHalf, cudaStream_t st);

@@ -2132,6 +2132,37 @@ double measure_fp32_tflops(int nsm, cudaStream_t st) {
   return best;
 }
 
+// The failure path of the tensor-core kernels, run on purpose: one CTA holds TMEM and
+// waits on an mbarrier that nothing arrives on, with the same bounded wait the kernels
+// use but `spins` tries; when the wait gives up it sets kErrTimeout, releases the TMEM
+// and returns.  out[0] = nanoseconds spent in the wait, out[1] = 1 if it gave up.
+__global__ void __launch_bounds__(32) k_wait_selftest(unsigned* err, long long spins,
+                                                      unsigned long long* out) {
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_base;
+  tc::tmem_alloc(tc::smem_u32(&tmem_base), 32);
+  if (threadIdx.x == 0) tc::mbar_init(tc::smem_u32(&mbar));
+  __syncwarp();
+  tc::fence_after();
+  if (threadIdx.x == 0) {
+    unsigned long long t0, t1;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    const bool done = tc::mbar_wait(tc::smem_u32(&mbar), 0, spins);
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+    if (!done) atomicOr(err, kErrTimeout);
+    out[0] = t1 - t0;
+    out[1] = done ? 0ull : 1ull;
+  }
+  __syncwarp();
+  tc::fence_before();
+  tc::tmem_dealloc(tmem_base, 32);
+}
+
+void launch_wait_selftest(unsigned* err, long long spins, unsigned long long* out,
+                          cudaStream_t st) {
+  k_wait_selftest<<<1, 32, 0, st>>>(err, spins, out);
+}
+
 void launch_forces(const DevView& d, bool mixed, const FENEParams& fp, int tpp,
                    cudaStream_t st) {
   if (d.n == 0) return;

@@ -54,8 +54,9 @@ __device__ __forceinline__ void commit(uint32_t mbar) {
       : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
-  for (long long it = 0; it < kSpin; ++it) {
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase,
+                                          long long spins = kSpin) {
+  for (long long it = 0; it < spins; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"

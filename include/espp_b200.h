@@ -344,6 +344,12 @@ ESPP_API int espp_set_tpp(espp_system* s, int32_t tpp);
  * independent scalar and packed f32x2 FMA chains, the higher of the two), for the FLOP
  * side of the step's roofline.  No reference counterpart. */
 ESPP_API int espp_fp32_peak(double* tflops);
+/* Runs the tensor-core kernels' failure path on purpose: one CTA holds TMEM and waits,
+ * for at most `spins` tries (1 to 2^20), on an mbarrier that nothing arrives on, then
+ * releases the TMEM and returns; *ns (may be NULL) receives the nanoseconds the wait took.
+ * Returns ESPP_ETIMEOUT ("a bounded wait inside a kernel ran out") when the wait gave up,
+ * as it must, and leaves the system usable.  No reference counterpart. */
+ESPP_API int espp_selftest_bounded_wait(espp_system* s, int64_t spins, double* ns);
 /* Times the force kernel on the current particle state for 1, 2, 4 and 8 threads per
  * particle (3 launches each, CUDA events), keeps the fastest and returns it; ms[c] (may
  * be NULL) receives the mean launch time of candidate c. */

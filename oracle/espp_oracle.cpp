@@ -2125,6 +2125,15 @@ int espp_fp32_peak(double* tflops) {
   return ESPP_OK;
 }
 
+// no device and no device waits: the CPU restatement has nothing to time out
+int espp_selftest_bounded_wait(espp_system* s, int64_t spins, double* ns) {
+  CHECK_S(s);
+  if (!(spins >= 1 && spins <= (int64_t)1 << 20))
+    return fail(ESPP_ERANGE, "spins must lie in [1, 2^20]");
+  if (ns) *ns = 0.0;
+  return fail(ESPP_ESTATE, "no device");
+}
+
 int espp_autotune(espp_system* s, int32_t* best, double ms[4]) {
   CHECK_S(s);
   if (best) *best = 1;
