@@ -12,7 +12,7 @@
 namespace espp {
 namespace tc {
 
-constexpr long long kSpin = 1ll << 26;  // bounded mbarrier wait (about a second)
+constexpr long long kSpin = 1ll << 24;  // bounded mbarrier wait: ~80 ns a try, ~1.3 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
