@@ -24,6 +24,7 @@ PROTOTYPES = {
     "espp_num_particles": (c_int32, [_P, _I64]),
     "espp_get_particles": (c_int32, [_P, c_int64, _I64, _D, _D, _D, _I32]),
     "espp_set_particles": (c_int32, [_P, c_int64, _I64, _D, _D]),
+    "espp_set_images": (c_int32, [_P, c_int64, _I64, _I32]),
     "espp_vl_create": (c_int32, [_P, c_double, c_int64, _I64]),
     "espp_vl_rebuild": (c_int32, [_P]),
     "espp_vl_size": (c_int32, [_P, _I64]),

@@ -7,8 +7,10 @@ particle state lives on the GPU behind one C-ABI system handle that the storage
 creates; the classes here keep configuration and forward to the handle.
 """
 import ctypes
+import json
 import math
 import os
+import sys
 
 import numpy as np
 
@@ -109,6 +111,7 @@ class RNG:
     def __init__(self, seed=12345):
         self.seed = int(seed)
         self._g = np.random.Generator(np.random.PCG64(self.seed))
+        self._keyed = False  # a storage has keyed its Langevin noise on this seed
 
     def __call__(self, n=None):
         if n is None:
@@ -123,6 +126,39 @@ class RNG:
 
     def get_seed(self):
         return self.seed
+
+    def saveState(self, step):
+        """Writes the generator state to the file "rng.<step>" in the working directory,
+        one line per rank (RNG::saveState, src/esutil/RNG.cpp:86-108).  The line holds
+        the seed, which keys the Langevin noise, and the host generator's state."""
+        line = json.dumps({"seed": self.seed, "state": self._g.bit_generator.state})
+        with open("rng." + str(int(step)), "w") as f:
+            f.write(line + "\n")
+
+    def loadState(self, fname):
+        """Restores a state written by saveState (RNG::loadState, RNG.cpp:110-138).  As
+        there, a file whose number of lines differs from the number of ranks (one) leaves
+        the state unchanged with a warning.  The Langevin noise of a system is keyed on
+        the seed it was created with, so a saved seed different from that key also leaves
+        the state unchanged with a warning."""
+        with open(fname) as f:
+            lines = [ln for ln in f.read().split("\n") if ln]
+        if len(lines) != 1:
+            sys.stderr.write("# Warning: The number of processes does not match the number "
+                             "of saved random number generators.\n"
+                             "           The old states are not restored.\n")
+            return
+        saved = json.loads(lines[0])
+        if self._keyed and int(saved["seed"]) != self.seed:
+            sys.stderr.write("# Warning: the saved seed %d differs from seed %d, which keys "
+                             "the Langevin noise of systems already created from this RNG.\n"
+                             "           The old states are not restored.\n"
+                             % (int(saved["seed"]), self.seed))
+            return
+        self.seed = int(saved["seed"])
+        g = np.random.Generator(np.random.PCG64(self.seed))
+        g.bit_generator.state = saved["state"]
+        self._g = g
 
 
 class OrthorhombicBC:
@@ -286,6 +322,8 @@ class DomainDecomposition:
         box = np.ascontiguousarray(system.bc.boxL, np.float64)
         cg = np.ascontiguousarray(self._cellGrid, np.int32)
         seed = system.rng.get_seed() if system.rng is not None else 12345
+        if system.rng is not None:
+            system.rng._keyed = True
         call(self._lib, "espp_system_create", dptr(box), float(system.skin), i32ptr(cg), prec,
              int(seed) & 0xFFFFFFFFFFFFFFFF, ctypes.byref(self._h))
         self._types = {}
@@ -353,14 +391,23 @@ class DomainDecomposition:
         return len(self._types)
 
     def modifyParticle(self, pid, prop, value):
+        """Storage.modifyParticle (src/storage/Storage.py:374-400) for 'pos', 'v' and
+        'img'.  As there, a new position is taken as unfolded: the image is reset."""
         ids = np.array([int(pid)], np.int64)
+        prop = prop.lower()
+        if prop == "img":
+            img = np.ascontiguousarray(tuple(value), np.int32)
+            call(self._lib, "espp_set_images", self._h, 1, i64ptr(ids), i32ptr(img))
+            return
         v = np.ascontiguousarray(tuple(value), np.float64)
         if prop == "pos":
             call(self._lib, "espp_set_particles", self._h, 1, i64ptr(ids), dptr(v), None)
+            zero = np.zeros(3, np.int32)
+            call(self._lib, "espp_set_images", self._h, 1, i64ptr(ids), i32ptr(zero))
         elif prop == "v":
             call(self._lib, "espp_set_particles", self._h, 1, i64ptr(ids), None, dptr(v))
         else:
-            raise ValueError("only 'pos' and 'v' can be modified on the GPU storage")
+            raise ValueError("only 'pos', 'v' and 'img' can be modified on the GPU storage")
 
     def getCellGrid(self):
         return self._cellGrid
@@ -388,6 +435,13 @@ class DomainDecomposition:
         ids = np.ascontiguousarray(ids, np.int64)
         v = np.ascontiguousarray(vel, np.float64).reshape(-1)
         call(self._lib, "espp_set_particles", self._h, len(ids), i64ptr(ids), None, dptr(v))
+
+    def setImages(self, ids, img):
+        """Image counts of many particles at once (modifyParticle(pid, 'img', ...) for
+        each), e.g. to restore a checkpoint written from getAll()."""
+        ids = np.ascontiguousarray(ids, np.int64)
+        im = np.ascontiguousarray(img, np.int32).reshape(-1)
+        call(self._lib, "espp_set_images", self._h, len(ids), i64ptr(ids), i32ptr(im))
 
 
 class VerletList:

@@ -1611,7 +1611,7 @@ int espp_set_particles(espp_system* s, int64_t n, const int64_t* ids, const doub
       cuda_check(cudaMemcpyAsync(s->stVel, vel, sizeof(double) * 3 * n, cudaMemcpyHostToDevice,
                                  s->st), "upload");
     launch_set_by_id(s->view(), (int)n, s->stIds, pos ? s->stPos : nullptr,
-                     vel ? s->stVel : nullptr, s->st);
+                     vel ? s->stVel : nullptr, nullptr, s->st);
     unsigned e = read_err(s);
     if (e & kErrIdRange) {
       cuda_check(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->st), "memset");
@@ -1619,6 +1619,26 @@ int espp_set_particles(espp_system* s, int64_t n, const int64_t* ids, const doub
     }
     // new positions: the reference re-sorts before the next force evaluation
     if (pos) s->resortFlag = true;
+  });
+}
+
+int espp_set_images(espp_system* s, int64_t n, const int64_t* ids, const int32_t* img) {
+  return guard([&] {
+    checked(s);
+    if (n <= 0) return;
+    if (!ids || !img) raise(ESPP_EINVAL, "null id or image array");
+    ensure_id_map(s);
+    ensure_stage(s, n);
+    cuda_check(cudaMemcpyAsync(s->stIds, ids, sizeof(int64_t) * n, cudaMemcpyHostToDevice,
+                               s->st), "upload ids");
+    cuda_check(cudaMemcpyAsync(s->stImg, img, sizeof(int32_t) * 3 * n, cudaMemcpyHostToDevice,
+                               s->st), "upload");
+    launch_set_by_id(s->view(), (int)n, s->stIds, nullptr, nullptr, s->stImg, s->st);
+    unsigned e = read_err(s);
+    if (e & kErrIdRange) {
+      cuda_check(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->st), "memset");
+      raise(ESPP_EINVAL, "unknown particle id");
+    }
   });
 }
 

@@ -246,7 +246,7 @@ void make_float_table(const LJTable& t, LJPairF* out);
 int observable_blocks(int n);
 int scan_tiles(int ncells);
 void launch_set_by_id(const DevView& d, int n, const int64_t* ids, const double* pos,
-                      const double* vel, cudaStream_t st);
+                      const double* vel, const int32_t* img, cudaStream_t st);
 void launch_get_by_id(const DevView& d, int n, const int64_t* ids, double* pos, double* vel,
                       double* force, int32_t* img, cudaStream_t st);
 

@@ -1937,7 +1937,7 @@ __global__ void k_pair_write(DevView d, const int64_t* offsets, int64_t* out) {
 // Particle state by id through the dense id map: scatter host rows into the sorted
 // arrays / gather them back out (Storage::lookupRealParticle on the device).
 __global__ void k_set_by_id(DevView d, int n, const int64_t* ids, const double* pos,
-                            const double* vel) {
+                            const double* vel, const int32_t* img) {
   const ParticleArrays a = d.pa[0];
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
@@ -1950,6 +1950,7 @@ __global__ void k_set_by_id(DevView d, int n, const int64_t* ids, const double* 
   for (int c = 0; c < 3; ++c) {
     if (pos) a.x[(size_t)c * d.cap + k] = pos[3 * (size_t)r + c];
     if (vel) a.v[(size_t)c * d.cap + k] = vel[3 * (size_t)r + c];
+    if (img) a.img[(size_t)c * d.cap + k] = img[3 * (size_t)r + c];
   }
   if (pos)
     d.posq[k] = fixed_coords(d, a.x[k], a.x[(size_t)d.cap + k], a.x[2 * (size_t)d.cap + k],
@@ -2288,8 +2289,8 @@ void launch_pair_write(const DevView& d, const int64_t* offsets, int64_t* out,
 int observable_blocks(int n) { return blocks_for(n > 0 ? n : 1); }
 
 void launch_set_by_id(const DevView& d, int n, const int64_t* ids, const double* pos,
-                      const double* vel, cudaStream_t st) {
-  if (n > 0) k_set_by_id<<<blocks_for(n), kBlock, 0, st>>>(d, n, ids, pos, vel);
+                      const double* vel, const int32_t* img, cudaStream_t st) {
+  if (n > 0) k_set_by_id<<<blocks_for(n), kBlock, 0, st>>>(d, n, ids, pos, vel, img);
 }
 
 void launch_get_by_id(const DevView& d, int n, const int64_t* ids, double* pos, double* vel,

@@ -98,6 +98,9 @@ ESPP_API int espp_get_particles(espp_system* s, int64_t n, const int64_t* ids, d
 /* Particle setters for existing ids (pos/vel may be NULL). */
 ESPP_API int espp_set_particles(espp_system* s, int64_t n, const int64_t* ids, const double* pos,
                        const double* vel);
+/* Image counts (3 n int32) of existing ids: Storage.modifyParticle(pid, 'img', value)
+ * (src/storage/Storage.py:385).  Positions are left as they are. */
+ESPP_API int espp_set_images(espp_system* s, int64_t n, const int64_t* ids, const int32_t* img);
 
 /* ---- VerletList (src/VerletList.cpp:196-270, :274-450) ----------------------------
  * cutoff is the interaction cutoff; the list holds pairs with |d| <= cutoff + skin.

@@ -1295,6 +1295,17 @@ int espp_set_particles(espp_system* s, int64_t n, const int64_t* ids, const doub
   return ESPP_OK;
 }
 
+int espp_set_images(espp_system* s, int64_t n, const int64_t* ids, const int32_t* img) {
+  CHECK_S(s);
+  if (n > 0 && (!ids || !img)) return fail(ESPP_EINVAL, "null id or image array");
+  for (int64_t i = 0; i < n; ++i) {
+    Particle* p = lookup(s, ids[i]);
+    if (!p) return fail(ESPP_EINVAL, "unknown particle id " + std::to_string(ids[i]));
+    for (int k = 0; k < 3; ++k) p->img[k] = img[3 * i + k];
+  }
+  return ESPP_OK;
+}
+
 int espp_vl_create(espp_system* s, double cutoff, int64_t nexcl, const int64_t* excl) {
   CHECK_S(s);
   s->has_vl = true;

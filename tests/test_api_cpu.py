@@ -65,3 +65,39 @@ def test_real3d_and_bc():
 def test_precision_selection():
     with pytest.raises(ValueError):
         espressopp.set_default_precision("half")
+
+
+def test_rng_save_and_load_state(tmp_path, monkeypatch, capsys):
+    """RNG.saveState(step) writes rng.<step>; loadState brings the draws back to that
+    point (RNG.cpp:86-138), and a file for another number of ranks is refused."""
+    monkeypatch.chdir(tmp_path)
+    rng = espressopp.esutil.RNG(42)
+    [rng() for _ in range(7)]
+    rng.saveState(1000)
+    after = [rng() for _ in range(5)] + [rng(10), rng.normal()]
+    other = espressopp.esutil.RNG(42)
+    other.loadState("rng.1000")
+    assert [other() for _ in range(5)] + [other(10), other.normal()] == after
+    fresh = espressopp.esutil.RNG(7)
+    fresh.loadState("rng.1000")
+    assert fresh.get_seed() == 42 and fresh() == after[0]
+    (tmp_path / "rng.two").write_text(open("rng.1000").read() * 2)
+    keep = espressopp.esutil.RNG(3)
+    first = espressopp.esutil.RNG(3)()
+    keep.loadState("rng.two")
+    assert keep.get_seed() == 3 and keep() == first
+    assert "number of processes does not match" in capsys.readouterr().err
+
+
+def test_potentials_pickle():
+    """Potentials survive pickling with their parameters (LennardJones_pickle,
+    LennardJones.hpp:176-191)."""
+    import pickle
+    for pot in (espressopp.interaction.LennardJones(1.2, 0.9, 2.5),
+                espressopp.interaction.LennardJonesCapped(1.0, 1.0, 2.5, caprad=0.9),
+                espressopp.interaction.FENE(K=25.0, r0=0.1, rMax=1.4),
+                espressopp.interaction.Cosine(K=1.5, theta0=3.0)):
+        q = pickle.loads(pickle.dumps(pot))
+        assert type(q) is type(pot) and vars(q) == vars(pot)
+    lj = pickle.loads(pickle.dumps(espressopp.interaction.LennardJones(1.2, 0.9, 2.5)))
+    assert lj.computeEnergy(2.5) == pytest.approx(0.0, abs=1e-15)
