@@ -347,6 +347,26 @@ struct espp_mlp {
   }
 };
 
+// ---- the vec twin's particle array (src/vec/ParticleArray.{hpp,cpp}) ------------------
+// SoA copy of every local cell (reals and ghosts), each cell padded to at least one spare
+// slot and then to whole 64-byte rows of doubles; padding slots sit at a far-away
+// position so that no distance test accepts them.
+constexpr size_t kVecWidth = 8;            // ESPP_VECTOR_WIDTH for double
+constexpr double kVecLargePos = 7.74099e150;  // large_pos (vec/include/simdconfig.hpp:60)
+inline size_t vecFit(size_t n) { return (n + kVecWidth - 1) / kVecWidth * kVecWidth; }
+
+struct VecArrays {
+  bool loaded = false;
+  std::vector<size_t> cellRange, sizes;  // first slot and particle count of each cell
+  std::vector<double> x, y, z, vx, vy, vz, fx, fy, fz, mass;
+  std::vector<int32_t> type;
+  // vec::VerletList::NeighborList: rows of neighbour slots per listed particle
+  std::vector<int> plist, nplist;
+  std::vector<std::pair<int, int>> prange;
+  std::vector<int> cj;                  // packed candidate slots of one cell's half shell
+  std::vector<double> cx, cy, cz;
+};
+
 struct espp_system {
   double L[3], invL[3], L2[3];
   double skin;
@@ -396,6 +416,9 @@ struct espp_system {
   int langPhase = 0;
   espp_mlp* mlp = nullptr;
   std::unordered_map<int64_t, std::array<double, 3>> facc;
+  bool vecMode = false;  // re-sorts load the SoA array and build the vec list
+  bool aosStale = false;  // a vec run left the AoS ghosts and pair list behind
+  VecArrays vec;
 };
 
 namespace {
@@ -629,8 +652,17 @@ void bondsRefresh(espp_system* s) {
   }
 }
 
+void vecLoad(espp_system* s);
+void vecRebuild(espp_system* s);
+
 void onParticlesChanged(espp_system* s) {
-  if (s->has_vl) vlRebuild(s);
+  if (s->vecMode) {
+    // StorageVec::loadCells, then vec::VerletList::rebuild (both on onParticlesChanged)
+    vecLoad(s);
+    if (s->has_vl) vecRebuild(s);
+  } else if (s->has_vl) {
+    vlRebuild(s);
+  }
   bondsRefresh(s);
 }
 
@@ -1137,6 +1169,7 @@ void integrate2(espp_system* s) {
 
 // VelocityVerlet::run (:63-169) with the Langevin runInit/recalc hooks (:179-214).
 int run(espp_system* s, int64_t nsteps) {
+  s->vec.loaded = false;
   double skinHalf = 0.5 * s->skin;
   s->nResorts = 0;
   if (s->lang_on) {
@@ -1171,6 +1204,307 @@ int run(espp_system* s, int64_t nsteps) {
     integrate2(s);
   }
   return ESPP_OK;
+}
+
+// ---- the vec twin of the step (src/vec/*), NVE Lennard-Jones --------------------------
+
+// ParticleArray::copyFrom (vec/ParticleArray.cpp:129-190) over all local cells in index
+// order: particle data, then padding slots at the far-away position.
+void vecLoad(espp_system* s) {
+  VecArrays& V = s->vec;
+  const size_t nc = s->cells.size();
+  V.cellRange.assign(nc + 1, 0);
+  V.sizes.assign(nc, 0);
+  size_t total = 0;
+  for (size_t c = 0; c < nc; ++c) {
+    V.cellRange[c] = total;
+    V.sizes[c] = s->cells[c].p.size();
+    total += vecFit(V.sizes[c] + 1);
+  }
+  V.cellRange[nc] = total;
+  for (auto* a : {&V.x, &V.y, &V.z}) a->assign(total, kVecLargePos);
+  for (auto* a : {&V.vx, &V.vy, &V.vz, &V.fx, &V.fy, &V.fz}) a->assign(total, 0.0);
+  V.mass.assign(total, 1.0);
+  V.type.assign(total, 0);
+  for (size_t c = 0; c < nc; ++c) {
+    const auto& P = s->cells[c].p;
+    const size_t o = V.cellRange[c];
+    for (size_t k = 0; k < P.size(); ++k) {
+      V.x[o + k] = P[k].r[0];
+      V.y[o + k] = P[k].r[1];
+      V.z[o + k] = P[k].r[2];
+      V.vx[o + k] = P[k].v[0];
+      V.vy[o + k] = P[k].v[1];
+      V.vz[o + k] = P[k].v[2];
+      V.fx[o + k] = P[k].f[0];
+      V.fy[o + k] = P[k].f[1];
+      V.fz[o + k] = P[k].f[2];
+      V.mass[o + k] = P[k].mass;
+      V.type[o + k] = P[k].type;
+    }
+  }
+  V.loaded = true;
+}
+
+// StorageVec::unloadCells: positions, velocities and forces back to the real particles.
+void vecUnload(espp_system* s) {
+  VecArrays& V = s->vec;
+  if (!V.loaded) return;
+  for (int c : s->realCells) {
+    auto& P = s->cells[c].p;
+    const size_t o = V.cellRange[c];
+    for (size_t k = 0; k < P.size(); ++k) {
+      P[k].r[0] = V.x[o + k];
+      P[k].r[1] = V.y[o + k];
+      P[k].r[2] = V.z[o + k];
+      P[k].v[0] = V.vx[o + k];
+      P[k].v[1] = V.vy[o + k];
+      P[k].v[2] = V.vz[o + k];
+      P[k].f[0] = V.fx[o + k];
+      P[k].f[1] = V.fy[o + k];
+      P[k].f[2] = V.fz[o + k];
+    }
+  }
+}
+
+// vec::VerletList::NeighborList::rebuildMulti<PACK_NEIGHBORS = 1, ARRAY_SELF = 1>
+// (vec/VerletList.cpp:129-432): per real cell, the half-shell neighbour cells' particles
+// are packed into one candidate array (padded to whole rows with a padding slot); each
+// particle's row holds the later particles of its own cell's data range and the accepted
+// candidates, and is padded to whole rows with the last neighbour cell's first padding
+// slot.  Exclusions are not applied (the reference builds the vec list without them).
+void vecRebuild(espp_system* s) {
+  VecArrays& V = s->vec;
+  s->vl_cutVerlet = s->vl_cut + s->skin;
+  s->vl_cutsq = s->vl_cutVerlet * s->vl_cutVerlet;
+  const double cutsq = s->vl_cutsq;
+  for (int ci : s->realCells)
+    for (const Particle& p : s->cells[ci].p) s->max_type = std::max(s->max_type, p.type);
+  V.plist.clear();
+  V.prange.clear();
+  V.nplist.clear();
+  for (int ci : s->realCells) {
+    const Cell& cell = s->cells[ci];
+    std::vector<int> half;
+    for (const NeighborCell& nc : cell.nbrs)
+      if (!nc.useForAllPairs) half.push_back(nc.cell);
+    V.cj.clear();
+    for (int nc : half)
+      for (size_t k = 0; k < V.sizes[nc]; ++k) V.cj.push_back((int)(V.cellRange[nc] + k));
+    const int lastNbr = half.back();
+    const int padding = (int)(V.cellRange[lastNbr] + V.sizes[lastNbr]);
+    while (V.cj.size() % kVecWidth) V.cj.push_back(padding);
+    V.cx.resize(V.cj.size());
+    V.cy.resize(V.cj.size());
+    V.cz.resize(V.cj.size());
+    for (size_t ii = 0; ii < V.cj.size(); ++ii) {
+      V.cx[ii] = V.x[V.cj[ii]];
+      V.cy[ii] = V.y[V.cj[ii]];
+      V.cz[ii] = V.z[V.cj[ii]];
+    }
+    const size_t start = V.cellRange[ci], end = start + V.sizes[ci];
+    const size_t dataEnd = V.cellRange[ci + 1];
+    for (size_t p = start; p < end; ++p) {
+      const double px = V.x[p], py = V.y[p], pz = V.z[p];
+      const size_t rowStart = V.nplist.size();
+      for (size_t np = start; np < dataEnd; ++np) {
+        const double dx = px - V.x[np], dy = py - V.y[np], dz = pz - V.z[np];
+        const double dsq = dx * dx + dy * dy + dz * dz;
+        if (p < np && dsq <= cutsq) V.nplist.push_back((int)np);
+      }
+      for (size_t ii = 0; ii < V.cj.size(); ++ii) {
+        const double dx = px - V.cx[ii], dy = py - V.cy[ii], dz = pz - V.cz[ii];
+        const double dsq = dx * dx + dy * dy + dz * dz;
+        if (!(dsq > cutsq)) V.nplist.push_back(V.cj[ii]);
+      }
+      const size_t added = V.nplist.size() - rowStart;
+      if (added) {
+        while ((V.nplist.size() - rowStart) % kVecWidth) V.nplist.push_back(padding);
+        V.plist.push_back((int)p);
+        V.prange.push_back({(int)rowStart, (int)V.nplist.size()});
+      }
+    }
+  }
+  s->builds++;
+}
+
+// StorageVec::updateGhostsVec / collectGhostForcesVec (vec/storage/DomainDecomposition.cpp:
+// 168-171, copyRealsToGhostsIntra :270-330): whole data ranges of the communication cells,
+// x, y, z in turn (ghost corners from already-filled frames); forces back in reverse.
+void vecGhosts(espp_system* s, bool realToGhosts) {
+  VecArrays& V = s->vec;
+  for (int _coord = 0; _coord < 3; ++_coord) {
+    const int coord = realToGhosts ? _coord : 2 - _coord;
+    for (int lr = 0; lr < 2; ++lr) {
+      const int dir = 2 * coord + lr;
+      double shift[3] = {0.0, 0.0, 0.0};
+      shift[coord] = (lr == 0 ? 1.0 : -1.0) * s->L[coord];
+      const auto& R = s->commReals[dir];
+      const auto& G = s->commGhosts[dir];
+      for (size_t i = 0; i < G.size(); ++i) {
+        const size_t r0 = V.cellRange[R[i]], g0 = V.cellRange[G[i]];
+        const size_t n = V.cellRange[R[i] + 1] - r0;
+        for (size_t k = 0; k < n; ++k) {
+          if (realToGhosts) {
+            V.x[g0 + k] = V.x[r0 + k] + shift[0];
+            V.y[g0 + k] = V.y[r0 + k] + shift[1];
+            V.z[g0 + k] = V.z[r0 + k] + shift[2];
+          } else {
+            V.fx[r0 + k] += V.fx[g0 + k];
+            V.fy[r0 + k] += V.fy[g0 + k];
+            V.fz[r0 + k] += V.fz[g0 + k];
+          }
+        }
+      }
+    }
+  }
+}
+
+// vec::interaction::VerletListLennardJones::addForces_impl<ONETYPE, N3L = true>
+// (vec/interaction/VerletListLennardJones.hpp:130-241): a particle's row sums into
+// registers, the partner's force is decremented at once.
+void vecLJForces(espp_system* s) {
+  VecArrays& V = s->vec;
+  const int nt = s->max_type + 1;
+  std::vector<double> ff1((size_t)nt * nt, 0.0), ff2((size_t)nt * nt, 0.0),
+      rcsq((size_t)nt * nt, -1.0);
+  for (int a = 0; a < nt; ++a)
+    for (int b = 0; b < nt; ++b) {
+      const LJParams* P = ljFor(s, a, b);
+      if (!P) continue;
+      ff1[(size_t)a * nt + b] = P->ff1;
+      ff2[(size_t)a * nt + b] = P->ff2;
+      rcsq[(size_t)a * nt + b] = P->rcsq;
+    }
+  for (size_t ip = 0; ip < V.plist.size(); ++ip) {
+    const int p = V.plist[ip];
+    const size_t pl = (size_t)std::min(V.type[p], nt - 1) * nt;
+    const double px = V.x[p], py = V.y[p], pz = V.z[p];
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    for (int in = V.prange[ip].first; in < V.prange[ip].second; ++in) {
+      const int np = V.nplist[in];
+      const double dx = px - V.x[np], dy = py - V.y[np], dz = pz - V.z[np];
+      const size_t t = pl + (size_t)std::min(V.type[np], nt - 1);
+      const double dsq = dx * dx + dy * dy + dz * dz;
+      if (dsq <= rcsq[t]) {
+        const double frac2 = 1.0 / dsq;
+        const double frac6 = frac2 * frac2 * frac2;
+        double ffactor = ff1[t] * frac6 - ff2[t];
+        ffactor = frac6 * ffactor * frac2;
+        fx += dx * ffactor;
+        fy += dy * ffactor;
+        fz += dz * ffactor;
+        V.fx[np] -= dx * ffactor;
+        V.fy[np] -= dy * ffactor;
+        V.fz[np] -= dz * ffactor;
+      }
+    }
+    V.fx[p] += fx;
+    V.fy[p] += fy;
+    V.fz[p] += fz;
+  }
+}
+
+// vec VelocityVerletBase::updateForces (vec/integrator/VelocityVerlet.cpp:228-245).
+void vecUpdateForces(espp_system* s) {
+  VecArrays& V = s->vec;
+  vecGhosts(s, true);
+  for (auto* a : {&V.fx, &V.fy, &V.fz}) std::fill(a->begin(), a->end(), 0.0);
+  vecLJForces(s);
+  vecGhosts(s, false);
+}
+
+// vec VelocityVerletBase::integrate1 / integrate2 (:167-207), real particles only.
+double vecIntegrate1(espp_system* s) {
+  VecArrays& V = s->vec;
+  double maxSq = 0.0;
+  for (int c : s->realCells)
+    for (size_t p = V.cellRange[c]; p < V.cellRange[c] + V.sizes[c]; ++p) {
+      const double dtfm = 0.5 * s->dt / V.mass[p];
+      V.vx[p] += dtfm * V.fx[p];
+      V.vy[p] += dtfm * V.fy[p];
+      V.vz[p] += dtfm * V.fz[p];
+      const double dx = V.vx[p] * s->dt, dy = V.vy[p] * s->dt, dz = V.vz[p] * s->dt;
+      V.x[p] += dx;
+      V.y[p] += dy;
+      V.z[p] += dz;
+      maxSq = std::max(maxSq, dx * dx + dy * dy + dz * dz);
+    }
+  return maxSq;
+}
+
+void vecIntegrate2(espp_system* s) {
+  VecArrays& V = s->vec;
+  for (int c : s->realCells)
+    for (size_t p = V.cellRange[c]; p < V.cellRange[c] + V.sizes[c]; ++p) {
+      const double dtfm = 0.5 * s->dt / V.mass[p];
+      V.vx[p] += dtfm * V.fx[p];
+      V.vy[p] += dtfm * V.fy[p];
+      V.vz[p] += dtfm * V.fz[p];
+    }
+  s->step++;
+}
+
+// vec VelocityVerletBase::run (vec/integrator/VelocityVerlet.cpp:67-165): NVE with
+// Lennard-Jones pairs only.
+int vecRun(espp_system* s, int64_t nsteps) {
+  if (!s->has_vl) return fail(ESPP_ESTATE, "the vec step needs a Verlet list");
+  if (s->fene_on || s->cos_on || s->tabAngle || !s->tabPair.empty() || s->tabBondOn ||
+      s->mlp || s->lang_on || s->capMode != ESPP_CAP_OFF)
+    return fail(ESPP_ESTATE, "the vec step restates NVE Lennard-Jones only");
+  for (const auto& kv : s->lj)
+    if (kv.second.set && kv.second.caprad > 0)
+      return fail(ESPP_ESTATE, "the vec step restates uncapped Lennard-Jones only");
+  const double skinHalf = 0.5 * s->skin;
+  s->nResorts = 0;
+  s->vecMode = true;
+  s->vlPairs.clear();  // points into cells that the re-sorts below rearrange
+  s->bondPtrs.clear();
+  s->aosStale = true;
+  if (s->resortFlag) {
+    int rc = decompose(s);
+    if (rc) return rc;
+    s->maxDist = 0.0;
+    s->resortFlag = false;
+  } else if (!s->vec.loaded) {
+    // the array and list that the reference's vec storage and VerletList set up when they
+    // are created; the list was counted when it was created
+    vecLoad(s);
+    const int64_t builds = s->builds;
+    vecRebuild(s);
+    s->builds = builds;
+  }
+  vecUpdateForces(s);
+  for (int64_t i = 0; i < nsteps; ++i) {
+    s->maxDist += std::sqrt(vecIntegrate1(s));
+    if (s->maxDist > skinHalf) s->resortFlag = true;
+    if (s->resortFlag) {
+      vecUnload(s);
+      int rc = decompose(s);
+      if (rc) return rc;
+      s->maxDist = 0.0;
+      s->resortFlag = false;
+      s->nResorts++;
+    }
+    vecUpdateForces(s);
+    vecIntegrate2(s);
+  }
+  vecUnload(s);
+  s->vecMode = false;
+  s->aosStale = true;  // the array and vec list stay loaded for the next vec run
+  return ESPP_OK;
+}
+
+// Before anything reads the AoS pair list or ghosts after a vec run: ghost positions
+// refreshed and the pair list rebuilt from the current positions (not counted as a build).
+void ensureAos(espp_system* s) {
+  if (!s->aosStale) return;
+  s->aosStale = false;
+  ghostComm(s, true, false);
+  const int64_t builds = s->builds;
+  if (s->has_vl) vlRebuild(s);
+  s->builds = builds;
+  bondsRefresh(s);
 }
 
 #define CHECK_S(s)                                              \
@@ -1229,6 +1563,8 @@ int espp_set_skin(espp_system* s, double skin) {
 int espp_add_particles(espp_system* s, int64_t n, const int64_t* id, const int32_t* type,
                        const double* mass, const double* pos, const double* vel) {
   CHECK_S(s);
+  ensureAos(s);
+  s->vec.loaded = false;  // the AoS side changes: the vec array reloads
   if (n < 0 || (n > 0 && (!id || !pos))) return fail(ESPP_EINVAL, "bad particle arrays");
   for (int64_t i = 0; i < n; ++i) {
     if (s->where.count(id[i])) return fail(ESPP_EINVAL, "duplicate particle id");
@@ -1251,6 +1587,8 @@ int espp_add_particles(espp_system* s, int64_t n, const int64_t* id, const int32
 
 int espp_decompose(espp_system* s) {
   CHECK_S(s);
+  ensureAos(s);
+  s->vec.loaded = false;  // the AoS side changes: the vec array reloads
   int rc = decompose(s);
   if (rc) return rc;
   s->maxDist = 0.0;
@@ -1283,6 +1621,8 @@ int espp_get_particles(espp_system* s, int64_t n, const int64_t* ids, double* po
 int espp_set_particles(espp_system* s, int64_t n, const int64_t* ids, const double* pos,
                        const double* vel) {
   CHECK_S(s);
+  ensureAos(s);
+  s->vec.loaded = false;  // the AoS side changes: the vec array reloads
   for (int64_t i = 0; i < n; ++i) {
     Particle* p = lookup(s, ids[i]);
     if (!p) return fail(ESPP_EINVAL, "unknown particle id " + std::to_string(ids[i]));
@@ -1297,6 +1637,8 @@ int espp_set_particles(espp_system* s, int64_t n, const int64_t* ids, const doub
 
 int espp_set_images(espp_system* s, int64_t n, const int64_t* ids, const int32_t* img) {
   CHECK_S(s);
+  ensureAos(s);
+  s->vec.loaded = false;  // the AoS side changes: the vec array reloads
   if (n > 0 && (!ids || !img)) return fail(ESPP_EINVAL, "null id or image array");
   for (int64_t i = 0; i < n; ++i) {
     Particle* p = lookup(s, ids[i]);
@@ -1317,6 +1659,7 @@ int espp_vl_create(espp_system* s, double cutoff, int64_t nexcl, const int64_t* 
 
 int espp_vl_rebuild(espp_system* s) {
   CHECK_S(s);
+  ensureAos(s);
   if (!s->has_vl) return fail(ESPP_ESTATE, "no Verlet list");
   vlRebuild(s);
   return ESPP_OK;
@@ -1324,12 +1667,14 @@ int espp_vl_rebuild(espp_system* s) {
 
 int espp_vl_size(espp_system* s, int64_t* npairs) {
   CHECK_S(s);
+  ensureAos(s);
   *npairs = (int64_t)s->vlPairs.size();
   return ESPP_OK;
 }
 
 int espp_vl_pairs(espp_system* s, int64_t cap, int64_t* pairs, int64_t* npairs) {
   CHECK_S(s);
+  ensureAos(s);
   std::vector<std::pair<int64_t, int64_t>> v;
   v.reserve(s->vlPairs.size());
   for (auto& pr : s->vlPairs) {
@@ -1625,6 +1970,7 @@ int espp_mlp_attach(espp_system* s, espp_mlp* m) {
 
 int espp_mlp_descriptors(espp_system* s, int64_t n, const int64_t* ids, double* G) {
   CHECK_S(s);
+  ensureAos(s);
   if (!s->mlp || !s->has_vl) return fail(ESPP_ESTATE, "no learned potential on a Verlet list");
   ghostComm(s, true, false);
   MlpEval ev;
@@ -1640,6 +1986,7 @@ int espp_mlp_descriptors(espp_system* s, int64_t n, const int64_t* ids, double* 
 int espp_mlp_fm_grad(espp_system* s, int64_t n, const int64_t* ids, const double* fref,
                      double* loss, double* grad) {
   CHECK_S(s);
+  ensureAos(s);
   if (!s->mlp || !s->has_vl) return fail(ESPP_ESTATE, "no learned potential on a Verlet list");
   ghostComm(s, true, false);
   MlpEval ev;
@@ -1677,7 +2024,15 @@ int espp_mlp_adam_step(espp_mlp* m, double lr, double beta1, double beta2, doubl
 
 int espp_run(espp_system* s, int64_t nsteps) {
   CHECK_S(s);
+  ensureAos(s);
   return run(s, nsteps);
+}
+
+// The vec twin of VelocityVerlet::run (NVE Lennard-Jones): the reference's SoA CPU path,
+// a second CPU baseline; not part of the GPU library's ABI.
+int espp_vec_run(espp_system* s, int64_t nsteps) {
+  CHECK_S(s);
+  return vecRun(s, nsteps);
 }
 
 int espp_num_resorts(espp_system* s, int64_t* n) {
@@ -1694,6 +2049,7 @@ int espp_timers(espp_system* s, double t[10]) {
 
 int espp_energy(espp_system* s, int32_t which, double* e) {
   CHECK_S(s);
+  ensureAos(s);
   double es = 0.0;
   if (which == ESPP_IA_LJ) {
     for (auto& pr : s->vlPairs) {
@@ -1774,6 +2130,7 @@ int espp_energy(espp_system* s, int32_t which, double* e) {
 }
 
 static int virialImpl(espp_system* s, int32_t which, double* wsc, double w6[6]) {
+  ensureAos(s);
   double w = 0.0;
   double t[6] = {0, 0, 0, 0, 0, 0};
   auto acc = [&](const double d[3], const double f[3]) {

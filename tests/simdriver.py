@@ -36,6 +36,7 @@ def oracle_lib():
             "espp_oracle_philox": (ctypes.c_int32, [U, U, U]),
             "espp_oracle_lj_eval": (ctypes.c_int32, [ctypes.c_double] * 5 + [D, D, D]),
             "espp_oracle_fene_eval": (ctypes.c_int32, [ctypes.c_double] * 5 + [D, D, D]),
+            "espp_vec_run": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int64]),
         })
         _oracle = lib
     return _oracle

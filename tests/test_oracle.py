@@ -322,3 +322,66 @@ def test_polymer_melt_step0_angle_energy_matches_result_dat():
     assert round(2 * 1.5 * len(angles) - e, 3) == gold["eangle"]
     # the angular virial vanishes: d12.F12 + d32.F32 = 0 for any angular force
     assert abs(s.virial(_abi.IA_COSINE)) < 1e-6
+
+
+def _lj2048_nve(lib_run_vec):
+    pid, pos, vel, box = load_lj2048()
+    s = Sim(oracle_lib(), box, 0.3, cell_grid(box, 2.5, 0.3))
+    s.add(pid + 1, pos, vel)
+    s.decompose()
+    s.vl(2.5)
+    s.lj(0, 0, 1.0, 1.0, 2.5, 0.0)
+    s.integrator(0.005)
+    return s
+
+
+@pytest.mark.parametrize("steps", [10, 400])
+def test_vec_twin_matches_classic(steps):
+    """The vec twin (SoA cells padded to 64-byte rows, packed half-shell candidates,
+    padded neighbour rows, N3L force rows) against the classic AoS step on the 2048-particle
+    fluid with velocities: the reference's test_vec_lennard_jones.py runs 10 NVE steps and
+    asks |dx|^2 = 0 to 8 places; 400 steps take many re-sorts through both paths."""
+    pid, pos, vel, box = load_lj2048()
+    ids = pid + 1
+    classic, vec = _lj2048_nve(False), _lj2048_nve(True)
+    classic.run(steps)
+    _abi.call(vec.lib, "espp_vec_run", vec.h, steps)
+    a, b = classic.particles(ids), vec.particles(ids)
+    unf = lambda p: p[0] + p[3] * box
+    d2 = np.sum((unf(a) - unf(b)) ** 2, axis=1)
+    assert np.max(d2) < (5e-9 if steps == 10 else 1e-12)
+    assert np.max(np.abs(a[1] - b[1])) < 1e-6
+    assert vec.step() == classic.step() == steps
+    assert vec.num_resorts() == classic.num_resorts()
+    if steps == 400:
+        assert classic.num_resorts() > 5
+        assert vec.builds() == classic.builds()
+    # the AoS side is consistent after a vec run: energies over the rebuilt pair list
+    assert vec.energy(_abi.IA_LJ) == pytest.approx(classic.energy(_abi.IA_LJ), rel=1e-9)
+
+
+def test_vec_twin_refuses_what_it_does_not_restate():
+    pid, pos, vel, box = load_lj2048()
+    s = _lj2048_nve(True)
+    s.langevin(1.0, 1.0)
+    with pytest.raises(RuntimeError, match="NVE Lennard-Jones only"):
+        _abi.call(s.lib, "espp_vec_run", s.h, 1)
+
+
+def test_vec_twin_runs_interleave_with_classic_runs():
+    """Consecutive vec runs keep their SoA array and list; a classic run after them, and
+    observables in between, see the particles where the vec run left them."""
+    pid, pos, vel, box = load_lj2048()
+    ids = pid + 1
+    classic, vec = _lj2048_nve(False), _lj2048_nve(True)
+    for n in (150, 150):
+        classic.run(n)
+        _abi.call(vec.lib, "espp_vec_run", vec.h, n)
+        assert vec.energy(_abi.IA_LJ) == pytest.approx(classic.energy(_abi.IA_LJ), rel=1e-9)
+        assert vec.vl_size() > 0
+    classic.run(50)
+    vec.run(50)
+    a, b = classic.particles(ids), vec.particles(ids)
+    assert np.max(np.abs((a[0] + a[3] * box) - (b[0] + b[3] * box))) < 1e-8
+    assert vec.step() == classic.step() == 350
+    assert vec.builds() == classic.builds()
