@@ -6,7 +6,7 @@ import ctypes
 import numpy as np
 
 from ._abi import call
-from .core import Tensor
+from .core import Real3D, Tensor
 
 
 class _Observable:
@@ -87,15 +87,34 @@ class RadialDistrF(_Observable):
 class Configuration:
     """One snapshot (analysis/Configuration.cpp:103-240): values by particle id."""
 
-    def __init__(self, ids, xyz):
+    def __init__(self, ids, xyz, vel=None, force=None, radius=None):
         self._ids = [int(i) for i in ids]
         self._index = {pid: k for k, pid in enumerate(self._ids)}
-        self._xyz = np.asarray(xyz, np.float64).reshape(-1, 3)
+        self._xyz = None if xyz is None else np.asarray(xyz, np.float64).reshape(-1, 3)
+        self._vel = None if vel is None else np.asarray(vel, np.float64).reshape(-1, 3)
+        self._frc = None if force is None else np.asarray(force, np.float64).reshape(-1, 3)
+        self._rad = None if radius is None else np.asarray(radius, np.float64).reshape(-1)
+
+    def _row(self, a, pid, what):
+        if a is None:
+            raise RuntimeError("configuration has no %s" % what)
+        return Real3D(a[self._index[int(pid)]])
 
     def getCoordinates(self, pid):
-        return tuple(float(v) for v in self._xyz[self._index[int(pid)]])
+        return self._row(self._xyz, pid, "coordinates")
 
     __getitem__ = getCoordinates
+
+    def getVelocities(self, pid):
+        return self._row(self._vel, pid, "velocities")
+
+    def getForces(self, pid):
+        return self._row(self._frc, pid, "forces")
+
+    def getRadius(self, pid):
+        if self._rad is None:
+            raise RuntimeError("configuration has no radius")
+        return float(self._rad[self._index[int(pid)]])
 
     def getIds(self):
         return list(self._ids)
@@ -106,6 +125,75 @@ class Configuration:
     @property
     def size(self):
         return len(self._ids)
+
+
+class Configurations(_Observable):
+    """analysis.Configurations(system, pos=True, vel=False, force=False, radius=False,
+    folded=True) (src/analysis/Configurations.{py,cpp}): a trajectory of snapshots of all
+    particles, kept on the host.  Positions are folded into the box (BC::foldPosition) or
+    unfolded with their images (BC::unfoldPosition).  `capacity` 0 keeps every snapshot;
+    otherwise the oldest is dropped before a new one is added.  `[n]` counts back from the
+    newest snapshot (Configurations::get); iteration runs from the oldest.  The radius is
+    the reference's default particle radius, 1.0, since the GPU storage holds none."""
+
+    def __init__(self, system, pos=True, vel=False, force=False, radius=False, folded=True):
+        _Observable.__init__(self, system)
+        self._pos, self._vel, self._force, self._radius = pos, vel, force, radius
+        self.folded = folded
+        self._confs = []
+        self._cap = 0
+
+    @property
+    def capacity(self):
+        return self._cap
+
+    @capacity.setter
+    def capacity(self, max_configs):
+        max_configs = int(max_configs)
+        if max_configs < 0:
+            return  # the reference logs an error and keeps its capacity
+        self._cap = max_configs
+        if max_configs and len(self._confs) > max_configs:
+            del self._confs[:len(self._confs) - max_configs]
+
+    @property
+    def size(self):
+        return len(self._confs)
+
+    def gather(self):
+        ids, pos, vel, frc, img = self._st().getAll()
+        xyz = None
+        if self._pos:
+            L = np.asarray(self.system.bc.boxL, np.float64)
+            if self.folded:
+                t = np.floor(pos * (1.0 / L))
+                xyz = pos - t * L
+            else:
+                xyz = pos + img * L
+        conf = Configuration(ids, xyz, vel if self._vel else None,
+                             frc if self._force else None,
+                             np.ones(len(ids)) if self._radius else None)
+        if self._cap and len(self._confs) >= self._cap:
+            del self._confs[0]
+        self._confs.append(conf)
+
+    def __getitem__(self, stackpos):
+        n = len(self._confs)
+        if 0 <= stackpos < n:
+            return self._confs[n - 1 - stackpos]
+        return None  # Configurations::get <out-of-range>: a null configuration
+
+    def back(self):
+        return self._confs[-1]
+
+    def all(self):
+        return list(self._confs)
+
+    def __iter__(self):
+        return iter(list(self._confs))
+
+    def clear(self):
+        self._confs = []
 
 
 class ConfigsParticleDecomp(_Observable):

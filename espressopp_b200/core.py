@@ -395,6 +395,8 @@ class DomainDecomposition:
         'img'.  As there, a new position is taken as unfolded: the image is reset."""
         ids = np.array([int(pid)], np.int64)
         prop = prop.lower()
+        if prop not in ("pos", "v", "img"):
+            raise ValueError("only 'pos', 'v' and 'img' can be modified on the GPU storage")
         if prop == "img":
             img = np.ascontiguousarray(tuple(value), np.int32)
             call(self._lib, "espp_set_images", self._h, 1, i64ptr(ids), i32ptr(img))
@@ -404,10 +406,8 @@ class DomainDecomposition:
             call(self._lib, "espp_set_particles", self._h, 1, i64ptr(ids), dptr(v), None)
             zero = np.zeros(3, np.int32)
             call(self._lib, "espp_set_images", self._h, 1, i64ptr(ids), i32ptr(zero))
-        elif prop == "v":
-            call(self._lib, "espp_set_particles", self._h, 1, i64ptr(ids), None, dptr(v))
         else:
-            raise ValueError("only 'pos', 'v' and 'img' can be modified on the GPU storage")
+            call(self._lib, "espp_set_particles", self._h, 1, i64ptr(ids), None, dptr(v))
 
     def getCellGrid(self):
         return self._cellGrid

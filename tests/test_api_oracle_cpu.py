@@ -1,0 +1,133 @@
+"""Host logic of the Python mirror driven through the CPU oracle library, which exports
+the same C ABI as the CUDA library: here the mirror's own bookkeeping is under test, not
+the GPU kernels (those are checked against the oracle in the gpu-marked tests)."""
+import numpy as np
+import pytest
+
+import espressopp_b200 as espressopp
+from espressopp_b200 import _lib
+from simdriver import oracle_lib
+
+
+@pytest.fixture
+def on_oracle(monkeypatch):
+    monkeypatch.setattr(_lib, "_lib", oracle_lib())
+
+
+def _fluid(seed=5, n=1000):
+    x, y, z, Lx, Ly, Lz = espressopp.tools.lattice.createCubic(
+        n, 0.8442, perfect=False, RNG=espressopp.esutil.RNG(7))
+    system = espressopp.System()
+    system.rng = espressopp.esutil.RNG(seed)
+    system.bc = espressopp.bc.OrthorhombicBC(system.rng, (Lx, Ly, Lz))
+    system.skin = 0.3
+    cgrid = espressopp.tools.decomp.cellGrid((Lx, Ly, Lz), (1, 1, 1), 2.5, 0.3)
+    system.storage = espressopp.storage.DomainDecomposition(system, (1, 1, 1), cgrid)
+    system.storage.addParticles([[k, espressopp.Real3D(x[k], y[k], z[k])]
+                                 for k in range(len(x))], "id", "pos")
+    system.storage.decompose()
+    vl = espressopp.VerletList(system, cutoff=2.5)
+    lj = espressopp.interaction.VerletListLennardJones(vl)
+    lj.setPotential(0, 0, espressopp.interaction.LennardJones(1.0, 1.0, 2.5))
+    system.addInteraction(lj)
+    integ = espressopp.integrator.VelocityVerlet(system)
+    integ.dt = 0.005
+    lang = espressopp.integrator.LangevinThermostat(system)
+    lang.gamma = 1.0
+    lang.temperature = 1.0
+    integ.addExtension(lang)
+    return system, integ
+
+
+def test_configurations_trajectory(on_oracle):
+    """analysis.Configurations (Configurations.cpp:44-110): folded and unfolded positions,
+    velocities and forces by id, [n] counting back from the newest, capacity trimming."""
+    system, integ = _fluid()
+    L = np.asarray(system.bc.boxL)
+    folded = espressopp.analysis.Configurations(system, vel=True, force=True)
+    unfolded = espressopp.analysis.Configurations(system, folded=False, radius=True)
+    for _ in range(4):
+        integ.run(100)
+        folded.gather()
+        unfolded.gather()
+    assert folded.size == unfolded.size == 4
+    ids, pos, vel, frc, img = system.storage.getAll()
+    assert np.any(img != 0)
+    newest, u = folded[0], unfolded[0]
+    assert newest is folded.back() and folded[4] is None
+    for pid in (0, 17, 999):
+        k = int(np.searchsorted(ids, pid))
+        p = np.asarray(newest[pid])
+        assert np.all(p >= 0.0) and np.all(p < L)
+        assert np.allclose(np.asarray(u[pid]), pos[k] + img[k] * L, rtol=0, atol=1e-12)
+        assert np.allclose(p, pos[k] - np.floor(pos[k] / L) * L, rtol=0, atol=1e-12)
+        assert tuple(newest.getVelocities(pid)) == tuple(vel[k])
+        assert tuple(newest.getForces(pid)) == tuple(frc[k])
+        assert u.getRadius(pid) == 1.0
+    with pytest.raises(RuntimeError):
+        u.getVelocities(0)
+    assert [c for c in folded] == folded.all() and folded.all()[-1] is newest
+    folded.capacity = 2
+    assert folded.size == 2 and folded[0] is newest
+    folded.gather()
+    assert folded.size == 2 and folded[1] is newest
+    folded.capacity = -1
+    assert folded.capacity == 2
+    folded.clear()
+    assert folded.size == 0
+
+
+def test_checkpoint_resume_host_logic(on_oracle, tmp_path, monkeypatch):
+    """The checkpoint/resume recipe of the Python mirror (RNG.saveState / loadState, a
+    settable step, images through setImages) continues the uninterrupted Langevin run."""
+    monkeypatch.chdir(tmp_path)
+    full, integ_full = _fluid(2024)
+    integ_full.run(120)
+    integ_full.run(80)
+    part, integ_part = _fluid(2024)
+    integ_part.run(120)
+    ids, pos, vel, _, img = part.storage.getAll()
+    L = np.asarray(part.bc.boxL)
+    t = np.floor(pos * (1.0 / L))
+    pos, img = pos - t * L, img + t.astype(np.int32)
+    part.rng.saveState(integ_part.step)
+    # rebuild from the checkpoint in a fresh system keyed on the saved seed
+    res = espressopp.System()
+    res.rng = espressopp.esutil.RNG(99)
+    res.rng.loadState("rng.120")
+    assert res.rng.get_seed() == 2024
+    res.bc = espressopp.bc.OrthorhombicBC(res.rng, tuple(L))
+    res.skin = 0.3
+    cgrid = espressopp.tools.decomp.cellGrid(tuple(L), (1, 1, 1), 2.5, 0.3)
+    res.storage = espressopp.storage.DomainDecomposition(res, (1, 1, 1), cgrid)
+    res.storage.addParticles([[int(ids[k]), espressopp.Real3D(pos[k]), espressopp.Real3D(vel[k])]
+                              for k in range(len(ids))], "id", "pos", "v")
+    res.storage.setImages(ids, img)
+    res.storage.decompose()
+    vl = espressopp.VerletList(res, cutoff=2.5)
+    lj = espressopp.interaction.VerletListLennardJones(vl)
+    lj.setPotential(0, 0, espressopp.interaction.LennardJones(1.0, 1.0, 2.5))
+    res.addInteraction(lj)
+    ri = espressopp.integrator.VelocityVerlet(res)
+    ri.dt = 0.005
+    lang = espressopp.integrator.LangevinThermostat(res)
+    lang.gamma = 1.0
+    lang.temperature = 1.0
+    ri.addExtension(lang)
+    ri.step = 120
+    ri.run(80)
+    a, b = full.storage.getAll(), res.storage.getAll()
+    unf = lambda s: s[1] + s[4] * L
+    assert np.max(np.abs(unf(a) - unf(b))) < 1e-8
+
+
+def test_modify_particle_image_semantics(on_oracle):
+    system, integ = _fluid()
+    st = system.storage
+    st.modifyParticle(3, "img", (2, -1, 4))
+    assert tuple(st.getAll()[4][3]) == (2, -1, 4)
+    st.modifyParticle(3, "pos", (1.0, 2.0, 3.0))
+    _, pos, _, _, img = st.getAll()
+    assert tuple(img[3]) == (0, 0, 0) and tuple(pos[3]) == (1.0, 2.0, 3.0)
+    with pytest.raises(ValueError):
+        st.modifyParticle(3, "q", 1.0)
