@@ -1360,21 +1360,32 @@ void vecGhosts(espp_system* s, bool realToGhosts) {
   }
 }
 
-// vec::interaction::VerletListLennardJones::addForces_impl<ONETYPE, N3L = true>
-// (vec/interaction/VerletListLennardJones.hpp:130-241): a particle's row sums into
-// registers, the partner's force is decremented at once.
+// vec::interaction::VerletListLennardJones(Capped)::addForces_impl<ONETYPE, N3L = true>
+// (vec/interaction/VerletListLennardJones.hpp:130-241, VerletListLennardJonesCapped.hpp:
+// 60-72, 149-256): a particle's row sums into registers, the partner's force is
+// decremented at once; inside caprad the capped force 48 eps c6 (c6 - 1/2) / (caprad r)
+// with c6 = (sigma / caprad)^6.
 void vecLJForces(espp_system* s) {
   VecArrays& V = s->vec;
   const int nt = s->max_type + 1;
-  std::vector<double> ff1((size_t)nt * nt, 0.0), ff2((size_t)nt * nt, 0.0),
-      rcsq((size_t)nt * nt, -1.0);
+  const size_t nt2 = (size_t)nt * nt;
+  std::vector<double> ff1(nt2, 0.0), ff2(nt2, 0.0), rcsq(nt2, -1.0), capsq(nt2, -1.0),
+      capnum(nt2, 0.0), caprad(nt2, 0.0);
   for (int a = 0; a < nt; ++a)
     for (int b = 0; b < nt; ++b) {
       const LJParams* P = ljFor(s, a, b);
       if (!P) continue;
-      ff1[(size_t)a * nt + b] = P->ff1;
-      ff2[(size_t)a * nt + b] = P->ff2;
-      rcsq[(size_t)a * nt + b] = P->rcsq;
+      const size_t t = (size_t)a * nt + b;
+      ff1[t] = P->ff1;
+      ff2[t] = P->ff2;
+      rcsq[t] = P->rcsq;
+      if (P->caprad > 0) {
+        const double cfrac2 = (P->sig / P->caprad) * (P->sig / P->caprad);
+        const double cfrac6 = cfrac2 * cfrac2 * cfrac2;
+        caprad[t] = P->caprad;
+        capsq[t] = P->caprad * P->caprad;
+        capnum[t] = 48.0 * P->eps * cfrac6 * (cfrac6 - 0.5);
+      }
     }
   for (size_t ip = 0; ip < V.plist.size(); ++ip) {
     const int p = V.plist[ip];
@@ -1387,10 +1398,15 @@ void vecLJForces(espp_system* s) {
       const size_t t = pl + (size_t)std::min(V.type[np], nt - 1);
       const double dsq = dx * dx + dy * dy + dz * dz;
       if (dsq <= rcsq[t]) {
-        const double frac2 = 1.0 / dsq;
-        const double frac6 = frac2 * frac2 * frac2;
-        double ffactor = ff1[t] * frac6 - ff2[t];
-        ffactor = frac6 * ffactor * frac2;
+        double ffactor;
+        if (dsq > capsq[t]) {
+          const double frac2 = 1.0 / dsq;
+          const double frac6 = frac2 * frac2 * frac2;
+          ffactor = ff1[t] * frac6 - ff2[t];
+          ffactor = frac6 * ffactor * frac2;
+        } else {
+          ffactor = capnum[t] / (caprad[t] * std::sqrt(dsq));
+        }
         fx += dx * ffactor;
         fy += dy * ffactor;
         fz += dz * ffactor;
@@ -1446,15 +1462,12 @@ void vecIntegrate2(espp_system* s) {
 }
 
 // vec VelocityVerletBase::run (vec/integrator/VelocityVerlet.cpp:67-165): NVE with
-// Lennard-Jones pairs only.
+// Lennard-Jones or capped Lennard-Jones pairs only.
 int vecRun(espp_system* s, int64_t nsteps) {
   if (!s->has_vl) return fail(ESPP_ESTATE, "the vec step needs a Verlet list");
   if (s->fene_on || s->cos_on || s->tabAngle || !s->tabPair.empty() || s->tabBondOn ||
       s->mlp || s->lang_on || s->capMode != ESPP_CAP_OFF)
     return fail(ESPP_ESTATE, "the vec step restates NVE Lennard-Jones only");
-  for (const auto& kv : s->lj)
-    if (kv.second.set && kv.second.caprad > 0)
-      return fail(ESPP_ESTATE, "the vec step restates uncapped Lennard-Jones only");
   const double skinHalf = 0.5 * s->skin;
   s->nResorts = 0;
   s->vecMode = true;

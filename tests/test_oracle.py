@@ -324,26 +324,34 @@ def test_polymer_melt_step0_angle_energy_matches_result_dat():
     assert abs(s.virial(_abi.IA_COSINE)) < 1e-6
 
 
-def _lj2048_nve(lib_run_vec):
+def _lj2048_nve(capped=False):
+    """The setup of test_vec_lennard_jones.py: 2048-particle fluid with velocities, VL
+    cutoff 2.5, skin 0.3, dt 0.005; LJ(rc 2.5, shift 0) or LJCapped(rc 2^(1/6), caprad
+    0.6, shift auto)."""
     pid, pos, vel, box = load_lj2048()
     s = Sim(oracle_lib(), box, 0.3, cell_grid(box, 2.5, 0.3))
     s.add(pid + 1, pos, vel)
     s.decompose()
     s.vl(2.5)
-    s.lj(0, 0, 1.0, 1.0, 2.5, 0.0)
+    if capped:
+        rc = 2.0 ** (1.0 / 6.0)
+        s.lj(0, 0, 1.0, 1.0, rc, 4.0 * (rc ** -12 - rc ** -6), caprad=0.6)
+    else:
+        s.lj(0, 0, 1.0, 1.0, 2.5, 0.0)
     s.integrator(0.005)
     return s
 
 
+@pytest.mark.parametrize("capped", [False, True])
 @pytest.mark.parametrize("steps", [10, 400])
-def test_vec_twin_matches_classic(steps):
+def test_vec_twin_matches_classic(steps, capped):
     """The vec twin (SoA cells padded to 64-byte rows, packed half-shell candidates,
     padded neighbour rows, N3L force rows) against the classic AoS step on the 2048-particle
     fluid with velocities: the reference's test_vec_lennard_jones.py runs 10 NVE steps and
     asks |dx|^2 = 0 to 8 places; 400 steps take many re-sorts through both paths."""
     pid, pos, vel, box = load_lj2048()
     ids = pid + 1
-    classic, vec = _lj2048_nve(False), _lj2048_nve(True)
+    classic, vec = _lj2048_nve(capped), _lj2048_nve(capped)
     classic.run(steps)
     _abi.call(vec.lib, "espp_vec_run", vec.h, steps)
     a, b = classic.particles(ids), vec.particles(ids)
@@ -362,7 +370,7 @@ def test_vec_twin_matches_classic(steps):
 
 def test_vec_twin_refuses_what_it_does_not_restate():
     pid, pos, vel, box = load_lj2048()
-    s = _lj2048_nve(True)
+    s = _lj2048_nve()
     s.langevin(1.0, 1.0)
     with pytest.raises(RuntimeError, match="NVE Lennard-Jones only"):
         _abi.call(s.lib, "espp_vec_run", s.h, 1)
@@ -373,7 +381,7 @@ def test_vec_twin_runs_interleave_with_classic_runs():
     observables in between, see the particles where the vec run left them."""
     pid, pos, vel, box = load_lj2048()
     ids = pid + 1
-    classic, vec = _lj2048_nve(False), _lj2048_nve(True)
+    classic, vec = _lj2048_nve(), _lj2048_nve()
     for n in (150, 150):
         classic.run(n)
         _abi.call(vec.lib, "espp_vec_run", vec.h, n)
