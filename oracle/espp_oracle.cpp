@@ -365,6 +365,9 @@ struct VecArrays {
   std::vector<std::pair<int, int>> prange;
   std::vector<int> cj;                  // packed candidate slots of one cell's half shell
   std::vector<double> cx, cy, cz;
+  // vec::FixedPairList / FixedTripleList: bonds and angles as slots of real particles
+  std::vector<std::pair<int, int>> bonds;
+  std::vector<std::array<int, 3>> triples;
 };
 
 struct espp_system {
@@ -1243,6 +1246,24 @@ void vecLoad(espp_system* s) {
       V.type[o + k] = P[k].type;
     }
   }
+  // bonded lists refreshed on the same signal (vec/FixedPairList.cpp,
+  // vec/FixedTripleList.cpp): ids resolved to the slots of the real particles
+  std::unordered_map<int64_t, int> slot;
+  for (int c : s->realCells) {
+    const auto& P = s->cells[c].p;
+    for (size_t k = 0; k < P.size(); ++k) slot[P[k].id] = (int)(V.cellRange[c] + k);
+  }
+  V.bonds.clear();
+  for (const auto& b : s->bondsGlobal) {
+    auto i1 = slot.find(b.first), i2 = slot.find(b.second);
+    if (i1 != slot.end() && i2 != slot.end()) V.bonds.push_back({i1->second, i2->second});
+  }
+  V.triples.clear();
+  for (const auto& t : s->triplesGlobal) {
+    auto i1 = slot.find(t[0]), i2 = slot.find(t[1]), i3 = slot.find(t[2]);
+    if (i1 != slot.end() && i2 != slot.end() && i3 != slot.end())
+      V.triples.push_back({i1->second, i2->second, i3->second});
+  }
   V.loaded = true;
 }
 
@@ -1421,12 +1442,59 @@ void vecLJForces(espp_system* s) {
   }
 }
 
+// vec FixedPairListInteractionTemplate<FENE>::addForces and
+// FixedTripleListInteractionTemplate<Cosine>::addForces (vec/interaction/
+// FixedPairListInteractionTemplate.hpp:121-170, FixedTripleListInteractionTemplate.hpp):
+// minimum-image distances of the slot positions, the scalar potentials' force arithmetic.
+void vecBondedForces(espp_system* s) {
+  VecArrays& V = s->vec;
+  auto pos = [&](int p, double r[3]) {
+    r[0] = V.x[p];
+    r[1] = V.y[p];
+    r[2] = V.z[p];
+  };
+  auto add = [&](int p, const double f[3], double sign) {
+    V.fx[p] += sign * f[0];
+    V.fy[p] += sign * f[1];
+    V.fz[p] += sign * f[2];
+  };
+  if (s->fene_on)
+    for (const auto& b : V.bonds) {
+      double r1[3], r2[3], d[3], f[3];
+      pos(b.first, r1);
+      pos(b.second, r2);
+      minImageBox(s, r1, r2, d);
+      const double dsq = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+      if (dsq > s->ltMaxBondSqr) s->ltMaxBondSqr = dsq;
+      if (feneForce(s, d, f)) {
+        add(b.first, f, 1.0);
+        add(b.second, f, -1.0);
+      }
+    }
+  if (s->cos_on)
+    for (const auto& t : V.triples) {
+      double r1[3], r2[3], r3[3], d12[3], d32[3], f12[3], f32[3];
+      pos(t[0], r1);
+      pos(t[1], r2);
+      pos(t[2], r3);
+      minImageBox(s, r1, r2, d12);
+      minImageBox(s, r3, r2, d32);
+      cosineForce(s, d12, d32, f12, f32);
+      add(t[0], f12, 1.0);
+      V.fx[t[1]] -= f12[0] + f32[0];
+      V.fy[t[1]] -= f12[1] + f32[1];
+      V.fz[t[1]] -= f12[2] + f32[2];
+      add(t[2], f32, 1.0);
+    }
+}
+
 // vec VelocityVerletBase::updateForces (vec/integrator/VelocityVerlet.cpp:228-245).
 void vecUpdateForces(espp_system* s) {
   VecArrays& V = s->vec;
   vecGhosts(s, true);
   for (auto* a : {&V.fx, &V.fy, &V.fz}) std::fill(a->begin(), a->end(), 0.0);
   vecLJForces(s);
+  vecBondedForces(s);
   vecGhosts(s, false);
 }
 
@@ -1462,12 +1530,12 @@ void vecIntegrate2(espp_system* s) {
 }
 
 // vec VelocityVerletBase::run (vec/integrator/VelocityVerlet.cpp:67-165): NVE with
-// Lennard-Jones or capped Lennard-Jones pairs only.
+// (capped) Lennard-Jones pairs, FENE bonds and Cosine angles.
 int vecRun(espp_system* s, int64_t nsteps) {
   if (!s->has_vl) return fail(ESPP_ESTATE, "the vec step needs a Verlet list");
-  if (s->fene_on || s->cos_on || s->tabAngle || !s->tabPair.empty() || s->tabBondOn ||
-      s->mlp || s->lang_on || s->capMode != ESPP_CAP_OFF)
-    return fail(ESPP_ESTATE, "the vec step restates NVE Lennard-Jones only");
+  if (s->tabAngle || !s->tabPair.empty() || s->tabBondOn || s->mlp || s->lang_on ||
+      s->capMode != ESPP_CAP_OFF)
+    return fail(ESPP_ESTATE, "the vec step restates NVE Lennard-Jones, FENE and Cosine only");
   const double skinHalf = 0.5 * s->skin;
   s->nResorts = 0;
   s->vecMode = true;

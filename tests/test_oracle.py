@@ -372,7 +372,7 @@ def test_vec_twin_refuses_what_it_does_not_restate():
     pid, pos, vel, box = load_lj2048()
     s = _lj2048_nve()
     s.langevin(1.0, 1.0)
-    with pytest.raises(RuntimeError, match="NVE Lennard-Jones only"):
+    with pytest.raises(RuntimeError, match="restates NVE Lennard-Jones, FENE and Cosine only"):
         _abi.call(s.lib, "espp_vec_run", s.h, 1)
 
 
@@ -393,3 +393,34 @@ def test_vec_twin_runs_interleave_with_classic_runs():
     assert np.max(np.abs((a[0] + a[3] * box) - (b[0] + b[3] * box))) < 1e-8
     assert vec.step() == classic.step() == 350
     assert vec.builds() == classic.builds()
+
+
+def test_vec_twin_matches_classic_on_the_polymer_melt():
+    """test_vec_polymer_melt.py's check: the 40 000-bead melt with WCA (rc 2^(1/6), shift
+    0), FENE(30, 0, 1.5) and Cosine(1.5, 3.1415926), skin 0.4, dt 0.005, 10 NVE steps from
+    rest; vec and classic positions agree, |dx|^2 = 0 to 8 places."""
+    pos, bonds, box, _, angles = load_polymer40k(angles=True)
+    ids = np.arange(1, len(pos) + 1)
+    rc = 2.0 ** (1.0 / 6.0)
+    sims = []
+    for _ in range(2):
+        s = Sim(oracle_lib(), box, 0.4, cell_grid(box, rc, 0.4))
+        s.add(ids, pos)
+        s.decompose()
+        s.vl(rc)
+        s.lj(0, 0, 1.0, 1.0, rc, 0.0)
+        s.bonds(bonds)
+        s.fene(30.0, 0.0, 1.5)
+        s.triples(angles)
+        s.cosine(1.5, 3.1415926)
+        s.integrator(0.005)
+        sims.append(s)
+    classic, vec = sims
+    classic.run(10)
+    _abi.call(vec.lib, "espp_vec_run", vec.h, 10)
+    a, b = classic.particles(ids), vec.particles(ids)
+    d2 = np.sum(((a[0] + a[3] * box) - (b[0] + b[3] * box)) ** 2, axis=1)
+    assert np.max(d2) < 5e-9
+    assert np.max(np.abs(a[1] - b[1])) < 1e-6
+    for which in (_abi.IA_LJ, _abi.IA_FENE, _abi.IA_COSINE):
+        assert vec.energy(which) == pytest.approx(classic.energy(which), rel=1e-9)
