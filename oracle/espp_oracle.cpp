@@ -360,6 +360,7 @@ struct VecArrays {
   std::vector<size_t> cellRange, sizes;  // first slot and particle count of each cell
   std::vector<double> x, y, z, vx, vy, vz, fx, fy, fz, mass;
   std::vector<int32_t> type;
+  std::vector<int64_t> id;
   // vec::VerletList::NeighborList: rows of neighbour slots per listed particle
   std::vector<int> plist, nplist;
   std::vector<std::pair<int, int>> prange;
@@ -1229,6 +1230,7 @@ void vecLoad(espp_system* s) {
   for (auto* a : {&V.vx, &V.vy, &V.vz, &V.fx, &V.fy, &V.fz}) a->assign(total, 0.0);
   V.mass.assign(total, 1.0);
   V.type.assign(total, 0);
+  V.id.assign(total, -1);
   for (size_t c = 0; c < nc; ++c) {
     const auto& P = s->cells[c].p;
     const size_t o = V.cellRange[c];
@@ -1244,6 +1246,7 @@ void vecLoad(espp_system* s) {
       V.fz[o + k] = P[k].f[2];
       V.mass[o + k] = P[k].mass;
       V.type[o + k] = P[k].type;
+      V.id[o + k] = P[k].id;
     }
   }
   // bonded lists refreshed on the same signal (vec/FixedPairList.cpp,
@@ -1493,9 +1496,22 @@ void vecUpdateForces(espp_system* s) {
   VecArrays& V = s->vec;
   vecGhosts(s, true);
   for (auto* a : {&V.fx, &V.fy, &V.fz}) std::fill(a->begin(), a->end(), 0.0);
-  vecLJForces(s);
+  if (s->has_vl) vecLJForces(s);
   vecBondedForces(s);
   vecGhosts(s, false);
+  // aftCalcF: vec LangevinThermostat::thermalize_impl (vec/integrator/
+  // LangevinThermostat.cpp:120-141) over the real slots, the oracle's Philox draws
+  if (s->lang_on)
+    for (int c : s->realCells)
+      for (size_t p = V.cellRange[c]; p < V.cellRange[c] + V.sizes[c]; ++p) {
+        if (s->langExcl.count(V.id[p])) continue;
+        const double massf = std::sqrt(V.mass[p]);
+        double u[3];
+        langevin_uniforms(s->seed, V.id[p], s->step, s->langPhase, u);
+        V.fx[p] += s->pref1 * V.vx[p] * V.mass[p] + s->pref2 * (u[0] - 0.5) * massf;
+        V.fy[p] += s->pref1 * V.vy[p] * V.mass[p] + s->pref2 * (u[1] - 0.5) * massf;
+        V.fz[p] += s->pref1 * V.vz[p] * V.mass[p] + s->pref2 * (u[2] - 0.5) * massf;
+      }
 }
 
 // vec VelocityVerletBase::integrate1 / integrate2 (:167-207), real particles only.
@@ -1529,15 +1545,19 @@ void vecIntegrate2(espp_system* s) {
   s->step++;
 }
 
-// vec VelocityVerletBase::run (vec/integrator/VelocityVerlet.cpp:67-165): NVE with
-// (capped) Lennard-Jones pairs, FENE bonds and Cosine angles.
+// vec VelocityVerletBase::run (vec/integrator/VelocityVerlet.cpp:67-165) with the
+// Langevin runInit/recalc hooks: (capped) Lennard-Jones pairs, FENE bonds, Cosine angles.
 int vecRun(espp_system* s, int64_t nsteps) {
-  if (!s->has_vl) return fail(ESPP_ESTATE, "the vec step needs a Verlet list");
-  if (s->tabAngle || !s->tabPair.empty() || s->tabBondOn || s->mlp || s->lang_on ||
+  if (s->tabAngle || !s->tabPair.empty() || s->tabBondOn || s->mlp ||
       s->capMode != ESPP_CAP_OFF)
-    return fail(ESPP_ESTATE, "the vec step restates NVE Lennard-Jones, FENE and Cosine only");
+    return fail(ESPP_ESTATE,
+                "the vec step restates Lennard-Jones, FENE, Cosine and Langevin only");
   const double skinHalf = 0.5 * s->skin;
   s->nResorts = 0;
+  if (s->lang_on) {
+    s->pref1 = -s->gamma;
+    s->pref2 = std::sqrt(24.0 * s->temperature * s->gamma / s->dt);
+  }
   s->vecMode = true;
   s->vlPairs.clear();  // points into cells that the re-sorts below rearrange
   s->bondPtrs.clear();
@@ -1552,10 +1572,18 @@ int vecRun(espp_system* s, int64_t nsteps) {
     // are created; the list was counted when it was created
     vecLoad(s);
     const int64_t builds = s->builds;
-    vecRebuild(s);
+    if (s->has_vl) vecRebuild(s);
     s->builds = builds;
   }
+  // start-of-run force with the Langevin heat-up (recalc1/recalc2)
+  if (s->lang_on) {
+    s->pref2buffer = s->pref2;
+    s->pref2 *= std::sqrt(3.0);
+  }
+  s->langPhase = 1;
   vecUpdateForces(s);
+  s->langPhase = 0;
+  if (s->lang_on) s->pref2 = s->pref2buffer;
   for (int64_t i = 0; i < nsteps; ++i) {
     s->maxDist += std::sqrt(vecIntegrate1(s));
     if (s->maxDist > skinHalf) s->resortFlag = true;

@@ -369,11 +369,41 @@ def test_vec_twin_matches_classic(steps, capped):
 
 
 def test_vec_twin_refuses_what_it_does_not_restate():
-    pid, pos, vel, box = load_lj2048()
     s = _lj2048_nve()
-    s.langevin(1.0, 1.0)
-    with pytest.raises(RuntimeError, match="restates NVE Lennard-Jones, FENE and Cosine only"):
+    s.capforce(_abi.CAP_ABS, [10.0, 10.0, 10.0])
+    with pytest.raises(RuntimeError, match="restates Lennard-Jones, FENE, Cosine and Langevin"):
         _abi.call(s.lib, "espp_vec_run", s.h, 1)
+
+
+def test_vec_twin_langevin_matches_classic():
+    """Langevin (gamma 1, T 1.5) with one excluded particle: the vec twin's thermalize
+    draws the same counter-based noise, so vec and classic runs agree to rounding."""
+    pid, pos, vel, box = load_lj2048()
+    ids = pid + 1
+    classic, vec = _lj2048_nve(), _lj2048_nve()
+    for s in (classic, vec):
+        s.langevin(1.0, 1.5, excl=[5])
+    classic.run(100)
+    _abi.call(vec.lib, "espp_vec_run", vec.h, 100)
+    a, b = classic.particles(ids), vec.particles(ids)
+    assert np.max(np.abs((a[0] + a[3] * box) - (b[0] + b[3] * box))) < 1e-8
+    assert vec.builds() == classic.builds()
+
+
+def test_vec_twin_langevin_exclusion_keeps_a_free_particle_still():
+    """test_vec_langevin_thermostat.py: three particles at rest without interactions; the
+    excluded one does not move, the thermostat moves the other two."""
+    box = np.array([10.0, 10.0, 10.0])
+    s = Sim(oracle_lib(), box, 0.3, cell_grid(box, 1.0, 0.3))
+    s.add(np.array([1, 2, 3]), np.array([[1.0, 1.0, 1.0], [5.0, 5.0, 5.0], [8.0, 2.0, 6.0]]))
+    s.decompose()
+    s.integrator(0.01)
+    s.langevin(1.0, 1.0, excl=[1])
+    before = s.particles(np.array([1, 2, 3]))[0]
+    _abi.call(s.lib, "espp_vec_run", s.h, 10)
+    after = s.particles(np.array([1, 2, 3]))[0]
+    assert np.array_equal(before[0], after[0])
+    assert np.all(before[1:] != after[1:])
 
 
 def test_vec_twin_runs_interleave_with_classic_runs():
