@@ -2144,6 +2144,31 @@ int espp_vec_run(espp_system* s, int64_t nsteps) {
   return vecRun(s, nsteps);
 }
 
+// The vec twin's current neighbour list as sorted (smaller id, larger id) pairs, padding
+// slots left out (the verlet_list_buffer.py comparison); ESPP_ESTATE before a vec run.
+int espp_vec_pairs(espp_system* s, int64_t cap, int64_t* pairs, int64_t* npairs) {
+  CHECK_S(s);
+  const VecArrays& V = s->vec;
+  if (!V.loaded) return fail(ESPP_ESTATE, "no vec list: run espp_vec_run first");
+  std::vector<std::pair<int64_t, int64_t>> v;
+  for (size_t ip = 0; ip < V.plist.size(); ++ip) {
+    const int64_t a = V.id[V.plist[ip]];
+    for (int in = V.prange[ip].first; in < V.prange[ip].second; ++in) {
+      const int64_t b = V.id[V.nplist[in]];
+      if (b < 0) continue;  // padding slot
+      v.push_back({std::min(a, b), std::max(a, b)});
+    }
+  }
+  std::sort(v.begin(), v.end());
+  *npairs = (int64_t)v.size();
+  if (pairs)
+    for (int64_t i = 0; i < std::min<int64_t>(cap, (int64_t)v.size()); ++i) {
+      pairs[2 * i] = v[i].first;
+      pairs[2 * i + 1] = v[i].second;
+    }
+  return ESPP_OK;
+}
+
 int espp_num_resorts(espp_system* s, int64_t* n) {
   CHECK_S(s);
   *n = s->nResorts;

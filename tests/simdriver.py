@@ -37,6 +37,9 @@ def oracle_lib():
             "espp_oracle_lj_eval": (ctypes.c_int32, [ctypes.c_double] * 5 + [D, D, D]),
             "espp_oracle_fene_eval": (ctypes.c_int32, [ctypes.c_double] * 5 + [D, D, D]),
             "espp_vec_run": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int64]),
+            "espp_vec_pairs": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int64,
+                                                ctypes.POINTER(ctypes.c_int64),
+                                                ctypes.POINTER(ctypes.c_int64)]),
         })
         _oracle = lib
     return _oracle

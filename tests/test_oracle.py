@@ -454,3 +454,23 @@ def test_vec_twin_matches_classic_on_the_polymer_melt():
     assert np.max(np.abs(a[1] - b[1])) < 1e-6
     for which in (_abi.IA_LJ, _abi.IA_FENE, _abi.IA_COSINE):
         assert vec.energy(which) == pytest.approx(classic.energy(which), rel=1e-9)
+
+
+@pytest.mark.parametrize("steps", [10, 200])
+def test_vec_list_equals_classic_list(steps):
+    """verlet_list_buffer.py's check, classic AoS list against the vec twin's list: the
+    same sorted id pairs after Langevin steps (both rebuilt on the same steps)."""
+    classic, vec = _lj2048_nve(), _lj2048_nve()
+    for s in (classic, vec):
+        s.langevin(1.0, 1.0)
+    classic.run(steps)
+    _abi.call(vec.lib, "espp_vec_run", vec.h, steps)
+    want = classic.pairs()
+    n = ctypes.c_int64()
+    _abi.call(vec.lib, "espp_vec_pairs", vec.h, 0, None, ctypes.byref(n))
+    got = np.zeros((n.value, 2), np.int64)
+    _abi.call(vec.lib, "espp_vec_pairs", vec.h, n.value,
+              got.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), ctypes.byref(n))
+    assert vec.builds() == classic.builds()
+    assert len(got) == len(want) > 0
+    assert np.array_equal(got, want)
