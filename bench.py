@@ -159,6 +159,17 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0}, "fallback"
 
 
+def max_over_ranks(dist, value, device="cuda"):
+    """The largest of the ranks' values (every multi-GPU time is the max over ranks);
+    `value` itself without a process group."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ---- CPU baseline (the oracle: a restatement of the reference algorithm) ------------
 def _oracle_sample(args):
     """Steps one 32^3 sample system with the FP64 CPU oracle, through `entry`
@@ -294,12 +305,7 @@ def gpu_arm(args, rank, world, local_rank):
     call(lib, "espp_profile", h, dptr(ph_g), i64ptr(launches))
     resorts = ctypes.c_int64()
     call(lib, "espp_num_resorts", h, ctypes.byref(resorts))
-    loop_ms = float(ms[1])
-    if dist is not None:
-        import torch
-        t = torch.tensor([loop_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        loop_ms = float(t.item())
+    loop_ms = max_over_ranks(dist, float(ms[1]))
 
 
     log("rank %d: profiled pass" % rank)
@@ -328,11 +334,7 @@ def gpu_arm(args, rank, world, local_rank):
     call(lib, "espp_get_particles", h, N, i64ptr(pin_ids), dptr(pin_pos), dptr(pin_vel), None,
          None)
     barrier()
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(dist, time.perf_counter() - t0)
 
     log("rank %d: FP64 comparison" % rank)
     # mixed vs all-FP64 GPU on the same positions: force error and step throughput
@@ -368,11 +370,7 @@ def gpu_arm(args, rank, world, local_rank):
         drift32 = (total_energy(h) - e32_before) / N / (args.steps * DT)
         ms64 = np.zeros(2)
         call(lib, "espp_last_run_ms", h64, dptr(ms64))
-        loop64 = float(ms64[1])
-        if dist is not None:
-            t = torch.tensor([loop64], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            loop64 = float(t.item())
+        loop64 = max_over_ranks(dist, float(ms64[1]))
         lib.espp_system_destroy(h64)
         cmp = {"force_rel_rms_err": rel_rms, "force_rel_max_err": rel_max,
                "fp64_value": world * N * args.steps / (loop64 * 1e-3),
