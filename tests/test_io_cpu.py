@@ -77,3 +77,51 @@ def test_dumpxyz_backup_and_readxyz_round_trip(tmp_path, monkeypatch):
     assert np.allclose(np.c_[xp, yp, zp], pos, atol=1e-10)
     assert np.allclose(np.c_[xv, yv, zv], vel, atol=1e-10)
     assert (Lx, Ly, Lz) == (10.0, 12.5, 8.0)
+
+
+def _lammps_file(path, natoms, nbonds, nangles, ndih, ntypes, velocities=False):
+    lines = ["LAMMPS data file", "",
+             "%d atoms" % natoms, "%d bonds" % nbonds, "%d angles" % nangles,
+             "%d dihedrals" % ndih, "0 impropers", "",
+             "%d atom types%s" % (ntypes, " velocities" if velocities else ""), "",
+             "0.0 10.0 xlo xhi", "-1.0 11.0 ylo yhi", "2.0 14.0 zlo zhi", "", "Atoms", ""]
+    for i in range(natoms):
+        if ntypes == 1:
+            mol = ["1"] if nbonds else []
+            lines.append(" ".join([str(i + 1)] + mol + ["1", "%g" % (i + 0.5), "%g" % (i + 1.5),
+                                                        "%g" % (i + 2.5)]))
+        else:
+            lines.append("%d 1 %d %g %g %g %g" % (i + 1, i % 2, 0.5 * i, i + 0.5, i + 1.5,
+                                                  i + 2.5))
+    for name, n, width in (("Bonds", nbonds, 2), ("Angles", nangles, 3),
+                           ("Dihedrals", ndih, 4)):
+        if n:
+            lines += ["", name, ""]
+            for k in range(n):
+                lines.append(" ".join(map(str, [k + 1, 1] + [k + 1 + j for j in range(width)])))
+    if velocities:
+        lines += ["", "Velocities", ""]
+        for i in range(natoms):
+            lines.append("%d %g %g %g" % (i + 1, 0.1 * i, -0.1 * i, 0.2))
+    path.write_text("\n".join(lines) + "\n")
+    return str(path)
+
+
+def test_lammps_read_return_shapes(tmp_path):
+    """tools.lammps.read returns what the reference returns for each kind of file
+    (src/tools/lammps.py:142-155)."""
+    from espressopp_b200.tools import lammps
+    r = lammps.read(_lammps_file(tmp_path / "a.data", 3, 0, 0, 0, 1))
+    assert len(r) == 6 and r[0] == [0.5, 1.5, 2.5] and r[3:] == (10.0, 12.0, 12.0)
+    r = lammps.read(_lammps_file(tmp_path / "v.data", 3, 0, 0, 0, 1, velocities=True))
+    assert len(r) == 9 and r[6] == [0.0, 0.1, 0.2] and r[8] == [0.2] * 3
+    r = lammps.read(_lammps_file(tmp_path / "b.data", 4, 3, 0, 0, 1))
+    assert len(r) == 7 and r[0] == [(1, 2), (2, 3), (3, 4)] and r[1] == [0.5, 1.5, 2.5, 3.5]
+    r = lammps.read(_lammps_file(tmp_path / "ba.data", 4, 3, 2, 0, 1))
+    assert len(r) == 8 and r[1] == [(1, 2, 3), (2, 3, 4)] and r[4] == [2.5, 3.5, 4.5, 5.5]
+    r = lammps.read(_lammps_file(tmp_path / "bad.data", 5, 4, 3, 2, 1))
+    assert len(r) == 9 and r[2] == [(1, 2, 3, 4), (2, 3, 4, 5)]
+    r = lammps.read(_lammps_file(tmp_path / "t.data", 4, 3, 2, 0, 2))
+    p_type, bonds, angles, q, x, y, z, Lx, Ly, Lz = r
+    assert p_type == [0, 1, 0, 1] and q == [0.0, 0.5, 1.0, 1.5] and x[3] == 3.5
+    assert bonds == [(1, 2), (2, 3), (3, 4)] and (Lx, Ly, Lz) == (10.0, 12.0, 12.0)
