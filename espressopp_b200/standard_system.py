@@ -1,5 +1,6 @@
-"""standard_system.Default / LennardJones / PolymerMelt (src/standard_system/Default.py,
-LennardJones.py:1-145, PolymerMelt.py:62-175)."""
+"""standard_system.Default / Minimal / LennardJones / PolymerMelt
+(src/standard_system/Default.py, Minimal.py:50-86, LennardJones.py:1-145,
+PolymerMelt.py:62-175)."""
 from . import core, integrator as _integrator, interaction, storage as _storage
 from .tools import decomp
 from .tools.DumpConfigurations import readxyz
@@ -22,6 +23,19 @@ def Default(box, rc=1.12246, skin=0.3, dt=0.005, temperature=None, halfCellInt=1
         t.gamma = 1.0
         t.temperature = temperature
         integ.addExtension(t)
+    return system, integ
+
+
+def Minimal(num_particles, box, rc=1.12246, skin=0.3, dt=0.005, temperature=None,
+            precision=None):
+    """A system of num_particles at random positions in the box, at rest, with no
+    interactions (Minimal.py:50-86); ids 1..num_particles, type 0, mass 1."""
+    system, integ = Default(box, rc, skin, dt, temperature, precision=precision)
+    props = ["id", "type", "mass", "pos", "v"]
+    parts = [[pid, 0, 1.0, system.bc.getRandomPos(), core.Real3D(0.0, 0.0, 0.0)]
+             for pid in range(1, num_particles + 1)]
+    system.storage.addParticles(parts, *props)
+    system.storage.decompose()
     return system, integ
 
 

@@ -131,3 +131,26 @@ def test_modify_particle_image_semantics(on_oracle):
     assert tuple(img[3]) == (0, 0, 0) and tuple(pos[3]) == (1.0, 2.0, 3.0)
     with pytest.raises(ValueError):
         st.modifyParticle(3, "q", 1.0)
+
+
+def test_standard_systems_and_info(on_oracle, capsys):
+    """standard_system.Minimal / LennardJones build what the reference builds, and
+    tools.analyse.info / timers.show print from them."""
+    system, integ = espressopp.standard_system.Minimal(200, (10.0, 10.0, 10.0), rc=2.5,
+                                                       skin=0.3)
+    ids, pos, vel, _, _ = system.storage.getAll()
+    assert list(ids) == list(range(1, 201)) and np.all(vel == 0.0)
+    assert np.all(pos >= 0.0) and np.all(pos < 10.0)
+    assert system.getNumberOfInteractions() == 0
+    integ.run(5)
+    assert integ.step == 5
+    # random positions overlap: the reference's recipe needs a capped warm-up before
+    # stepping, so only the start-of-run forces are taken here
+    system, integ = espressopp.standard_system.LennardJones(500, box=(9.0, 9.0, 9.0), rc=2.5,
+                                                            temperature=1.0)
+    assert system.getNumberOfInteractions() == 1
+    integ.run(0)
+    espressopp.tools.analyse.info(system, integ)
+    espressopp.tools.timers.show(integ.getTimers())
+    out = capsys.readouterr().out
+    assert out.strip()
