@@ -101,3 +101,19 @@ def test_potentials_pickle():
         assert type(q) is type(pot) and vars(q) == vars(pot)
     lj = pickle.loads(pickle.dumps(espressopp.interaction.LennardJones(1.2, 0.9, 2.5)))
     assert lj.computeEnergy(2.5) == pytest.approx(0.0, abs=1e-15)
+
+
+def test_replicate_copies_positions_and_topology():
+    """tools.replicate (src/tools/replicate.py): copies in (i, j, k) order, k fastest,
+    positions shifted by the box edges, ids by the copy index times N."""
+    from espressopp_b200.tools import replicate
+    x, y, z = [0.1, 0.2, 0.3], [0.4, 0.5, 0.6], [0.7, 0.8, 0.9]
+    b, a, xs, ys, zs, Lx, Ly, Lz = replicate([(1, 2), (2, 3)], [(1, 2, 3)], x, y, z,
+                                             1.0, 2.0, 3.0, xdim=2, ydim=1, zdim=2)
+    assert (Lx, Ly, Lz) == (2.0, 2.0, 6.0) and len(xs) == 12
+    assert xs[3:6] == x and zs[3:6] == [v + 3.0 for v in z]      # copy 1: (0, 0, 1)
+    assert xs[6:9] == [v + 1.0 for v in x] and zs[6:9] == z       # copy 2: (1, 0, 0)
+    assert b[2:4] == [(4, 5), (5, 6)] and b[-1] == (11, 12)
+    assert a == [(1, 2, 3), (4, 5, 6), (7, 8, 9), (10, 11, 12)]
+    assert replicate([], [], x, y, z, 1.0, 1.0, 1.0) == ([], [], x, y, z, 1.0, 1.0, 1.0)
+    assert espressopp.tools.readxyz is espressopp.tools.DumpConfigurations.readxyz
