@@ -55,7 +55,39 @@ class Pressure(_Observable):
 
 class PressureTensor(_Observable):
     """P_ab = (sum m v_a v_b + W_ab) / V (PressureTensor.hpp:51-80); the kinetic sum and
-    the virials are reduced on the GPU."""
+    the virials are reduced on the GPU.  performMeasurement / getAverageValue / reset /
+    getNumberOfMeasurements keep the reference's running average and variance
+    (PressureTensor.hpp:96-143, Knuth's update): getAverageValue returns the six averages
+    followed by the six standard deviations sqrt(M2 / (n - 1))."""
+
+    def __init__(self, system):
+        _Observable.__init__(self, system)
+        self.reset()
+
+    def reset(self):
+        self._n = 0
+        self._avg = np.zeros(6)
+        self._m2 = np.zeros(6)
+
+    def performMeasurement(self):
+        res = np.asarray(self.compute(), np.float64)
+        self._n += 1
+        if self._n == 1:
+            self._avg = res.copy()
+        else:
+            new = self._avg + (res - self._avg) / self._n
+            self._m2 = self._m2 + (res - self._avg) * (res - new)
+            self._avg = new
+
+    def getNumberOfMeasurements(self):
+        return self._n
+
+    def getAverageValue(self):
+        if self._n == 0:
+            return [0.0] * 12
+        std = [float(np.sqrt(v / (self._n - 1))) if self._n > 1 else float("nan")
+               for v in self._m2]
+        return [float(a) for a in self._avg] + std
 
     def compute(self):
         st = self._st()

@@ -154,3 +154,24 @@ def test_standard_systems_and_info(on_oracle, capsys):
     espressopp.tools.timers.show(integ.getTimers())
     out = capsys.readouterr().out
     assert out.strip()
+
+
+def test_pressure_tensor_running_average(on_oracle):
+    """PressureTensor.performMeasurement / getAverageValue: the running mean and the
+    sample standard deviation of the measured tensors (PressureTensor.hpp:96-143)."""
+    system, integ = _fluid()
+    pt = espressopp.analysis.PressureTensor(system)
+    assert pt.getAverageValue() == [0.0] * 12 and pt.getNumberOfMeasurements() == 0
+    seen = []
+    for _ in range(4):
+        integ.run(20)
+        seen.append(list(pt.compute()))
+        pt.performMeasurement()
+    avg = pt.getAverageValue()
+    assert pt.getNumberOfMeasurements() == 4 and len(avg) == 12
+    assert np.allclose(avg[:6], np.mean(seen, axis=0), rtol=1e-12, atol=1e-14)
+    assert np.allclose(avg[6:], np.std(seen, axis=0, ddof=1), rtol=1e-9, atol=1e-14)
+    pt.reset()
+    pt.performMeasurement()
+    assert pt.getNumberOfMeasurements() == 1 and all(np.isnan(avg_) for avg_ in
+                                                     pt.getAverageValue()[6:])
