@@ -33,11 +33,35 @@ class NPart(_Observable):
 
 
 class Temperature(_Observable):
-    """T = sum m v^2 / (3 N), k_B = 1."""
+    """T = sum m v^2 / (3 N), k_B = 1 (Temperature.hpp:57-126), reduced on the GPU.  After
+    add_type, only particles of the added types count; that selection is summed on the
+    host from one state download."""
+
+    def __init__(self, system):
+        _Observable.__init__(self, system)
+        self._valid_types = set()
+
+    def add_type(self, type_id):
+        self._valid_types.add(int(type_id))
+
+    def remove_type(self, type_id):
+        if int(type_id) in self._valid_types:
+            self._valid_types.discard(int(type_id))
+            return True
+        return False
 
     def compute(self):
-        v2, n = self._kinetic()
-        return v2 / (3.0 * n) if n else 0.0
+        if not self._valid_types:
+            v2, n = self._kinetic()
+            return v2 / (3.0 * n) if n else 0.0
+        st = self._st()
+        ids, _, vel, _, _ = st.getAll()
+        sel = [k for k, pid in enumerate(ids) if st._types[int(pid)] in self._valid_types]
+        if not sel:
+            return float("nan")
+        m = np.array([st._masses[int(ids[k])] for k in sel])
+        v = vel[sel]
+        return float(np.sum(m * np.sum(v * v, axis=1))) / (3.0 * len(sel))
 
     def compute_real(self):
         return self.compute()

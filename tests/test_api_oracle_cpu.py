@@ -175,3 +175,20 @@ def test_pressure_tensor_running_average(on_oracle):
     pt.performMeasurement()
     assert pt.getNumberOfMeasurements() == 1 and all(np.isnan(avg_) for avg_ in
                                                      pt.getAverageValue()[6:])
+
+
+def test_temperature_of_selected_types(on_oracle):
+    """Temperature.add_type / remove_type (Temperature.hpp:104-141): only the selected
+    types count; with none selected every particle does."""
+    system, integ = _fluid(n=512)
+    st = system.storage
+    T = espressopp.analysis.Temperature(system)
+    integ.run(30)
+    ids, _, vel, _, _ = st.getAll()
+    all_T = float(np.sum(vel * vel)) / (3 * len(ids))
+    assert T.compute() == pytest.approx(all_T, rel=1e-12)
+    st._types[7] = 1  # the bookkeeping of a particle added with type 1
+    T.add_type(1)
+    assert T.compute() == pytest.approx(float(np.sum(vel[7] ** 2)) / 3.0, rel=1e-12)
+    assert T.remove_type(1) and not T.remove_type(1)
+    assert T.compute() == pytest.approx(all_T, rel=1e-12)
