@@ -12,10 +12,19 @@ fixed-point force sums, FP64 positions / velocities / energies).  Particle data
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 A step is one velocity-Verlet step (force, aftCalcF, integrate2 + integrate1, and the
-re-sort + Verlet rebuild whenever the accumulated displacement exceeds skin/2).  W
-untimed steps run first; the K timed steps are one espp_run call whose step loop is
-timed by CUDA events on the library's stream (max over ranks).  Under torchrun each
-rank steps its own independent copy of the system on its GPU (replicas, weak scaling).
+re-sort + Verlet rebuild whenever the accumulated displacement exceeds skin/2).  As the
+workload prescribes, 1,000 Langevin steps (gamma 1, T 1) first melt the lattice into the
+fluid; then W untimed NVE steps; the K timed NVE steps are one espp_run call whose step
+loop is timed by CUDA events on the library's stream (max over ranks).  Under torchrun
+each rank steps its own independent copy of the system on its GPU (replicas, weak
+scaling).
+
+The accuracy block compares the mixed-precision forces with the all-FP64 kernel on the
+same positions, measures NVE energy drift of both precisions on a fixed 2,000-step
+segment, and (1 GPU) compares the pair set of a list built inside the captured step loop
+and the forces with the FP64 CPU oracle at 4,096,000 particles.  other_configs carries
+the Kremer-Grest melt, the 32k LJ fluid and the 64 parallel-tempering replicas (batched
+against sequential).
 
 ``--impl reference`` times the CPU restatement of the reference algorithm (the FP64
 oracle; the reference itself cannot be built on this image: it needs Boost, MPI, FFTW
@@ -268,6 +277,14 @@ def gpu_arm(args, rank, world, local_rank):
             dist.all_reduce(t)
             torch.cuda.synchronize()
 
+    # the workload's protocol: 1,000 Langevin steps (gamma 1, T 1) melt the lattice into
+    # the equilibrated fluid; the timed segment is NVE from that state
+    t_eq = time.perf_counter()
+    if args.equil > 0:
+        call(lib, "espp_langevin_set", h, 1, 1.0, 1.0, 0, None)
+        call(lib, "espp_run", h, args.equil)
+        call(lib, "espp_langevin_set", h, 0, 1.0, 1.0, 0, None)
+    log("rank %d: %d Langevin steps in %.1f s" % (rank, args.equil, time.perf_counter() - t_eq))
     # warm-up (untimed), then pick threads per particle for the force kernel
     call(lib, "espp_run", h, args.warmup)
     tpp = ctypes.c_int32(args.tpp)
@@ -355,33 +372,46 @@ def gpu_arm(args, rank, world, local_rank):
         call(lib, "espp_run", h64, args.warmup)
         tpp64 = ctypes.c_int32()
         call(lib, "espp_autotune", h64, ctypes.byref(tpp64), None)
-        # both precisions step the same K NVE steps from the same state
+        # throughput of the all-FP64 kernel: the same K NVE steps from the same state
+        call(lib, "espp_set_particles", h64, N, i64ptr(pin_ids), dptr(pin_pos), dptr(pin_vel))
+        call(lib, "espp_run", h64, 0)
+        barrier()
+        call(lib, "espp_run", h64, args.steps)
+        barrier()
+        ms64 = np.zeros(2)
+        call(lib, "espp_last_run_ms", h64, dptr(ms64))
+        loop64 = max_over_ranks(dist, float(ms64[1]))
+        # NVE drift on a fixed segment, both precisions from the same state
         call(lib, "espp_set_particles", h64, N, i64ptr(pin_ids), dptr(pin_pos), dptr(pin_vel))
         call(lib, "espp_set_particles", h, N, i64ptr(pin_ids), dptr(pin_pos), dptr(pin_vel))
         call(lib, "espp_run", h64, 0)
         call(lib, "espp_run", h, 0)
         e64_before = total_energy(h64)
         e32_before = total_energy(h)
-        barrier()
-        call(lib, "espp_run", h64, args.steps)
-        barrier()
-        call(lib, "espp_run", h, args.steps)
-        drift64 = (total_energy(h64) - e64_before) / N / (args.steps * DT)
-        drift32 = (total_energy(h) - e32_before) / N / (args.steps * DT)
-        ms64 = np.zeros(2)
-        call(lib, "espp_last_run_ms", h64, dptr(ms64))
-        loop64 = max_over_ranks(dist, float(ms64[1]))
+        call(lib, "espp_run", h64, args.drift_steps)
+        call(lib, "espp_run", h, args.drift_steps)
+        drift64 = (total_energy(h64) - e64_before) / N / (args.drift_steps * DT)
+        drift32 = (total_energy(h) - e32_before) / N / (args.drift_steps * DT)
         lib.espp_system_destroy(h64)
         cmp = {"force_rel_rms_err": rel_rms, "force_rel_max_err": rel_max,
+               "force_rel_max_err_definition": "max over particles of |F_mixed - F_fp64| "
+                                                "divided by the RMS force",
                "fp64_value": world * N * args.steps / (loop64 * 1e-3),
                "fp64_ms_per_step": loop64 / args.steps,
                "mixed_over_fp64": loop64 / loop_ms,
                "fp64_threads_per_particle": int(tpp64.value),
-               "same_segment_nve_drift_per_particle_per_tau": {"mixed": drift32, "fp64": drift64,
-                                                               "e0_per_particle": e64_before / N}}
+               "nve_drift_per_particle_per_tau": {
+                   "mixed": drift32, "fp64": drift64, "e0_per_particle": e64_before / N,
+                   "segment_steps": args.drift_steps,
+                   "definition": "(E_after - E_before) / N / (steps dt), both precisions "
+                                 "stepping the same NVE segment from the same equilibrated "
+                                 "state"}}
+        if rank == 0 and world == 1 and not args.no_oracle:
+            cmp.update(oracle_parity(lib, h, ids, box))
 
     lib.espp_system_destroy(h)
-    configs = small_configs(lib) if (rank == 0 and world == 1 and not args.no_configs) else None
+    configs = (small_configs(lib, args.replica_steps)
+               if (rank == 0 and world == 1 and not args.no_configs) else None)
     if rank != 0:
         if dist is not None:
             dist.barrier()
@@ -436,9 +466,7 @@ def gpu_arm(args, rank, world, local_rank):
                              "launches": [int(x) for x in launches_p[:5]]},
         "gpu_launches": int(launches.sum()),
         "accuracy": dict(cmp, note="forces of the mixed and the all-FP64 kernel on identical "
-                                   "positions; drift = (E_after - E_before) / N / (K dt) with "
-                                   "both precisions stepping the same K NVE steps from the "
-                                   "same state"),
+                                   "positions of the equilibrated fluid"),
         "clocks": clocks,
         "other_configs": configs,
         "e2e": {"value": world * N * args.steps / e2e_s, "unit": "particle-steps/s",
@@ -457,6 +485,59 @@ def gpu_arm(args, rank, world, local_rank):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def oracle_parity(lib, h, ids, box):
+    """The running system's Verlet pair set and mixed-precision forces against the FP64
+    oracle (the CPU restatement of VerletList.cpp:274-450 and the LJ loop) at the same
+    positions.  The system is stepped until a re-sort happens inside the captured step
+    loop, so the list in use was built at the positions the run ends on; the pair sets
+    are compared through espp_vl_digest (each unordered pair once, by id)."""
+    from espressopp_b200 import _abi
+    from espressopp_b200._abi import call, dptr, i32ptr, i64ptr
+    log("oracle parity: stepping to an in-graph re-sort")
+    N = len(ids)
+    r0, r1 = ctypes.c_int64(), ctypes.c_int64()
+    call(lib, "espp_num_resorts", h, ctypes.byref(r0))
+    steps = 0
+    for steps in range(1, 41):
+        call(lib, "espp_run", h, 1)
+        call(lib, "espp_num_resorts", h, ctypes.byref(r1))
+        if r1.value > r0.value:
+            break
+    x = np.zeros((N, 3))
+    f = np.zeros((N, 3))
+    call(lib, "espp_get_particles", h, N, i64ptr(ids), dptr(x), None, dptr(f), None)
+    dg = (ctypes.c_uint64 * 4)()
+    call(lib, "espp_vl_digest", h, dg)
+    t0 = time.perf_counter()
+    olib = _abi.bind(ctypes.CDLL(os.path.join(REPO, "oracle", "_build", "liboracle_espp.so")))
+    ho = ctypes.c_void_p()
+    cg = np.array([int(b / (RC + SKIN)) for b in box], np.int32)
+    call(olib, "espp_system_create", dptr(np.asarray(box, np.float64)), SKIN, i32ptr(cg), 0, 1,
+         ctypes.byref(ho))
+    call(olib, "espp_add_particles", ho, N, i64ptr(ids), None, None,
+         dptr(np.ascontiguousarray(x.reshape(-1))), None)
+    call(olib, "espp_decompose", ho)
+    call(olib, "espp_vl_create", ho, RC, 0, None)
+    call(olib, "espp_lj_set", ho, 0, 0, 1.0, 1.0, RC, 4.0 * (RC ** -12 - RC ** -6), 0.0)
+    call(olib, "espp_integrator_set", ho, DT)
+    call(olib, "espp_run", ho, 0)
+    do = (ctypes.c_uint64 * 4)()
+    call(olib, "espp_vl_digest", ho, do)
+    fo = np.zeros((N, 3))
+    call(olib, "espp_get_particles", ho, N, i64ptr(ids), None, None, dptr(fo), None)
+    olib.espp_system_destroy(ho)
+    df = f - fo
+    log("oracle parity: %d pairs, digests %s, %.1f s" %
+        (do[0], "equal" if list(dg) == list(do) else "DIFFER", time.perf_counter() - t0))
+    return {"pairs_bit_exact_vs_oracle": list(dg) == list(do),
+            "pairs_vs_oracle": {"pairs": int(do[0]), "steps_to_in_graph_resort": steps,
+                                "compared": "espp_vl_digest (count, sum, xor, sum2 of 64-bit "
+                                            "pair hashes)"},
+            "force_rel_rms_err_vs_oracle": float(np.sqrt(np.sum(df * df) / np.sum(fo * fo))),
+            "force_rel_max_err_vs_oracle": float(np.max(np.linalg.norm(df, axis=1)) /
+                                                 np.sqrt(np.mean(np.sum(fo * fo, axis=1))))}
 
 
 # ---- the smaller configurations: Kremer-Grest melt and 32k LJ fluid ----------------
@@ -524,7 +605,7 @@ def lj32k_config(lib, prec, steps=1000):
     return {"value": 32768 * steps / (ms[1] * 1e-3), "ms_per_step": float(ms[1]) / steps}
 
 
-def small_configs(lib):
+def small_configs(lib, replica_steps=1000):
     from espressopp_b200 import _abi
     out = {}
     for name, prec in (("fp64", _abi.PREC_FP64), ("mixed", _abi.PREC_MIXED)):
@@ -533,6 +614,19 @@ def small_configs(lib):
         log("configs: 32k LJ, " + name)
         out["lj_32k_" + name] = lj32k_config(lib, prec)
     out["unit"] = "particle-steps/s (device-timed step loop)"
+    if replica_steps > 0:
+        log("configs: 64 PT replicas, %d steps" % replica_steps)
+        rep, total, seg, segments = run_replicas(lib, _abi.PREC_MIXED, replica_steps, 20)
+        out["pt_replicas_64"] = {
+            "workload": "64 LJ replicas, N ~ U{2000..64000} (seed 4), %d particles, mixed, "
+                        "Langevin T 0.7..2.0, exchange every %d steps, %d steps (config: "
+                        "20,000)" % (total, seg, seg * segments),
+            "batched_value": rep["batched"]["value"],
+            "sequential_value": rep["sequential"]["value"],
+            "batched_over_sequential": rep["batched"]["value"] / rep["sequential"]["value"],
+            "swaps": {"batched": rep["batched"]["swaps"],
+                      "sequential": rep["sequential"]["swaps"]},
+            "unit": "particle-steps/s (wall clock around run calls and exchanges)"}
     return out
 
 
@@ -759,24 +853,20 @@ def mlp_arm(args, rank, world, local_rank):
 
 
 # ---- batched parallel-tempering replicas ------------------------------------------
-def replicas_arm(args, rank, world, local_rank):
-    """64 LJ replicas, N ~ U{2000..64000} (seed 4), rho 0.8442, rc 2.5, skin 0.3,
-    T_r = 0.7 (2.0/0.7)^(r/63), Langevin gamma 1, dt 0.005, Metropolis exchange between
-    neighbours every 100 steps (ParallelTempering.exchange rule).  Times K steps of all
-    replicas with one graph launch per 100-step segment against the same steps run
-    replica by replica (espp_run each), wall clock around the calls."""
-    import espressopp_b200
-    from espressopp_b200 import _abi
+def run_replicas(lib, prec, steps, warmup, R=64):
+    """R LJ replicas, N ~ U{2000..64000} (seed 4), rho 0.8442, rc 2.5, skin 0.3,
+    T_r = 0.7 (2.0/0.7)^(r/(R-1)), Langevin gamma 1, dt 0.005, Metropolis exchange between
+    neighbours every 100 steps (ParallelTempering.exchange rule).  Times `steps` steps of
+    all replicas with one graph launch per 100-step segment (espp_batch_run) against the
+    same steps run replica by replica (espp_run each), wall clock around the calls and
+    exchanges.  Returns ({mode: result}, total particles, steps per segment)."""
     from espressopp_b200._abi import call, dptr, i32ptr, i64ptr
     from espressopp_b200.parallel_tempering import exchange_decisions
-    lib = espressopp_b200.load_library()
-    call(lib, "espp_select_device", local_rank)
-    R = 64
     rng = np.random.Generator(np.random.PCG64(4))
     sizes = rng.integers(2000, 64001, size=R)
     temps = [0.7 * (2.0 / 0.7) ** (r / (R - 1)) for r in range(R)]
 
-    def make(r, prec):
+    def make(r):
         N = int(sizes[r])
         L = (N / RHO) ** (1.0 / 3.0)
         a = int(math.ceil(N ** (1.0 / 3.0)))
@@ -800,7 +890,6 @@ def replicas_arm(args, rank, world, local_rank):
         call(lib, "espp_set_tpp", h, 1)
         return h
 
-    prec = _abi.PREC_MIXED if args.precision == "mixed" else _abi.PREC_FP64
     T = list(temps)
 
     def set_T(hs):
@@ -826,12 +915,12 @@ def replicas_arm(args, rank, world, local_rank):
 
     import random
     total = int(sizes.sum())
-    segments = max(1, args.steps // 100)
-    seg = args.steps // segments
+    segments = max(1, steps // 100)
+    seg = steps // segments
     out = {}
     for mode in ("sequential", "batched"):
         T[:] = temps
-        hs = [make(r, prec) for r in range(R)]
+        hs = [make(r) for r in range(R)]
         set_T(hs)
         b = None
         if mode == "batched":
@@ -847,7 +936,7 @@ def replicas_arm(args, rank, world, local_rank):
                 for h in hs:
                     call(lib, "espp_run", h, n)
 
-        step_all(args.warmup)
+        step_all(warmup)
         swaps = 0
         t0 = time.perf_counter()
         for k in range(segments):
@@ -860,6 +949,18 @@ def replicas_arm(args, rank, world, local_rank):
             lib.espp_batch_destroy(b)
         for h in hs:
             lib.espp_system_destroy(h)
+    return out, total, seg, segments
+
+
+def replicas_arm(args, rank, world, local_rank):
+    """The parallel-tempering workload alone: run_replicas at --steps steps."""
+    import espressopp_b200
+    from espressopp_b200 import _abi
+    from espressopp_b200._abi import call
+    lib = espressopp_b200.load_library()
+    call(lib, "espp_select_device", local_rank)
+    prec = _abi.PREC_MIXED if args.precision == "mixed" else _abi.PREC_FP64
+    out, total, seg, segments = run_replicas(lib, prec, args.steps, args.warmup)
     if rank == 0:
         line = {"metric": "PT replica particle-steps/s, 64 LJ replicas on 1 B200",
                 "value": out["batched"]["value"], "unit": "particle-steps/s", "n_gpus": world,
@@ -900,6 +1001,14 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=20.0)
     ap.add_argument("--steps-ref", type=int, default=1)
     ap.add_argument("--no-fp64", action="store_true", help="skip the all-FP64 comparison")
+    ap.add_argument("--equil", type=int, default=1000,
+                    help="Langevin steps (gamma 1, T 1) before the NVE segment")
+    ap.add_argument("--drift-steps", type=int, default=2000,
+                    help="NVE steps of the drift measurement (both precisions)")
+    ap.add_argument("--replica-steps", type=int, default=1000,
+                    help="steps of the 64-replica measurement in the default line (0: skip)")
+    ap.add_argument("--no-oracle", action="store_true",
+                    help="skip the pair-set and force comparison with the FP64 oracle")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the Kremer-Grest melt and 32k LJ configurations")
     ap.add_argument("--tpp", type=int, default=0, choices=[0, 1, 2, 4, 8],

@@ -30,6 +30,7 @@ PROTOTYPES = {
     "espp_vl_size": (c_int32, [_P, _I64]),
     "espp_vl_pairs": (c_int32, [_P, c_int64, _I64, _I64]),
     "espp_vl_builds": (c_int32, [_P, _I64]),
+    "espp_vl_digest": (c_int32, [_P, POINTER(c_uint64)]),
     "espp_lj_set": (c_int32, [_P, c_int32, c_int32, c_double, c_double, c_double, c_double,
                               c_double]),
     "espp_bonds_add": (c_int32, [_P, c_int64, _I64]),
@@ -58,6 +59,7 @@ PROTOTYPES = {
     "espp_virial_tensor": (c_int32, [_P, c_int32, _D]),
     "espp_kinetic": (c_int32, [_P, _D, _I64]),
     "espp_kinetic_tensor": (c_int32, [_P, _D]),
+    "espp_kinetic_types": (c_int32, [_P, c_uint64, _D, _I64]),
     "espp_rdf": (c_int32, [_P, c_int32, _D]),
     "espp_confs_create": (c_int32, [_P, c_int32, c_int64, _I64, POINTER(c_void_p)]),
     "espp_confs_destroy": (c_int32, [_P]),

@@ -33,13 +33,17 @@ class NPart(_Observable):
 
 
 class Temperature(_Observable):
-    """T = sum m v^2 / (3 N), k_B = 1 (Temperature.hpp:57-126), reduced on the GPU.  After
-    add_type, only particles of the added types count; that selection is summed on the
-    host from one state download."""
+    """T = sum m v^2 / (3 N), k_B = 1 (Temperature.hpp:57-126), reduced on the GPU in
+    FP64.  After add_type, only particles of the added types count (valid_type_ids):
+    types 0..63 are selected by a bit mask inside the same device reduction; a larger
+    type id is summed from one state download.  With no (selected) particle the result
+    is sumT / (3 * 0) = nan, as in the reference.  getEkin returns 0.5 sum m v^2 of the
+    last compute."""
 
     def __init__(self, system):
         _Observable.__init__(self, system)
         self._valid_types = set()
+        self._ekin = 0.0
 
     def add_type(self, type_id):
         self._valid_types.add(int(type_id))
@@ -50,21 +54,33 @@ class Temperature(_Observable):
             return True
         return False
 
-    def compute(self):
-        if not self._valid_types:
-            v2, n = self._kinetic()
-            return v2 / (3.0 * n) if n else 0.0
+    def _typed(self):
         st = self._st()
+        if all(0 <= t < 64 for t in self._valid_types):
+            mask = 0
+            for t in self._valid_types:
+                mask |= 1 << t
+            v = ctypes.c_double()
+            n = ctypes.c_int64()
+            call(st._lib, "espp_kinetic_types", st._h, ctypes.c_uint64(mask), ctypes.byref(v),
+                 ctypes.byref(n))
+            return v.value, n.value
         ids, _, vel, _, _ = st.getAll()
-        sel = [k for k, pid in enumerate(ids) if st._types[int(pid)] in self._valid_types]
-        if not sel:
-            return float("nan")
-        m = np.array([st._masses[int(ids[k])] for k in sel])
-        v = vel[sel]
-        return float(np.sum(m * np.sum(v * v, axis=1))) / (3.0 * len(sel))
+        types = np.array([st._types[int(p)] for p in ids], np.int64)
+        masses = np.array([st._masses[int(p)] for p in ids], np.float64)
+        sel = np.isin(types, np.array(sorted(self._valid_types), np.int64))
+        return float(np.sum(masses[sel] * np.sum(vel[sel] ** 2, axis=1))), int(sel.sum())
+
+    def compute(self):
+        v2, n = self._typed() if self._valid_types else self._kinetic()
+        self._ekin = 0.5 * v2
+        return v2 / (3.0 * n) if n else float("nan")
 
     def compute_real(self):
         return self.compute()
+
+    def getEkin(self):
+        return self._ekin
 
 
 class Pressure(_Observable):

@@ -7,6 +7,7 @@
 // with the Langevin heat-up factor, then per step integrate1 -> (re-sort + list build
 // when the accumulated max displacement exceeds skin/2) -> forces -> aftCalcF ->
 // integrate2.  integrate2 of step n and integrate1 of step n+1 run as one kernel.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -1384,15 +1385,48 @@ constexpr int kNoAllocMaxBlocks = 32768;
 constexpr long long kNoAllocMaxParticles = (long long)kNoAllocMaxBlocks * 256;
 static __device__ __align__(256) double g_noalloc_scratch[8 + 7 * kNoAllocMaxBlocks];
 
-// Device address of g_noalloc_scratch per device, looked up once with that device
-// current (the host-side name of the array is only a stand-in, not a device address).
+// Device address of g_noalloc_scratch per device, looked up with that device current
+// (the host-side name of the array is only a stand-in, not a device address).  The
+// address belongs to the context the module was loaded into: a caller that resets the
+// device or releases and retains its primary context gets the module loaded again,
+// possibly elsewhere.  So each cached address is stored with the unique id of the
+// context it was looked up in (cuCtxGetId) and looked up again when the current
+// context's id differs.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
 std::mutex g_noalloc_mutex;
 double* g_noalloc_addr[256] = {nullptr};
+unsigned long long g_noalloc_ctx[256] = {0};
+
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  if (!get_current || !get_id) {
+    void* f0 = nullptr;
+    void* f1 = nullptr;
+    cudaDriverEntryPointQueryResult q0, q1;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0) != cudaSuccess ||
+        q0 != cudaDriverEntryPointSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || !f0 || !f1) {
+      cudaGetLastError();
+      raise(ESPP_ECUDA, "driver entry points cuCtxGetCurrent / cuCtxGetId unavailable");
+    }
+    get_current = (CtxGetCurrentFn)f0;
+    get_id = (CtxGetIdFn)f1;
+  }
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+    raise(ESPP_ECUDA, "no current CUDA context for the energy scratch lookup");
+  return id;
+}
 
 double* noalloc_scratch(int device) {
   if (device < 0 || device >= 256) raise(ESPP_ERANGE, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_addr[device]) {
+  const unsigned long long ctx = current_context_id();
+  if (!g_noalloc_addr[device] || g_noalloc_ctx[device] != ctx) {
     void* ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
     if (e != cudaSuccess || !ptr) {
@@ -1401,6 +1435,7 @@ double* noalloc_scratch(int device) {
                             cudaGetErrorString(e));
     }
     g_noalloc_addr[device] = (double*)ptr;
+    g_noalloc_ctx[device] = ctx;
   }
   return g_noalloc_addr[device];
 }
@@ -1719,6 +1754,24 @@ int espp_vl_size(espp_system* s, int64_t* npairs) {
     int64_t t = 0;
     for (int32_t c : h) t += c;
     *npairs = t;
+  });
+}
+
+int espp_vl_digest(espp_system* s, uint64_t out[4]) {
+  return guard([&] {
+    checked(s);
+    if (!out) raise(ESPP_EINVAL, "null output pointer");
+    for (int k = 0; k < 4; ++k) out[k] = 0;
+    if (!s->has_vl || s->n == 0) return;
+    int nb;
+    // the observable partials hold 7 doubles per block; the digest needs 4 words
+    unsigned long long* part = reinterpret_cast<unsigned long long*>(obs_partials(s, nb));
+    unsigned long long* res = reinterpret_cast<unsigned long long*>(s->obs);
+    launch_pair_digest(s->view(), part, nb, res, s->st);
+    cuda_check(cudaGetLastError(), "digest kernels");
+    cuda_check(cudaMemcpyAsync(out, res, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost, s->st),
+               "download");
+    sync(s);
   });
 }
 
@@ -2055,6 +2108,25 @@ int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n) {
     cuda_check(cudaMemcpyAsync(sum_mv2, s->obs, sizeof(double), cudaMemcpyDeviceToHost, s->st),
                "download");
     sync(s);
+  });
+}
+
+int espp_kinetic_types(espp_system* s, uint64_t type_mask, double* sum_mv2, int64_t* n) {
+  return guard([&] {
+    checked(s);
+    if (!sum_mv2 || !n) raise(ESPP_EINVAL, "null output pointer");
+    *sum_mv2 = 0.0;
+    *n = 0;
+    if (s->n == 0 || type_mask == 0) return;
+    int nb;
+    double* part = obs_partials(s, nb);
+    launch_kinetic_types(s->view(), (unsigned long long)type_mask, part, nb, s->obs, s->st);
+    double out[2];
+    cuda_check(cudaMemcpyAsync(out, s->obs, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st),
+               "download");
+    sync(s);
+    *sum_mv2 = out[0];
+    *n = (int64_t)out[1];
   });
 }
 

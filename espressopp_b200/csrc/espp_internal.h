@@ -234,10 +234,16 @@ void launch_kinetic(const DevView& d, double* partials, int nblocks, double* out
                     cudaStream_t st);
 void launch_kinetic_tensor(const DevView& d, double* partials, int nblocks, double* out,
                            cudaStream_t st);
+// sum m v^2 (out[0]) and count (out[1]) over the particles of the types in typeMask
+void launch_kinetic_types(const DevView& d, unsigned long long typeMask, double* partials,
+                          int nblocks, double* out, cudaStream_t st);
 // Verlet pair export: counts per particle (pairs with id_j > id_i), then the pairs.
 void launch_pair_count(const DevView& d, int32_t* counts, cudaStream_t st);
 void launch_pair_write(const DevView& d, const int64_t* offsets, int64_t* out,
                        cudaStream_t st);
+// order-independent digest of the Verlet pair set: out[0..4) = count, sum, xor, sum2
+void launch_pair_digest(const DevView& d, unsigned long long* partials, int nblocks,
+                        unsigned long long* out, cudaStream_t st);
 void launch_bond_maxsq(const DevView& d, double* partials, int nblocks, double* out,
                        cudaStream_t st);
 

@@ -2,7 +2,7 @@
 //
 //  re-binning     k_fold_bin -> k_scan_cells -> k_scatter -> k_sort_in_cell -> k_gather
 //                 (storage::DomainDecomposition::decomposeRealParticles, one node)
-//  Verlet list    k_build_nl_lane (k_build_nl_tc: tcgen05 distance prefilter, opt-in):
+//  Verlet list    k_build_nl_lane:
 //                 FP32 test with the reference's FP64 ghost-shift arithmetic near the
 //                 cutoff, full per-particle list (VerletList::_rebuildUsingBuffers)
 //  forces         k_force_mixed (FP32 on box-wrapped int32 coordinates, int64 2^-32
@@ -15,8 +15,6 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
-
-#include <cuda_fp16.h>
 
 #include "espp_internal.h"
 #include "espp_tab.h"
@@ -607,308 +605,6 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build_nl_lane(DevView d, d
     const int wmax = __reduce_max_sync(0xffffffffu, own ? total : 0);
     if (lane == 0 && wmax > 0) atomicMax(&d.ctr->nnMax, wmax);
     __syncwarp();
-  }
-}
-
-// ---- Verlet build with a tensor-core distance prefilter ----------------------------
-// Tiles of whole cells of one x-row of the cell grid (at most 128 particles, at most
-// kTbMaxCells cells; a cell with more particles is split into tiles of 128).  The
-// tile's candidates are the particles of its 9 stencil rows over the x-cells from one
-// before to one after the tile ("columns"), enumerated column-major.  Chunks of 128
-// candidates are staged in shared memory and one tcgen05.mma (kind::f16, M = N = 128,
-// K = 16, FP32 accumulators in TMEM) gives for every (tile particle, candidate) slot
-//   D = |x_i|^2 + |x_j|^2 - 2 x_i.x_j - thr,   thr = 1.02 (rc+skin)^2 + 0.05,
-// with the coordinates in a frame centred on the tile and each coordinate carried as an
-// FP16 pair (hi + lo: 22 significant bits); the neglected lo*lo products and the FP32
-// accumulation leave an error far below the margin in thr.  Thread t reads its row of D
-// with tcgen05.ld and collects the sign bits; only those candidates (about 1.02 times
-// the neighbours) are tested exactly, in FP32, with the same borderline band and FP64
-// decision (exact_pair_test) as the other build forms, and against the 27-cell stencil
-// of the particle's own cell.  The pair set is therefore the reference's
-// (VerletList.cpp:274-450); each list is in a fixed order (column-major candidates).
-constexpr int kTbRows = 128;                    // tile particles (MMA M)
-constexpr int kTbN = 128;                       // candidates per chunk (MMA N, TMEM columns)
-constexpr int kTbMaxCells = 32;                 // cells per tile
-constexpr int kTbMaxW = kTbMaxCells + 2;        // candidate columns
-constexpr int kTbSegs = 9 * kTbMaxW;            // (column, stencil row) segments
-constexpr int kTbSmem = 50 * 1024;              // dynamic shared memory: at most 4 CTAs / SM
-
-struct TbSmem {
-  alignas(128) uint8_t A[kTbRows * 32];          // tile particles: 16 FP16 terms each
-  alignas(128) uint8_t B[2][kTbN * 32];          // candidates: 16 FP16 terms each
-  float4 cand[2][kTbN];                          // x, y, z in the tile frame; j as bits
-  int cseg[2][kTbN];                             // segment (column * 9 + row) of each
-  int cw[2][2];                                  // first and last column of the chunk
-  int segStart[kTbSegs];
-  int segPre[kTbSegs + 1];
-  alignas(16) int stage[kTbRows * kStageLd];  // rows read and written as 16-byte vectors
-  alignas(8) unsigned long long mbar;
-  uint32_t tmem;
-  int abort;
-};
-static_assert(sizeof(TbSmem) + 128 <= kTbSmem, "tile build shared memory");
-static_assert(offsetof(TbSmem, stage) % 16 == 0 && (kStageLd * 4) % 16 == 0,
-              "staging rows are accessed as 16-byte vectors");
-static_assert(offsetof(TbSmem, cand) % 16 == 0, "candidates are read as 16-byte vectors");
-
-__device__ __forceinline__ uint32_t pack_h2(float a, float b) {
-  const __half2 h = __floats2half2_rn(a, b);
-  return *reinterpret_cast<const uint32_t*>(&h);
-}
-__device__ __forceinline__ void split_h(float v, float& hi, float& lo) {
-  hi = __half2float(__float2half_rn(v));
-  lo = v - hi;
-}
-
-template <bool EXCL>
-__global__ void __launch_bounds__(kTbRows, 4) k_build_nl_tc(DevView d, double cutsq) {
-  extern __shared__ __align__(128) uint8_t tb_raw[];
-  TbSmem& S = *reinterpret_cast<TbSmem*>(((uintptr_t)tb_raw + 127) & ~(uintptr_t)127);
-  const ParticleArrays a = d.pa[0];
-  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  const int nx = d.nc[0], ny = d.nc[1], nz = d.nc[2];
-  const float lo = (float)(cutsq * (1.0 - 2e-5)), hi = (float)(cutsq * (1.0 + 2e-5));
-  const float thr = (float)(cutsq * 1.02 + 0.05);
-  const float hx = (float)d.cellSize[0], hy = (float)d.cellSize[1], hz = (float)d.cellSize[2];
-  const float4* __restrict__ xr = d.xrel;
-  const int* __restrict__ cs = d.cellStart;
-  const int K = d.K;
-  const size_t cap = d.cap;
-  int* __restrict__ nl = d.nl;
-  int* __restrict__ srow = &S.stage[t * kStageLd];
-  const uint32_t mbar = tc::smem_u32(&S.mbar);
-  if (t == 0) {
-    S.abort = 0;
-    tc::mbar_init(mbar);
-  }
-  if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tmem), kTbN);
-  tc::fence_before();
-  __syncthreads();
-  tc::fence_after();
-  const uint32_t tmem = S.tmem;
-  const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
-  const uint32_t idesc = tc::idesc_f16(kTbRows, kTbN, false);
-  const uint64_t dA = tc::desc(tc::smem_u32(S.A), kTbRows);
-  uint32_t phase = 0;
-  bool abort = false;
-  int nmax = 0;
-  for (int row = blockIdx.x; row < ny * nz && !abort; row += gridDim.x) {
-    const int cy = row % ny, cz = row / ny;
-    const int rb = nx * row;
-    for (int ca = 0; ca < nx && !abort;) {
-      // the tile: cells ca..cb of this row, together at most 128 particles (or one cell)
-      int cb = ca;
-      while (cb + 1 < nx && cb + 1 - ca < kTbMaxCells && cs[rb + cb + 2] - cs[rb + ca] <= kTbRows)
-        ++cb;
-      const int p0 = cs[rb + ca], p1 = cs[rb + cb + 1];
-      if (p0 == p1) {
-        ca = cb + 1;
-        continue;
-      }
-      const int c0 = ca - 1, W = cb - ca + 3;
-      const float wc = 0.5f * (float)W;
-      // candidate segments (column w, stencil row rr), column-major
-      __syncthreads();  // the previous tile's readers of the segment table are done
-      for (int s = t; s < 9 * W; s += kTbRows) {
-        const int w = s / 9, rr = s % 9;
-        const int oz = rr / 3 - 1, oy = rr % 3 - 1;
-        int ncy = cy + oy, ncz = cz + oz;
-        ncy += ncy < 0 ? ny : (ncy >= ny ? -ny : 0);
-        ncz += ncz < 0 ? nz : (ncz >= nz ? -nz : 0);
-        int ncx = (c0 + w) % nx;
-        ncx += ncx < 0 ? nx : 0;
-        const int cell = ncx + nx * (ncy + ny * ncz);
-        S.segStart[s] = cs[cell];
-        S.segPre[s] = cs[cell + 1] - cs[cell];
-      }
-      __syncthreads();
-      if (warp == 0) {
-        int run = 0;
-        for (int base = 0; base < 9 * W; base += 32) {
-          const int s = base + lane;
-          const int c = s < 9 * W ? S.segPre[s] : 0;
-          int incl = c;
-#pragma unroll
-          for (int o = 1; o < 32; o <<= 1) {
-            const int u = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += u;
-          }
-          if (s < 9 * W) S.segPre[s] = run + incl - c;
-          run += __shfl_sync(0xffffffffu, incl, 31);
-        }
-        if (lane == 0) S.segPre[9 * W] = run;
-      }
-      __syncthreads();
-      const int ncand = S.segPre[9 * W];
-      const int nchunks = (ncand + kTbN - 1) / kTbN;
-      for (int s0 = p0; s0 < p1 && !abort; s0 += kTbRows) {
-        __syncthreads();  // the previous sub-tile's readers of the chunk buffers are done
-        const int ni = min(kTbRows, p1 - s0);
-        const bool own = t < ni;
-        const int i = own ? s0 + t : s0;
-        // this particle in the tile frame, and its column
-        const float4 ri = xr[i];
-        const int wi = d.pcell[i] % nx - c0;
-        const float xi = ri.x + ((float)wi - wc) * hx, yi = ri.y - 0.5f * hy, zi = ri.z - 0.5f * hz;
-        {
-          float xh, xl, yh, yl, zh, zl, sh, sl;
-          split_h(xi, xh, xl);
-          split_h(yi, yh, yl);
-          split_h(zi, zh, zl);
-          split_h(xi * xi + yi * yi + zi * zi, sh, sl);
-          uint4 q0, q1;
-          if (own) {
-            q0 = make_uint4(pack_h2(xh, xl), pack_h2(xh, yh), pack_h2(yl, yh), pack_h2(zh, zl));
-            q1 = make_uint4(pack_h2(zh, sh), pack_h2(sl, 1.f), pack_h2(1.f, 0.f), 0u);
-          } else {
-            q0 = make_uint4(0u, 0u, 0u, 0u);
-            q1 = q0;
-          }
-          *reinterpret_cast<uint4*>(S.A + tc::canon_off(t, 0, kTbRows)) = q0;
-          *reinterpret_cast<uint4*>(S.A + tc::canon_off(t, 8, kTbRows)) = q1;
-        }
-        const int64_t idi = (EXCL && own) ? a.id[i] : -3;
-        // column range of this warp's particles (for skipping far chunks)
-        const int wlo = __reduce_min_sync(0xffffffffu, own ? wi : 1 << 20);
-        const int whi = __reduce_max_sync(0xffffffffu, own ? wi : -(1 << 20));
-        int pend = 0, blk = 0;
-        for (int q = 0; q < nchunks; ++q) {
-          const int buf = q & 1;
-          // stage candidate q * 128 + t
-          {
-            const int n = q * kTbN + t;
-            uint4 q0 = make_uint4(0u, 0u, 0u, 0u), q1 = q0;
-            int sg = -1;
-            if (n < ncand) {
-              int lo_s = 0, hi_s = 9 * W - 1;  // largest s with segPre[s] <= n
-              while (lo_s < hi_s) {
-                const int mid = (lo_s + hi_s + 1) >> 1;
-                if (S.segPre[mid] <= n) lo_s = mid;
-                else hi_s = mid - 1;
-              }
-              sg = lo_s;
-              const int w = sg / 9, rr = sg % 9;
-              const int j = S.segStart[sg] + (n - S.segPre[sg]);
-              const float4 rj = xr[j];
-              const float fx = rj.x + ((float)w - wc) * hx;
-              const float fy = rj.y + ((float)(rr % 3 - 1) - 0.5f) * hy;
-              const float fz = rj.z + ((float)(rr / 3 - 1) - 0.5f) * hz;
-              S.cand[buf][t] = make_float4(fx, fy, fz, __int_as_float(j));
-              float xh, xl, yh, yl, zh, zl, th, tlw;
-              split_h(-2.f * fx, xh, xl);
-              split_h(-2.f * fy, yh, yl);
-              split_h(-2.f * fz, zh, zl);
-              split_h(fx * fx + fy * fy + fz * fz - thr, th, tlw);
-              q0 = make_uint4(pack_h2(xh, xh), pack_h2(xl, yh), pack_h2(yh, yl), pack_h2(zh, zh));
-              q1 = make_uint4(pack_h2(zl, 1.f), pack_h2(1.f, th), pack_h2(tlw, 0.f), 0u);
-            } else {
-              // no candidate: D = 60000 > 0
-              q1 = make_uint4(0u, pack_h2(0.f, 60000.f), 0u, 0u);
-            }
-            S.cseg[buf][t] = sg;
-            *reinterpret_cast<uint4*>(S.B[buf] + tc::canon_off(t, 0, kTbN)) = q0;
-            *reinterpret_cast<uint4*>(S.B[buf] + tc::canon_off(t, 8, kTbN)) = q1;
-            if (t == 0) S.cw[buf][0] = sg / 9;
-            const int last = min(kTbN, ncand - q * kTbN) - 1;
-            if (t == last) S.cw[buf][1] = sg / 9;
-          }
-          tc::fence_async_smem();
-          tc::fence_before();
-          __syncthreads();
-          tc::fence_after();
-          if (S.abort) {
-            abort = true;
-            break;
-          }
-          if (t == 0) {
-            tc::mma_f16(tmem, dA, tc::desc(tc::smem_u32(S.B[buf]), kTbN), idesc, 0);
-            tc::commit(mbar);
-          }
-          if (!tc::mbar_wait(mbar, phase)) {
-            S.abort = 1;
-            atomicOr(d.err, kErrTimeout);
-          }
-          phase ^= 1u;
-          tc::fence_after();
-          // warps whose particles are more than one column away from the whole chunk
-          // skip it (all its candidates are outside their stencils)
-          if (whi >= 0 && S.cw[buf][1] >= wlo - 1 && S.cw[buf][0] <= whi + 1) {
-#pragma unroll 1
-            for (int h = 0; h < kTbN / 32; ++h) {
-              uint32_t v[32];
-              tc::tmem_ld32(tl + 32 * h, v);
-              tc::wait_ld();
-              uint32_t m = 0;
-#pragma unroll
-              for (int k = 0; k < 32; ++k) m = __funnelshift_l(v[k], m, 1);
-              m = own ? __brev(m) : 0u;
-              while (m) {
-                const int b = __ffs(m) - 1;
-                m &= m - 1;
-                const int n = 32 * h + b;
-                const int sg = S.cseg[buf][n];
-                const int w = sg / 9;
-                const int ox = w - wi;
-                if (ox < -1 || ox > 1) continue;
-                const float4 c = S.cand[buf][n];
-                const int j = __float_as_int(c.w);
-                if (j == i) continue;
-                const float dx = xi - c.x, dy = yi - c.y, dz = zi - c.z;
-                const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-                bool in;
-                if (r2 < lo) {
-                  in = true;
-                } else if (r2 > hi) {
-                  in = false;
-                } else {
-                  const int rr = sg % 9;
-                  const int oz = rr / 3 - 1, oy = rr % 3 - 1;
-                  const int cxi = wi + c0;
-                  const int wx = cxi + ox < 0 ? -1 : (cxi + ox >= nx ? 1 : 0);
-                  const int ncy = cy + oy, ncz = cz + oz;
-                  const int wy = ncy < 0 ? -1 : (ncy >= ny ? 1 : 0);
-                  const int wz = ncz < 0 ? -1 : (ncz >= nz ? 1 : 0);
-                  const bool fwd = oz > 0 || (oz == 0 && (oy > 0 || (oy == 0 && ox > 0)));
-                  in = exact_pair_test_inl(a.x, d.cap, i, j, fwd, wx * d.L[0], wy * d.L[1],
-                                       wz * d.L[2], cutsq);
-                }
-                if (EXCL && in && is_excluded(d, idi, a.id[j])) in = false;
-                if (in) srow[pend++] = j;
-              }
-              if (pend >= 8) stage_flush(srow, pend, blk, nl, i, cap, K >> 3);
-            }
-          }
-          tc::fence_before();
-        }
-        if (abort) break;
-        const int total = blk * 8 + pend;
-        if (own) {
-          if (total > K) atomicOr(d.err, kErrNlOverflow);
-          d.nn[i] = min(total, K);
-          // pad to a multiple of 8 with the particle itself (r^2 = 0, masked by the
-          // force kernels) so that batches of 8 need no bounds checks
-          if (pend > 0) {
-            for (int k = pend; k < 8; ++k) srow[k] = i;
-            pend = 8;
-            stage_flush(srow, pend, blk, nl, i, cap, K >> 3);
-          }
-          nmax = max(nmax, total);
-        }
-      }
-      ca = cb + 1;
-    }
-  }
-  const int wmax = __reduce_max_sync(0xffffffffu, nmax);
-  if (lane == 0 && wmax > 0) atomicMax(&d.ctr->nnMax, wmax);
-  tc::fence_before();
-  __syncthreads();
-  // after a timed-out wait, give the outstanding product its own bounded wait before the
-  // tensor memory is released
-  if (S.abort && t == 0) tc::mbar_wait(mbar, phase);
-  __syncthreads();
-  if (warp == 0) {
-    tc::fence_after();
-    tc::tmem_dealloc(tmem, kTbN);
   }
 }
 
@@ -1889,6 +1585,23 @@ __global__ void k_kinetic(DevView d, double* partials) {
   block_sum_store<1>(acc, partials);
 }
 
+// sum m v^2 and count of the particles whose type t < 64 has bit t set in typeMask
+// (Temperature::compute_real with add_type, Temperature.hpp:57-125)
+__global__ void k_kinetic_types(DevView d, unsigned long long typeMask, double* partials) {
+  const ParticleArrays a = d.pa[0];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[2] = {0.0, 0.0};
+  if (i < d.n) {
+    const int t = a.type[i];
+    if (t >= 0 && t < 64 && ((typeMask >> t) & 1ull)) {
+      const double vx = a.v[i], vy = a.v[(size_t)d.cap + i], vz = a.v[2 * (size_t)d.cap + i];
+      acc[0] = a.mass[i] * (vx * vx + vy * vy + vz * vz);
+      acc[1] = 1.0;
+    }
+  }
+  block_sum_store<2>(acc, partials);
+}
+
 // mass * Tensor(v, v) of each particle: (xx, yy, zz, xy, xz, yz), m (v_a v_b)
 __global__ void k_kinetic_tensor(DevView d, double* partials) {
   const ParticleArrays a = d.pa[0];
@@ -1933,6 +1646,75 @@ __global__ void k_pair_write(DevView d, const int64_t* offsets, int64_t* out) {
   }
 }
 
+// Order-independent digest of the pair set: each unordered pair once (from the particle
+// with the smaller id), hashed as mix(mix(smaller id) ^ larger id) with the splitmix64
+// finaliser (Steele, Lea and Flood, OOPSLA 2014); per block the count, the wrapping sum,
+// the xor and the wrapping sum of a second hash.  Integer sums: the result does not
+// depend on the order of the lists.
+__device__ __forceinline__ unsigned long long digest_mix(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ void digest_block_store(unsigned long long (&v)[4],
+                                                   unsigned long long* partials) {
+  __shared__ unsigned long long sm[4][kBlock / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], o);
+    v[1] += __shfl_xor_sync(0xffffffffu, v[1], o);
+    v[2] ^= __shfl_xor_sync(0xffffffffu, v[2], o);
+    v[3] += __shfl_xor_sync(0xffffffffu, v[3], o);
+  }
+  if ((threadIdx.x & 31) == 0)
+    for (int c = 0; c < 4; ++c) sm[c][threadIdx.x >> 5] = v[c];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t[4] = {0ull, 0ull, 0ull, 0ull};
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) {
+      t[0] += sm[0][w];
+      t[1] += sm[1][w];
+      t[2] ^= sm[2][w];
+      t[3] += sm[3][w];
+    }
+    for (int c = 0; c < 4; ++c) partials[(size_t)blockIdx.x * 4 + c] = t[c];
+  }
+}
+
+__global__ void k_pair_digest(DevView d, unsigned long long* partials) {
+  const ParticleArrays a = d.pa[0];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long v[4] = {0ull, 0ull, 0ull, 0ull};
+  if (i < d.n) {
+    const int64_t idi = a.id[i];
+    const unsigned long long hi0 = digest_mix((unsigned long long)idi);
+    for (int k = 0; k < d.nn[i]; ++k) {
+      const int64_t idj = a.id[d.nl[nl_index(k, i, d.cap)]];
+      if (idj > idi) {
+        const unsigned long long h = digest_mix(hi0 ^ (unsigned long long)idj);
+        v[0] += 1ull;
+        v[1] += h;
+        v[2] ^= h;
+        v[3] += digest_mix(h);
+      }
+    }
+  }
+  digest_block_store(v, partials);
+}
+
+__global__ void k_digest_reduce(const unsigned long long* partials, int nb,
+                                unsigned long long* out) {
+  unsigned long long v[4] = {0ull, 0ull, 0ull, 0ull};
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    v[0] += partials[(size_t)b * 4];
+    v[1] += partials[(size_t)b * 4 + 1];
+    v[2] ^= partials[(size_t)b * 4 + 2];
+    v[3] += partials[(size_t)b * 4 + 3];
+  }
+  digest_block_store(v, out);
+}
 
 // Particle state by id through the dense id map: scatter host rows into the sorted
 // arrays / gather them back out (Storage::lookupRealParticle on the device).
@@ -2047,33 +1829,7 @@ void launch_posq(const DevView& d, cudaStream_t st) {
   if (d.n > 0) k_posq<<<blocks_for(d.n), kBlock, 0, st>>>(d);
 }
 
-// The particle-per-lane form is the default; ESPP_B200_BUILD=tc selects the form with the
-// tensor-core prefilter (same pair set, slower on the LJ benchmark: its survivor pass is
-// latency-bound).
 void launch_build_nl(const DevView& d, double cutsq, cudaStream_t st) {
-  const char* form = getenv("ESPP_B200_BUILD");
-  // the tensor-core form keeps every tile-frame coordinate well inside the FP16 range
-  const bool tcok = d.nc[0] >= 3 && (0.5 * kTbMaxW + 1.0) * d.cellSize[0] <= 100.0 &&
-                    2.0 * d.cellSize[1] <= 100.0 && 2.0 * d.cellSize[2] <= 100.0;
-  if (form && !strcmp(form, "tc") && tcok) {
-    static int nsm[64] = {0};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    dev &= 63;
-    if (!nsm[dev]) {
-      cudaFuncSetAttribute(k_build_nl_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmem);
-      cudaFuncSetAttribute(k_build_nl_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmem);
-      cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
-      if (nsm[dev] <= 0) nsm[dev] = 148;
-    }
-    const int rows = d.nc[1] * d.nc[2];
-    const int grid = rows < 4 * nsm[dev] ? rows : 4 * nsm[dev];
-    if (d.exclStart)
-      k_build_nl_tc<true><<<grid, kTbRows, kTbSmem, st>>>(d, cutsq);
-    else
-      k_build_nl_tc<false><<<grid, kTbRows, kTbSmem, st>>>(d, cutsq);
-    return;
-  }
   const int nb = blocks_for((long long)d.ncells * 32, kBuildWarps * 32);
   if (d.exclStart)
     k_build_nl_lane<true><<<nb, kBuildWarps * 32, 0, st>>>(d, cutsq);
@@ -2265,6 +2021,12 @@ void launch_kinetic(const DevView& d, double* partials, int nblocks, double* out
   k_sum_partials<1><<<1, 256, 0, st>>>(partials, nblocks, out);
 }
 
+void launch_kinetic_types(const DevView& d, unsigned long long typeMask, double* partials,
+                          int nblocks, double* out, cudaStream_t st) {
+  k_kinetic_types<<<nblocks, kBlock, 0, st>>>(d, typeMask, partials);
+  k_sum_partials<2><<<1, 256, 0, st>>>(partials, nblocks, out);
+}
+
 void launch_kinetic_tensor(const DevView& d, double* partials, int nblocks, double* out,
                            cudaStream_t st) {
   k_kinetic_tensor<<<nblocks, kBlock, 0, st>>>(d, partials);
@@ -2284,6 +2046,12 @@ void launch_pair_count(const DevView& d, int32_t* counts, cudaStream_t st) {
 void launch_pair_write(const DevView& d, const int64_t* offsets, int64_t* out,
                        cudaStream_t st) {
   if (d.n > 0) k_pair_write<<<blocks_for(d.n), kBlock, 0, st>>>(d, offsets, out);
+}
+
+void launch_pair_digest(const DevView& d, unsigned long long* partials, int nblocks,
+                        unsigned long long* out, cudaStream_t st) {
+  k_pair_digest<<<nblocks, kBlock, 0, st>>>(d, partials);
+  k_digest_reduce<<<1, kBlock, 0, st>>>(partials, nblocks, out);
 }
 
 int observable_blocks(int n) { return blocks_for(n > 0 ? n : 1); }

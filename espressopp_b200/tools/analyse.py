@@ -33,10 +33,16 @@ def info(system, integrator, per_atom=False):
 
 
 def final_info(system, integrator, vl, start_time, end_time):
-    NPart = system.storage.getNRealParticles()
-    print("total time: %.1f" % (end_time - start_time))
-    print("number of particles:", NPart)
-    print("number of verlet-list pairs:", vl.totalSize())
-    print("neighbours per particle: %.2f" % (vl.totalSize() / float(NPart)))
-    print("number of verlet-list builds:", vl.builds)
-    print("number of resorts:", integrator.getNumResorts())
+    """Final report (src/tools/analyse.py:66-76): the integrator's timers, the Verlet
+    list's size, neighbours per particle and builds, the step count, and the wall time
+    of the one process that drives the GPU (the reference prints its MPI rank count and
+    the time per rank on that line)."""
+    from .. import analysis
+    from . import timers
+    NPart = analysis.NPart(system).compute()
+    timers.show(integrator.getTimers(), precision=3)
+    sys.stdout.write("Total # of neighbors = %d\n" % vl.totalSize())
+    sys.stdout.write("Ave neighs/atom = %.1f\n" % (vl.totalSize() / float(NPart)))
+    sys.stdout.write("Neighbor list builds = %d\n" % vl.builds)
+    sys.stdout.write("Integration steps = %d\n" % integrator.step)
+    sys.stdout.write("CPUs = %i CPU time per CPU = %.5f\n" % (1, end_time - start_time))

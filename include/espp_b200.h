@@ -114,6 +114,13 @@ ESPP_API int espp_vl_size(espp_system* s, int64_t* npairs);
  * Writes at most cap pairs (2*cap int64); *npairs receives the total. */
 ESPP_API int espp_vl_pairs(espp_system* s, int64_t cap, int64_t* pairs, int64_t* npairs);
 ESPP_API int espp_vl_builds(espp_system* s, int64_t* builds);
+/* Order-independent digest of the Verlet pair set, each unordered pair once by id:
+ * out[0] the number of pairs, out[1] the wrapping sum and out[2] the xor of the 64-bit
+ * hash h = mix(mix(smaller id) ^ larger id) (mix: the splitmix64 finaliser), out[3] the
+ * wrapping sum of mix(h).  Equal pair sets give equal digests whatever the list order;
+ * it compares lists of millions of pairs without exporting them (the reference's
+ * VerletList::getAllPairs, VerletList.cpp:515-536, exports the pairs themselves). */
+ESPP_API int espp_vl_digest(espp_system* s, uint64_t out[4]);
 
 /* ---- interaction::LennardJones / LennardJonesCapped on the Verlet list -------------
  * VerletListInteractionTemplate::setPotential (src/interaction/
@@ -227,6 +234,10 @@ ESPP_API int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n);
 /* sum over real particles of mass * Tensor(v, v) (analysis/PressureTensor.hpp:60-70):
  * out = (xx, yy, zz, xy, xz, yz), each m (v_a v_b). */
 ESPP_API int espp_kinetic_tensor(espp_system* s, double out[6]);
+/* Sum of m v^2 and count over the particles whose type t (0 <= t < 64) has bit t set in
+ * type_mask: Temperature::compute_real with add_type (src/analysis/Temperature.hpp:57-125,
+ * valid_type_ids). */
+ESPP_API int espp_kinetic_types(espp_system* s, uint64_t type_mask, double* sum_mv2, int64_t* n);
 
 /* analysis::RadialDistrF::computeArray(rdfN) (src/analysis/RadialDistrF.cpp:47-150): histogram
  * of all pair distances (minimum image) in rdfN bins of width dr = L_y / (2 rdfN), each
@@ -322,7 +333,10 @@ ESPP_API int espp_mlp_adam_step(espp_mlp* m, double lr, double beta1, double bet
  *   - The system must be ready: particles sorted and, for ESPP_IA_LJ, the Verlet list
  *     built (after espp_decompose, espp_run or espp_energy); otherwise ESPP_ESTATE.
  *   - The first call on a device looks up the array's device address with that device
- *     current; make that first call before any stream capture on that device.
+ *     current; make that first call before any stream capture on that device.  The
+ *     address is kept per device together with the id of the CUDA context it belongs
+ *     to; after a device reset (or a released and re-retained primary context) the next
+ *     call looks it up again, so that call too should come before any stream capture.
  *   - All calls share the one array, which keeps the last call's contents; calls that
  *     overlap on the GPU (two systems on different streams or threads) race. */
 ESPP_API int espp_energy_noalloc(espp_system* s, int32_t which, double* e);

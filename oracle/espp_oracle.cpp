@@ -1799,6 +1799,35 @@ int espp_vl_pairs(espp_system* s, int64_t cap, int64_t* pairs, int64_t* npairs) 
   return ESPP_OK;
 }
 
+// splitmix64 finaliser (Steele, Lea and Flood, "Fast splittable pseudorandom number
+// generators", OOPSLA 2014): the mixing function of the pair-set digest.
+static uint64_t digest_mix(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+int espp_vl_digest(espp_system* s, uint64_t out[4]) {
+  CHECK_S(s);
+  if (!out) return fail(ESPP_EINVAL, "null output pointer");
+  ensureAos(s);
+  uint64_t cnt = 0, sum = 0, x = 0, sum2 = 0;
+  for (auto& pr : s->vlPairs) {
+    const int64_t a = pr.first->id, b = pr.second->id;
+    const uint64_t h = digest_mix(digest_mix((uint64_t)std::min(a, b)) ^ (uint64_t)std::max(a, b));
+    cnt += 1;
+    sum += h;
+    x ^= h;
+    sum2 += digest_mix(h);
+  }
+  out[0] = cnt;
+  out[1] = sum;
+  out[2] = x;
+  out[3] = sum2;
+  return ESPP_OK;
+}
+
 int espp_vl_builds(espp_system* s, int64_t* builds) {
   CHECK_S(s);
   *builds = s->builds;
@@ -2581,6 +2610,22 @@ int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n) {
   int64_t cnt = 0;
   for (int ci : s->realCells)
     for (auto& p : s->cells[ci].p) {
+      v2 += p.mass * (p.v[0] * p.v[0] + p.v[1] * p.v[1] + p.v[2] * p.v[2]);
+      cnt++;
+    }
+  *sum_mv2 = v2;
+  *n = cnt;
+  return ESPP_OK;
+}
+
+int espp_kinetic_types(espp_system* s, uint64_t type_mask, double* sum_mv2, int64_t* n) {
+  CHECK_S(s);
+  if (!sum_mv2 || !n) return fail(ESPP_EINVAL, "null output pointer");
+  double v2 = 0.0;
+  int64_t cnt = 0;
+  for (int ci : s->realCells)
+    for (auto& p : s->cells[ci].p) {
+      if (p.type < 0 || p.type >= 64 || !((type_mask >> p.type) & 1u)) continue;
       v2 += p.mass * (p.v[0] * p.v[0] + p.v[1] * p.v[1] + p.v[2] * p.v[2]);
       cnt++;
     }

@@ -1,8 +1,9 @@
 """Regenerates the golden fixtures in this directory from the ESPResSo++ test suite.
 
-Run in a checkout that has the reference source tree (default /root/reference):
+Run with the path of an ESPResSo++ source tree, given as the argument or in the
+environment variable ESPRESSOPP_SRC:
 
-    python tests/golden/make_golden.py [REFERENCE_ROOT]
+    python tests/golden/make_golden.py REFERENCE_ROOT
 
 Outputs (all committed; nothing at test time reads the reference tree):
 
@@ -137,4 +138,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ESPRESSOPP_SRC")
+    if not root:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT (or set ESPRESSOPP_SRC)")
+    main(root)

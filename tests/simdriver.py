@@ -184,6 +184,11 @@ class Sim:
         call(self.lib, "espp_vl_pairs", self.h, n, i64ptr(out), ctypes.byref(got))
         return out[:got.value]
 
+    def digest(self):
+        out = (ctypes.c_uint64 * 4)()
+        call(self.lib, "espp_vl_digest", self.h, out)
+        return tuple(int(v) for v in out)
+
     def confs(self, key, ids):
         ids = np.ascontiguousarray(ids, np.int64)
         h = ctypes.c_void_p()
@@ -232,6 +237,26 @@ class Confs:
         out = np.zeros(self.size())
         call(self.lib, "espp_msd_chain_com", self.h, int(chainlength), dptr(out))
         return out
+
+
+def _mix64(z):
+    z = (z + np.uint64(0x9E3779B97F4A7C15))
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def pair_digest(pairs):
+    """espp_vl_digest of an (n, 2) array of id pairs, computed with numpy."""
+    p = np.asarray(pairs, np.int64).reshape(-1, 2)
+    lo = np.minimum(p[:, 0], p[:, 1]).astype(np.uint64)
+    hi = np.maximum(p[:, 0], p[:, 1]).astype(np.uint64)
+    with np.errstate(over="ignore"):
+        h = _mix64(_mix64(lo) ^ hi)
+        s1 = int(np.sum(h, dtype=np.uint64))
+        s2 = int(np.sum(_mix64(h), dtype=np.uint64))
+    x = int(np.bitwise_xor.reduce(h)) if len(h) else 0
+    return (len(p), s1, x, s2)
 
 
 def cosine_angle_table(K=1.5, theta0=3.1415926, n=4001):

@@ -154,6 +154,15 @@ def test_standard_systems_and_info(on_oracle, capsys):
     espressopp.tools.timers.show(integ.getTimers())
     out = capsys.readouterr().out
     assert out.strip()
+    vl = system.getInteraction(0).getVerletList()
+    espressopp.tools.analyse.final_info(system, integ, vl, 1.0, 3.5)
+    lines = capsys.readouterr().out.splitlines()
+    # the reference's report (tools/analyse.py:66-76) after the timers block
+    assert lines[-5] == "Total # of neighbors = %d" % vl.totalSize()
+    assert lines[-4] == "Ave neighs/atom = %.1f" % (vl.totalSize() / 500.0)
+    assert lines[-3] == "Neighbor list builds = %d" % vl.builds
+    assert lines[-2] == "Integration steps = 0"
+    assert lines[-1] == "CPUs = 1 CPU time per CPU = 2.50000"
 
 
 def test_pressure_tensor_running_average(on_oracle):
@@ -179,16 +188,42 @@ def test_pressure_tensor_running_average(on_oracle):
 
 def test_temperature_of_selected_types(on_oracle):
     """Temperature.add_type / remove_type (Temperature.hpp:104-141): only the selected
-    types count; with none selected every particle does."""
-    system, integ = _fluid(n=512)
+    types count; with none selected every particle does; no selected particle gives
+    sumT / (3 * 0) = nan; getEkin is half the last sum of m v^2."""
+    x, y, z, Lx, Ly, Lz = espressopp.tools.lattice.createCubic(
+        512, 0.8442, perfect=False, RNG=espressopp.esutil.RNG(7))
+    system = espressopp.System()
+    system.rng = espressopp.esutil.RNG(5)
+    system.bc = espressopp.bc.OrthorhombicBC(system.rng, (Lx, Ly, Lz))
+    system.skin = 0.3
+    cgrid = espressopp.tools.decomp.cellGrid((Lx, Ly, Lz), (1, 1, 1), 2.5, 0.3)
+    system.storage = espressopp.storage.DomainDecomposition(system, (1, 1, 1), cgrid)
+    types = [1 if k % 5 == 0 else (70 if k % 7 == 0 else 0) for k in range(len(x))]
+    system.storage.addParticles([[k, espressopp.Real3D(x[k], y[k], z[k]), types[k]]
+                                 for k in range(len(x))], "id", "pos", "type")
+    system.storage.decompose()
+    integ = espressopp.integrator.VelocityVerlet(system)
+    integ.dt = 0.005
+    lang = espressopp.integrator.LangevinThermostat(system)
+    lang.gamma = 1.0
+    lang.temperature = 1.0
+    integ.addExtension(lang)
+    integ.run(30)
     st = system.storage
     T = espressopp.analysis.Temperature(system)
-    integ.run(30)
     ids, _, vel, _, _ = st.getAll()
-    all_T = float(np.sum(vel * vel)) / (3 * len(ids))
+    typ = np.array([types[int(p)] for p in ids])
+    v2 = np.sum(vel * vel, axis=1)
+    all_T = float(np.sum(v2)) / (3 * len(ids))
     assert T.compute() == pytest.approx(all_T, rel=1e-12)
-    st._types[7] = 1  # the bookkeeping of a particle added with type 1
+    assert T.getEkin() == pytest.approx(0.5 * float(np.sum(v2)), rel=1e-12)
     T.add_type(1)
-    assert T.compute() == pytest.approx(float(np.sum(vel[7] ** 2)) / 3.0, rel=1e-12)
-    assert T.remove_type(1) and not T.remove_type(1)
+    sel = typ == 1
+    assert T.compute() == pytest.approx(float(np.sum(v2[sel])) / (3 * sel.sum()), rel=1e-12)
+    T.add_type(70)  # a type id beyond the 64-bit mask of the device reduction
+    sel = (typ == 1) | (typ == 70)
+    assert T.compute() == pytest.approx(float(np.sum(v2[sel])) / (3 * sel.sum()), rel=1e-12)
+    assert T.remove_type(1) and T.remove_type(70) and not T.remove_type(1)
     assert T.compute() == pytest.approx(all_T, rel=1e-12)
+    T.add_type(3)  # no particle of type 3
+    assert np.isnan(T.compute())

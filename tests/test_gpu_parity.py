@@ -162,31 +162,6 @@ def test_large_cells_pairs_and_forces(prec):
     assert np.max(np.abs(rg[0] - ro[0])) < (1e-9 if prec == _abi.PREC_FP64 else 1e-5)
 
 
-@pytest.mark.parametrize("grid", [None, [3, 3, 3]])
-def test_tensor_core_build_form_pairs_bit_exact(grid, monkeypatch):
-    """The Verlet build with the tcgen05 distance prefilter (ESPP_B200_BUILD=tc) gives the
-    reference's pair set, at the decomposition and after 10 steps with re-sorts."""
-    monkeypatch.setenv("ESPP_B200_BUILD", "tc")
-    pid, pos, vel, box = load_lj2048()
-    sims = []
-    for lib, p in ((oracle_lib(), _abi.PREC_FP64), (cuda_lib(), _abi.PREC_MIXED)):
-        if grid is None:
-            s = _lj_setup(lib, p, pid, pos, vel, box)
-        else:
-            s = Sim(lib, box, 0.3, grid, precision=p)
-            s.add(pid, pos, vel)
-            s.decompose()
-            s.vl(2.5)
-            s.lj(0, 0, 1.0, 1.0, 2.5, 4.0 * (2.5 ** -12 - 2.5 ** -6))
-        sims.append(s)
-    assert np.array_equal(sims[0].pairs(), sims[1].pairs())
-    for s in sims:
-        s.integrator(0.005)
-        s.run(10)
-    assert np.array_equal(sims[0].pairs(), sims[1].pairs())
-    assert sims[0].vl_size() == sims[1].vl_size()
-
-
 @pytest.mark.parametrize("prec", [_abi.PREC_FP64, _abi.PREC_MIXED])
 def test_polymer_melt_langevin_run_matches_oracle(prec):
     """40 000-bead ring melt: WCA (rc 1.12, shift 0) + FENE + Langevin, 15 steps."""

@@ -19,7 +19,8 @@ import pytest
 
 from espressopp_b200 import _abi
 from simdriver import (Sim, cell_grid, cosine_angle_table, lattice, load_lj2048, load_polymer40k,
-                       mb_velocities, msd_chain_reference, msd_reference, oracle_lib)
+                       mb_velocities, msd_chain_reference, msd_reference, oracle_lib,
+                       pair_digest)
 
 
 def _lj(eps, sig, rc, shift, d, caprad=0.0):
@@ -127,6 +128,25 @@ def test_verlet_list_complete_vs_brute_force():
     s2.vl(2.5)
     folded = p2 - np.floor(p2 / b2) * b2
     assert s2.vl_size() == _brute_pairs(folded, b2, 2.8)
+
+
+def test_pair_digest_matches_the_exported_pairs():
+    """espp_vl_digest is the order-independent digest of the exported id pairs, it tells
+    apart lists that differ by one pair, and it does not depend on the list order."""
+    pid, pos, vel, box = load_lj2048()
+    s = Sim(oracle_lib(), box, 0.3, cell_grid(box, 2.5, 0.3))
+    s.add(pid, pos, vel)
+    s.decompose()
+    s.vl(2.5)
+    pairs = s.pairs()
+    d = s.digest()
+    assert d == pair_digest(pairs)
+    assert d == pair_digest(pairs[::-1][:, ::-1])
+    assert d[0] == s.vl_size() == len(pairs)
+    assert pair_digest(pairs[1:]) != d
+    swapped = pairs.copy()
+    swapped[0, 1] += 1
+    assert pair_digest(swapped)[1:] != d[1:]
 
 
 def test_nve_energy_conserved():
