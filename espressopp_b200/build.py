@@ -16,7 +16,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libespp_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["espp_kernels.cu", "espp_tables.cu", "espp_mlp.cu", "espp_analysis.cu", "espp_api.cu"]
+SOURCES = ["espp_kernels.cu", "espp_brick.cu", "espp_tables.cu", "espp_mlp.cu", "espp_analysis.cu",
+           "espp_api.cu"]
 FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",
     "-gencode", "arch=compute_100a,code=sm_100a",

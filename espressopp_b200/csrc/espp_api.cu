@@ -147,6 +147,19 @@ struct espp_system {
   ParticleArrays snap{};
   int snapCap = 0;
 
+  // brick path of the Verlet list and pair kernels (BrickView)
+  bool brickAllowed = false;  // ESPP_B200_BRICK=1 selects the brick form
+  bool brickOn = false;       // the current list is in the brick form
+  int brickG = 2;             // particles per group
+  int brickB[3] = {0, 0, 0};  // brick extent in cells (0: chosen from the density)
+  int brickWmax = 0;          // window capacity
+  uint16_t* bnl = nullptr;
+  int32_t* bnnG = nullptr;
+  int32_t* cellGroupStart = nullptr;
+  int bgcap = 0, bKb = 0;
+  double* bpartials = nullptr;  // one row of 7 per brick (observables, digest)
+  int bpartialsCap = 0;
+
   // Verlet list
   bool has_vl = false;
   double vl_cut = 0.0;
@@ -213,6 +226,25 @@ struct espp_system {
   std::vector<int64_t> allIds;
   int maxType = 0;
 
+  BrickView brick_view() const {
+    BrickView b{};
+    b.on = brickOn ? 1 : 0;
+    b.G = brickG;
+    b.nbricks = 1;
+    for (int k = 0; k < 3; ++k) {
+      b.b[k] = brickB[k] > 0 ? brickB[k] : 1;
+      b.nb[k] = (nc[k] + b.b[k] - 1) / b.b[k];
+      b.nbricks *= b.nb[k];
+    }
+    b.wmax = brickWmax;
+    b.nl = bnl;
+    b.nnG = bnnG;
+    b.cellGroupStart = cellGroupStart;
+    b.gcap = bgcap;
+    b.Kb = bKb;
+    return b;
+  }
+
   DevView view() const {
     DevView d{};
     d.pa = d_pa;
@@ -272,6 +304,7 @@ struct espp_system {
     d.tripEntry = tripEntry;
     d.tripF = tripF;
     d.cosine = cosine;
+    d.brick = brick_view();
     d.err = err;
     d.ctr = ctr;
     return d;
@@ -477,6 +510,10 @@ void rebuild_id_tables(espp_system* s) {
       ex.push_back(e);
   if (!ex.empty()) csr(ex, s->exclStart, s->exclIds);
   // triples: ids and, per particle, the triples it belongs to with its role
+  dfree(s->bnl);
+  dfree(s->bnnG);
+  dfree(s->cellGroupStart);
+  dfree(s->bpartials);
   dfree(s->d_triples);
   dfree(s->tripStart);
   dfree(s->tripEntry);
@@ -569,11 +606,88 @@ int estimate_K(espp_system* s) {
   return (K + 7) / 8 * 8;
 }
 
-void build_list(espp_system* s) {
-  if (!s->has_vl) return;
-  if (!s->binned) bin(s, false);
-  double cutVerlet = s->vl_cut + s->skin;
-  double cutsq = cutVerlet * cutVerlet;
+DevCounters get_counters(espp_system* s);
+
+// Whether the list and pair kernels take the brick form: LJ (plain or capped, FENE
+// bonds, exclusions) on a grid of at least 2 cells per dimension.  Tabulated pair
+// potentials and the learned potential read the per-particle form.
+bool pair_any(const espp_system* s);
+bool brick_wanted(const espp_system* s) {
+  if (!s->brickAllowed || !s->has_vl || !s->lj_any || s->tabNT > 0 || s->mlp) return false;
+  for (int k = 0; k < 3; ++k)
+    if (s->nc[k] < 2) return false;
+  return true;
+}
+
+// Brick extent: about 160 particles per brick, at most kBrickMax cells per edge.
+void choose_brick(espp_system* s) {
+  const double ncells = (double)s->nc[0] * s->nc[1] * s->nc[2];
+  const double occ = std::max(s->n / ncells, 0.05);
+  int b = (int)std::lround(std::cbrt(160.0 / occ));
+  b = std::max(1, std::min(kBrickMax, b));
+  for (int k = 0; k < 3; ++k) s->brickB[k] = std::min(b, s->nc[k]);
+}
+
+int brick_window_limit(const espp_system* s) {
+  const int bits = 16 - s->brickG;
+  const int byBits = 1 << bits;
+  const int bySmem = (int)(brick_smem_limit() / (sizeof(double) * 4 + sizeof(int)));
+  return std::min(byBits, bySmem) / 32 * 32;
+}
+
+// Buffers of the brick form sized for the current particles and grid.
+void ensure_brick_buffers(espp_system* s) {
+  if (s->brickB[0] == 0) choose_brick(s);
+  const long long ncells = (long long)s->nc[0] * s->nc[1] * s->nc[2];
+  if (!s->cellGroupStart) s->cellGroupStart = dalloc<int32_t>(ncells + 1);
+  // groups never straddle cells: sum over cells of ceil(n_c / G) <= (n + ncells (G-1)) / G
+  const long long gcap = (s->n + ncells * (s->brickG - 1)) / s->brickG + 1;
+  if (gcap > (1LL << 31) - 1) raise(ESPP_ERANGE, "too many particle groups");
+  if (s->bKb == 0) {
+    const int K1 = estimate_K(s);  // per-particle capacity with margin
+    // a group's list is the union of its members' lists: about 1.4 (G = 2) or 1.9
+    // (G = 4) times one member's
+    s->bKb = ((int)std::ceil(K1 * (s->brickG == 2 ? 1.45 : 1.95)) + 7) / 8 * 8;
+    dfree(s->bnl);
+  }
+  if (gcap > s->bgcap || !s->bnl) {
+    dfree(s->bnl);
+    dfree(s->bnnG);
+    s->bgcap = (int)gcap;
+    s->bnl = dalloc<uint16_t>((size_t)s->bKb * s->bgcap);
+    s->bnnG = dalloc<int32_t>(s->bgcap);
+  }
+  if (s->brickWmax == 0) {
+    double V = 1.0;
+    for (int k = 0; k < 3; ++k) V *= (s->brickB[k] + 2) * (s->L[k] / s->nc[k]);
+    const double rho = s->n / (s->L[0] * s->L[1] * s->L[2]);
+    int w = (int)std::ceil(1.35 * rho * V) + 96;
+    w = std::max(256, (w + 31) / 32 * 32);
+    s->brickWmax = std::min(w, brick_window_limit(s));
+  }
+  BrickView bv = s->brick_view();
+  if (bv.nbricks * 7 > s->bpartialsCap) {
+    dfree(s->bpartials);
+    s->bpartialsCap = bv.nbricks * 7;
+    s->bpartials = dalloc<double>(s->bpartialsCap);
+  }
+}
+
+void grow_brick_lists(espp_system* s, int need) {
+  s->bKb = (std::max(s->bKb * 2, need + 32) + 7) / 8 * 8;
+  dfree(s->bnl);
+  s->bnl = dalloc<uint16_t>((size_t)s->bKb * s->bgcap);
+}
+
+// Doubles the window capacity; false when it is at its limit.
+bool grow_brick_window(espp_system* s) {
+  const int lim = brick_window_limit(s);
+  if (s->brickWmax >= lim) return false;
+  s->brickWmax = std::min(lim, s->brickWmax * 2);
+  return true;
+}
+
+void build_list_plain(espp_system* s, double cutsq) {
   if (s->K == 0 || !s->nl) {
     s->K = estimate_K(s);
     dfree(s->nl);
@@ -592,6 +706,40 @@ void build_list(espp_system* s) {
     dfree(s->nl);
     s->nl = dalloc<int32_t>((size_t)s->K * s->cap);
   }
+}
+
+// Brick form; false when a window cannot be staged (the caller falls back to the
+// per-particle form).
+bool build_list_brick(espp_system* s, double cutsq) {
+  ensure_brick_buffers(s);
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    DevView d = s->view();
+    launch_brick_layout(d, s->scr, s->st);
+    launch_build_brick(d, cutsq, s->st);
+    cuda_check(cudaGetLastError(), "brick Verlet list kernels");
+    unsigned e = read_err(s);
+    if (!(e & (kErrNlOverflow | kErrWindow))) return true;
+    cuda_check(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->st), "memset");
+    if (e & kErrWindow) {
+      if (!grow_brick_window(s)) return false;
+      ensure_brick_buffers(s);
+    }
+    if (e & kErrNlOverflow) grow_brick_lists(s, get_counters(s).nnMax);
+  }
+  return false;
+}
+
+void build_list(espp_system* s) {
+  if (!s->has_vl) return;
+  if (!s->binned) bin(s, false);
+  double cutVerlet = s->vl_cut + s->skin;
+  double cutsq = cutVerlet * cutVerlet;
+  s->brickOn = brick_wanted(s) && s->n > 0;
+  if (s->brickOn && !build_list_brick(s, cutsq)) {
+    s->brickOn = false;
+    s->brickAllowed = false;  // a window too dense for the stage: per-particle form from now on
+  }
+  if (!s->brickOn) build_list_plain(s, cutsq);
   check_err(s);
   s->builds++;
   s->listValid = true;
@@ -713,8 +861,12 @@ void launch_all_forces(espp_system* s, cudaStream_t st) {
   DevView d = s->view();
   const bool mixed = s->precision == ESPP_PREC_MIXED;
   DevView dm = d;
-  if (!s->has_vl || !s->lj_any) dm.nn = s->nnZero;  // no LJ term: bonds only
-  launch_forces(dm, mixed, s->fene, s->tpp, st);
+  if (s->brickOn) {
+    launch_forces_brick(d, mixed, s->fene, st);
+  } else {
+    if (!s->has_vl || !s->lj_any) dm.nn = s->nnZero;  // no LJ term: bonds only
+    launch_forces(dm, mixed, s->fene, s->tpp, st);
+  }
   if (!s->has_vl) d.tabNT = 0;
   launch_force_tab(d, mixed, st);
   if (d.mlp.on) launch_mlp_forces(d, mixed, nullptr, st);
@@ -850,7 +1002,12 @@ void launch_rebuild_kernels(espp_system* s, cudaStream_t st) {
   launch_id_map(d, st);
   if (s->has_vl) {
     const double cv = s->vl_cut + s->skin;
-    launch_build_nl(d, cv * cv, st);
+    if (s->brickOn) {
+      launch_brick_layout(d, s->scr, st);
+      launch_build_brick(d, cv * cv, st);
+    } else {
+      launch_build_nl(d, cv * cv, st);
+    }
   }
 }
 
@@ -944,6 +1101,16 @@ int K_high_water(espp_system* s) { return get_counters(s).nnMax; }
 
 // Grows the Verlet capacity ahead of need when the builds came within 10 % of it.
 void maybe_grow_K(espp_system* s) {
+  if (s->has_vl && s->brickOn) {
+    const int hw = K_high_water(s);
+    if (hw * 10 > s->bKb * 9) {
+      s->bKb = (hw * 3 / 2 + 15) / 8 * 8;
+      dfree(s->bnl);
+      s->bnl = dalloc<uint16_t>((size_t)s->bKb * s->bgcap);
+      s->listValid = false;
+    }
+    return;
+  }
   if (!s->has_vl || s->K == 0) return;
   int hw = K_high_water(s);
   if (hw * 10 > s->K * 9) {
@@ -1108,6 +1275,7 @@ RunSnapshot take_snapshot(espp_system* s) {
 // until the next re-sort.
 void recover_overflow(espp_system* s, const RunSnapshot& r) {
   const int hw = K_high_water(s);  // the graph's largest count, before the restore
+  const unsigned why = read_err(s);
   cuda_check(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->st), "memset");
   s->paHostValid = false;
   sync_pa(s);
@@ -1116,9 +1284,20 @@ void recover_overflow(espp_system* s, const RunSnapshot& r) {
   s->step = r.step;
   s->resortFlag = r.resortFlag;
   s->binned = false;
-  s->K = (std::max(s->K * 2, hw + 32) + 7) / 8 * 8;  // multiple of 8
-  dfree(s->nl);
-  s->nl = dalloc<int32_t>((size_t)s->K * s->cap);
+  if (s->brickOn) {
+    if (why & kErrWindow) {
+      if (!grow_brick_window(s)) {
+        s->brickOn = false;
+        s->brickAllowed = false;
+      }
+    } else {
+      grow_brick_lists(s, hw);
+    }
+  } else {
+    s->K = (std::max(s->K * 2, hw + 32) + 7) / 8 * 8;  // multiple of 8
+    dfree(s->nl);
+    s->nl = dalloc<int32_t>((size_t)s->K * s->cap);
+  }
   s->listValid = false;
   destroy_graph(s);
   if (!s->resortFlag) {
@@ -1149,7 +1328,7 @@ void run(espp_system* s, int64_t nsteps) {
   cuda_check(cudaGraphLaunch(s->graphExec, s->st), "cudaGraphLaunch");
   cuda_check(cudaEventRecord(s->runEnd, s->st), "event");
   sync(s);
-  if (read_err(s) & kErrNlOverflow) {
+  if (read_err(s) & (kErrNlOverflow | kErrWindow)) {
     // back to the state before the run, a larger list, and the run again on the host loop
     recover_overflow(s, snap);
     run_host(s, nsteps);
@@ -1266,7 +1445,10 @@ void observable(espp_system* s, int which, int energy, double out[7]) {
   DevView d = s->view();
   if (which == ESPP_IA_LJ) {
     if (!s->has_vl || !s->lj_any) return;
-    launch_lj_observables(d, part, nb, s->obs, energy, s->st);
+    if (s->brickOn)
+      launch_lj_observables_brick(d, s->bpartials, 0, s->obs, energy, s->st);
+    else
+      launch_lj_observables(d, part, nb, s->obs, energy, s->st);
   } else if (which == ESPP_IA_FENE) {
     if (!s->fene.on) return;
     launch_fene_observables(d, s->fene, part, nb, s->obs, energy, s->st);
@@ -1496,6 +1678,11 @@ int espp_system_create(const double box[3], double skin, const int32_t cell_grid
     cuda_check(cudaMemset(s->d_pa, 0, 2 * sizeof(ParticleArrays)), "memset");
     cuda_check(cudaMallocHost(&s->hctr, sizeof(DevCounters)), "pinned counters");
     if (const char* g = std::getenv("ESPP_B200_GRAPH")) s->useGraph = std::atoi(g) != 0;
+    if (const char* b = std::getenv("ESPP_B200_BRICK")) s->brickAllowed = std::atoi(b) != 0;
+    if (const char* g = std::getenv("ESPP_B200_GROUP")) {
+      const int v = std::atoi(g);
+      if (v == 2 || v == 4) s->brickG = v;
+    }
     if (const char* t = std::getenv("ESPP_B200_TPP")) {
       const int v = std::atoi(t);
       if (v == 1 || v == 2 || v == 4 || v == 8) s->tpp = v;
@@ -1744,7 +1931,10 @@ int espp_vl_size(espp_system* s, int64_t* npairs) {
     if (!s->has_vl || s->n == 0) return;
     DevView d = s->view();
     int32_t* counts = dalloc<int32_t>(s->n);
-    launch_pair_count(d, counts, s->st);
+    if (s->brickOn)
+      launch_pair_count_brick(d, counts, s->st);
+    else
+      launch_pair_count(d, counts, s->st);
     std::vector<int32_t> h(s->n);
     cudaError_t e = cudaMemcpyAsync(h.data(), counts, sizeof(int32_t) * s->n,
                                     cudaMemcpyDeviceToHost, s->st);
@@ -1767,7 +1957,11 @@ int espp_vl_digest(espp_system* s, uint64_t out[4]) {
     // the observable partials hold 7 doubles per block; the digest needs 4 words
     unsigned long long* part = reinterpret_cast<unsigned long long*>(obs_partials(s, nb));
     unsigned long long* res = reinterpret_cast<unsigned long long*>(s->obs);
-    launch_pair_digest(s->view(), part, nb, res, s->st);
+    if (s->brickOn)
+      launch_pair_digest_brick(s->view(), reinterpret_cast<unsigned long long*>(s->bpartials),
+                               res, s->st);
+    else
+      launch_pair_digest(s->view(), part, nb, res, s->st);
     cuda_check(cudaGetLastError(), "digest kernels");
     cuda_check(cudaMemcpyAsync(out, res, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost, s->st),
                "download");
@@ -1782,12 +1976,14 @@ int espp_vl_pairs(espp_system* s, int64_t capn, int64_t* pairs, int64_t* npairs)
     if (!s->has_vl || s->n == 0) return;
     DevView d = s->view();
     int32_t* counts = dalloc<int32_t>(s->n);
-    launch_pair_count(d, counts, s->st);
+    if (s->brickOn)
+      launch_pair_count_brick(d, counts, s->st);
+    else
+      launch_pair_count(d, counts, s->st);
     std::vector<int32_t> h(s->n);
     cuda_check(cudaMemcpyAsync(h.data(), counts, sizeof(int32_t) * s->n,
                                cudaMemcpyDeviceToHost, s->st), "download");
     sync(s);
-    dfree(counts);
     std::vector<int64_t> off(s->n);
     int64_t t = 0;
     for (int i = 0; i < s->n; ++i) {
@@ -1798,10 +1994,14 @@ int espp_vl_pairs(espp_system* s, int64_t capn, int64_t* pairs, int64_t* npairs)
     int64_t* dout = dalloc<int64_t>(2 * std::max<int64_t>(t, 1));
     std::vector<int64_t> out(2 * std::max<int64_t>(t, 1));
     cudaMemcpy(doff, off.data(), sizeof(int64_t) * s->n, cudaMemcpyHostToDevice);
-    launch_pair_write(d, doff, dout, s->st);
+    if (s->brickOn)
+      launch_pair_write_brick(d, doff, counts, dout, s->st);
+    else
+      launch_pair_write(d, doff, dout, s->st);
     cudaError_t e = cudaMemcpyAsync(out.data(), dout, sizeof(int64_t) * 2 * t,
                                     cudaMemcpyDeviceToHost, s->st);
     cudaStreamSynchronize(s->st);
+    dfree(counts);
     dfree(doff);
     dfree(dout);
     cuda_check(e, "download");
@@ -2040,7 +2240,19 @@ int espp_langevin_set(espp_system* s, int32_t enabled, double gamma, double T, i
     s->gamma = gamma;
     s->temperature = T;
     s->langExclIds.assign(excl, excl + nexcl);
-    s->idDirty = true;
+    if (s->idDirty || !s->langExcl) {
+      s->idDirty = true;
+      return;
+    }
+    // the id map is current: only the thermostat's exclusion flags change, so the
+    // particles keep their order and the Verlet list stays valid (setting up a thermostat
+    // triggers no re-sort or list build in the reference either)
+    std::vector<uint8_t> le(s->idSpan, 0);
+    for (int64_t id : s->langExclIds)
+      if (id >= s->idMin && id - s->idMin < s->idSpan) le[id - s->idMin] = 1;
+    cuda_check(cudaMemcpyAsync(s->langExcl, le.data(), le.size(), cudaMemcpyHostToDevice, s->st),
+               "upload");
+    sync(s);
   });
 }
 
@@ -2728,9 +2940,13 @@ int espp_energy_noalloc(espp_system* s, int32_t which, double* e) {
     double* partials = scratch + 8;
     double* out = scratch;
     DevView d = s->view();
-    if (which == ESPP_IA_LJ)
+    if (which == ESPP_IA_LJ && s->brickOn) {
+      if (d.brick.nbricks > kNoAllocMaxBlocks)
+        raise(ESPP_ERANGE, "espp_energy_noalloc handles at most 32768 bricks; use espp_energy");
+      launch_lj_observables_brick(d, partials, 0, out, 1, s->st);
+    } else if (which == ESPP_IA_LJ) {
       launch_lj_observables(d, partials, nb, out, 1, s->st);
-    else
+    } else
       launch_fene_observables(d, s->fene, partials, nb, out, 1, s->st);
     cuda_check(cudaGetLastError(), "energy kernels");
     cuda_check(cudaMemcpyAsync(e, out, sizeof(double), cudaMemcpyDeviceToHost, s->st),

@@ -28,6 +28,7 @@ enum : unsigned {
   kErrBondMissing = 1u << 3,   // bond partner id not present
   kErrIdRange = 1u << 4,       // particle id outside the dense id map
   kErrTimeout = 1u << 5,       // a bounded wait inside a kernel ran out
+  kErrWindow = 1u << 6,        // a brick window holds more particles than its stage
 };
 
 // Lennard-Jones parameters of one type pair (LennardJones.hpp:79-87 preset()).
@@ -121,6 +122,29 @@ struct TabDesc {
   double rcsq, shift;
 };
 
+// Brick path of the Verlet build and the pair kernels: the cell grid tiled into bricks
+// of b[0] x b[1] x b[2] cells.  A brick's window (its cells and one layer of cells
+// around them) holds every candidate of every particle of the brick; a kernel block
+// stages it in shared memory once.  Particles of a cell are taken G at a time
+// ("groups", consecutive in the in-cell order); each group keeps one list, the union of
+// its members' Verlet lists, as 16-bit entries: the candidate's window index in the low
+// (16 - G) bits and one bit per member above them.  Lists are stored in blocks of 8
+// entries (16 bytes): block k of group g at entries [(k * gcap + g) * 8, +8).
+constexpr int kBrickMax = 4;  // cells per brick edge
+struct BrickView {
+  int on;                  // the brick path is in use
+  int G;                   // particles per group (2 or 4)
+  int b[3];                // brick extent in cells
+  int nb[3];               // bricks per dimension
+  int nbricks;
+  int wmax;                // window capacity (entries) of the shared-memory stage
+  uint16_t* nl;            // Kb * gcap entries
+  int32_t* nnG;            // entries per group
+  int32_t* cellGroupStart; // ncells + 1: first group of each cell
+  int gcap;                // group capacity
+  int Kb;                  // entries per group (multiple of 8)
+};
+
 struct DevView {
   ParticleArrays* pa;     // device: pa[0] current arrays, pa[1] target of the re-sort
   int n;                  // particles
@@ -167,6 +191,7 @@ struct DevView {
   const int32_t* tripEntry; // triple index * 4 + role (0 p1, 1 centre, 2 p3)
   double* tripF;          // 6 * ntriples: force12, force32 of each triple
   CosineParams cosine;
+  BrickView brick;        // brick path (brick.on)
   unsigned* err;          // device error word
   DevCounters* ctr;       // step-loop state
 };
@@ -244,6 +269,21 @@ void launch_pair_write(const DevView& d, const int64_t* offsets, int64_t* out,
 // order-independent digest of the Verlet pair set: out[0..4) = count, sum, xor, sum2
 void launch_pair_digest(const DevView& d, unsigned long long* partials, int nblocks,
                         unsigned long long* out, cudaStream_t st);
+// brick path (espp_brick.cu; the group layout in espp_kernels.cu)
+void launch_brick_layout(const DevView& d, RebuildScratch& s, cudaStream_t st);
+void launch_build_brick(const DevView& d, double cutsq, cudaStream_t st);
+void launch_forces_brick(const DevView& d, bool mixed, const FENEParams& fene, cudaStream_t st);
+void launch_lj_observables_brick(const DevView& d, double* partials, int nblocks, double* out,
+                                 int energy, cudaStream_t st);
+void launch_pair_count_brick(const DevView& d, int32_t* counts, cudaStream_t st);
+void launch_pair_write_brick(const DevView& d, const int64_t* offsets, int32_t* fill,
+                             int64_t* out, cudaStream_t st);
+void launch_pair_digest_brick(const DevView& d, unsigned long long* partials,
+                              unsigned long long* out, cudaStream_t st);
+// shared memory (bytes) a brick window of wmax entries needs: FP32 and FP64 stages
+size_t brick_smem_f32(int wmax);
+size_t brick_smem_f64(int wmax);
+size_t brick_smem_limit();
 void launch_bond_maxsq(const DevView& d, double* partials, int nblocks, double* out,
                        cudaStream_t st);
 
