@@ -615,7 +615,7 @@ def small_configs(lib, replica_steps=1000):
     out["unit"] = "particle-steps/s (device-timed step loop)"
     if replica_steps > 0:
         log("configs: 64 PT replicas, %d steps" % replica_steps)
-        rep, total, seg, segments = run_replicas(lib, _abi.PREC_MIXED, replica_steps, 20)
+        rep, total, seg, segments, _ = run_replicas(lib, _abi.PREC_MIXED, replica_steps, 20)
         out["pt_replicas_64"] = {
             "workload": "64 LJ replicas, N ~ U{2000..64000} (seed 4), %d particles, mixed, "
                         "Langevin T 0.7..2.0, exchange every %d steps, %d steps (config: "
@@ -852,18 +852,26 @@ def mlp_arm(args, rank, world, local_rank):
 
 
 # ---- batched parallel-tempering replicas ------------------------------------------
-def run_replicas(lib, prec, steps, warmup, R=64):
+def run_replicas(lib, prec, steps, warmup, R=64, dist=None):
     """R LJ replicas, N ~ U{2000..64000} (seed 4), rho 0.8442, rc 2.5, skin 0.3,
     T_r = 0.7 (2.0/0.7)^(r/(R-1)), Langevin gamma 1, dt 0.005, Metropolis exchange between
     neighbours every 100 steps (ParallelTempering.exchange rule).  Times `steps` steps of
     all replicas with one graph launch per 100-step segment (espp_batch_run) against the
     same steps run replica by replica (espp_run each), wall clock around the calls and
-    exchanges.  Returns ({mode: result}, total particles, steps per segment)."""
+    exchanges.  Under torchrun the replicas are shared out among the ranks by particle
+    count; the exchange gathers (E_pot, T, N) of every replica with one all-reduce and
+    every rank applies the same decisions; the time is the max over ranks.
+    Returns ({mode: result}, total particles, steps per segment, segments, this rank's
+    replica count)."""
     from espressopp_b200._abi import call, dptr, i32ptr, i64ptr
-    from espressopp_b200.parallel_tempering import exchange_decisions
+    from espressopp_b200.parallel_tempering import (exchange_decisions, gather_replica_rows,
+                                                    partition_replicas)
     rng = np.random.Generator(np.random.PCG64(4))
     sizes = rng.integers(2000, 64001, size=R)
     temps = [0.7 * (2.0 / 0.7) ** (r / (R - 1)) for r in range(R)]
+    rank, world = (dist.get_rank(), dist.get_world_size()) if dist is not None else (0, 1)
+    group = dist.group.WORLD if dist is not None else None
+    local = [r for r, o in enumerate(partition_replicas(sizes, world)) if o == rank]
 
     def make(r):
         N = int(sizes[r])
@@ -892,25 +900,32 @@ def run_replicas(lib, prec, steps, warmup, R=64):
     T = list(temps)
 
     def set_T(hs):
-        for r, h in enumerate(hs):
+        for r, h in zip(local, hs):
             call(lib, "espp_langevin_set", h, 1, 1.0, T[r], 0, None)
 
     def exchange(hs, oddeven, urng):
-        e = []
-        kin = []
-        for h in hs:
+        rows = {}
+        for r, h in zip(local, hs):
             v = ctypes.c_double()
             call(lib, "espp_energy", h, 0, ctypes.byref(v))
-            e.append(v.value)
             k2 = ctypes.c_double()
             nn = ctypes.c_int64()
             call(lib, "espp_kinetic", h, ctypes.byref(k2), ctypes.byref(nn))
-            kin.append(k2.value / (3.0 * nn.value))
-        dec = exchange_decisions(e, kin, [int(x) for x in sizes], oddeven, urng.random)
+            rows[r] = (v.value, k2.value / (3.0 * nn.value), float(nn.value))
+        allrows = gather_replica_rows(rows, R, group)
+        dec = exchange_decisions(list(allrows[:, 0]), list(allrows[:, 1]),
+                                 [int(x) for x in allrows[:, 2]], oddeven, urng.random)
         for m, n, _, _, ok in dec:
             if ok:
                 T[m], T[n] = T[n], T[m]
         return sum(ok for *_, ok in dec)
+
+    def barrier():
+        if dist is not None:
+            import torch
+            t = torch.zeros(1, device="cuda")
+            dist.all_reduce(t)
+            torch.cuda.synchronize()
 
     import random
     total = int(sizes.sum())
@@ -919,13 +934,13 @@ def run_replicas(lib, prec, steps, warmup, R=64):
     out = {}
     for mode in ("sequential", "batched"):
         T[:] = temps
-        hs = [make(r) for r in range(R)]
+        hs = [make(r) for r in local]
         set_T(hs)
         b = None
-        if mode == "batched":
-            arr = (ctypes.c_void_p * R)(*[h.value for h in hs])
+        if mode == "batched" and hs:
+            arr = (ctypes.c_void_p * len(hs))(*[h.value for h in hs])
             b = ctypes.c_void_p()
-            call(lib, "espp_batch_create", arr, R, ctypes.byref(b))
+            call(lib, "espp_batch_create", arr, len(hs), ctypes.byref(b))
         urng = random.Random(335977)
 
         def step_all(n):
@@ -937,40 +952,60 @@ def run_replicas(lib, prec, steps, warmup, R=64):
 
         step_all(warmup)
         swaps = 0
+        barrier()
         t0 = time.perf_counter()
         for k in range(segments):
             step_all(seg)
             swaps += exchange(hs, k % 2, urng)
             set_T(hs)
-        el = time.perf_counter() - t0
+        barrier()
+        el = max_over_ranks(dist, time.perf_counter() - t0)
         out[mode] = {"seconds": el, "value": total * seg * segments / el, "swaps": swaps}
         if b is not None:
             lib.espp_batch_destroy(b)
         for h in hs:
             lib.espp_system_destroy(h)
-    return out, total, seg, segments
+    return out, total, seg, segments, len(local)
 
 
 def replicas_arm(args, rank, world, local_rank):
-    """The parallel-tempering workload alone: run_replicas at --steps steps."""
+    """The parallel-tempering workload alone: run_replicas at --steps steps, the replicas
+    shared out among the ranks under torchrun (strong scaling: 64 replicas in total)."""
     import espressopp_b200
     from espressopp_b200 import _abi
     from espressopp_b200._abi import call
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist_mod
+        torch.cuda.set_device(local_rank)
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = dist_mod
     lib = espressopp_b200.load_library()
     call(lib, "espp_select_device", local_rank)
     prec = _abi.PREC_MIXED if args.precision == "mixed" else _abi.PREC_FP64
-    out, total, seg, segments = run_replicas(lib, prec, args.steps, args.warmup)
+    out, total, seg, segments, nlocal = run_replicas(lib, prec, args.steps, args.warmup,
+                                                      dist=dist)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
     if rank == 0:
         line = {"metric": "PT replica particle-steps/s, 64 LJ replicas on 1 B200",
                 "value": out["batched"]["value"], "unit": "particle-steps/s", "n_gpus": world,
                 "steps": seg * segments, "warmup": args.warmup, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec else "f64",
+                "scaling": "strong", "vs_baseline": None, "dtype": "f32" if prec else "f64",
                 "data": "synthetic",
                 "config": {"workload": "64 LJ replicas, N ~ U{2000..64000} (seed 4), total %d "
                                        "particles, rho 0.8442, rc 2.5, skin 0.3, Langevin gamma 1, "
                                        "T 0.7..2.0 geometric, dt 0.005, exchange every %d steps"
                                        % (total, seg),
-                           "timing": "wall clock around the run calls and exchanges"},
+                           "timing": "wall clock around the run calls and exchanges, max over "
+                                     "ranks",
+                           "parallelism": "replicas shared out over %d rank(s) by particle "
+                                          "count; exchange rows all-reduced" % world,
+                           "replicas_on_rank0": nlocal},
                 "batched": out["batched"], "sequential": out["sequential"],
                 "batched_over_sequential": out["batched"]["value"] / out["sequential"]["value"]}
         print(json.dumps(line), flush=True)

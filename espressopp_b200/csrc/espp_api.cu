@@ -1099,26 +1099,45 @@ void copy_arrays(espp_system* s, const ParticleArrays& dst, const ParticleArrays
 
 int K_high_water(espp_system* s) { return get_counters(s).nnMax; }
 
-// Grows the Verlet capacity ahead of need when the builds came within 10 % of it.
+// Grows the Verlet capacity ahead of need when the builds came within 10 % of it.  The
+// position of an entry in either list form does not depend on the capacity (block k of
+// row i sits at (k * rows + i) * 8), so the current lists are copied into the larger
+// buffer and stay valid: no rebuild, which the reference would not do either.
 void maybe_grow_K(espp_system* s) {
-  if (s->has_vl && s->brickOn) {
-    const int hw = K_high_water(s);
-    if (hw * 10 > s->bKb * 9) {
-      s->bKb = (hw * 3 / 2 + 15) / 8 * 8;
-      dfree(s->bnl);
-      s->bnl = dalloc<uint16_t>((size_t)s->bKb * s->bgcap);
-      s->listValid = false;
-    }
+  if (!s->has_vl) return;
+  const int hw = K_high_water(s);
+  if (s->brickOn) {
+    if (hw * 10 <= s->bKb * 9) return;
+    const int Kn = (hw * 3 / 2 + 15) / 8 * 8;
+    uint16_t* nl = dalloc<uint16_t>((size_t)Kn * s->bgcap);
+    cuda_check(cudaMemcpyAsync(nl, s->bnl, sizeof(uint16_t) * (size_t)s->bKb * s->bgcap,
+                               cudaMemcpyDeviceToDevice, s->st), "copy");
+    sync(s);
+    dfree(s->bnl);
+    s->bnl = nl;
+    s->bKb = Kn;
     return;
   }
-  if (!s->has_vl || s->K == 0) return;
-  int hw = K_high_water(s);
-  if (hw * 10 > s->K * 9) {
-    s->K = (hw * 3 / 2 + 15) / 8 * 8;
-    dfree(s->nl);
-    s->nl = dalloc<int32_t>((size_t)s->K * s->cap);
-    s->listValid = false;
-  }
+  if (s->K == 0 || hw * 10 <= s->K * 9) return;
+  const int Kn = (hw * 3 / 2 + 15) / 8 * 8;
+  int32_t* nl = dalloc<int32_t>((size_t)Kn * s->cap);
+  cuda_check(cudaMemcpyAsync(nl, s->nl, sizeof(int32_t) * (size_t)s->K * s->cap,
+                             cudaMemcpyDeviceToDevice, s->st), "copy");
+  sync(s);
+  dfree(s->nl);
+  s->nl = nl;
+  s->K = Kn;
+}
+
+// The list form follows the interactions (brick_wanted); a list built before the
+// potentials were set (espp_vl_create comes first) is rebuilt in the other form at the
+// same positions, without counting a build.
+void ensure_list_form(espp_system* s) {
+  if (!s->has_vl || !s->listValid || s->n == 0) return;
+  if (brick_wanted(s) == s->brickOn) return;
+  const int64_t builds = s->builds;
+  build_list(s);
+  s->builds = builds;
 }
 
 // Everything of VelocityVerlet::run before the step loop (src/integrator/
@@ -1145,6 +1164,7 @@ IntegrateArgs run_prologue(espp_system* s, int64_t nsteps, double& tResort) {
   }
   if (!s->binned) bin(s, false);
   if (s->has_vl && !s->listValid) build_list(s);
+  ensure_list_form(s);
   IntegrateArgs a = integrate_args(s);
   DevCounters c0 = get_counters(s);
   c0.maxSq = 0ull;
@@ -1434,6 +1454,7 @@ void prepare_observables(espp_system* s) {
   if (s->idDirty) rebuild_id_tables(s);
   if (!s->binned) bin(s, false);
   if (s->has_vl && !s->listValid) build_list(s);
+  ensure_list_form(s);
 }
 
 void observable(espp_system* s, int which, int energy, double out[7]) {

@@ -808,19 +808,25 @@ __global__ void k_digest_reduce_brick(const unsigned long long* partials, int nb
 
 // ---- launchers ----------------------------------------------------------------------------
 
+// Opt in to more than 48 KB of dynamic shared memory.  Not while the stream is being
+// captured: the same launch ran uncaptured before every capture (start-of-run forces,
+// host-side list build), which set the attribute for the same size.
 template <class Kern>
-void allow_smem(Kern k, size_t bytes) {
-  if (bytes > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+void allow_smem(Kern k, size_t bytes, cudaStream_t st) {
+  if (bytes <= 48 * 1024) return;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) return;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 template <int G>
 void build_brick_g(const DevView& d, double cutsq, cudaStream_t st) {
   const size_t sm = brick_smem_f32(d.brick.wmax);
   if (d.exclStart) {
-    allow_smem(k_build_brick<G, true>, sm);
+    allow_smem(k_build_brick<G, true>, sm, st);
     k_build_brick<G, true><<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, cutsq);
   } else {
-    allow_smem(k_build_brick<G, false>, sm);
+    allow_smem(k_build_brick<G, false>, sm, st);
     k_build_brick<G, false><<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, cutsq);
   }
 }
@@ -832,10 +838,10 @@ void forces_brick_g(const DevView& d, const FENEParams& fp, cudaStream_t st) {
 #define ESPP_BRICK_CASE(S, C, F)                                                         \
   if (single == S && capped == C && fene == F) {                                         \
     if (MIXED) {                                                                         \
-      allow_smem(k_force_brick_mixed<G, S, C, F>, sm);                                   \
+      allow_smem(k_force_brick_mixed<G, S, C, F>, sm, st);                                   \
       k_force_brick_mixed<G, S, C, F><<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, fp); \
     } else {                                                                             \
-      allow_smem(k_force_brick_fp64<G, S, C, F>, sm);                                    \
+      allow_smem(k_force_brick_fp64<G, S, C, F>, sm, st);                                    \
       k_force_brick_fp64<G, S, C, F><<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, fp);  \
     }                                                                                    \
     return;                                                                              \
@@ -885,10 +891,10 @@ void launch_lj_observables_brick(const DevView& d, double* partials, int nblocks
   (void)nblocks;
   const size_t sm = brick_smem_f64(d.brick.wmax);
   if (d.brick.G == 4) {
-    allow_smem(k_lj_obs_brick<4>, sm);
+    allow_smem(k_lj_obs_brick<4>, sm, st);
     k_lj_obs_brick<4><<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, energy, partials);
   } else {
-    allow_smem(k_lj_obs_brick<2>, sm);
+    allow_smem(k_lj_obs_brick<2>, sm, st);
     k_lj_obs_brick<2><<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, energy, partials);
   }
   k_sum_partials<7><<<1, 256, 0, st>>>(partials, d.brick.nbricks, out);
