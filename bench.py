@@ -63,9 +63,10 @@ STEP_FLOPS = 24.0 * N_HALF
 # force kernel: packed coordinates read 12 + 4 B per half-list pair + int64 F write 24
 FORCE_BYTES = 12.0 + 4.0 * N_HALF + 24.0
 # DRAM bytes (read + write) per particle of one force-kernel launch, measured by ncu on
-# the 1,000,000-particle case (profiles/force_mixed_lj_1M_ncu.txt: 345.0 MB + 6.7 MB);
-# traffic grows in proportion to the particle count at fixed density
-FORCE_TRAFFIC_PER_PARTICLE = 351.7
+# the 1,000,000-particle case (profiles/force_mixed_lj_1M_ncu.txt: 345.0 MB + 6.7 MB for
+# the global-list kernel); traffic grows in proportion to the particle count at fixed
+# density
+FORCE_TRAFFIC_PER_PARTICLE = {"k_force_mixed": 351.7}
 
 
 def log(*a):
@@ -280,21 +281,21 @@ def gpu_arm(args, rank, world, local_rank):
     # the workload's protocol: 1,000 Langevin steps (gamma 1, T 1) melt the lattice into
     # the equilibrated fluid; the timed segment is NVE from that state
     t_eq = time.perf_counter()
+    steps_per_build = 10.0
     if args.equil > 0:
         call(lib, "espp_langevin_set", h, 1, 1.0, 1.0, 0, None)
         call(lib, "espp_run", h, args.equil)
         call(lib, "espp_langevin_set", h, 0, 1.0, 1.0, 0, None)
+        rs = ctypes.c_int64()
+        call(lib, "espp_num_resorts", h, ctypes.byref(rs))
+        steps_per_build = args.equil / max(1, rs.value)
     log("rank %d: %d Langevin steps in %.1f s" % (rank, args.equil, time.perf_counter() - t_eq))
-    # warm-up (untimed), then pick threads per particle for the force kernel
+    # warm-up (untimed), then the list layout: per-particle global lists (1, 2, 4, 8
+    # threads per particle) or brick windows of several extents, each timed (one build,
+    # three force launches) and scored by force time + build time / steps per build
     call(lib, "espp_run", h, args.warmup)
-    tpp = ctypes.c_int32(args.tpp)
-    tune_ms = np.zeros(4)
-    if args.tpp:
-        call(lib, "espp_set_tpp", h, args.tpp)
-    else:
-        call(lib, "espp_autotune", h, ctypes.byref(tpp), dptr(tune_ms))
-    log("rank %d: autotune tpp=%d (1,2,4,8 -> %s ms)" % (rank, tpp.value,
-                                                        np.round(tune_ms, 4).tolist()))
+    layout, tune = autotune_layout(lib, h, args, steps_per_build)
+    log("rank %d: layout %s (steps per build %.1f)" % (rank, layout, steps_per_build))
 
     def total_energy(hh):
         e = ctypes.c_double()
@@ -370,8 +371,7 @@ def gpu_arm(args, rank, world, local_rank):
         rel_max = float(np.max(np.linalg.norm(df, axis=1)) /
                         np.sqrt(np.mean(np.sum(f64 * f64, axis=1))))
         call(lib, "espp_run", h64, args.warmup)
-        tpp64 = ctypes.c_int32()
-        call(lib, "espp_autotune", h64, ctypes.byref(tpp64), None)
+        layout64, tune64 = autotune_layout(lib, h64, args, steps_per_build)
         # throughput of the all-FP64 kernel: the same K NVE steps from the same state
         call(lib, "espp_set_particles", h64, N, i64ptr(pin_ids), dptr(pin_pos), dptr(pin_vel))
         call(lib, "espp_run", h64, 0)
@@ -399,7 +399,7 @@ def gpu_arm(args, rank, world, local_rank):
                "fp64_value": world * N * args.steps / (loop64 * 1e-3),
                "fp64_ms_per_step": loop64 / args.steps,
                "mixed_over_fp64": loop64 / loop_ms,
-               "fp64_threads_per_particle": int(tpp64.value),
+               "fp64_layout": layout64,
                "nve_drift_per_particle_per_tau": {
                    "mixed": drift32, "fp64": drift64, "e0_per_particle": e64_before / N,
                    "segment_steps": args.drift_steps,
@@ -410,7 +410,7 @@ def gpu_arm(args, rank, world, local_rank):
             cmp.update(oracle_parity(lib, h, ids, box))
 
     lib.espp_system_destroy(h)
-    configs = (small_configs(lib, args.replica_steps)
+    configs = (small_configs(lib, args.replica_steps, args.cg_small)
                if (rank == 0 and world == 1 and not args.no_configs) else None)
     if rank != 0:
         if dist is not None:
@@ -429,7 +429,10 @@ def gpu_arm(args, rank, world, local_rank):
     cpu_rate, cpu_cores = cpu_baseline(1, budget_s=args.cpu_budget) if world == 1 else (None, 1)
     cpu_classic = (cpu_baseline(1, budget_s=args.cpu_budget, entry="espp_run")[0]
                    if world == 1 else None)
-    traffic = (FORCE_TRAFFIC_PER_PARTICLE * N) if (FORCE_TRAFFIC_PER_PARTICLE and prec) else None
+    force_kernel = ("k_force_brick_" if layout["form"] == "brick" else "k_force_") + \
+        ("mixed" if prec else "fp64")
+    tr = FORCE_TRAFFIC_PER_PARTICLE.get(force_kernel)
+    traffic = tr * N if tr else None
     line = {
         "metric": "LJ particle-steps/s", "value": value, "unit": "particle-steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -445,9 +448,9 @@ def gpu_arm(args, rank, world, local_rank):
                    "cell_grid": list(map(int, cg)), "l2": "inputs larger than L2 (262 MB)",
                    "parallelism": "replicas x%d" % world if world > 1 else "1 GPU",
                    "resorts_in_timed_steps": int(resorts.value),
-                   "threads_per_particle": int(tpp.value),
-                   "autotune_force_ms": {str(c): float(t) for c, t in zip((1, 2, 4, 8), tune_ms)}},
-        "roofline": {"kernel": "k_force_mixed" if prec else "k_force_fp64", "bound": "hbm",
+                   "layout": layout, "steps_per_build": steps_per_build,
+                   "autotune": tune},
+        "roofline": {"kernel": force_kernel, "bound": "hbm",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": peak_kind,
                      "alg_bytes_per_particle": FORCE_BYTES, "traffic": traffic,
@@ -485,6 +488,30 @@ def gpu_arm(args, rank, world, local_rank):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def autotune_layout(lib, h, args, steps_per_build):
+    """espp_autotune_layout (or the layout forced by --layout): returns the layout in use
+    {form, tpp, brick} and the timed candidates."""
+    from espressopp_b200._abi import call, dptr, i32ptr
+    best = np.zeros(5, np.int32)
+    table = np.zeros((32, 8))
+    n = ctypes.c_int32(0)
+    if args.layout == "auto":
+        call(lib, "espp_autotune_layout", h, steps_per_build, i32ptr(best), dptr(table), 32,
+             ctypes.byref(n))
+    else:
+        form = {"global": 0, "brick": 1, "global-brick-build": 2}[args.layout]
+        b = np.zeros(3, np.int32)
+        call(lib, "espp_set_layout", h, form, max(1, args.tpp), i32ptr(b))
+        call(lib, "espp_get_layout", h, i32ptr(best))
+    names = {0: "global", 1: "brick", 2: "global-brick-build"}
+    lay = {"form": names[int(best[0])], "threads_per_particle": int(best[1]),
+           "brick": [int(x) for x in best[2:5]]}
+    rows = [{"form": names[int(r[0])], "threads_per_particle": int(r[1]),
+             "brick": [int(x) for x in r[2:5]], "force_ms": float(r[5]),
+             "build_ms": float(r[6]), "score_ms": float(r[7])} for r in table[:n.value]]
+    return lay, rows
 
 
 def oracle_parity(lib, h, ids, box):
@@ -604,7 +631,7 @@ def lj32k_config(lib, prec, steps=1000):
     return {"value": 32768 * steps / (ms[1] * 1e-3), "ms_per_step": float(ms[1]) / steps}
 
 
-def small_configs(lib, replica_steps=1000):
+def small_configs(lib, replica_steps=1000, cg_chains=200):
     from espressopp_b200 import _abi
     out = {}
     for name, prec in (("fp64", _abi.PREC_FP64), ("mixed", _abi.PREC_MIXED)):
@@ -626,25 +653,49 @@ def small_configs(lib, replica_steps=1000):
             "swaps": {"batched": rep["batched"]["swaps"],
                       "sequential": rep["sequential"]["swaps"]},
             "unit": "particle-steps/s (wall clock around run calls and exchanges)"}
+    if cg_chains > 0:
+        log("configs: learned CG potential, %d chains" % cg_chains)
+        t0 = time.perf_counter()
+        line = cg_workflow(cg_chains, 100, 5, 20000, 5, 50)
+        q = line["cg_quality"]
+        out["cg_learned_potential"] = {
+            "workload": "Kremer-Grest melt %d x 200 beads -> %d CG sites (4:1), 100 frames, "
+                        "5 epochs, 5 IBI iterations, 20,000 CG steps (the full configuration: "
+                        "1000 chains, 500 frames, 100,000 steps: --workload cg)"
+                        % (cg_chains, cg_chains * 50),
+            "force_matching_rel_err": q["force_matching_rel_err"],
+            "rdf_l2": {k: v for k, v in q["rdf_l2"].items() if k != "curves"},
+            "particle_steps_per_chain_motion_fg_over_cg":
+                q["particle_steps_per_chain_motion_fg_over_cg"],
+            "cg_ms_per_step": q["cg_ms_per_step"],
+            "site_steps_per_s_learned": line["value"],
+            "seconds": time.perf_counter() - t0}
     return out
 
 
 # ---- learned coarse-grained potential ---------------------------------------------
 def cg_arm(args, rank, world, local_rank):
-    """Learned CG potential workload: a fine-grained Kremer-Grest melt of 1000 x 200 beads
-    (200,000 beads) mapped 4 -> 1 (50,000 sites); 500 frames of mapped conservative
-    forces; CG bonds and angles from Boltzmann-inverted tables; an MLP 16-64-64-1 trained
-    by force matching on the GPU; a force-matched pair table as the fallback; CG runs
-    compared with the fine-grained melt by force-matching error, RDF and chain motion.
-    Sizes scale with --cg-chains and --cg-frames."""
-    from espressopp_b200 import cg
-    from espressopp_b200._abi import call, dptr
+    """Learned CG potential workload (cg_workflow at the sizes of the arguments)."""
     if rank != 0:
         return
-    nch, nfr = args.cg_chains, args.cg_frames
+    line = cg_workflow(args.cg_chains, args.cg_frames, args.cg_epochs, args.cg_steps,
+                       args.cg_ibi, args.cg_window)
+    print(json.dumps(line), flush=True)
+
+
+def cg_workflow(nch, nfr, epochs, cg_steps, ibi_iters, window):
+    """Learned CG potential: a fine-grained Kremer-Grest melt of nch x 200 beads mapped
+    4 -> 1 (nch x 50 sites); nfr frames of mapped conservative forces averaged over
+    `window` steps; CG bonds and angles from Boltzmann-inverted tables; an MLP 16-64-64-1
+    trained by force matching on the GPU for `epochs` epochs; a force-matched pair table as
+    the fallback; ibi_iters of iterative Boltzmann inversion; CG runs of cg_steps steps
+    compared with the fine-grained melt by force-matching error, RDF and chain motion.
+    Returns the result line."""
+    from espressopp_b200 import cg
+    from espressopp_b200._abi import call, dptr
     t0 = time.perf_counter()
     pos, frc, L, bonds = cg.fg_frames(nch, 200, nfr, 20, warm_capped=1000, warm=4000,
-                                      window=args.cg_window, log=log)
+                                      window=window, log=log)
     t_fg = time.perf_counter() - t0
     log("fine-grained frames: %d x %d sites in %.1f s" % (nfr, pos.shape[1], t_fg))
     ntrain = int(0.8 * nfr)
@@ -688,7 +739,7 @@ def cg_arm(args, rank, world, local_rank):
     shift, scale = cg.descriptor_norm(s, pos)
     model.set_norm(shift, scale)
     t2 = time.perf_counter()
-    hist = cg.train_mlp(s, model, pos[:ntrain], resid[:ntrain], epochs=args.cg_epochs,
+    hist = cg.train_mlp(s, model, pos[:ntrain], resid[:ntrain], epochs=epochs,
                         batch=4, lr=1e-3, log=log)
     t_train = time.perf_counter() - t2
     del resid
@@ -708,7 +759,7 @@ def cg_arm(args, rank, world, local_rank):
         sysm.set_pos(sysm.ids, cg.wrap(pos[-1], L))
         call(sysm.lib, "espp_integrator_set", sysm.h, 0.01)
         sysm.thermostat(True)
-        _, ibi[name], g_cg[name] = cg.ibi_refine(sysm, ptab, g_fg, nb, iters=args.cg_ibi,
+        _, ibi[name], g_cg[name] = cg.ibi_refine(sysm, ptab, g_fg, nb, iters=ibi_iters,
                                                  log=log, bonded=(bonds, tab, blen))
     t_ibi = time.perf_counter() - t3
     err_mlp = cg.fm_error(s, pos[ntrain:], target[ntrain:], fbond_test)
@@ -737,11 +788,11 @@ def cg_arm(args, rank, world, local_rank):
                 log("CG run (%s) step %d: T %.3f, max |F| %.3g" %
                     (name, 100 * (k + 1), np.sum(4 * v * v) / (3 * len(v)), np.max(np.abs(f))))
         traj = []
-        window = nfr * 20
+        window_steps = nfr * 20
         ms_total = 0.0
         g = np.zeros(nb)
         ng = 0
-        for k in range(window // 100):
+        for k in range(window_steps // 100):
             sysm.run(100)
             ms = np.zeros(2)
             call(sysm.lib, "espp_last_run_ms", sysm.h, dptr(ms))
@@ -751,7 +802,7 @@ def cg_arm(args, rank, world, local_rank):
             if k % 4 == 0:
                 g += sysm.rdf(nb)
                 ng += 1
-        steps_rest = args.cg_steps - window - 2000
+        steps_rest = cg_steps - window_steps - 2000
         if steps_rest > 0:
             sysm.run(steps_rest)
             ms = np.zeros(2)
@@ -765,7 +816,7 @@ def cg_arm(args, rank, world, local_rank):
         sel = r < 3.0 * 2
         l2 = float(np.sqrt(np.mean((g[sel] - g_fg[sel]) ** 2)))
         out[name] = {"rdf_l2": l2, "chain_msd_100tau": float(msd_cg[-1]),
-                     "ms_per_step": ms_total / (window // 100 * 100 + max(steps_rest, 0))}
+                     "ms_per_step": ms_total / (window_steps // 100 * 100 + max(steps_rest, 0))}
         log("CG run (%s): RDF L2 %.4f, chain MSD %.3f (FG %.3f)" %
             (name, l2, msd_cg[-1], msd_fg[-1]))
     n_fg = nch * 200
@@ -802,13 +853,13 @@ def cg_arm(args, rank, world, local_rank):
             "seconds": {"fg_frames": t_fg, "pair_table_fit": t_tab, "ibi": t_ibi,
                         "mlp_training": t_train},
             "force_target": "mapped conservative forces averaged over %d fine-grained "
-                            "steps, minus the CG bond forces" % args.cg_window,
+                            "steps, minus the CG bond forces" % window,
             "note": "force-matching error on held-out frames (20 %) relative to the "
                     "window-averaged mapped forces; what remains of the fine-grained "
                     "fluctuation after the average is noise that no CG model can fit"},
     }
-    print(json.dumps(line), flush=True)
     model.close()
+    return line
 
 
 # ---- learned potential: force evaluation micro-benchmark --------------------------
@@ -1039,6 +1090,8 @@ def main():
                     help="Langevin steps (gamma 1, T 1) before the NVE segment")
     ap.add_argument("--drift-steps", type=int, default=2000,
                     help="NVE steps of the drift measurement (both precisions)")
+    ap.add_argument("--cg-small", type=int, default=200,
+                    help="chains of the reduced learned-CG run in the default line (0: skip)")
     ap.add_argument("--replica-steps", type=int, default=1000,
                     help="steps of the 64-replica measurement in the default line (0: skip)")
     ap.add_argument("--no-oracle", action="store_true",
@@ -1046,7 +1099,11 @@ def main():
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the Kremer-Grest melt and 32k LJ configurations")
     ap.add_argument("--tpp", type=int, default=0, choices=[0, 1, 2, 4, 8],
-                    help="threads per particle of the force kernel (0: autotune)")
+                    help="threads per particle of the global-list force kernel")
+    ap.add_argument("--layout", default="auto",
+                    choices=["auto", "global", "brick", "global-brick-build"],
+                    help="list layout: autotuned, global per-particle lists (per-cell build), "
+                         "brick windows, global lists built by brick windows")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")

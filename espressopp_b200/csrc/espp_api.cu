@@ -149,14 +149,14 @@ struct espp_system {
 
   // brick path of the Verlet list and pair kernels (BrickView)
   bool brickAllowed = false;  // ESPP_B200_BRICK=1 selects the brick form
+  bool brickBuild = false;    // the global-form list is built by brick windows
+                              // (ESPP_B200_BRICK_BUILD=1) instead of the per-cell lanes
+  bool brickBuildUsed = false;  // the current global-form list came from the brick build
   bool brickOn = false;       // the current list is in the brick form
-  int brickG = 2;             // particles per group
   int brickB[3] = {0, 0, 0};  // brick extent in cells (0: chosen from the density)
-  int brickWmax = 0;          // window capacity
-  uint16_t* bnl = nullptr;
-  int32_t* bnnG = nullptr;
-  int32_t* cellGroupStart = nullptr;
-  int bgcap = 0, bKb = 0;
+  int brickWmax = 0;          // window slots (sentinel included)
+  uint16_t* bnl = nullptr;    // bKb * cap entries
+  int bKb = 0;
   double* bpartials = nullptr;  // one row of 7 per brick (observables, digest)
   int bpartialsCap = 0;
 
@@ -229,7 +229,6 @@ struct espp_system {
   BrickView brick_view() const {
     BrickView b{};
     b.on = brickOn ? 1 : 0;
-    b.G = brickG;
     b.nbricks = 1;
     for (int k = 0; k < 3; ++k) {
       b.b[k] = brickB[k] > 0 ? brickB[k] : 1;
@@ -238,9 +237,6 @@ struct espp_system {
     }
     b.wmax = brickWmax;
     b.nl = bnl;
-    b.nnG = bnnG;
-    b.cellGroupStart = cellGroupStart;
-    b.gcap = bgcap;
     b.Kb = bKb;
     return b;
   }
@@ -436,7 +432,12 @@ void upload(espp_system* s, const HostParticles& h) {
     cuda_check(cudaMemset(s->nn, 0, sizeof(int32_t) * cap), "memset");
     s->K = 0;
     dfree(s->nl);
+    s->bKb = 0;
+    dfree(s->bnl);
   }
+  // the brick extent and window capacity follow the density
+  s->brickB[0] = s->brickB[1] = s->brickB[2] = 0;
+  s->brickWmax = 0;
   s->n = n;
   push_pa(s);
   copy_soa_up(s, s->A.id, h.id, 1);
@@ -511,8 +512,6 @@ void rebuild_id_tables(espp_system* s) {
   if (!ex.empty()) csr(ex, s->exclStart, s->exclIds);
   // triples: ids and, per particle, the triples it belongs to with its role
   dfree(s->bnl);
-  dfree(s->bnnG);
-  dfree(s->cellGroupStart);
   dfree(s->bpartials);
   dfree(s->d_triples);
   dfree(s->tripStart);
@@ -619,49 +618,47 @@ bool brick_wanted(const espp_system* s) {
   return true;
 }
 
-// Brick extent: about 160 particles per brick, at most kBrickMax cells per edge.
+// Brick extent: the largest brick of at most 240 particles (the block has 256 threads,
+// one per particle) and at most kBrickMax cells per edge, grown one dimension at a time.
 void choose_brick(espp_system* s) {
   const double ncells = (double)s->nc[0] * s->nc[1] * s->nc[2];
   const double occ = std::max(s->n / ncells, 0.05);
-  int b = (int)std::lround(std::cbrt(160.0 / occ));
-  b = std::max(1, std::min(kBrickMax, b));
-  for (int k = 0; k < 3; ++k) s->brickB[k] = std::min(b, s->nc[k]);
+  const double target = 240.0;
+  int b[3] = {1, 1, 1};
+  for (bool grew = true; grew;) {
+    grew = false;
+    for (int k = 2; k >= 0; --k) {
+      if (b[k] >= std::min(kBrickMax, s->nc[k])) continue;
+      const double vol = occ * (b[0] + (k == 0)) * (b[1] + (k == 1)) * (b[2] + (k == 2));
+      if (vol > target) continue;
+      ++b[k];
+      grew = true;
+    }
+  }
+  for (int k = 0; k < 3; ++k) s->brickB[k] = b[k];
 }
 
 int brick_window_limit(const espp_system* s) {
-  const int bits = 16 - s->brickG;
-  const int byBits = 1 << bits;
+  (void)s;
   const int bySmem = (int)(brick_smem_limit() / (sizeof(double) * 4 + sizeof(int)));
-  return std::min(byBits, bySmem) / 32 * 32;
+  return std::min(65536, bySmem) / 32 * 32;
 }
 
-// Buffers of the brick form sized for the current particles and grid.
-void ensure_brick_buffers(espp_system* s) {
+bool brick_geometry_ok(const espp_system* s) {
+  for (int k = 0; k < 3; ++k)
+    if (s->nc[k] < 2) return false;
+  return s->n > 0;
+}
+
+// Brick extent, window capacity and partial-sum rows for the current particles and grid.
+void ensure_brick_window(espp_system* s) {
   if (s->brickB[0] == 0) choose_brick(s);
-  const long long ncells = (long long)s->nc[0] * s->nc[1] * s->nc[2];
-  if (!s->cellGroupStart) s->cellGroupStart = dalloc<int32_t>(ncells + 1);
-  // groups never straddle cells: sum over cells of ceil(n_c / G) <= (n + ncells (G-1)) / G
-  const long long gcap = (s->n + ncells * (s->brickG - 1)) / s->brickG + 1;
-  if (gcap > (1LL << 31) - 1) raise(ESPP_ERANGE, "too many particle groups");
-  if (s->bKb == 0) {
-    const int K1 = estimate_K(s);  // per-particle capacity with margin
-    // a group's list is the union of its members' lists: about 1.4 (G = 2) or 1.9
-    // (G = 4) times one member's
-    s->bKb = ((int)std::ceil(K1 * (s->brickG == 2 ? 1.45 : 1.95)) + 7) / 8 * 8;
-    dfree(s->bnl);
-  }
-  if (gcap > s->bgcap || !s->bnl) {
-    dfree(s->bnl);
-    dfree(s->bnnG);
-    s->bgcap = (int)gcap;
-    s->bnl = dalloc<uint16_t>((size_t)s->bKb * s->bgcap);
-    s->bnnG = dalloc<int32_t>(s->bgcap);
-  }
   if (s->brickWmax == 0) {
     double V = 1.0;
     for (int k = 0; k < 3; ++k) V *= (s->brickB[k] + 2) * (s->L[k] / s->nc[k]);
     const double rho = s->n / (s->L[0] * s->L[1] * s->L[2]);
-    int w = (int)std::ceil(1.35 * rho * V) + 96;
+    int ncw = (s->brickB[0] + 2) * (s->brickB[1] + 2) * (s->brickB[2] + 2);
+    int w = (int)std::ceil(1.35 * rho * V) + 3 * ncw + 96;  // up to 3 spare slots a cell
     w = std::max(256, (w + 31) / 32 * 32);
     s->brickWmax = std::min(w, brick_window_limit(s));
   }
@@ -673,10 +670,20 @@ void ensure_brick_buffers(espp_system* s) {
   }
 }
 
+// Buffers of the brick form: the window and the window-index lists.
+void ensure_brick_buffers(espp_system* s) {
+  ensure_brick_window(s);
+  if (s->bKb == 0 || !s->bnl) {
+    if (s->bKb == 0) s->bKb = estimate_K(s);
+    dfree(s->bnl);
+    s->bnl = dalloc<uint16_t>((size_t)s->bKb * s->cap);
+  }
+}
+
 void grow_brick_lists(espp_system* s, int need) {
   s->bKb = (std::max(s->bKb * 2, need + 32) + 7) / 8 * 8;
   dfree(s->bnl);
-  s->bnl = dalloc<uint16_t>((size_t)s->bKb * s->bgcap);
+  s->bnl = dalloc<uint16_t>((size_t)s->bKb * s->cap);
 }
 
 // Doubles the window capacity; false when it is at its limit.
@@ -687,25 +694,38 @@ bool grow_brick_window(espp_system* s) {
   return true;
 }
 
+// The per-particle global form: built by brick windows when the grid allows (every
+// candidate read once per brick from shared memory), else by the per-cell lane kernel.
 void build_list_plain(espp_system* s, double cutsq) {
   if (s->K == 0 || !s->nl) {
     s->K = estimate_K(s);
     dfree(s->nl);
     s->nl = dalloc<int32_t>((size_t)s->K * s->cap);
   }
-  if (!s->xrelFresh) launch_xrel(s->view(), s->st);
-  s->xrelFresh = false;
-  for (int attempt = 0; attempt < 6; ++attempt) {
+  bool useBrick = s->brickBuild && brick_geometry_ok(s);
+  if (useBrick) ensure_brick_window(s);
+  for (int attempt = 0; attempt < 12; ++attempt) {
     DevView d = s->view();
-    launch_build_nl(d, cutsq, s->st);
+    if (useBrick) {
+      launch_build_brick(d, cutsq, s->st);
+    } else {
+      if (!s->xrelFresh) launch_xrel(d, s->st);
+      s->xrelFresh = false;
+      launch_build_nl(d, cutsq, s->st);
+    }
     cuda_check(cudaGetLastError(), "Verlet list kernel");
     unsigned e = read_err(s);
-    if (!(e & kErrNlOverflow)) break;
+    if (!(e & (kErrNlOverflow | kErrWindow))) break;
     cuda_check(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->st), "memset");
+    if (e & kErrWindow) {
+      if (!grow_brick_window(s)) useBrick = false;  // too dense for the stage
+      continue;
+    }
     s->K *= 2;
     dfree(s->nl);
     s->nl = dalloc<int32_t>((size_t)s->K * s->cap);
   }
+  s->brickBuildUsed = useBrick;
 }
 
 // Brick form; false when a window cannot be staged (the caller falls back to the
@@ -714,7 +734,6 @@ bool build_list_brick(espp_system* s, double cutsq) {
   ensure_brick_buffers(s);
   for (int attempt = 0; attempt < 8; ++attempt) {
     DevView d = s->view();
-    launch_brick_layout(d, s->scr, s->st);
     launch_build_brick(d, cutsq, s->st);
     cuda_check(cudaGetLastError(), "brick Verlet list kernels");
     unsigned e = read_err(s);
@@ -1002,9 +1021,8 @@ void launch_rebuild_kernels(espp_system* s, cudaStream_t st) {
   launch_id_map(d, st);
   if (s->has_vl) {
     const double cv = s->vl_cut + s->skin;
-    if (s->brickOn) {
-      launch_brick_layout(d, s->scr, st);
-      launch_build_brick(d, cv * cv, st);
+    if (s->brickOn || s->brickBuildUsed) {
+      launch_build_brick(d, cv * cv, st);  // window-index or global form (d.brick.on)
     } else {
       launch_build_nl(d, cv * cv, st);
     }
@@ -1032,6 +1050,19 @@ void add_step_loop(espp_system* s, cudaGraph_t g, const IntegrateArgs& ai) {
              "conditional handle");
   cudaStream_t cs;
   cuda_check(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
+  // on an error inside a capture: end it and release the stream before the error leaves
+  struct CaptureGuard {
+    cudaStream_t cs;
+    ~CaptureGuard() {
+      cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(cs, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(cs, &g);
+      }
+      cudaGetLastError();
+      cudaStreamDestroy(cs);
+    }
+  } guard{cs};
   const double skinHalf = 0.5 * s->skin;
   // body: decide
   cuda_check(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
@@ -1060,16 +1091,20 @@ void add_step_loop(espp_system* s, cudaGraph_t g, const IntegrateArgs& ai) {
                                            cudaStreamCaptureModeThreadLocal), "capture");
   launch_rebuild_kernels(s, cs);
   cuda_check(cudaStreamEndCapture(cs, &done), "end capture");
-  cudaStreamDestroy(cs);
 }
 
 void capture_graph(espp_system* s, const IntegrateArgs& ai) {
   destroy_graph(s);
   cudaGraph_t g;
   cuda_check(cudaGraphCreate(&g, 0), "cudaGraphCreate");
-  add_step_loop(s, g, ai);
-  cudaGraphExec_t ex;
-  cuda_check(cudaGraphInstantiate(&ex, g, 0), "cudaGraphInstantiate");
+  cudaGraphExec_t ex = nullptr;
+  try {
+    add_step_loop(s, g, ai);
+    cuda_check(cudaGraphInstantiate(&ex, g, 0), "cudaGraphInstantiate");
+  } catch (...) {
+    cudaGraphDestroy(g);
+    throw;
+  }
   s->graph = g;
   s->graphExec = ex;
 }
@@ -1109,8 +1144,8 @@ void maybe_grow_K(espp_system* s) {
   if (s->brickOn) {
     if (hw * 10 <= s->bKb * 9) return;
     const int Kn = (hw * 3 / 2 + 15) / 8 * 8;
-    uint16_t* nl = dalloc<uint16_t>((size_t)Kn * s->bgcap);
-    cuda_check(cudaMemcpyAsync(nl, s->bnl, sizeof(uint16_t) * (size_t)s->bKb * s->bgcap,
+    uint16_t* nl = dalloc<uint16_t>((size_t)Kn * s->cap);
+    cuda_check(cudaMemcpyAsync(nl, s->bnl, sizeof(uint16_t) * (size_t)s->bKb * s->cap,
                                cudaMemcpyDeviceToDevice, s->st), "copy");
     sync(s);
     dfree(s->bnl);
@@ -1304,15 +1339,14 @@ void recover_overflow(espp_system* s, const RunSnapshot& r) {
   s->step = r.step;
   s->resortFlag = r.resortFlag;
   s->binned = false;
-  if (s->brickOn) {
-    if (why & kErrWindow) {
-      if (!grow_brick_window(s)) {
-        s->brickOn = false;
-        s->brickAllowed = false;
-      }
-    } else {
-      grow_brick_lists(s, hw);
+  if (why & kErrWindow) {
+    if (!grow_brick_window(s)) {  // too dense for the stage: no brick kernels from now on
+      s->brickOn = false;
+      s->brickAllowed = false;
+      s->brickBuild = false;
     }
+  } else if (s->brickOn) {
+    grow_brick_lists(s, hw);
   } else {
     s->K = (std::max(s->K * 2, hw + 32) + 7) / 8 * 8;  // multiple of 8
     dfree(s->nl);
@@ -1416,8 +1450,13 @@ void batch_run(espp_batch* b, int64_t nsteps) {
   if (!b->ex || key != b->key) {
     batch_destroy_graph(b);
     cuda_check(cudaGraphCreate(&b->g, 0), "cudaGraphCreate");
-    for (size_t r = 0; r < R; ++r) add_step_loop(b->sys[r], b->g, ags[r]);
-    cuda_check(cudaGraphInstantiate(&b->ex, b->g, 0), "cudaGraphInstantiate");
+    try {
+      for (size_t r = 0; r < R; ++r) add_step_loop(b->sys[r], b->g, ags[r]);
+      cuda_check(cudaGraphInstantiate(&b->ex, b->g, 0), "cudaGraphInstantiate");
+    } catch (...) {
+      batch_destroy_graph(b);
+      throw;
+    }
     b->key = key;
   }
   cuda_check(cudaEventRecord(b->beg, b->st), "event");
@@ -1430,7 +1469,7 @@ void batch_run(espp_batch* b, int64_t nsteps) {
   b->lastMs = ms;
   for (size_t r = 0; r < R; ++r) {
     espp_system* s = b->sys[r];
-    if (read_err(s) & kErrNlOverflow) {
+    if (read_err(s) & (kErrNlOverflow | kErrWindow)) {
       recover_overflow(s, snaps[r]);
       run_host(s, nsteps);
       continue;
@@ -1700,10 +1739,7 @@ int espp_system_create(const double box[3], double skin, const int32_t cell_grid
     cuda_check(cudaMallocHost(&s->hctr, sizeof(DevCounters)), "pinned counters");
     if (const char* g = std::getenv("ESPP_B200_GRAPH")) s->useGraph = std::atoi(g) != 0;
     if (const char* b = std::getenv("ESPP_B200_BRICK")) s->brickAllowed = std::atoi(b) != 0;
-    if (const char* g = std::getenv("ESPP_B200_GROUP")) {
-      const int v = std::atoi(g);
-      if (v == 2 || v == 4) s->brickG = v;
-    }
+    if (const char* b = std::getenv("ESPP_B200_BRICK_BUILD")) s->brickBuild = std::atoi(b) != 0;
     if (const char* t = std::getenv("ESPP_B200_TPP")) {
       const int v = std::atoi(t);
       if (v == 1 || v == 2 || v == 4 || v == 8) s->tpp = v;
@@ -1930,6 +1966,8 @@ int espp_vl_create(espp_system* s, double cutoff, int64_t nexcl, const int64_t* 
     if (nexcl > 0) s->idDirty = true;
     s->K = 0;
     dfree(s->nl);
+    s->bKb = 0;
+    dfree(s->bnl);
     if (s->idDirty) rebuild_id_tables(s);
     if (!s->binned) bin(s, false);
     build_list(s);
@@ -2841,6 +2879,162 @@ int espp_set_tpp(espp_system* s, int32_t tpp) {
     if (tpp != 1 && tpp != 2 && tpp != 4 && tpp != 8)
       raise(ESPP_EINVAL, "threads per particle must be 1, 2, 4 or 8");
     s->tpp = tpp;
+  });
+}
+
+namespace {
+
+// Puts the list into `form` (0: per-particle global list with tpp threads per particle,
+// 1: brick windows of extent b, zeros choosing it from the density) at the current
+// positions; the rebuild is not counted as a list build.
+void apply_layout(espp_system* s, int form, int tpp, const int b[3]) {
+  s->brickBuild = form == 2;
+  if (form == 1 || form == 2) {
+    for (int k = 0; k < 3; ++k) s->brickB[k] = (b && b[k] > 0) ? std::min(b[k], s->nc[k]) : 0;
+    if (s->brickB[0] == 0 || s->brickB[1] == 0 || s->brickB[2] == 0)
+      s->brickB[0] = s->brickB[1] = s->brickB[2] = 0;
+    s->brickWmax = 0;
+  }
+  if (form == 2) {
+    s->brickAllowed = false;
+    if (tpp == 1 || tpp == 2 || tpp == 4 || tpp == 8) s->tpp = tpp;
+  } else if (form == 1) {
+    s->brickAllowed = true;
+    for (int k = 0; k < 3; ++k) s->brickB[k] = (b && b[k] > 0) ? std::min(b[k], s->nc[k]) : 0;
+    if (s->brickB[0] == 0 || s->brickB[1] == 0 || s->brickB[2] == 0)
+      s->brickB[0] = s->brickB[1] = s->brickB[2] = 0;
+    s->brickWmax = 0;
+  } else {
+    s->brickAllowed = false;
+    if (tpp == 1 || tpp == 2 || tpp == 4 || tpp == 8) s->tpp = tpp;
+  }
+  if (s->idDirty) rebuild_id_tables(s);
+  if (!s->binned) bin(s, false);
+  if (!s->has_vl) return;
+  const int64_t builds = s->builds;
+  build_list(s);
+  s->builds = builds;
+}
+
+// Device time (ms) of one list build in the current form and the mean of 3 force
+// launches on it.
+void time_layout(espp_system* s, double& build_ms, double& force_ms) {
+  cudaEvent_t e0, e1;
+  cuda_check(cudaEventCreate(&e0), "event");
+  cuda_check(cudaEventCreate(&e1), "event");
+  const double cv = s->vl_cut + s->skin;
+  DevView d = s->view();
+  cuda_check(cudaEventRecord(e0, s->st), "event");
+  if (s->brickOn || s->brickBuildUsed)
+    launch_build_brick(d, cv * cv, s->st);
+  else
+    launch_build_nl(d, cv * cv, s->st);
+  cuda_check(cudaEventRecord(e1, s->st), "event");
+  sync(s);
+  float t = 0.f;
+  cuda_check(cudaEventElapsedTime(&t, e0, e1), "event time");
+  build_ms = t;
+  launch_force_kernel(s, s->st);  // warm
+  cuda_check(cudaEventRecord(e0, s->st), "event");
+  for (int r = 0; r < 3; ++r) launch_force_kernel(s, s->st);
+  cuda_check(cudaEventRecord(e1, s->st), "event");
+  sync(s);
+  cuda_check(cudaEventElapsedTime(&t, e0, e1), "event time");
+  force_ms = t / 3.0;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cuda_check(cudaGetLastError(), "layout timing");
+  check_err(s);
+}
+
+}  // namespace
+
+int espp_set_layout(espp_system* s, int32_t form, int32_t tpp, const int32_t brick[3]) {
+  return guard([&] {
+    checked(s);
+    if (form < 0 || form > 2) raise(ESPP_EINVAL, "layout form must be 0, 1 or 2");
+    if (form != 1 && tpp != 1 && tpp != 2 && tpp != 4 && tpp != 8)
+      raise(ESPP_EINVAL, "threads per particle must be 1, 2, 4 or 8");
+    int b[3] = {0, 0, 0};
+    for (int k = 0; k < 3 && brick; ++k) {
+      if (brick[k] < 0 || brick[k] > kBrickMax)
+        raise(ESPP_EINVAL, "brick extent must be 0 (automatic) or 1.." + std::to_string(kBrickMax));
+      b[k] = brick[k];
+    }
+    apply_layout(s, form, tpp, b);
+  });
+}
+
+int espp_get_layout(espp_system* s, int32_t out[5]) {
+  return guard([&] {
+    checked(s);
+    if (!out) raise(ESPP_EINVAL, "null output pointer");
+    out[0] = s->brickOn ? 1 : (s->brickBuildUsed ? 2 : 0);
+    out[1] = s->tpp;
+    for (int k = 0; k < 3; ++k) out[2 + k] = (s->brickOn || s->brickBuildUsed) ? s->brickB[k] : 0;
+  });
+}
+
+int espp_autotune_layout(espp_system* s, double steps_per_build, int32_t best[5],
+                         double* table, int32_t cap, int32_t* ncand) {
+  return guard([&] {
+    checked(s);
+    if (s->idDirty) rebuild_id_tables(s);
+    if (!s->binned) bin(s, false);
+    if (!s->has_vl) raise(ESPP_ESTATE, "no Verlet list");
+    const double interval = steps_per_build > 0 ? steps_per_build : 10.0;
+    struct Cand {
+      int form, tpp, b[3];
+    };
+    std::vector<Cand> cands;
+    for (int t : {1, 2, 4, 8}) cands.push_back({0, t, {0, 0, 0}});
+    if (brick_geometry_ok(s)) cands.push_back({2, 1, {0, 0, 0}});
+    const bool brickable = [&] {
+      const bool was = s->brickAllowed;
+      s->brickAllowed = true;
+      const bool ok = brick_wanted(s);
+      s->brickAllowed = was;
+      return ok;
+    }();
+    if (brickable) {
+      const int shapes[][3] = {{0, 0, 0}, {1, 2, 2}, {2, 2, 2}, {2, 2, 3}, {2, 3, 3},
+                               {3, 3, 3}, {4, 4, 4}};
+      for (auto& sh : shapes) cands.push_back({1, 0, {sh[0], sh[1], sh[2]}});
+    }
+    double bestScore = 1e300;
+    int pick = -1;
+    int row = 0;
+    for (size_t c = 0; c < cands.size(); ++c) {
+      apply_layout(s, cands[c].form, cands[c].tpp, cands[c].b);
+      if (cands[c].form == 1 && !s->brickOn) continue;       // the window did not fit
+      if (cands[c].form == 2 && !s->brickBuildUsed) continue;
+      double bms = 0.0, fms = 0.0;
+      time_layout(s, bms, fms);
+      const double score = fms + bms / interval;
+      if (table && row < cap) {
+        double* r = table + (size_t)row * 8;
+        r[0] = cands[c].form;
+        r[1] = cands[c].form != 1 ? cands[c].tpp : 0;
+        for (int k = 0; k < 3; ++k) r[2 + k] = cands[c].form != 0 ? s->brickB[k] : 0;
+        r[5] = fms;
+        r[6] = bms;
+        r[7] = score;
+      }
+      ++row;
+      if (score < bestScore) {
+        bestScore = score;
+        pick = (int)c;
+      }
+    }
+    if (pick < 0) raise(ESPP_ESTATE, "no list layout could be timed");
+    apply_layout(s, cands[pick].form, cands[pick].tpp, cands[pick].b);
+    if (ncand) *ncand = row;
+    if (best) {
+      best[0] = s->brickOn ? 1 : (s->brickBuildUsed ? 2 : 0);
+      best[1] = s->tpp;
+      for (int k = 0; k < 3; ++k)
+        best[2 + k] = (s->brickOn || s->brickBuildUsed) ? s->brickB[k] : 0;
+    }
   });
 }
 

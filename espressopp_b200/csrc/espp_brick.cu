@@ -6,19 +6,20 @@
 // every particle of the brick.  One block per brick stages the window in shared memory
 // once, each particle's coordinates in a frame centred on the brick: the position
 // relative to the centre of its own cell plus that cell's offset in the window.  The
-// offset carries the periodic image, so pair distances need no minimum-image step, and
-// the frame spans at most (b/2 + 1) cells from its centre, so FP32 frame coordinates
-// keep about 2.4e-7 absolute precision for cells of 2.8.
+// offset carries the periodic image, so pair distances need no minimum-image step and
+// no integer-to-float conversion per pair, and the frame spans at most (b/2 + 1) cells
+// from its centre, so FP32 frame coordinates keep about 2.4e-7 absolute precision for
+// cells of 2.8.  Each window cell takes a multiple of 4 slots (the spare ones hold a
+// particle far away), so the build reads candidates four at a time with aligned
+// 16-byte loads.
 //
-// Particles of a cell are taken G at a time ("groups", consecutive in the in-cell
-// Morton order).  One thread owns one group and keeps one list for it: the union of
-// its members' Verlet lists, each entry the candidate's window index plus one bit per
-// member.  A candidate is loaded once from shared memory for all G members, and the
-// members' FP32 arithmetic runs two at a time in packed f32x2 instructions.
+// One thread per particle.  Its Verlet list holds 16-bit window indices of its brick;
+// a warp's coordinate reads hit shared memory instead of scattered global lines, and
+// two list entries are evaluated at once with packed f32x2 arithmetic.
 //
-//  k_build_brick        union lists at cutoff + skin; the FP32 test with the
-//                       reference's FP64 arithmetic near the cutoff (exact pair set of
-//                       VerletList.cpp:274-450), candidates from the 27 reference cells
+//  k_build_brick        lists at cutoff + skin: FP32 test of every candidate of the 27
+//                       reference cells, the reference's FP64 arithmetic near the
+//                       cutoff (exact pair set of VerletList.cpp:274-450)
 //  k_force_brick_mixed  FP32 LJ (+ capped) forces on frame coordinates, FP32 sums along
 //                       the list, int64 2^-32 fixed-point output; FENE bonds
 //  k_force_brick_fp64   the plain FP64 form of the same kernel
@@ -26,27 +27,37 @@
 //  k_pair_*_brick       export, count and digest of the pair set
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 
 #include "espp_device.h"
+
+#include <mutex>
+#include <set>
+#include <utility>
 #include "espp_internal.h"
 
 namespace espp {
 namespace {
 
-constexpr int kBrickThreads = 128;
+constexpr int kBrickThreads = 256;
 constexpr int kMaxWinCells = (kBrickMax + 2) * (kBrickMax + 2) * (kBrickMax + 2);
 constexpr int kMaxBrickCells = kBrickMax * kBrickMax * kBrickMax;
+constexpr float kFar = 1.0e18f;  // coordinate of the spare and sentinel slots
 
 // Tables of one brick, built by the whole block.
 struct BrickTables {
-  int winStart[kMaxWinCells + 1];   // window index of each window cell's first particle
+  int winStart[kMaxWinCells + 1];   // first slot of each window cell (a multiple of 4)
+  int winCount[kMaxWinCells];       // particles of each window cell
   int winGlob[kMaxWinCells];        // sorted index of each window cell's first particle
-  int bgStart[kMaxBrickCells + 1];  // local index of each brick cell's first group
-  int bgGlob[kMaxBrickCells];       // global index of each brick cell's first group
+  int cc[kMaxWinCells][3];          // box-wrapped int32 coordinates of each window cell's centre
+  float off[kMaxWinCells][3];       // frame position of each window cell's centre (FP32)
+  double shift[kMaxWinCells][3];    // FP64 frame = position - shift
+  int bpStart[kMaxBrickCells + 1];  // brick-local index of each brick cell's first particle
+  int bcInfo[kMaxBrickCells];       // brick cell: rx | ry << 8 | rz << 16
   int o[3];                         // brick origin (cell coordinates)
   int e[3];                         // brick extent in cells
   int w[3];                         // window extent in cells (e + 2)
-  int nwin, nwc, nbc, ngroups;
+  int nwin, nwc, nbc, npart;
 };
 
 __device__ __forceinline__ int wrap_cell(int c, int n) { return c < 0 ? c + n : (c >= n ? c - n : c); }
@@ -80,7 +91,7 @@ __device__ void warp_scan_inplace(int* vals, int n) {
   if (lane == 0) vals[n] = total;
 }
 
-// Window and group tables of brick `brick` (uniform over the block; ends with a barrier).
+// Window and particle tables of brick `brick` (uniform over the block; ends with a barrier).
 __device__ void brick_tables(const DevView& d, BrickTables& t, int brick) {
   const BrickView& bv = d.brick;
   if (threadIdx.x == 0) {
@@ -98,30 +109,38 @@ __device__ void brick_tables(const DevView& d, BrickTables& t, int brick) {
   }
   __syncthreads();
   for (int c = threadIdx.x; c < t.nwc; c += blockDim.x) {
-    const int wx = c % t.w[0], wy = (c / t.w[0]) % t.w[1], wz = c / (t.w[0] * t.w[1]);
-    const int gx = wrap_cell(t.o[0] - 1 + wx, d.nc[0]);
-    const int gy = wrap_cell(t.o[1] - 1 + wy, d.nc[1]);
-    const int gz = wrap_cell(t.o[2] - 1 + wz, d.nc[2]);
-    const int gc = gx + d.nc[0] * (gy + d.nc[1] * gz);
-    const int s0 = d.cellStart[gc];
+    const int wk[3] = {c % t.w[0], (c / t.w[0]) % t.w[1], c / (t.w[0] * t.w[1])};
+    int gk[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      gk[k] = wrap_cell(t.o[k] - 1 + wk[k], d.nc[k]);
+      // the cell's centre, and its position in the frame centred on the brick
+      const double centre = ((double)gk[k] + 0.5) * d.cellSize[k];
+      const double frame = ((double)(wk[k] - 1) + 0.5 - 0.5 * (double)t.e[k]) * d.cellSize[k];
+      t.cc[c][k] = (int)(unsigned)__double2ll_rn(centre * d.fixScale[k]);
+      t.off[c][k] = (float)frame;
+      t.shift[c][k] = centre - frame;
+    }
+    const int gc = gk[0] + d.nc[0] * (gk[1] + d.nc[1] * gk[2]);
+    const int s0 = d.cellStart[gc], n = d.cellStart[gc + 1] - s0;
     t.winGlob[c] = s0;
-    t.winStart[c] = d.cellStart[gc + 1] - s0;
+    t.winCount[c] = n;
+    t.winStart[c] = (n + 3) & ~3;
   }
   for (int c = threadIdx.x; c < t.nbc; c += blockDim.x) {
     const int rx = c % t.e[0], ry = (c / t.e[0]) % t.e[1], rz = c / (t.e[0] * t.e[1]);
     const int gc = (t.o[0] + rx) + d.nc[0] * ((t.o[1] + ry) + d.nc[1] * (t.o[2] + rz));
-    const int g0 = bv.cellGroupStart[gc];
-    t.bgGlob[c] = g0;
-    t.bgStart[c] = bv.cellGroupStart[gc + 1] - g0;
+    t.bpStart[c] = d.cellStart[gc + 1] - d.cellStart[gc];
+    t.bcInfo[c] = rx | (ry << 8) | (rz << 16);
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5;
   if (warp == 0) warp_scan_inplace(t.winStart, t.nwc);
-  if (warp == 1) warp_scan_inplace(t.bgStart, t.nbc);
+  if (warp == 1) warp_scan_inplace(t.bpStart, t.nbc);
   __syncthreads();
   if (threadIdx.x == 0) {
     t.nwin = t.winStart[t.nwc];
-    t.ngroups = t.bgStart[t.nbc];
+    t.npart = t.bpStart[t.nbc];
   }
   __syncthreads();
 }
@@ -131,250 +150,198 @@ __device__ __forceinline__ int own_wcell(const BrickTables& t, int rx, int ry, i
   return (rx + 1) + t.w[0] * ((ry + 1) + t.w[1] * (rz + 1));
 }
 
-// One group of the brick: its cell, members and list index.
-struct Group {
-  int g;        // global group index (list row)
+// One particle of the brick.
+struct Member {
+  int i;        // sorted index
+  int w;        // window slot
   int rx, ry, rz;
-  int wc;       // window cell of its cell
-  int w0;       // window index of its first member
-  int i0;       // sorted index of its first member
-  int nm;       // members (1..G)
 };
 
-template <int G>
-__device__ __forceinline__ Group brick_group(const BrickTables& t, int q) {
-  int lo = 0, hi = t.nbc - 1;  // last brick cell with bgStart <= q
+__device__ __forceinline__ Member brick_member(const BrickTables& t, int q) {
+  int lo = 0, hi = t.nbc - 1;  // last brick cell with bpStart <= q
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (t.bgStart[mid] <= q) lo = mid; else hi = mid - 1;
+    if (t.bpStart[mid] <= q) lo = mid; else hi = mid - 1;
   }
-  Group gr;
-  const int bc = lo, k = q - t.bgStart[bc];
-  gr.g = t.bgGlob[bc] + k;
-  gr.rx = bc % t.e[0];
-  gr.ry = (bc / t.e[0]) % t.e[1];
-  gr.rz = bc / (t.e[0] * t.e[1]);
-  gr.wc = own_wcell(t, gr.rx, gr.ry, gr.rz);
-  const int cnt = t.winStart[gr.wc + 1] - t.winStart[gr.wc];
-  gr.w0 = t.winStart[gr.wc] + G * k;
-  gr.i0 = t.winGlob[gr.wc] + G * k;
-  gr.nm = min(G, cnt - G * k);
-  return gr;
+  Member m;
+  const int k = q - t.bpStart[lo];
+  const int info = t.bcInfo[lo];
+  m.rx = info & 0xFF;
+  m.ry = (info >> 8) & 0xFF;
+  m.rz = info >> 16;
+  const int wc = own_wcell(t, m.rx, m.ry, m.rz);
+  m.w = t.winStart[wc] + k;
+  m.i = t.winGlob[wc] + k;
+  return m;
 }
 
-// Window cell of window index w (binary search over the window cells)
-__device__ __forceinline__ int window_cell_of(const BrickTables& t, int w) {
+// Sorted index of window slot w (a particle slot: not a spare one)
+__device__ __forceinline__ int window_glob(const BrickTables& t, int w) {
   int lo = 0, hi = t.nwc - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
     if (t.winStart[mid] <= w) lo = mid; else hi = mid - 1;
   }
-  return lo;
+  return t.winGlob[lo] + (w - t.winStart[lo]);
 }
 
-__device__ __forceinline__ int window_glob(const BrickTables& t, int w) {
-  const int c = window_cell_of(t, w);
-  return t.winGlob[c] + (w - t.winStart[c]);
+// the window fits the stage: its slots plus the sentinel, 16-bit indices
+__device__ __forceinline__ bool window_fits(const DevView& d, const BrickTables& t) {
+  return t.nwin + 1 <= d.brick.wmax;
 }
 
-// Frame offset (FP64) of window cell coordinate wk along dimension k: the window cell's
-// centre relative to the brick centre.
-__device__ __forceinline__ double frame_offset(const DevView& d, const BrickTables& t, int k,
-                                               int wk) {
-  return ((double)(wk - 1) + 0.5 - 0.5 * (double)t.e[k]) * d.cellSize[k];
-}
-
-// Stage the window in FP32 frame coordinates (x, y, z, type bits) from the box-wrapped
-// int32 coordinates: each particle relative to the centre of its cell (exact integer
-// difference, one conversion), plus the cell's frame offset.
-__device__ void stage_window_f32(const DevView& d, const BrickTables& t, float4* win) {
+// Visits every slot of the window: f(slot, sorted index or -1 for a spare slot, window
+// cell).  Warps take whole cells.
+template <class F>
+__device__ __forceinline__ void for_window(const BrickTables& t, F&& f) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   for (int c = warp; c < t.nwc; c += nw) {
-    const int wx = c % t.w[0], wy = (c / t.w[0]) % t.w[1], wz = c / (t.w[0] * t.w[1]);
-    const int gk[3] = {wrap_cell(t.o[0] - 1 + wx, d.nc[0]), wrap_cell(t.o[1] - 1 + wy, d.nc[1]),
-                       wrap_cell(t.o[2] - 1 + wz, d.nc[2])};
-    const int wk[3] = {wx, wy, wz};
-    int cc[3];
-    float off[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const double centre = ((double)gk[k] + 0.5) * d.cellSize[k];
-      cc[k] = (int)(unsigned)__double2ll_rn(centre * d.fixScale[k]);
-      off[k] = (float)frame_offset(d, t, k, wk[k]);
-    }
-    const int s0 = t.winStart[c], n = t.winStart[c + 1] - s0, g0 = t.winGlob[c];
-    for (int p = lane; p < n; p += 32) {
-      const int4 q = d.posq[g0 + p];
-      win[s0 + p] = make_float4(fmaf(wrapped_diff(q.x, cc[0], 1.0f), d.fixUnit[0], off[0]),
-                                fmaf(wrapped_diff(q.y, cc[1], 1.0f), d.fixUnit[1], off[1]),
-                                fmaf(wrapped_diff(q.z, cc[2], 1.0f), d.fixUnit[2], off[2]),
-                                __int_as_float(q.w));
-    }
+    const int s0 = t.winStart[c], ns = t.winStart[c + 1] - s0, n = t.winCount[c];
+    const int g0 = t.winGlob[c];
+    for (int p = lane; p < ns; p += 32) f(s0 + p, p < n ? g0 + p : -1, c);
   }
 }
 
-// Stage the window in FP64 frame coordinates from the FP64 positions; wglob (optional)
-// receives each entry's sorted index.
-__device__ void stage_window_f64(const DevView& d, const BrickTables& t, double4* win,
-                                 int* wglob) {
-  const ParticleArrays a = d.pa[0];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  const size_t cap = d.cap;
-  for (int c = warp; c < t.nwc; c += nw) {
-    const int wx = c % t.w[0], wy = (c / t.w[0]) % t.w[1], wz = c / (t.w[0] * t.w[1]);
-    const int gk[3] = {wrap_cell(t.o[0] - 1 + wx, d.nc[0]), wrap_cell(t.o[1] - 1 + wy, d.nc[1]),
-                       wrap_cell(t.o[2] - 1 + wz, d.nc[2])};
-    const int wk[3] = {wx, wy, wz};
-    double cen[3], off[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      cen[k] = ((double)gk[k] + 0.5) * d.cellSize[k];
-      off[k] = frame_offset(d, t, k, wk[k]);
-    }
-    const int s0 = t.winStart[c], n = t.winStart[c + 1] - s0, g0 = t.winGlob[c];
-    for (int p = lane; p < n; p += 32) {
-      const int j = g0 + p;
-      win[s0 + p] = make_double4((a.x[j] - cen[0]) + off[0], (a.x[cap + j] - cen[1]) + off[1],
-                                 (a.x[2 * cap + j] - cen[2]) + off[2], (double)a.type[j]);
-      if (wglob) wglob[s0 + p] = j;
-    }
-  }
-}
-
-template <int G>
-struct BrickBits {
-  static constexpr int kIdx = 16 - G;                 // window-index bits of an entry
-  static constexpr unsigned kIdxMask = (1u << kIdx) - 1u;
-  static constexpr int kMaxWindow = 1 << kIdx;
-};
-
-__device__ __forceinline__ unsigned long long f2_bcast(float v) { return f2_pack(v, v); }
-
-// 16-byte list block of group g (8 entries), read without L1 allocation
-__device__ __forceinline__ uint4 ld_block(const uint16_t* nl, size_t gcap, int g, int b) {
-  const int4 v = ld_list(reinterpret_cast<const int4*>(nl) + ((size_t)b * gcap + (size_t)g));
-  return make_uint4((unsigned)v.x, (unsigned)v.y, (unsigned)v.z, (unsigned)v.w);
-}
-
-__device__ __forceinline__ unsigned entry_of(const uint4& v, int e) {
-  const unsigned w = e < 2 ? v.x : (e < 4 ? v.y : (e < 6 ? v.z : v.w));
-  return (e & 1) ? (w >> 16) : (w & 0xFFFFu);
+// FP32 frame coordinates from the box-wrapped int32 coordinates: relative to the centre
+// of the particle's cell (an exact integer difference, one conversion) plus the cell's
+// frame position.
+__device__ __forceinline__ float4 f32_frame(const DevView& d, const BrickTables& t, int g, int c) {
+  if (g < 0) return make_float4(kFar, kFar, kFar, __int_as_float(0));
+  const int4 q = d.posq[g];
+  return make_float4(fmaf(wrapped_diff(q.x, t.cc[c][0], 1.0f), d.fixUnit[0], t.off[c][0]),
+                     fmaf(wrapped_diff(q.y, t.cc[c][1], 1.0f), d.fixUnit[1], t.off[c][1]),
+                     fmaf(wrapped_diff(q.z, t.cc[c][2], 1.0f), d.fixUnit[2], t.off[c][2]),
+                     __int_as_float(q.w));
 }
 
 // ---- Verlet build -----------------------------------------------------------------------
 
-template <int G, bool EXCL>
+constexpr int kStage = 8;  // staging entries per thread (one list block)
+
+// GOUT: the list in the per-particle global form (sorted indices as int32, blocks of 8 at
+// nl_index, padded with the particle itself) read by the global-list kernels; otherwise
+// window indices (16 bits) for the brick kernels.
+template <bool EXCL, bool GOUT>
 __global__ void __launch_bounds__(kBrickThreads) k_build_brick(DevView d, double cutsq) {
-  extern __shared__ __align__(16) float4 win[];
+  extern __shared__ __align__(16) float bsm[];  // x | y | z, wmax slots each
   __shared__ BrickTables t;
-  __shared__ __align__(16) uint16_t stg[kBrickThreads][8];
-  using B = BrickBits<G>;
+  __shared__ __align__(16) uint32_t stg[kBrickThreads][kStage];
   brick_tables(d, t, blockIdx.x);
-  if (t.nwin > d.brick.wmax || t.nwin > B::kMaxWindow) {
+  if (!window_fits(d, t)) {
     if (threadIdx.x == 0) atomicOr(d.err, kErrWindow);
     return;
   }
-  stage_window_f32(d, t, win);
+  const int wmax = d.brick.wmax;
+  float* wx = bsm;
+  float* wy = bsm + wmax;
+  float* wz = bsm + 2 * wmax;
+  for_window(t, [&](int s, int g, int c) {
+    const float4 r = f32_frame(d, t, g, c);
+    wx[s] = r.x;
+    wy[s] = r.y;
+    wz[s] = r.z;
+  });
   __syncthreads();
   const ParticleArrays a = d.pa[0];
   const float lo = (float)(cutsq * (1.0 - 2e-5)), hi = (float)(cutsq * (1.0 + 2e-5));
-  const float mid = (float)cutsq, hw = (float)(cutsq * 3e-5);
-  const unsigned long long mid2 = f2_bcast(mid);
-  const size_t gcap = d.brick.gcap;
-  const int K = d.brick.Kb, KB = K >> 3;
+  const size_t cap = d.cap;
+  const int K = GOUT ? d.K : d.brick.Kb, KB = K >> 3;
+  const uint16_t sentinel = (uint16_t)(wmax - 1);
   uint16_t* __restrict__ nl = d.brick.nl;
-  uint16_t* srow = stg[threadIdx.x];
-  constexpr int P = G / 2;  // packed member pairs
-  int mymax = 0;            // largest list of this thread's groups
-  for (int q = threadIdx.x; q < t.ngroups; q += blockDim.x) {
-    const Group gr = brick_group<G>(t, q);
-    unsigned long long X[P], Y[P], Z[P];
-    int mw[G];
-    int64_t mid_[G];
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-      float4 c0 = make_float4(1e18f, 1e18f, 1e18f, 0.f), c1 = c0;
-      if (2 * p < gr.nm) c0 = win[gr.w0 + 2 * p];
-      if (2 * p + 1 < gr.nm) c1 = win[gr.w0 + 2 * p + 1];
-      X[p] = f2_pack(c0.x, c1.x);
-      Y[p] = f2_pack(c0.y, c1.y);
-      Z[p] = f2_pack(c0.z, c1.z);
-    }
-#pragma unroll
-    for (int m = 0; m < G; ++m) {
-      mw[m] = m < gr.nm ? gr.w0 + m : -1;
-      mid_[m] = (EXCL && m < gr.nm) ? a.id[gr.i0 + m] : -3;
-    }
-    const int gx = t.o[0] + gr.rx, gy = t.o[1] + gr.ry, gz = t.o[2] + gr.rz;
+  int32_t* __restrict__ gnl = d.nl;
+  uint32_t* srow = stg[threadIdx.x];
+  uint16_t* srow16 = reinterpret_cast<uint16_t*>(srow);
+  int mymax = 0;
+  for (int q = threadIdx.x; q < t.npart; q += blockDim.x) {
+    const Member me = brick_member(t, q);
+    const float xs = wx[me.w], ys = wy[me.w], zs = wz[me.w];
+    const unsigned long long xi2 = f2_pack(xs, xs), yi2 = f2_pack(ys, ys);
+    const unsigned long long zi2 = f2_pack(zs, zs);
+    const int64_t idi = EXCL ? a.id[me.i] : -3;
+    const int gx = t.o[0] + me.rx, gy = t.o[1] + me.ry, gz = t.o[2] + me.rz;
     int pend = 0, blk = 0, total = 0;
     for (int rr = 0; rr < 9; ++rr) {
       const int oz = rr / 3 - 1, oy = rr % 3 - 1;
-      const int c0 = gr.rx + t.w[0] * ((gr.ry + 1 + oy) + t.w[1] * (gr.rz + 1 + oz));
-      const int t0 = t.winStart[c0], t1 = t.winStart[c0 + 1], t2 = t.winStart[c0 + 2];
-      const int t3 = t.winStart[c0 + 3];
-      for (int tt = t0; tt < t3; ++tt) {
-        const float4 c = win[tt];
-        const unsigned long long cx = f2_bcast(c.x), cy = f2_bcast(c.y), cz = f2_bcast(c.z);
-        unsigned mask = 0;
-        bool band = false;
-        float r2v[G];
+      // window cells of this stencil row: x-offsets -1, 0, +1 of the particle's cell
+      const int c0 = me.rx + t.w[0] * ((me.ry + 1 + oy) + t.w[1] * (me.rz + 1 + oz));
+      const int t0 = t.winStart[c0], t3 = t.winStart[c0 + 3];
+      for (int tt = t0; tt < t3; tt += 4) {
+        // four candidates: two packed pairs per coordinate straight from shared memory
+        const ulonglong2 cx = *reinterpret_cast<const ulonglong2*>(wx + tt);
+        const ulonglong2 cy = *reinterpret_cast<const ulonglong2*>(wy + tt);
+        const ulonglong2 cz = *reinterpret_cast<const ulonglong2*>(wz + tt);
+        const unsigned long long dx0 = f2_sub(xi2, cx.x), dy0 = f2_sub(yi2, cy.x);
+        const unsigned long long dz0 = f2_sub(zi2, cz.x);
+        const unsigned long long dx1 = f2_sub(xi2, cx.y), dy1 = f2_sub(yi2, cy.y);
+        const unsigned long long dz1 = f2_sub(zi2, cz.y);
+        const unsigned long long r01 = f2_fma(dz0, dz0, f2_fma(dy0, dy0, f2_mul(dx0, dx0)));
+        const unsigned long long r23 = f2_fma(dz1, dz1, f2_fma(dy1, dy1, f2_mul(dx1, dx1)));
+        const float r2v[4] = {f2_lo(r01), f2_hi(r01), f2_lo(r23), f2_hi(r23)};
+        if (!((r2v[0] <= hi) | (r2v[1] <= hi) | (r2v[2] <= hi) | (r2v[3] <= hi))) continue;
+        // at least one candidate within the cutoff or its borderline band
+        const int t1 = t.winStart[c0 + 1], t2 = t.winStart[c0 + 2];
 #pragma unroll
-        for (int p = 0; p < P; ++p) {
-          const unsigned long long dx = f2_sub(X[p], cx), dy = f2_sub(Y[p], cy);
-          const unsigned long long dz = f2_sub(Z[p], cz);
-          const unsigned long long r2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
-          const unsigned long long tb = f2_sub(r2, mid2);
-          band |= (fabsf(f2_lo(tb)) <= hw) | (fabsf(f2_hi(tb)) <= hw);
-          r2v[2 * p] = f2_lo(r2);
-          r2v[2 * p + 1] = f2_hi(r2);
-          mask |= ((r2v[2 * p] < lo && tt != mw[2 * p]) ? 1u : 0u) << (2 * p);
-          mask |= ((r2v[2 * p + 1] < lo && tt != mw[2 * p + 1]) ? 1u : 0u) << (2 * p + 1);
-        }
-        if (__builtin_expect(band, 0)) {
-          // candidates near the cutoff: the reference's FP64 test decides
-          const int ox = tt < t1 ? -1 : (tt < t2 ? 0 : 1);
-          const int wcj = c0 + ox + 1;
-          const int j = t.winGlob[wcj] + (tt - t.winStart[wcj]);
-          const int nx = gx + ox, ny = gy + oy, nz = gz + oz;
-          const double sx = (nx < 0 ? -1 : (nx >= d.nc[0] ? 1 : 0)) * d.L[0];
-          const double sy = (ny < 0 ? -1 : (ny >= d.nc[1] ? 1 : 0)) * d.L[1];
-          const double sz = (nz < 0 ? -1 : (nz >= d.nc[2] ? 1 : 0)) * d.L[2];
-          const bool fwd = oz > 0 || (oz == 0 && (oy > 0 || (oy == 0 && ox > 0)));
-#pragma unroll
-          for (int m = 0; m < G; ++m) {
-            if (m >= gr.nm || tt == mw[m] || !(r2v[m] >= lo && r2v[m] <= hi)) continue;
-            const bool in = exact_pair_test(a.x, d.cap, gr.i0 + m, j, fwd, sx, sy, sz, cutsq);
-            mask = in ? (mask | (1u << m)) : (mask & ~(1u << m));
+        for (int h = 0; h < 4; ++h) {
+          const int th = tt + h;
+          const float rh = r2v[h];
+          if (!(rh <= hi) || th == me.w) continue;
+          bool in = rh < lo;
+          int j = -1;
+          if (!in || EXCL || GOUT) {
+            const int ox = th < t1 ? -1 : (th < t2 ? 0 : 1);
+            const int wcj = c0 + ox + 1;
+            j = t.winGlob[wcj] + (th - t.winStart[wcj]);
+            if (!in) {
+              // near the cutoff: the reference's FP64 test decides (spare slots lie far)
+              const int nx = gx + ox, ny = gy + oy, nz = gz + oz;
+              const double sx = (nx < 0 ? -1 : (nx >= d.nc[0] ? 1 : 0)) * d.L[0];
+              const double sy = (ny < 0 ? -1 : (ny >= d.nc[1] ? 1 : 0)) * d.L[1];
+              const double sz = (nz < 0 ? -1 : (nz >= d.nc[2] ? 1 : 0)) * d.L[2];
+              const bool fwd = oz > 0 || (oz == 0 && (oy > 0 || (oy == 0 && ox > 0)));
+              in = exact_pair_test(a.x, cap, me.i, j, fwd, sx, sy, sz, cutsq);
+            }
           }
-        }
-        if (EXCL && mask) {
-          const int wcj = c0 + (tt < t1 ? 0 : (tt < t2 ? 1 : 2));
-          const int64_t idj = a.id[t.winGlob[wcj] + (tt - t.winStart[wcj])];
-#pragma unroll
-          for (int m = 0; m < G; ++m)
-            if (((mask >> m) & 1u) && is_excluded(d, mid_[m], idj)) mask &= ~(1u << m);
-        }
-        if (mask) {
-          srow[pend++] = (uint16_t)((unsigned)tt | (mask << B::kIdx));
-          ++total;
+          if (EXCL && in && is_excluded(d, idi, a.id[j])) in = false;
+          if (!in) continue;
+          if (GOUT)
+            srow[pend++] = (uint32_t)j;
+          else
+            srow16[pend++] = (uint16_t)th;
           if (pend == 8) {
-            if (blk < KB)
-              *reinterpret_cast<uint4*>(nl + ((size_t)blk * gcap + gr.g) * 8) =
-                  *reinterpret_cast<const uint4*>(srow);
+            if (blk < KB) {
+              if (GOUT) {
+                uint4* dst = reinterpret_cast<uint4*>(gnl + nl_index(8 * blk, me.i, cap));
+                dst[0] = *reinterpret_cast<const uint4*>(srow);
+                dst[1] = *reinterpret_cast<const uint4*>(srow + 4);
+              } else {
+                *reinterpret_cast<uint4*>(nl + ((size_t)blk * cap + me.i) * 8) =
+                    *reinterpret_cast<const uint4*>(srow);
+              }
+            }
             ++blk;
+            total += 8;
             pend = 0;
           }
         }
       }
     }
-    if (pend > 0) {  // pad the last block with entries that name no member
-      for (int k = pend; k < 8; ++k) srow[k] = 0;
-      if (blk < KB)
-        *reinterpret_cast<uint4*>(nl + ((size_t)blk * gcap + gr.g) * 8) =
+    total += pend;
+    if (pend > 0 && blk < KB) {
+      // pad the last block: the particle itself (global form, r^2 = 0, masked by the
+      // force kernels) or the sentinel slot
+      if (GOUT) {
+        for (int k = pend; k < 8; ++k) srow[k] = (uint32_t)me.i;
+        uint4* dst = reinterpret_cast<uint4*>(gnl + nl_index(8 * blk, me.i, cap));
+        dst[0] = *reinterpret_cast<const uint4*>(srow);
+        dst[1] = *reinterpret_cast<const uint4*>(srow + 4);
+      } else {
+        for (int k = pend; k < 8; ++k) srow16[k] = sentinel;
+        *reinterpret_cast<uint4*>(nl + ((size_t)blk * cap + me.i) * 8) =
             *reinterpret_cast<const uint4*>(srow);
+      }
     }
     if (total > K) atomicOr(d.err, kErrNlOverflow);
-    d.brick.nnG[gr.g] = min(total, K);
+    d.nn[me.i] = min(total, K);
     mymax = max(mymax, total);
   }
   // high-water mark of the list lengths: one atomic per block
@@ -471,255 +438,256 @@ __device__ __forceinline__ void fene_fp64(const DevView& d, const FENEParams& fp
   }
 }
 
-// Mixed precision: per entry one shared-memory load of the candidate, the members'
-// distances two at a time (f32x2), r^2 replaced by +inf for members the entry does not
-// name or beyond the cutoff (1/inf = 0: no force, no special case).
-template <int G, bool SINGLE, bool CAPPED, bool FENE>
+// 16-byte list block b of particle i (8 entries), read without L1 allocation
+__device__ __forceinline__ uint4 ld_block(const uint16_t* nl, size_t cap, int i, int b) {
+  const int4 v = ld_list(reinterpret_cast<const int4*>(nl) + ((size_t)b * cap + (size_t)i));
+  return make_uint4((unsigned)v.x, (unsigned)v.y, (unsigned)v.z, (unsigned)v.w);
+}
+
+__device__ __forceinline__ unsigned word_of(const uint4& v, int k) {
+  return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
+}
+
+// Mixed precision: the list entries two at a time (one 32-bit word), the pair of
+// candidates in packed f32x2 registers; r^2 beyond the cutoff becomes +inf (1/inf = 0:
+// no force, no special case).  The two halves sum even and odd entries in list order
+// and are added at the end: a fixed order, so the result is reproducible.
+// PACK: two list entries at a time in packed f32x2 arithmetic, the halves summing even
+// and odd entries; otherwise scalar FP32 in list order.
+template <bool SINGLE, bool CAPPED, bool FENE, bool PACK>
 __global__ void __launch_bounds__(kBrickThreads) k_force_brick_mixed(DevView d, FENEParams fp) {
   extern __shared__ __align__(16) float4 win[];
   __shared__ BrickTables t;
   __shared__ LJPairF sP[kMaxTypes * kMaxTypes];
-  using B = BrickBits<G>;
-  constexpr int P = G / 2;
   if (!SINGLE)
     for (int k = threadIdx.x; k < d.ntypes * d.ntypes; k += blockDim.x) sP[k] = d.ljf[k];
   brick_tables(d, t, blockIdx.x);
-  if (t.nwin > d.brick.wmax || t.nwin > B::kMaxWindow) {
+  if (!window_fits(d, t)) {
     if (threadIdx.x == 0) atomicOr(d.err, kErrWindow);
     return;
   }
-  stage_window_f32(d, t, win);
+  for_window(t, [&](int s, int g, int c) { win[s] = f32_frame(d, t, g, c); });
+  if (threadIdx.x == 0) win[d.brick.wmax - 1] = make_float4(kFar, kFar, kFar, __int_as_float(0));
   __syncthreads();
   const LJPairF P0 = d.ljf[0];
   const float inf = __int_as_float(0x7f800000);
-  const size_t gcap = d.brick.gcap;
+  const size_t cap = d.cap;
   const uint16_t* __restrict__ nl = d.brick.nl;
   const int ntypes = d.ntypes;
-  for (int q = threadIdx.x; q < t.ngroups; q += blockDim.x) {
-    const Group gr = brick_group<G>(t, q);
-    unsigned long long X[P], Y[P], Z[P], FX[P], FY[P], FZ[P];
-    int ti[G];
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-      float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f), c1 = c0;
-      if (2 * p < gr.nm) c0 = win[gr.w0 + 2 * p];
-      if (2 * p + 1 < gr.nm) c1 = win[gr.w0 + 2 * p + 1];
-      X[p] = f2_pack(c0.x, c1.x);
-      Y[p] = f2_pack(c0.y, c1.y);
-      Z[p] = f2_pack(c0.z, c1.z);
-      FX[p] = FY[p] = FZ[p] = 0ull;
-      ti[2 * p] = __float_as_int(c0.w);
-      ti[2 * p + 1] = __float_as_int(c1.w);
-    }
-    const int cnt = d.brick.nnG[gr.g];
-    const int nblk = (cnt + 7) >> 3;
+  const unsigned long long ff1 = f2_pack(P0.ff1, P0.ff1), mff2 = f2_pack(-P0.ff2, -P0.ff2);
+  for (int q = threadIdx.x; q < t.npart; q += blockDim.x) {
+    const Member me = brick_member(t, q);
+    const float4 ci = win[me.w];
+    const int ti = __float_as_int(ci.w);
+    const unsigned long long xi2 = f2_pack(ci.x, ci.x), yi2 = f2_pack(ci.y, ci.y);
+    const unsigned long long zi2 = f2_pack(ci.z, ci.z);
+    unsigned long long FX = 0ull, FY = 0ull, FZ = 0ull;
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    const int nblk = (d.nn[me.i] + 7) >> 3;
     uint4 blk = make_uint4(0, 0, 0, 0);
-    if (nblk > 0) blk = ld_block(nl, gcap, gr.g, 0);
+    if (nblk > 0) blk = ld_block(nl, cap, me.i, 0);
     for (int b = 0; b < nblk; ++b) {
       const uint4 cur = blk;
-      if (b + 1 < nblk) blk = ld_block(nl, gcap, gr.g, b + 1);
+      if (b + 1 < nblk) blk = ld_block(nl, cap, me.i, b + 1);
+      if (!PACK) {
 #pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        const unsigned ent = entry_of(cur, e);
-        const float4 c = win[ent & B::kIdxMask];
-        const unsigned bits = ent >> B::kIdx;
-        const unsigned long long cx = f2_bcast(c.x), cy = f2_bcast(c.y), cz = f2_bcast(c.z);
-#pragma unroll
-        for (int p = 0; p < P; ++p) {
-          const unsigned long long dx = f2_sub(X[p], cx), dy = f2_sub(Y[p], cy);
-          const unsigned long long dz = f2_sub(Z[p], cz);
-          const unsigned long long r2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
-          float ra = f2_lo(r2), rb = f2_hi(r2);
-          LJPairF Pa = P0, Pb = P0;
-          if (!SINGLE) {
-            const int tj = __float_as_int(c.w);
-            Pa = sP[ti[2 * p] * ntypes + tj];
-            Pb = sP[ti[2 * p + 1] * ntypes + tj];
-          }
-          const bool va = ((bits >> (2 * p)) & 1u) && ra <= Pa.rcsq;
-          const bool vb = ((bits >> (2 * p + 1)) & 1u) && rb <= Pb.rcsq;
-          float capa = 0.f, capb = 0.f;
-          if (CAPPED) {
-            capa = (va && ra <= Pa.capsq) ? Pa.capff * rsqrtf(ra) : 0.f;
-            capb = (vb && rb <= Pb.capsq) ? Pb.capff * rsqrtf(rb) : 0.f;
-          }
-          ra = va ? ra : inf;
-          rb = vb ? rb : inf;
-          const unsigned long long ri2 = f2_pack(fast_rcp(ra), fast_rcp(rb));
-          const unsigned long long ri6 = f2_mul(f2_mul(ri2, ri2), ri2);
-          unsigned long long ff;
-          if (SINGLE) {
-            ff = f2_mul(f2_mul(ri6, f2_fma(f2_bcast(P0.ff1), ri6, f2_bcast(-P0.ff2))), ri2);
-          } else {
-            ff = f2_mul(f2_mul(ri6, f2_fma(f2_pack(Pa.ff1, Pb.ff1), ri6,
-                                           f2_pack(-Pa.ff2, -Pb.ff2))), ri2);
-          }
-          if (CAPPED) {
-            const float fa = (va && ra <= Pa.capsq) ? capa : f2_lo(ff);
-            const float fb = (vb && rb <= Pb.capsq) ? capb : f2_hi(ff);
-            ff = f2_pack(fa, fb);
-          }
-          FX[p] = f2_fma(dx, ff, FX[p]);
-          FY[p] = f2_fma(dy, ff, FY[p]);
-          FZ[p] = f2_fma(dz, ff, FZ[p]);
+        for (int e = 0; e < 8; ++e) {
+          const unsigned wd = word_of(cur, e >> 1);
+          const float4 c = win[(e & 1) ? (wd >> 16) : (wd & 0xFFFFu)];
+          const float dx = ci.x - c.x, dy = ci.y - c.y, dz = ci.z - c.z;
+          float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+          const LJPairF P = SINGLE ? P0 : sP[ti * ntypes + __float_as_int(c.w)];
+          const bool isc = CAPPED && r2 <= P.capsq;
+          const float capf = CAPPED ? P.capff * rsqrtf(r2) : 0.f;
+          r2 = r2 <= P.rcsq ? r2 : inf;
+          const float ri2 = fast_rcp(r2);
+          const float ri6 = ri2 * ri2 * ri2;
+          float ff = ri6 * fmaf(P.ff1, ri6, -P.ff2) * ri2;
+          if (CAPPED && isc) ff = capf;
+          sx = fmaf(dx, ff, sx);
+          sy = fmaf(dy, ff, sy);
+          sz = fmaf(dz, ff, sz);
         }
+      } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const unsigned wd = word_of(cur, k);
+        const float4 ca = win[wd & 0xFFFFu], cb = win[wd >> 16];
+        const unsigned long long dx = f2_sub(xi2, f2_pack(ca.x, cb.x));
+        const unsigned long long dy = f2_sub(yi2, f2_pack(ca.y, cb.y));
+        const unsigned long long dz = f2_sub(zi2, f2_pack(ca.z, cb.z));
+        const unsigned long long r2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
+        float ra = f2_lo(r2), rb = f2_hi(r2);
+        LJPairF Pa = P0, Pb = P0;
+        if (!SINGLE) {
+          Pa = sP[ti * ntypes + __float_as_int(ca.w)];
+          Pb = sP[ti * ntypes + __float_as_int(cb.w)];
+        }
+        float capa = 0.f, capb = 0.f;
+        bool isca = false, iscb = false;
+        if (CAPPED) {
+          isca = ra <= Pa.capsq;
+          iscb = rb <= Pb.capsq;
+          capa = Pa.capff * rsqrtf(ra);
+          capb = Pb.capff * rsqrtf(rb);
+        }
+        ra = ra <= Pa.rcsq ? ra : inf;
+        rb = rb <= Pb.rcsq ? rb : inf;
+        const unsigned long long ri2 = f2_pack(fast_rcp(ra), fast_rcp(rb));
+        const unsigned long long ri6 = f2_mul(f2_mul(ri2, ri2), ri2);
+        unsigned long long ff;
+        if (SINGLE)
+          ff = f2_mul(f2_mul(ri6, f2_fma(ff1, ri6, mff2)), ri2);
+        else
+          ff = f2_mul(f2_mul(ri6, f2_fma(f2_pack(Pa.ff1, Pb.ff1), ri6, f2_pack(-Pa.ff2, -Pb.ff2))),
+                      ri2);
+        if (CAPPED) {
+          // capped pairs lie inside the cutoff, so ra and rb kept their value there
+          ff = f2_pack(isca ? capa : f2_lo(ff), iscb ? capb : f2_hi(ff));
+        }
+        FX = f2_fma(dx, ff, FX);
+        FY = f2_fma(dy, ff, FY);
+        FZ = f2_fma(dz, ff, FZ);
+      }
       }
     }
-#pragma unroll
-    for (int m = 0; m < G; ++m) {
-      if (m >= gr.nm) break;
-      const int p = m >> 1;
-      const float fx = (m & 1) ? f2_hi(FX[p]) : f2_lo(FX[p]);
-      const float fy = (m & 1) ? f2_hi(FY[p]) : f2_lo(FY[p]);
-      const float fz = (m & 1) ? f2_hi(FZ[p]) : f2_lo(FZ[p]);
-      long long Fx = to_fix(fx, d.err), Fy = to_fix(fy, d.err), Fz = to_fix(fz, d.err);
-      const int i = gr.i0 + m;
-      if (FENE) fene_mixed(d, fp, i, Fx, Fy, Fz);
-      d.ffix[i] = Fx;
-      d.ffix[(size_t)d.cap + i] = Fy;
-      d.ffix[2 * (size_t)d.cap + i] = Fz;
-    }
+    const float fx = PACK ? f2_lo(FX) + f2_hi(FX) : sx;
+    const float fy = PACK ? f2_lo(FY) + f2_hi(FY) : sy;
+    const float fz = PACK ? f2_lo(FZ) + f2_hi(FZ) : sz;
+    long long Fx = to_fix(fx, d.err), Fy = to_fix(fy, d.err), Fz = to_fix(fz, d.err);
+    if (FENE) fene_mixed(d, fp, me.i, Fx, Fy, Fz);
+    d.ffix[me.i] = Fx;
+    d.ffix[cap + me.i] = Fy;
+    d.ffix[2 * cap + me.i] = Fz;
   }
 }
 
+// FP64 frame coordinates from the FP64 positions: the position minus the window cell's
+// shift (its centre less its frame position).
+__device__ __forceinline__ double4 f64_frame(const DevView& d, const BrickTables& t, int g, int c) {
+  if (g < 0) return make_double4(kFar, kFar, kFar, 0.0);
+  const ParticleArrays a = d.pa[0];
+  const size_t cap = d.cap;
+  return make_double4(a.x[g] - t.shift[c][0], a.x[cap + g] - t.shift[c][1],
+                      a.x[2 * cap + g] - t.shift[c][2], (double)a.type[g]);
+}
+
 // Plain FP64 form: the same lists and frame, LennardJones.hpp:137-143 in FP64.
-template <int G, bool SINGLE, bool CAPPED, bool FENE>
+template <bool SINGLE, bool CAPPED, bool FENE>
 __global__ void __launch_bounds__(kBrickThreads) k_force_brick_fp64(DevView d, FENEParams fp) {
   extern __shared__ __align__(16) double4 win64[];
   __shared__ BrickTables t;
-  using B = BrickBits<G>;
   brick_tables(d, t, blockIdx.x);
-  if (t.nwin > d.brick.wmax || t.nwin > B::kMaxWindow) {
+  if (!window_fits(d, t)) {
     if (threadIdx.x == 0) atomicOr(d.err, kErrWindow);
     return;
   }
-  stage_window_f64(d, t, win64, nullptr);
+  for_window(t, [&](int s, int g, int c) { win64[s] = f64_frame(d, t, g, c); });
+  if (threadIdx.x == 0) win64[d.brick.wmax - 1] = make_double4(kFar, kFar, kFar, 0.0);
   __syncthreads();
-  const size_t gcap = d.brick.gcap;
+  const size_t cap = d.cap;
   const uint16_t* __restrict__ nl = d.brick.nl;
   const int ntypes = d.ntypes;
-  for (int q = threadIdx.x; q < t.ngroups; q += blockDim.x) {
-    const Group gr = brick_group<G>(t, q);
-    double xm[G], ym[G], zm[G], fx[G], fy[G], fz[G];
-    int ti[G];
-#pragma unroll
-    for (int m = 0; m < G; ++m) {
-      double4 c = make_double4(0, 0, 0, 0);
-      if (m < gr.nm) c = win64[gr.w0 + m];
-      xm[m] = c.x;
-      ym[m] = c.y;
-      zm[m] = c.z;
-      ti[m] = (int)c.w;
-      fx[m] = fy[m] = fz[m] = 0.0;
-    }
-    const int cnt = d.brick.nnG[gr.g];
+  for (int q = threadIdx.x; q < t.npart; q += blockDim.x) {
+    const Member me = brick_member(t, q);
+    const double4 ci = win64[me.w];
+    const int ti = (int)ci.w;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    const int cnt = d.nn[me.i];
     const int nblk = (cnt + 7) >> 3;
     for (int b = 0; b < nblk; ++b) {
-      const uint4 cur = ld_block(nl, gcap, gr.g, b);
+      const uint4 cur = ld_block(nl, cap, me.i, b);
 #pragma unroll
       for (int e = 0; e < 8; ++e) {
-        const unsigned ent = entry_of(cur, e);
-        const unsigned bits = ent >> B::kIdx;
-        if (!bits) continue;
-        const double4 c = win64[ent & B::kIdxMask];
-#pragma unroll
-        for (int m = 0; m < G; ++m) {
-          if (!((bits >> m) & 1u)) continue;
-          const double dx = xm[m] - c.x, dy = ym[m] - c.y, dz = zm[m] - c.z;
-          const double r2 = dx * dx + dy * dy + dz * dz;
-          const LJPair& P = SINGLE ? d.lj[0] : d.lj[ti[m] * ntypes + (int)c.w];
-          if (!P.set || r2 > P.rcsq) continue;
-          double ff;
-          if (CAPPED && P.caprad > 0 && !(r2 > P.caprad * P.caprad)) {
-            ff = P.capff / sqrt(r2);
-          } else {
-            const double ri2 = 1.0 / r2;
-            const double ri6 = ri2 * ri2 * ri2;
-            ff = ri6 * (P.ff1 * ri6 - P.ff2) * ri2;
-          }
-          fx[m] += dx * ff;
-          fy[m] += dy * ff;
-          fz[m] += dz * ff;
+        if (b * 8 + e >= cnt) break;
+        const unsigned wd = word_of(cur, e >> 1);
+        const double4 c = win64[(e & 1) ? (wd >> 16) : (wd & 0xFFFFu)];
+        const double dx = ci.x - c.x, dy = ci.y - c.y, dz = ci.z - c.z;
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        const LJPair& P = SINGLE ? d.lj[0] : d.lj[ti * ntypes + (int)c.w];
+        if (!P.set || r2 > P.rcsq) continue;
+        double ff;
+        if (CAPPED && P.caprad > 0 && !(r2 > P.caprad * P.caprad)) {
+          ff = P.capff / sqrt(r2);
+        } else {
+          const double ri2 = 1.0 / r2;
+          const double ri6 = ri2 * ri2 * ri2;
+          ff = ri6 * (P.ff1 * ri6 - P.ff2) * ri2;
         }
+        fx += dx * ff;
+        fy += dy * ff;
+        fz += dz * ff;
       }
     }
-#pragma unroll
-    for (int m = 0; m < G; ++m) {
-      if (m >= gr.nm) break;
-      const int i = gr.i0 + m;
-      if (FENE) fene_fp64(d, fp, i, fx[m], fy[m], fz[m]);
-      d.f64[i] = fx[m];
-      d.f64[(size_t)d.cap + i] = fy[m];
-      d.f64[2 * (size_t)d.cap + i] = fz[m];
-    }
+    if (FENE) fene_fp64(d, fp, me.i, fx, fy, fz);
+    d.f64[me.i] = fx;
+    d.f64[cap + me.i] = fy;
+    d.f64[2 * cap + me.i] = fz;
   }
 }
 
 // ---- observables ------------------------------------------------------------------------
 
 // LJ energy (energy = 1) or virial and its tensor (energy = 0) over each listed pair
-// once (sorted index of the candidate above the member's), FP64, as k_lj_obs.
-template <int G>
+// once (sorted index of the candidate above the particle's), FP64, as k_lj_obs.
 __global__ void __launch_bounds__(kBrickThreads) k_lj_obs_brick(DevView d, int energy,
                                                                 double* partials) {
   extern __shared__ __align__(16) double4 win64[];
   __shared__ BrickTables t;
-  using B = BrickBits<G>;
   brick_tables(d, t, blockIdx.x);
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  const bool fits = t.nwin <= d.brick.wmax && t.nwin <= B::kMaxWindow;
+  const bool fits = window_fits(d, t);
   if (!fits && threadIdx.x == 0) atomicOr(d.err, kErrWindow);
   int* wglob = reinterpret_cast<int*>(win64 + d.brick.wmax);
-  if (fits) stage_window_f64(d, t, win64, wglob);
+  if (fits)
+    for_window(t, [&](int s, int g, int c) {
+      win64[s] = f64_frame(d, t, g, c);
+      wglob[s] = g;
+    });
   __syncthreads();
   if (fits) {
-    const size_t gcap = d.brick.gcap;
+    const size_t cap = d.cap;
     const uint16_t* __restrict__ nl = d.brick.nl;
-    for (int q = threadIdx.x; q < t.ngroups; q += blockDim.x) {
-      const Group gr = brick_group<G>(t, q);
-      const int cnt = d.brick.nnG[gr.g];
+    for (int q = threadIdx.x; q < t.npart; q += blockDim.x) {
+      const Member me = brick_member(t, q);
+      const double4 ci = win64[me.w];
+      const int cnt = d.nn[me.i];
       for (int b = 0; b < ((cnt + 7) >> 3); ++b) {
-        const uint4 cur = ld_block(nl, gcap, gr.g, b);
-        for (int e = 0; e < 8; ++e) {
-          const unsigned ent = entry_of(cur, e);
-          const unsigned bits = ent >> B::kIdx;
-          if (!bits) continue;
-          const int w = ent & B::kIdxMask;
+        const uint4 cur = ld_block(nl, cap, me.i, b);
+        for (int e = 0; e < 8 && b * 8 + e < cnt; ++e) {
+          const unsigned wd = word_of(cur, e >> 1);
+          const int w = (e & 1) ? (wd >> 16) : (wd & 0xFFFFu);
+          if (wglob[w] < me.i) continue;
           const double4 c = win64[w];
-          const int j = wglob[w];
-          for (int m = 0; m < gr.nm; ++m) {
-            if (!((bits >> m) & 1u) || j < gr.i0 + m) continue;
-            const double4 cm = win64[gr.w0 + m];
-            const double dx = cm.x - c.x, dy = cm.y - c.y, dz = cm.z - c.z;
-            const double r2 =
-                __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-            const LJPair& P = d.lj[(int)cm.w * d.ntypes + (int)c.w];
-            if (!P.set || r2 > P.rcsq) continue;
-            if (energy) {
-              double ds = r2;
-              if (P.caprad > 0 && !(ds > P.caprad * P.caprad)) ds = P.caprad * P.caprad;
-              const double frac2 = __ddiv_rn(P.ef2, ds);
-              const double frac6 = __dmul_rn(__dmul_rn(frac2, frac2), frac2);
-              acc[0] += __dsub_rn(__dmul_rn(P.ef1, __dsub_rn(__dmul_rn(frac6, frac6), frac6)),
-                                  P.shift);
+          const double dx = ci.x - c.x, dy = ci.y - c.y, dz = ci.z - c.z;
+          const double r2 =
+              __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+          const LJPair& P = d.lj[(int)ci.w * d.ntypes + (int)c.w];
+          if (!P.set || r2 > P.rcsq) continue;
+          if (energy) {
+            double ds = r2;
+            if (P.caprad > 0 && !(ds > P.caprad * P.caprad)) ds = P.caprad * P.caprad;
+            const double frac2 = __ddiv_rn(P.ef2, ds);
+            const double frac6 = __dmul_rn(__dmul_rn(frac2, frac2), frac2);
+            acc[0] += __dsub_rn(__dmul_rn(P.ef1, __dsub_rn(__dmul_rn(frac6, frac6), frac6)),
+                                P.shift);
+          } else {
+            double ff;
+            if (P.caprad > 0 && !(r2 > P.caprad * P.caprad)) {
+              ff = P.capff / sqrt(r2);
             } else {
-              double ff;
-              if (P.caprad > 0 && !(r2 > P.caprad * P.caprad)) {
-                ff = P.capff / sqrt(r2);
-              } else {
-                const double ri2 = 1.0 / r2;
-                const double ri6 = ri2 * ri2 * ri2;
-                ff = ri6 * (P.ff1 * ri6 - P.ff2) * ri2;
-              }
-              const double f0 = dx * ff, f1 = dy * ff, f2 = dz * ff;
-              acc[0] += dx * f0 + dy * f1 + dz * f2;
-              acc[1] += dx * f0;
-              acc[2] += dy * f1;
-              acc[3] += dz * f2;
-              acc[4] += dx * f1;
-              acc[5] += dx * f2;
-              acc[6] += dy * f2;
+              const double ri2 = 1.0 / r2;
+              const double ri6 = ri2 * ri2 * ri2;
+              ff = ri6 * (P.ff1 * ri6 - P.ff2) * ri2;
             }
+            const double f0 = dx * ff, f1 = dy * ff, f2 = dz * ff;
+            acc[0] += dx * f0 + dy * f1 + dz * f2;
+            acc[1] += dx * f0;
+            acc[2] += dy * f1;
+            acc[3] += dz * f2;
+            acc[4] += dx * f1;
+            acc[5] += dx * f2;
+            acc[6] += dy * f2;
           }
         }
       }
@@ -730,60 +698,52 @@ __global__ void __launch_bounds__(kBrickThreads) k_lj_obs_brick(DevView d, int e
 
 // ---- pair export ------------------------------------------------------------------------
 
-// Visits every listed pair once, from the member with the smaller id:
-// op(member sorted index, member id, candidate id).
-template <int G, class Op>
+// Visits every listed pair once, from the particle with the smaller id:
+// op(sorted index, own id, partner id).
+template <class Op>
 __device__ void brick_pairs(const DevView& d, const BrickTables& t, Op&& op) {
-  using B = BrickBits<G>;
   const ParticleArrays a = d.pa[0];
-  const size_t gcap = d.brick.gcap;
-  for (int q = threadIdx.x; q < t.ngroups; q += blockDim.x) {
-    const Group gr = brick_group<G>(t, q);
-    int64_t idm[G];
-    for (int m = 0; m < gr.nm; ++m) idm[m] = a.id[gr.i0 + m];
-    const int cnt = d.brick.nnG[gr.g];
+  const size_t cap = d.cap;
+  for (int q = threadIdx.x; q < t.npart; q += blockDim.x) {
+    const Member me = brick_member(t, q);
+    const int64_t idi = a.id[me.i];
+    const int cnt = d.nn[me.i];
     for (int b = 0; b < ((cnt + 7) >> 3); ++b) {
-      const uint4 cur = ld_block(d.brick.nl, gcap, gr.g, b);
-      for (int e = 0; e < 8; ++e) {
-        const unsigned ent = entry_of(cur, e);
-        const unsigned bits = ent >> B::kIdx;
-        if (!bits) continue;
-        const int64_t idj = a.id[window_glob(t, ent & B::kIdxMask)];
-        for (int m = 0; m < gr.nm; ++m)
-          if (((bits >> m) & 1u) && idj > idm[m]) op(gr.i0 + m, idm[m], idj);
+      const uint4 cur = ld_block(d.brick.nl, cap, me.i, b);
+      for (int e = 0; e < 8 && b * 8 + e < cnt; ++e) {
+        const unsigned wd = word_of(cur, e >> 1);
+        const int w = (e & 1) ? (wd >> 16) : (wd & 0xFFFFu);
+        const int64_t idj = a.id[window_glob(t, w)];
+        if (idj > idi) op(me.i, idi, idj);
       }
     }
   }
 }
 
-template <int G>
 __global__ void __launch_bounds__(kBrickThreads) k_pair_count_brick(DevView d, int32_t* counts) {
   __shared__ BrickTables t;
   brick_tables(d, t, blockIdx.x);
-  // counts of the brick's particles are zeroed by the host; atomics per member
-  brick_pairs<G>(d, t, [&](int i, int64_t, int64_t) { atomicAdd(&counts[i], 1); });
+  brick_pairs(d, t, [&](int i, int64_t, int64_t) { counts[i] += 1; });
 }
 
-template <int G>
 __global__ void __launch_bounds__(kBrickThreads) k_pair_write_brick(DevView d,
                                                                     const int64_t* offsets,
                                                                     int32_t* fill, int64_t* out) {
   __shared__ BrickTables t;
   brick_tables(d, t, blockIdx.x);
-  brick_pairs<G>(d, t, [&](int i, int64_t idi, int64_t idj) {
-    const int64_t o = offsets[i] + atomicAdd(&fill[i], 1);
+  brick_pairs(d, t, [&](int i, int64_t idi, int64_t idj) {
+    const int64_t o = offsets[i] + fill[i]++;
     out[2 * o] = idi;
     out[2 * o + 1] = idj;
   });
 }
 
-template <int G>
 __global__ void __launch_bounds__(kBrickThreads) k_pair_digest_brick(DevView d,
                                                                      unsigned long long* partials) {
   __shared__ BrickTables t;
   brick_tables(d, t, blockIdx.x);
   unsigned long long v[4] = {0ull, 0ull, 0ull, 0ull};
-  brick_pairs<G>(d, t, [&](int, int64_t idi, int64_t idj) {
+  brick_pairs(d, t, [&](int, int64_t idi, int64_t idj) {
     const unsigned long long h =
         digest_mix(digest_mix((unsigned long long)idi) ^ (unsigned long long)idj);
     v[0] += 1ull;
@@ -808,43 +768,85 @@ __global__ void k_digest_reduce_brick(const unsigned long long* partials, int nb
 
 // ---- launchers ----------------------------------------------------------------------------
 
-// Opt in to more than 48 KB of dynamic shared memory.  Not while the stream is being
-// captured: the same launch ran uncaptured before every capture (start-of-run forces,
-// host-side list build), which set the attribute for the same size.
+template <class Kern>
+void allow_smem(Kern k, size_t bytes, cudaStream_t st);
+
+template <bool PACK>
+void forces_brick_mixed(const DevView& d, const FENEParams& fp, cudaStream_t st) {
+  const bool single = d.ljSingle != 0, capped = d.ljCapped != 0, fene = fp.on != 0;
+  const size_t sm = brick_smem_f32(d.brick.wmax);
+#define ESPP_BRICK_MIXED(S, C, F)                                                        \
+  if (single == S && capped == C && fene == F) {                                         \
+    allow_smem(k_force_brick_mixed<S, C, F, PACK>, sm, st);                              \
+    k_force_brick_mixed<S, C, F, PACK><<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, fp); \
+    return;                                                                              \
+  }
+  ESPP_BRICK_MIXED(true, false, false)
+  ESPP_BRICK_MIXED(true, false, true)
+  ESPP_BRICK_MIXED(true, true, false)
+  ESPP_BRICK_MIXED(true, true, true)
+  ESPP_BRICK_MIXED(false, false, false)
+  ESPP_BRICK_MIXED(false, false, true)
+  ESPP_BRICK_MIXED(false, true, false)
+  ESPP_BRICK_MIXED(false, true, true)
+#undef ESPP_BRICK_MIXED
+}
+
+// Opt in, once per kernel and device, to all the dynamic shared memory a block may have
+// beside the kernel's static tables, so that launches of any window size (systems of
+// different densities, captured graphs) stay within the opt-in.  Not while the stream
+// is being captured; every kernel launches uncaptured before its first capture
+// (start-of-run forces, host-side list build).
+// (keyed on the kernel's address: kernels of one signature share a template instance)
 template <class Kern>
 void allow_smem(Kern k, size_t bytes, cudaStream_t st) {
-  if (bytes <= 48 * 1024) return;
+  (void)bytes;
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const std::pair<const void*, int> key((const void*)k, dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count(key)) return;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) return;
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, k) != cudaSuccess) return;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(227 * 1024 - fa.sharedSizeBytes)) == cudaSuccess)
+    done.insert(key);
 }
 
-template <int G>
-void build_brick_g(const DevView& d, double cutsq, cudaStream_t st) {
-  const size_t sm = brick_smem_f32(d.brick.wmax);
-  if (d.exclStart) {
-    allow_smem(k_build_brick<G, true>, sm, st);
-    k_build_brick<G, true><<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, cutsq);
-  } else {
-    allow_smem(k_build_brick<G, false>, sm, st);
-    k_build_brick<G, false><<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, cutsq);
+// packed f32x2 (ESPP_B200_F2=1) or scalar FP32 (default) arithmetic in the brick force
+// kernel; the scalar form measured faster (FFMA2 issues once but occupies the FMA pipe
+// for two cycles, and packing the candidates costs moves)
+bool use_packed() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("ESPP_B200_F2");
+    v = (e && atoi(e) != 0) ? 1 : 0;
   }
+  return v == 1;
 }
 
-template <int G, bool MIXED>
-void forces_brick_g(const DevView& d, const FENEParams& fp, cudaStream_t st) {
+template <bool MIXED>
+void forces_brick(const DevView& d, const FENEParams& fp, cudaStream_t st) {
+  if (MIXED && use_packed()) {
+    forces_brick_mixed<true>(d, fp, st);
+    return;
+  }
   const bool single = d.ljSingle != 0, capped = d.ljCapped != 0, fene = fp.on != 0;
   const size_t sm = MIXED ? brick_smem_f32(d.brick.wmax) : brick_smem_f64(d.brick.wmax);
-#define ESPP_BRICK_CASE(S, C, F)                                                         \
-  if (single == S && capped == C && fene == F) {                                         \
-    if (MIXED) {                                                                         \
-      allow_smem(k_force_brick_mixed<G, S, C, F>, sm, st);                                   \
-      k_force_brick_mixed<G, S, C, F><<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, fp); \
-    } else {                                                                             \
-      allow_smem(k_force_brick_fp64<G, S, C, F>, sm, st);                                    \
-      k_force_brick_fp64<G, S, C, F><<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, fp);  \
-    }                                                                                    \
-    return;                                                                              \
+#define ESPP_BRICK_CASE(S, C, F)                                                       \
+  if (single == S && capped == C && fene == F) {                                       \
+    if (MIXED) {                                                                       \
+      allow_smem(k_force_brick_mixed<S, C, F, false>, sm, st);                         \
+      k_force_brick_mixed<S, C, F, false><<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, fp); \
+    } else {                                                                           \
+      allow_smem(k_force_brick_fp64<S, C, F>, sm, st);                                 \
+      k_force_brick_fp64<S, C, F><<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, fp);  \
+    }                                                                                  \
+    return;                                                                            \
   }
   ESPP_BRICK_CASE(true, false, false)
   ESPP_BRICK_CASE(true, false, true)
@@ -859,72 +861,63 @@ void forces_brick_g(const DevView& d, const FENEParams& fp, cudaStream_t st) {
 
 }  // namespace
 
+// FP32 stage: the force kernel's float4 slots (the build's x | y | z arrays take less)
 size_t brick_smem_f32(int wmax) { return (size_t)wmax * sizeof(float4); }
-// FP64 stage plus the sorted index of each entry (observables)
+// FP64 stage plus the sorted index of each slot (observables)
 size_t brick_smem_f64(int wmax) { return (size_t)wmax * (sizeof(double4) + sizeof(int)); }
 size_t brick_smem_limit() {
   // dynamic shared memory a block may use beside the static tables (227 KB per block)
-  return 227 * 1024 - sizeof(BrickTables) - sizeof(uint16_t) * kBrickThreads * 8 -
+  return 227 * 1024 - sizeof(BrickTables) - sizeof(uint32_t) * kBrickThreads * kStage -
          sizeof(LJPairF) * kMaxTypes * kMaxTypes - 1024;
 }
 
 void launch_build_brick(const DevView& d, double cutsq, cudaStream_t st) {
   if (d.n == 0) return;
-  if (d.brick.G == 4)
-    build_brick_g<4>(d, cutsq, st);
-  else
-    build_brick_g<2>(d, cutsq, st);
+  const size_t sm = (size_t)d.brick.wmax * 3 * sizeof(float);
+  const bool gout = !d.brick.on;
+#define ESPP_BUILD(E, G)                                                          \
+  if (!!d.exclStart == E && gout == G) {                                          \
+    allow_smem(k_build_brick<E, G>, sm, st);                                      \
+    k_build_brick<E, G><<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, cutsq);    \
+    return;                                                                       \
+  }
+  ESPP_BUILD(true, true)
+  ESPP_BUILD(true, false)
+  ESPP_BUILD(false, true)
+  ESPP_BUILD(false, false)
+#undef ESPP_BUILD
 }
 
 void launch_forces_brick(const DevView& d, bool mixed, const FENEParams& fp, cudaStream_t st) {
   if (d.n == 0) return;
-  if (d.brick.G == 4) {
-    mixed ? forces_brick_g<4, true>(d, fp, st) : forces_brick_g<4, false>(d, fp, st);
-  } else {
-    mixed ? forces_brick_g<2, true>(d, fp, st) : forces_brick_g<2, false>(d, fp, st);
-  }
+  mixed ? forces_brick<true>(d, fp, st) : forces_brick<false>(d, fp, st);
 }
 
 void launch_lj_observables_brick(const DevView& d, double* partials, int nblocks, double* out,
                                  int energy, cudaStream_t st) {
-  // partials hold one row of 7 per brick
-  (void)nblocks;
+  (void)nblocks;  // one row of 7 partial sums per brick
   const size_t sm = brick_smem_f64(d.brick.wmax);
-  if (d.brick.G == 4) {
-    allow_smem(k_lj_obs_brick<4>, sm, st);
-    k_lj_obs_brick<4><<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, energy, partials);
-  } else {
-    allow_smem(k_lj_obs_brick<2>, sm, st);
-    k_lj_obs_brick<2><<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, energy, partials);
-  }
+  allow_smem(k_lj_obs_brick, sm, st);
+  k_lj_obs_brick<<<d.brick.nbricks, kBrickThreads, sm, st>>>(d, energy, partials);
   k_sum_partials<7><<<1, 256, 0, st>>>(partials, d.brick.nbricks, out);
 }
 
 void launch_pair_count_brick(const DevView& d, int32_t* counts, cudaStream_t st) {
   if (d.n == 0) return;
   cudaMemsetAsync(counts, 0, sizeof(int32_t) * d.n, st);
-  if (d.brick.G == 4)
-    k_pair_count_brick<4><<<d.brick.nbricks, kBrickThreads, 0, st>>>(d, counts);
-  else
-    k_pair_count_brick<2><<<d.brick.nbricks, kBrickThreads, 0, st>>>(d, counts);
+  k_pair_count_brick<<<d.brick.nbricks, kBrickThreads, 0, st>>>(d, counts);
 }
 
 void launch_pair_write_brick(const DevView& d, const int64_t* offsets, int32_t* fill,
                              int64_t* out, cudaStream_t st) {
   if (d.n == 0) return;
   cudaMemsetAsync(fill, 0, sizeof(int32_t) * d.n, st);
-  if (d.brick.G == 4)
-    k_pair_write_brick<4><<<d.brick.nbricks, kBrickThreads, 0, st>>>(d, offsets, fill, out);
-  else
-    k_pair_write_brick<2><<<d.brick.nbricks, kBrickThreads, 0, st>>>(d, offsets, fill, out);
+  k_pair_write_brick<<<d.brick.nbricks, kBrickThreads, 0, st>>>(d, offsets, fill, out);
 }
 
 void launch_pair_digest_brick(const DevView& d, unsigned long long* partials,
                               unsigned long long* out, cudaStream_t st) {
-  if (d.brick.G == 4)
-    k_pair_digest_brick<4><<<d.brick.nbricks, kBrickThreads, 0, st>>>(d, partials);
-  else
-    k_pair_digest_brick<2><<<d.brick.nbricks, kBrickThreads, 0, st>>>(d, partials);
+  k_pair_digest_brick<<<d.brick.nbricks, kBrickThreads, 0, st>>>(d, partials);
   k_digest_reduce_brick<<<1, kBlock, 0, st>>>(partials, d.brick.nbricks, out);
 }
 

@@ -80,8 +80,12 @@ __device__ __noinline__ bool exact_pair_test(const double* __restrict__ x, size_
 
 // Packed FP32 pairs (sm_100 f32x2 arithmetic): two particles' coordinates in one 64-bit
 // register, low half first.
+// The two halves form one 64-bit register pair (mov.b64 with a vector operand), so
+// packing and unpacking are register moves rather than 64-bit shifts.
 __device__ __forceinline__ unsigned long long f2_pack(float lo, float hi) {
-  return ((unsigned long long)__float_as_uint(hi) << 32) | __float_as_uint(lo);
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
 }
 __device__ __forceinline__ unsigned long long f2_sub(unsigned long long a, unsigned long long b) {
   unsigned long long r;
@@ -100,10 +104,18 @@ __device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsig
   return r;
 }
 
-__device__ __forceinline__ float f2_lo(unsigned long long v) { return __uint_as_float((unsigned)v); }
-__device__ __forceinline__ float f2_hi(unsigned long long v) {
-  return __uint_as_float((unsigned)(v >> 32));
+#pragma nv_diag_suppress 550  // the other half of the unpacked pair is not needed
+__device__ __forceinline__ float f2_lo(unsigned long long v) {
+  float lo, hi;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+  return lo;
 }
+__device__ __forceinline__ float f2_hi(unsigned long long v) {
+  float lo, hi;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+  return hi;
+}
+#pragma nv_diag_default 550
 
 __device__ __forceinline__ long long to_fix(float f, unsigned* err) {
   if (!(fabsf(f) < 1.0e9f)) atomicOr(err, kErrFixOverflow);

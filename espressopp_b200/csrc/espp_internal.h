@@ -125,24 +125,19 @@ struct TabDesc {
 // Brick path of the Verlet build and the pair kernels: the cell grid tiled into bricks
 // of b[0] x b[1] x b[2] cells.  A brick's window (its cells and one layer of cells
 // around them) holds every candidate of every particle of the brick; a kernel block
-// stages it in shared memory once.  Particles of a cell are taken G at a time
-// ("groups", consecutive in the in-cell order); each group keeps one list, the union of
-// its members' Verlet lists, as 16-bit entries: the candidate's window index in the low
-// (16 - G) bits and one bit per member above them.  Lists are stored in blocks of 8
-// entries (16 bytes): block k of group g at entries [(k * gcap + g) * 8, +8).
+// stages it in shared memory once, each window cell padded to an even number of slots.
+// Each particle keeps its Verlet list as 16-bit window indices of its brick, in blocks
+// of 8 entries (16 bytes): block k of particle i at entries [(k * cap + i) * 8, +8),
+// padded with the window's sentinel slot wmax - 1 (a particle far away).
 constexpr int kBrickMax = 4;  // cells per brick edge
 struct BrickView {
   int on;                  // the brick path is in use
-  int G;                   // particles per group (2 or 4)
   int b[3];                // brick extent in cells
   int nb[3];               // bricks per dimension
   int nbricks;
-  int wmax;                // window capacity (entries) of the shared-memory stage
-  uint16_t* nl;            // Kb * gcap entries
-  int32_t* nnG;            // entries per group
-  int32_t* cellGroupStart; // ncells + 1: first group of each cell
-  int gcap;                // group capacity
-  int Kb;                  // entries per group (multiple of 8)
+  int wmax;                // window slots of the shared-memory stage (sentinel included)
+  uint16_t* nl;            // Kb * cap entries
+  int Kb;                  // entries per particle (multiple of 8)
 };
 
 struct DevView {
@@ -269,8 +264,7 @@ void launch_pair_write(const DevView& d, const int64_t* offsets, int64_t* out,
 // order-independent digest of the Verlet pair set: out[0..4) = count, sum, xor, sum2
 void launch_pair_digest(const DevView& d, unsigned long long* partials, int nblocks,
                         unsigned long long* out, cudaStream_t st);
-// brick path (espp_brick.cu; the group layout in espp_kernels.cu)
-void launch_brick_layout(const DevView& d, RebuildScratch& s, cudaStream_t st);
+// brick path (espp_brick.cu)
 void launch_build_brick(const DevView& d, double cutsq, cudaStream_t st);
 void launch_forces_brick(const DevView& d, bool mixed, const FENEParams& fene, cudaStream_t st);
 void launch_lj_observables_brick(const DevView& d, double* partials, int nblocks, double* out,

@@ -1637,23 +1637,6 @@ void launch_sort_cells(const DevView& d, RebuildScratch& s, cudaStream_t st) {
 
 int scan_tiles(int ncells) { return (ncells + kScanTile - 1) / kScanTile; }
 
-// groups of the brick path: ceil(count / G) per cell, then their exclusive scan
-__global__ void k_cell_group_counts(DevView d, int32_t* out) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.ncells) return;
-  const int n = d.cellStart[c + 1] - d.cellStart[c];
-  out[c] = (n + d.brick.G - 1) / d.brick.G;
-}
-
-void launch_brick_layout(const DevView& d, RebuildScratch& s, cudaStream_t st) {
-  const int ntiles = (d.ncells + kScanTile - 1) / kScanTile;
-  k_cell_group_counts<<<blocks_for(d.ncells), kBlock, 0, st>>>(d, s.cellCount);
-  k_scan_tiles<<<ntiles, kScanBlock, 0, st>>>(s.cellCount, d.ncells, s.tileSum);
-  k_scan_tile_sums<<<1, kScanBlock, 0, st>>>(s.tileSum, ntiles);
-  k_scan_apply<<<ntiles, kScanBlock, 0, st>>>(s.cellCount, d.ncells, s.tileSum,
-                                              d.brick.cellGroupStart);
-}
-
 void launch_gather(const DevView& d, const RebuildScratch& s, cudaStream_t st) {
   if (d.n > 0) k_gather<<<blocks_for(d.n), kBlock, 0, st>>>(d, s);
   k_swap_arrays<<<1, 1, 0, st>>>(d.pa);

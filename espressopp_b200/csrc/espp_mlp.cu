@@ -432,6 +432,8 @@ int mlp_grad_blocks(int n) {
 }
 
 void launch_mlp_site_tc(const DevView& d, cudaStream_t st);
+int launch_mlp_grad_tc(const DevView& d, const float* tangent, float* partials, int maxblocks,
+                       cudaStream_t st);
 
 void launch_mlp_energy_terms(const DevView& d, cudaStream_t st) {
   if (d.n == 0) return;
@@ -472,6 +474,12 @@ void launch_mlp_fm_grad(const DevView& d, const float* fmodel, const double* fre
   k_mlp_fm_err<<<nloss_blocks, 256, 0, st>>>(d.n, fmodel, fref, err, loss_partials);
   k_sum_blocks<<<1, 256, 0, st>>>(loss_partials, nloss_blocks, loss_out);
   k_mlp_vpass<<<(d.n + 255) / 256, 256, 0, st>>>(d, err, tangent);
+  if (d.mlp.tc) {
+    // the weight-gradient products on the tensor cores
+    const int nb = launch_mlp_grad_tc(d, tangent, partials, npart_blocks, st);
+    k_mlp_reduce<<<(kMlpParams + 255) / 256, 256, 0, st>>>(partials, nb, grad);
+    return;
+  }
   k_mlp_site_grad<<<npart_blocks, H, 0, st>>>(d.mlp, d.n, tangent, partials);
   k_mlp_reduce<<<(kMlpParams + 255) / 256, 256, 0, st>>>(partials, npart_blocks, grad);
 }
@@ -809,9 +817,375 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_site_tc(MlpDev m, int n, unsign
   }
 }
 
+// ---- force-matching gradient on the tensor cores ---------------------------------------
+// The forward-over-reverse weight gradient of k_mlp_site_grad with every matrix product
+// on tcgen05 (BF16 operands, FP32 accumulators in tensor memory), 128 sites a tile, one
+// CTA of 128 threads per SM looping over tiles; thread t owns site t of the tile (TMEM
+// lane t).  Per tile:
+//   Z1 = X W1^T, Zd1 = Xd W1^T                      (M 128, N 64, K 16)
+//   H1 = silu(Z1 + b1), Hd1 = silu'(.) Zd1
+//   Z2 = H1 W2^T, Zd2 = Hd1 W2^T                    (M 128, N 64, K 64)
+//   az2 = w3 Zd2 silu''(Z2 + b2), azd2 = w3 silu'(Z2 + b2)
+//   AH1 = az2 W2, AHd1 = azd2 W2                    (M 128, N 64, K 64)
+//   D12 += [az2^T; azd2^T] [H1 | Hd1]               (M 128, N 64, K 128 sites)
+//   az1 = AH1 silu'(Z1 + b1) + AHd1 Zd1 silu''(.), azd1 = AHd1 silu'(.)
+//   D34 += [az1^T; azd1^T] [X | Xd]                 (M 128, N 16, K 128 sites)
+// The weight gradients are the upper half of one accumulator plus the lower half of the
+// other: gW2 = D1[0:64] + D2[64:128], gW1 = D3[0:64] + D4[64:128] (the stacked A
+// operand keeps every product at M = 128).  They stay in tensor memory across the
+// CTA's tiles.  Bias and w3 gradients are column sums of FP32 rows in shared memory,
+// in a fixed order.  Each CTA writes one row of partial gradients (k_mlp_reduce).
+constexpr int kGtCols = 512;  // Z1 0, Zd1 64, Z2 / AH1 128, Zd2 / AHd1 192, D1 256,
+                              // D2 320, D3 384, D4 400
+struct GtSmem {
+  alignas(128) uint8_t X[kTcRows * K * 2];       // A of Z1 (site rows)
+  alignas(128) uint8_t Xd[kTcRows * K * 2];
+  alignas(128) uint8_t XT[K * kTcRows * 2];      // B of D3: X^T (16 rows, K = sites)
+  alignas(128) uint8_t XdT[K * kTcRows * 2];
+  alignas(128) uint8_t H1[kTcRows * H * 2];      // A of Z2
+  alignas(128) uint8_t Hd1[kTcRows * H * 2];
+  alignas(128) uint8_t H1T[H * kTcRows * 2];     // B of D1: H1^T (64 rows, K = sites)
+  alignas(128) uint8_t Hd1T[H * kTcRows * 2];
+  alignas(128) uint8_t A2[kTcRows * H * 2];      // A of AH1: az2 (site rows)
+  alignas(128) uint8_t Ad2[kTcRows * H * 2];
+  alignas(128) uint8_t AT[2 * H * kTcRows * 2];  // A of D12 / D34: [a^T; ad^T]
+  alignas(128) uint8_t W1[H * K * 2];            // B of Z1
+  alignas(128) uint8_t W2[H * H * 2];            // B of Z2
+  alignas(128) uint8_t W2T[H * H * 2];           // B of AH1
+  float F[kTcRows][H + 1];                       // FP32 rows for the column sums
+  float b1[H], b2[H], w3[H], scale[K], shift[K];
+  alignas(8) unsigned long long mbar;
+  uint32_t tmem;
+  int abort;
+};
+
+__device__ __forceinline__ void store_bf16(uint8_t* base, int r, int k, int R, float v) {
+  *reinterpret_cast<__nv_bfloat16*>(base + canon_off(r, k, R)) = __float2bfloat16_rn(v);
+}
+
+// writes 16 values of row r into a canonical 128-row operand with K = 16
+__device__ __forceinline__ void store_row16(uint8_t* base, int r, const float* v) {
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    uint4 q;
+    q.x = pack_bf16(v[8 * c + 0], v[8 * c + 1]);
+    q.y = pack_bf16(v[8 * c + 2], v[8 * c + 3]);
+    q.z = pack_bf16(v[8 * c + 4], v[8 * c + 5]);
+    q.w = pack_bf16(v[8 * c + 6], v[8 * c + 7]);
+    *reinterpret_cast<uint4*>(base + canon_off(r, 8 * c, kTcRows)) = q;
+  }
+}
+
+__global__ void __launch_bounds__(kTcRows) k_mlp_grad_tc(MlpDev m, int n, const float* tangent,
+                                                          float* partials, unsigned* err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  GtSmem& S = *reinterpret_cast<GtSmem*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int t = threadIdx.x;
+  const int warp = t >> 5;
+  const float* th = m.theta;
+  for (int e = t; e < H * K; e += kTcRows) {
+    const int o = e / K, k = e % K;  // W1[o][k]
+    store_bf16(S.W1, o, k, H, th[e]);
+  }
+  for (int e = t; e < H * H; e += kTcRows) {
+    const int o = e / H, u = e % H;  // W2[o][u]
+    store_bf16(S.W2, o, u, H, th[kOffW2 + e]);
+    store_bf16(S.W2T, u, o, H, th[kOffW2 + e]);
+  }
+  if (t < H) {
+    S.b1[t] = th[kOffB1 + t];
+    S.b2[t] = th[kOffB2 + t];
+    S.w3[t] = th[kOffW3 + t];
+  }
+  if (t < K) {
+    S.scale[t] = m.scale[t];
+    S.shift[t] = m.shift[t];
+  }
+  const uint32_t mbar = smem_u32(&S.mbar);
+  if (t == 0) {
+    S.abort = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&S.tmem)),
+                 "r"(kGtCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = S.tmem;
+  const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's lanes
+  const uint32_t aX = smem_u32(S.X), aXd = smem_u32(S.Xd), aXT = smem_u32(S.XT),
+                 aXdT = smem_u32(S.XdT), aH1 = smem_u32(S.H1), aHd1 = smem_u32(S.Hd1),
+                 aH1T = smem_u32(S.H1T), aHd1T = smem_u32(S.Hd1T), aA2 = smem_u32(S.A2),
+                 aAd2 = smem_u32(S.Ad2), aAT = smem_u32(S.AT), aW1 = smem_u32(S.W1),
+                 aW2 = smem_u32(S.W2), aW2T = smem_u32(S.W2T);
+  uint32_t phase = 0;
+  auto wait_mma = [&]() {
+    if (!mbar_wait(mbar, phase)) {
+      S.abort = 1;
+      atomicOr(err, kErrTimeout);
+    }
+    phase ^= 1u;
+    tc_fence_after();
+  };
+  // operands written by the threads, visible to the tensor cores; then one thread issues
+  auto sync_for_mma = [&]() {
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+  };
+  // column sums of S.F over the tile's rows (fixed order): thread u < H adds column u
+  auto colsum = [&](float& acc) {
+    __syncthreads();
+    if (t < H) {
+      float c = 0.f;
+      for (int r = 0; r < kTcRows; ++r) c += S.F[r][t];
+      acc += c;
+    }
+    __syncthreads();
+  };
+  float gb1 = 0.f, gb2 = 0.f, gw3 = 0.f;
+  int acc = 0;  // the D accumulators hold earlier tiles
+  for (int s0 = blockIdx.x * kTcRows; s0 < n; s0 += gridDim.x * kTcRows) {
+    const int i = s0 + t;
+    {
+      float x[K], xd[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        x[k] = i < n ? (m.G[(size_t)i * K + k] - S.shift[k]) * S.scale[k] : 0.f;
+        xd[k] = i < n ? tangent[(size_t)i * K + k] : 0.f;
+      }
+      store_row16(S.X, t, x);
+      store_row16(S.Xd, t, xd);
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        store_bf16(S.XT, k, t, K, x[k]);
+        store_bf16(S.XdT, k, t, K, xd[k]);
+      }
+    }
+    sync_for_mma();
+    if (S.abort) break;
+    if (t == 0) {
+      tc_fence_after();
+      umma(tmem + 0, umma_desc(aX, kTcRows), umma_desc(aW1, H), umma_idesc(H), 0);
+      umma(tmem + 64, umma_desc(aXd, kTcRows), umma_desc(aW1, H), umma_idesc(H), 0);
+      umma_commit(mbar);
+    }
+    wait_mma();
+    // H1, Hd1
+    {
+      float z[H], zd[H];
+#pragma unroll
+      for (int q = 0; q < H / 16; ++q) {
+        tmem_ld16(tl + 0 + 16 * q, z + 16 * q);
+        tmem_ld16(tl + 64 + 16 * q, zd + 16 * q);
+      }
+      tmem_wait_ld();
+#pragma unroll
+      for (int u = 0; u < H; ++u) {
+        const float zz = z[u] + S.b1[u];
+        z[u] = silu(zz);
+        zd[u] = silu1(zz) * zd[u];
+      }
+      store_row64(S.H1, t, z);
+      store_row64(S.Hd1, t, zd);
+#pragma unroll
+      for (int u = 0; u < H; ++u) {
+        store_bf16(S.H1T, u, t, H, z[u]);
+        store_bf16(S.Hd1T, u, t, H, zd[u]);
+      }
+    }
+    sync_for_mma();
+    if (S.abort) break;
+    if (t == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (int kb = 0; kb < H / 16; ++kb) {
+        umma(tmem + 128, umma_desc(aH1 + kb * 2 * kTcRows * 16, kTcRows),
+             umma_desc(aW2 + kb * 2 * H * 16, H), umma_idesc(H), kb > 0);
+        umma(tmem + 192, umma_desc(aHd1 + kb * 2 * kTcRows * 16, kTcRows),
+             umma_desc(aW2 + kb * 2 * H * 16, H), umma_idesc(H), kb > 0);
+      }
+      umma_commit(mbar);
+    }
+    wait_mma();
+    // az2 = w3 zd2 silu''(z2), azd2 = w3 silu'(z2); rows for gb2 and gw3
+    {
+      float z[H], zd[H];
+#pragma unroll
+      for (int q = 0; q < H / 16; ++q) {
+        tmem_ld16(tl + 128 + 16 * q, z + 16 * q);
+        tmem_ld16(tl + 192 + 16 * q, zd + 16 * q);
+      }
+      tmem_wait_ld();
+      const bool live = i < n;
+#pragma unroll
+      for (int u = 0; u < H; ++u) {
+        const float zz = z[u] + S.b2[u];
+        const float s1 = silu1(zz);
+        const float q = live ? s1 * zd[u] : 0.f;       // gw3 term
+        const float az = live ? S.w3[u] * zd[u] * silu2(zz) : 0.f;
+        const float azd = live ? S.w3[u] * s1 : 0.f;
+        z[u] = az;
+        zd[u] = azd;
+        S.F[t][u] = q;
+      }
+      store_row64(S.A2, t, z);
+      store_row64(S.Ad2, t, zd);
+#pragma unroll
+      for (int u = 0; u < H; ++u) {
+        store_bf16(S.AT, u, t, 2 * H, z[u]);
+        store_bf16(S.AT, H + u, t, 2 * H, zd[u]);
+      }
+      colsum(gw3);
+#pragma unroll
+      for (int u = 0; u < H; ++u) S.F[t][u] = z[u];
+      colsum(gb2);
+    }
+    sync_for_mma();
+    if (S.abort) break;
+    if (t == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (int kb = 0; kb < H / 16; ++kb) {
+        umma(tmem + 128, umma_desc(aA2 + kb * 2 * kTcRows * 16, kTcRows),
+             umma_desc(aW2T + kb * 2 * H * 16, H), umma_idesc(H), kb > 0);
+        umma(tmem + 192, umma_desc(aAd2 + kb * 2 * kTcRows * 16, kTcRows),
+             umma_desc(aW2T + kb * 2 * H * 16, H), umma_idesc(H), kb > 0);
+      }
+#pragma unroll
+      for (int kb = 0; kb < kTcRows / 16; ++kb) {
+        umma(tmem + 256, umma_desc(aAT + kb * 2 * (2 * H) * 16, 2 * H),
+             umma_desc(aH1T + kb * 2 * H * 16, H), umma_idesc(H), (acc | kb) > 0);
+        umma(tmem + 320, umma_desc(aAT + kb * 2 * (2 * H) * 16, 2 * H),
+             umma_desc(aHd1T + kb * 2 * H * 16, H), umma_idesc(H), (acc | kb) > 0);
+      }
+      umma_commit(mbar);
+    }
+    wait_mma();
+    // az1 = ah1 silu'(z1) + ahd1 zd1 silu''(z1), azd1 = ahd1 silu'(z1)
+    {
+      float ah[H], ahd[H], z[H], zd[H];
+#pragma unroll
+      for (int q = 0; q < H / 16; ++q) {
+        tmem_ld16(tl + 128 + 16 * q, ah + 16 * q);
+        tmem_ld16(tl + 192 + 16 * q, ahd + 16 * q);
+        tmem_ld16(tl + 0 + 16 * q, z + 16 * q);
+        tmem_ld16(tl + 64 + 16 * q, zd + 16 * q);
+      }
+      tmem_wait_ld();
+#pragma unroll
+      for (int u = 0; u < H; ++u) {
+        const float zz = z[u] + S.b1[u];
+        const float s1 = silu1(zz);
+        const float az = ah[u] * s1 + ahd[u] * zd[u] * silu2(zz);
+        const float azd = ahd[u] * s1;
+        store_bf16(S.AT, u, t, 2 * H, az);
+        store_bf16(S.AT, H + u, t, 2 * H, azd);
+        S.F[t][u] = az;
+      }
+      colsum(gb1);
+    }
+    sync_for_mma();
+    if (S.abort) break;
+    if (t == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (int kb = 0; kb < kTcRows / 16; ++kb) {
+        umma(tmem + 384, umma_desc(aAT + kb * 2 * (2 * H) * 16, 2 * H),
+             umma_desc(aXT + kb * 2 * K * 16, K), umma_idesc(K), (acc | kb) > 0);
+        umma(tmem + 400, umma_desc(aAT + kb * 2 * (2 * H) * 16, 2 * H),
+             umma_desc(aXdT + kb * 2 * K * 16, K), umma_idesc(K), (acc | kb) > 0);
+      }
+      umma_commit(mbar);
+    }
+    wait_mma();
+    acc = 1;
+    tc_fence_before();
+    __syncthreads();
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (S.abort && t == 0) mbar_wait(mbar, phase);  // a bounded wait for the last product
+  __syncthreads();
+  tc_fence_after();
+  // gradient rows: thread t < 64 holds rows t of D1 and D3, thread 64 + t rows 64 + t of
+  // D2 and D4; combined through shared memory
+  float* p = partials + (size_t)blockIdx.x * kMlpParams;
+  {
+    float g2[H], g1[K];
+    if (acc && !S.abort) {
+#pragma unroll
+      for (int q = 0; q < H / 16; ++q) tmem_ld16(tl + (t < H ? 256 : 320) + 16 * q, g2 + 16 * q);
+      tmem_ld16(tl + (t < H ? 384 : 400), g1);
+      tmem_wait_ld();
+    } else {
+#pragma unroll
+      for (int u = 0; u < H; ++u) g2[u] = 0.f;
+#pragma unroll
+      for (int k = 0; k < K; ++k) g1[k] = 0.f;
+    }
+    if (t >= H) {
+#pragma unroll
+      for (int u = 0; u < H; ++u) S.F[t - H][u] = g2[u];
+#pragma unroll
+      for (int k = 0; k < K; ++k) S.F[t][k] = g1[k];  // rows 64..127 of F
+    }
+    __syncthreads();
+    if (t < H) {
+#pragma unroll
+      for (int u = 0; u < H; ++u) p[kOffW2 + t * H + u] = g2[u] + S.F[t][u];
+#pragma unroll
+      for (int k = 0; k < K; ++k) p[t * K + k] = g1[k] + S.F[H + t][k];
+      p[kOffB1 + t] = gb1;
+      p[kOffB2 + t] = gb2;
+      p[kOffW3 + t] = gw3;
+    }
+    if (t == 0) p[kOffB3] = 0.f;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kGtCols));
+  }
+}
+
 }  // namespace
 
 size_t mlp_tc_smem() { return sizeof(TcSmem) + 1024; }
+size_t mlp_grad_tc_smem() { return sizeof(GtSmem) + 1024; }
+
+// CTAs of the tensor-core gradient: one per SM (each holds all 512 TMEM columns)
+int mlp_grad_tc_blocks(int n) {
+  static int nsm[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  dev &= 63;
+  if (!nsm[dev]) {
+    cudaFuncSetAttribute(k_mlp_grad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)mlp_grad_tc_smem());
+    cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
+    if (nsm[dev] <= 0) nsm[dev] = 148;
+  }
+  const int tiles = (n + kTcRows - 1) / kTcRows;
+  return tiles < nsm[dev] ? (tiles > 0 ? tiles : 1) : nsm[dev];
+}
+
+// Launches the tensor-core gradient (one CTA per SM, at most maxblocks partial rows);
+// returns the number of partial rows written.
+int launch_mlp_grad_tc(const DevView& d, const float* tangent, float* partials, int maxblocks,
+                       cudaStream_t st) {
+  int nb = mlp_grad_tc_blocks(d.n);
+  if (nb > maxblocks) nb = maxblocks;
+  k_mlp_grad_tc<<<nb, kTcRows, mlp_grad_tc_smem(), st>>>(d.mlp, d.n, tangent, partials, d.err);
+  return nb;
+}
 
 void launch_mlp_site_tc(const DevView& d, cudaStream_t st) {
   static int nsm[64] = {0};

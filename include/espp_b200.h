@@ -371,6 +371,27 @@ ESPP_API int espp_selftest_bounded_wait(espp_system* s, int64_t spins, double* n
  * particle (3 launches each, CUDA events), keeps the fastest and returns it; ms[c] (may
  * be NULL) receives the mean launch time of candidate c. */
 ESPP_API int espp_autotune(espp_system* s, int32_t* best_tpp, double ms[4]);
+/* List layout of the Verlet list and pair kernels (tuning of the GPU kernels; no
+ * reference counterpart).  form 0: one global list per particle (sorted indices) built
+ * one warp per cell, tpp (1, 2, 4, 8) threads per particle in the force kernel;
+ * form 2: the same global list built by brick windows (brick[3] cells per brick edge,
+ * 1..4, or all 0 to choose from the density); form 1: brick windows for the build and
+ * the force kernels, one thread per particle with its list as 16-bit window indices.
+ * Forms 1 and 2 need grids of at least 2 cells per dimension; form 1 serves
+ * Lennard-Jones (plain or capped), FENE bonds and exclusions, tabulated and learned pair
+ * potentials use the global list.  All forms give the reference's pair set; the
+ * mixed-precision forces differ in rounding (within the 1e-5 budget).  The list is
+ * rebuilt at the current positions (not counted as a build). */
+ESPP_API int espp_set_layout(espp_system* s, int32_t form, int32_t tpp, const int32_t brick[3]);
+/* out = (form, tpp, brick extent x, y, z) of the list in use. */
+ESPP_API int espp_get_layout(espp_system* s, int32_t out[5]);
+/* Times each candidate layout on the current particle state (one list build and 3
+ * force launches each, CUDA events), keeps the one with the smallest force time plus
+ * build time / steps_per_build (<= 0: 10), and returns it in best (as espp_get_layout).
+ * table (may be NULL) receives up to cap rows (form, tpp, bx, by, bz, force ms, build ms,
+ * score); ncand the number of candidates timed. */
+ESPP_API int espp_autotune_layout(espp_system* s, double steps_per_build, int32_t best[5],
+                                  double* table, int32_t cap, int32_t* ncand);
 /* Device time of the last espp_run on the system's stream (ms): ms[0] whole call,
  * ms[1] the step loop after the start-of-run force evaluation. */
 ESPP_API int espp_last_run_ms(espp_system* s, double ms[2]);

@@ -2681,6 +2681,30 @@ int espp_selftest_bounded_wait(espp_system* s, int64_t spins, double* ns) {
   return fail(ESPP_ESTATE, "no device");
 }
 
+// the CPU restatement has one list layout
+int espp_set_layout(espp_system* s, int32_t, int32_t, const int32_t*) {
+  CHECK_S(s);
+  return ESPP_OK;
+}
+
+int espp_get_layout(espp_system* s, int32_t out[5]) {
+  CHECK_S(s);
+  if (!out) return fail(ESPP_EINVAL, "null output pointer");
+  for (int k = 0; k < 5; ++k) out[k] = 0;
+  out[1] = 1;
+  return ESPP_OK;
+}
+
+int espp_autotune_layout(espp_system* s, double, int32_t best[5], double* table, int32_t cap,
+                         int32_t* ncand) {
+  CHECK_S(s);
+  if (best) espp_get_layout(s, best);
+  if (table && cap > 0)
+    for (int k = 0; k < 8; ++k) table[k] = (k == 1) ? 1.0 : 0.0;
+  if (ncand) *ncand = 1;
+  return ESPP_OK;
+}
+
 int espp_autotune(espp_system* s, int32_t* best, double ms[4]) {
   CHECK_S(s);
   if (best) *best = 1;

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from espressopp_b200 import _abi
-from simdriver import Sim, cell_grid, cuda_lib, oracle_lib
+from simdriver import Sim, cell_grid, cuda_lib, lattice, oracle_lib
 from test_mlp_cpu import NP, cg_system, make_model
 
 pytestmark = pytest.mark.gpu
@@ -65,6 +65,59 @@ def test_mlp_force_matching_gradient_matches_oracle():
     # each weight block separately (W1, b1, W2, b2, w3)
     for a, b in ((0, 1024), (1024, 1088), (1088, 5184), (5184, 5248), (5248, 5312)):
         assert _rel(gg[a:b], go[a:b]) < 2e-3
+
+
+def _lattice_pair(n_side):
+    """CG-like sites on a jittered simple-cubic lattice at density 0.21 (both libraries)."""
+    pos, box = lattice(n_side, 0.21, 0.3, 11)
+    out = []
+    for lib in (oracle_lib(), cuda_lib()):
+        s = Sim(lib, box, 0.3, cell_grid(box, 3.0, 0.3))
+        s.add(np.arange(1, len(pos) + 1), pos, np.zeros_like(pos))
+        s.decompose()
+        s.vl(3.0)
+        m, _ = make_model(lib, seed=5)
+        _abi.call(lib, "espp_mlp_attach", s.h, m)
+        out.append((s, m))
+    return out, len(pos)
+
+
+@pytest.mark.parametrize("n_side", [0, 27])
+def test_mlp_tensor_core_gradient_matches_oracle(n_side):
+    """The force-matching gradient with its matrix products on the tensor cores (BF16
+    operands, FP32 accumulation; espp_mlp_set_mode 1) against the FP64 oracle and the
+    FP32 CUDA-core gradient: the BF16 rounding of the operands leaves a few 1e-3 relative
+    per weight block.  400 random sites fill part of one 128-site tile per CTA; 27^3 =
+    19,683 lattice sites give every CTA several tiles, so the accumulators carry over
+    tiles."""
+    if n_side:
+        ((o, mo), (g, mg)), nsites = _lattice_pair(n_side)
+    else:
+        nsites = 400
+        (o, mo), (g, mg) = _pair(n=nsites)[0]
+    ids = np.arange(1, nsites + 1)
+    rng = np.random.Generator(np.random.PCG64(4))
+    fref = np.ascontiguousarray(rng.normal(0, 1.0, (nsites, 3)).reshape(-1))
+    go = np.zeros(NP)
+    lo = ctypes.c_double()
+    _abi.call(o.lib, "espp_mlp_fm_grad", o.h, nsites, _abi.i64ptr(ids), _abi.dptr(fref),
+              ctypes.byref(lo), _abi.dptr(go))
+    res = {}
+    for mode in (0, 1):
+        _abi.call(g.lib, "espp_mlp_set_mode", mg, mode)
+        gg = np.zeros(NP)
+        lg = ctypes.c_double()
+        _abi.call(g.lib, "espp_mlp_fm_grad", g.h, nsites, _abi.i64ptr(ids), _abi.dptr(fref),
+                  ctypes.byref(lg), _abi.dptr(gg))
+        res[mode] = gg
+    _abi.call(g.lib, "espp_mlp_set_mode", mg, 0)
+    assert _rel(res[0], go) < 1e-3
+    assert _rel(res[1], go) < 2e-2
+    for a, b in ((0, 1024), (1024, 1088), (1088, 5184), (5184, 5248), (5248, 5312)):
+        assert _rel(res[1][a:b], go[a:b]) < 3e-2
+    # the direction that Adam follows
+    cos = float(np.dot(res[1], go) / (np.linalg.norm(res[1]) * np.linalg.norm(go)))
+    assert cos > 0.999
 
 
 def test_mlp_training_lowers_the_loss_and_md_runs():
