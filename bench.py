@@ -245,7 +245,7 @@ def reference_arm(args, rank, world):
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
+    emit(line)
 
 
 # ---- GPU arm ---------------------------------------------------------------------
@@ -410,6 +410,10 @@ def gpu_arm(args, rank, world, local_rank):
             cmp.update(oracle_parity(lib, h, ids, box))
 
     lib.espp_system_destroy(h)
+    if rank == 0:
+        log("LJ: %.4g particle-steps/s, %.4f ms/step%s" % (
+            world * N * args.steps / (loop_ms * 1e-3), loop_ms / args.steps,
+            ", mixed/fp64 %.3f" % cmp["mixed_over_fp64"] if "mixed_over_fp64" in cmp else ""))
     configs = (small_configs(lib, args.replica_steps, args.cg_small)
                if (rank == 0 and world == 1 and not args.no_configs) else None)
     if rank != 0:
@@ -484,7 +488,7 @@ def gpu_arm(args, rank, world, local_rank):
                                           "%.0f s of stepping on 1 core, vec SoA twin of the "
                                           "oracle" % args.cpu_budget,
                                 "classic_aos_value": cpu_classic}
-    print(json.dumps(line), flush=True)
+    emit(line)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -631,6 +635,24 @@ def lj32k_config(lib, prec, steps=1000):
     return {"value": 32768 * steps / (ms[1] * 1e-3), "ms_per_step": float(ms[1]) / steps}
 
 
+def _plain(o):
+    """JSON encoding of numpy scalars and arrays."""
+    if isinstance(o, np.integer):
+        return int(o)
+    if isinstance(o, np.floating):
+        return float(o)
+    if isinstance(o, np.bool_):
+        return bool(o)
+    if isinstance(o, np.ndarray):
+        return o.tolist()
+    raise TypeError("not JSON serialisable: %r" % type(o))
+
+
+def emit(line):
+    """Prints one JSON line."""
+    print(json.dumps(line, default=_plain), flush=True)
+
+
 def small_configs(lib, replica_steps=1000, cg_chains=200):
     from espressopp_b200 import _abi
     out = {}
@@ -654,6 +676,8 @@ def small_configs(lib, replica_steps=1000, cg_chains=200):
                       "sequential": rep["sequential"]["swaps"]},
             "unit": "particle-steps/s (wall clock around run calls and exchanges)"}
     if cg_chains > 0:
+        log("configs: learned-potential training gradient, 50,000 sites")
+        out["mlp_training_gradient_50k"] = mlp_gradient_config(50000)
         log("configs: learned CG potential, %d chains" % cg_chains)
         t0 = time.perf_counter()
         line = cg_workflow(cg_chains, 100, 5, 20000, 5, 50)
@@ -680,7 +704,7 @@ def cg_arm(args, rank, world, local_rank):
         return
     line = cg_workflow(args.cg_chains, args.cg_frames, args.cg_epochs, args.cg_steps,
                        args.cg_ibi, args.cg_window)
-    print(json.dumps(line), flush=True)
+    emit(line)
 
 
 def cg_workflow(nch, nfr, epochs, cg_steps, ibi_iters, window):
@@ -863,6 +887,60 @@ def cg_workflow(nch, nfr, epochs, cg_steps, ibi_iters, window):
 
 
 # ---- learned potential: force evaluation micro-benchmark --------------------------
+def mlp_gradient_config(n_sites=50000, calls=20, warmup=3):
+    """Force-matching gradient of the learned potential (espp_mlp_fm_grad: descriptor,
+    site network forward, forward-mode tangent, weight-gradient products) on n_sites CG
+    sites at density 0.2125 (jittered lattice), seeded weights and seeded reference forces,
+    with the weight products on the tensor cores (BF16, FP32 accumulation) and on CUDA
+    cores (FP32).  Wall clock around synchronous calls (each returns its loss), after
+    `warmup` calls; the relative difference of the two gradients is reported."""
+    from espressopp_b200 import cg
+    from espressopp_b200._abi import call, dptr, i64ptr
+    n_side = int(round(n_sites ** (1.0 / 3.0)))
+    pos, L = lattice(n_side, 0.2125, 0.3, 7)
+    n = len(pos)
+    fref = np.random.Generator(np.random.PCG64(9)).normal(0.0, 3.0, size=(n, 3))
+    zero = ([0.5, 1.0, 1.5, 2.0], [0.0] * 4, [0.0] * 4)
+    out, grads = {}, {}
+    for mode, name in ((1, "tensor_cores_bf16"), (0, "cuda_cores_fp32")):
+        sysm = cg.CGSystem(pos, L, np.zeros((0, 2), np.int64), zero)
+        model = cg.MLPModel(seed=5)
+        call(model.lib, "espp_mlp_set_mode", model.m, mode)
+        model.set_norm(np.full(16, 0.5), np.full(16, 1.0))
+        sysm.attach(model)
+        call(sysm.lib, "espp_integrator_set", sysm.h, 0.005)
+        sysm.run(0)
+        npar = ctypes.c_int64()
+        call(sysm.lib, "espp_mlp_num_params", ctypes.byref(npar))
+        g = np.zeros(npar.value)
+        loss = ctypes.c_double()
+        ids = np.ascontiguousarray(sysm.ids, np.int64)
+        f = np.ascontiguousarray(fref.reshape(-1))
+
+        def grad_call():
+            call(sysm.lib, "espp_mlp_fm_grad", sysm.h, n, i64ptr(ids), dptr(f),
+                 ctypes.byref(loss), dptr(g))
+        for _ in range(warmup):
+            grad_call()
+        t0 = time.perf_counter()
+        for _ in range(calls):
+            grad_call()
+        dt = time.perf_counter() - t0
+        out[name] = {"ms_per_gradient": dt / calls * 1e3,
+                     "site_gradients_per_s": n * calls / dt, "loss": loss.value}
+        grads[name] = g.copy()
+        sysm.close()
+        model.close()
+    a, b = grads["tensor_cores_bf16"], grads["cuda_cores_fp32"]
+    out["gradient_rel_diff_bf16_vs_fp32"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    out["speedup_tensor_cores"] = (out["cuda_cores_fp32"]["ms_per_gradient"] /
+                                   out["tensor_cores_bf16"]["ms_per_gradient"])
+    out["workload"] = ("force-matching gradient, %d CG sites, rc 3.0, 16 basis functions, "
+                       "MLP 16-64-64-1, %d calls" % (n, calls))
+    out["unit"] = "wall clock around synchronous espp_mlp_fm_grad calls"
+    return out
+
+
 def mlp_arm(args, rank, world, local_rank):
     """Device time of the learned potential's force pass (descriptor, site network,
     pair forces) on a CG-like configuration: --mlp-sites sites at density 0.2125 on a
@@ -898,8 +976,8 @@ def mlp_arm(args, rank, world, local_rank):
             "data": "synthetic",
             "config": {"workload": "learned CG potential force pass, %d sites, rc 3.0, "
                                    "16 basis functions, MLP 16-64-64-1" % n},
-            "modes": out}
-    print(json.dumps(line), flush=True)
+            "modes": out, "training_gradient": mlp_gradient_config(args.mlp_sites)}
+    emit(line)
 
 
 # ---- batched parallel-tempering replicas ------------------------------------------
@@ -1059,7 +1137,7 @@ def replicas_arm(args, rank, world, local_rank):
                            "replicas_on_rank0": nlocal},
                 "batched": out["batched"], "sequential": out["sequential"],
                 "batched_over_sequential": out["batched"]["value"] / out["sequential"]["value"]}
-        print(json.dumps(line), flush=True)
+        emit(line)
 
 
 def main():

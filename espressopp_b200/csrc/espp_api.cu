@@ -709,9 +709,10 @@ void build_list_plain(espp_system* s, double cutsq) {
     if (useBrick) {
       launch_build_brick(d, cutsq, s->st);
     } else {
-      if (!s->xrelFresh) launch_xrel(d, s->st);
+      const bool fresh = s->xrelFresh;
+      if (!fresh) launch_xrel(d, s->st);
       s->xrelFresh = false;
-      launch_build_nl(d, cutsq, s->st);
+      launch_build_nl(d, cutsq, fresh, s->st);
     }
     cuda_check(cudaGetLastError(), "Verlet list kernel");
     unsigned e = read_err(s);
@@ -1024,7 +1025,7 @@ void launch_rebuild_kernels(espp_system* s, cudaStream_t st) {
     if (s->brickOn || s->brickBuildUsed) {
       launch_build_brick(d, cv * cv, st);  // window-index or global form (d.brick.on)
     } else {
-      launch_build_nl(d, cv * cv, st);
+      launch_build_nl(d, cv * cv, true, st);
     }
   }
 }
@@ -2928,7 +2929,7 @@ void time_layout(espp_system* s, double& build_ms, double& force_ms) {
   if (s->brickOn || s->brickBuildUsed)
     launch_build_brick(d, cv * cv, s->st);
   else
-    launch_build_nl(d, cv * cv, s->st);
+    launch_build_nl(d, cv * cv, true, s->st);  // the form the step loop's rebuilds use
   cuda_check(cudaEventRecord(e1, s->st), "event");
   sync(s);
   float t = 0.f;

@@ -204,7 +204,9 @@ void launch_fold_bin(const DevView& d, RebuildScratch& s, bool fold, cudaStream_
 void launch_sort_cells(const DevView& d, RebuildScratch& s, cudaStream_t st);
 void launch_gather(const DevView& d, const RebuildScratch& s, cudaStream_t st);
 void launch_id_map(const DevView& d, cudaStream_t st);
-void launch_build_nl(const DevView& d, double cutsq, cudaStream_t st);
+// Verlet list in the global form; fresh: the particles were binned at their current
+// positions (the run form may then be used).
+void launch_build_nl(const DevView& d, double cutsq, bool fresh, cudaStream_t st);
 void launch_posq(const DevView& d, cudaStream_t st);
 void launch_xrel(const DevView& d, cudaStream_t st);
 void launch_forces(const DevView& d, bool mixed, const FENEParams& fene, int tpp,

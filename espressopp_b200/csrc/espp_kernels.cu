@@ -218,7 +218,9 @@ __device__ __forceinline__ uint64_t in_cell_key(const DevView& d, const Particle
     const int b = (int)(f * 8.0);
     q[i] = (unsigned)(b < 0 ? 0 : (b > 7 ? 7 : b));
   }
-  const uint64_t morton = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
+  // x in the most significant bit: a run of consecutive particles of one row of cells
+  // (the Verlet build's groups) then spans a short range of x
+  const uint64_t morton = spread3(q[2]) | (spread3(q[1]) << 1) | (spread3(q[0]) << 2);
   return (morton << 54) | (uint64_t)(a.id[v] - d.idMin);
 }
 
@@ -339,8 +341,8 @@ struct BuildChunk {
 
 // Fast tests of one chunk (nv valid candidates) against the lane's particle.  Returns
 // whether any candidate came near the cutoff (a superset of the borderline band).
-template <bool SELF, bool EXCL>
-__device__ __forceinline__ bool chunk_scan(const DevView& d, const BuildChunk& c, int nv,
+template <bool SELF, bool EXCL, class Chunk>
+__device__ __forceinline__ bool chunk_scan(const DevView& d, const Chunk& c, int nv,
                                            unsigned long long xi2, unsigned long long yi2,
                                            unsigned long long zi2, int i, int64_t idi,
                                            float lo, unsigned long long mid2, float hw,
@@ -509,6 +511,225 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build_nl_lane(DevView d, d
       }
     }
     const int wmax = __reduce_max_sync(0xffffffffu, own ? total : 0);
+    if (lane == 0 && wmax > 0) atomicMax(&d.ctr->nnMax, wmax);
+    __syncwarp();
+  }
+}
+
+
+// ---- Verlet build, run form ---------------------------------------------------------
+// One warp per 32 consecutive sorted particles, split where they change row of cells
+// (cy, cz); lane l holds particle g + l.  A group spans the x-cells ca..cb of one row; its
+// candidates are the particles of x-cells ca-1 .. cb+1 of the nine rows (cy+dy, cz+dz),
+// staged in the frame of cell (ca, cy, cz).  A candidate farther than the cutoff from the
+// bounding box of the group's particles cannot be a partner of any of them and is dropped
+// before it takes a slot of a chunk (ballot + prefix count), so the 32 lanes test only
+// survivors and no lane idles for lack of particles.  Tests, the band decided in FP64
+// and the staging of the list are those of the per-cell form.
+// Used for lists built right after the particles were binned at their current positions
+// in cells whose edges all exceed the list cutoff by 0.1 %: a particle's partners then
+// all lie in its 27 neighbour cells, and a candidate from a farther cell (a group spans
+// several x-cells) neither passes the test nor comes near the cutoff.  Grids with fewer
+// than 3 cells in a dimension, and lists rebuilt on cells of an earlier re-sort, use the
+// per-cell form.
+constexpr int kRunWarps = 4;
+constexpr int kRunSpan = 29;  // x-cells a group may span (candidate x-cells <= 31)
+
+struct RunChunk {  // 64 slots: a scan takes 32, the rest waits for the next
+  float x[64], y[64], z[64];
+  int j[64];
+  int xo[64];  // x-cell of the candidate, relative to ca
+  int64_t id[64];
+};
+
+__device__ __forceinline__ float warp_fmin(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ float warp_fmax(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+template <bool EXCL>
+__global__ void __launch_bounds__(kRunWarps * 32) k_build_nl_run(DevView d, double cutsq) {
+  const ParticleArrays a = d.pa[0];
+  __shared__ __align__(16) int s_stage[kRunWarps][32 * kStageLd];
+  __shared__ __align__(16) RunChunk s_chunk[kRunWarps];
+  __shared__ int s_pre[kRunWarps][33];  // prefix of the candidate x-cells' counts
+  __shared__ int s_st[kRunWarps][32];   // their first sorted index
+  const int wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int g = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
+  if (g >= d.n) return;
+  const unsigned full = 0xffffffffu;
+  const float lo = (float)(cutsq * (1.0 - 2e-5)), hi = (float)(cutsq * (1.0 + 2e-5));
+  const float mid = (float)cutsq, hw = (float)(cutsq * 3e-5);
+  const float keepsq = (float)(cutsq * (1.0 + 1e-4));
+  const unsigned long long mid2 = f2_pack(mid, mid);
+  const float hx = (float)d.cellSize[0], hy = (float)d.cellSize[1], hz = (float)d.cellSize[2];
+  const int nx = d.nc[0], ny = d.nc[1], nz = d.nc[2];
+  const float4* __restrict__ xr = d.xrel;
+  const int K = d.K;
+  const size_t cap = d.cap;
+  int* __restrict__ nl = d.nl;
+  RunChunk& ch = s_chunk[wib];
+  int* __restrict__ srow = &s_stage[wib][lane * kStageLd];
+  const int ip = g + lane;
+  const bool valid = ip < d.n;
+  const int mcell = valid ? d.pcell[ip] : 0;
+  const int mcx = mcell % nx, mrow = mcell / nx;
+  unsigned todo = __ballot_sync(full, valid);
+  while (todo) {
+    const int leader = __ffs(todo) - 1;
+    const int row = __shfl_sync(full, mrow, leader);
+    const int ca = __shfl_sync(full, mcx, leader);
+    const unsigned grp = __ballot_sync(full, ((todo >> lane) & 1u) && mrow == row &&
+                                                 mcx - ca <= kRunSpan);
+    todo &= ~grp;
+    const bool own = (grp >> lane) & 1u;
+    const int cb = __shfl_sync(full, mcx, 31 - __clz(grp));
+    const int cy = row % ny, cz = row / ny;
+    const int i = own ? ip : g + leader;
+    // the lane's particle in the frame of cell (ca, cy, cz); lanes outside the group far away
+    float fx = 1e18f, fy = 1e18f, fz = 1e18f;
+    if (own) {
+      const float4 r = xr[ip];
+      fx = r.x + (float)(mcx - ca) * hx;
+      fy = r.y;
+      fz = r.z;
+    }
+    const float bxl = warp_fmin(own ? fx : 3e38f), bxh = warp_fmax(own ? fx : -3e38f);
+    const float byl = warp_fmin(own ? fy : 3e38f), byh = warp_fmax(own ? fy : -3e38f);
+    const float bzl = warp_fmin(own ? fz : 3e38f), bzh = warp_fmax(own ? fz : -3e38f);
+    const unsigned long long xi2 = f2_pack(fx, fx), yi2 = f2_pack(fy, fy), zi2 = f2_pack(fz, fz);
+    const int64_t idi = (EXCL && own) ? a.id[ip] : -3;
+    const int nxs = cb - ca + 3;  // candidate x-cells ca-1 .. cb+1
+    int pend = 0, blk = 0;
+    for (int rr = 0; rr < 9; ++rr) {
+      const int oz = rr / 3 - 1, oy = rr % 3 - 1;
+      const int ncy = cy + oy, ncz = cz + oz;
+      const int wcy = ncy < 0 ? ncy + ny : (ncy >= ny ? ncy - ny : ncy);
+      const int wcz = ncz < 0 ? ncz + nz : (ncz >= nz ? ncz - nz : ncz);
+      const int rb = nx * (wcy + ny * wcz);
+      {
+        int st = 0, ct = 0;
+        if (lane < nxs) {
+          int xc = ca - 1 + lane;
+          xc += xc < 0 ? nx : (xc >= nx ? -nx : 0);
+          st = d.cellStart[rb + xc];
+          ct = d.cellStart[rb + xc + 1] - st;
+        }
+        int pre = ct;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int t = __shfl_up_sync(full, pre, o);
+          if (lane >= o) pre += t;
+        }
+        s_st[wib][lane] = st;
+        s_pre[wib][lane + 1] = pre;
+        if (lane == 0) s_pre[wib][0] = 0;
+      }
+      __syncwarp();
+      const int nrow = s_pre[wib][nxs];
+      const float ofy = (float)oy * hy, ofz = (float)oz * hz;
+      int fill = 0;
+      for (int cb0 = 0; cb0 < nrow; cb0 += 32) {
+        const int t = cb0 + lane;
+        bool keep = false;
+        float cx = 0.f, cy2 = 0.f, cz2 = 0.f;
+        int j = 0, k = 0;
+        if (t < nrow) {
+          while (s_pre[wib][k + 1] <= t) ++k;
+          j = s_st[wib][k] + (t - s_pre[wib][k]);
+          const float4 rj = xr[j];
+          cx = rj.x + (float)(k - 1) * hx;
+          cy2 = rj.y + ofy;
+          cz2 = rj.z + ofz;
+          const float ex = fmaxf(0.f, fmaxf(bxl - cx, cx - bxh));
+          const float ey = fmaxf(0.f, fmaxf(byl - cy2, cy2 - byh));
+          const float ez = fmaxf(0.f, fmaxf(bzl - cz2, cz2 - bzh));
+          keep = fmaf(ez, ez, fmaf(ey, ey, ex * ex)) <= keepsq;
+        }
+        const unsigned km = __ballot_sync(full, keep);
+        if (keep) {
+          const int pos = fill + __popc(km & ((1u << lane) - 1u));
+          ch.x[pos] = cx;
+          ch.y[pos] = cy2;
+          ch.z[pos] = cz2;
+          ch.j[pos] = j;
+          ch.xo[pos] = k - 1;
+          if (EXCL) ch.id[pos] = a.id[j];
+        }
+        fill += __popc(km);
+        const bool last = cb0 + 32 >= nrow;
+        while (fill >= 32 || (last && fill > 0)) {
+          const int nv = min(fill, 32);
+          // the scan reads candidates in pairs: an odd count gets a far-away partner slot
+          if ((nv & 1) && lane == 0) {
+            ch.x[nv] = ch.y[nv] = ch.z[nv] = -1e18f;
+            ch.j[nv] = -1;
+            if (EXCL) ch.id[nv] = -2;
+          }
+          __syncwarp();
+          const bool band =
+              rr == 4 ? chunk_scan<true, EXCL>(d, ch, nv, xi2, yi2, zi2, i, idi, lo, mid2, hw, srow,
+                                               pend)
+                      : chunk_scan<false, EXCL>(d, ch, nv, xi2, yi2, zi2, i, idi, lo, mid2, hw,
+                                                srow, pend);
+          if (__builtin_expect(__any_sync(full, band), 0) && own) {
+            // borderline candidates of this chunk: the reference's FP64 test decides
+            const int wy = ncy < 0 ? -1 : (ncy >= ny ? 1 : 0);
+            const int wz = ncz < 0 ? -1 : (ncz >= nz ? 1 : 0);
+            for (int m = 0; m < nv; ++m) {
+              const unsigned long long dx = f2_sub(xi2, f2_pack(ch.x[m], ch.x[m]));
+              const unsigned long long dy = f2_sub(yi2, f2_pack(ch.y[m], ch.y[m]));
+              const unsigned long long dz = f2_sub(zi2, f2_pack(ch.z[m], ch.z[m]));
+              const float r2 = f2_lo(f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx))));
+              const int jm = ch.j[m];
+              if (!(r2 >= lo && r2 <= hi) || jm == i) continue;
+              const int xu = ca + ch.xo[m];  // the candidate's x-cell, unwrapped
+              const int ox = xu - mcx;
+              if (ox < -1 || ox > 1) continue;  // not a neighbour cell of this particle
+              const int wx = xu < 0 ? -1 : (xu >= nx ? 1 : 0);
+              const bool fwd = oz > 0 || (oz == 0 && (oy > 0 || (oy == 0 && ox > 0)));
+              bool in = exact_pair_test(a.x, d.cap, i, jm, fwd, wx * d.L[0], wy * d.L[1],
+                                        wz * d.L[2], cutsq);
+              if (EXCL && in && is_excluded(d, idi, ch.id[m])) in = false;
+              if (in) srow[pend++] = jm;
+            }
+          }
+          stage_flush(srow, pend, blk, nl, i, cap, K >> 3);
+          __syncwarp();
+          // slots 32 .. fill-1 move to the front
+          if (lane < fill - 32) {
+            const int sidx = 32 + lane;
+            ch.x[lane] = ch.x[sidx];
+            ch.y[lane] = ch.y[sidx];
+            ch.z[lane] = ch.z[sidx];
+            ch.j[lane] = ch.j[sidx];
+            ch.xo[lane] = ch.xo[sidx];
+            if (EXCL) ch.id[lane] = ch.id[sidx];
+          }
+          fill -= nv;
+          __syncwarp();
+        }
+      }
+      __syncwarp();
+    }
+    const int total = blk * 8 + pend;
+    if (own) {
+      if (total > K) atomicOr(d.err, kErrNlOverflow);
+      d.nn[i] = min(total, K);
+      if (pend > 0) {
+        for (int k = pend; k < 8; ++k) srow[k] = i;
+        pend = 8;
+        stage_flush(srow, pend, blk, nl, i, cap, K >> 3);
+      }
+    }
+    const int wmax = __reduce_max_sync(full, own ? total : 0);
     if (lane == 0 && wmax > 0) atomicMax(&d.ctr->nnMax, wmax);
     __syncwarp();
   }
@@ -1654,7 +1875,31 @@ void launch_posq(const DevView& d, cudaStream_t st) {
   if (d.n > 0) k_posq<<<blocks_for(d.n), kBlock, 0, st>>>(d);
 }
 
-void launch_build_nl(const DevView& d, double cutsq, cudaStream_t st) {
+// The run form needs cells binned at the current positions (fresh), at least 3 cells in
+// every dimension and cell edges 0.1 % above the list cutoff; ESPP_B200_BUILD=cell keeps
+// the per-cell form.
+bool run_build_ok(const DevView& d, double cutsq, bool fresh) {
+  static int env = -1;
+  if (env < 0) {
+    const char* e = getenv("ESPP_B200_BUILD");
+    env = (e && strcmp(e, "cell") == 0) ? 0 : 1;
+  }
+  if (!fresh || env == 0 || d.n == 0) return false;
+  const double rc = sqrt(cutsq) * (1.0 + 1e-3);
+  for (int k = 0; k < 3; ++k)
+    if (d.nc[k] < 3 || d.cellSize[k] < rc) return false;
+  return true;
+}
+
+void launch_build_nl(const DevView& d, double cutsq, bool fresh, cudaStream_t st) {
+  if (run_build_ok(d, cutsq, fresh)) {
+    const int nb = blocks_for((long long)d.n, kRunWarps * 32);
+    if (d.exclStart)
+      k_build_nl_run<true><<<nb, kRunWarps * 32, 0, st>>>(d, cutsq);
+    else
+      k_build_nl_run<false><<<nb, kRunWarps * 32, 0, st>>>(d, cutsq);
+    return;
+  }
   const int nb = blocks_for((long long)d.ncells * 32, kBuildWarps * 32);
   if (d.exclStart)
     k_build_nl_lane<true><<<nb, kBuildWarps * 32, 0, st>>>(d, cutsq);

@@ -300,7 +300,9 @@ typedef struct espp_mlp espp_mlp;
 ESPP_API int espp_mlp_create(double rc, double r0, espp_mlp** out);
 ESPP_API int espp_mlp_destroy(espp_mlp* m);
 /* Site network arithmetic: 1 (default) BF16 operands on the tensor cores (tcgen05) with
- * FP32 accumulation, 0 FP32 on the CUDA cores.  The force-matching gradient is FP32. */
+ * FP32 accumulation, 0 FP32 on the CUDA cores.  The mode applies to the force pass and to
+ * the weight-gradient products of espp_mlp_fm_grad (the descriptor, the tangent and the
+ * bias sums stay FP32). */
 ESPP_API int espp_mlp_set_mode(espp_mlp* m, int32_t tensor_cores);
 ESPP_API int espp_mlp_num_params(int64_t* n);
 ESPP_API int espp_mlp_set_params(espp_mlp* m, int64_t n, const double* theta);
