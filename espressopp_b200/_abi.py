@@ -96,6 +96,7 @@ PROTOTYPES = {
     "espp_batch_last_run_ms": (c_int32, [_P, _D]),
     "espp_autotune": (c_int32, [_P, _I32, _D]),
     "espp_set_layout": (c_int32, [_P, c_int32, c_int32, _I32]),
+    "espp_set_half_cell_int": (c_int32, [_P, c_int32]),
     "espp_get_layout": (c_int32, [_P, _I32]),
     "espp_autotune_layout": (c_int32, [_P, c_double, _I32, _D, c_int32, _I32]),
 }

@@ -305,8 +305,7 @@ class DomainDecomposition:
                              "must be (1,1,1)")
         if halfCellInt == "auto":
             halfCellInt = 1
-        if int(halfCellInt) != 1:
-            raise ValueError("halfCellInt > 1 is not supported by the GPU storage")
+        halfCellInt = int(halfCellInt)
         if cellGrid == "auto":
             cellGrid = Int3D(2, 2, 2)
         cellGrid = list(Int3D(cellGrid))
@@ -326,6 +325,9 @@ class DomainDecomposition:
             system.rng._keyed = True
         call(self._lib, "espp_system_create", dptr(box), float(system.skin), i32ptr(cg), prec,
              int(seed) & 0xFFFFFFFFFFFFFFFF, ctypes.byref(self._h))
+        self.halfCellInt = halfCellInt
+        if halfCellInt != 1:
+            call(self._lib, "espp_set_half_cell_int", self._h, halfCellInt)
         self._types = {}
         self._masses = {}
         self.next_id = 0

@@ -75,6 +75,7 @@ struct espp_system {
   double L[3];
   double skin;
   int nc[3];
+  int hci = 1;  // halfCellInt
   int precision;
   uint64_t seed;
   int device = 0;
@@ -257,6 +258,7 @@ struct espp_system {
       d.fixUnit[k] = (float)(L[k] / kFix);
     }
     d.ncells = nc[0] * nc[1] * nc[2];
+    d.hci = hci;
     d.posq = posq;
     d.xrel = xrel;
     d.pcell = pcell;
@@ -613,6 +615,7 @@ DevCounters get_counters(espp_system* s);
 bool pair_any(const espp_system* s);
 bool brick_wanted(const espp_system* s) {
   if (!s->brickAllowed || !s->has_vl || !s->lj_any || s->tabNT > 0 || s->mlp) return false;
+  if (s->hci != 1) return false;
   for (int k = 0; k < 3; ++k)
     if (s->nc[k] < 2) return false;
   return true;
@@ -645,6 +648,7 @@ int brick_window_limit(const espp_system* s) {
 }
 
 bool brick_geometry_ok(const espp_system* s) {
+  if (s->hci != 1) return false;  // brick windows hold one cell layer
   for (int k = 0; k < 3; ++k)
     if (s->nc[k] < 2) return false;
   return s->n > 0;
@@ -2871,6 +2875,19 @@ int espp_fp32_peak(double* tflops) {
     cuda_check(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "attribute");
     *tflops = measure_fp32_tflops(nsm, 0);
     cuda_check(cudaGetLastError(), "fp32 probe");
+  });
+}
+
+int espp_set_half_cell_int(espp_system* s, int32_t h) {
+  return guard([&] {
+    checked(s);
+    if (h < 1 || h > 4) raise(ESPP_EINVAL, "halfCellInt must be 1 .. 4");
+    for (int k = 0; k < 3; ++k)
+      if (s->nc[k] < 2 * h + 1)
+        raise(ESPP_EINVAL, "the cell grid needs at least 2 halfCellInt + 1 cells a dimension");
+    if (s->n > 0) raise(ESPP_ESTATE, "halfCellInt is set before particles are added");
+    s->hci = h;
+    s->listValid = false;
   });
 }
 

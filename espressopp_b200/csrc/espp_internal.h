@@ -147,6 +147,7 @@ struct DevView {
   double L[3], invL[3], halfL[3];
   double cellSize[3], invCellSize[3];
   int nc[3];              // inner cells per dim
+  int hci;                // halfCellInt: Verlet candidates from cells within hci cells
   int ncells;
   double fixScale[3];     // 2^32 / L_d   (double -> box-wrapped int32)
   float fixUnit[3];       // L_d / 2^32   (int32 difference -> float length)

@@ -341,12 +341,16 @@ struct BuildChunk {
 
 // Fast tests of one chunk (nv valid candidates) against the lane's particle.  Returns
 // whether any candidate came near the cutoff (a superset of the borderline band).
-template <bool SELF, bool EXCL, class Chunk>
+// STENCIL: candidate m counts only when its x-cell offset c.xo[m] lies within h cells of
+// the lane's own (rel, relative to the same origin): the reference's neighbour cells when
+// particles may have left the cells of the last re-sort.
+template <bool SELF, bool EXCL, class Chunk, bool STENCIL = false>
 __device__ __forceinline__ bool chunk_scan(const DevView& d, const Chunk& c, int nv,
                                            unsigned long long xi2, unsigned long long yi2,
                                            unsigned long long zi2, int i, int64_t idi,
                                            float lo, unsigned long long mid2, float hw,
-                                           int* __restrict__ srow, int& pend) {
+                                           int* __restrict__ srow, int& pend, int rel = 0,
+                                           int h = 1) {
   bool band = false;
 #pragma unroll
   for (int m = 0; m < 32; m += 2) {
@@ -363,6 +367,11 @@ __device__ __forceinline__ bool chunk_scan(const DevView& d, const Chunk& c, int
     if (SELF) {
       ina &= jj.x != i;
       inb &= jj.y != i;
+    }
+    if constexpr (STENCIL) {
+      const int2 xo = *reinterpret_cast<const int2*>(&c.xo[m]);
+      ina &= (unsigned)(xo.x - rel + h) <= (unsigned)(2 * h);
+      inb &= (unsigned)(xo.y - rel + h) <= (unsigned)(2 * h);
     }
     if (EXCL) {
       if (ina && is_excluded(d, idi, c.id[m])) ina = false;
@@ -533,7 +542,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build_nl_lane(DevView d, d
 // than 3 cells in a dimension, and lists rebuilt on cells of an earlier re-sort, use the
 // per-cell form.
 constexpr int kRunWarps = 4;
-constexpr int kRunSpan = 29;  // x-cells a group may span (candidate x-cells <= 31)
+// x-cells a group may span: its candidate x-cells ca-h .. cb+h number at most 32
 
 struct RunChunk {  // 64 slots: a scan takes 32, the rest waits for the next
   float x[64], y[64], z[64];
@@ -553,7 +562,7 @@ __device__ __forceinline__ float warp_fmax(float v) {
   return v;
 }
 
-template <bool EXCL>
+template <bool EXCL, bool STALE>
 __global__ void __launch_bounds__(kRunWarps * 32) k_build_nl_run(DevView d, double cutsq) {
   const ParticleArrays a = d.pa[0];
   __shared__ __align__(16) int s_stage[kRunWarps][32 * kStageLd];
@@ -571,6 +580,8 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_build_nl_run(DevView d, doub
   const unsigned long long mid2 = f2_pack(mid, mid);
   const float hx = (float)d.cellSize[0], hy = (float)d.cellSize[1], hz = (float)d.cellSize[2];
   const int nx = d.nc[0], ny = d.nc[1], nz = d.nc[2];
+  const int h = d.hci, sw = 2 * h + 1;  // stencil reach and width (halfCellInt)
+  const int span = 31 - 2 * h;
   const float4* __restrict__ xr = d.xrel;
   const int K = d.K;
   const size_t cap = d.cap;
@@ -587,7 +598,7 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_build_nl_run(DevView d, doub
     const int row = __shfl_sync(full, mrow, leader);
     const int ca = __shfl_sync(full, mcx, leader);
     const unsigned grp = __ballot_sync(full, ((todo >> lane) & 1u) && mrow == row &&
-                                                 mcx - ca <= kRunSpan);
+                                                 mcx - ca <= span);
     todo &= ~grp;
     const bool own = (grp >> lane) & 1u;
     const int cb = __shfl_sync(full, mcx, 31 - __clz(grp));
@@ -606,10 +617,10 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_build_nl_run(DevView d, doub
     const float bzl = warp_fmin(own ? fz : 3e38f), bzh = warp_fmax(own ? fz : -3e38f);
     const unsigned long long xi2 = f2_pack(fx, fx), yi2 = f2_pack(fy, fy), zi2 = f2_pack(fz, fz);
     const int64_t idi = (EXCL && own) ? a.id[ip] : -3;
-    const int nxs = cb - ca + 3;  // candidate x-cells ca-1 .. cb+1
+    const int nxs = cb - ca + sw;  // candidate x-cells ca-h .. cb+h
     int pend = 0, blk = 0;
-    for (int rr = 0; rr < 9; ++rr) {
-      const int oz = rr / 3 - 1, oy = rr % 3 - 1;
+    for (int rr = 0; rr < sw * sw; ++rr) {
+      const int oz = rr / sw - h, oy = rr % sw - h;
       const int ncy = cy + oy, ncz = cz + oz;
       const int wcy = ncy < 0 ? ncy + ny : (ncy >= ny ? ncy - ny : ncy);
       const int wcz = ncz < 0 ? ncz + nz : (ncz >= nz ? ncz - nz : ncz);
@@ -617,7 +628,7 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_build_nl_run(DevView d, doub
       {
         int st = 0, ct = 0;
         if (lane < nxs) {
-          int xc = ca - 1 + lane;
+          int xc = ca - h + lane;
           xc += xc < 0 ? nx : (xc >= nx ? -nx : 0);
           st = d.cellStart[rb + xc];
           ct = d.cellStart[rb + xc + 1] - st;
@@ -645,7 +656,7 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_build_nl_run(DevView d, doub
           while (s_pre[wib][k + 1] <= t) ++k;
           j = s_st[wib][k] + (t - s_pre[wib][k]);
           const float4 rj = xr[j];
-          cx = rj.x + (float)(k - 1) * hx;
+          cx = rj.x + (float)(k - h) * hx;
           cy2 = rj.y + ofy;
           cz2 = rj.z + ofz;
           const float ex = fmaxf(0.f, fmaxf(bxl - cx, cx - bxh));
@@ -660,7 +671,7 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_build_nl_run(DevView d, doub
           ch.y[pos] = cy2;
           ch.z[pos] = cz2;
           ch.j[pos] = j;
-          ch.xo[pos] = k - 1;
+          ch.xo[pos] = k - h;
           if (EXCL) ch.id[pos] = a.id[j];
         }
         fill += __popc(km);
@@ -674,11 +685,13 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_build_nl_run(DevView d, doub
             if (EXCL) ch.id[nv] = -2;
           }
           __syncwarp();
+          const bool self = oy == 0 && oz == 0;
           const bool band =
-              rr == 4 ? chunk_scan<true, EXCL>(d, ch, nv, xi2, yi2, zi2, i, idi, lo, mid2, hw, srow,
-                                               pend)
-                      : chunk_scan<false, EXCL>(d, ch, nv, xi2, yi2, zi2, i, idi, lo, mid2, hw,
-                                                srow, pend);
+              self ? chunk_scan<true, EXCL, RunChunk, STALE>(d, ch, nv, xi2, yi2, zi2, i, idi, lo,
+                                                             mid2, hw, srow, pend, mcx - ca, h)
+                   : chunk_scan<false, EXCL, RunChunk, STALE>(d, ch, nv, xi2, yi2, zi2, i, idi,
+                                                              lo, mid2, hw, srow, pend, mcx - ca,
+                                                              h);
           if (__builtin_expect(__any_sync(full, band), 0) && own) {
             // borderline candidates of this chunk: the reference's FP64 test decides
             const int wy = ncy < 0 ? -1 : (ncy >= ny ? 1 : 0);
@@ -692,7 +705,7 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_build_nl_run(DevView d, doub
               if (!(r2 >= lo && r2 <= hi) || jm == i) continue;
               const int xu = ca + ch.xo[m];  // the candidate's x-cell, unwrapped
               const int ox = xu - mcx;
-              if (ox < -1 || ox > 1) continue;  // not a neighbour cell of this particle
+              if (ox < -h || ox > h) continue;  // not a neighbour cell of this particle
               const int wx = xu < 0 ? -1 : (xu >= nx ? 1 : 0);
               const bool fwd = oz > 0 || (oz == 0 && (oy > 0 || (oy == 0 && ox > 0)));
               bool in = exact_pair_test(a.x, d.cap, i, jm, fwd, wx * d.L[0], wy * d.L[1],
@@ -1885,9 +1898,9 @@ bool run_build_ok(const DevView& d, double cutsq, bool fresh) {
     env = (e && strcmp(e, "cell") == 0) ? 0 : 1;
   }
   if (!fresh || env == 0 || d.n == 0) return false;
-  const double rc = sqrt(cutsq) * (1.0 + 1e-3);
+  const double rc = sqrt(cutsq) * (1.0 + 1e-3) / d.hci;
   for (int k = 0; k < 3; ++k)
-    if (d.nc[k] < 3 || d.cellSize[k] < rc) return false;
+    if (d.nc[k] < 2 * d.hci + 1 || d.cellSize[k] < rc) return false;
   return true;
 }
 
@@ -1895,9 +1908,20 @@ void launch_build_nl(const DevView& d, double cutsq, bool fresh, cudaStream_t st
   if (run_build_ok(d, cutsq, fresh)) {
     const int nb = blocks_for((long long)d.n, kRunWarps * 32);
     if (d.exclStart)
-      k_build_nl_run<true><<<nb, kRunWarps * 32, 0, st>>>(d, cutsq);
+      k_build_nl_run<true, false><<<nb, kRunWarps * 32, 0, st>>>(d, cutsq);
     else
-      k_build_nl_run<false><<<nb, kRunWarps * 32, 0, st>>>(d, cutsq);
+      k_build_nl_run<false, false><<<nb, kRunWarps * 32, 0, st>>>(d, cutsq);
+    return;
+  }
+  if (d.hci > 1) {
+    // the per-cell form reaches one cell; the run form with each particle's own
+    // neighbour cells enforced serves any cells (also cells of an earlier re-sort)
+    if (d.n == 0) return;
+    const int nb = blocks_for((long long)d.n, kRunWarps * 32);
+    if (d.exclStart)
+      k_build_nl_run<true, true><<<nb, kRunWarps * 32, 0, st>>>(d, cutsq);
+    else
+      k_build_nl_run<false, true><<<nb, kRunWarps * 32, 0, st>>>(d, cutsq);
     return;
   }
   const int nb = blocks_for((long long)d.ncells * 32, kBuildWarps * 32);

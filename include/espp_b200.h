@@ -373,6 +373,12 @@ ESPP_API int espp_selftest_bounded_wait(espp_system* s, int64_t spins, double* n
  * particle (3 launches each, CUDA events), keeps the fastest and returns it; ms[c] (may
  * be NULL) receives the mean launch time of candidate c. */
 ESPP_API int espp_autotune(espp_system* s, int32_t* best_tpp, double ms[4]);
+/* DomainDecomposition's halfCellInt (src/storage/DomainDecomposition.cpp:325-357,
+ * tools/decomp.py:322): the cell grid given to espp_system_create is the fine grid, and a
+ * particle's Verlet candidates come from the cells within h cells in each direction (a
+ * (2h + 1)^3 stencil).  1 .. 4, the grid at least 2h + 1 cells a dimension; set before
+ * any particle is added (ESPP_ESTATE otherwise).  h > 1 takes the global list form. */
+ESPP_API int espp_set_half_cell_int(espp_system* s, int32_t h);
 /* List layout of the Verlet list and pair kernels (tuning of the GPU kernels; no
  * reference counterpart).  form 0: one global list per particle (sorted indices) built
  * one warp per cell, tpp (1, 2, 4, 8) threads per particle in the force kernel;

@@ -376,7 +376,8 @@ struct espp_system {
   double skin;
   int precision;
   uint64_t seed;
-  int n[3], F[3];  // inner cells, frame cells (n + 2)
+  int n[3], F[3];  // inner cells, frame cells (n + 2 H)
+  int H = 1;       // halfCellInt: ghost frame width and neighbour-cell reach
   double cellSize[3], invCellSize[3];
   std::vector<Cell> cells;
   std::vector<int> realCells, ghostCells;
@@ -440,16 +441,17 @@ void foldCoordinate(const espp_system* s, double* pos, int32_t* img, int dir) {
   pos[dir] -= tmp * s->L[dir];
 }
 
-// CellGrid::mapPositionToCellClipped (src/storage/CellGrid.cpp:87-107), myLeft = 0.
+// CellGrid::mapPositionToCellClipped (src/storage/CellGrid.cpp:87-107), myLeft = 0,
+// frame width H.
 int mapClipped(const espp_system* s, const double* pos) {
   int c[3];
   for (int i = 0; i < 3; ++i) {
     double lpos = pos[i] - 0.0;
-    c[i] = static_cast<int>(lpos * s->invCellSize[i]) + 1;
-    if (c[i] < 1)
-      c[i] = 1;
-    else if (c[i] >= s->F[i] - 1)
-      c[i] = s->F[i] - 2;
+    c[i] = static_cast<int>(lpos * s->invCellSize[i]) + s->H;
+    if (c[i] < s->H)
+      c[i] = s->H;
+    else if (c[i] >= s->F[i] - s->H)
+      c[i] = s->F[i] - s->H - 1;
   }
   return cellIndex(s, c[0], c[1], c[2]);
 }
@@ -459,15 +461,15 @@ int mapChecked(const espp_system* s, const double* pos) {
   int c[3];
   for (int i = 0; i < 3; ++i) {
     double lpos = pos[i] - 0.0;
-    c[i] = static_cast<int>(lpos * s->invCellSize[i]) + 1;
-    if (c[i] < 1) {
+    c[i] = static_cast<int>(lpos * s->invCellSize[i]) + s->H;
+    if (c[i] < s->H) {
       if (lpos >= -ROUND_ERROR_PREC)
-        c[i] = 1;
+        c[i] = s->H;
       else
         return -1;
-    } else if (c[i] >= s->F[i] - 1) {
+    } else if (c[i] >= s->F[i] - s->H) {
       if (pos[i] <= s->L[i] + ROUND_ERROR_PREC)
-        c[i] = s->F[i] - 2;
+        c[i] = s->F[i] - s->H - 1;
       else
         return -1;
     }
@@ -491,10 +493,12 @@ Particle* lookup(espp_system* s, int64_t id) {
 
 // DomainDecomposition::createCellGrid/markCells/initCellInteractions/
 // prepareGhostCommunication (src/storage/DomainDecomposition.cpp:87-170, 325-374,
-// 1243-1308) for nodeGrid (1,1,1) and halfCellInt 1.
+// 1243-1308) for nodeGrid (1,1,1): a ghost frame of H = halfCellInt cells, neighbour
+// cells within H cells in each direction, ghost slabs H cells thick.
 void buildGrid(espp_system* s) {
+  const int H = s->H;
   for (int i = 0; i < 3; ++i) {
-    s->F[i] = s->n[i] + 2;
+    s->F[i] = s->n[i] + 2 * H;
     s->cellSize[i] = (s->L[i] - 0.0) / double(s->n[i]);
     s->invCellSize[i] = 1.0 / s->cellSize[i];
   }
@@ -504,17 +508,17 @@ void buildGrid(espp_system* s) {
   for (int o = 0; o < s->F[2]; ++o)
     for (int n = 0; n < s->F[1]; ++n)
       for (int m = 0; m < s->F[0]; ++m) {
-        bool inner = m >= 1 && m < s->F[0] - 1 && n >= 1 && n < s->F[1] - 1 && o >= 1 &&
-                     o < s->F[2] - 1;
+        bool inner = m >= H && m < s->F[0] - H && n >= H && n < s->F[1] - H && o >= H &&
+                     o < s->F[2] - H;
         (inner ? s->realCells : s->ghostCells).push_back(cellIndex(s, m, n, o));
       }
-  for (int o = 1; o < s->F[2] - 1; ++o)
-    for (int n = 1; n < s->F[1] - 1; ++n)
-      for (int m = 1; m < s->F[0] - 1; ++m) {
+  for (int o = H; o < s->F[2] - H; ++o)
+    for (int n = H; n < s->F[1] - H; ++n)
+      for (int m = H; m < s->F[0] - H; ++m) {
         int ci = cellIndex(s, m, n, o);
-        for (int p = o - 1; p <= o + 1; ++p)
-          for (int q = n - 1; q <= n + 1; ++q)
-            for (int r = m - 1; r <= m + 1; ++r)
+        for (int p = o - H; p <= o + H; ++p)
+          for (int q = n - H; q <= n + H; ++q)
+            for (int r = m - H; r <= m + H; ++r)
               if (p != o || q != n || r != m) {
                 int c2 = cellIndex(s, r, q, p);
                 s->cells[ci].nbrs.push_back({c2, c2 < ci});
@@ -535,26 +539,26 @@ void buildGrid(espp_system* s) {
         lb[oc] = 0;
         rb[oc] = s->F[oc];
       } else {
-        lb[oc] = 1;
-        rb[oc] = s->F[oc] - 1;
+        lb[oc] = H;
+        rb[oc] = s->F[oc] - H;
       }
     }
     for (int lr = 0; lr < 2; ++lr) {
       int dir = 2 * coord + lr;
       if (lr == 0) {
-        lb[coord] = 1;
-        rb[coord] = 2;
+        lb[coord] = H;
+        rb[coord] = 2 * H;
       } else {
-        lb[coord] = s->F[coord] - 2;
-        rb[coord] = s->F[coord] - 1;
+        lb[coord] = s->F[coord] - 2 * H;
+        rb[coord] = s->F[coord] - H;
       }
       fill(s->commReals[dir], lb, rb);
       if (lr == 0) {
-        lb[coord] = s->F[coord] - 1;
+        lb[coord] = s->F[coord] - H;
         rb[coord] = s->F[coord];
       } else {
         lb[coord] = 0;
-        rb[coord] = 1;
+        rb[coord] = H;
       }
       fill(s->commGhosts[dir], lb, rb);
     }
@@ -1663,6 +1667,20 @@ int espp_system_destroy(espp_system* s) {
   return ESPP_OK;
 }
 
+// DomainDecomposition's halfCellInt (DomainDecomposition.cpp:325-357): neighbour cells
+// within h cells, a ghost frame h cells wide.  Before any particle is added.
+int espp_set_half_cell_int(espp_system* s, int32_t h) {
+  CHECK_S(s);
+  if (h < 1 || h > 4) return fail(ESPP_EINVAL, "halfCellInt must be 1 .. 4");
+  for (int i = 0; i < 3; ++i)
+    if (s->n[i] < 2 * h + 1)
+      return fail(ESPP_EINVAL, "the cell grid needs at least 2 halfCellInt + 1 cells a dimension");
+  if (!s->where.empty()) return fail(ESPP_ESTATE, "halfCellInt is set before particles are added");
+  s->H = h;
+  buildGrid(s);
+  return ESPP_OK;
+}
+
 int espp_set_skin(espp_system* s, double skin) {
   CHECK_S(s);
   s->skin = skin;
@@ -2170,6 +2188,7 @@ int espp_run(espp_system* s, int64_t nsteps) {
 // a second CPU baseline; not part of the GPU library's ABI.
 int espp_vec_run(espp_system* s, int64_t nsteps) {
   CHECK_S(s);
+  if (s->H != 1) return fail(ESPP_EINVAL, "the vec twin takes halfCellInt 1 only");
   return vecRun(s, nsteps);
 }
 

@@ -51,13 +51,16 @@ def cuda_lib():
 
 
 class Sim:
-    def __init__(self, lib, box, skin, cell_grid, precision=_abi.PREC_FP64, seed=12345):
+    def __init__(self, lib, box, skin, cell_grid, precision=_abi.PREC_FP64, seed=12345,
+                 half_cell_int=1):
         self.lib = lib
         self.h = ctypes.c_void_p()
         b = np.ascontiguousarray(box, np.float64)
         cg = np.ascontiguousarray(cell_grid, np.int32)
         call(lib, "espp_system_create", dptr(b), float(skin), i32ptr(cg), int(precision),
              int(seed), ctypes.byref(self.h))
+        if half_cell_int != 1:
+            call(lib, "espp_set_half_cell_int", self.h, int(half_cell_int))
 
     def __del__(self):
         try:
