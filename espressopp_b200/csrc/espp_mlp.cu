@@ -4,6 +4,7 @@
 #include <math.h>
 #include <stdint.h>
 
+#include "espp_device.h"
 #include "espp_mlp.h"
 #include "espp_tc.h"
 
@@ -21,9 +22,13 @@ constexpr int kOffB3 = kOffW3 + H;
 constexpr int kSiteTile = 16;  // sites per tile of the site kernel
 constexpr int kGradTile = 8;   // sites per tile of the gradient kernel
 constexpr int kGradBlocks = 296;
+constexpr int kMlpTpp = 4;  // threads per site in the pair loops (a site's list split 4 ways)
 
-__device__ __forceinline__ double mimg(double dx, double L, double hL) {
-  return dx < -hL ? dx + L : (dx > hL ? dx - L : dx);
+// sum over the kMlpTpp lanes of a site, in a fixed order
+__device__ __forceinline__ float tpp_sum(float v) {
+#pragma unroll
+  for (int o = 1; o < kMlpTpp; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
 }
 
 __device__ __forceinline__ float sigm(float z) { return 1.0f / (1.0f + expf(-z)); }
@@ -44,19 +49,6 @@ __device__ __forceinline__ float silu2(float z) {
   return s * (1.0f - s) * (2.0f + z * (1.0f - 2.0f * s));
 }
 
-// Pair vector d = x_i - x_j (minimum image, FP64) and r^2.
-__device__ __forceinline__ double pair_d(const DevView& d, const double* X, int i, int j,
-                                         float& dx, float& dy, float& dz) {
-  const size_t c = d.cap;
-  const double ex = mimg(X[i] - X[j], d.L[0], d.halfL[0]);
-  const double ey = mimg(X[c + i] - X[c + j], d.L[1], d.halfL[1]);
-  const double ez = mimg(X[2 * c + i] - X[2 * c + j], d.L[2], d.halfL[2]);
-  dx = (float)ex;
-  dy = (float)ey;
-  dz = (float)ez;
-  return ex * ex + ey * ey + ez * ez;
-}
-
 // basis values g[k] (gp == nullptr) or derivatives gp[k] = dg_k/dr at distance r < rc;
 // FAST takes the fast exponential (for the BF16 tensor-core network, whose operand
 // rounding dominates the error)
@@ -75,30 +67,79 @@ __device__ __forceinline__ void rbf(const MlpDev& m, float r, float* g, float* g
   }
 }
 
+// The same basis for the tensor-core mode, without one exponential per function: with
+// u = (r - r0) / dmu and gamma dmu^2 = 1/2, g_k = exp(-(u - k)^2 / 2) fc and
+// g_{k+1} / g_k = exp(u - k) exp(-1/2), so e_{k+1} = e_k a_k c, a_{k+1} = a_k b
+// (c = exp(-1/2), b = exp(-1)).  The recurrence starts afresh at k = 0 and k = K/2, so
+// no start value underflows where the functions it feeds are not negligible; 4 fast
+// exponentials and 2 products a function instead of 16 exponentials.  g or gp may be null.
+__device__ __forceinline__ void rbf_rec(const MlpDev& m, float r, float inv_dmu, float* g,
+                                        float* gp) {
+  float sn, cs;
+  sincospif(r / m.rc, &sn, &cs);
+  const float fc = 0.5f * (cs + 1.0f);
+  const float dfc = -0.5f * 3.14159265358979f / m.rc * sn;
+  const float u = (r - m.r0) * inv_dmu;
+  const float c = 0.60653065971f, b = 0.36787944117f;  // exp(-1/2), exp(-1)
+#pragma unroll
+  for (int h = 0; h < K; h += K / 2) {
+    const float uh = u - (float)h;
+    float e = __expf(-0.5f * uh * uh);
+    float a = __expf(uh);
+#pragma unroll
+    for (int k = h; k < h + K / 2; ++k) {
+      if (g) g[k] = e * fc;
+      if (gp) gp[k] = e * (dfc - (u - (float)k) * inv_dmu * fc);
+      e = e * a * c;
+      a = a * b;
+    }
+  }
+}
+
+// Pair vector d = x_i - x_j from the box-wrapped int32 coordinates (the minimum image is
+// the 32-bit wrap of the exact integer difference) and r^2 in FP32.
+__device__ __forceinline__ float pair_q(const DevView& d, const int4 pi, int j, float& dx,
+                                        float& dy, float& dz) {
+  const int4 pj = __ldg(&d.posq[j]);
+  dx = wrapped_diff(pi.x, pj.x, d.fixUnit[0]);
+  dy = wrapped_diff(pi.y, pj.y, d.fixUnit[1]);
+  dz = wrapped_diff(pi.z, pj.z, d.fixUnit[2]);
+  return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+}
+
 // G_i = sum_j g(r_ij) over the list partners within rc.
 template <bool FAST>
 __global__ void k_mlp_desc(DevView d) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.n) return;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int sub = gt % kMlpTpp;
+  const bool act = gt / kMlpTpp < d.n;
+  const int i = act ? gt / kMlpTpp : 0;  // every lane stays for the sums
   const MlpDev m = d.mlp;
-  const double* X = d.pa[0].x;
-  const double rc2 = (double)m.rc * (double)m.rc;
+  const float rc2 = m.rc * m.rc, inv_dmu = 1.0f / m.dmu;
+  const int4 pi = d.posq[i];
   float G[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) G[k] = 0.f;
-  const int cnt = d.nn[i];
-  for (int q = 0; q < cnt; ++q) {
+  const int cnt = act ? d.nn[i] : 0;
+  for (int q = sub; q < cnt; q += kMlpTpp) {
     const int j = d.nl[nl_index(q, i, d.cap)];
     float dx, dy, dz;
-    const double r2 = pair_d(d, X, i, j, dx, dy, dz);
+    const float r2 = pair_q(d, pi, j, dx, dy, dz);
     if (!(r2 < rc2) || j == i) continue;
     float g[K];
-    rbf<FAST>(m, sqrtf((float)r2), g, nullptr);
+    if (FAST)
+      rbf_rec(m, sqrtf(r2), inv_dmu, g, nullptr);
+    else
+      rbf<false>(m, sqrtf(r2), g, nullptr);
 #pragma unroll
     for (int k = 0; k < K; ++k) G[k] += g[k];
   }
 #pragma unroll
-  for (int k = 0; k < K; ++k) m.G[(size_t)i * K + k] = G[k];
+  for (int k = 0; k < K; ++k) G[k] = tpp_sum(G[k]);
+  if (act && sub == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) m.G[(size_t)i * K + k] = G[k];
+  }
 }
 
 // Site network on CUDA cores: block of H threads (one per hidden unit), tiles of
@@ -173,24 +214,29 @@ __device__ __forceinline__ long long mlp_fix(float f, unsigned* err) {
 // F_i = -sum_j phi_ij d_ij / r_ij, phi_ij = sum_k (D_ik + D_jk) g'_k(r_ij).
 template <bool MIXED, bool FAST>
 __global__ void k_mlp_force(DevView d, float* fout) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.n) return;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int sub = gt % kMlpTpp;
+  const bool act = gt / kMlpTpp < d.n;
+  const int i = act ? gt / kMlpTpp : 0;  // every lane stays for the sums
   const MlpDev m = d.mlp;
-  const double* X = d.pa[0].x;
-  const double rc2 = (double)m.rc * (double)m.rc;
+  const float rc2 = m.rc * m.rc, inv_dmu = 1.0f / m.dmu;
+  const int4 pi = d.posq[i];
   float Di[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) Di[k] = m.D[(size_t)i * K + k];
   float fx = 0.f, fy = 0.f, fz = 0.f;
-  const int cnt = d.nn[i];
-  for (int q = 0; q < cnt; ++q) {
+  const int cnt = act ? d.nn[i] : 0;
+  for (int q = sub; q < cnt; q += kMlpTpp) {
     const int j = d.nl[nl_index(q, i, d.cap)];
     float dx, dy, dz;
-    const double r2 = pair_d(d, X, i, j, dx, dy, dz);
+    const float r2 = pair_q(d, pi, j, dx, dy, dz);
     if (!(r2 < rc2) || j == i) continue;
-    const float r = sqrtf((float)r2);
+    const float r = sqrtf(r2);
     float gp[K];
-    rbf<FAST>(m, r, nullptr, gp);
+    if (FAST)
+      rbf_rec(m, r, inv_dmu, nullptr, gp);
+    else
+      rbf<false>(m, r, nullptr, gp);
     const float4* Dj = reinterpret_cast<const float4*>(m.D + (size_t)j * K);
     float phi = 0.f;
 #pragma unroll
@@ -204,6 +250,10 @@ __global__ void k_mlp_force(DevView d, float* fout) {
     fy -= s * dy;
     fz -= s * dz;
   }
+  fx = tpp_sum(fx);
+  fy = tpp_sum(fy);
+  fz = tpp_sum(fz);
+  if (!act || sub != 0) return;
   const size_t c = d.cap;
   if (fout) {
     fout[3 * (size_t)i] = fx;
@@ -270,32 +320,42 @@ __global__ void __launch_bounds__(256) k_mlp_fm_err(int n, const float* fm, cons
 }
 
 // tangent of the site networks: xdot_i[k] = -scale[k] sum_j g'_k(r_ij) (e_i - e_j).d_ij/r_ij
+template <bool FAST>
 __global__ void k_mlp_vpass(DevView d, const float* err, float* tangent) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.n) return;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int sub = gt % kMlpTpp;
+  const bool act = gt / kMlpTpp < d.n;
+  const int i = act ? gt / kMlpTpp : 0;  // every lane stays for the sums
   const MlpDev m = d.mlp;
-  const double* X = d.pa[0].x;
-  const double rc2 = (double)m.rc * (double)m.rc;
+  const float rc2 = m.rc * m.rc, inv_dmu = 1.0f / m.dmu;
+  const int4 pi = d.posq[i];
   const float ex = err[3 * (size_t)i], ey = err[3 * (size_t)i + 1], ez = err[3 * (size_t)i + 2];
   float v[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) v[k] = 0.f;
-  const int cnt = d.nn[i];
-  for (int q = 0; q < cnt; ++q) {
+  const int cnt = act ? d.nn[i] : 0;
+  for (int q = sub; q < cnt; q += kMlpTpp) {
     const int j = d.nl[nl_index(q, i, d.cap)];
     float dx, dy, dz;
-    const double r2 = pair_d(d, X, i, j, dx, dy, dz);
+    const float r2 = pair_q(d, pi, j, dx, dy, dz);
     if (!(r2 < rc2) || j == i) continue;
-    const float r = sqrtf((float)r2);
+    const float r = sqrtf(r2);
     float gp[K];
-    rbf(m, r, nullptr, gp);
+    if (FAST)
+      rbf_rec(m, r, inv_dmu, nullptr, gp);
+    else
+      rbf<false>(m, r, nullptr, gp);
     const float proj = ((ex - err[3 * (size_t)j]) * dx + (ey - err[3 * (size_t)j + 1]) * dy +
                         (ez - err[3 * (size_t)j + 2]) * dz) / r;
 #pragma unroll
     for (int k = 0; k < K; ++k) v[k] += gp[k] * proj;
   }
 #pragma unroll
-  for (int k = 0; k < K; ++k) tangent[(size_t)i * K + k] = -v[k] * m.scale[k];
+  for (int k = 0; k < K; ++k) v[k] = tpp_sum(v[k]);
+  if (act && sub == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) tangent[(size_t)i * K + k] = -v[k] * m.scale[k];
+  }
 }
 
 // Weight gradient of sum_i d/dt E_i(x_i + t xdot_i) at t = 0 (forward-over-reverse):
@@ -438,9 +498,9 @@ int launch_mlp_grad_tc(const DevView& d, const float* tangent, float* partials, 
 void launch_mlp_energy_terms(const DevView& d, cudaStream_t st) {
   if (d.n == 0) return;
   if (d.mlp.tc)
-    k_mlp_desc<true><<<(d.n + 255) / 256, 256, 0, st>>>(d);
+    k_mlp_desc<true><<<(d.n * kMlpTpp + 255) / 256, 256, 0, st>>>(d);
   else
-    k_mlp_desc<false><<<(d.n + 255) / 256, 256, 0, st>>>(d);
+    k_mlp_desc<false><<<(d.n * kMlpTpp + 255) / 256, 256, 0, st>>>(d);
   if (d.mlp.tc) {
     launch_mlp_site_tc(d, st);
   } else {
@@ -452,7 +512,7 @@ void launch_mlp_energy_terms(const DevView& d, cudaStream_t st) {
 void launch_mlp_forces(const DevView& d, bool mixed, float* fout, cudaStream_t st) {
   if (d.n == 0 || !d.mlp.on) return;
   launch_mlp_energy_terms(d, st);
-  const unsigned nb = (d.n + 255) / 256;
+  const unsigned nb = (d.n * kMlpTpp + 255) / 256;
   if (mixed)
     d.mlp.tc ? k_mlp_force<true, true><<<nb, 256, 0, st>>>(d, fout)
              : k_mlp_force<true, false><<<nb, 256, 0, st>>>(d, fout);
@@ -473,7 +533,10 @@ void launch_mlp_fm_grad(const DevView& d, const float* fmodel, const double* fre
                         cudaStream_t st) {
   k_mlp_fm_err<<<nloss_blocks, 256, 0, st>>>(d.n, fmodel, fref, err, loss_partials);
   k_sum_blocks<<<1, 256, 0, st>>>(loss_partials, nloss_blocks, loss_out);
-  k_mlp_vpass<<<(d.n + 255) / 256, 256, 0, st>>>(d, err, tangent);
+  if (d.mlp.tc)
+    k_mlp_vpass<true><<<(d.n * kMlpTpp + 255) / 256, 256, 0, st>>>(d, err, tangent);
+  else
+    k_mlp_vpass<false><<<(d.n * kMlpTpp + 255) / 256, 256, 0, st>>>(d, err, tangent);
   if (d.mlp.tc) {
     // the weight-gradient products on the tensor cores
     const int nb = launch_mlp_grad_tc(d, tangent, partials, npart_blocks, st);
