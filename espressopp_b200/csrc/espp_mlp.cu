@@ -673,6 +673,21 @@ __device__ __forceinline__ void store_row64(uint8_t* base, int r, const float* v
   }
 }
 
+// writes 32 values of row r, columns c0 .. c0 + 31, into a canonical 128-row operand
+__device__ __forceinline__ void store_row32(uint8_t* base, int r, int c0, const float* v) {
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    uint4 q;
+    q.x = pack_bf16(v[8 * c + 0], v[8 * c + 1]);
+    q.y = pack_bf16(v[8 * c + 2], v[8 * c + 3]);
+    q.z = pack_bf16(v[8 * c + 4], v[8 * c + 5]);
+    q.w = pack_bf16(v[8 * c + 6], v[8 * c + 7]);
+    *reinterpret_cast<uint4*>(base + canon_off(r, c0 + 8 * c, kTcRows)) = q;
+  }
+}
+
+constexpr int kTcThreads = 2 * kTcRows;  // site network: two threads a row (32 columns each)
+
 struct TcSmem {
   alignas(128) uint8_t P[kTcRows * H * 2];  // X (first 4 KB), then H1, then P1
   alignas(128) uint8_t Q[kTcRows * H * 2];  // P2
@@ -681,42 +696,48 @@ struct TcSmem {
   alignas(128) uint8_t W2T[H * H * 2];      // B of G1: W2^T
   alignas(128) uint8_t W1T[K * H * 2];      // B of DX: W1^T [16 x 64]
   float b1[H], b2[H], w3[H], scale[K], shift[K];
+  float epart[kTcRows];  // energy of each row's upper 32 hidden units
   alignas(8) unsigned long long mbar;
   uint32_t tmem;
   int abort;
 };
 
-__global__ void __launch_bounds__(kTcRows) k_mlp_site_tc(MlpDev m, int n, unsigned* err) {
+// Thread t serves row t % 128 (TMEM lane) and, in each 64-column phase, columns
+// 32 (t / 128) .. + 31: warps w and w + 4 read the same lanes, so 8 warps share the
+// epilogues of one 128-site tile.
+__global__ void __launch_bounds__(kTcThreads) k_mlp_site_tc(MlpDev m, int n, unsigned* err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   TcSmem& S = *reinterpret_cast<TcSmem*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  const int t = threadIdx.x;
-  const int warp = t >> 5;
+  const int tid = threadIdx.x;
+  const int t = tid & (kTcRows - 1);  // tile row (TMEM lane)
+  const int hf = tid >> 7;            // column half
+  const int warp = tid >> 5;
   const float* th = m.theta;
   // weights as BF16 operands
-  for (int e = t; e < H * K; e += kTcRows) {
+  for (int e = tid; e < H * K; e += kTcThreads) {
     const int o = e / K, k = e % K;  // W1[o][k]
     const __nv_bfloat16 v = __float2bfloat16_rn(th[e]);
     *reinterpret_cast<__nv_bfloat16*>(S.W1 + canon_off(o, k, H)) = v;
     *reinterpret_cast<__nv_bfloat16*>(S.W1T + canon_off(k, o, K)) = v;
   }
-  for (int e = t; e < H * H; e += kTcRows) {
+  for (int e = tid; e < H * H; e += kTcThreads) {
     const int o = e / H, u = e % H;  // W2[o][u]
     const __nv_bfloat16 v = __float2bfloat16_rn(th[kOffW2 + e]);
     *reinterpret_cast<__nv_bfloat16*>(S.W2 + canon_off(o, u, H)) = v;
     *reinterpret_cast<__nv_bfloat16*>(S.W2T + canon_off(u, o, H)) = v;
   }
-  if (t < H) {
+  if (tid < H) {
     S.b1[t] = th[kOffB1 + t];
     S.b2[t] = th[kOffB2 + t];
     S.w3[t] = th[kOffW3 + t];
   }
-  if (t < K) {
+  if (tid < K) {
     S.scale[t] = m.scale[t];
     S.shift[t] = m.shift[t];
   }
   const float b3 = th[kOffB3];
   const uint32_t mbar = smem_u32(&S.mbar);
-  if (t == 0) {
+  if (tid == 0) {
     S.abort = 0;
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -732,7 +753,8 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_site_tc(MlpDev m, int n, unsign
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = S.tmem;
-  const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's lanes
+  const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);  // this warp's lanes
+  const int c0 = 32 * hf;  // this thread's first column in a 64-column phase
   const uint32_t aP = smem_u32(S.P), aQ = smem_u32(S.Q);
   const uint32_t aW1 = smem_u32(S.W1), aW2 = smem_u32(S.W2), aW2T = smem_u32(S.W2T),
                  aW1T = smem_u32(S.W1T);
@@ -747,27 +769,26 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_site_tc(MlpDev m, int n, unsign
   };
   for (int s0 = blockIdx.x * kTcRows; s0 < n; s0 += gridDim.x * kTcRows) {
     const int i = s0 + t;
-    // X tile: 16 normalised descriptor values of site row t (zeros past n)
+    // X tile: 16 normalised descriptor values of site row t (zeros past n), 8 a thread
     {
-      float x[16];
+      float x[8];
 #pragma unroll
-      for (int k = 0; k < K; ++k)
-        x[k] = i < n ? (m.G[(size_t)i * K + k] - S.shift[k]) * S.scale[k] : 0.f;
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        uint4 q;
-        q.x = pack_bf16(x[8 * c + 0], x[8 * c + 1]);
-        q.y = pack_bf16(x[8 * c + 2], x[8 * c + 3]);
-        q.z = pack_bf16(x[8 * c + 4], x[8 * c + 5]);
-        q.w = pack_bf16(x[8 * c + 6], x[8 * c + 7]);
-        *reinterpret_cast<uint4*>(S.P + canon_off(t, 8 * c, kTcRows)) = q;
+      for (int k = 0; k < 8; ++k) {
+        const int kk = 8 * hf + k;
+        x[k] = i < n ? (m.G[(size_t)i * K + kk] - S.shift[kk]) * S.scale[kk] : 0.f;
       }
+      uint4 q;
+      q.x = pack_bf16(x[0], x[1]);
+      q.y = pack_bf16(x[2], x[3]);
+      q.z = pack_bf16(x[4], x[5]);
+      q.w = pack_bf16(x[6], x[7]);
+      *reinterpret_cast<uint4*>(S.P + canon_off(t, 8 * hf, kTcRows)) = q;
     }
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
     if (S.abort) break;
-    if (t == 0) {
+    if (tid == 0) {
       tc_fence_after();
       umma(tmem + 0, umma_desc(aP, kTcRows), umma_desc(aW1, H), umma_idesc(H), 0);
       umma_commit(mbar);
@@ -775,19 +796,19 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_site_tc(MlpDev m, int n, unsign
     wait_mma();
     // H1 = silu(Z1 + b1)
     {
-      float v[H];
-#pragma unroll
-      for (int q = 0; q < H / 16; ++q) tmem_ld16(tl + 0 + 16 * q, v + 16 * q);
+      float v[32];
+      tmem_ld16(tl + c0, v);
+      tmem_ld16(tl + c0 + 16, v + 16);
       tmem_wait_ld();
 #pragma unroll
-      for (int u = 0; u < H; ++u) v[u] = silu_fast(v[u] + S.b1[u]);
-      store_row64(S.P, t, v);
+      for (int u = 0; u < 32; ++u) v[u] = silu_fast(v[u] + S.b1[c0 + u]);
+      store_row32(S.P, t, c0, v);
     }
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
     if (S.abort) break;
-    if (t == 0) {
+    if (tid == 0) {
       tc_fence_after();
 #pragma unroll
       for (int kb = 0; kb < H / 16; ++kb)
@@ -796,27 +817,29 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_site_tc(MlpDev m, int n, unsign
       umma_commit(mbar);
     }
     wait_mma();
-    // E and P2 = w3 * silu'(Z2 + b2)
+    // E and P2 = w3 * silu'(Z2 + b2); the upper half's energy joins through shared memory
     {
-      float v[H];
-#pragma unroll
-      for (int q = 0; q < H / 16; ++q) tmem_ld16(tl + 64 + 16 * q, v + 16 * q);
+      float v[32];
+      tmem_ld16(tl + 64 + c0, v);
+      tmem_ld16(tl + 64 + c0 + 16, v + 16);
       tmem_wait_ld();
-      float e = b3;
+      float e = 0.f;
 #pragma unroll
-      for (int u = 0; u < H; ++u) {
-        const float z = v[u] + S.b2[u];
-        e += S.w3[u] * silu_fast(z);
-        v[u] = S.w3[u] * silu1_fast(z);
+      for (int u = 0; u < 32; ++u) {
+        const float z = v[u] + S.b2[c0 + u];
+        e += S.w3[c0 + u] * silu_fast(z);
+        v[u] = S.w3[c0 + u] * silu1_fast(z);
       }
-      if (i < n) m.E[i] = e;
-      store_row64(S.Q, t, v);
+      if (hf) S.epart[t] = e;
+      store_row32(S.Q, t, c0, v);
+      __syncthreads();
+      if (!hf && i < n) m.E[i] = (b3 + e) + S.epart[t];
     }
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
     if (S.abort) break;
-    if (t == 0) {
+    if (tid == 0) {
       tc_fence_after();
 #pragma unroll
       for (int kb = 0; kb < H / 16; ++kb)
@@ -827,22 +850,21 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_site_tc(MlpDev m, int n, unsign
     wait_mma();
     // P1 = G1 * silu'(Z1 + b1)
     {
-      float g[H], z[H];
-#pragma unroll
-      for (int q = 0; q < H / 16; ++q) {
-        tmem_ld16(tl + 128 + 16 * q, g + 16 * q);
-        tmem_ld16(tl + 0 + 16 * q, z + 16 * q);
-      }
+      float g[32], z[32];
+      tmem_ld16(tl + 128 + c0, g);
+      tmem_ld16(tl + 128 + c0 + 16, g + 16);
+      tmem_ld16(tl + c0, z);
+      tmem_ld16(tl + c0 + 16, z + 16);
       tmem_wait_ld();
 #pragma unroll
-      for (int u = 0; u < H; ++u) g[u] *= silu1_fast(z[u] + S.b1[u]);
-      store_row64(S.P, t, g);
+      for (int u = 0; u < 32; ++u) g[u] *= silu1_fast(z[u] + S.b1[c0 + u]);
+      store_row32(S.P, t, c0, g);
     }
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
     if (S.abort) break;
-    if (t == 0) {
+    if (tid == 0) {
       tc_fence_after();
 #pragma unroll
       for (int kb = 0; kb < H / 16; ++kb)
@@ -855,7 +877,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_site_tc(MlpDev m, int n, unsign
       float dx[16];
       tmem_ld16(tl + 192, dx);
       tmem_wait_ld();
-      if (i < n) {
+      if (!hf && i < n) {
         float4* o = reinterpret_cast<float4*>(m.D + (size_t)i * K);
 #pragma unroll
         for (int q = 0; q < 4; ++q)
@@ -871,7 +893,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_site_tc(MlpDev m, int n, unsign
   __syncthreads();
   // after a timed-out wait, give the outstanding product its own bounded wait before the
   // tensor memory is released
-  if (S.abort && t == 0) mbar_wait(mbar, phase);
+  if (S.abort && tid == 0) mbar_wait(mbar, phase);
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
@@ -1263,7 +1285,7 @@ void launch_mlp_site_tc(const DevView& d, cudaStream_t st) {
   }
   const int tiles = (d.n + kTcRows - 1) / kTcRows;
   const int grid = tiles < 2 * nsm[dev] ? tiles : 2 * nsm[dev];
-  if (grid > 0) k_mlp_site_tc<<<grid, kTcRows, mlp_tc_smem(), st>>>(d.mlp, d.n, d.err);
+  if (grid > 0) k_mlp_site_tc<<<grid, kTcThreads, mlp_tc_smem(), st>>>(d.mlp, d.n, d.err);
 }
 
 }  // namespace espp
