@@ -961,33 +961,38 @@ __device__ __forceinline__ void store_row16(uint8_t* base, int r, const float* v
   }
 }
 
-__global__ void __launch_bounds__(kTcRows) k_mlp_grad_tc(MlpDev m, int n, const float* tangent,
-                                                          float* partials, unsigned* err) {
+// Thread t serves row t % 128 (TMEM lane) and columns 32 (t / 128) .. + 31 of each
+// 64-column phase (warps w and w + 4 read the same lanes).
+__global__ void __launch_bounds__(kTcThreads) k_mlp_grad_tc(MlpDev m, int n, const float* tangent,
+                                                            float* partials, unsigned* err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   GtSmem& S = *reinterpret_cast<GtSmem*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  const int t = threadIdx.x;
-  const int warp = t >> 5;
+  const int tid = threadIdx.x;
+  const int t = tid & (kTcRows - 1);  // tile row (TMEM lane)
+  const int hf = tid >> 7;            // column half
+  const int c0 = 32 * hf;             // first column of this thread in a 64-column phase
+  const int warp = tid >> 5;
   const float* th = m.theta;
-  for (int e = t; e < H * K; e += kTcRows) {
+  for (int e = tid; e < H * K; e += kTcThreads) {
     const int o = e / K, k = e % K;  // W1[o][k]
     store_bf16(S.W1, o, k, H, th[e]);
   }
-  for (int e = t; e < H * H; e += kTcRows) {
+  for (int e = tid; e < H * H; e += kTcThreads) {
     const int o = e / H, u = e % H;  // W2[o][u]
     store_bf16(S.W2, o, u, H, th[kOffW2 + e]);
     store_bf16(S.W2T, u, o, H, th[kOffW2 + e]);
   }
-  if (t < H) {
+  if (tid < H) {
     S.b1[t] = th[kOffB1 + t];
     S.b2[t] = th[kOffB2 + t];
     S.w3[t] = th[kOffW3 + t];
   }
-  if (t < K) {
+  if (tid < K) {
     S.scale[t] = m.scale[t];
     S.shift[t] = m.shift[t];
   }
   const uint32_t mbar = smem_u32(&S.mbar);
-  if (t == 0) {
+  if (tid == 0) {
     S.abort = 0;
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -1003,7 +1008,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_grad_tc(MlpDev m, int n, const 
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = S.tmem;
-  const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's lanes
+  const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);  // this warp's lanes
   const uint32_t aX = smem_u32(S.X), aXd = smem_u32(S.Xd), aXT = smem_u32(S.XT),
                  aXdT = smem_u32(S.XdT), aH1 = smem_u32(S.H1), aHd1 = smem_u32(S.Hd1),
                  aH1T = smem_u32(S.H1T), aHd1T = smem_u32(S.Hd1T), aA2 = smem_u32(S.A2),
@@ -1027,7 +1032,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_grad_tc(MlpDev m, int n, const 
   // column sums of S.F over the tile's rows (fixed order): thread u < H adds column u
   auto colsum = [&](float& acc) {
     __syncthreads();
-    if (t < H) {
+    if (tid < H) {
       float c = 0.f;
       for (int r = 0; r < kTcRows; ++r) c += S.F[r][t];
       acc += c;
@@ -1039,23 +1044,20 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_grad_tc(MlpDev m, int n, const 
   for (int s0 = blockIdx.x * kTcRows; s0 < n; s0 += gridDim.x * kTcRows) {
     const int i = s0 + t;
     {
-      float x[K], xd[K];
+      // the lower half writes X (and its transpose), the upper half the tangent Xd
+      float x[K];
 #pragma unroll
-      for (int k = 0; k < K; ++k) {
-        x[k] = i < n ? (m.G[(size_t)i * K + k] - S.shift[k]) * S.scale[k] : 0.f;
-        xd[k] = i < n ? tangent[(size_t)i * K + k] : 0.f;
-      }
-      store_row16(S.X, t, x);
-      store_row16(S.Xd, t, xd);
+      for (int k = 0; k < K; ++k)
+        x[k] = i >= n ? 0.f
+                      : (hf ? tangent[(size_t)i * K + k]
+                            : (m.G[(size_t)i * K + k] - S.shift[k]) * S.scale[k]);
+      store_row16(hf ? S.Xd : S.X, t, x);
 #pragma unroll
-      for (int k = 0; k < K; ++k) {
-        store_bf16(S.XT, k, t, K, x[k]);
-        store_bf16(S.XdT, k, t, K, xd[k]);
-      }
+      for (int k = 0; k < K; ++k) store_bf16(hf ? S.XdT : S.XT, k, t, K, x[k]);
     }
     sync_for_mma();
     if (S.abort) break;
-    if (t == 0) {
+    if (tid == 0) {
       tc_fence_after();
       umma(tmem + 0, umma_desc(aX, kTcRows), umma_desc(aW1, H), umma_idesc(H), 0);
       umma(tmem + 64, umma_desc(aXd, kTcRows), umma_desc(aW1, H), umma_idesc(H), 0);
@@ -1064,30 +1066,30 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_grad_tc(MlpDev m, int n, const 
     wait_mma();
     // H1, Hd1
     {
-      float z[H], zd[H];
+      float z[32], zd[32];
 #pragma unroll
-      for (int q = 0; q < H / 16; ++q) {
-        tmem_ld16(tl + 0 + 16 * q, z + 16 * q);
-        tmem_ld16(tl + 64 + 16 * q, zd + 16 * q);
+      for (int q = 0; q < 2; ++q) {
+        tmem_ld16(tl + 0 + c0 + 16 * q, z + 16 * q);
+        tmem_ld16(tl + 64 + c0 + 16 * q, zd + 16 * q);
       }
       tmem_wait_ld();
 #pragma unroll
-      for (int u = 0; u < H; ++u) {
-        const float zz = z[u] + S.b1[u];
+      for (int u = 0; u < 32; ++u) {
+        const float zz = z[u] + S.b1[c0 + u];
         z[u] = silu(zz);
         zd[u] = silu1(zz) * zd[u];
       }
-      store_row64(S.H1, t, z);
-      store_row64(S.Hd1, t, zd);
+      store_row32(S.H1, t, c0, z);
+      store_row32(S.Hd1, t, c0, zd);
 #pragma unroll
-      for (int u = 0; u < H; ++u) {
-        store_bf16(S.H1T, u, t, H, z[u]);
-        store_bf16(S.Hd1T, u, t, H, zd[u]);
+      for (int u = 0; u < 32; ++u) {
+        store_bf16(S.H1T, c0 + u, t, H, z[u]);
+        store_bf16(S.Hd1T, c0 + u, t, H, zd[u]);
       }
     }
     sync_for_mma();
     if (S.abort) break;
-    if (t == 0) {
+    if (tid == 0) {
       tc_fence_after();
 #pragma unroll
       for (int kb = 0; kb < H / 16; ++kb) {
@@ -1101,40 +1103,41 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_grad_tc(MlpDev m, int n, const 
     wait_mma();
     // az2 = w3 zd2 silu''(z2), azd2 = w3 silu'(z2); rows for gb2 and gw3
     {
-      float z[H], zd[H];
+      float z[32], zd[32];
 #pragma unroll
-      for (int q = 0; q < H / 16; ++q) {
-        tmem_ld16(tl + 128 + 16 * q, z + 16 * q);
-        tmem_ld16(tl + 192 + 16 * q, zd + 16 * q);
+      for (int q = 0; q < 2; ++q) {
+        tmem_ld16(tl + 128 + c0 + 16 * q, z + 16 * q);
+        tmem_ld16(tl + 192 + c0 + 16 * q, zd + 16 * q);
       }
       tmem_wait_ld();
       const bool live = i < n;
 #pragma unroll
-      for (int u = 0; u < H; ++u) {
-        const float zz = z[u] + S.b2[u];
+      for (int u = 0; u < 32; ++u) {
+        const int c = c0 + u;
+        const float zz = z[u] + S.b2[c];
         const float s1 = silu1(zz);
         const float q = live ? s1 * zd[u] : 0.f;       // gw3 term
-        const float az = live ? S.w3[u] * zd[u] * silu2(zz) : 0.f;
-        const float azd = live ? S.w3[u] * s1 : 0.f;
+        const float az = live ? S.w3[c] * zd[u] * silu2(zz) : 0.f;
+        const float azd = live ? S.w3[c] * s1 : 0.f;
         z[u] = az;
         zd[u] = azd;
-        S.F[t][u] = q;
+        S.F[t][c] = q;
       }
-      store_row64(S.A2, t, z);
-      store_row64(S.Ad2, t, zd);
+      store_row32(S.A2, t, c0, z);
+      store_row32(S.Ad2, t, c0, zd);
 #pragma unroll
-      for (int u = 0; u < H; ++u) {
-        store_bf16(S.AT, u, t, 2 * H, z[u]);
-        store_bf16(S.AT, H + u, t, 2 * H, zd[u]);
+      for (int u = 0; u < 32; ++u) {
+        store_bf16(S.AT, c0 + u, t, 2 * H, z[u]);
+        store_bf16(S.AT, H + c0 + u, t, 2 * H, zd[u]);
       }
       colsum(gw3);
 #pragma unroll
-      for (int u = 0; u < H; ++u) S.F[t][u] = z[u];
+      for (int u = 0; u < 32; ++u) S.F[t][c0 + u] = z[u];
       colsum(gb2);
     }
     sync_for_mma();
     if (S.abort) break;
-    if (t == 0) {
+    if (tid == 0) {
       tc_fence_after();
 #pragma unroll
       for (int kb = 0; kb < H / 16; ++kb) {
@@ -1155,30 +1158,31 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_grad_tc(MlpDev m, int n, const 
     wait_mma();
     // az1 = ah1 silu'(z1) + ahd1 zd1 silu''(z1), azd1 = ahd1 silu'(z1)
     {
-      float ah[H], ahd[H], z[H], zd[H];
+      float ah[32], ahd[32], z[32], zd[32];
 #pragma unroll
-      for (int q = 0; q < H / 16; ++q) {
-        tmem_ld16(tl + 128 + 16 * q, ah + 16 * q);
-        tmem_ld16(tl + 192 + 16 * q, ahd + 16 * q);
-        tmem_ld16(tl + 0 + 16 * q, z + 16 * q);
-        tmem_ld16(tl + 64 + 16 * q, zd + 16 * q);
+      for (int q = 0; q < 2; ++q) {
+        tmem_ld16(tl + 128 + c0 + 16 * q, ah + 16 * q);
+        tmem_ld16(tl + 192 + c0 + 16 * q, ahd + 16 * q);
+        tmem_ld16(tl + 0 + c0 + 16 * q, z + 16 * q);
+        tmem_ld16(tl + 64 + c0 + 16 * q, zd + 16 * q);
       }
       tmem_wait_ld();
 #pragma unroll
-      for (int u = 0; u < H; ++u) {
-        const float zz = z[u] + S.b1[u];
+      for (int u = 0; u < 32; ++u) {
+        const int c = c0 + u;
+        const float zz = z[u] + S.b1[c];
         const float s1 = silu1(zz);
         const float az = ah[u] * s1 + ahd[u] * zd[u] * silu2(zz);
         const float azd = ahd[u] * s1;
-        store_bf16(S.AT, u, t, 2 * H, az);
-        store_bf16(S.AT, H + u, t, 2 * H, azd);
-        S.F[t][u] = az;
+        store_bf16(S.AT, c, t, 2 * H, az);
+        store_bf16(S.AT, H + c, t, 2 * H, azd);
+        S.F[t][c] = az;
       }
       colsum(gb1);
     }
     sync_for_mma();
     if (S.abort) break;
-    if (t == 0) {
+    if (tid == 0) {
       tc_fence_after();
 #pragma unroll
       for (int kb = 0; kb < kTcRows / 16; ++kb) {
@@ -1196,7 +1200,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_grad_tc(MlpDev m, int n, const 
   }
   tc_fence_before();
   __syncthreads();
-  if (S.abort && t == 0) mbar_wait(mbar, phase);  // a bounded wait for the last product
+  if (S.abort && tid == 0) mbar_wait(mbar, phase);  // a bounded wait for the last product
   __syncthreads();
   tc_fence_after();
   // gradient rows: thread t < 64 holds rows t of D1 and D3, thread 64 + t rows 64 + t of
@@ -1215,14 +1219,14 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_grad_tc(MlpDev m, int n, const 
 #pragma unroll
       for (int k = 0; k < K; ++k) g1[k] = 0.f;
     }
-    if (t >= H) {
+    if (!hf && t >= H) {
 #pragma unroll
       for (int u = 0; u < H; ++u) S.F[t - H][u] = g2[u];
 #pragma unroll
       for (int k = 0; k < K; ++k) S.F[t][k] = g1[k];  // rows 64..127 of F
     }
     __syncthreads();
-    if (t < H) {
+    if (!hf && t < H) {
 #pragma unroll
       for (int u = 0; u < H; ++u) p[kOffW2 + t * H + u] = g2[u] + S.F[t][u];
 #pragma unroll
@@ -1231,7 +1235,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_grad_tc(MlpDev m, int n, const 
       p[kOffB2 + t] = gb2;
       p[kOffW3 + t] = gw3;
     }
-    if (t == 0) p[kOffB3] = 0.f;
+    if (tid == 0) p[kOffB3] = 0.f;
   }
   __syncthreads();
   if (warp == 0) {
@@ -1268,7 +1272,7 @@ int launch_mlp_grad_tc(const DevView& d, const float* tangent, float* partials, 
                        cudaStream_t st) {
   int nb = mlp_grad_tc_blocks(d.n);
   if (nb > maxblocks) nb = maxblocks;
-  k_mlp_grad_tc<<<nb, kTcRows, mlp_grad_tc_smem(), st>>>(d.mlp, d.n, tangent, partials, d.err);
+  k_mlp_grad_tc<<<nb, kTcThreads, mlp_grad_tc_smem(), st>>>(d.mlp, d.n, tangent, partials, d.err);
   return nb;
 }
 
