@@ -2,9 +2,10 @@
 //
 //  re-binning     k_fold_bin -> k_scan_cells -> k_scatter -> k_sort_in_cell -> k_gather
 //                 (storage::DomainDecomposition::decomposeRealParticles, one node)
-//  Verlet list    k_build_nl_lane:
-//                 FP32 test with the reference's FP64 ghost-shift arithmetic near the
-//                 cutoff, full per-particle list (VerletList::_rebuildUsingBuffers)
+//  Verlet list    k_build_nl_run (runs of 32 particles of a row of cells, candidates
+//                 filtered against the group's bounding box) / k_build_nl_lane (one warp
+//                 per cell): FP32 test with the reference's FP64 ghost-shift arithmetic
+//                 near the cutoff, full per-particle list (VerletList::_rebuildUsingBuffers)
 //  forces         k_force_mixed (FP32 on box-wrapped int32 coordinates, int64 2^-32
 //                 fixed-point output) / k_force_fp64 (plain FP64); LJ + FENE fused
 //  integrator     k_integrate: aftCalcF (Langevin, CapForce) + integrate2 of step n +

@@ -381,7 +381,8 @@ ESPP_API int espp_autotune(espp_system* s, int32_t* best_tpp, double ms[4]);
 ESPP_API int espp_set_half_cell_int(espp_system* s, int32_t h);
 /* List layout of the Verlet list and pair kernels (tuning of the GPU kernels; no
  * reference counterpart).  form 0: one global list per particle (sorted indices) built
- * one warp per cell, tpp (1, 2, 4, 8) threads per particle in the force kernel;
+ * by runs of 32 particles of a row of cells (one warp per cell where cells were binned
+ * at other positions), tpp (1, 2, 4, 8) threads per particle in the force kernel;
  * form 2: the same global list built by brick windows (brick[3] cells per brick edge,
  * 1..4, or all 0 to choose from the density); form 1: brick windows for the build and
  * the force kernels, one thread per particle with its list as 16-bit window indices.

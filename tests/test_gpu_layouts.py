@@ -1,7 +1,7 @@
 """Every list layout of the GPU path (espp_set_layout) against the FP64 oracle.
 
-Layouts: the global per-particle list built one warp per cell with 1, 2, 4 or 8 threads
-per particle in the force kernel (form 0); the same list built by brick windows (form 2);
+Layouts: the global per-particle list (built by runs of 32 particles) with 1, 2, 4 or 8
+threads per particle in the force kernel (form 0); the same list built by brick windows (form 2);
 brick windows for the build and the force kernels with 16-bit window-index lists (form 1),
 for several brick shapes.  For each: the sorted id-pair set equals the oracle's
 (VerletList.cpp:274-450), forces agree (FP64 1e-12, mixed 1e-5 relative RMS and 5e-3 of
