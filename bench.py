@@ -578,6 +578,7 @@ def kg_melt_config(lib, prec, nchains=200, nbeads=200, cap_steps=1000, steps=900
     steps cap the pair force (LennardJonesCapped, caprad 0.9) so that the growth overlaps
     relax while FENE keeps every bond below R0 (a cap on the total force would let bonds
     stretch past R0, where FENE turns repulsive); then `steps` more with plain WCA.
+    The list layout is the autotuner's choice at the start (before the timed steps).
     Returns device-timed throughput and end-state observables."""
     from espressopp_b200._abi import call, dptr, i32ptr, i64ptr
     from espressopp_b200.tools import topology
@@ -599,6 +600,7 @@ def kg_melt_config(lib, prec, nchains=200, nbeads=200, cap_steps=1000, steps=900
     call(lib, "espp_fene_set", h, 30.0, 0.0, 1.5, math.inf, 0.0)
     call(lib, "espp_integrator_set", h, 0.01)
     call(lib, "espp_langevin_set", h, 1, 0.5, 1.0, 0, None)
+    layout = _tune(lib, h, 10.0)
     ms = np.zeros(2)
     call(lib, "espp_run", h, cap_steps)
     call(lib, "espp_last_run_ms", h, dptr(ms))
@@ -619,20 +621,37 @@ def kg_melt_config(lib, prec, nchains=200, nbeads=200, cap_steps=1000, steps=900
     return {"value": n * (cap_steps + steps) / ((t_cap + t_run) * 1e-3),
             "ms_per_step": (t_cap + t_run) / (cap_steps + steps),
             "ms_per_step_capped": t_cap / cap_steps, "T_end": v2.value / (3 * n),
-            "fene_energy_per_bond": e.value / len(bonds), "max_bond": math.sqrt(mx.value)}
+            "fene_energy_per_bond": e.value / len(bonds), "max_bond": math.sqrt(mx.value),
+            "layout": layout}
 
 
 def lj32k_config(lib, prec, steps=1000):
     """LJ fluid 32^3 = 32,768 particles (the reference's CPU-runnable case): rho 0.8442,
-    rc 2.5, skin 0.3, dt 0.005, Langevin gamma 1 T 1, 1000 steps."""
+    rc 2.5, skin 0.3, dt 0.005, Langevin gamma 1 T 1, 1000 steps; the list layout is the
+    autotuner's choice (before the timed steps)."""
     from espressopp_b200._abi import call, dptr
     h = make_system(lib, 32, prec)[0]
     call(lib, "espp_langevin_set", h, 1, 1.0, 1.0, 0, None)
+    layout = _tune(lib, h, 6.0)
     call(lib, "espp_run", h, steps)
     ms = np.zeros(2)
     call(lib, "espp_last_run_ms", h, dptr(ms))
     lib.espp_system_destroy(h)
-    return {"value": 32768 * steps / (ms[1] * 1e-3), "ms_per_step": float(ms[1]) / steps}
+    return {"value": 32768 * steps / (ms[1] * 1e-3), "ms_per_step": float(ms[1]) / steps,
+            "layout": layout}
+
+
+def _tune(lib, h, steps_per_build):
+    """espp_autotune_layout on the system as it stands; the chosen layout as a dict."""
+    from espressopp_b200._abi import call, dptr, i32ptr
+    best = np.zeros(5, np.int32)
+    table = np.zeros((32, 8))
+    n = ctypes.c_int32(0)
+    call(lib, "espp_autotune_layout", h, steps_per_build, i32ptr(best), dptr(table), 32,
+         ctypes.byref(n))
+    names = {0: "global", 1: "brick", 2: "global-brick-build"}
+    return {"form": names[int(best[0])], "threads_per_particle": int(best[1]),
+            "brick": [int(x) for x in best[2:5]]}
 
 
 def _plain(o):
