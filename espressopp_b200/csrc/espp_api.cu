@@ -3006,7 +3006,8 @@ int espp_autotune_layout(espp_system* s, double steps_per_build, int32_t best[5]
     };
     std::vector<Cand> cands;
     for (int t : {1, 2, 4, 8}) cands.push_back({0, t, {0, 0, 0}});
-    if (brick_geometry_ok(s)) cands.push_back({2, 1, {0, 0, 0}});
+    if (brick_geometry_ok(s))
+      for (int t : {1, 2, 4}) cands.push_back({2, t, {0, 0, 0}});
     const bool brickable = [&] {
       const bool was = s->brickAllowed;
       s->brickAllowed = true;
