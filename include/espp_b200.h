@@ -76,8 +76,9 @@ ESPP_API size_t espp_last_error(char* buf, size_t cap);
 /* ---- System + bc::OrthorhombicBC + storage::DomainDecomposition -------------------
  * Replaces System (src/System.cpp:40-105), OrthorhombicBC::setBoxL
  * (src/bc/OrthorhombicBC.cpp:40-50) and the DomainDecomposition constructor
- * (src/storage/DomainDecomposition.cpp:70-85) on one node: nodeGrid = (1,1,1),
- * halfCellInt = 1, cell grid as given (tools/decomp.py:322-342 computes it). */
+ * (src/storage/DomainDecomposition.cpp:70-85) on one node: nodeGrid = (1,1,1), cell
+ * grid as given (tools/decomp.py:322-342 computes it), at least 3 cells a dimension;
+ * halfCellInt 1 (espp_set_half_cell_int sets another). */
 ESPP_API int espp_system_create(const double box[3], double skin, const int32_t cell_grid[3],
                        int32_t precision, uint64_t seed, espp_system** out);
 ESPP_API int espp_system_destroy(espp_system* s);
