@@ -66,7 +66,7 @@ FORCE_BYTES = 12.0 + 4.0 * N_HALF + 24.0
 # the 1,000,000-particle case (profiles/force_mixed_lj_1M_ncu.txt: 345.0 MB + 6.7 MB for
 # the global-list kernel); traffic grows in proportion to the particle count at fixed
 # density
-FORCE_TRAFFIC_PER_PARTICLE = {"k_force_mixed": 351.7}
+FORCE_TRAFFIC_PER_PARTICLE = {"k_force_mixed": 347.4}
 
 
 def log(*a):
