@@ -212,6 +212,17 @@ class System:
         self._storage = None
         self.shortRangeInteractions = []
         self.maxCutoff = 0.0
+        self._interaction2id = {}  # name -> index in shortRangeInteractions (System.py:134-192)
+        self._integrator = None
+        self._trace = False
+
+    @property
+    def integrator(self):
+        return self._integrator
+
+    @integrator.setter
+    def integrator(self, integ):
+        self._integrator = integ
 
     @property
     def skin(self):
@@ -232,16 +243,58 @@ class System:
         self._storage = st
 
     def addInteraction(self, interaction, name=None):
+        if name is not None and name in self._interaction2id:
+            raise RuntimeError('Interaction with name {} already defined.'.format(name))
+        kind = getattr(interaction, "kind", None)
+        if kind is not None and any(getattr(ia, "kind", None) == kind
+                                    for ia in self.shortRangeInteractions):
+            # the device holds one parameter table per interaction kind, so a second one
+            # would overwrite the first one's table
+            raise RuntimeError("a system holds one interaction of each kind; {} is already "
+                               "added".format(type(interaction).__name__))
         self.shortRangeInteractions.append(interaction)
         interaction._attach(self)
         self.maxCutoff = max(self.maxCutoff, interaction.getMaxCutoff())
+        if name is not None:
+            self._interaction2id[name] = len(self.shortRangeInteractions) - 1
         return True
 
     def removeInteraction(self, i):
         ia = self.shortRangeInteractions.pop(i)
         ia._detach()
+        # names above the removed index move down by one; the removed one's name is dropped
+        self._interaction2id = {k: (v if v < i else v - 1)
+                                for k, v in self._interaction2id.items() if v != i}
+
+    def removeInteractionByName(self, name):
+        if name not in self._interaction2id:
+            raise RuntimeError('Interaction {} not found'.format(name))
+        self.removeInteraction(self._interaction2id[name])
+
+    def getAllInteractions(self):
+        return {k: self.getInteraction(v) for k, v in self._interaction2id.items()}
+
+    def getInteractionByName(self, name):
+        return self.getInteraction(self._interaction2id[name])
+
+    def getNameOfInteraction(self, number):
+        for name, iid in self._interaction2id.items():
+            if iid == number:
+                return name
+        return None
+
+    def setTrace(self, switch):
+        """System::setTrace (tracing of the reference's C++ calls): kept as a flag; the GPU
+        library has no trace output."""
+        self._trace = bool(switch)
 
     def getInteraction(self, i):
+        """System.py:167-176: an empty list and an index out of range are errors."""
+        ni = len(self.shortRangeInteractions)
+        if ni == 0:
+            raise RuntimeError("interaction list of system is empty")
+        if not 0 <= i < ni:
+            raise RuntimeError("Interaction number %i does not exist" % i)
         return self.shortRangeInteractions[i]
 
     def getNumberOfInteractions(self):

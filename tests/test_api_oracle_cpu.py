@@ -227,3 +227,42 @@ def test_temperature_of_selected_types(on_oracle):
     assert T.compute() == pytest.approx(all_T, rel=1e-12)
     T.add_type(3)  # no particle of type 3
     assert np.isnan(T.compute())
+
+
+def test_named_interactions(on_oracle):
+    """System.py:134-192: interactions added under a name are found, listed and removed by
+    it; a repeated name, an unknown name and an index out of range are errors, and the
+    names above a removed interaction move down with it.  The device holds one parameter
+    table per interaction kind, so a second interaction of a kind is refused."""
+    system, integ = _fluid(n=512)
+    lj0 = system.getInteraction(0)
+    fpl = espressopp.FixedPairList(system.storage)
+    fpl.addBonds([(0, 1), (2, 3)])
+    fene = espressopp.interaction.FixedPairListFENE(
+        system, fpl, espressopp.interaction.FENE(K=30.0, r0=0.0, rMax=1.5))
+    cos_ = espressopp.interaction.FixedTripleListCosine(
+        system, espressopp.FixedTripleList(system.storage),
+        espressopp.interaction.Cosine(K=1.5, theta0=0.0))
+    system.addInteraction(fene, "bonds")
+    system.addInteraction(cos_, "angles")
+    with pytest.raises(RuntimeError, match="already defined"):
+        system.addInteraction(cos_, "bonds")
+    lj1 = espressopp.interaction.VerletListLennardJones(lj0.getVerletList())
+    with pytest.raises(RuntimeError, match="one interaction of each kind"):
+        system.addInteraction(lj1)
+    assert system.getNumberOfInteractions() == 3
+    assert system.getInteractionByName("angles") is cos_
+    assert system.getNameOfInteraction(1) == "bonds" and system.getNameOfInteraction(0) is None
+    assert set(system.getAllInteractions()) == {"bonds", "angles"}
+    assert fene.computeEnergy() > 0.0
+    system.removeInteractionByName("bonds")
+    assert system.getNumberOfInteractions() == 2
+    assert system.getNameOfInteraction(1) == "angles"
+    assert system.getInteractionByName("angles") is cos_
+    with pytest.raises(RuntimeError, match="not found"):
+        system.removeInteractionByName("bonds")
+    with pytest.raises(RuntimeError, match="does not exist"):
+        system.getInteraction(2)
+    integ.run(10)
+    system.integrator = integ
+    assert system.integrator is integ
