@@ -35,10 +35,13 @@ PROTOTYPES = {
                               c_double]),
     "espp_bonds_add": (c_int32, [_P, c_int64, _I64]),
     "espp_bonds_size": (c_int32, [_P, _I64]),
+    "espp_bonds_clear": (c_int32, [_P]),
     "espp_fene_set": (c_int32, [_P, c_double, c_double, c_double, c_double, c_double]),
     "espp_bonds_max_sqr": (c_int32, [_P, _D]),
+    "espp_bonds_reset_max": (c_int32, [_P]),
     "espp_triples_add": (c_int32, [_P, c_int64, _I64]),
     "espp_triples_size": (c_int32, [_P, _I64]),
+    "espp_triples_clear": (c_int32, [_P]),
     "espp_cosine_set": (c_int32, [_P, c_double, c_double]),
     "espp_tab_read": (c_int32, [c_char_p, c_int64, _D, _D, _D, _I64]),
     "espp_tab_eval": (c_int32, [c_int32, c_int64, _D, _D, _D, c_int64, _D, _D, _D]),

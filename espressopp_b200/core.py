@@ -595,13 +595,32 @@ class FixedPairList:
 
     totalSize = size
 
+    def getAllBonds(self):
+        """FixedPairList::getAllBonds (FixedPairList.cpp:167-200): every bond as a
+        (pid1, pid2) tuple, pid1 < pid2."""
+        return list(self._bonds)
+
+    def remove(self):
+        """FixedPairList::remove (FixedPairList.cpp:317-324): empties the list."""
+        call(self.storage._lib, "espp_bonds_clear", self.storage._h)
+        self._bonds = []
+
     def getLongtimeMaxBondSqr(self):
+        """The longest bond^2 seen by any force pass since the last reset
+        (FixedPairListInteractionTemplate.hpp:145-150)."""
         v = ctypes.c_double()
         call(self.storage._lib, "espp_bonds_max_sqr", self.storage._h, ctypes.byref(v))
         return v.value
 
+    def resetLongtimeMaxBond(self):
+        call(self.storage._lib, "espp_bonds_reset_max", self.storage._h)
+
+    def getLongtimeMaxBondLocal(self):
+        """One value per worker, as the reference's pmiinvoke returns it."""
+        return [math.sqrt(self.getLongtimeMaxBondSqr())]
+
     def getLongtimeMaxBond(self):
-        return math.sqrt(self.getLongtimeMaxBondSqr())
+        return max(self.getLongtimeMaxBondLocal())
 
 
 class FixedTripleList:
@@ -626,6 +645,11 @@ class FixedTripleList:
 
     def getTriples(self):
         return [list(self._triples)]
+
+    def remove(self):
+        """FixedTripleList.remove (FixedTripleList.py:97-100): empties the list."""
+        call(self.storage._lib, "espp_triples_clear", self.storage._h)
+        self._triples = []
 
     def size(self):
         return len(self._triples)

@@ -2133,6 +2133,14 @@ int espp_bonds_size(espp_system* s, int64_t* n) {
   return guard([&] { *n = (int64_t)checked(s)->bonds.size(); });
 }
 
+// FixedPairList::remove (FixedPairList.cpp:317-324): the list is emptied.
+int espp_bonds_clear(espp_system* s) {
+  return guard([&] {
+    checked(s)->bonds.clear();
+    s->idDirty = true;
+  });
+}
+
 int espp_fene_set(espp_system* s, double K, double r0, double rmax, double rc, double shift) {
   return guard([&] {
     checked(s);
@@ -2158,6 +2166,14 @@ int espp_triples_add(espp_system* s, int64_t n, const int64_t* triples) {
         if (!have.count(id)) raise(ESPP_EINVAL, "triple member does not exist");
       s->triples.push_back(tr);
     }
+    s->idDirty = true;
+  });
+}
+
+// FixedTripleList::remove (FixedTripleList.py:97-100): the list is emptied.
+int espp_triples_clear(espp_system* s) {
+  return guard([&] {
+    checked(s)->triples.clear();
     s->idDirty = true;
   });
 }
@@ -2265,17 +2281,22 @@ int espp_tab_angle_set(espp_system* s, int32_t itype, int64_t n, const double* t
   });
 }
 
+// FixedPairList::getLongtimeMaxBondSqr / resetLongtimeMaxBondSqr (FixedPairList.cpp:82-86):
+// the force kernels raise the counter to the longest bond of each force pass.
 int espp_bonds_max_sqr(espp_system* s, double* m) {
   return guard([&] {
     checked(s);
-    prepare_observables(s);
-    *m = 0.0;
-    if (s->n == 0 || s->bonds.empty()) return;
-    int nb;
-    double* part = obs_partials(s, nb);
-    launch_bond_maxsq(s->view(), part, nb, s->obs, s->st);
-    cuda_check(cudaMemcpyAsync(m, s->obs, sizeof(double), cudaMemcpyDeviceToHost, s->st),
-               "download");
+    const unsigned long long b = get_counters(s).ltMaxBondSq;
+    std::memcpy(m, &b, sizeof(double));
+  });
+}
+
+int espp_bonds_reset_max(espp_system* s) {
+  return guard([&] {
+    checked(s);
+    DevCounters c = get_counters(s);
+    c.ltMaxBondSq = 0ull;
+    set_counters(s, c);
     sync(s);
   });
 }

@@ -366,7 +366,7 @@ __device__ __forceinline__ void fene_mixed(const DevView& d, const FENEParams& f
   const int4 pi = d.posq[i];
   const int64_t off = a.id[i] - d.idMin;
   const int b0 = d.bondStart[off], b1 = d.bondStart[off + 1];
-  float bx = 0.f, by = 0.f, bz = 0.f;
+  float bx = 0.f, by = 0.f, bz = 0.f, bmax = 0.f;
   const float rmaxsq = (float)fp.rmaxsq, K = (float)fp.K, r0 = (float)fp.r0;
   for (int b = b0; b < b1; ++b) {
     const int64_t po = d.bondPartner[b] - d.idMin;
@@ -380,6 +380,7 @@ __device__ __forceinline__ void fene_mixed(const DevView& d, const FENEParams& f
     const float dy = wrapped_diff(pi.y, pj.y, d.fixUnit[1]);
     const float dz = wrapped_diff(pi.z, pj.z, d.fixUnit[2]);
     const float r2 = dx * dx + dy * dy + dz * dz;
+    bmax = fmaxf(bmax, r2);
     if (!(r2 <= (float)fp.rcsq)) continue;
     float ff;
     if (fp.r0 > 2.220446049250313e-16) {
@@ -392,6 +393,7 @@ __device__ __forceinline__ void fene_mixed(const DevView& d, const FENEParams& f
     by += dy * ff;
     bz += dz * ff;
   }
+  if (b1 > b0) note_bond_sq(d.ctr, (double)bmax);
   Fx += to_fix(bx, d.err);
   Fy += to_fix(by, d.err);
   Fz += to_fix(bz, d.err);
@@ -413,6 +415,7 @@ __device__ __forceinline__ void fene_fp64(const DevView& d, const FENEParams& fp
   const double xi = a.x[i], yi = a.x[cap + i], zi = a.x[2 * cap + i];
   const int64_t off = a.id[i] - d.idMin;
   const int b0 = d.bondStart[off], b1 = d.bondStart[off + 1];
+  double bmax = 0.0;
   for (int b = b0; b < b1; ++b) {
     const int64_t po = d.bondPartner[b] - d.idMin;
     const int j = (po >= 0 && po < d.idSpan) ? d.id2idx[po] : -1;
@@ -424,6 +427,7 @@ __device__ __forceinline__ void fene_fp64(const DevView& d, const FENEParams& fp
     const double dy = min_image_d(yi - a.x[cap + j], d.L[1], d.halfL[1]);
     const double dz = min_image_d(zi - a.x[2 * cap + j], d.L[2], d.halfL[2]);
     const double r2 = dx * dx + dy * dy + dz * dz;
+    bmax = fmax(bmax, r2);
     if (r2 > fp.rcsq) continue;
     double ff;
     if (fp.r0 > 2.220446049250313e-16) {
@@ -436,6 +440,7 @@ __device__ __forceinline__ void fene_fp64(const DevView& d, const FENEParams& fp
     fy += dy * ff;
     fz += dz * ff;
   }
+  if (b1 > b0) note_bond_sq(d.ctr, bmax);
 }
 
 // 16-byte list block b of particle i (8 entries), read without L1 allocation

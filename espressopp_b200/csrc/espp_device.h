@@ -23,6 +23,15 @@ __device__ __forceinline__ int4 fixed_coords(const DevView& d, double x, double 
   return make_int4((int)(unsigned)qx, (int)(unsigned)qy, (int)(unsigned)qz, type);
 }
 
+// FixedPairListInteractionTemplate.hpp:145-150: every force pass raises the list's
+// long-time maximum bond length^2 to the longest bond it saw.  The maximum is kept as the
+// bits of a non-negative double, which order like unsigned integers; the atomic is issued
+// only by a thread whose bond is longer than the stored value.
+__device__ __forceinline__ void note_bond_sq(DevCounters* c, double r2) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(r2);
+  if (b > *(volatile unsigned long long*)&c->ltMaxBondSq) atomicMax(&c->ltMaxBondSq, b);
+}
+
 __device__ __forceinline__ float wrapped_diff(int a, int b, float unit) {
   return (float)(int)((unsigned)a - (unsigned)b) * unit;
 }

@@ -88,6 +88,7 @@ struct DevCounters {
   int flag;                  // re-sort needed this step
   int nnMax;                 // largest neighbour count seen by the Verlet builds
   double pref1, pref2;       // Langevin prefactors of the step loop (-gamma, sqrt(24 T gamma/dt))
+  unsigned long long ltMaxBondSq;  // longest bond^2 seen by the force passes, as double bits
 };
 
 // Pointers and scalars every kernel needs; passed by value.
@@ -281,8 +282,6 @@ void launch_pair_digest_brick(const DevView& d, unsigned long long* partials,
 size_t brick_smem_f32(int wmax);
 size_t brick_smem_f64(int wmax);
 size_t brick_smem_limit();
-void launch_bond_maxsq(const DevView& d, double* partials, int nblocks, double* out,
-                       cudaStream_t st);
 
 // float copy of an LJ table for the mixed-precision kernel
 void make_float_table(const LJTable& t, LJPairF* out);

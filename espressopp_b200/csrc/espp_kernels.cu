@@ -849,7 +849,7 @@ __global__ void __launch_bounds__(256) k_force_mixed(DevView d, FENEParams fp) {
   if (FENE && sub == 0 && act) {
     const int64_t off = a.id[i] - d.idMin;
     const int b0 = d.bondStart[off], b1 = d.bondStart[off + 1];
-    float bx = 0.f, by = 0.f, bz = 0.f;
+    float bx = 0.f, by = 0.f, bz = 0.f, bmax = 0.f;
     const float rmaxsq = (float)fp.rmaxsq, K = (float)fp.K, r0 = (float)fp.r0;
     for (int b = b0; b < b1; ++b) {
       const int64_t po = d.bondPartner[b] - d.idMin;
@@ -863,6 +863,7 @@ __global__ void __launch_bounds__(256) k_force_mixed(DevView d, FENEParams fp) {
       const float dy = wrapped_diff(pi.y, pj.y, uy);
       const float dz = wrapped_diff(pi.z, pj.z, uz);
       const float r2 = dx * dx + dy * dy + dz * dz;
+      bmax = fmaxf(bmax, r2);
       if (!(r2 <= (float)fp.rcsq)) continue;
       float ff;
       if (fp.r0 > 2.220446049250313e-16) {
@@ -875,6 +876,7 @@ __global__ void __launch_bounds__(256) k_force_mixed(DevView d, FENEParams fp) {
       by += dy * ff;
       bz += dz * ff;
     }
+    if (b1 > b0) note_bond_sq(d.ctr, (double)bmax);
     Fx += to_fix(bx, d.err);
     Fy += to_fix(by, d.err);
     Fz += to_fix(bz, d.err);
@@ -967,6 +969,7 @@ __global__ void __launch_bounds__(256) k_force_fp64(DevView d, FENEParams fp) {
   if (FENE && sub == 0 && act) {
     const int64_t off = a.id[i] - d.idMin;
     const int b0 = d.bondStart[off], b1 = d.bondStart[off + 1];
+    double bmax = 0.0;
     for (int b = b0; b < b1; ++b) {
       const int64_t po = d.bondPartner[b] - d.idMin;
       const int j = (po >= 0 && po < d.idSpan) ? d.id2idx[po] : -1;
@@ -978,6 +981,7 @@ __global__ void __launch_bounds__(256) k_force_fp64(DevView d, FENEParams fp) {
       const double dy = min_image(yi - Y[j], d.L[1], d.halfL[1]);
       const double dz = min_image(zi - Z[j], d.L[2], d.halfL[2]);
       const double r2 = dx * dx + dy * dy + dz * dz;
+      bmax = fmax(bmax, r2);
       if (r2 > fp.rcsq) continue;
       double ff;
       if (fp.r0 > 2.220446049250313e-16) {
@@ -990,6 +994,7 @@ __global__ void __launch_bounds__(256) k_force_fp64(DevView d, FENEParams fp) {
       fy += dy * ff;
       fz += dz * ff;
     }
+    if (b1 > b0) note_bond_sq(d.ctr, bmax);
   }
   if (TPP > 1) {
 #pragma unroll
@@ -1251,44 +1256,6 @@ __global__ void k_fene_obs(DevView d, FENEParams fp, int energy, double* partial
     }
   }
   block_sum_store<7>(acc, partials);
-}
-
-// max bond length^2 over all bonds (FixedPairList::getLongtimeMaxBondSqr)
-__global__ void k_bond_maxsq(DevView d, double* partials) {
-  const ParticleArrays a = d.pa[0];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double acc[1] = {0.0};
-  __shared__ double sm[kBlock / 32];
-  if (i < d.n && d.bondStart) {
-    const int64_t off = a.id[i] - d.idMin;
-    for (int b = d.bondStart[off]; b < d.bondStart[off + 1]; ++b) {
-      const int j = d.id2idx[d.bondPartner[b] - d.idMin];
-      if (j < 0) continue;
-      double r2 = 0;
-      for (int k = 0; k < 3; ++k) {
-        const double dk = min_image(a.x[(size_t)k * d.cap + i] - a.x[(size_t)k * d.cap + j],
-                                    d.L[k], d.halfL[k]);
-        r2 += dk * dk;
-      }
-      acc[0] = fmax(acc[0], r2);
-    }
-  }
-  double v = warp_max(acc[0]);
-  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0;
-    for (int w = 0; w < (int)(blockDim.x / 32); ++w) t = fmax(t, sm[w]);
-    partials[blockIdx.x] = t;
-  }
-}
-
-__global__ void k_max_partials(const double* partials, int nb, double* out) {
-  if (threadIdx.x == 0) {
-    double t = 0;
-    for (int b = 0; b < nb; ++b) t = fmax(t, partials[b]);
-    *out = t;
-  }
 }
 
 // ---- analysis::RadialDistrF -----------------------------------------------------------
@@ -1571,12 +1538,13 @@ __global__ void k_force_tab(DevView d) {
     const TabDesc& T = d.tabs[t];
     double dx, dy, dz;
     const double r2 = tab_dist(d, X, i, j, dx, dy, dz);
-    if (r2 > T.rcsq) return;
+    if (r2 > T.rcsq) return r2;
     const double r = sqrt(r2);
     const double ff = tab_value(T, d.tabCoef, true, r) / r;
     fx += dx * ff;
     fy += dy * ff;
     fz += dz * ff;
+    return r2;
   };
   if (d.tabNT > 0) {
     const int ti = a.type[i];
@@ -1591,15 +1559,18 @@ __global__ void k_force_tab(DevView d) {
   }
   if (d.tabBond >= 0 && d.bondStart) {
     const int64_t off = a.id[i] - d.idMin;
-    for (int b = d.bondStart[off]; b < d.bondStart[off + 1]; ++b) {
+    const int b0 = d.bondStart[off], b1 = d.bondStart[off + 1];
+    double bmax = 0.0;
+    for (int b = b0; b < b1; ++b) {
       const int64_t po = d.bondPartner[b] - d.idMin;
       const int j = (po >= 0 && po < d.idSpan) ? d.id2idx[po] : -1;
       if (j < 0) {
         atomicOr(d.err, kErrBondMissing);
         continue;
       }
-      add(d.tabBond, j);
+      bmax = fmax(bmax, add(d.tabBond, j));
     }
+    if (b1 > b0) note_bond_sq(d.ctr, bmax);
   }
   const size_t c = d.cap;
   if (MIXED) {
@@ -2126,12 +2097,6 @@ void launch_kinetic_tensor(const DevView& d, double* partials, int nblocks, doub
                            cudaStream_t st) {
   k_kinetic_tensor<<<nblocks, kBlock, 0, st>>>(d, partials);
   k_sum_partials<6><<<1, 256, 0, st>>>(partials, nblocks, out);
-}
-
-void launch_bond_maxsq(const DevView& d, double* partials, int nblocks, double* out,
-                       cudaStream_t st) {
-  k_bond_maxsq<<<nblocks, kBlock, 0, st>>>(d, partials);
-  k_max_partials<<<1, 32, 0, st>>>(partials, nblocks, out);
 }
 
 void launch_pair_count(const DevView& d, int32_t* counts, cudaStream_t st) {

@@ -135,12 +135,19 @@ ESPP_API int espp_lj_set(espp_system* s, int32_t type1, int32_t type2, double ep
  * FixedPairList::add (src/FixedPairList.cpp:88-141): pairs are id pairs. */
 ESPP_API int espp_bonds_add(espp_system* s, int64_t n, const int64_t* pairs);
 ESPP_API int espp_bonds_size(espp_system* s, int64_t* n);
+/* FixedPairList::remove (src/FixedPairList.cpp:317-324): empties the bond list. */
+ESPP_API int espp_bonds_clear(espp_system* s);
 /* FixedPairListFENE(system, fpl, FENE(K, r0, rMax, cutoff, shift))
  * (src/interaction/FENE.hpp:35-115, src/interaction/FENE.cpp:45-53). */
 ESPP_API int espp_fene_set(espp_system* s, double K, double r0, double rmax, double cutoff,
                   double shift);
-/* FixedPairList::getLongtimeMaxBondSqr. */
+/* FixedPairList::getLongtimeMaxBondSqr (src/FixedPairList.cpp:82): the longest bond^2
+ * seen by any force pass since the system was made or the maximum was last reset
+ * (every force pass raises it, FixedPairListInteractionTemplate.hpp:145-150); 0 before
+ * the first force pass. */
 ESPP_API int espp_bonds_max_sqr(espp_system* s, double* maxsq);
+/* FixedPairList::resetLongtimeMaxBondSqr (src/FixedPairList.cpp:86): sets it to 0. */
+ESPP_API int espp_bonds_reset_max(espp_system* s);
 
 /* ---- FixedTripleList + interaction::Cosine ---------------------------------------------
  * FixedTripleList::add (src/FixedTripleList.cpp): triples of ids (p1, p2, p3), p2 the
@@ -149,6 +156,8 @@ ESPP_API int espp_bonds_max_sqr(espp_system* s, double* maxsq);
  * E = K (1 + cos(theta - theta0)). */
 ESPP_API int espp_triples_add(espp_system* s, int64_t n, const int64_t* triples);
 ESPP_API int espp_triples_size(espp_system* s, int64_t* n);
+/* FixedTripleList::remove (src/FixedTripleList.py:97-100): empties the triple list. */
+ESPP_API int espp_triples_clear(espp_system* s);
 ESPP_API int espp_cosine_set(espp_system* s, double K, double theta0);
 
 /* ---- interaction::Tabulated -----------------------------------------------------------

@@ -1884,6 +1884,14 @@ int espp_bonds_add(espp_system* s, int64_t n, const int64_t* pairs) {
   return ESPP_OK;
 }
 
+// FixedPairList::remove (FixedPairList.cpp:317-324).
+int espp_bonds_clear(espp_system* s) {
+  CHECK_S(s);
+  s->bondsGlobal.clear();
+  bondsRefresh(s);
+  return ESPP_OK;
+}
+
 int espp_bonds_size(espp_system* s, int64_t* n) {
   CHECK_S(s);
   *n = (int64_t)s->bondsGlobal.size();
@@ -1904,9 +1912,16 @@ int espp_fene_set(espp_system* s, double K, double r0, double rmax, double rc,
   return ESPP_OK;
 }
 
+// FixedPairList.cpp:82-86: the long-time maximum, raised by every force pass.
 int espp_bonds_max_sqr(espp_system* s, double* m) {
   CHECK_S(s);
   *m = s->ltMaxBondSqr;
+  return ESPP_OK;
+}
+
+int espp_bonds_reset_max(espp_system* s) {
+  CHECK_S(s);
+  s->ltMaxBondSqr = 0.0;
   return ESPP_OK;
 }
 
@@ -1918,6 +1933,13 @@ int espp_triples_add(espp_system* s, int64_t n, const int64_t* triples) {
       if (!lookup(s, id)) return fail(ESPP_EINVAL, "triple member does not exist");
     s->triplesGlobal.push_back(tr);
   }
+  return ESPP_OK;
+}
+
+// FixedTripleList::remove (FixedTripleList.py:97-100).
+int espp_triples_clear(espp_system* s) {
+  CHECK_S(s);
+  s->triplesGlobal.clear();
   return ESPP_OK;
 }
 

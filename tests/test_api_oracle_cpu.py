@@ -266,3 +266,40 @@ def test_named_interactions(on_oracle):
     integ.run(10)
     system.integrator = integ
     assert system.integrator is integ
+
+
+def test_fixed_pair_list_longtime_max_and_remove(on_oracle):
+    """FixedPairList (FixedPairList.py:85-148, FixedPairList.cpp:82-86 and 167-324): the
+    long-time maximum bond is 0 before a force pass and the longest bond after it, a reset
+    sets it to 0, getAllBonds lists every (pid1 < pid2) pair, remove empties the list;
+    FixedTripleList.remove likewise."""
+    system, integ = _fluid(n=512)
+    fpl = espressopp.FixedPairList(system.storage)
+    fpl.addBonds([(1, 0), (2, 3), (10, 11)])
+    assert fpl.getAllBonds() == [(0, 1), (2, 3), (10, 11)]
+    fene = espressopp.interaction.FixedPairListFENE(
+        system, fpl, espressopp.interaction.FENE(K=30.0, r0=0.0, rMax=2.5))
+    system.addInteraction(fene)
+    assert fpl.getLongtimeMaxBond() == 0.0
+    integ.run(0)
+    ids, pos = system.storage.getAll()[:2]
+    L = np.asarray(system.bc.boxL)
+    d = np.array([pos[np.searchsorted(ids, a)] - pos[np.searchsorted(ids, b)]
+                  for a, b in fpl.getAllBonds()])
+    d -= L * np.round(d / L)
+    longest = float(np.sqrt(np.max(np.sum(d * d, axis=1))))
+    assert abs(fpl.getLongtimeMaxBond() - longest) < 1e-12 * longest
+    assert fpl.getLongtimeMaxBondLocal() == [fpl.getLongtimeMaxBond()]
+    integ.run(20)
+    assert fpl.getLongtimeMaxBond() >= longest
+    fpl.resetLongtimeMaxBond()
+    assert fpl.getLongtimeMaxBond() == 0.0
+    fpl.remove()
+    assert fpl.size() == 0 and fpl.getAllBonds() == []
+    integ.run(5)
+    assert fpl.getLongtimeMaxBond() == 0.0 and fene.computeEnergy() == 0.0
+    ftl = espressopp.FixedTripleList(system.storage)
+    ftl.addTriples([(0, 1, 2), (3, 4, 5)])
+    assert ftl.size() == 2
+    ftl.remove()
+    assert ftl.size() == 0 and ftl.getTriples() == [[]]

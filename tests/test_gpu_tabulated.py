@@ -63,6 +63,12 @@ def test_tabulated_forces_and_observables_match_oracle(tmp_path, itype):
     fo = o.particles(ids)[2]
     assert _rel_rms(g64.particles(ids)[2], fo) < 1e-12
     assert _rel_rms(gmx.particles(ids)[2], fo) < 1e-9
+    # the bond list's long-time maximum, raised by the tabulated bond pass on FP64
+    # distances in both precisions
+    mx = np.zeros(3)
+    for k, s in enumerate((o, g64, gmx)):
+        _abi.call(s.lib, "espp_bonds_max_sqr", s.h, _abi.dptr(mx[k:]))
+    assert mx[0] > 0 and np.all(np.abs(mx[1:] - mx[0]) <= 1e-14 * mx[0])
     for which in (_abi.IA_TAB_PAIR, _abi.IA_TAB_BOND):
         eo, wo = o.energy(which), o.virial(which)
         for g in (g64, gmx):
