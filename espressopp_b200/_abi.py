@@ -6,12 +6,14 @@ exports the ABI.  ``call(lib, name, *args)`` runs one entry point and raises
 reference's Boost.Python layer turns ``std::runtime_error`` into a Python exception.
 """
 import ctypes
-from ctypes import POINTER, c_char_p, c_double, c_int32, c_int64, c_size_t, c_uint64, c_void_p
+from ctypes import (POINTER, c_char_p, c_double, c_int32, c_int64, c_size_t, c_uint8,
+                    c_uint64, c_void_p)
 
 _P = c_void_p
 _D = POINTER(c_double)
 _I64 = POINTER(c_int64)
 _I32 = POINTER(c_int32)
+_U8 = POINTER(c_uint8)
 
 PROTOTYPES = {
     "espp_abi_version": (c_int32, []),
@@ -56,6 +58,11 @@ PROTOTYPES = {
     "espp_capforce_set": (c_int32, [_P, c_int32, _D]),
     "espp_run": (c_int32, [_P, c_int64]),
     "espp_num_resorts": (c_int32, [_P, _I64]),
+    "espp_dd_load": (c_int32, [_P, c_int64, _I64, _I32, _D, _D, _D, _I32, _U8]),
+    "espp_dd_set_halo_positions": (c_int32, [_P, c_int64, _I64, _D]),
+    "espp_dd_run_begin": (c_int32, [_P, c_int64, _D]),
+    "espp_dd_step": (c_int32, [_P, c_int32, _D]),
+    "espp_dd_run_end": (c_int32, [_P]),
     "espp_timers": (c_int32, [_P, _D]),
     "espp_energy": (c_int32, [_P, c_int32, _D]),
     "espp_virial": (c_int32, [_P, c_int32, _D]),
@@ -148,6 +155,10 @@ def call(lib, name, *args):
 def dptr(a):
     """Pointer to a C-contiguous float64 numpy array (or None)."""
     return None if a is None else a.ctypes.data_as(_D)
+
+
+def u8ptr(a):
+    return None if a is None else a.ctypes.data_as(_U8)
 
 
 def i64ptr(a):

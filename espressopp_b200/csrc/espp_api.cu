@@ -125,6 +125,7 @@ struct espp_system {
   int32_t* bondStart = nullptr;
   int64_t* bondPartner = nullptr;
   uint8_t* langExcl = nullptr;
+  uint8_t* halo = nullptr;  // idSpan, built when haloIds is not empty
   int32_t* exclStart = nullptr;
   int64_t* exclIds = nullptr;
   bool idDirty = true;
@@ -218,6 +219,13 @@ struct espp_system {
   bool lang_on = false;
   double gamma = 0.0, temperature = 0.0;
   std::vector<int64_t> langExclIds;
+  // spatial decomposition: ids of the halo copies of other domains' particles, and the
+  // step-loop state of a run driven step by step by the decomposition's host loop
+  std::vector<int64_t> haloIds;
+  bool ddRun = false;
+  int64_t ddSteps = 0, ddDone = 0;
+  double ddT0 = 0.0, ddTResort = 0.0;
+  IntegrateArgs ddArgs{};
   int capMode = ESPP_CAP_OFF;
   double cap3[3] = {0, 0, 0};
   int tpp = 4;
@@ -275,6 +283,7 @@ struct espp_system {
     d.bondStart = bondStart;
     d.bondPartner = bondPartner;
     d.langExcl = langExcl;
+    d.halo = halo;
     d.exclStart = exclStart;
     d.exclIds = exclIds;
     d.lj = d_lj;
@@ -463,6 +472,7 @@ void rebuild_id_tables(espp_system* s) {
   dfree(s->bondStart);
   dfree(s->bondPartner);
   dfree(s->langExcl);
+  dfree(s->halo);
   dfree(s->exclStart);
   dfree(s->exclIds);
   if (s->allIds.empty()) {
@@ -474,7 +484,8 @@ void rebuild_id_tables(espp_system* s) {
   auto mm = std::minmax_element(s->allIds.begin(), s->allIds.end());
   s->idMin = *mm.first;
   int64_t span = *mm.second - *mm.first + 1;
-  if (span > 4 * (int64_t)s->allIds.size() + (1 << 20) || span > (1LL << 31) - 2)
+  // a domain of a spatial decomposition holds a slab of the ids of the whole system
+  if (span > 16 * (int64_t)s->allIds.size() + (1 << 24) || span > (1LL << 31) - 2)
     raise(ESPP_ERANGE, "particle ids are too sparse for the dense id map (span " +
                            std::to_string(span) + ")");
   s->idSpan = (int)span;
@@ -551,6 +562,12 @@ void rebuild_id_tables(espp_system* s) {
     if (id >= s->idMin && id - s->idMin < span) le[id - s->idMin] = 1;
   s->langExcl = dalloc<uint8_t>(span);
   cuda_check(cudaMemcpy(s->langExcl, le.data(), span, cudaMemcpyHostToDevice), "upload");
+  if (!s->haloIds.empty()) {
+    std::vector<uint8_t> hl(span, 0);
+    for (int64_t id : s->haloIds) hl[id - s->idMin] = 1;
+    s->halo = dalloc<uint8_t>(span);
+    cuda_check(cudaMemcpy(s->halo, hl.data(), span, cudaMemcpyHostToDevice), "upload");
+  }
   s->idDirty = false;
   s->binned = false;
 }
@@ -615,7 +632,7 @@ DevCounters get_counters(espp_system* s);
 bool pair_any(const espp_system* s);
 bool brick_wanted(const espp_system* s) {
   if (!s->brickAllowed || !s->has_vl || !s->lj_any || s->tabNT > 0 || s->mlp) return false;
-  if (s->hci != 1) return false;
+  if (s->hci != 1 || !s->haloIds.empty()) return false;
   for (int k = 0; k < 3; ++k)
     if (s->nc[k] < 2) return false;
   return true;
@@ -649,6 +666,7 @@ int brick_window_limit(const espp_system* s) {
 
 bool brick_geometry_ok(const espp_system* s) {
   if (s->hci != 1) return false;  // brick windows hold one cell layer
+  if (!s->haloIds.empty()) return false;  // the brick kernels know no halo particles
   for (int k = 0; k < 3; ++k)
     if (s->nc[k] < 2) return false;
   return s->n > 0;
@@ -1523,6 +1541,10 @@ void observable(espp_system* s, int which, int energy, double out[7]) {
   } else if (which == ESPP_IA_TAB_BOND) {
     if (s->tabBond < 0) return;
     launch_tab_observables(d, 1, part, nb, s->obs, energy, s->st);
+  } else if (!s->haloIds.empty() &&
+             (which == ESPP_IA_COSINE || which == ESPP_IA_TAB_ANGLE || which == ESPP_IA_MLP)) {
+    raise(ESPP_EINVAL, "angle and learned-potential observables are not available with halo "
+                       "particles (spatial decomposition)");
   } else if (which == ESPP_IA_COSINE) {
     if (s->triples.empty() || !s->cosine.on) return;
     launch_angle_observables(d, part, nb, s->obs, energy, 0, s->st);
@@ -1578,6 +1600,7 @@ void destroy(espp_system* s) {
   dfree(s->bondStart);
   dfree(s->bondPartner);
   dfree(s->langExcl);
+  dfree(s->halo);
   dfree(s->exclStart);
   dfree(s->exclIds);
   dfree(s->err);
@@ -2358,6 +2381,143 @@ int espp_run(espp_system* s, int64_t nsteps) {
   });
 }
 
+// ---- spatial decomposition: one system per domain --------------------------------------
+// The host loop of a decomposition over several domains (DomainDecomposition.cpp:1031-1158
+// migration, :1243-1391 ghost frames) moves particles between the domains' systems at a
+// re-sort and refreshes the halo copies every step; the phases below split the step loop
+// at those points.  The host takes the maximum displacement over the domains and decides
+// the re-sort with the device rule (maxDist += sqrt(max |dx|^2) > skin / 2).
+
+namespace {
+
+// sqrt of the integrate1 maximum |dx|^2 since the last call, which is reset
+double take_max_disp(espp_system* s) {
+  DevCounters c = get_counters(s);
+  double m;
+  std::memcpy(&m, &c.maxSq, sizeof(double));
+  c.maxSq = 0ull;
+  set_counters(s, c);
+  return std::sqrt(m);
+}
+
+}  // namespace
+
+int espp_dd_load(espp_system* s, int64_t n, const int64_t* id, const int32_t* type,
+                 const double* mass, const double* pos, const double* vel, const int32_t* img,
+                 const uint8_t* halo) {
+  return guard([&] {
+    checked(s);
+    if (n < 0 || (n > 0 && (!id || !pos))) raise(ESPP_EINVAL, "bad particle arrays");
+    if ((int64_t)n > (1LL << 30)) raise(ESPP_ERANGE, "too many particles");
+    HostParticles h;
+    h.id.assign(id, id + n);
+    std::unordered_map<int64_t, int> seen;
+    seen.reserve(n);
+    std::vector<int64_t> haloIds;
+    for (int64_t i = 0; i < n; ++i) {
+      if (seen.count(id[i])) raise(ESPP_EINVAL, "duplicate particle id " + std::to_string(id[i]));
+      seen[id[i]] = 1;
+      const int ty = type ? type[i] : 0;
+      if (ty < 0 || ty >= kMaxTypes) raise(ESPP_ERANGE, "particle type out of range [0, 8)");
+      h.type.push_back(ty);
+      s->maxType = std::max(s->maxType, ty);
+      h.mass.push_back(mass ? mass[i] : 1.0);
+      for (int k = 0; k < 3; ++k) {
+        h.x.push_back(pos[3 * i + k]);  // as integrated: the next step re-sorts and folds
+        h.v.push_back(vel ? vel[3 * i + k] : 0.0);
+        h.f.push_back(0.0);
+        h.img.push_back(img ? img[3 * i + k] : 0);
+      }
+      if (halo && halo[i]) haloIds.push_back(id[i]);
+    }
+    upload(s, h);
+    upload_lj(s);
+    s->allIds = h.id;
+    s->haloIds.swap(haloIds);
+    s->idDirty = true;
+    s->resortFlag = true;
+    s->binned = false;
+    s->listValid = false;
+  });
+}
+
+int espp_dd_set_halo_positions(espp_system* s, int64_t n, const int64_t* ids,
+                               const double* pos) {
+  return guard([&] {
+    checked(s);
+    if (n <= 0) return;
+    if (!ids || !pos) raise(ESPP_EINVAL, "null id or position array");
+    ensure_id_map(s);
+    ensure_stage(s, n);
+    cuda_check(cudaMemcpyAsync(s->stIds, ids, sizeof(int64_t) * n, cudaMemcpyHostToDevice,
+                               s->st), "upload ids");
+    cuda_check(cudaMemcpyAsync(s->stPos, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice,
+                               s->st), "upload");
+    launch_set_by_id(s->view(), (int)n, s->stIds, s->stPos, nullptr, nullptr, s->st);
+    unsigned e = read_err(s);
+    if (e & kErrIdRange) {
+      cuda_check(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->st), "memset");
+      raise(ESPP_EINVAL, "unknown particle id");
+    }
+    // the pair list stays: halo copies move like the particles they copy
+  });
+}
+
+int espp_dd_run_begin(espp_system* s, int64_t nsteps, double* maxd) {
+  return guard([&] {
+    checked(s);
+    if (nsteps < 0 || !maxd) raise(ESPP_EINVAL, "bad arguments");
+    if (!s->haloIds.empty() && (!s->triples.empty() || s->mlp))
+      raise(ESPP_EINVAL, "angles and the learned potential are not available with halo "
+                         "particles (spatial decomposition)");
+    s->ddT0 = now_s();
+    s->ddTResort = 0.0;
+    s->ddArgs = run_prologue(s, nsteps, s->ddTResort);
+    s->ddRun = true;
+    s->ddSteps = nsteps;
+    s->ddDone = 0;
+    *maxd = nsteps > 0 ? take_max_disp(s) : 0.0;
+  });
+}
+
+int espp_dd_step(espp_system* s, int32_t resort, double* maxd) {
+  return guard([&] {
+    checked(s);
+    if (!maxd) raise(ESPP_EINVAL, "null output pointer");
+    if (!s->ddRun || s->ddDone >= s->ddSteps)
+      raise(ESPP_ESTATE, "no step of a decomposed run is pending");
+    if (resort || s->resortFlag) {
+      const double tr = now_s();
+      if (s->idDirty) rebuild_id_tables(s);
+      timed_decompose(s);
+      s->resortFlag = false;
+      s->nResorts++;
+      s->ddTResort += now_s() - tr;
+    }
+    timed_forces(s);
+    const bool last = s->ddDone + 1 == s->ddSteps;
+    IntegrateArgs aj = s->ddArgs;
+    aj.step = s->step;
+    aj.do_i1 = last ? 0 : 1;
+    aj.storeFtot = last ? 1 : 0;
+    timed_integrate(s, aj);
+    cuda_check(cudaGetLastError(), "step kernels");
+    s->step++;
+    s->ddDone++;
+    *maxd = last ? 0.0 : take_max_disp(s);
+  });
+}
+
+int espp_dd_run_end(espp_system* s) {
+  return guard([&] {
+    checked(s);
+    if (!s->ddRun) raise(ESPP_ESTATE, "no decomposed run in progress");
+    s->ddRun = false;
+    cuda_check(cudaEventRecord(s->runEnd, s->st), "event");
+    run_epilogue(s, s->ddT0, s->ddTResort, false);
+  });
+}
+
 int espp_num_resorts(espp_system* s, int64_t* n) {
   return guard([&] { *n = checked(s)->nResorts; });
 }
@@ -2397,7 +2557,7 @@ int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n) {
   return guard([&] {
     checked(s);
     *sum_mv2 = 0.0;
-    *n = s->n;
+    *n = s->n - (int64_t)s->haloIds.size();
     if (s->n == 0) return;
     int nb;
     double* part = obs_partials(s, nb);
@@ -2678,6 +2838,8 @@ int espp_rdf(espp_system* s, int32_t rdfN, double* out) {
   return guard([&] {
     checked(s);
     if (rdfN <= 0 || !out) raise(ESPP_EINVAL, "rdfN must be positive");
+    if (!s->haloIds.empty())
+      raise(ESPP_EINVAL, "the RDF is not available with halo particles (spatial decomposition)");
     if (s->idDirty) rebuild_id_tables(s);
     if (!s->binned) bin(s, false);
     // dr from half the y edge, as the reference does (RadialDistrF.cpp:59-60)

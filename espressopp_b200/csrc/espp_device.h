@@ -23,6 +23,24 @@ __device__ __forceinline__ int4 fixed_coords(const DevView& d, double x, double 
   return make_int4((int)(unsigned)qx, (int)(unsigned)qy, (int)(unsigned)qz, type);
 }
 
+// A halo particle is a copy of a particle that another domain of a spatial
+// decomposition owns (a ghost of DomainDecomposition's frame cells, DomainDecomposition.
+// cpp:1243-1391): it takes part in this domain's pairs and bonds as a partner only, is not
+// integrated or thermostatted, and is skipped as the first particle of every observable.
+__device__ __forceinline__ bool is_halo(const DevView& d, int64_t id) {
+  return d.halo && d.halo[id - d.idMin];
+}
+
+// Pair (i, j) of a full list is counted once by the observables: by its lower sorted index
+// in a system without halo particles; with halo particles, a pair of two owned particles
+// by the lower index and a pair with a halo partner by the lower id, so that the domains
+// of a decomposition together count every pair once.
+__device__ __forceinline__ bool pair_counted_here(const DevView& d, int i, int j, int64_t idi,
+                                                  int64_t idj) {
+  if (!d.halo) return j > i;
+  return d.halo[idj - d.idMin] ? idj > idi : j > i;
+}
+
 // FixedPairListInteractionTemplate.hpp:145-150: every force pass raises the list's
 // long-time maximum bond length^2 to the longest bond it saw.  The maximum is kept as the
 // bits of a non-negative double, which order like unsigned integers; the atomic is issued

@@ -168,6 +168,7 @@ struct DevView {
   int32_t* bondStart;     // idSpan + 1, CSR of bond partners by id - idMin
   int64_t* bondPartner;   // partner ids
   uint8_t* langExcl;      // idSpan: 1 if the Langevin thermostat skips this id
+  uint8_t* halo;          // idSpan: 1 for a copy of another domain's particle (or null)
   int32_t* exclStart;     // idSpan + 1, Verlet-list exclusions by id (or null)
   int64_t* exclIds;
   const LJPair* lj;       // ntypes*ntypes FP64 table (device)

@@ -1037,7 +1037,7 @@ __global__ void __launch_bounds__(256) k_integrate(DevView d, IntegrateArgs a) {
   }
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double sq = 0.0;
-  if (i < d.n) {
+  if (i < d.n && !(d.halo && d.halo[P.id[i] - d.idMin])) {  // halo copies stay put
     const size_t cap = d.cap;
     const double m = P.mass[i];
     double F[3], v[3], x[3];
@@ -1164,7 +1164,7 @@ __global__ void k_lj_obs(DevView d, int energy, double* partials) {
   const ParticleArrays a = d.pa[0];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  if (i < d.n) {
+  if (i < d.n && !is_halo(d, a.id[i])) {
     const double* X = a.x;
     const double* Y = a.x + d.cap;
     const double* Z = a.x + 2 * (size_t)d.cap;
@@ -1173,7 +1173,7 @@ __global__ void k_lj_obs(DevView d, int energy, double* partials) {
     const int cnt = d.nn[i];
     for (int k = 0; k < cnt; ++k) {
       const int j = d.nl[nl_index(k, i, d.cap)];
-      if (j < i) continue;
+      if (d.halo ? !pair_counted_here(d, i, j, a.id[i], a.id[j]) : j < i) continue;
       const double dx = min_image(xi - X[j], d.L[0], d.halfL[0]);
       const double dy = min_image(yi - Y[j], d.L[1], d.halfL[1]);
       const double dz = min_image(zi - Z[j], d.L[2], d.halfL[2]);
@@ -1215,7 +1215,7 @@ __global__ void k_fene_obs(DevView d, FENEParams fp, int energy, double* partial
   const ParticleArrays a = d.pa[0];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  if (i < d.n && fp.on) {
+  if (i < d.n && fp.on && !is_halo(d, a.id[i])) {
     const double* X = a.x;
     const double* Y = a.x + d.cap;
     const double* Z = a.x + 2 * (size_t)d.cap;
@@ -1611,13 +1611,13 @@ __global__ void k_tab_obs(DevView d, int bond, int energy, double* partials) {
       acc[6] += dy * f2;
     }
   };
-  if (i < d.n) {
+  if (i < d.n && !is_halo(d, a.id[i])) {
     if (!bond && d.tabNT > 0) {
       const int ti = a.type[i];
       const int cnt = d.nn[i];
       for (int k = 0; k < cnt; ++k) {
         const int j = d.nl[nl_index(k, i, d.cap)];
-        if (j < i) continue;
+        if (d.halo ? !pair_counted_here(d, i, j, a.id[i], a.id[j]) : j < i) continue;
         const int tj = a.type[j];
         if (ti >= d.tabNT || tj >= d.tabNT) continue;
         const int t = d.tabPair[ti * d.tabNT + tj];
@@ -1641,7 +1641,7 @@ __global__ void k_kinetic(DevView d, double* partials) {
   const ParticleArrays a = d.pa[0];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[1] = {0.0};
-  if (i < d.n) {
+  if (i < d.n && !is_halo(d, a.id[i])) {
     const double vx = a.v[i], vy = a.v[(size_t)d.cap + i], vz = a.v[2 * (size_t)d.cap + i];
     acc[0] = a.mass[i] * (vx * vx + vy * vy + vz * vz);
   }
@@ -1654,7 +1654,7 @@ __global__ void k_kinetic_types(DevView d, unsigned long long typeMask, double* 
   const ParticleArrays a = d.pa[0];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[2] = {0.0, 0.0};
-  if (i < d.n) {
+  if (i < d.n && !is_halo(d, a.id[i])) {
     const int t = a.type[i];
     if (t >= 0 && t < 64 && ((typeMask >> t) & 1ull)) {
       const double vx = a.v[i], vy = a.v[(size_t)d.cap + i], vz = a.v[2 * (size_t)d.cap + i];
@@ -1670,7 +1670,7 @@ __global__ void k_kinetic_tensor(DevView d, double* partials) {
   const ParticleArrays a = d.pa[0];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  if (i < d.n) {
+  if (i < d.n && !is_halo(d, a.id[i])) {
     const double v[3] = {a.v[i], a.v[(size_t)d.cap + i], a.v[2 * (size_t)d.cap + i]};
     const double m = a.mass[i];
     acc[0] = __dmul_rn(m, __dmul_rn(v[0], v[0]));
@@ -1688,6 +1688,10 @@ __global__ void k_pair_count(DevView d, int32_t* counts) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.n) return;
   const int64_t idi = a.id[i];
+  if (is_halo(d, idi)) {  // pairs of a halo particle are listed by the domain owning it
+    counts[i] = 0;
+    return;
+  }
   int c = 0;
   for (int k = 0; k < d.nn[i]; ++k) c += a.id[d.nl[nl_index(k, i, d.cap)]] > idi;
   counts[i] = c;
@@ -1698,6 +1702,7 @@ __global__ void k_pair_write(DevView d, const int64_t* offsets, int64_t* out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.n) return;
   const int64_t idi = a.id[i];
+  if (is_halo(d, idi)) return;
   int64_t o = offsets[i];
   for (int k = 0; k < d.nn[i]; ++k) {
     const int64_t idj = a.id[d.nl[nl_index(k, i, d.cap)]];
@@ -1718,7 +1723,7 @@ __global__ void k_pair_digest(DevView d, unsigned long long* partials) {
   const ParticleArrays a = d.pa[0];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long v[4] = {0ull, 0ull, 0ull, 0ull};
-  if (i < d.n) {
+  if (i < d.n && !is_halo(d, a.id[i])) {
     const int64_t idi = a.id[i];
     const unsigned long long hi0 = digest_mix((unsigned long long)idi);
     for (int k = 0; k < d.nn[i]; ++k) {

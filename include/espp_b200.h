@@ -213,6 +213,33 @@ ESPP_API int espp_capforce_set(espp_system* s, int32_t mode, const double cap[3]
 /* VelocityVerlet::run (src/integrator/VelocityVerlet.cpp:63-169). */
 ESPP_API int espp_run(espp_system* s, int64_t nsteps);
 /* VelocityVerlet::getNumResorts (:246). */
+/* ---- spatial decomposition: one system per domain -------------------------------------
+ * DomainDecomposition over several domains (src/storage/DomainDecomposition.cpp:1031-1158
+ * migration, :1243-1391 ghost frames; one domain per GPU).  Each domain's system holds the
+ * particles it owns and halo copies of the particles of the neighbouring domains' boundary
+ * cells; halo particles are partners only: not integrated, not thermostatted, and skipped
+ * as the first particle of every observable, so that energies, virials, kinetic sums and
+ * pair sets of all domains add up to the undecomposed system's (a pair with a halo partner
+ * is counted by the domain owning the smaller id).  Angles, the learned potential and the
+ * RDF are refused while halo particles are present.
+ * espp_dd_load replaces every particle of the system (positions as integrated, not
+ * folded: the next step re-sorts them; halo[i] != 0 marks halo copies).
+ * espp_dd_set_halo_positions moves halo copies to their owners' positions (no re-sort).
+ * A run of nsteps is espp_dd_run_begin (re-sort if loaded, start-of-run force with the
+ * Langevin heat-up, integrate1 of step 0), nsteps x espp_dd_step (re-sort when resort or
+ * after a load, force, aftCalcF + integrate2, integrate1 of the next step), then
+ * espp_dd_run_end; begin and step return the step's largest displacement sqrt(max |dx|^2)
+ * over the owned particles (0 after the last step), from which the host decides the next
+ * re-sort (VelocityVerlet.cpp:63-169). */
+ESPP_API int espp_dd_load(espp_system* s, int64_t n, const int64_t* id, const int32_t* type,
+                          const double* mass, const double* pos, const double* vel,
+                          const int32_t* img, const uint8_t* halo);
+ESPP_API int espp_dd_set_halo_positions(espp_system* s, int64_t n, const int64_t* ids,
+                                        const double* pos);
+ESPP_API int espp_dd_run_begin(espp_system* s, int64_t nsteps, double* maxd);
+ESPP_API int espp_dd_step(espp_system* s, int32_t resort, double* maxd);
+ESPP_API int espp_dd_run_end(espp_system* s);
+
 ESPP_API int espp_num_resorts(espp_system* s, int64_t* n);
 /* VelocityVerlet::loadTimers (:206-218): run, pair, FENE, angle, comm1, comm2, int1,
  * int2, resort, other (seconds). */

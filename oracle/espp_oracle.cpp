@@ -29,6 +29,7 @@
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
+#include <unordered_set>
 #include <utility>
 #include <vector>
 
@@ -94,6 +95,7 @@ struct Particle {
   double f[3] = {0, 0, 0};
   int32_t img[3] = {0, 0, 0};
   bool ghost = false;
+  bool halo = false;  // copy of a particle another domain of a decomposition owns
 };
 
 struct NeighborCell {
@@ -421,6 +423,11 @@ struct espp_system {
   int langPhase = 0;
   espp_mlp* mlp = nullptr;
   std::unordered_map<int64_t, std::array<double, 3>> facc;
+  // spatial decomposition (one system per domain): halo particles are copies of other
+  // domains' particles; a run is driven step by step by the decomposition's host loop
+  int64_t nHalo = 0;
+  bool ddRun = false;
+  int64_t ddSteps = 0, ddDone = 0;
   bool vecMode = false;  // re-sorts load the SoA array and build the vec list
   bool aosStale = false;  // a vec run left the AoS ghosts and pair list behind
   VecArrays vec;
@@ -432,6 +439,15 @@ const double ROUND_ERROR_PREC = std::numeric_limits<double>::epsilon();
 
 int cellIndex(const espp_system* s, int m, int n, int o) {
   return m + s->F[0] * (n + s->F[1] * o);
+}
+
+// A pair (or bond) is counted by the observables of the domain that owns both particles,
+// or, with one halo partner, by the domain that owns the smaller id: the domains of a
+// decomposition together count each pair once (one domain: every pair).
+bool countedHere(const Particle* a, const Particle* b) {
+  if (!a->halo && !b->halo) return true;
+  if (a->halo && b->halo) return false;
+  return a->halo ? b->id < a->id : a->id < b->id;
 }
 
 // OrthorhombicBC::foldCoordinate (src/bc/OrthorhombicBC.cpp:144-161).
@@ -1113,7 +1129,7 @@ void updateForces(espp_system* s) {
   if (s->lang_on) {
     for (int ci : s->realCells)
       for (auto& p : s->cells[ci].p) {
-        if (s->langExcl.count(p.id)) continue;
+        if (p.halo || s->langExcl.count(p.id)) continue;
         double massf = std::sqrt(p.mass);
         double u[3];
         langevin_uniforms(s->seed, p.id, s->step, s->langPhase, u);
@@ -1150,6 +1166,7 @@ double integrate1(espp_system* s) {
   double maxSqDist = 0.0;
   for (int ci : s->realCells)
     for (auto& p : s->cells[ci].p) {
+      if (p.halo) continue;  // integrated by the domain that owns it
       double dtfm = 0.5 * s->dt / p.mass;
       double sq = 0.0;
       double dp[3];
@@ -1169,6 +1186,7 @@ void integrate2(espp_system* s) {
   double half_dt = 0.5 * s->dt;
   for (int ci : s->realCells)
     for (auto& p : s->cells[ci].p) {
+      if (p.halo) continue;
       double dtfm = half_dt / p.mass;
       for (int k = 0; k < 3; ++k) p.v[k] += dtfm * p.f[k];
     }
@@ -1795,7 +1813,9 @@ int espp_vl_rebuild(espp_system* s) {
 int espp_vl_size(espp_system* s, int64_t* npairs) {
   CHECK_S(s);
   ensureAos(s);
-  *npairs = (int64_t)s->vlPairs.size();
+  int64_t n = 0;
+  for (auto& pr : s->vlPairs) n += countedHere(pr.first, pr.second) ? 1 : 0;
+  *npairs = n;
   return ESPP_OK;
 }
 
@@ -1805,6 +1825,7 @@ int espp_vl_pairs(espp_system* s, int64_t cap, int64_t* pairs, int64_t* npairs) 
   std::vector<std::pair<int64_t, int64_t>> v;
   v.reserve(s->vlPairs.size());
   for (auto& pr : s->vlPairs) {
+    if (!countedHere(pr.first, pr.second)) continue;
     int64_t a = pr.first->id, b = pr.second->id;
     v.push_back({std::min(a, b), std::max(a, b)});
   }
@@ -1832,6 +1853,7 @@ int espp_vl_digest(espp_system* s, uint64_t out[4]) {
   ensureAos(s);
   uint64_t cnt = 0, sum = 0, x = 0, sum2 = 0;
   for (auto& pr : s->vlPairs) {
+    if (!countedHere(pr.first, pr.second)) continue;
     const int64_t a = pr.first->id, b = pr.second->id;
     const uint64_t h = digest_mix(digest_mix((uint64_t)std::min(a, b)) ^ (uint64_t)std::max(a, b));
     cnt += 1;
@@ -2239,6 +2261,120 @@ int espp_vec_pairs(espp_system* s, int64_t cap, int64_t* pairs, int64_t* npairs)
   return ESPP_OK;
 }
 
+// ---- spatial decomposition: one system per domain --------------------------------------
+// DomainDecomposition over several domains (DomainDecomposition.cpp:1031-1158 for the
+// migration, :1243-1391 for the ghost frames): the decomposition's host loop moves
+// particles between the domains' systems and refreshes the halo copies between the
+// phases of a run below, which split VelocityVerlet::run (:63-169) at the points where
+// the reference communicates.
+
+int espp_dd_load(espp_system* s, int64_t n, const int64_t* id, const int32_t* type,
+                 const double* mass, const double* pos, const double* vel, const int32_t* img,
+                 const uint8_t* halo) {
+  CHECK_S(s);
+  ensureAos(s);
+  s->vec.loaded = false;
+  if (n < 0 || (n > 0 && (!id || !pos))) return fail(ESPP_EINVAL, "bad particle arrays");
+  std::unordered_set<int64_t> seen;
+  for (int64_t i = 0; i < n; ++i)
+    if (!seen.insert(id[i]).second) return fail(ESPP_EINVAL, "duplicate particle id");
+  for (auto& c : s->cells) c.p.clear();
+  s->where.clear();
+  s->vlPairs.clear();
+  s->bondPtrs.clear();
+  s->nHalo = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    Particle p;
+    p.id = id[i];
+    p.type = type ? type[i] : 0;
+    p.mass = mass ? mass[i] : 1.0;
+    for (int k = 0; k < 3; ++k) {
+      p.r[k] = pos[3 * i + k];  // as integrated: the next step re-sorts and folds
+      p.v[k] = vel ? vel[3 * i + k] : 0.0;
+      p.img[k] = img ? img[3 * i + k] : 0;
+    }
+    p.halo = halo && halo[i];
+    s->nHalo += p.halo ? 1 : 0;
+    const int c = mapClipped(s, p.r);
+    s->cells[c].p.push_back(p);
+    s->where[p.id] = {c, (int)s->cells[c].p.size() - 1};
+  }
+  s->resortFlag = true;
+  return ESPP_OK;
+}
+
+int espp_dd_set_halo_positions(espp_system* s, int64_t n, const int64_t* ids,
+                               const double* pos) {
+  CHECK_S(s);
+  for (int64_t i = 0; i < n; ++i) {
+    Particle* p = lookup(s, ids[i]);
+    if (!p) return fail(ESPP_EINVAL, "unknown particle id");
+    if (!p->halo) return fail(ESPP_EINVAL, "not a halo particle");
+    for (int k = 0; k < 3; ++k) p->r[k] = pos[3 * i + k];
+  }
+  return ESPP_OK;
+}
+
+int espp_dd_run_begin(espp_system* s, int64_t nsteps, double* maxd) {
+  CHECK_S(s);
+  ensureAos(s);
+  if (nsteps < 0 || !maxd) return fail(ESPP_EINVAL, "bad arguments");
+  if (s->nHalo > 0 && (!s->triplesGlobal.empty() || s->mlp))
+    return fail(ESPP_EINVAL, "angles and the learned potential are not available with halo "
+                             "particles (spatial decomposition)");
+  s->vec.loaded = false;
+  s->nResorts = 0;
+  if (s->lang_on) {
+    s->pref1 = -s->gamma;
+    s->pref2 = std::sqrt(24.0 * s->temperature * s->gamma / s->dt);
+  }
+  if (s->resortFlag) {
+    int rc = decompose(s);
+    if (rc) return rc;
+    s->maxDist = 0.0;
+    s->resortFlag = false;
+  }
+  if (s->lang_on) {
+    s->pref2buffer = s->pref2;
+    s->pref2 *= std::sqrt(3.0);
+  }
+  s->langPhase = 1;
+  updateForces(s);
+  s->langPhase = 0;
+  if (s->lang_on) s->pref2 = s->pref2buffer;
+  s->ddRun = true;
+  s->ddSteps = nsteps;
+  s->ddDone = 0;
+  *maxd = nsteps > 0 ? integrate1(s) : 0.0;
+  return ESPP_OK;
+}
+
+int espp_dd_step(espp_system* s, int32_t resort, double* maxd) {
+  CHECK_S(s);
+  if (!maxd) return fail(ESPP_EINVAL, "null output pointer");
+  if (!s->ddRun || s->ddDone >= s->ddSteps)
+    return fail(ESPP_ESTATE, "no step of a decomposed run is pending");
+  if (resort || s->resortFlag) {
+    int rc = decompose(s);
+    if (rc) return rc;
+    s->maxDist = 0.0;
+    s->resortFlag = false;
+    s->nResorts++;
+  }
+  updateForces(s);
+  integrate2(s);
+  s->ddDone++;
+  *maxd = s->ddDone < s->ddSteps ? integrate1(s) : 0.0;
+  return ESPP_OK;
+}
+
+int espp_dd_run_end(espp_system* s) {
+  CHECK_S(s);
+  if (!s->ddRun) return fail(ESPP_ESTATE, "no decomposed run in progress");
+  s->ddRun = false;
+  return ESPP_OK;
+}
+
 int espp_num_resorts(espp_system* s, int64_t* n) {
   CHECK_S(s);
   *n = s->nResorts;
@@ -2254,9 +2390,14 @@ int espp_timers(espp_system* s, double t[10]) {
 int espp_energy(espp_system* s, int32_t which, double* e) {
   CHECK_S(s);
   ensureAos(s);
+  if (s->nHalo > 0 &&
+      (which == ESPP_IA_COSINE || which == ESPP_IA_TAB_ANGLE || which == ESPP_IA_MLP))
+    return fail(ESPP_EINVAL, "angle and learned-potential observables are not available with "
+                             "halo particles (spatial decomposition)");
   double es = 0.0;
   if (which == ESPP_IA_LJ) {
     for (auto& pr : s->vlPairs) {
+      if (!countedHere(pr.first, pr.second)) continue;
       const LJParams* P = ljFor(s, pr.first->type, pr.second->type);
       if (!P) continue;
       double d[3] = {pr.first->r[0] - pr.second->r[0], pr.first->r[1] - pr.second->r[1],
@@ -2266,6 +2407,7 @@ int espp_energy(espp_system* s, int32_t which, double* e) {
   } else if (which == ESPP_IA_FENE) {
     if (s->fene_on)
       for (auto& pr : s->bondPtrs) {
+        if (!countedHere(pr.first, pr.second)) continue;
         double d[3];
         minImageBox(s, pr.first->r, pr.second->r, d);
         es += feneEnergy(s, d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
@@ -2273,6 +2415,7 @@ int espp_energy(espp_system* s, int32_t which, double* e) {
   } else if (which == ESPP_IA_TAB_PAIR) {
     if (s->has_vl)
       for (auto& pr : s->vlPairs) {
+        if (!countedHere(pr.first, pr.second)) continue;
         auto it = s->tabPair.find({std::min(pr.first->type, pr.second->type),
                                    std::max(pr.first->type, pr.second->type)});
         if (it == s->tabPair.end()) continue;
@@ -2283,6 +2426,7 @@ int espp_energy(espp_system* s, int32_t which, double* e) {
   } else if (which == ESPP_IA_TAB_BOND) {
     if (s->tabBondOn)
       for (auto& pr : s->bondPtrs) {
+        if (!countedHere(pr.first, pr.second)) continue;
         double d[3];
         minImageBox(s, pr.first->r, pr.second->r, d);
         es += s->tabBond.energy(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
@@ -2335,6 +2479,9 @@ int espp_energy(espp_system* s, int32_t which, double* e) {
 
 static int virialImpl(espp_system* s, int32_t which, double* wsc, double w6[6]) {
   ensureAos(s);
+  if (s->nHalo > 0 && (which == ESPP_IA_COSINE || which == ESPP_IA_TAB_ANGLE))
+    return fail(ESPP_EINVAL, "angle observables are not available with halo particles "
+                             "(spatial decomposition)");
   double w = 0.0;
   double t[6] = {0, 0, 0, 0, 0, 0};
   auto acc = [&](const double d[3], const double f[3]) {
@@ -2348,6 +2495,7 @@ static int virialImpl(espp_system* s, int32_t which, double* wsc, double w6[6]) 
   };
   if (which == ESPP_IA_LJ) {
     for (auto& pr : s->vlPairs) {
+      if (!countedHere(pr.first, pr.second)) continue;
       const LJParams* P = ljFor(s, pr.first->type, pr.second->type);
       if (!P) continue;
       double d[3] = {pr.first->r[0] - pr.second->r[0], pr.first->r[1] - pr.second->r[1],
@@ -2358,6 +2506,7 @@ static int virialImpl(espp_system* s, int32_t which, double* wsc, double w6[6]) 
   } else if (which == ESPP_IA_FENE) {
     if (s->fene_on)
       for (auto& pr : s->bondPtrs) {
+        if (!countedHere(pr.first, pr.second)) continue;
         double d[3];
         minImageBox(s, pr.first->r, pr.second->r, d);
         double f[3];
@@ -2394,6 +2543,7 @@ static int virialImpl(espp_system* s, int32_t which, double* wsc, double w6[6]) 
   } else if (which == ESPP_IA_TAB_PAIR) {
     if (s->has_vl)
       for (auto& pr : s->vlPairs) {
+        if (!countedHere(pr.first, pr.second)) continue;
         auto it = s->tabPair.find({std::min(pr.first->type, pr.second->type),
                                    std::max(pr.first->type, pr.second->type)});
         if (it == s->tabPair.end()) continue;
@@ -2405,6 +2555,7 @@ static int virialImpl(espp_system* s, int32_t which, double* wsc, double w6[6]) 
   } else if (which == ESPP_IA_TAB_BOND) {
     if (s->tabBondOn)
       for (auto& pr : s->bondPtrs) {
+        if (!countedHere(pr.first, pr.second)) continue;
         double d[3];
         minImageBox(s, pr.first->r, pr.second->r, d);
         double f[3];
@@ -2592,6 +2743,9 @@ int espp_msd_chain_com(espp_confs* c, int32_t chainlength, double* out) {
 int espp_rdf(espp_system* s, int32_t rdfN, double* out) {
   CHECK_S(s);
   if (rdfN <= 0 || !out) return fail(ESPP_EINVAL, "rdfN must be positive");
+  if (s->nHalo > 0)
+    return fail(ESPP_EINVAL, "the RDF is not available with halo particles (spatial "
+                             "decomposition)");
   double Li[3] = {s->L[0], s->L[1], s->L[2]};
   double Li_half[3] = {Li[0] / 2., Li[1] / 2., Li[2] / 2.};
   std::vector<double> histogram(rdfN, 0.0);
@@ -2636,6 +2790,7 @@ int espp_kinetic_tensor(espp_system* s, double out[6]) {
   double t[6] = {0, 0, 0, 0, 0, 0};
   for (int ci : s->realCells)
     for (auto& p : s->cells[ci].p) {
+      if (p.halo) continue;
       const double* v = p.v;
       const double vv[6] = {v[0] * v[0], v[1] * v[1], v[2] * v[2],
                             v[0] * v[1], v[0] * v[2], v[1] * v[2]};
@@ -2651,6 +2806,7 @@ int espp_kinetic(espp_system* s, double* sum_mv2, int64_t* n) {
   int64_t cnt = 0;
   for (int ci : s->realCells)
     for (auto& p : s->cells[ci].p) {
+      if (p.halo) continue;
       v2 += p.mass * (p.v[0] * p.v[0] + p.v[1] * p.v[1] + p.v[2] * p.v[2]);
       cnt++;
     }
@@ -2666,7 +2822,7 @@ int espp_kinetic_types(espp_system* s, uint64_t type_mask, double* sum_mv2, int6
   int64_t cnt = 0;
   for (int ci : s->realCells)
     for (auto& p : s->cells[ci].p) {
-      if (p.type < 0 || p.type >= 64 || !((type_mask >> p.type) & 1u)) continue;
+      if (p.halo || p.type < 0 || p.type >= 64 || !((type_mask >> p.type) & 1u)) continue;
       v2 += p.mass * (p.v[0] * p.v[0] + p.v[1] * p.v[1] + p.v[2] * p.v[2]);
       cnt++;
     }

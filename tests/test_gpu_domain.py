@@ -1,0 +1,127 @@
+"""Spatial domain decomposition on the GPU: two and three slab domains, each a system of
+the CUDA library, driven in one process on one device (the halo refresh and the
+migration go through the host, so no kernel waits on another domain).  Against one
+undecomposed CUDA system and against the FP64 oracle: the pair set (bit-exact), energies,
+virials, kinetic sums and forces, and a Langevin run with the same re-sort steps
+(DomainDecomposition.cpp:1031-1391, VelocityVerlet.cpp:63-169).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from espressopp_b200 import _abi
+from espressopp_b200.domain import SpatialDecomposition
+from simdriver import Sim, cell_grid, cuda_lib, lattice, mb_velocities, oracle_lib
+
+pytestmark = pytest.mark.gpu
+
+RC, SKIN = 2.5, 0.3
+SHIFT = 4.0 * (RC ** -12 - RC ** -6)
+
+
+def _inputs(n_side):
+    pos, box = lattice(n_side, 0.8442, 0.05, 3)
+    vel = mb_velocities(len(pos), 1.0, 4)
+    return np.arange(len(pos), dtype=np.int64), pos, vel, box
+
+
+def _plain(lib, prec, ids, pos, vel, box, cg):
+    s = Sim(lib, box, SKIN, cg, precision=prec, seed=4)
+    s.add(ids, pos, vel)
+    s.decompose()
+    s.vl(RC)
+    s.lj(0, 0, 1.0, 1.0, RC, SHIFT)
+    s.integrator(0.005)
+    s.langevin(1.0, 1.0)
+    return s
+
+
+def _decomposed(prec, ids, pos, vel, box, cg, D):
+    dd = SpatialDecomposition(box, SKIN, cg, D, precision=prec, seed=4, lib=cuda_lib())
+    dd.add_particles(ids, pos, vel)
+    dd.decompose()
+    dd.vl_create(RC)
+    dd.lj_set(0, 0, 1.0, 1.0, RC, SHIFT)
+    dd.integrator_set(0.005)
+    dd.langevin_set(1, 1.0, 1.0)
+    return dd
+
+
+@pytest.mark.parametrize("D", [2, 3])
+@pytest.mark.parametrize("prec", [_abi.PREC_FP64, _abi.PREC_MIXED])
+def test_decomposed_fluid_matches_one_system(D, prec):
+    ids, pos, vel, box = _inputs(16)  # 4096 particles, 5^3 cells
+    cg = cell_grid(box, RC, SKIN)
+    one = _plain(cuda_lib(), prec, ids, pos, vel, box, cg)
+    orc = _plain(oracle_lib(), _abi.PREC_FP64, ids, pos, vel, box, cg)
+    dd = _decomposed(prec, ids, pos, vel, box, cg, D)
+    assert all(h > 0 for _, h in dd.domain_sizes())
+    for s in (one, orc, dd):
+        s.run(0)
+    assert dd.vl_size() == orc.vl_size()
+    assert np.array_equal(dd.vl_pairs(), orc.pairs())
+    assert dd.vl_digest() == orc.digest() == one.digest()
+    fp64 = prec == _abi.PREC_FP64
+    assert math.isclose(dd.energy(_abi.IA_LJ), orc.energy(_abi.IA_LJ), rel_tol=1e-10)
+    assert math.isclose(dd.virial(_abi.IA_LJ), orc.virial(_abi.IA_LJ), rel_tol=1e-10)
+    k, n = dd.kinetic()
+    assert n == len(ids) and math.isclose(k, orc.kinetic()[0], rel_tol=1e-12)
+    f, fo = dd.get_particles(ids)[2], orc.particles(ids)[2]
+    assert math.sqrt(np.sum((f - fo) ** 2) / np.sum(fo ** 2)) < (1e-12 if fp64 else 1e-5)
+    # against the undecomposed CUDA system: the same kernels on lists in another order
+    # (mixed precision: FP32 sums in that order)
+    f1 = one.particles(ids)[2]
+    assert math.sqrt(np.sum((f - f1) ** 2) / np.sum(f1 ** 2)) < (1e-12 if fp64 else 1e-6)
+    for s in (one, dd):
+        s.run(120)
+    assert dd.resorts == one.num_resorts() > 3
+    x, _, _, img = dd.get_particles(ids)
+    x1, _, _, i1 = one.particles(ids)
+    if fp64:
+        assert np.array_equal(img, i1) and np.max(np.abs(x - x1)) < 1e-9
+        assert dd.vl_digest() == one.digest()
+    else:  # the FP32 rounding differences grow along the run
+        assert np.max(np.abs((x + img * box) - (x1 + i1 * box))) < 1e-3
+
+
+def test_decomposed_melt_bonds_on_gpu():
+    """Kremer-Grest melt over 3 slabs (FP64): FENE bonds across slab boundaries, capped
+    WCA, Langevin; energies and positions against one CUDA system, and the long-time
+    maximum bond."""
+    from espressopp_b200.tools import topology
+    pos, bonds, L = topology.polymer_melt(20, 50, 0.85, seed=3)
+    box = np.array([L, L, L])
+    rc = 2.0 ** (1.0 / 6.0)
+    shift = 4.0 * ((1.0 / rc ** 2) ** 6 - (1.0 / rc ** 2) ** 3)
+    ids = np.arange(1, len(pos) + 1, dtype=np.int64)
+    cg = cell_grid(box, rc, 0.3)
+    one = Sim(cuda_lib(), box, 0.3, cg, seed=11)
+    one.add(ids, pos)
+    one.decompose()
+    one.vl(rc)
+    one.lj(0, 0, 1.0, 1.0, rc, shift, caprad=0.9)
+    one.bonds(bonds)
+    one.fene(30.0, 0.0, 1.5)
+    one.integrator(0.01)
+    one.langevin(0.5, 1.0)
+    dd = SpatialDecomposition(box, 0.3, cg, 3, seed=11, lib=cuda_lib())
+    dd.add_particles(ids, pos)
+    dd.decompose()
+    dd.vl_create(rc)
+    dd.lj_set(0, 0, 1.0, 1.0, rc, shift, caprad=0.9)
+    dd.bonds_add(bonds)
+    dd.fene_set(30.0, 0.0, 1.5)
+    dd.integrator_set(0.01)
+    dd.langevin_set(1, 0.5, 1.0)
+    for s in (one, dd):
+        s.run(100)
+    assert dd.resorts == one.num_resorts() > 0
+    for which in (_abi.IA_LJ, _abi.IA_FENE):
+        assert math.isclose(dd.energy(which), one.energy(which), rel_tol=1e-9)
+    x, _, _, img = dd.get_particles(ids)
+    x1, _, _, i1 = one.particles(ids)
+    assert np.max(np.abs(x - x1)) < 1e-8 and np.array_equal(img, i1)
+    m1 = np.zeros(1)
+    _abi.call(one.lib, "espp_bonds_max_sqr", one.h, _abi.dptr(m1))
+    assert math.isclose(dd.bonds_max_sqr(), m1[0], rel_tol=1e-12)
