@@ -498,6 +498,117 @@ class DomainDecomposition:
         im = np.ascontiguousarray(img, np.int32).reshape(-1)
         call(self._lib, "espp_set_images", self._h, len(ids), i64ptr(ids), i32ptr(im))
 
+    _ARRAY_PROPS = ("id", "posx", "posy", "posz", "vx", "vy", "vz", "type", "mass")
+
+    def addParticlesArray(self, particleList, *properties):
+        """Storage.addParticlesArray (src/storage/Storage.py:432-535): particles as the
+        rows of a 2-d array whose columns the properties name (default id, posx, posy,
+        posz); id and the three position columns are mandatory.  Columns of properties the
+        GPU storage does not hold (modepos, f, q, radius, AdResS, ...) are accepted and
+        ignored; an unknown name is a SyntaxError, as there."""
+        known = set(self._ARRAY_PROPS) | {
+            "modeposx", "modeposy", "modeposz", "modemomx", "modemomy", "modemomz", "fx",
+            "fy", "fz", "fmx", "fmy", "fmz", "q", "radius", "fradius", "vradius", "varmass",
+            "adrat", "lambda_adr", "lambda_adrd", "state", "pib"}
+        props = [p.lower() for p in properties] if properties else ["id", "posx", "posy",
+                                                                     "posz"]
+        for p in props:
+            if p not in known:
+                raise SyntaxError("unknown particle property: %s" % p)
+        col = {p: k for k, p in enumerate(props)}
+        for p in ("id", "posx", "posy", "posz"):
+            if p not in col:
+                raise AssertionError("particle property %s is mandatory" % p)
+        for trio in (("vx", "vy", "vz"), ("fx", "fy", "fz"), ("modeposx", "modeposy",
+                     "modeposz"), ("modemomx", "modemomy", "modemomz"), ("fmx", "fmy", "fmz")):
+            if len({t in col for t in trio}) != 1:
+                raise AssertionError("Missing at least one of the 3d coordinates of property "
+                                     "\"%s\"" % trio[0][:-1])
+        arr = np.asarray(particleList, np.float64)
+        if arr.size == 0:
+            return
+        arr = arr.reshape(len(arr), -1)
+        names = ["id", "pos"]
+        rows = [[int(r[col["id"]]), Real3D(r[col["posx"]], r[col["posy"]], r[col["posz"]])]
+                for r in arr]
+        if "vx" in col:
+            names.append("v")
+            for row, r in zip(rows, arr):
+                row.append(Real3D(r[col["vx"]], r[col["vy"]], r[col["vz"]]))
+        for p in ("type", "mass"):
+            if p in col:
+                names.append(p)
+                for row, r in zip(rows, arr):
+                    row.append(int(r[col[p]]) if p == "type" else float(r[col[p]]))
+        self.addParticles(rows, *names)
+
+    def _reload(self, keep):
+        """Replaces the particle set by the particles with the given ids, state kept;
+        the next step re-sorts them."""
+        ids = np.array(sorted(keep), np.int64)
+        pos, vel, _, img = self._fetch(ids) if len(ids) else (np.zeros((0, 3)),) * 2 + (
+            None, np.zeros((0, 3), np.int32))
+        typ = np.array([self._types[int(i)] for i in ids], np.int32)
+        mass = np.array([self._masses[int(i)] for i in ids], np.float64)
+        call(self._lib, "espp_dd_load", self._h, len(ids), i64ptr(ids), i32ptr(typ),
+             dptr(mass), dptr(np.ascontiguousarray(pos)), dptr(np.ascontiguousarray(vel)),
+             i32ptr(np.ascontiguousarray(img, np.int32)), None)
+        self._types = {int(i): self._types[int(i)] for i in ids}
+        self._masses = {int(i): self._masses[int(i)] for i in ids}
+
+    def removeParticle(self, pid):
+        """Storage::removeParticle (src/storage/Storage.cpp:315-348): 1 if the particle
+        existed and was removed, else 0.  Bonds and triples of a removed particle must be
+        removed by the caller, as in the reference."""
+        pid = int(pid)
+        if pid not in self._types:
+            return 0
+        self._reload([i for i in self._types if i != pid])
+        return 1
+
+    def removeAllParticles(self):
+        """Storage::removeAllParticles (src/storage/Storage.cpp:350-358)."""
+        self._reload([])
+
+    def savePositions(self, idList):
+        """Storage::savePosition for each id (src/storage/Storage.cpp:804-829): position
+        and image of each existing particle, restored by restorePositions."""
+        ids = np.array([int(i) for i in idList if int(i) in self._types], np.int64)
+        if not hasattr(self, "_saved"):
+            self._saved = {}
+        if len(ids):
+            pos, _, _, img = self._fetch(ids)
+            for k, i in enumerate(ids):
+                self._saved[int(i)] = (pos[k].copy(), img[k].copy())
+
+    def restorePositions(self):
+        """Storage::restorePositions (src/storage/Storage.cpp:830-869)."""
+        saved = getattr(self, "_saved", {})
+        if not saved:
+            raise RuntimeError(" There is nothing to restore. Check whether you saved positions")
+        ids = np.array([i for i in saved if i in self._types], np.int64)
+        if len(ids):
+            pos = np.ascontiguousarray([saved[int(i)][0] for i in ids], np.float64)
+            img = np.ascontiguousarray([saved[int(i)][1] for i in ids], np.int32)
+            call(self._lib, "espp_set_particles", self._h, len(ids), i64ptr(ids),
+                 dptr(pos.reshape(-1)), None)
+            call(self._lib, "espp_set_images", self._h, len(ids), i64ptr(ids),
+                 i32ptr(img.reshape(-1)))
+
+    def clearSavedPositions(self):
+        self._saved = {}
+
+    def printRealParticles(self):
+        """Storage.printRealParticles (src/storage/Storage.py:426-430): one line per
+        particle, with rank 0 as the CPU column."""
+        ids = np.array(self.getRealParticleIDs(), np.int64)
+        if len(ids) == 0:
+            return
+        pos = self._fetch(ids)[0]
+        for k, pid in enumerate(ids):
+            sys.stdout.write("CPU %-3i ID %-5i TYPE %-3i POS(%8.3f, %8.3f, %8.3f)\n" % (
+                0, pid, self._types[int(pid)], pos[k][0], pos[k][1], pos[k][2]))
+
 
 class VerletList:
     """VerletList(system, cutoff, exclusionlist=[], useBuffers=True, useSOA=False)

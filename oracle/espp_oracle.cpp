@@ -2299,6 +2299,11 @@ int espp_dd_load(espp_system* s, int64_t n, const int64_t* id, const int32_t* ty
     s->cells[c].p.push_back(p);
     s->where[p.id] = {c, (int)s->cells[c].p.size() - 1};
   }
+  // lists of the new set at the unfolded positions (onParticlesChanged); the next step
+  // re-sorts
+  reindex(s);
+  ghostComm(s, true, true);
+  onParticlesChanged(s);
   s->resortFlag = true;
   return ESPP_OK;
 }

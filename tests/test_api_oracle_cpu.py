@@ -303,3 +303,40 @@ def test_fixed_pair_list_longtime_max_and_remove(on_oracle):
     assert ftl.size() == 2
     ftl.remove()
     assert ftl.size() == 0 and ftl.getTriples() == [[]]
+
+
+def test_storage_remove_save_restore_and_arrays(on_oracle, capsys):
+    """Storage (src/storage/Storage.py:198-535, Storage.cpp:315-358 and 804-869):
+    removeParticle / removeAllParticles, savePositions / restorePositions /
+    clearSavedPositions, printRealParticles and addParticlesArray."""
+    system, integ = _fluid(n=512)
+    st = system.storage
+    lj = system.getInteraction(0)
+    e_all = lj.computeEnergy()
+    assert st.removeParticle(7) == 1 and st.removeParticle(7) == 0
+    assert not st.particleExists(7) and st.getNRealParticles() == 511
+    e_less = lj.computeEnergy()
+    assert e_less != e_all
+    integ.run(20)
+    st.savePositions([3, 4, 999999])
+    p3 = np.asarray(st.getParticle(3).pos)
+    integ.run(20)
+    assert not np.allclose(np.asarray(st.getParticle(3).pos), p3)
+    st.restorePositions()
+    assert np.array_equal(np.asarray(st.getParticle(3).pos), p3)
+    st.clearSavedPositions()
+    with pytest.raises(RuntimeError, match="nothing to restore"):
+        st.restorePositions()
+    st.printRealParticles()
+    out = capsys.readouterr().out.splitlines()
+    assert len(out) == 511 and out[0].startswith("CPU 0   ID 0     TYPE 0   POS(")
+    st.removeAllParticles()
+    assert st.getNRealParticles() == 0 and lj.computeEnergy() == 0.0
+    arr = np.array([[10, 1.0, 1.0, 1.0, 0.1, 0.0, 0.0], [11, 2.2, 1.0, 1.0, 0.0, 0.0, 0.0]])
+    st.addParticlesArray(arr, "id", "posx", "posy", "posz", "vx", "vy", "vz")
+    assert st.getRealParticleIDs() == [10, 11]
+    assert np.allclose(np.asarray(st.getParticle(10).v), [0.1, 0.0, 0.0])
+    with pytest.raises(SyntaxError):
+        st.addParticlesArray(arr, "id", "posx", "posy", "posz", "bogus", "vy", "vz")
+    with pytest.raises(AssertionError):
+        st.addParticlesArray(arr[:, :3], "id", "posx", "posy")

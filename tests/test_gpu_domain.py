@@ -125,3 +125,48 @@ def test_decomposed_melt_bonds_on_gpu():
     m1 = np.zeros(1)
     _abi.call(one.lib, "espp_bonds_max_sqr", one.h, _abi.dptr(m1))
     assert math.isclose(dd.bonds_max_sqr(), m1[0], rel_tol=1e-12)
+
+
+def test_storage_removal_matches_the_oracle():
+    """storage.removeParticle / removeAllParticles of the Python mirror replace the
+    particle set through espp_dd_load (state kept, no halo copies): energies before and
+    after a run against the oracle driven the same way."""
+    import espressopp_b200 as espressopp
+    from espressopp_b200 import _lib
+    saved = _lib._lib
+    out = []
+    try:
+        for lib in (oracle_lib(), cuda_lib()):
+            _lib._lib = lib
+            x, y, z, Lx, Ly, Lz = espressopp.tools.lattice.createCubic(
+                1000, 0.8442, perfect=False, RNG=espressopp.esutil.RNG(5))
+            system = espressopp.System()
+            system.rng = espressopp.esutil.RNG(6)
+            system.bc = espressopp.bc.OrthorhombicBC(system.rng, (Lx, Ly, Lz))
+            system.skin = SKIN
+            cg = espressopp.tools.decomp.cellGrid((Lx, Ly, Lz), (1, 1, 1), RC, SKIN)
+            system.storage = espressopp.storage.DomainDecomposition(system, (1, 1, 1), cg)
+            system.storage.addParticles([[k, espressopp.Real3D(x[k], y[k], z[k])]
+                                         for k in range(len(x))], "id", "pos")
+            system.storage.decompose()
+            vl = espressopp.VerletList(system, cutoff=RC)
+            lj = espressopp.interaction.VerletListLennardJones(vl)
+            lj.setPotential(0, 0, espressopp.interaction.LennardJones(1.0, 1.0, RC, "auto"))
+            system.addInteraction(lj)
+            integ = espressopp.integrator.VelocityVerlet(system)
+            integ.dt = 0.005
+            integ.run(10)
+            for pid in (0, 17, 500):
+                system.storage.removeParticle(pid)
+            e1 = lj.computeEnergy()
+            integ.run(20)
+            ids, pos = system.storage.getAll()[:2]
+            out.append((e1, lj.computeEnergy(), ids, pos, vl.totalSize()))
+            system.storage.removeAllParticles()
+            assert lj.computeEnergy() == 0.0
+    finally:
+        _lib._lib = saved
+    (o1, o2, oi, op, on), (g1, g2, gi, gp, gn) = out
+    assert np.array_equal(oi, gi) and len(gi) == 997 and on == gn
+    assert math.isclose(g1, o1, rel_tol=1e-10) and math.isclose(g2, o2, rel_tol=1e-9)
+    assert np.max(np.abs(gp - op)) < 1e-9
