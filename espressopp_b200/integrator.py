@@ -60,25 +60,46 @@ class LangevinThermostat(Extension):
 
 
 class CapForce(Extension):
-    """integrator.CapForce(system, capForce, particleGroup=None): a scalar caps |F|,
-    a 3-vector caps each component."""
+    """integrator.CapForce(system, capForce, particleGroup=None) (CapForce.cpp:38-102,
+    170-200): a scalar caps |F| (absolute capping), a 3-vector caps each component; the
+    kind is fixed by the constructor, the setters change the values."""
 
     def __init__(self, system, capForce, particleGroup=None):
         Extension.__init__(self, system)
         if particleGroup is not None:
             raise NotImplementedError("CapForce on a particle group is not supported")
-        self.capForce = capForce
+        self._absCapping = bool(np.isscalar(capForce))
+        self._absCapForce = float(capForce) if self._absCapping else 0.0
+        self._capForce = (np.zeros(3) if self._absCapping
+                          else np.asarray(tuple(capForce), np.float64))
         self._connected = True
+
+    @property
+    def capForce(self):
+        return self._absCapForce if self._absCapping else tuple(self._capForce)
+
+    def setCapForce(self, capForce):
+        self._capForce = np.asarray(tuple(capForce), np.float64)
+
+    def setAbsCapForce(self, absCapForce):
+        self._absCapForce = float(absCapForce)
+
+    def getCapForce(self):
+        from .core import Real3D
+        return Real3D(self._capForce)
+
+    def getAbsCapForce(self):
+        return self._absCapForce
 
     def _push(self, st):
         if not self._connected:
             call(st._lib, "espp_capforce_set", st._h, _abi.CAP_OFF, None)
             return
-        if np.isscalar(self.capForce):
-            cap = np.array([float(self.capForce)] * 3)
+        if self._absCapping:
+            cap = np.array([self._absCapForce] * 3)
             mode = _abi.CAP_ABS
         else:
-            cap = np.ascontiguousarray(tuple(self.capForce), np.float64)
+            cap = np.ascontiguousarray(self._capForce, np.float64)
             mode = _abi.CAP_COMPONENT
         call(st._lib, "espp_capforce_set", st._h, mode, dptr(cap))
 

@@ -340,3 +340,25 @@ def test_storage_remove_save_restore_and_arrays(on_oracle, capsys):
         st.addParticlesArray(arr, "id", "posx", "posy", "posz", "bogus", "vy", "vz")
     with pytest.raises(AssertionError):
         st.addParticlesArray(arr[:, :3], "id", "posx", "posy")
+
+
+def test_capforce_setters(on_oracle):
+    """CapForce (CapForce.cpp:38-102, 170-200): the constructor fixes absolute or
+    per-component capping, setAbsCapForce / setCapForce change the value, the getters
+    return it; the forces after a run obey the cap."""
+    system, integ = _fluid(n=512)
+    cap = espressopp.integrator.CapForce(system, 1.0e6)
+    integ.addExtension(cap)
+    cap.setAbsCapForce(0.5)
+    assert cap.getAbsCapForce() == 0.5
+    integ.run(0)
+    f = system.storage.getAll()[3]
+    assert np.max(np.sqrt(np.sum(f * f, axis=1))) <= 0.5 * (1 + 1e-12)
+    system2, integ2 = _fluid(n=512)
+    cap2 = espressopp.integrator.CapForce(system2, espressopp.Real3D(1e6, 1e6, 1e6))
+    integ2.addExtension(cap2)
+    cap2.setCapForce(espressopp.Real3D(0.1, 0.2, 0.3))
+    assert tuple(cap2.getCapForce()) == (0.1, 0.2, 0.3)
+    integ2.run(0)
+    f2 = system2.storage.getAll()[3]
+    assert np.all(np.abs(f2) <= np.array([0.1, 0.2, 0.3]) * (1 + 1e-12))
