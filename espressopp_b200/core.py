@@ -343,19 +343,23 @@ class Particle:
 
 
 class DomainDecomposition:
-    """storage.DomainDecomposition(system, nodeGrid, cellGrid, halfCellInt) on one node
+    """storage.DomainDecomposition(system, nodeGrid, cellGrid, halfCellInt)
     (src/storage/DomainDecomposition.py:84-130, DomainDecomposition.cpp:70-85).
 
-    Creates the GPU system handle.  ``precision`` ('fp64' or 'mixed') selects the pair
-    force arithmetic; it defaults to set_default_precision()."""
+    With nodeGrid (1,1,1) it creates one GPU system handle.  With more nodes (cellGrid is
+    then one node's grid, as from tools.decomp.cellGrid) the box is cut into
+    nodeGrid[0] * nodeGrid[1] * nodeGrid[2] slabs along z, one system per slab
+    (espressopp_b200.domain): one slab per rank under torch.distributed, or all slabs in
+    this process without it.  ``precision`` ('fp64' or 'mixed') selects the pair force
+    arithmetic; it defaults to set_default_precision()."""
 
     def __init__(self, system, nodeGrid="auto", cellGrid="auto", halfCellInt="auto",
                  nocheck=False, precision=None):
         if system.bc is None:
             raise RuntimeError("system has no boundary conditions")
-        if nodeGrid != "auto" and tuple(Int3D(nodeGrid)) != (1, 1, 1):
-            raise ValueError("the GPU storage holds all particles on one device: nodeGrid "
-                             "must be (1,1,1)")
+        ng = Int3D(1, 1, 1) if nodeGrid == "auto" else Int3D(nodeGrid)
+        if min(ng) < 1:
+            raise ValueError("invalid node grid %s" % (tuple(ng),))
         if halfCellInt == "auto":
             halfCellInt = 1
         halfCellInt = int(halfCellInt)
@@ -363,24 +367,49 @@ class DomainDecomposition:
             cellGrid = Int3D(2, 2, 2)
         cellGrid = list(Int3D(cellGrid))
         for k in range(3):
-            if cellGrid[k] == 1:
+            # one node: a 1-cell dimension takes 2 cells; with several nodes the whole box
+            # has cellGrid x nodeGrid cells and the node's grid stays as given
+            if cellGrid[k] == 1 and ng[k] == 1:
                 cellGrid[k] = 2
         self.system = system
         self._cellGrid = Int3D(cellGrid)
+        self._nodeGrid = ng
         self._lib = load_library()
         self._h = ctypes.c_void_p()
         prec = _precision_code(precision if precision is not None else _DEFAULT_PRECISION)
         self.precision = prec
         box = np.ascontiguousarray(system.bc.boxL, np.float64)
-        cg = np.ascontiguousarray(self._cellGrid, np.int32)
         seed = system.rng.get_seed() if system.rng is not None else 12345
         if system.rng is not None:
             system.rng._keyed = True
-        call(self._lib, "espp_system_create", dptr(box), float(system.skin), i32ptr(cg), prec,
-             int(seed) & 0xFFFFFFFFFFFFFFFF, ctypes.byref(self._h))
         self.halfCellInt = halfCellInt
-        if halfCellInt != 1:
-            call(self._lib, "espp_set_half_cell_int", self._h, halfCellInt)
+        nodes = ng[0] * ng[1] * ng[2]
+        if nodes > 1:
+            # cellGrid is the grid of one node (DomainDecomposition.cpp:87-170): the whole
+            # box has cellGrid x nodeGrid cells, cut here into `nodes` slabs along z, one
+            # system per slab (espressopp_b200.domain)
+            from . import domain
+            from ._decomposed import DecomposedLibrary
+            comm = domain.LocalComm()
+            try:
+                import torch.distributed as dist
+                if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+                    comm = domain.TorchComm(dist)
+            except ImportError:
+                pass
+            full = [self._cellGrid[k] * ng[k] for k in range(3)]
+            self._sd = domain.SpatialDecomposition(
+                box, float(system.skin), full, nodes, precision=prec,
+                seed=int(seed) & 0xFFFFFFFFFFFFFFFF, comm=comm, lib=self._lib,
+                half_cell_int=halfCellInt)
+            self._lib = DecomposedLibrary(self._sd)
+            self._h = ctypes.c_void_p(1)  # stands for the decomposition in mirror calls
+        else:
+            cg = np.ascontiguousarray(self._cellGrid, np.int32)
+            call(self._lib, "espp_system_create", dptr(box), float(system.skin), i32ptr(cg),
+                 prec, int(seed) & 0xFFFFFFFFFFFFFFFF, ctypes.byref(self._h))
+            if halfCellInt != 1:
+                call(self._lib, "espp_set_half_cell_int", self._h, halfCellInt)
         self._types = {}
         self._masses = {}
         self.next_id = 0
@@ -468,7 +497,7 @@ class DomainDecomposition:
         return self._cellGrid
 
     def getNodeGrid(self):
-        return Int3D(1, 1, 1)
+        return self._nodeGrid
 
     def _fetch(self, ids):
         n = len(ids)

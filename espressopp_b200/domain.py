@@ -134,6 +134,7 @@ class SpatialDecomposition:
         self.export = {d: {} for d in self.local}
         self.maxDist = 0.0
         self.resorts = 0
+        self.last_resorts = 0  # re-sorts of the last run
         self._ids = np.zeros(0, np.int64)  # sorted ids and their types and masses
         self._type = np.zeros(0, np.int32)
         self._mass = np.zeros(0, np.float64)
@@ -234,6 +235,7 @@ class SpatialDecomposition:
         step the global re-sort decision, migration or halo refresh, force and
         integration."""
         nsteps = int(nsteps)
+        self.last_resorts = 0
         m = self._global_max([self._phase("espp_dd_run_begin", d, nsteps)
                               for d in self.local])
         for _ in range(nsteps):
@@ -242,6 +244,7 @@ class SpatialDecomposition:
             if resort:
                 self.maxDist = 0.0
                 self.resorts += 1
+                self.last_resorts += 1
                 self._load(self.comm.allgather(self._bucket_all(self._collect_owned())))
             else:
                 self._refresh_halo()
@@ -369,6 +372,77 @@ class SpatialDecomposition:
         if len(b):
             call(self.lib, "espp_bonds_add", self.handles[e], len(b) // 2, i64ptr(b))
 
+    # ---- changes of the particle set and state -----------------------------------------
+    def replace_particles(self, ids, pos, vel, img, types=None, mass=None):
+        """Every rank passes the same whole new set (positions as integrated, images as
+        they are); it replaces the particles of all domains, and the next step re-sorts."""
+        ids = np.asarray(ids, np.int64)
+        n = len(ids)
+        if types is not None or mass is not None:
+            known = np.isin(ids, self._ids)
+            new_ids = ids[~known]
+            if len(new_ids):
+                t = np.zeros(n, np.int32) if types is None else np.asarray(types, np.int32)
+                ms = np.ones(n) if mass is None else np.asarray(mass, np.float64)
+                allids = np.concatenate([self._ids, new_ids])
+                order = np.argsort(allids, kind="stable")
+                self._ids = allids[order]
+                self._type = np.concatenate([self._type, t[~known]])[order]
+                self._mass = np.concatenate([self._mass, ms[~known]])[order]
+        held = (ids, np.array(pos, np.float64).reshape(n, 3),
+                np.array(vel, np.float64).reshape(n, 3), np.array(img, np.int32).reshape(n, 3))
+        self._load([self._bucket_all(held)])
+        keep = np.isin(self._ids, ids)
+        self._ids, self._type, self._mass = self._ids[keep], self._type[keep], self._mass[keep]
+
+    def all_particles(self):
+        """(ids, pos, vel, img) of every particle, sorted by id, on every rank."""
+        parts = self.comm.allgather(self._collect_owned())
+        ids = np.concatenate([p[0] for p in parts])
+        order = np.argsort(ids)
+        return tuple(np.concatenate([p[k] for p in parts])[order] for k in range(4))
+
+    def set_velocities(self, ids, vel):
+        ids = np.asarray(ids, np.int64)
+        vel = np.asarray(vel, np.float64).reshape(-1, 3)
+        for d in self.local:
+            sel = np.isin(ids, self.owned[d])
+            if sel.any():
+                call(self.lib, "espp_set_particles", self.handles[d], int(sel.sum()),
+                     i64ptr(np.ascontiguousarray(ids[sel])), None,
+                     dptr(np.ascontiguousarray(vel[sel])))
+
+    def set_images(self, ids, img):
+        ids = np.asarray(ids, np.int64)
+        img = np.asarray(img, np.int32).reshape(-1, 3)
+        for d in self.local:
+            sel = np.isin(ids, self.owned[d])
+            if sel.any():
+                call(self.lib, "espp_set_images", self.handles[d], int(sel.sum()),
+                     i64ptr(np.ascontiguousarray(ids[sel])),
+                     i32ptr(np.ascontiguousarray(img[sel])))
+
+    def set_positions(self, ids, pos):
+        """New positions (taken as they are): the particles may change owner, so the set
+        is redistributed, and the next step re-sorts."""
+        all_ids, p, v, im = self.all_particles()
+        k = np.searchsorted(all_ids, np.asarray(ids, np.int64))
+        p[k] = np.asarray(pos, np.float64).reshape(-1, 3)
+        self.replace_particles(all_ids, p, v, im)
+
+    def step_get(self):
+        v = ctypes.c_int64()
+        call(self.lib, "espp_step_get", self.handles[self.local[0]], ctypes.byref(v))
+        return v.value
+
+    def builds(self):
+        out = []
+        for d in self.local:
+            v = ctypes.c_int64()
+            call(self.lib, "espp_vl_builds", self.handles[d], ctypes.byref(v))
+            out.append(v.value)
+        return int(self._global_max(out))
+
     # ---- observables ----------------------------------------------------------------
     def _sum(self, values):
         return sum(sum(v) for v in self.comm.allgather(values))
@@ -402,6 +476,25 @@ class SpatialDecomposition:
             s = ctypes.c_double()
             k = ctypes.c_int64()
             call(self.lib, "espp_kinetic", self.handles[d], ctypes.byref(s), ctypes.byref(k))
+            v2.append(s.value)
+            n.append(k.value)
+        return self._sum(v2), int(self._sum(n))
+
+    def kinetic_tensor(self):
+        out = []
+        for d in self.local:
+            w = np.zeros(6)
+            call(self.lib, "espp_kinetic_tensor", self.handles[d], dptr(w))
+            out.append(w)
+        return sum(sum(v) for v in self.comm.allgather(out))
+
+    def kinetic_types(self, type_mask):
+        v2, n = [], []
+        for d in self.local:
+            s = ctypes.c_double()
+            k = ctypes.c_int64()
+            call(self.lib, "espp_kinetic_types", self.handles[d], ctypes.c_uint64(type_mask),
+                 ctypes.byref(s), ctypes.byref(k))
             v2.append(s.value)
             n.append(k.value)
         return self._sum(v2), int(self._sum(n))

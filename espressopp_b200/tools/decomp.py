@@ -4,9 +4,13 @@ from ..core import Int3D
 
 def nodeGrid(n=1, box_size=None, rc=None, skin=None, eh_size=0, ratioMS=0, idealGas=0,
              slabMSDims=None):
-    if n != 1:
-        raise ValueError("the GPU storage runs on one node; nodeGrid is (1,1,1)")
-    return Int3D(1, 1, 1)
+    """The node grid for n nodes (tools/decomp.py:28-320).  The GPU storage decomposes
+    space into slabs along z, so n nodes give (1, 1, n); the reference's balanced 3-d
+    factorisation is not used."""
+    n = int(n)
+    if n < 1:
+        raise ValueError("the number of nodes must be positive")
+    return Int3D(1, 1, n)
 
 
 def nodeGridSimple(n=1):

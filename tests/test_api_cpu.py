@@ -37,8 +37,11 @@ def test_fene_potential_matches_reference_tests():
 def test_decomp_cellgrid():
     assert tuple(espressopp.tools.decomp.cellGrid((33.8585,) * 3, (1, 1, 1), 2.5, 0.3)) == (12,) * 3
     assert tuple(espressopp.tools.decomp.cellGrid((36.1033,) * 3, (1, 1, 1), 1.12, 0.3)) == (25,) * 3
+    assert tuple(espressopp.tools.decomp.nodeGrid(2, (10,) * 3, 2.5, 0.3)) == (1, 1, 2)
+    assert tuple(espressopp.tools.decomp.cellGrid((33.8585,) * 3, (1, 1, 2), 2.5, 0.3)) == (
+        12, 12, 6)
     with pytest.raises(ValueError):
-        espressopp.tools.decomp.nodeGrid(2, (10,) * 3, 2.5, 0.3)
+        espressopp.tools.decomp.nodeGrid(0)
 
 
 def test_lattice_and_velocities():

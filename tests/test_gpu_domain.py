@@ -170,3 +170,25 @@ def test_storage_removal_matches_the_oracle():
     assert np.array_equal(oi, gi) and len(gi) == 997 and on == gn
     assert math.isclose(g1, o1, rel_tol=1e-10) and math.isclose(g2, o2, rel_tol=1e-9)
     assert np.max(np.abs(gp - op)) < 1e-9
+
+
+def test_mirror_script_with_two_nodes_on_gpu():
+    """A reference-style script with nodeGrid (1, 1, 2) (two slab systems on one device)
+    against the same script with one node, both on the CUDA library (FP64): energy,
+    temperature, pressure, pair count, re-sorts and trajectory."""
+    import sys as _sys
+    import os as _os
+    _sys.path.insert(0, _os.path.dirname(_os.path.abspath(__file__)))
+    import test_domain_mirror_cpu as m
+    from espressopp_b200 import _lib
+    saved = _lib._lib
+    _lib._lib = cuda_lib()
+    try:
+        one = m._script(1, True)
+        dec = m._script(2, True)
+    finally:
+        _lib._lib = saved
+    assert dec["pairs"] == one["pairs"] and dec["resorts"] == one["resorts"] > 0
+    for k in ("E", "T", "P", "Eb"):
+        assert math.isclose(dec[k], one[k], rel_tol=1e-9, abs_tol=1e-12)
+    assert np.max(np.abs(dec["pos"] - one["pos"])) < 1e-9
