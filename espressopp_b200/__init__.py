@@ -16,8 +16,9 @@ from .core import (FixedPairList, FixedTripleList, Int3D, Real3D, System,  # noq
 from . import analysis, bc, esutil, integrator, interaction, io, storage, tools  # noqa: F401
 from . import standard_system  # noqa: F401
 from .parallel_tempering import ParallelTempering  # noqa: F401
+from ._mpi import MPI  # noqa: F401
 
 __all__ = ["System", "VerletList", "FixedPairList", "FixedTripleList", "Real3D", "Int3D",
            "Tensor", "analysis",
            "bc", "esutil", "integrator", "interaction", "storage", "tools", "standard_system",
-           "set_default_precision", "load_library", "infinity", "ParallelTempering"]
+           "set_default_precision", "load_library", "infinity", "ParallelTempering", "MPI"]

@@ -42,6 +42,8 @@ def test_decomp_cellgrid():
         12, 12, 6)
     with pytest.raises(ValueError):
         espressopp.tools.decomp.nodeGrid(0)
+    # one process without torch.distributed: a world of one
+    assert espressopp.MPI.COMM_WORLD.size == 1 and espressopp.MPI.COMM_WORLD.rank == 0
 
 
 def test_lattice_and_velocities():

@@ -116,6 +116,9 @@ def _rank(rank, world, port, out_dir):
     dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank,
                             world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
+        import espressopp_b200 as espressopp
+        assert espressopp.MPI.COMM_WORLD.size == world
+        assert espressopp.MPI.COMM_WORLD.rank == rank
         res = _script(2, True, steps=100)
         np.save(os.path.join(out_dir, "pos%d.npy" % rank), res["pos"])
         with open(os.path.join(out_dir, "rank%d.txt" % rank), "w") as f:
