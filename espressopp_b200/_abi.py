@@ -61,6 +61,9 @@ PROTOTYPES = {
     "espp_dd_load": (c_int32, [_P, c_int64, _I64, _I32, _D, _D, _D, _I32, _U8]),
     "espp_dd_set_halo_positions": (c_int32, [_P, c_int64, _I64, _D]),
     "espp_dd_run_begin": (c_int32, [_P, c_int64, _D]),
+    "espp_memory_space": (c_int32, [_I32]),
+    "espp_dd_read_positions": (c_int32, [_P, c_int64, _I64, _D]),
+    "espp_dd_write_halo": (c_int32, [_P, c_int64, _I64, _D]),
     "espp_dd_step": (c_int32, [_P, c_int32, _D]),
     "espp_dd_run_end": (c_int32, [_P]),
     "espp_timers": (c_int32, [_P, _D]),

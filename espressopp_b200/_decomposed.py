@@ -10,8 +10,6 @@ state), or summed over the domains (observables).  Entry points that need the wh
 system in one place (angles, the RDF, configurations, the learned potential) raise an
 error naming the limitation.
 """
-import ctypes
-
 import numpy as np
 
 from . import _abi

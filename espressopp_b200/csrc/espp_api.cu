@@ -2463,6 +2463,46 @@ int espp_dd_set_halo_positions(espp_system* s, int64_t n, const int64_t* ids,
   });
 }
 
+int espp_memory_space(int32_t* kind) {
+  return guard([&] {
+    if (!kind) raise(ESPP_EINVAL, "null output pointer");
+    *kind = 1;  // device memory of the system's GPU
+  });
+}
+
+// Halo refresh without host copies: ids and pos are device arrays of the system's GPU.
+int espp_dd_read_positions(espp_system* s, int64_t n, const int64_t* ids, double* pos) {
+  return guard([&] {
+    checked(s);
+    if (n <= 0) return;
+    if (!ids || !pos) raise(ESPP_EINVAL, "null id or position array");
+    if (n > (1LL << 30)) raise(ESPP_ERANGE, "too many ids");
+    ensure_id_map(s);
+    launch_get_by_id(s->view(), (int)n, ids, pos, nullptr, nullptr, nullptr, s->st);
+    unsigned e = read_err(s);  // synchronises the stream: pos is complete on return
+    if (e & kErrIdRange) {
+      cuda_check(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->st), "memset");
+      raise(ESPP_EINVAL, "unknown particle id");
+    }
+  });
+}
+
+int espp_dd_write_halo(espp_system* s, int64_t n, const int64_t* ids, const double* pos) {
+  return guard([&] {
+    checked(s);
+    if (n <= 0) return;
+    if (!ids || !pos) raise(ESPP_EINVAL, "null id or position array");
+    if (n > (1LL << 30)) raise(ESPP_ERANGE, "too many ids");
+    ensure_id_map(s);
+    launch_set_by_id(s->view(), (int)n, ids, pos, nullptr, nullptr, s->st);
+    unsigned e = read_err(s);
+    if (e & kErrIdRange) {
+      cuda_check(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->st), "memset");
+      raise(ESPP_EINVAL, "unknown particle id");
+    }
+  });
+}
+
 int espp_dd_run_begin(espp_system* s, int64_t nsteps, double* maxd) {
   return guard([&] {
     checked(s);

@@ -92,9 +92,17 @@ class SpatialDecomposition:
     system; observables are summed over all domains and returned on every rank."""
 
     def __init__(self, box, skin, cell_grid, ndomains, precision=_abi.PREC_FP64, seed=12345,
-                 comm=None, lib=None, half_cell_int=1):
+                 comm=None, lib=None, half_cell_int=1, exchange="host"):
+        """exchange: how the per-step halo positions travel. "host": through host arrays
+        (espp_get_particles / espp_dd_set_halo_positions, gathered with the communicator);
+        "direct": in buffers of the library's memory space (device memory for the CUDA
+        library), copied between domains of this process and sent between ranks with
+        torch.distributed point-to-point operations (NCCL between GPUs, gloo on CPU)."""
         self.comm = comm or LocalComm()
         self.lib = lib or load_library()
+        if exchange not in ("host", "direct"):
+            raise ValueError("exchange must be 'host' or 'direct'")
+        self.exchange = exchange
         self.box = np.asarray(box, np.float64).copy()
         self.skin = float(skin)
         self.cg = np.asarray(cell_grid, np.int32).copy()
@@ -140,6 +148,9 @@ class SpatialDecomposition:
         self._mass = np.zeros(0, np.float64)
         self._pending = None
         self._bonds = np.zeros((0, 2), np.int64)
+        self._per = per
+        self._xids = {}  # direct exchange: id arrays in the library's memory space
+        self._hids = {}
 
     # ---- set-up -------------------------------------------------------------------
     def add_particles(self, ids, pos, vel=None, types=None, mass=None):
@@ -331,10 +342,29 @@ class SpatialDecomposition:
         for d in self.local:
             self.export[d] = {e: ids for w in gathered for e, per in w.items()
                               for o, ids in per.items() if o == d}
+        if self.exchange == "direct":
+            self._xids = {d: {e: self._space(ids) for e, ids in sorted(self.export[d].items())}
+                          for d in self.local}
+            self._hids = {e: {o: self._space(w) for o, w in sorted(want[e].items())}
+                          for e in self.local}
+
+    def _space(self, a):
+        """A torch tensor with a's contents in the library's memory space."""
+        import torch
+        kind = ctypes.c_int32()
+        call(self.lib, "espp_memory_space", ctypes.byref(kind))
+        dev = torch.device("cuda", torch.cuda.current_device()) if kind.value == 1 else "cpu"
+        return torch.as_tensor(np.ascontiguousarray(a)).to(dev)
+
+    @staticmethod
+    def _ptr(t, ctype):
+        return ctypes.cast(t.data_ptr(), ctypes.POINTER(ctype))
 
     def _refresh_halo(self):
         """Every owner sends the current positions of its particles that other domains
         hold as halo copies (the reference's per-step ghost update)."""
+        if self.exchange == "direct":
+            return self._refresh_halo_direct()
         out = {}
         for d in self.local:
             ex = self.export[d]
@@ -356,6 +386,44 @@ class SpatialDecomposition:
                     if len(ids):
                         call(self.lib, "espp_dd_set_halo_positions", self.handles[e], len(ids),
                              i64ptr(ids), dptr(np.ascontiguousarray(pos)))
+
+    def _refresh_halo_direct(self):
+        """The halo refresh in the library's memory space: positions read into a buffer
+        on the owner, copied or sent (one message per (owner, holder) pair, posted in
+        (owner, holder) order on both sides), written into the holder's halo copies."""
+        import torch
+        c_i64, c_d = ctypes.c_int64, ctypes.c_double
+        sends, recvs = [], []
+        for d in self.local:
+            for e, ids in self._xids[d].items():
+                buf = torch.empty(3 * len(ids), dtype=torch.float64, device=ids.device)
+                call(self.lib, "espp_dd_read_positions", self.handles[d], len(ids),
+                     self._ptr(ids, c_i64), self._ptr(buf, c_d))
+                if e in self.handles:
+                    hid = self._hids[e][d]
+                    call(self.lib, "espp_dd_write_halo", self.handles[e], len(hid),
+                         self._ptr(hid, c_i64), self._ptr(buf, c_d))
+                else:
+                    sends.append((d, e, buf))
+        for e in self.local:
+            for o, hid in self._hids[e].items():
+                if o not in self.handles:
+                    recvs.append((o, e, hid, torch.empty(3 * len(hid), dtype=torch.float64,
+                                                         device=hid.device)))
+        if sends or recvs:
+            dist = self.comm._dist
+            group = self.comm._group
+            reqs = [dist.isend(buf, dst=e // self._per, group=group, tag=d * self.D + e)
+                    for d, e, buf in sends]
+            reqs += [dist.irecv(buf, src=o // self._per, group=group, tag=o * self.D + e)
+                     for o, e, _, buf in sorted(recvs, key=lambda r: (r[0], r[1]))]
+            for r in reqs:
+                r.wait()
+            if recvs and recvs[0][3].is_cuda:
+                torch.cuda.current_stream().synchronize()
+            for o, e, hid, buf in recvs:
+                call(self.lib, "espp_dd_write_halo", self.handles[e], len(hid),
+                     self._ptr(hid, c_i64), self._ptr(buf, c_d))
 
     def _push_bonds(self, e):
         """The bonds with an owned member of domain e; both members must be held."""

@@ -236,6 +236,18 @@ ESPP_API int espp_dd_load(espp_system* s, int64_t n, const int64_t* id, const in
                           const int32_t* img, const uint8_t* halo);
 ESPP_API int espp_dd_set_halo_positions(espp_system* s, int64_t n, const int64_t* ids,
                                         const double* pos);
+/* The memory space of the library's particle arrays: 0 host memory (the CPU oracle),
+ * 1 device memory of the system's GPU (the CUDA library). */
+ESPP_API int espp_memory_space(int32_t* kind);
+/* Halo refresh without host round trips: ids (n) and pos (3n doubles) lie in the
+ * library's memory space (device arrays for the CUDA library), so the positions can move
+ * between domains by NCCL or a device copy.  espp_dd_read_positions copies the positions
+ * of the listed particles out, espp_dd_write_halo moves halo copies to the given
+ * positions; both return when the copy is complete. */
+ESPP_API int espp_dd_read_positions(espp_system* s, int64_t n, const int64_t* ids,
+                                    double* pos);
+ESPP_API int espp_dd_write_halo(espp_system* s, int64_t n, const int64_t* ids,
+                                const double* pos);
 ESPP_API int espp_dd_run_begin(espp_system* s, int64_t nsteps, double* maxd);
 ESPP_API int espp_dd_step(espp_system* s, int32_t resort, double* maxd);
 ESPP_API int espp_dd_run_end(espp_system* s);

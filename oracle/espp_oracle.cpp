@@ -2320,6 +2320,26 @@ int espp_dd_set_halo_positions(espp_system* s, int64_t n, const int64_t* ids,
   return ESPP_OK;
 }
 
+int espp_memory_space(int32_t* kind) {
+  if (!kind) return fail(ESPP_EINVAL, "null output pointer");
+  *kind = 0;  // host memory
+  return ESPP_OK;
+}
+
+int espp_dd_read_positions(espp_system* s, int64_t n, const int64_t* ids, double* pos) {
+  CHECK_S(s);
+  for (int64_t i = 0; i < n; ++i) {
+    const Particle* p = lookup(s, ids[i]);
+    if (!p) return fail(ESPP_EINVAL, "unknown particle id");
+    for (int k = 0; k < 3; ++k) pos[3 * i + k] = p->r[k];
+  }
+  return ESPP_OK;
+}
+
+int espp_dd_write_halo(espp_system* s, int64_t n, const int64_t* ids, const double* pos) {
+  return espp_dd_set_halo_positions(s, n, ids, pos);
+}
+
 int espp_dd_run_begin(espp_system* s, int64_t nsteps, double* maxd) {
   CHECK_S(s);
   ensureAos(s);

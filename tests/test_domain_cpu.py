@@ -44,9 +44,9 @@ def _plain(ids, pos, vel, box, cg, h=1):
     return s
 
 
-def _decomposed(ids, pos, vel, box, cg, D, comm=None, h=1):
+def _decomposed(ids, pos, vel, box, cg, D, comm=None, h=1, exchange="host"):
     dd = SpatialDecomposition(box, SKIN, cg, D, lib=oracle_lib(), seed=4, comm=comm,
-                              half_cell_int=h)
+                              half_cell_int=h, exchange=exchange)
     dd.add_particles(ids, pos, vel)
     dd.decompose()
     dd.vl_create(RC)
@@ -190,7 +190,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _rank(rank, world, port, out_dir, D):
+def _rank(rank, world, port, out_dir, D, exchange):
     import torch.distributed as dist
     for p in (REPO, os.path.join(REPO, "tests")):
         if p not in sys.path:
@@ -200,7 +200,8 @@ def _rank(rank, world, port, out_dir, D):
                             world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
         ids, pos, vel, box = _fluid_inputs(13)
-        dd = _decomposed(ids, pos, vel, box, cell_grid(box, RC, SKIN), D, comm=TorchComm(dist))
+        dd = _decomposed(ids, pos, vel, box, cell_grid(box, RC, SKIN), D, comm=TorchComm(dist),
+                         exchange=exchange)
         dd.run(150)
         x, v, _, img = dd.get_particles(ids)
         out = (dd.local, dd.resorts, dd.vl_digest(), dd.energy(_abi.IA_LJ), dd.kinetic())
@@ -212,16 +213,18 @@ def _rank(rank, world, port, out_dir, D):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("D", [2, 4])
-def test_two_gloo_ranks_match_one_process(tmp_path, D):
+@pytest.mark.parametrize("D,exchange", [(2, "host"), (4, "host"), (4, "direct")])
+def test_two_gloo_ranks_match_one_process(tmp_path, D, exchange):
+    """Also with the halo positions sent point to point in library-space buffers
+    (exchange 'direct': gloo isend/irecv of CPU tensors for the oracle)."""
     ids, pos, vel, box = _fluid_inputs(13)  # 4 cells along z
     cg = cell_grid(box, RC, SKIN)
     ref = _decomposed(ids, pos, vel, box, cg, D)
     ref.run(150)
     xr, vr, _, ir = ref.get_particles(ids)
     port = _free_port()
-    mp.start_processes(_rank, args=(2, port, str(tmp_path), D), nprocs=2, join=True,
-                       start_method="spawn")
+    mp.start_processes(_rank, args=(2, port, str(tmp_path), D, exchange), nprocs=2,
+                       join=True, start_method="spawn")
     held = []
     for r in range(2):
         local, resorts, digest, e, kin = eval((tmp_path / ("rank%d.txt" % r)).read_text())
@@ -233,3 +236,19 @@ def test_two_gloo_ranks_match_one_process(tmp_path, D):
         assert np.array_equal(z["img"], ir)
         held += local
     assert sorted(held) == list(range(D))
+
+
+def test_direct_halo_exchange_in_one_process():
+    """The halo refresh through library-space buffers gives the host-array refresh's
+    trajectory bit for bit (3 domains in one process)."""
+    ids, pos, vel, box = _fluid_inputs(10)
+    cg = cell_grid(box, RC, SKIN)
+    out = []
+    for exchange in ("host", "direct"):
+        dd = _decomposed(ids, pos, vel, box, cg, 3, exchange=exchange)
+        dd.run(120)
+        out.append((dd.get_particles(ids), dd.resorts, dd.vl_digest()))
+    (a, ra, ga), (b, rb, gb) = out
+    assert ra == rb > 0 and ga == gb
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)

@@ -37,8 +37,9 @@ def _plain(lib, prec, ids, pos, vel, box, cg):
     return s
 
 
-def _decomposed(prec, ids, pos, vel, box, cg, D):
-    dd = SpatialDecomposition(box, SKIN, cg, D, precision=prec, seed=4, lib=cuda_lib())
+def _decomposed(prec, ids, pos, vel, box, cg, D, exchange="host"):
+    dd = SpatialDecomposition(box, SKIN, cg, D, precision=prec, seed=4, lib=cuda_lib(),
+                              exchange=exchange)
     dd.add_particles(ids, pos, vel)
     dd.decompose()
     dd.vl_create(RC)
@@ -192,3 +193,22 @@ def test_mirror_script_with_two_nodes_on_gpu():
     for k in ("E", "T", "P", "Eb"):
         assert math.isclose(dec[k], one[k], rel_tol=1e-9, abs_tol=1e-12)
     assert np.max(np.abs(dec["pos"] - one["pos"])) < 1e-9
+
+
+def test_direct_halo_exchange_on_gpu():
+    """The halo refresh in device buffers (espp_dd_read_positions / espp_dd_write_halo,
+    device-to-device, no host copies) gives the host-array refresh's trajectory bit for
+    bit (3 domains on one device, FP64 and mixed)."""
+    ids, pos, vel, box = _inputs(16)
+    cg = cell_grid(box, RC, SKIN)
+    for prec in (_abi.PREC_FP64, _abi.PREC_MIXED):
+        out = []
+        for exchange in ("host", "direct"):
+            dd = _decomposed(prec, ids, pos, vel, box, cg, 3, exchange)
+            dd.run(100)
+            out.append((dd.get_particles(ids), dd.resorts, dd.vl_digest()))
+            dd.close()
+        (a, ra, ga), (b, rb, gb) = out
+        assert ra == rb > 0 and ga == gb
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
