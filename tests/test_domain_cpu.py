@@ -252,3 +252,61 @@ def test_direct_halo_exchange_in_one_process():
     assert ra == rb > 0 and ga == gb
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
+
+
+def test_decomposed_melt_with_tables_exclusions_and_caps(tmp_path):
+    """Tabulated pair and bond potentials (Akima tables of the reference's tabulated
+    test), Verlet-list exclusions of the bonded pairs, Langevin exclusions and a
+    per-component CapForce on a melt over 3 slabs: energies of both tables, pair set,
+    re-sorts and trajectory equal one system's (oracle)."""
+    from espressopp_b200.tools import topology
+    from simdriver import polymer_tab_tables
+    tl, tf, _, _ = polymer_tab_tables(tmp_path, oracle_lib())
+    pos, bonds, L = topology.polymer_melt(12, 30, 0.85, seed=8)
+    box = np.array([L, L, L])
+    ids = np.arange(1, len(pos) + 1, dtype=np.int64)
+    cg = cell_grid(box, 1.12, 0.3)
+    excl = np.asarray(bonds, np.int64)
+    lexcl = ids[::7]
+    cap = np.array([50.0, 60.0, 70.0])
+
+    def setup(s, dd):
+        if dd:
+            s.vl_create(1.12, excl)
+            s.tab_pair_set(0, 0, 2, *tl, 1.12)
+            s.bonds_add(bonds)
+            s.tab_bond_set(2, *tf)
+            s.integrator_set(0.005)
+            s.langevin_set(1, 1.0, 1.0, lexcl)
+            s.capforce_set(_abi.CAP_COMPONENT, cap)
+        else:
+            s.vl(1.12, excl)
+            r, e, f = tl
+            _abi.call(s.lib, "espp_tab_pair_set", s.h, 0, 0, 2, len(r), _abi.dptr(r),
+                      _abi.dptr(e), _abi.dptr(f), 1.12, 0.0)
+            s.bonds(bonds)
+            r, e, f = tf
+            _abi.call(s.lib, "espp_tab_bond_set", s.h, 2, len(r), _abi.dptr(r), _abi.dptr(e),
+                      _abi.dptr(f), math.inf, 0.0)
+            s.integrator(0.005)
+            s.langevin(1.0, 1.0, excl=lexcl)
+            s.capforce(_abi.CAP_COMPONENT, cap)
+
+    ref = Sim(oracle_lib(), box, 0.3, cg, seed=9)
+    ref.add(ids, pos)
+    ref.decompose()
+    setup(ref, False)
+    dd = SpatialDecomposition(box, 0.3, cg, 3, lib=oracle_lib(), seed=9)
+    dd.add_particles(ids, pos)
+    dd.decompose()
+    setup(dd, True)
+    for s in (ref, dd):
+        s.run(80)
+    assert dd.resorts == ref.num_resorts() > 0
+    assert np.array_equal(dd.vl_pairs(), ref.pairs())
+    for which in (_abi.IA_TAB_PAIR, _abi.IA_TAB_BOND):
+        assert math.isclose(dd.energy(which), ref.energy(which), rel_tol=1e-9)
+        assert math.isclose(dd.virial(which), ref.virial(which), rel_tol=1e-8)
+    x, v, _, img = dd.get_particles(ids)
+    xr, vr, _, ir = ref.particles(ids)
+    assert np.max(np.abs(x - xr)) < 1e-8 and np.array_equal(img, ir)
