@@ -351,10 +351,12 @@ class SpatialDecomposition:
     def _space(self, a):
         """A torch tensor with a's contents in the library's memory space."""
         import torch
-        kind = ctypes.c_int32()
-        call(self.lib, "espp_memory_space", ctypes.byref(kind))
-        dev = torch.device("cuda", torch.cuda.current_device()) if kind.value == 1 else "cpu"
-        return torch.as_tensor(np.ascontiguousarray(a)).to(dev)
+        if not hasattr(self, "_device"):
+            kind = ctypes.c_int32()
+            call(self.lib, "espp_memory_space", ctypes.byref(kind))
+            self._device = (torch.device("cuda", torch.cuda.current_device())
+                            if kind.value == 1 else torch.device("cpu"))
+        return torch.as_tensor(np.ascontiguousarray(a)).to(self._device)
 
     @staticmethod
     def _ptr(t, ctype):
