@@ -8,6 +8,7 @@ sums and forces must agree, and a Langevin run must re-sort on the same steps an
 the same trajectory (summation order aside).  The same holds with the domains shared out
 among two gloo ranks (world size 2).
 """
+import ctypes
 import datetime
 import math
 import os
@@ -310,3 +311,33 @@ def test_decomposed_melt_with_tables_exclusions_and_caps(tmp_path):
     x, v, _, img = dd.get_particles(ids)
     xr, vr, _, ir = ref.particles(ids)
     assert np.max(np.abs(x - xr)) < 1e-8 and np.array_equal(img, ir)
+
+
+def test_phase_entry_points_refuse_misuse():
+    """espp_dd_step without a run in progress, a step past the run's end, a halo write
+    to a particle that is not a halo copy: errors with the reason (oracle)."""
+    ids, pos, vel, box = _fluid_inputs(6)
+    cg = cell_grid(box, 1.5, SKIN)
+    s = Sim(oracle_lib(), box, SKIN, cg)
+    s.add(ids, pos, vel)
+    s.decompose()
+    s.vl(1.5)
+    s.integrator(0.005)
+    out = np.zeros(1)
+    with pytest.raises(RuntimeError, match="no step of a decomposed run is pending"):
+        _abi.call(s.lib, "espp_dd_step", s.h, 0, _abi.dptr(out))
+    with pytest.raises(RuntimeError, match="no decomposed run in progress"):
+        _abi.call(s.lib, "espp_dd_run_end", s.h)
+    _abi.call(s.lib, "espp_dd_run_begin", s.h, 1, _abi.dptr(out))
+    assert out[0] > 0.0
+    _abi.call(s.lib, "espp_dd_step", s.h, 0, _abi.dptr(out))
+    assert out[0] == 0.0  # the last step has no integrate1
+    with pytest.raises(RuntimeError, match="no step of a decomposed run is pending"):
+        _abi.call(s.lib, "espp_dd_step", s.h, 0, _abi.dptr(out))
+    _abi.call(s.lib, "espp_dd_run_end", s.h)
+    p = np.zeros(3)
+    with pytest.raises(RuntimeError, match="not a halo particle"):
+        _abi.call(s.lib, "espp_dd_write_halo", s.h, 1, _abi.i64ptr(ids[:1]), _abi.dptr(p))
+    kind = ctypes.c_int32()
+    _abi.call(s.lib, "espp_memory_space", ctypes.byref(kind))
+    assert kind.value == 0
