@@ -81,6 +81,13 @@ def slab_bounds(nz, ndomains):
     return [(d * nz // ndomains, (d + 1) * nz // ndomains) for d in range(ndomains)]
 
 
+class _Failed:
+    """An error of one rank, carried to all ranks by the next gather."""
+
+    def __init__(self, msg):
+        self.msg = msg
+
+
 def _cat(parts, k, shape, dtype):
     return np.concatenate([p[k] for p in parts]) if parts else np.zeros(shape, dtype)
 
@@ -184,8 +191,9 @@ class SpatialDecomposition:
     def decompose(self):
         """Storage.decompose: the particles added so far (and those already held) are
         distributed to their owners, with halo copies."""
-        held = self._collect_owned()
-        parts = self.comm.allgather(self._bucket_all(held))
+        held = self._guarded(self._collect_owned)
+        parts = self.comm.allgather(held if isinstance(held, _Failed) else self._bucket_all(held))
+        self._raise_failed(parts)
         if self._pending is not None:
             # every rank passed the whole set of new particles: each buckets it itself
             parts.append(self._bucket_all(self._pending))
@@ -247,20 +255,26 @@ class SpatialDecomposition:
         integration."""
         nsteps = int(nsteps)
         self.last_resorts = 0
-        m = self._global_max([self._phase("espp_dd_run_begin", d, nsteps)
-                              for d in self.local])
+        m = self._global_max(self._guarded(
+            lambda: [self._phase("espp_dd_run_begin", d, nsteps) for d in self.local]))
         for _ in range(nsteps):
             self.maxDist = self.maxDist + m
             resort = self.maxDist > 0.5 * self.skin
+            pending = None
             if resort:
                 self.maxDist = 0.0
                 self.resorts += 1
                 self.last_resorts += 1
-                self._load(self.comm.allgather(self._bucket_all(self._collect_owned())))
+                held = self._guarded(self._collect_owned)
+                parts = self.comm.allgather(
+                    held if isinstance(held, _Failed) else self._bucket_all(held))
+                self._raise_failed(parts)
+                self._load(parts)
             else:
-                self._refresh_halo()
-            m = self._global_max([self._phase("espp_dd_step", d, int(resort))
-                                  for d in self.local])
+                pending = self._refresh_halo()
+            step = pending if isinstance(pending, _Failed) else self._guarded(
+                lambda: [self._phase("espp_dd_step", d, int(resort)) for d in self.local])
+            m = self._global_max(step)
         for d in self.local:
             call(self.lib, "espp_dd_run_end", self.handles[d])
 
@@ -269,8 +283,25 @@ class SpatialDecomposition:
         call(self.lib, name, self.handles[d], arg, ctypes.byref(out))
         return out.value
 
+    def _guarded(self, fn):
+        """fn's result, or the error it raised as a _Failed value that the next gather
+        turns into an error on every rank (esutil::Error, Error.cpp:52-64: the ranks'
+        errors are collected and thrown together instead of leaving the others waiting)."""
+        try:
+            return fn()
+        except Exception as e:  # noqa: BLE001 - reported to every rank below
+            return _Failed("rank %d: %s" % (self.comm.rank, e))
+
+    @staticmethod
+    def _raise_failed(parts):
+        errs = [p.msg for p in parts if isinstance(p, _Failed)]
+        if errs:
+            raise RuntimeError("; ".join(errs))
+
     def _global_max(self, values):
-        return max(max(v) if v else 0.0 for v in self.comm.allgather(values))
+        parts = self.comm.allgather(values)
+        self._raise_failed(parts)
+        return max(max(v) if v else 0.0 for v in parts)
 
     # ---- migration and halo refresh ----------------------------------------------
     def _lookup(self, ids):
@@ -311,6 +342,24 @@ class SpatialDecomposition:
 
     def _load(self, gathered):
         """Replaces every local domain's particles with the rows sent to it."""
+        failed = self._guarded(lambda: self._load_local(gathered))
+        # who exports what: domain d sends to e the positions of the halo copies e holds
+        # of d's particles (the receivers tell the owners); a load error travels along
+        want = failed if isinstance(failed, _Failed) else {
+            e: {int(o): self.halo[e][0][self.halo[e][1] == o]
+                for o in np.unique(self.halo[e][1])} for e in self.local}
+        gathered = self.comm.allgather(want)
+        self._raise_failed(gathered)
+        for d in self.local:
+            self.export[d] = {e: ids for w in gathered for e, per in w.items()
+                              for o, ids in per.items() if o == d}
+        if self.exchange == "direct":
+            self._xids = {d: {e: self._space(ids) for e, ids in sorted(self.export[d].items())}
+                          for d in self.local}
+            self._hids = {e: {o: self._space(w) for o, w in sorted(want[e].items())}
+                          for e in self.local}
+
+    def _load_local(self, gathered):
         for e in self.local:
             mine = [b[e] for b in gathered if e in b]
             own = [m[0] for m in mine]
@@ -334,19 +383,6 @@ class SpatialDecomposition:
             self.owned[e] = ids_o
             self.halo[e] = (ids_h, src)
             self._push_bonds(e)
-        # who exports what: domain d sends to e the positions of the halo copies e holds
-        # of d's particles (the receivers tell the owners)
-        want = {e: {int(o): self.halo[e][0][self.halo[e][1] == o]
-                    for o in np.unique(self.halo[e][1])} for e in self.local}
-        gathered = self.comm.allgather(want)
-        for d in self.local:
-            self.export[d] = {e: ids for w in gathered for e, per in w.items()
-                              for o, ids in per.items() if o == d}
-        if self.exchange == "direct":
-            self._xids = {d: {e: self._space(ids) for e, ids in sorted(self.export[d].items())}
-                          for d in self.local}
-            self._hids = {e: {o: self._space(w) for o, w in sorted(want[e].items())}
-                          for e in self.local}
 
     def _space(self, a):
         """A torch tensor with a's contents in the library's memory space."""
@@ -364,9 +400,14 @@ class SpatialDecomposition:
 
     def _refresh_halo(self):
         """Every owner sends the current positions of its particles that other domains
-        hold as halo copies (the reference's per-step ghost update)."""
+        hold as halo copies (the reference's per-step ghost update).  Returns None, or a _Failed that the caller passes on to the next gather."""
         if self.exchange == "direct":
             return self._refresh_halo_direct()
+        parts = self.comm.allgather(self._guarded(self._halo_rows))
+        self._raise_failed(parts)
+        return self._guarded(lambda: self._write_halo_rows(parts))
+
+    def _halo_rows(self):
         out = {}
         for d in self.local:
             ex = self.export[d]
@@ -380,7 +421,10 @@ class SpatialDecomposition:
             for e, ids in ex.items():
                 out.setdefault(e, []).append((ids, pos[o:o + len(ids)]))
                 o += len(ids)
-        for part in self.comm.allgather(out):
+        return out
+
+    def _write_halo_rows(self, parts):
+        for part in parts:
             for e, rows in part.items():
                 if e not in self.handles:
                     continue
@@ -396,17 +440,26 @@ class SpatialDecomposition:
         import torch
         c_i64, c_d = ctypes.c_int64, ctypes.c_double
         sends, recvs = [], []
-        for d in self.local:
-            for e, ids in self._xids[d].items():
-                buf = torch.empty(3 * len(ids), dtype=torch.float64, device=ids.device)
-                call(self.lib, "espp_dd_read_positions", self.handles[d], len(ids),
-                     self._ptr(ids, c_i64), self._ptr(buf, c_d))
-                if e in self.handles:
-                    hid = self._hids[e][d]
-                    call(self.lib, "espp_dd_write_halo", self.handles[e], len(hid),
-                         self._ptr(hid, c_i64), self._ptr(buf, c_d))
-                else:
-                    sends.append((d, e, buf))
+
+        def local_part():
+            for d in self.local:
+                for e, ids in self._xids[d].items():
+                    buf = torch.empty(3 * len(ids), dtype=torch.float64, device=ids.device)
+                    call(self.lib, "espp_dd_read_positions", self.handles[d], len(ids),
+                         self._ptr(ids, c_i64), self._ptr(buf, c_d))
+                    if e in self.handles:
+                        hid = self._hids[e][d]
+                        call(self.lib, "espp_dd_write_halo", self.handles[e], len(hid),
+                             self._ptr(hid, c_i64), self._ptr(buf, c_d))
+                    else:
+                        sends.append((d, e, buf))
+
+        failed = self._guarded(local_part)
+        if self.comm.world > 1:
+            # every rank learns of a failed read before any point-to-point message
+            self._raise_failed(self.comm.allgather(failed))
+        elif failed is not None:
+            return failed
         for e in self.local:
             for o, hid in self._hids[e].items():
                 if o not in self.handles:
@@ -423,9 +476,14 @@ class SpatialDecomposition:
                 r.wait()
             if recvs and recvs[0][3].is_cuda:
                 torch.cuda.current_stream().synchronize()
-            for o, e, hid, buf in recvs:
-                call(self.lib, "espp_dd_write_halo", self.handles[e], len(hid),
-                     self._ptr(hid, c_i64), self._ptr(buf, c_d))
+
+            def write_received():
+                for o, e, hid, buf in recvs:
+                    call(self.lib, "espp_dd_write_halo", self.handles[e], len(hid),
+                         self._ptr(hid, c_i64), self._ptr(buf, c_d))
+
+            return self._guarded(write_received)
+        return None
 
     def _push_bonds(self, e):
         """The bonds with an owned member of domain e; both members must be held."""

@@ -341,3 +341,50 @@ def test_phase_entry_points_refuse_misuse():
     kind = ctypes.c_int32()
     _abi.call(s.lib, "espp_memory_space", ctypes.byref(kind))
     assert kind.value == 0
+
+
+def _rank_fails(rank, world, port, out_dir, exchange):
+    import torch.distributed as dist
+    for p in (REPO, os.path.join(REPO, "tests")):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    from espressopp_b200.domain import TorchComm
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank,
+                            world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        ids, pos, vel, box = _fluid_inputs(13)
+        dd = _decomposed(ids, pos, vel, box, cell_grid(box, RC, SKIN), 4, comm=TorchComm(dist),
+                         exchange=exchange)
+        if rank == 1:  # this rank's step 7 raises, as a failing library call would
+            real, count = dd._phase, [0]
+
+            def failing(name, d, arg):
+                if name == "espp_dd_step":
+                    count[0] += 1
+                    if count[0] == 7:
+                        raise RuntimeError("injected failure")
+                return real(name, d, arg)
+            dd._phase = failing
+        try:
+            dd.run(20)
+            msg = "no error"
+        except RuntimeError as e:
+            msg = str(e)
+        with open(os.path.join(out_dir, "rank%d.txt" % rank), "w") as f:
+            f.write(msg)
+    finally:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("exchange", ["host", "direct"])
+def test_a_failing_rank_raises_on_every_rank(tmp_path, exchange):
+    """Failure detection (esutil::Error, Error.cpp:52-64), made on the host: a library
+    error on one rank in the middle of a run reaches both gloo ranks as the same error at
+    the next gather, instead of leaving the other rank waiting."""
+    port = _free_port()
+    mp.start_processes(_rank_fails, args=(2, port, str(tmp_path), exchange), nprocs=2,
+                       join=True, start_method="spawn")
+    for r in range(2):
+        msg = (tmp_path / ("rank%d.txt" % r)).read_text()
+        assert "rank 1: injected failure" in msg
