@@ -388,3 +388,37 @@ def test_a_failing_rank_raises_on_every_rank(tmp_path, exchange):
     for r in range(2):
         msg = (tmp_path / ("rank%d.txt" % r)).read_text()
         assert "rank 1: injected failure" in msg
+
+
+@pytest.mark.parametrize("h,slabs", [(1, 5), (2, "one cell each")])
+def test_thin_and_uneven_slabs(h, slabs):
+    """Slabs of one cell layer at halfCellInt 2 (each halo layer then comes from two
+    neighbouring domains on either side) and uneven slabs (8 layers over 5 domains): the
+    run equals one system's (oracle, direct halo refresh)."""
+    rc = 1.5
+    shift = 4.0 * (rc ** -12 - rc ** -6)
+    pos, box = lattice(14, 0.8442, 0.05, 3)
+    vel = mb_velocities(len(pos), 1.0, 4)
+    ids = np.arange(len(pos), dtype=np.int64)
+    cg = cell_grid(box, rc, SKIN, h)
+    D = int(cg[2]) if slabs == "one cell each" else slabs
+    ref = Sim(oracle_lib(), box, SKIN, cg, seed=4, half_cell_int=h)
+    ref.add(ids, pos, vel)
+    ref.decompose()
+    ref.vl(rc)
+    ref.lj(0, 0, 1.0, 1.0, rc, shift)
+    ref.integrator(0.005)
+    ref.langevin(1.0, 1.0)
+    dd = SpatialDecomposition(box, SKIN, cg, D, lib=oracle_lib(), seed=4, half_cell_int=h,
+                              exchange="direct")
+    dd.add_particles(ids, pos, vel)
+    dd.decompose()
+    dd.vl_create(rc)
+    dd.lj_set(0, 0, 1.0, 1.0, rc, shift)
+    dd.integrator_set(0.005)
+    dd.langevin_set(1, 1.0, 1.0)
+    for s in (ref, dd):
+        s.run(150)
+    assert dd.resorts == ref.num_resorts() > 10
+    assert dd.vl_digest() == ref.digest()
+    assert np.max(np.abs(dd.get_particles(ids)[0] - ref.particles(ids)[0])) < 1e-9
